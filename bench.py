@@ -1,0 +1,458 @@
+"""Benchmark: LBVH build + progressive path tracing on one B200 (or N, one process each).
+
+Workload (default, "c2"): 4,194,304-triangle fBm-displaced lat-long sphere
+(2048 x 1024 quads) + 1,048,576 thin "hairball" triangles + a 2-triangle quad
+emitter = 5,242,882 triangles, 63-bit Morton LBVH, 1920 x 1080, 16 samples per
+pixel per frame, depth 8 (7 indirect bounces), Philox random stream. Synthetic
+scene, generated on the host from a fixed seed.
+
+One step = one progressive frame (16 spp) rendered with the BVH resident in HBM.
+`value` is rays traced (primary + extension + shadow, counted on the device) per
+second over the K timed frames, max over ranks. The LBVH build of the same scene
+is timed separately (`lbvh`). `e2e` is the same metric through the
+reference-facing tracer object with host buffers: every step uploads the scene
+(triangles + shading records, pinned host memory), rebuilds the LBVH, renders the
+frame and reads the image back.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2|c1]
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "cuda-path-tracer_b200"))
+
+WORKLOADS = {
+    "c2": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
+               bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0),
+    "c1": dict(kind="random", n=65536, bits=30, width=512, height=512, spp=1, bounces=3, eye=(0.5, 0.5, -1.2),
+               target=(0.5, 0.5, 0.0), seed=0),
+}
+METRIC = "Mrays/s"
+
+
+def make_scene(w):
+    import cpt
+
+    if w["kind"] == "random":
+        return cpt.scene_random(w["n"], seed=w["seed"])
+    return cpt.scene_sphere_hairball(w["nu"], w["nv"], w["n_hair"], seed=w["seed"])
+
+
+def workload_config(name, w, n_tris, l2_note):
+    c = {"workload": f"{name}: " + ("fBm sphere 2048x1024x2 + 1M hairball + quad light" if name == "c2"
+                                     else "65,536 random triangles + quad light"),
+         "triangles": int(n_tris), "morton_bits": w["bits"], "resolution": f'{w["width"]}x{w["height"]}',
+         "spp_per_step": w["spp"], "depth": w["bounces"] + 1, "l2": l2_note}
+    return c
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def dist_setup(n_gpus):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------- CPU baseline
+def cpu_reference_run(w, tris, infos, cam, bits, target_s=12.0, rows_hint=None):
+    """The reference's own builder (oracle/_ref, OpenMP over all host threads) on the
+    full scene, then its trace functions inside the restated integrator on a band
+    of rows, sized for ~target_s seconds. Falls back to the oracle port."""
+    from oracle import cpu
+
+    threads = os.cpu_count() or 1
+    kind = "reference" if cpu.ref_available(bits) else "port"
+    t0 = time.perf_counter()
+    b = cpu.build(tris, bits, use_ref=(kind == "reference"))
+    build_s = time.perf_counter() - t0
+    width, height, spp = w["width"], w["height"], w["spp"]
+    mid = height // 2
+    cam15 = cam.as_array()
+
+    def run(rows):
+        r0 = max(0, mid - rows // 2)
+        r1 = min(height, r0 + rows)
+        t1 = time.perf_counter()
+        if kind == "reference":
+            _, cnt = cpu.ref_render(b, infos, None, width, height, (r0, r1), spp, 0, w["bounces"], 3.0, True,
+                                    w["seed"], cam15, threads)
+        else:
+            _, cnt = cpu.render(b, infos, None, width, height, spp, 0, w["bounces"], 3.0, True, w["seed"],
+                                cpu.ocam_from(cam.eye, cam15[3:]), rows=(r0, r1))
+        return time.perf_counter() - t1, int(cnt.sum()), r1 - r0
+
+    rows = rows_hint
+    if rows is None:
+        dt, _, _ = run(1)
+        rows = int(max(1, min(height, target_s / max(dt, 1e-3))))
+    dt, rays, rows = run(rows)
+    return {"kind": kind, "threads": threads, "build_s": build_s, "build_mtris_s": len(tris) / build_s / 1e6,
+            "render_s": dt, "rays": rays, "rows": rows, "mrays_s": rays / dt / 1e6,
+            "sample": f"{rows} of {height} rows (centre band) x {width} px x {spp} spp, depth {w['bounces'] + 1}; "
+                      f"build of all {len(tris)} triangles"}
+
+
+def run_reference_arm(args, w, world, rank):
+    if rank != 0:
+        return 0
+    import cpt
+
+    t0 = time.perf_counter()
+    tris, infos = make_scene(w)
+    gen_s = time.perf_counter() - t0
+    cam = cpt.camera_look_at(w["eye"], w["target"], fov_deg=45.0, aspect=w["width"] / w["height"])
+    # size one step for ~8 s of CPU work, then warm up and time K steps of that size
+    probe = cpu_reference_run(w, tris, infos, cam, w["bits"], target_s=8.0)
+    rows = probe["rows"]
+    for _ in range(max(0, args.warmup - 1)):
+        cpu_reference_run(w, tris, infos, cam, w["bits"], rows_hint=rows)
+    rays = 0
+    secs = 0.0
+    last = probe
+    for _ in range(args.steps):
+        last = cpu_reference_run(w, tris, infos, cam, w["bits"], rows_hint=rows)
+        rays += last["rays"]
+        secs += last["render_s"]
+    value = rays / secs / 1e6
+    line = {"metric": METRIC, "value": round(value, 4), "unit": METRIC, "impl": "reference", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * secs / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded host generator)",
+            "config": workload_config(args.workload, w, len(tris), "n/a (CPU)"),
+            "cpu_baseline": {"value": round(value, 4), "unit": METRIC, "cores": last["threads"], "kind": last["kind"],
+                             "sample": last["sample"]},
+            "lbvh": {"mtris_s": round(last["build_mtris_s"], 3), "ms": round(1e3 * last["build_s"], 3)},
+            "e2e": {"value": round(value, 4), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "scene_gen_s": round(gen_s, 2)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- our arm
+def run_ours(args, w, world, rank, local):
+    import torch
+
+    import cpt
+    from cpt.device import DeviceLbvh, DeviceRenderer, DeviceScene, make_params, stream_handle, to_device
+
+    dev = torch.device("cuda", local if world > 1 else 0)
+    t0 = time.perf_counter()
+    tris, infos = make_scene(w)
+    gen_s = time.perf_counter() - t0
+    n = len(tris)
+    W_, H_, spp = w["width"], w["height"], w["spp"]
+    cam = cpt.camera_look_at(w["eye"], w["target"], fov_deg=45.0, aspect=W_ / H_)
+    d_tris = to_device(tris, dev)
+    scene = DeviceScene(infos, None, dev)
+    lb = DeviceLbvh(n, w["bits"], dev)
+    lb.build(d_tris, check_root=True)
+    params = make_params(W_, H_, spp, 0, w["bounces"], 3.0, True, w["seed"] + 7919 * rank, cpt.ACCUM_KAHAN)
+    rend = DeviceRenderer(params, dev)
+    stream = torch.cuda.current_stream()
+
+    # --- one instrumented frame: node fetches and triangle tests per closest-hit ray
+    rend.reset()
+    rend.render(lb, scene, cam, frame0=0, trace_stats=True)
+    torch.cuda.synchronize()
+    rend.check_status()
+    c = rend.counts.cpu().numpy()
+    inst_rays_closest = int(c[0] + c[1])
+    mean_nodes = c[3] / max(inst_rays_closest, 1)
+    mean_tris = c[4] / max(inst_rays_closest, 1)
+
+    # --- warm-up frames
+    rend.reset()
+    frame = 0
+    for _ in range(args.warmup):
+        rend.render(lb, scene, cam, frame0=frame + rank * 1_000_000)
+        frame += spp
+    torch.cuda.synchronize()
+    rend.counts.zero_()
+
+    # --- timed frames
+    sampler = ClockSampler(local if world > 1 else 0) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    launches0 = cpt.launch_count()
+    barrier(world)
+    torch.cuda.synchronize()
+    cpt.profile_begin()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for k in range(args.steps):
+        rend.render(lb, scene, cam, frame0=frame + rank * 1_000_000)
+        frame += spp
+        if world > 1:  # the one exchange of the path: framebuffer reduce to rank 0 every frame
+            import torch.distributed as dist
+
+            dist.reduce(rend.accum.view(torch.float32), dst=0)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    prof = cpt.profile_end()
+    barrier(world)
+    launches = cpt.launch_count() - launches0
+    clocks = sampler.stop() if sampler else None
+    rend.check_status()
+    ms_total = ev0.elapsed_time(ev1)
+    counts = rend.counts.cpu().numpy()
+    rays_local = int(counts[0] + counts[1] + counts[2])
+    ms_max = max_over_ranks(ms_total, world)
+    rays_all = sum_over_ranks(rays_local, world)
+    value = rays_all / (ms_max / 1e3) / 1e6
+
+    # --- roofline of the dominant kernel (closest-hit traversal, k_extend)
+    ext_ms, ext_launches = prof.get("k_extend", (0.0, 0))
+    rays_closest = int(counts[0] + counts[1])
+    alg_bytes = rays_closest * (32 + 16) + rays_closest * (64.0 * mean_nodes + 48.0 * mean_tris)
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "k_extend_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tj = json.load(f)
+        traffic = round(float(tj["dram_bytes_per_closest_ray"]) * rays_closest / max(ext_launches, 1), 1)
+    roofline = {"bound": "hbm", "kernel": "k_extend", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6650 GB/s",
+                "traffic": traffic, "algorithmic_bytes_per_launch": round(alg_bytes / max(ext_launches, 1), 1),
+                "avg_launch_ms": round(ext_ms / max(ext_launches, 1), 4),
+                "bytes_per_ray": f"32 ray + 16 hit + 64 x {mean_nodes:.2f} nodes + 48 x {mean_tris:.2f} triangles",
+                "kernel_share": {k: round(v[0] / ms_total, 4) for k, v in sorted(prof.items())}}
+
+    # --- LBVH build of the same scene (device-resident triangles)
+    for _ in range(max(3, args.warmup)):
+        lb.build(d_tris)
+    torch.cuda.synchronize()
+    nb = max(5, args.steps)
+    cpt.profile_begin()
+    b0 = torch.cuda.Event(enable_timing=True)
+    b1 = torch.cuda.Event(enable_timing=True)
+    b0.record(stream)
+    for _ in range(nb):
+        lb.build(d_tris)
+    b1.record(stream)
+    torch.cuda.synchronize()
+    bprof = cpt.profile_end()
+    lb.status()
+    build_ms = max_over_ranks(b0.elapsed_time(b1) / nb, world)
+    key_bytes = 4 if w["bits"] == 30 else 8
+    passes = 4 if w["bits"] == 30 else 8
+    # algorithmic bytes per triangle: Morton 36 in + K+4 out, histogram K, sort 2P(K+4),
+    # gather 40+40, topology K + 4 + 8, refit 8 + 36 + 8 + 4 + 24, plus the 64-B node and 48-B record
+    bpt = 36 + key_bytes + 4 + key_bytes + 2 * passes * (key_bytes + 4) + 80 + key_bytes + 12 + 80 + 64 + 48
+    b_ach = n * bpt / (build_ms / 1e3) / 1e9
+    lbvh = {"mtris_s": round(n / build_ms / 1e3, 2), "ms": round(build_ms, 4),
+            "roofline": {"bound": "hbm", "achieved": round(b_ach, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(b_ach / peak, 4), "bytes_per_triangle": bpt},
+            "kernel_ms_per_build": {k: round(v[0] / nb, 4) for k, v in sorted(bprof.items())}}
+
+    # --- end to end through the tracer object (host buffers, pinned)
+    e2e = None
+    if rank == 0 or world > 1:
+        tr = cpt.Tracer(w["bits"])
+        tr.set_settings(bounces=w["bounces"], intensity=3.0, stratified=True, seed=w["seed"] + 7919 * rank)
+        tr.set_camera(cam)
+        h_tris = torch.empty(tris.nbytes, dtype=torch.uint8, pin_memory=True)
+        h_tris.numpy()[:] = tris.view(np.uint8)
+        h_infos = torch.empty(infos.nbytes, dtype=torch.uint8, pin_memory=True)
+        h_infos.numpy()[:] = infos.view(np.uint8)
+        h_img = torch.empty(W_ * H_ * 16, dtype=torch.uint8, pin_memory=True)
+        lib = cpt.lib
+
+        def e2e_step():
+            cpt.check(lib.cpt_tracer_upload(tr._h, h_tris.data_ptr(), n, h_infos.data_ptr(), n, None, 0, None),
+                      "upload")
+            tr.raytrace(W_, H_, spp)
+            cpt.check(lib.cpt_tracer_read_image(tr._h, h_img.data_ptr()), "read_image")
+
+        for _ in range(max(1, min(args.warmup, 2))):
+            e2e_step()
+        ts = torch.cuda.ExternalStream(tr.stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        ne = max(2, min(args.steps, 5))
+        c0 = tr.ray_counts()
+        w0 = time.perf_counter()
+        e0.record(ts)
+        for _ in range(ne):
+            e2e_step()
+        e1.record(ts)
+        e1.synchronize()
+        wall = time.perf_counter() - w0
+        c1 = tr.ray_counts()
+        e_ms = e0.elapsed_time(e1)
+        e_rays = float(c1.sum()) if c1.sum() < c0.sum() else float((c1 - c0).sum())
+        e_ms_max = max_over_ranks(e_ms, world)
+        e_rays_all = sum_over_ranks(e_rays, world)
+        e2e = {"value": round(e_rays_all / (e_ms_max / 1e3) / 1e6, 3), "unit": METRIC,
+               "h2d_bytes_per_step": int(tris.nbytes + infos.nbytes), "d2h_bytes_per_step": int(W_ * H_ * 16),
+               "ms_per_step": round(e_ms_max / ne, 3), "wall_ms_per_step": round(1e3 * wall / ne, 3),
+               "steps": ne, "includes": "H2D soup+shading records (pinned), LBVH build, 16-spp frame, D2H image"}
+        tr.close()
+
+    # --- CPU baseline (rank 0, N = 1)
+    cpu_base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference_run(w, tris, infos, cam, w["bits"], target_s=args.cpu_seconds)
+        cpu_base = {"value": round(r["mrays_s"], 4), "unit": METRIC, "cores": r["threads"], "kind": r["kind"],
+                    "sample": r["sample"], "build_mtris_s": round(r["build_mtris_s"], 3)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded host generator)",
+                "config": workload_config(args.workload, w, n, "scene arrays 1.4 GB > 126 MB L2, no flush needed"),
+                "rays_per_step": int(rays_all / args.steps), "roofline": roofline, "lbvh": lbvh,
+                "cpu_baseline": cpu_base, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+                "parallelism": f"replicas x{world}: own BVH per GPU, disjoint sample streams, "
+                               f"framebuffer reduce to rank 0 per frame" if world > 1 else "1 GPU",
+                "scene_gen_s": round(gen_s, 2)}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        return run_reference_arm(args, w, world, rank)
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        return run_ours(args, w, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,143 @@
+"""Device-memory plumbing for the C ABI using torch tensors as allocations.
+
+torch provides the allocator, the stream and (for several GPUs) torch.distributed;
+all compute is in libcpt.so. Buffers are uint8 tensors on the current CUDA device;
+their addresses go to the library.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import (ACCUM_KAHAN, BBOX_DTYPE, BUILD_CHECK, TRIANGLE_DTYPE, Bvh, Camera, RenderParams, Scene, accum_bytes,
+               bvh_bind, bvh_bytes, check, lbvh_build, lbvh_scratch_bytes, lib, render, render_scratch_bytes, resolve,
+               status_check, trace)
+
+
+def stream_handle(stream: torch.cuda.Stream | None = None) -> int:
+    s = stream or torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def dev_bytes(nbytes: int, device=None) -> torch.Tensor:
+    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=device or "cuda")
+
+
+def to_device(a: np.ndarray, device=None) -> torch.Tensor:
+    """Copy a numpy array (any dtype) into a fresh uint8 device tensor."""
+    flat = np.ascontiguousarray(a).view(np.uint8).reshape(-1)
+    return torch.from_numpy(flat.copy()).to(device or "cuda")
+
+
+def to_host(t: torch.Tensor, dtype, count: int | None = None, offset_bytes: int = 0) -> np.ndarray:
+    raw = t.detach().cpu().numpy().view(np.uint8)
+    dt = np.dtype(dtype)
+    n = (raw.size - offset_bytes) // dt.itemsize if count is None else count
+    return raw[offset_bytes:offset_bytes + n * dt.itemsize].view(dt).copy()
+
+
+class DeviceLbvh:
+    """A built LBVH in device memory: one allocation for the outputs, one for scratch."""
+
+    def __init__(self, n: int, bits: int, device=None):
+        self.n, self.bits = int(n), int(bits)
+        self.mem = dev_bytes(bvh_bytes(self.n, self.bits), device)
+        self.scratch_bytes = lbvh_scratch_bytes(self.n, self.bits)
+        self.scratch = dev_bytes(self.scratch_bytes, device)
+        self.bvh: Bvh = bvh_bind(self.mem.data_ptr(), self.mem.numel(), self.n, self.bits)
+
+    def build(self, tris: torch.Tensor | int, box=None, check_root: bool = False, stream: int | None = None) -> None:
+        ptr = tris if isinstance(tris, int) else tris.data_ptr()
+        lbvh_build(ptr, self.n, self.bits, self.bvh, self.scratch.data_ptr(), self.scratch_bytes, box=box,
+                   flags=BUILD_CHECK if check_root else 0, stream=stream_handle() if stream is None else stream)
+
+    def status(self, stream: int | None = None) -> None:
+        status_check(self.bvh.status, stream_handle() if stream is None else stream)
+
+    def download(self) -> dict:
+        """Reference-format arrays plus the compact records, as numpy."""
+        n, b = self.n, self.bvh
+        base = self.mem.data_ptr()
+
+        def get(ptr, dtype, count):
+            off = ptr - base
+            nbytes = np.dtype(dtype).itemsize * count
+            return self.mem[off:off + nbytes].cpu().numpy().view(dtype).copy()
+
+        return {
+            "tris": get(b.tris, TRIANGLE_DTYPE, n),
+            "keys": get(b.keys, np.uint32 if self.bits == 30 else np.uint64, n),
+            "children": get(b.children, np.uint32, n - 1),
+            "parents_leaf": get(b.parents_leaf, np.uint32, n),
+            "parents_internal": get(b.parents_internal, np.uint32, n - 1),
+            "node_boxes": get(b.node_boxes, BBOX_DTYPE, n - 1),
+            "nodes": get(b.nodes, np.float32, 16 * (n - 1)).reshape(n - 1, 16),
+            "tri_records": get(b.tri_records, np.float32, 12 * n).reshape(n, 12),
+        }
+
+    def trace(self, rays: torch.Tensor, any_hit: bool = False, stats: bool = False):
+        """rays: float32 device tensor (m, 8). Returns (hits (m,4) float32 tensor, stats (m,2) int32 or None)."""
+        m = rays.shape[0]
+        hits = torch.empty((m, 4), dtype=torch.float32, device=rays.device)
+        st = torch.zeros((m, 2), dtype=torch.int32, device=rays.device) if stats else None
+        trace(self.bvh, rays.data_ptr(), m, any_hit, hits.data_ptr(), st.data_ptr() if stats else 0, stream_handle())
+        return hits, st
+
+
+class DeviceScene:
+    """Shading inputs (TriangleInfo records, directional lights) in device memory."""
+
+    def __init__(self, infos: np.ndarray, lights: np.ndarray | None = None, device=None):
+        self.infos = to_device(infos, device)
+        self.n_infos = len(infos)
+        self.n_lights = 0 if lights is None else len(lights)
+        self.lights = to_device(lights, device) if self.n_lights else None
+        self.scene = Scene(self.infos.data_ptr(), self.n_infos, self.lights.data_ptr() if self.n_lights else None,
+                           self.n_lights)
+
+
+def make_params(width, height, spp, frame0=0, bounces=3, intensity=3.0, stratified=True, seed=0,
+                accum_mode=ACCUM_KAHAN, ref_grid=False, wave_paths=0, trace_stats=False) -> RenderParams:
+    return RenderParams(width, height, spp, frame0, bounces, intensity, int(stratified), seed & 0xFFFFFFFF,
+                        (seed >> 32) & 0xFFFFFFFF, accum_mode, int(ref_grid), wave_paths, int(trace_stats))
+
+
+class DeviceRenderer:
+    """Accumulator + wave scratch for one image size / mode."""
+
+    def __init__(self, params: RenderParams, device=None):
+        self.params = params
+        self.accum = dev_bytes(accum_bytes(params.width, params.height, params.accum_mode), device)
+        self.accum.zero_()
+        self.scratch_bytes = render_scratch_bytes(params)
+        if not self.scratch_bytes:
+            raise ValueError("render parameters rejected")
+        self.scratch = dev_bytes(self.scratch_bytes, device)
+        self.counts = torch.zeros(8, dtype=torch.int64, device=device or "cuda")
+        self.status = torch.zeros(4, dtype=torch.int32, device=device or "cuda")
+        self.image = torch.empty((params.height, params.width, 4), dtype=torch.float32, device=device or "cuda")
+
+    def reset(self) -> None:
+        self.accum.zero_()
+        self.counts.zero_()
+        self.status.zero_()
+
+    def render(self, lbvh: DeviceLbvh, scene: DeviceScene, cam: Camera, spp: int | None = None,
+               frame0: int | None = None, trace_stats: bool | None = None) -> None:
+        p = RenderParams.from_buffer_copy(self.params)
+        if spp is not None:
+            p.spp = spp
+        if frame0 is not None:
+            p.frame0 = frame0
+        if trace_stats is not None:
+            p.trace_stats = int(trace_stats)
+        render(lbvh.bvh, scene.scene, cam, p, self.accum.data_ptr(), self.scratch.data_ptr(), self.scratch_bytes,
+               self.counts.data_ptr(), self.status.data_ptr(), stream_handle())
+
+    def resolve(self) -> torch.Tensor:
+        p = self.params
+        resolve(self.accum.data_ptr(), p.width, p.height, p.accum_mode, self.image.data_ptr(), stream_handle())
+        return self.image
+
+    def check_status(self) -> None:
+        status_check(self.status.data_ptr(), stream_handle())

@@ -1,0 +1,726 @@
+// LBVH construction for sm_100a: Morton codes, onesweep radix sort, Karras
+// topology, atomic bottom-up refit.
+//
+// Replaces CUDA::BVHBuilder::build (source/application/cuda/BVHBuilder.cu:207-269)
+// and its four thrust passes. Outputs are the reference's arrays, bit for bit,
+// plus the compact traversal records used by trace.cu / render.cu:
+//
+//   kernel             reference                               reads / writes per triangle
+//   k_bounds*          caller's enclosingBBox (PathTracingApp.cpp:113), optional
+//   k_morton           morton_encoder (BVHBuilder.cu:12-32)    40 B tri -> K B key, digit histograms
+//   k_scan_offsets     (part of thrust::sort_by_key)           P x 256 counters
+//   k_onesweep x P     thrust::sort_by_key (BVHBuilder.cu:234) K+4 B in, K+4 B out per pass
+//   k_topology         radix_tree_construction_kernel (:107-201) keys -> Node, parents
+//   k_gather_refit     compute_internal_node_bbox_kernel (:39-98) + the triangle permutation
+//
+// The sort is a least-significant-digit radix sort with 8-bit digits in the
+// onesweep form (one global histogram pass, then one pass per digit in which each
+// tile ranks its keys with warp-level match/popc scans and finds its output base
+// by decoupled look-back over the preceding tiles). LSD radix sorting is stable,
+// which reproduces thrust's stable sort_by_key order for equal keys. The
+// look-back wait is bounded: after kLookbackPolls polls it records
+// CPT_STATUS_TIMEOUT and proceeds, so no launch can hang.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+#include <algorithm>
+#include "cpt.h"
+#include "cpt_device.cuh"
+#include "cpt_internal.h"
+
+namespace cpt {
+
+constexpr int kRadix = 256;
+constexpr int kSortBlock = 256;  // one thread per digit in the per-tile digit work
+constexpr int kSortWarps = kSortBlock / 32;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortBlock * kSortItems;  // 4096 keys per tile
+constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kValueMask = (1u << 30) - 1;
+constexpr uint32_t kLookbackPolls = 1u << 22;
+constexpr int kMortonBlock = 256;
+constexpr int kBoundsBlock = 256;
+constexpr int kBoundsBlocks = 1024;
+
+template <typename K> struct KeyTraits;
+template <> struct KeyTraits<uint32_t> { static constexpr int passes = 4, order = 10, total_bits = 32; };
+template <> struct KeyTraits<uint64_t> { static constexpr int passes = 8, order = 21, total_bits = 64; };
+
+// Bit spreading for the 3-D interleave (x -> bit 3i, y -> 3i+1, z -> 3i+2, the
+// layout of morton.h:63-102): the standard shift-and-mask "part 1 by 2" sequence
+// on 64 bits, valid for inputs of up to 21 bits.
+__device__ __forceinline__ uint64_t spread3(uint32_t v)
+{
+    uint64_t x = v & 0x1FFFFFull;
+    x = (x | (x << 32)) & 0x001F00000000FFFFull;
+    x = (x | (x << 16)) & 0x001F0000FF0000FFull;
+    x = (x | (x << 8)) & 0x100F00F00F00F00Full;
+    x = (x | (x << 4)) & 0x10C30C30C30C30C3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+
+// quantize (math_util.h:10-13): clamp(int(x * n), 0, n - 1); cvt.rzi saturates and maps NaN to 0.
+__device__ __forceinline__ uint32_t quantize(float x, uint32_t n)
+{
+    int32_t q = __float2int_rz(__fmul_rn(x, (float)n));
+    int32_t hi = (int32_t)(n - 1);
+    q = q < hi ? q : hi;
+    return (uint32_t)(q > 0 ? q : 0);
+}
+
+struct BoxArg {
+    float mn[3];
+    float inv[3];
+    const float* dev;  // device box (min, max) when the host gave none
+};
+
+// ---------------------------------------------------------------------------
+// Enclosing box on the device (when the caller passes none): per-block partial
+// boxes, then one block folds them in a fixed order.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBoundsBlock) k_bounds_partial(const float* __restrict__ tris, uint32_t n,
+                                                                 float* __restrict__ partial)
+{
+    float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* t = tris + 10ull * i;
+#pragma unroll
+        for (int v = 0; v < 3; ++v)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                float c = t[3 * v + a];
+                mn[a] = gmin(mn[a], c);
+                mx[a] = gmax(mx[a], c);
+            }
+    }
+    __shared__ float s[6][kBoundsBlock];
+    for (int a = 0; a < 3; ++a) { s[a][threadIdx.x] = mn[a]; s[3 + a][threadIdx.x] = mx[a]; }
+    __syncthreads();
+    for (int w = kBoundsBlock / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            for (int a = 0; a < 3; ++a) {
+                s[a][threadIdx.x] = gmin(s[a][threadIdx.x], s[a][threadIdx.x + w]);
+                s[3 + a][threadIdx.x] = gmax(s[3 + a][threadIdx.x], s[3 + a][threadIdx.x + w]);
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) partial[6 * blockIdx.x + threadIdx.x] = s[threadIdx.x][0];
+}
+
+__global__ void k_bounds_final(const float* __restrict__ partial, int blocks, float* __restrict__ box)
+{
+    if (threadIdx.x != 0) return;
+    float b[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int i = 0; i < blocks; ++i)
+        for (int a = 0; a < 3; ++a) {
+            b[a] = gmin(b[a], partial[6 * i + a]);
+            b[3 + a] = gmax(b[3 + a], partial[6 * i + 3 + a]);
+        }
+    for (int a = 0; a < 6; ++a) box[a] = b[a];
+}
+
+// ---------------------------------------------------------------------------
+// Morton codes + per-pass digit histograms + zeroing of the sort's look-back
+// state. One key per triangle: centroid (v0 + v1 + v2) / 3 quantized to
+// 2^order cells per axis of the enclosing box (BVHBuilder.cu:19-28).
+// ---------------------------------------------------------------------------
+template <typename K>
+__global__ void __launch_bounds__(kMortonBlock) k_morton(const float* __restrict__ tris, uint32_t n, BoxArg box,
+                                                         K* __restrict__ keys, uint32_t* __restrict__ hist,
+                                                         uint32_t* __restrict__ zero, size_t zero_words,
+                                                         uint32_t* __restrict__ status)
+{
+    constexpr int P = KeyTraits<K>::passes;
+    constexpr int order = KeyTraits<K>::order;
+    __shared__ uint32_t s_hist[P * kRadix];
+    __shared__ float s_box[6];
+    for (int i = threadIdx.x; i < P * kRadix; i += blockDim.x) s_hist[i] = 0;
+    if (threadIdx.x < 3) {
+        if (box.dev) {
+            float mn = box.dev[threadIdx.x], mx = box.dev[3 + threadIdx.x];
+            s_box[threadIdx.x] = mn;
+            s_box[3 + threadIdx.x] = __frcp_rn(__fsub_rn(mx, mn));  // 1.0f / scale (BVHBuilder.cu:17)
+        } else {
+            s_box[threadIdx.x] = box.mn[threadIdx.x];
+            s_box[3 + threadIdx.x] = box.inv[threadIdx.x];
+        }
+    }
+    const size_t gtid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t gsize = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = gtid; i < zero_words; i += gsize) zero[i] = 0;
+    __syncthreads();
+    const uint32_t cells = 1u << order;
+    uint32_t bad = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float2* t2 = reinterpret_cast<const float2*>(tris + 10ull * i);
+        float2 a = __ldg(t2), b = __ldg(t2 + 1), c = __ldg(t2 + 2), d = __ldg(t2 + 3), e = __ldg(t2 + 4);
+        float v[9] = {a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x};
+#pragma unroll
+        for (int j = 0; j < 9; ++j) bad |= !isfinite(v[j]);
+        uint32_t q[3];
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            float cen = __fdiv_rn(__fadd_rn(__fadd_rn(v[ax], v[3 + ax]), v[6 + ax]), 3.0f);
+            q[ax] = quantize(__fmul_rn(__fsub_rn(cen, s_box[ax]), s_box[3 + ax]), cells);
+        }
+        uint64_t k = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+        keys[i] = (K)k;
+#pragma unroll
+        for (int p = 0; p < P; ++p) atomicAdd(&s_hist[p * kRadix + (uint32_t)((k >> (8 * p)) & 0xFF)], 1u);
+    }
+    if (bad) atomicOr(status, CPT_STATUS_NONFINITE);
+    __syncthreads();
+    for (int i = threadIdx.x; i < P * kRadix; i += blockDim.x)
+        if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
+}
+
+// Exclusive prefix of each pass's 256 digit counts (one block per pass).
+__global__ void __launch_bounds__(kRadix) k_scan_offsets(const uint32_t* __restrict__ hist,
+                                                         uint32_t* __restrict__ offsets)
+{
+    __shared__ uint32_t s_warp[kRadix / 32];
+    const uint32_t* h = hist + blockIdx.x * kRadix;
+    uint32_t v = h[threadIdx.x];
+    uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kRadix / 32 ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+            if (lane >= (uint32_t)o) w += y;
+        }
+        if (lane < kRadix / 32) s_warp[lane] = w;
+    }
+    __syncthreads();
+    uint32_t before = warp ? s_warp[warp - 1] : 0;
+    offsets[blockIdx.x * kRadix + threadIdx.x] = before + x - v;
+}
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *reinterpret_cast<const volatile uint32_t*>(p); }
+__device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) { *reinterpret_cast<volatile uint32_t*>(p) = v; }
+
+template <typename K>
+constexpr size_t onesweep_smem() { return (size_t)kSortTile * sizeof(K) + (size_t)kSortTile * 4 + (size_t)kSortWarps * kRadix * 4 + 2 * kRadix * 4; }
+
+// One digit pass. Tiles are claimed in launch order through tile_counter, so a
+// tile only ever waits on tiles already owned by running blocks (which publish
+// their own counts before they wait): the look-back always completes; the poll
+// bound is a guard, not a scheduling assumption.
+template <typename K, bool kFirst>
+__global__ void __launch_bounds__(kSortBlock) k_onesweep(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                         K* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t n,
+                                                         int shift, const uint32_t* __restrict__ offsets,
+                                                         uint32_t* __restrict__ lookback,
+                                                         uint32_t* __restrict__ tile_counter,
+                                                         uint32_t* __restrict__ status)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    K* s_keys = reinterpret_cast<K*>(smem);
+    uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_keys + kSortTile);
+    uint32_t* s_hist = s_vals + kSortTile;       // [warp][digit]
+    uint32_t* s_off = s_hist + kSortWarps * kRadix;  // tile-local exclusive offset per digit
+    uint32_t* s_base = s_off + kRadix;           // global output base per digit
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_wsum[kSortWarps];
+
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+    for (uint32_t i = tid; i < kSortWarps * kRadix; i += kSortBlock) s_hist[i] = 0;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t tile_start = tile * kSortTile;
+    const uint32_t wbase = tile_start + warp * (kSortItems * 32);
+
+    K key[kSortItems];
+    uint32_t val[kSortItems];
+    uint32_t rank[kSortItems];
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        uint32_t idx = wbase + k * 32 + lane;
+        bool valid = idx < n;
+        key[k] = valid ? kin[idx] : (K)0;
+        val[k] = kFirst ? idx : (valid ? vin[idx] : 0u);
+    }
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    uint32_t* my_hist = s_hist + warp * kRadix;
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        uint32_t idx = wbase + k * 32 + lane;
+        uint32_t dig = idx < n ? (uint32_t)((key[k] >> shift) & 0xFF) : kRadix;
+        unsigned peers = __match_any_sync(0xFFFFFFFFu, dig);
+        uint32_t cnt = dig < kRadix ? my_hist[dig] : 0u;
+        rank[k] = cnt + __popc(peers & lt_mask);
+        __syncwarp();
+        if (dig < kRadix && lane == (uint32_t)(__ffs(peers) - 1)) my_hist[dig] = cnt + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // Per digit (thread tid = digit): exclusive prefix over warps, tile count.
+    uint32_t count = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) {
+        uint32_t c = s_hist[w * kRadix + tid];
+        s_hist[w * kRadix + tid] = count;
+        count += c;
+    }
+    // Publish this tile's count as early as possible.
+    st_volatile(&lookback[(size_t)tile * kRadix + tid], (tile == 0 ? kFlagInc : kFlagAgg) | count);
+
+    // Tile-local exclusive scan of the digit counts (warp shuffles + warp totals).
+    uint32_t x = count;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) s_wsum[warp] = x;
+    __syncthreads();
+    uint32_t before = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) before += (w < (int)warp) ? s_wsum[w] : 0u;
+    s_off[tid] = before + x - count;
+
+    // Decoupled look-back over the preceding tiles for this digit.
+    uint32_t prefix = 0;
+    if (tile > 0) {
+        int j = (int)tile - 1;
+        uint32_t polls = 0;
+        bool timed_out = false;
+        while (j >= 0) {
+            uint32_t v = ld_volatile(&lookback[(size_t)j * kRadix + tid]);
+            uint32_t f = v & ~kValueMask;
+            if (f == 0) {
+                if (++polls > kLookbackPolls) { timed_out = true; break; }
+                if (polls > 32) __nanosleep(100);
+                continue;
+            }
+            prefix += v & kValueMask;
+            if (f == kFlagInc) break;
+            --j;
+        }
+        if (timed_out) atomicOr(status, CPT_STATUS_TIMEOUT);
+        st_volatile(&lookback[(size_t)tile * kRadix + tid], kFlagInc | ((prefix + count) & kValueMask));
+    }
+    s_base[tid] = offsets[tid] + prefix;
+    __syncthreads();
+
+    // Stage the tile in local sorted order, then write runs of equal digits.
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        uint32_t idx = wbase + k * 32 + lane;
+        if (idx < n) {
+            uint32_t dig = (uint32_t)((key[k] >> shift) & 0xFF);
+            uint32_t pos = s_off[dig] + my_hist[dig] + rank[k];
+            s_keys[pos] = key[k];
+            s_vals[pos] = val[k];
+        }
+    }
+    __syncthreads();
+    const uint32_t tile_n = min((uint32_t)kSortTile, n - tile_start);
+    for (uint32_t i = tid; i < tile_n; i += kSortBlock) {
+        K kk = s_keys[i];
+        uint32_t dig = (uint32_t)((kk >> shift) & 0xFF);
+        uint32_t o = s_base[dig] + (i - s_off[dig]);
+        kout[o] = kk;
+        vout[o] = s_vals[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Karras radix tree over the sorted keys (BVHBuilder.cu:107-201). Also writes
+// the Node word into the traversal record, zeroes the refit counters and marks
+// the root's parent.
+// ---------------------------------------------------------------------------
+template <typename K>
+__device__ __forceinline__ int key_delta(const K* __restrict__ keys, K ki, int n, int i, int j)
+{
+    if (j < 0 || j >= n) return -1;
+    K kj = __ldg(keys + j);
+    if (ki == kj) return __clz(i ^ j) + KeyTraits<K>::total_bits;
+    if (sizeof(K) == 8) return __clzll((long long)(ki ^ kj));
+    return __clz((int)(ki ^ kj));
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) k_topology(const K* __restrict__ keys, uint32_t n, uint32_t* __restrict__ children,
+                                                  uint32_t* __restrict__ parents_leaf,
+                                                  uint32_t* __restrict__ parents_internal, int* __restrict__ counters,
+                                                  float4* __restrict__ nodes)
+{
+    const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int nn = (int)n;
+    if (i >= nn - 1) return;
+    const K ki = keys[i];
+    int dd = key_delta(keys, ki, nn, i, i + 1) - key_delta(keys, ki, nn, i, i - 1);
+    int d = (dd > 0) - (dd < 0);
+    int dmin = key_delta(keys, ki, nn, i, i - d);
+    int lmax = 2;
+    while (key_delta(keys, ki, nn, i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    while (lmax > 1) {
+        lmax /= 2;
+        if (key_delta(keys, ki, nn, i, i + (l + lmax) * d) > dmin) l += lmax;
+    }
+    const int j = i + l * d;
+    const int dnode = key_delta(keys, ki, nn, i, j);
+    int s = 0;
+    while (l > 1) {
+        l = (l + 1) / 2;
+        if (key_delta(keys, ki, nn, i, i + (s + l) * d) > dnode) s += l;
+    }
+    s = i + s * d + (d < 0 ? d : 0);
+    uint32_t type = 0;
+    if (min(i, j) != s) { type |= 1u; parents_internal[s] = (uint32_t)i; }
+    else parents_leaf[s] = (uint32_t)i;
+    if (max(i, j) != s + 1) { type |= 2u; parents_internal[s + 1] = (uint32_t)i; }
+    else parents_leaf[s + 1] = (uint32_t)i;
+    const uint32_t word = ((uint32_t)s << 2) | type;
+    children[i] = word;
+    nodes[4 * (size_t)i + 3] = make_float4(__uint_as_float(word), 0.0f, 0.0f, 0.0f);
+    counters[i] = 0;
+    if (i == 0) parents_internal[0] = CPT_INVALID_INDEX;
+}
+
+// ---------------------------------------------------------------------------
+// Triangle permutation fused with the bottom-up refit. Thread i gathers sorted
+// triangle i (writing the 40-B reference record and the 48-B traversal record),
+// computes its leaf box, then walks up: at each parent it stores its child box
+// into the parent's traversal record, and the second child to arrive (atomic
+// counter) reads its sibling's box from there and forms left.unite(right).
+// Release/acquire fences order the box stores before the counter (the
+// reference's refit has no fence, BVHBuilder.cu:63-86).
+// ---------------------------------------------------------------------------
+struct Box { float mn[3], mx[3]; };
+
+__device__ __forceinline__ void store_slot(float* node, int side, const Box& b)
+{
+    if (side == 0) {
+        *reinterpret_cast<float4*>(node) = make_float4(b.mn[0], b.mn[1], b.mn[2], b.mx[0]);
+        *reinterpret_cast<float2*>(node + 4) = make_float2(b.mx[1], b.mx[2]);
+    } else {
+        *reinterpret_cast<float2*>(node + 6) = make_float2(b.mn[0], b.mn[1]);
+        *reinterpret_cast<float4*>(node + 8) = make_float4(b.mn[2], b.mx[0], b.mx[1], b.mx[2]);
+    }
+}
+
+__device__ __forceinline__ Box load_slot(const float* node, int side)
+{
+    Box b;
+    if (side == 0) {
+        float4 a = __ldcg(reinterpret_cast<const float4*>(node));
+        float2 c = __ldcg(reinterpret_cast<const float2*>(node + 4));
+        b.mn[0] = a.x; b.mn[1] = a.y; b.mn[2] = a.z; b.mx[0] = a.w; b.mx[1] = c.x; b.mx[2] = c.y;
+    } else {
+        float2 a = __ldcg(reinterpret_cast<const float2*>(node + 6));
+        float4 c = __ldcg(reinterpret_cast<const float4*>(node + 8));
+        b.mn[0] = a.x; b.mn[1] = a.y; b.mn[2] = c.x; b.mx[0] = c.y; b.mx[1] = c.z; b.mx[2] = c.w;
+    }
+    return b;
+}
+
+__global__ void __launch_bounds__(256) k_gather_refit(const float* __restrict__ tris_in, const uint32_t* __restrict__ order,
+                                                      uint32_t n, float* __restrict__ tris_out,
+                                                      float4* __restrict__ trirec, const uint32_t* __restrict__ children,
+                                                      const uint32_t* __restrict__ parents_leaf,
+                                                      const uint32_t* __restrict__ parents_internal,
+                                                      int* __restrict__ counters, float* __restrict__ nodes,
+                                                      cpt_bbox* __restrict__ node_boxes)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t src = order[i];
+    const float2* s2 = reinterpret_cast<const float2*>(tris_in + 10ull * src);
+    float2 a = __ldg(s2), b = __ldg(s2 + 1), c = __ldg(s2 + 2), d = __ldg(s2 + 3), e = __ldg(s2 + 4);
+    float2* o2 = reinterpret_cast<float2*>(tris_out + 10ull * i);
+    o2[0] = a; o2[1] = b; o2[2] = c; o2[3] = d; o2[4] = e;
+    const float v[9] = {a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x};
+    const float info = e.y;
+    trirec[3 * (size_t)i + 0] = make_float4(v[0], v[1], v[2], info);
+    trirec[3 * (size_t)i + 1] = make_float4(__fsub_rn(v[3], v[0]), __fsub_rn(v[4], v[1]), __fsub_rn(v[5], v[2]), 0.0f);
+    trirec[3 * (size_t)i + 2] = make_float4(__fsub_rn(v[6], v[0]), __fsub_rn(v[7], v[1]), __fsub_rn(v[8], v[2]), 0.0f);
+
+    // Leaf box: empty box united with v0, v1, v2 in order (BVHBuilder.cu:73-74, BBox.cpp:26-30).
+    Box box;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        float mn = FLT_MAX, mx = -FLT_MAX;
+#pragma unroll
+        for (int vv = 0; vv < 3; ++vv) { mn = gmin(mn, v[3 * vv + ax]); mx = gmax(mx, v[3 * vv + ax]); }
+        box.mn[ax] = mn;
+        box.mx[ax] = mx;
+    }
+    uint32_t child = i;
+    uint32_t p = parents_leaf[i];
+    while (p != CPT_INVALID_INDEX) {
+        const uint32_t word = children[p];
+        const int side = (word >> 2) == child ? 0 : 1;
+        float* node = nodes + 16 * (size_t)p;
+        store_slot(node, side, box);
+        __threadfence();
+        if (atomicAdd(&counters[p], 1) == 0) return;
+        __threadfence();
+        Box sib = load_slot(node, 1 - side);
+        const Box& L = side == 0 ? box : sib;
+        const Box& R = side == 0 ? sib : box;
+        Box u;
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) { u.mn[ax] = gmin(L.mn[ax], R.mn[ax]); u.mx[ax] = gmax(L.mx[ax], R.mx[ax]); }
+        box = u;
+        cpt_bbox out;
+        for (int ax = 0; ax < 3; ++ax) { out.min[ax] = box.mn[ax]; out.max[ax] = box.mx[ax]; }
+        node_boxes[p] = out;
+        child = p;
+        p = parents_internal[p];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+template <typename K>
+struct SortScratch {
+    K* keys_alt;
+    uint32_t* vals[2];
+    uint32_t* hist;
+    uint32_t* offsets;
+    uint32_t* zero_region;  // tile counters + look-back, zeroed by k_morton
+    size_t zero_words;
+    uint32_t* tile_counters;
+    uint32_t* lookback;
+    int* counters;
+    float* bounds_partial;
+    float* dev_box;
+    float* tris_copy;
+};
+
+inline uint32_t num_tiles(uint32_t n) { return (n + kSortTile - 1) / kSortTile; }
+
+template <typename K>
+size_t scratch_layout(uint32_t n, void* base, SortScratch<K>* s)
+{
+    constexpr int P = KeyTraits<K>::passes;
+    Carver c(base);
+    SortScratch<K> t;
+    t.keys_alt = c.take<K>(n);
+    t.vals[0] = c.take<uint32_t>(n);
+    t.vals[1] = c.take<uint32_t>(n);
+    t.hist = c.take<uint32_t>((size_t)P * kRadix);
+    t.offsets = c.take<uint32_t>((size_t)P * kRadix);
+    t.zero_words = 32 + (size_t)P * num_tiles(n) * kRadix;
+    t.zero_region = c.take<uint32_t>(t.zero_words);
+    t.tile_counters = t.zero_region;
+    t.lookback = t.zero_region ? t.zero_region + 32 : nullptr;
+    t.counters = c.take<int>(n);
+    t.bounds_partial = c.take<float>(6 * kBoundsBlocks);
+    t.dev_box = c.take<float>(8);
+    t.tris_copy = c.take<float>(10ull * n);
+    if (s) *s = t;
+    return c.used();
+}
+
+template <typename K>
+int build_impl(const cpt_triangle* tris_in, uint32_t n, const float* host_box, cpt_bvh* bvh, void* scratch,
+               cudaStream_t stream)
+{
+    constexpr int P = KeyTraits<K>::passes;
+    SortScratch<K> s;
+    scratch_layout<K>(n, scratch, &s);
+    const float* tri_src = reinterpret_cast<const float*>(tris_in);
+    if (tris_in == bvh->tris) {
+        // In-place build (the reference permutes DeviceSceneDescription::triangles):
+        // gather from a copy.
+        CPT_CUDA_TRY(cudaMemcpyAsync(s.tris_copy, tris_in, sizeof(cpt_triangle) * (size_t)n, cudaMemcpyDeviceToDevice, stream));
+        tri_src = s.tris_copy;
+    }
+    CPT_CUDA_TRY(cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * P * kRadix, stream));
+    CPT_CUDA_TRY(cudaMemsetAsync(bvh->status, 0, 4 * sizeof(uint32_t), stream));
+
+    BoxArg box{};
+    if (host_box) {
+        for (int a = 0; a < 3; ++a) {
+            box.mn[a] = host_box[a];
+            box.inv[a] = 1.0f / (host_box[3 + a] - host_box[a]);
+        }
+        box.dev = nullptr;
+    } else {
+        {
+            CPT_PROF(K_BOUNDS, stream);
+            k_bounds_partial<<<kBoundsBlocks, kBoundsBlock, 0, stream>>>(tri_src, n, s.bounds_partial);
+        }
+        CPT_LAUNCH_CHECK();
+        {
+            CPT_PROF(K_BOUNDS, stream);
+            k_bounds_final<<<1, 32, 0, stream>>>(s.bounds_partial, kBoundsBlocks, s.dev_box);
+        }
+        CPT_LAUNCH_CHECK();
+        box.dev = s.dev_box;
+    }
+
+    K* keys = static_cast<K*>(bvh->keys);
+    const int sms = sm_count();
+    const int morton_blocks = (int)std::min<size_t>((n + kMortonBlock - 1) / kMortonBlock, (size_t)sms * 8);
+    {
+        CPT_PROF(K_MORTON, stream);
+        k_morton<K><<<morton_blocks, kMortonBlock, 0, stream>>>(tri_src, n, box, keys, s.hist, s.zero_region,
+                                                                s.zero_words, bvh->status);
+    }
+    CPT_LAUNCH_CHECK();
+    {
+        CPT_PROF(K_SCAN, stream);
+        k_scan_offsets<<<P, kRadix, 0, stream>>>(s.hist, s.offsets);
+    }
+    CPT_LAUNCH_CHECK();
+
+    const size_t smem = onesweep_smem<K>();
+    CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const uint32_t tiles = num_tiles(n);
+    K* kbuf[2] = {keys, s.keys_alt};
+    for (int p = 0; p < P; ++p) {
+        const K* kin = kbuf[p & 1];
+        K* kout = kbuf[(p + 1) & 1];
+        const uint32_t* vin = p == 0 ? nullptr : s.vals[(p + 1) & 1];
+        uint32_t* vout = s.vals[p & 1];
+        uint32_t* lb = s.lookback + (size_t)p * tiles * kRadix;
+        CPT_PROF(K_ONESWEEP, stream);
+        if (p == 0)
+            k_onesweep<K, true><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, n, 8 * p, s.offsets + p * kRadix,
+                                                                     lb, s.tile_counters + p, bvh->status);
+        else
+            k_onesweep<K, false><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, n, 8 * p, s.offsets + p * kRadix,
+                                                                      lb, s.tile_counters + p, bvh->status);
+        CPT_LAUNCH_CHECK();
+    }
+    // P is even: keys end in bvh->keys, values in vals[(P - 1) & 1].
+    const uint32_t* order = s.vals[(P - 1) & 1];
+
+    const uint32_t inner = n - 1;
+    {
+        CPT_PROF(K_TOPOLOGY, stream);
+        k_topology<K><<<(inner + 255) / 256, 256, 0, stream>>>(keys, n, bvh->children, bvh->parents_leaf,
+                                                                bvh->parents_internal, s.counters,
+                                                                static_cast<float4*>(bvh->nodes));
+    }
+    CPT_LAUNCH_CHECK();
+    {
+        CPT_PROF(K_GATHER_REFIT, stream);
+        k_gather_refit<<<(n + 255) / 256, 256, 0, stream>>>(tri_src, order, n, reinterpret_cast<float*>(bvh->tris),
+                                                             static_cast<float4*>(bvh->tri_records), bvh->children,
+                                                             bvh->parents_leaf, bvh->parents_internal, s.counters,
+                                                             static_cast<float*>(bvh->nodes), bvh->node_boxes);
+    }
+    CPT_LAUNCH_CHECK();
+    return CPT_OK;
+}
+
+inline size_t key_bytes(int bits) { return bits == 30 ? 4 : 8; }
+
+}  // namespace cpt
+
+using namespace cpt;
+
+extern "C" size_t cpt_bvh_bytes(uint32_t n, int morton_bits)
+{
+    if (n < 2 || (morton_bits != 30 && morton_bits != 63)) return 0;
+    Carver c(nullptr);
+    c.take<cpt_triangle>(n);
+    c.take<char>(key_bytes(morton_bits) * n);
+    c.take<uint32_t>(n - 1);
+    c.take<uint32_t>(n);
+    c.take<uint32_t>(n - 1);
+    c.take<cpt_bbox>(n - 1);
+    c.take<float4>(4ull * (n - 1));
+    c.take<float4>(3ull * n);
+    c.take<uint32_t>(4);
+    return c.used();
+}
+
+extern "C" int cpt_bvh_bind(void* mem, size_t bytes, uint32_t n, int morton_bits, cpt_bvh* out)
+{
+    if (!mem || !out || n < 2 || n > kMaxTriangles || (morton_bits != 30 && morton_bits != 63))
+        return CPT_ERR_INVALID_ARGUMENT;
+    if (bytes < cpt_bvh_bytes(n, morton_bits)) return CPT_ERR_SCRATCH_TOO_SMALL;
+    Carver c(mem);
+    out->n = n;
+    out->morton_bits = morton_bits;
+    out->tris = c.take<cpt_triangle>(n);
+    out->keys = c.take<char>(key_bytes(morton_bits) * n);
+    out->children = c.take<uint32_t>(n - 1);
+    out->parents_leaf = c.take<uint32_t>(n);
+    out->parents_internal = c.take<uint32_t>(n - 1);
+    out->node_boxes = c.take<cpt_bbox>(n - 1);
+    out->nodes = c.take<float4>(4ull * (n - 1));
+    out->tri_records = c.take<float4>(3ull * n);
+    out->status = c.take<uint32_t>(4);
+    return CPT_OK;
+}
+
+extern "C" size_t cpt_lbvh_scratch_bytes(uint32_t n, int morton_bits)
+{
+    if (n < 2 || n > kMaxTriangles) return 0;
+    if (morton_bits == 30) return scratch_layout<uint32_t>(n, nullptr, nullptr);
+    if (morton_bits == 63) return scratch_layout<uint64_t>(n, nullptr, nullptr);
+    return 0;
+}
+
+extern "C" int cpt_status_check(const uint32_t* d_status, cudaStream_t stream)
+{
+    if (!d_status) return CPT_ERR_INVALID_ARGUMENT;
+    uint32_t h[4] = {0, 0, 0, 0};
+    CPT_CUDA_TRY(cudaMemcpyAsync(h, d_status, sizeof(h), cudaMemcpyDeviceToHost, stream));
+    CPT_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (h[0] & CPT_STATUS_NONFINITE) return CPT_ERR_NONFINITE_INPUT;
+    if (h[0] & CPT_STATUS_TIMEOUT) return CPT_ERR_DEVICE_TIMEOUT;
+    if (h[0] & CPT_STATUS_STACK_OVERFLOW) return CPT_ERR_STACK_OVERFLOW;
+    return CPT_OK;
+}
+
+extern "C" int cpt_lbvh_build(const cpt_triangle* tris_in, uint32_t n, const float* enclosing_box, int morton_bits,
+                              cpt_bvh* bvh, void* scratch, size_t scratch_bytes, uint32_t flags, cudaStream_t stream)
+{
+    if (!tris_in || !bvh || !scratch || n < 2 || n > kMaxTriangles) return CPT_ERR_INVALID_ARGUMENT;
+    if (morton_bits != 30 && morton_bits != 63) return CPT_ERR_INVALID_ARGUMENT;
+    if (bvh->n != n || bvh->morton_bits != morton_bits || !bvh->tris || !bvh->keys || !bvh->children ||
+        !bvh->parents_leaf || !bvh->parents_internal || !bvh->node_boxes || !bvh->nodes || !bvh->tri_records ||
+        !bvh->status)
+        return CPT_ERR_INVALID_ARGUMENT;
+    if ((reinterpret_cast<uintptr_t>(tris_in) & 15) || (reinterpret_cast<uintptr_t>(scratch) & 255) ||
+        (reinterpret_cast<uintptr_t>(bvh->nodes) & 15) || (reinterpret_cast<uintptr_t>(bvh->tri_records) & 15) ||
+        (reinterpret_cast<uintptr_t>(bvh->tris) & 15))
+        return CPT_ERR_INVALID_ARGUMENT;
+    if (scratch_bytes < cpt_lbvh_scratch_bytes(n, morton_bits)) return CPT_ERR_SCRATCH_TOO_SMALL;
+    int rc = morton_bits == 30 ? build_impl<uint32_t>(tris_in, n, enclosing_box, bvh, scratch, stream)
+                               : build_impl<uint64_t>(tris_in, n, enclosing_box, bvh, scratch, stream);
+    if (rc != CPT_OK || !(flags & CPT_BUILD_CHECK)) return rc;
+    rc = cpt_status_check(bvh->status, stream);
+    if (rc != CPT_OK) return rc;
+    // Root-volume self-check of BVHBuilder.cu:258-265 (absolute epsilon 1e-7,
+    // source/engine/util/math.h:22,68), against the host box or the device box.
+    cpt_bbox root;
+    CPT_CUDA_TRY(cudaMemcpyAsync(&root, bvh->node_boxes, sizeof(root), cudaMemcpyDeviceToHost, stream));
+    float eb[6];
+    if (enclosing_box) {
+        for (int a = 0; a < 6; ++a) eb[a] = enclosing_box[a];
+    } else {
+        SortScratch<uint32_t> s32;
+        SortScratch<uint64_t> s64;
+        const float* dev_box = morton_bits == 30 ? (scratch_layout<uint32_t>(n, scratch, &s32), s32.dev_box)
+                                                 : (scratch_layout<uint64_t>(n, scratch, &s64), s64.dev_box);
+        CPT_CUDA_TRY(cudaMemcpyAsync(eb, dev_box, sizeof(eb), cudaMemcpyDeviceToHost, stream));
+    }
+    CPT_CUDA_TRY(cudaStreamSynchronize(stream));
+    float ve = (eb[3] - eb[0]) * (eb[4] - eb[1]) * (eb[5] - eb[2]);
+    float vr = (root.max[0] - root.min[0]) * (root.max[1] - root.min[1]) * (root.max[2] - root.min[2]);
+    if (!(fabsf(ve - vr) <= 1e-7f)) return CPT_ERR_CHECK_FAILED;
+    return CPT_OK;
+}

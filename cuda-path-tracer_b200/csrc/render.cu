@@ -1,0 +1,558 @@
+// Wavefront path tracer for sm_100a (cpt_render, cpt_resolve).
+//
+// The reference traces each pixel's whole path in one megakernel thread
+// (raytrace_kernel, cuda_path_tracer.cu:385-421, with blinnPhongShadingPathTrace
+// :245-333). Here a wave of paths — whole samples of the image, sample-major —
+// advances one vertex at a time:
+//
+//   k_generate    primary rays for every (sample, pixel) of the wave  -> queue 0
+//   k_extend      closest hit for every ray in queue b                 -> hits
+//   k_shade       shading of vertex b, shadow rays inline (any-hit),
+//                 next bounce direction                                 -> queue b+1
+//   k_accumulate  per pixel, the wave's samples in sample order         -> accumulator
+//
+// Each path's radiance is the reference's estimator evaluated in the same
+// operation order (round-to-nearest intrinsics), with the random numbers drawn
+// from the counter-based Philox stream by (pixel, sample, bounce), so the result
+// of every path is independent of queue order and wave size. The pixel order of
+// a sample walks 8-row bands column by column so that a warp's primary rays
+// cover a 4x8 pixel patch.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include "cpt.h"
+#include "cpt_internal.h"
+#include "traverse.cuh"
+
+namespace cpt {
+
+constexpr int kExtendBlock = 128;
+constexpr int kShadeBlock = 128;
+constexpr int kGenBlock = 256;
+constexpr int kMaxDepth = 62;  // bounces + 1 queues; reference GUI allows 5 bounces (PathTracingSettings.h:27)
+constexpr uint32_t kDefaultWavePaths = 1u << 23;
+
+struct Wave {
+    uint32_t width, height, pixels;
+    uint32_t s0;          // first sample of this wave (relative to params.frame0)
+    uint32_t spw;         // samples in this wave
+    uint32_t frame0;
+    uint32_t bounces;
+    float intensity;
+    uint32_t stratified;
+    uint32_t k0, k1;
+    uint32_t ref_w, ref_h;  // rendered extent (reference grid truncation)
+    uint32_t light_count;
+};
+
+struct Camera {
+    float eye[3];
+    float dirs[4][3];
+    float m[16];
+    float jx, jy;
+    uint32_t jitter;
+};
+
+// Slot -> pixel: 8-row bands, column-major inside a band.
+__device__ __forceinline__ void slot_to_pixel(uint32_t slot, uint32_t w, uint32_t h, uint32_t& x, uint32_t& y)
+{
+    uint32_t band = slot / (8u * w);
+    uint32_t bh = min(8u, h - 8u * band);
+    uint32_t j = slot - band * 8u * w;
+    x = j / bh;
+    y = 8u * band + (j - x * bh);
+}
+
+__device__ __forceinline__ uint32_t pixel_to_slot(uint32_t x, uint32_t y, uint32_t w, uint32_t h)
+{
+    uint32_t band = y >> 3;
+    uint32_t bh = min(8u, h - 8u * band);
+    return band * 8u * w + x * bh + (y - 8u * band);
+}
+
+__device__ __forceinline__ void mat_vec(const float* m, float v0, float v1, float v2, float v3, float r[4])
+{
+#pragma unroll
+    for (int row = 0; row < 4; ++row) {
+        float a = __fmul_rn(m[row], v0), b = __fmul_rn(m[4 + row], v1);
+        float c = __fmul_rn(m[8 + row], v2), d = __fmul_rn(m[12 + row], v3);
+        r[row] = __fadd_rn(__fadd_rn(__fadd_rn(a, b), c), d);
+    }
+}
+
+// Corner directions of one sample (PathTracingApp.cpp:217-242 with the jitter
+// from the Philox camera stream).
+__device__ __forceinline__ void corner_dirs(const Camera& cam, uint32_t k0, uint32_t k1, uint32_t frame, f3 out[4])
+{
+    if (!cam.jitter) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) out[c] = mk3(cam.dirs[c][0], cam.dirs[c][1], cam.dirs[c][2]);
+        return;
+    }
+    uint4 r = philox4x32_10(make_uint4(0xFFFFFFFFu, frame, 0u, 1u), k0, k1);
+    float u0 = u01(r.x), u1 = u01(r.y);
+    float jx = __fmul_rn(__fsub_rn(__fmul_rn(2.0f, u0), 1.0f), cam.jx);
+    float jy = __fmul_rn(__fsub_rn(__fmul_rn(2.0f, u1), 1.0f), cam.jy);
+    const float cx[4] = {-1.f, 1.f, 1.f, -1.f}, cy[4] = {-1.f, -1.f, 1.f, 1.f};
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float nx = __fsub_rn(cx[c], jx), ny = __fsub_rn(cy[c], jy);
+        float ws[4], we[4];
+        mat_vec(cam.m, nx, ny, -1.0f, 1.0f, ws);
+        mat_vec(cam.m, nx, ny, 1.0f, 1.0f, we);
+        f3 ps = mk3(__fdiv_rn(ws[0], ws[3]), __fdiv_rn(ws[1], ws[3]), __fdiv_rn(ws[2], ws[3]));
+        f3 pe = mk3(__fdiv_rn(we[0], we[3]), __fdiv_rn(we[1], we[3]), __fdiv_rn(we[2], we[3]));
+        out[c] = normalize(sub(pe, ps));
+    }
+}
+
+__global__ void __launch_bounds__(kGenBlock) k_generate(Wave wv, Camera cam, float4* __restrict__ queue,
+                                                        uint32_t* __restrict__ counts, float4* __restrict__ state)
+{
+    const uint32_t total = wv.spw * wv.pixels;
+    for (uint32_t pid = blockIdx.x * kGenBlock + threadIdx.x; pid < total; pid += gridDim.x * kGenBlock) {
+        const uint32_t sl = pid / wv.pixels, slot = pid - sl * wv.pixels;
+        uint32_t x, y;
+        slot_to_pixel(slot, wv.width, wv.height, x, y);
+        const bool live = x < wv.ref_w && y < wv.ref_h;
+        state[2 * (size_t)pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+        const uint32_t q = warp_append(&counts[0], live);
+        if (!live) continue;
+        f3 c[4];
+        corner_dirs(cam, wv.k0, wv.k1, wv.frame0 + wv.s0 + sl, c);
+        // raytrace_kernel (cuda_path_tracer.cu:404-407): bilerp with (x/W, y/H), not normalised.
+        float tx = __fdiv_rn(__uint2float_rn(x), __uint2float_rn(wv.width));
+        float ty = __fdiv_rn(__uint2float_rn(y), __uint2float_rn(wv.height));
+        f3 d = mix3(mix3(c[0], c[1], tx), mix3(c[3], c[2], tx), ty);
+        queue[2 * (size_t)q] = make_float4(cam.eye[0], cam.eye[1], cam.eye[2], __uint_as_float(pid));
+        queue[2 * (size_t)q + 1] = make_float4(d.x, d.y, d.z, 0.f);
+    }
+}
+
+template <bool kStats>
+__global__ void __launch_bounds__(kExtendBlock) k_extend(const float4* __restrict__ nodes, const float4* __restrict__ tris,
+                                                         const float4* __restrict__ queue,
+                                                         const uint32_t* __restrict__ count, float4* __restrict__ hits,
+                                                         unsigned long long* __restrict__ ray_counts,
+                                                         uint32_t* __restrict__ status)
+{
+    __shared__ uint32_t s_stack[CPT_TRAVERSAL_STACK * kExtendBlock];
+    uint32_t* stack = s_stack + threadIdx.x;
+    const uint32_t n = *count;
+    bool overflow = false;
+    uint32_t nn = 0, nt = 0;
+    for (uint32_t i = blockIdx.x * kExtendBlock + threadIdx.x; i < n; i += gridDim.x * kExtendBlock) {
+        const float4 ro = queue[2 * (size_t)i], rd = queue[2 * (size_t)i + 1];
+        Hit h = traverse<false, kExtendBlock, kStats>(nodes, tris, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z), stack,
+                                                      overflow, nn, nt);
+        hits[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
+    }
+    if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
+    if (kStats && ray_counts) {
+        warp_count_u64(ray_counts + 3, nn);
+        warp_count_u64(ray_counts + 4, nt);
+    }
+}
+
+struct ShadeScene {
+    const float4* nodes;
+    const float4* tris;
+    const cpt_triangle_info* infos;
+    const cpt_dir_light* lights;
+};
+
+// blinnPhongBRDF (cuda_path_tracer.cu:36-50)
+__device__ __forceinline__ f3 blinn_phong(f3 Id, f3 kd, f3 Is, f3 ks, f3 n, f3 lv, f3 h, float shininess)
+{
+    float df = gmax(dot(n, lv), 0.0f);
+    f3 diffuse = muls(mul(Id, kd), df);
+    float sf = powf(gmax(dot(n, h), 0.0f), shininess);
+    f3 spec = mk3(0.f, 0.f, 0.f);
+    if (shininess > 0.0f && df > 0.0f) spec = muls(mul(Is, ks), sf);
+    return add(diffuse, spec);
+}
+
+// computeL (LightAlgorithms.h:12-20). The reference traces a full closest hit and
+// tests distance < FLT_MAX; the any-hit traversal visits nodes in the same order
+// until its first recorded triangle, so the visibility it returns is the same.
+template <int kBlock>
+__device__ __forceinline__ f3 light_l(const ShadeScene& sc, f3 p, const cpt_dir_light& l, uint32_t* stack, bool& overflow)
+{
+    f3 dir = mk3(l.direction[0], l.direction[1], l.direction[2]);
+    f3 o = sub(p, muls(dir, 1e-3f));
+    uint32_t nn = 0, nt = 0;
+    Hit h = traverse<true, kBlock, false>(sc.nodes, sc.tris, o, neg(dir), stack, overflow, nn, nt);
+    if (h.t < FLT_MAX) return mk3(0.f, 0.f, 0.f);
+    return muls(mk3(l.color[0], l.color[1], l.color[2]), l.intensity);
+}
+
+// toHemisphere (math_util.h:56-67)
+__device__ __forceinline__ f3 to_hemisphere(f3 v, f3 n)
+{
+    f3 x = fabsf(n.x) < FLT_EPSILON ? cross(n, mk3(1.0f, 0.0f, 0.0f)) : cross(n, mk3(0.0f, 1.0f, 0.0f));
+    x = normalize(x);
+    f3 y = normalize(cross(n, x));
+    return add(add(muls(x, v.x), muls(y, v.y)), muls(n, v.z));
+}
+
+template <bool kLights>
+__global__ void __launch_bounds__(kShadeBlock) k_shade(ShadeScene sc, Wave wv, uint32_t depth,
+                                                       const float4* __restrict__ queue_in,
+                                                       const float4* __restrict__ hits,
+                                                       const uint32_t* __restrict__ count_in,
+                                                       float4* __restrict__ queue_out, uint32_t* __restrict__ count_out,
+                                                       float4* __restrict__ state,
+                                                       unsigned long long* __restrict__ ray_counts,
+                                                       uint32_t* __restrict__ status)
+{
+    __shared__ uint32_t s_stack[kLights ? CPT_TRAVERSAL_STACK * kShadeBlock : 1];
+    uint32_t* stack = s_stack + (kLights ? threadIdx.x : 0);
+    const uint32_t n = *count_in;
+    bool overflow = false;
+    for (uint32_t base = blockIdx.x * kShadeBlock; base < n; base += gridDim.x * kShadeBlock) {
+        const uint32_t i = base + threadIdx.x;
+        bool emit = false;
+        float4 nro = make_float4(0.f, 0.f, 0.f, 0.f), nrd = nro;
+        uint32_t shadow = 0;
+        if (i < n) {
+            const float4 ro = queue_in[2 * (size_t)i], rd4 = queue_in[2 * (size_t)i + 1];
+            const float4 hit4 = hits[i];
+            const uint32_t tri = __float_as_uint(hit4.w);
+            const uint32_t pid = __float_as_uint(ro.w);
+            if (tri != CPT_INVALID_INDEX) {
+                const f3 o = mk3(ro.x, ro.y, ro.z), d = mk3(rd4.x, rd4.y, rd4.z);
+                const float t = hit4.x, u = hit4.y, v = hit4.z;
+                const uint32_t info_idx = __float_as_uint(__ldg(reinterpret_cast<const float*>(sc.tris + 3 * (size_t)tri) + 3));
+                const cpt_triangle_info& in = sc.infos[info_idx];
+                const f3 hp = add(muls(d, t), o);
+                f3 albedo = normalize(bary(ld3(in.vertices[0].color), ld3(in.vertices[1].color), ld3(in.vertices[2].color), u, v));
+                const f3 normal = normalize(bary(ld3(in.vertices[0].normal), ld3(in.vertices[1].normal), ld3(in.vertices[2].normal), u, v));
+                const f3 e = ld3(in.material.emission);
+                const bool emissive = __fadd_rn(__fadd_rn(e.x, e.y), e.z) > 1e-7f;
+                float4 acc4 = state[2 * (size_t)pid], ab4 = state[2 * (size_t)pid + 1];
+                f3 acc, absorbed;
+                if (depth == 0) {
+                    // blinnPhongShadingShadowTrace (cuda_path_tracer.cu:163-220)
+                    if (emissive) {
+                        albedo = mk3(1.f, 1.f, 1.f);
+                        acc = e;
+                    } else {
+                        f3 L = mk3(0.f, 0.f, 0.f), color = mk3(0.f, 0.f, 0.f);
+                        if (kLights) {
+                            for (uint32_t li = 0; li < wv.light_count; ++li) {
+                                const cpt_dir_light l = sc.lights[li];
+                                L = add(L, light_l<kShadeBlock>(sc, hp, l, stack, overflow));
+                                ++shadow;
+                                f3 ldir = ld3(l.direction);
+                                f3 half = muls(sub(neg(d), ldir), 0.5f);
+                                color = add(color, blinn_phong(L, albedo, L, mk3(0.5f, 0.5f, 0.5f), normal, neg(ldir), half,
+                                                               in.material.specularity));
+                            }
+                        }
+                        acc = color;
+                    }
+                    absorbed = albedo;
+                } else {
+                    // bounce vertex (cuda_path_tracer.cu:298-324)
+                    acc = mk3(acc4.x, acc4.y, acc4.z);
+                    absorbed = mk3(ab4.x, ab4.y, ab4.z);
+                    f3 L = mk3(0.f, 0.f, 0.f);
+                    if (emissive) {
+                        L = muls(e, gmax(dot(neg(d), normal), 0.0f));
+                        albedo = mk3(1.f, 1.f, 1.f);
+                    } else if (kLights) {
+                        for (uint32_t li = 0; li < wv.light_count; ++li) {
+                            const cpt_dir_light l = sc.lights[li];
+                            f3 c = light_l<kShadeBlock>(sc, hp, l, stack, overflow);
+                            ++shadow;
+                            L = add(L, muls(c, gmax(dot(neg(ld3(l.direction)), normal), 0.0f)));
+                        }
+                    }
+                    absorbed = mul(absorbed, albedo);
+                    acc = add(acc, muls(mul(absorbed, L), wv.intensity));
+                }
+                state[2 * (size_t)pid] = make_float4(acc.x, acc.y, acc.z, 0.f);
+                state[2 * (size_t)pid + 1] = make_float4(absorbed.x, absorbed.y, absorbed.z, 0.f);
+                if (depth < wv.bounces) {
+                    // next direction (cuda_path_tracer.cu:269-284)
+                    const uint32_t sl = pid / wv.pixels, slot = pid - sl * wv.pixels;
+                    uint32_t x, y;
+                    slot_to_pixel(slot, wv.width, wv.height, x, y);
+                    const uint32_t frame = wv.frame0 + wv.s0 + sl;
+                    const f3 no = add(hp, muls(normal, 1e-5f));
+                    uint4 r = philox4x32_10(make_uint4(y * wv.width + x, frame, depth, 0u), wv.k0, wv.k1);
+                    float rx = u01(r.x), ry = u01(r.y);
+                    if (wv.stratified && depth == 0) {
+                        uint32_t pos = frame % 64u;
+                        rx = __fdiv_rn(__fadd_rn((float)(int)(pos % 8u), rx), 8.0f);
+                        ry = __fdiv_rn(__fadd_rn((float)(int)(pos / 8u), ry), 8.0f);
+                    }
+                    float sn, cs;
+                    sincos_turns(ry, &sn, &cs);
+                    float rr = __fsqrt_rn(rx);
+                    f3 dl = mk3(__fmul_rn(rr, cs), __fmul_rn(rr, sn), __fsqrt_rn(__fsub_rn(1.0f, rx)));
+                    f3 nd = to_hemisphere(dl, normal);
+                    emit = true;
+                    nro = make_float4(no.x, no.y, no.z, __uint_as_float(pid));
+                    nrd = make_float4(nd.x, nd.y, nd.z, 0.f);
+                }
+            }
+        }
+        const uint32_t q = warp_append(count_out, emit);
+        if (emit) {
+            queue_out[2 * (size_t)q] = nro;
+            queue_out[2 * (size_t)q + 1] = nrd;
+        }
+        if (kLights) warp_count_u64(ray_counts ? ray_counts + 2 : nullptr, shadow);
+    }
+    if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
+}
+
+// Primary / extension ray totals of a wave from the queue counters.
+__global__ void k_wave_counts(const uint32_t* __restrict__ counts, uint32_t depth_count,
+                              unsigned long long* __restrict__ ray_counts)
+{
+    if (threadIdx.x != 0 || !ray_counts) return;
+    unsigned long long ext = 0;
+    for (uint32_t b = 1; b < depth_count; ++b) ext += counts[b];
+    atomicAdd(ray_counts + 0, (unsigned long long)counts[0]);
+    atomicAdd(ray_counts + 1, ext);
+}
+
+// Adds the wave's samples to the accumulator, per pixel in sample order.
+__global__ void __launch_bounds__(256) k_accumulate(Wave wv, uint32_t mode, const float4* __restrict__ state,
+                                                    void* __restrict__ accum)
+{
+    const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x;
+    if (px >= wv.pixels) return;
+    const uint32_t x = px % wv.width, y = px / wv.width;
+    if (x >= wv.ref_w || y >= wv.ref_h) return;
+    const uint32_t slot = pixel_to_slot(x, y, wv.width, wv.height);
+    if (mode == CPT_ACCUM_KAHAN) {
+        float4* sum = static_cast<float4*>(accum);
+        float4* comp = sum + wv.pixels;
+        float4 s = sum[px], c = comp[px];
+        for (uint32_t sl = 0; sl < wv.spw; ++sl) {
+            const float4 r = state[2 * ((size_t)sl * wv.pixels + slot)];
+            float yx = __fsub_rn(r.x, c.x), yy = __fsub_rn(r.y, c.y), yz = __fsub_rn(r.z, c.z);
+            float tx = __fadd_rn(s.x, yx), ty = __fadd_rn(s.y, yy), tz = __fadd_rn(s.z, yz);
+            c.x = __fsub_rn(__fsub_rn(tx, s.x), yx);
+            c.y = __fsub_rn(__fsub_rn(ty, s.y), yy);
+            c.z = __fsub_rn(__fsub_rn(tz, s.z), yz);
+            s.x = tx; s.y = ty; s.z = tz;
+            s.w = __fadd_rn(s.w, 1.0f);
+        }
+        sum[px] = s;
+        comp[px] = c;
+    } else if (mode == CPT_ACCUM_LERP) {
+        // cuda_path_tracer.cu:413-420: new = lerp(hit, prev, f / (f + 1))
+        float4* img = static_cast<float4*>(accum);
+        float4 p = img[px];
+        f3 prev = mk3(p.x, p.y, p.z);
+        for (uint32_t sl = 0; sl < wv.spw; ++sl) {
+            const float4 r = state[2 * ((size_t)sl * wv.pixels + slot)];
+            const float f = __uint2float_rn(wv.frame0 + wv.s0 + sl);
+            const float tt = __fdiv_rn(f, __fadd_rn(f, 1.0f));
+            prev = mix3(mk3(r.x, r.y, r.z), prev, tt);
+        }
+        img[px] = make_float4(prev.x, prev.y, prev.z, 1.0f);
+    } else {
+        double4* sum = static_cast<double4*>(accum);
+        double4 s = sum[px];
+        for (uint32_t sl = 0; sl < wv.spw; ++sl) {
+            const float4 r = state[2 * ((size_t)sl * wv.pixels + slot)];
+            s.x += (double)r.x; s.y += (double)r.y; s.z += (double)r.z; s.w += 1.0;
+        }
+        sum[px] = s;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_resolve(const void* __restrict__ accum, uint32_t pixels, uint32_t mode,
+                                                 float4* __restrict__ out)
+{
+    const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x;
+    if (px >= pixels) return;
+    if (mode == CPT_ACCUM_KAHAN) {
+        float4 s = static_cast<const float4*>(accum)[px];
+        float n = s.w;
+        out[px] = n > 0.f ? make_float4(__fdiv_rn(s.x, n), __fdiv_rn(s.y, n), __fdiv_rn(s.z, n), 1.0f)
+                          : make_float4(0.f, 0.f, 0.f, 1.0f);
+    } else if (mode == CPT_ACCUM_LERP) {
+        out[px] = static_cast<const float4*>(accum)[px];
+    } else {
+        double4 s = static_cast<const double4*>(accum)[px];
+        out[px] = s.w > 0.0 ? make_float4((float)(s.x / s.w), (float)(s.y / s.w), (float)(s.z / s.w), 1.0f)
+                            : make_float4(0.f, 0.f, 0.f, 1.0f);
+    }
+}
+
+struct RenderScratch {
+    float4* queue[2];
+    float4* hits;
+    float4* state;
+    uint32_t* counts;
+    uint32_t capacity;  // paths per wave
+};
+
+inline uint32_t wave_samples(const cpt_render_params* p)
+{
+    const uint64_t pixels = (uint64_t)p->width * p->height;
+    const uint64_t want = p->wave_paths ? p->wave_paths : kDefaultWavePaths;
+    uint64_t spw = want / pixels;
+    if (spw < 1) spw = 1;
+    if (spw > p->spp) spw = p->spp;
+    return (uint32_t)spw;
+}
+
+size_t render_layout(const cpt_render_params* p, void* base, RenderScratch* out)
+{
+    Carver c(base);
+    RenderScratch s;
+    const uint64_t pixels = (uint64_t)p->width * p->height;
+    s.capacity = (uint32_t)(pixels * wave_samples(p));
+    s.queue[0] = c.take<float4>(2ull * s.capacity);
+    s.queue[1] = c.take<float4>(2ull * s.capacity);
+    s.hits = c.take<float4>(s.capacity);
+    s.state = c.take<float4>(2ull * s.capacity);
+    s.counts = c.take<uint32_t>(kMaxDepth + 2);
+    if (out) *out = s;
+    return c.used();
+}
+
+bool params_ok(const cpt_render_params* p)
+{
+    if (!p || p->width == 0 || p->height == 0 || p->spp == 0) return false;
+    if ((uint64_t)p->width * p->height > (1ull << 31)) return false;
+    if (p->bounces + 1 > (uint32_t)kMaxDepth) return false;
+    if (p->accum_mode > CPT_ACCUM_F64) return false;
+    return (uint64_t)p->width * p->height * wave_samples(p) < (1ull << 31);
+}
+
+}  // namespace cpt
+
+using namespace cpt;
+
+extern "C" size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode)
+{
+    const size_t px = (size_t)width * height;
+    if (accum_mode == CPT_ACCUM_KAHAN) return px * 2 * sizeof(float4);
+    if (accum_mode == CPT_ACCUM_LERP) return px * sizeof(float4);
+    if (accum_mode == CPT_ACCUM_F64) return px * sizeof(double4);
+    return 0;
+}
+
+extern "C" size_t cpt_render_scratch_bytes(const cpt_render_params* params)
+{
+    if (!params_ok(params)) return 0;
+    return render_layout(params, nullptr, nullptr);
+}
+
+extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_camera* camera,
+                          const cpt_render_params* params, void* accum, void* scratch, size_t scratch_bytes,
+                          unsigned long long* ray_counts, uint32_t* status, cudaStream_t stream)
+{
+    if (!bvh || !scene || !camera || !accum || !scratch || !params_ok(params)) return CPT_ERR_INVALID_ARGUMENT;
+    if (!bvh->nodes || !bvh->tri_records || !scene->infos || (scene->light_count && !scene->lights))
+        return CPT_ERR_INVALID_ARGUMENT;
+    if (scratch_bytes < render_layout(params, nullptr, nullptr)) return CPT_ERR_SCRATCH_TOO_SMALL;
+    if ((reinterpret_cast<uintptr_t>(accum) & 15) || (reinterpret_cast<uintptr_t>(scratch) & 255))
+        return CPT_ERR_INVALID_ARGUMENT;
+    RenderScratch rs;
+    render_layout(params, scratch, &rs);
+    uint32_t* st = status ? status : bvh->status;
+
+    Camera cam;
+    for (int a = 0; a < 3; ++a) cam.eye[a] = camera->eye[a];
+    for (int c = 0; c < 4; ++c)
+        for (int a = 0; a < 3; ++a) cam.dirs[c][a] = camera->dirs[c][a];
+    for (int k = 0; k < 16; ++k) cam.m[k] = camera->inv_view_proj[k];
+    cam.jx = camera->jitter_x;
+    cam.jy = camera->jitter_y;
+    cam.jitter = camera->jitter;
+
+    Wave wv;
+    wv.width = params->width;
+    wv.height = params->height;
+    wv.pixels = params->width * params->height;
+    wv.frame0 = params->frame0;
+    wv.bounces = params->bounces;
+    wv.intensity = params->indirect_intensity;
+    wv.stratified = params->stratified;
+    wv.k0 = params->seed_lo;
+    wv.k1 = params->seed_hi;
+    wv.ref_w = params->ref_grid ? params->width / 8u * 8u : params->width;
+    wv.ref_h = params->ref_grid ? params->height / 8u * 8u : params->height;
+    wv.light_count = scene->light_count;
+
+    ShadeScene sc;
+    sc.nodes = static_cast<const float4*>(bvh->nodes);
+    sc.tris = static_cast<const float4*>(bvh->tri_records);
+    sc.infos = scene->infos;
+    sc.lights = scene->lights;
+
+    const int sms = sm_count();
+    const uint32_t spw_max = wave_samples(params);
+    for (uint32_t s0 = 0; s0 < params->spp; s0 += spw_max) {
+        wv.s0 = s0;
+        wv.spw = std::min(spw_max, params->spp - s0);
+        const uint32_t paths = wv.spw * wv.pixels;
+        CPT_CUDA_TRY(cudaMemsetAsync(rs.counts, 0, sizeof(uint32_t) * (kMaxDepth + 2), stream));
+        {
+            CPT_PROF(K_GENERATE, stream);
+            k_generate<<<(int)std::min<uint32_t>((paths + kGenBlock - 1) / kGenBlock, (uint32_t)sms * 16), kGenBlock, 0,
+                         stream>>>(wv, cam, rs.queue[0], rs.counts, rs.state);
+        }
+        CPT_LAUNCH_CHECK();
+        const int ext_blocks = std::min<int>((int)((paths + kExtendBlock - 1) / kExtendBlock), sms * 12);
+        const int shade_blocks = std::min<int>((int)((paths + kShadeBlock - 1) / kShadeBlock), sms * 16);
+        for (uint32_t b = 0; b <= params->bounces; ++b) {
+            const float4* qin = rs.queue[b & 1];
+            float4* qout = rs.queue[(b + 1) & 1];
+            {
+                CPT_PROF(K_EXTEND, stream);
+                if (params->trace_stats)
+                    k_extend<true><<<ext_blocks, kExtendBlock, 0, stream>>>(sc.nodes, sc.tris, qin, rs.counts + b, rs.hits,
+                                                                            ray_counts, st);
+                else
+                    k_extend<false><<<ext_blocks, kExtendBlock, 0, stream>>>(sc.nodes, sc.tris, qin, rs.counts + b,
+                                                                             rs.hits, ray_counts, st);
+            }
+            CPT_LAUNCH_CHECK();
+            {
+                CPT_PROF(K_SHADE, stream);
+                if (scene->light_count)
+                    k_shade<true><<<shade_blocks, kShadeBlock, 0, stream>>>(sc, wv, b, qin, rs.hits, rs.counts + b, qout,
+                                                                             rs.counts + b + 1, rs.state, ray_counts, st);
+                else
+                    k_shade<false><<<shade_blocks, kShadeBlock, 0, stream>>>(sc, wv, b, qin, rs.hits, rs.counts + b, qout,
+                                                                              rs.counts + b + 1, rs.state, ray_counts, st);
+            }
+            CPT_LAUNCH_CHECK();
+        }
+        if (ray_counts) {
+            {
+                CPT_PROF(K_WAVE_COUNTS, stream);
+                k_wave_counts<<<1, 32, 0, stream>>>(rs.counts, params->bounces + 1, ray_counts);
+            }
+            CPT_LAUNCH_CHECK();
+        }
+        {
+            CPT_PROF(K_ACCUMULATE, stream);
+            k_accumulate<<<(wv.pixels + 255) / 256, 256, 0, stream>>>(wv, params->accum_mode, rs.state, accum);
+        }
+        CPT_LAUNCH_CHECK();
+    }
+    return CPT_OK;
+}
+
+extern "C" int cpt_resolve(const void* accum, uint32_t width, uint32_t height, uint32_t accum_mode, float* rgba,
+                           cudaStream_t stream)
+{
+    if (!accum || !rgba || width == 0 || height == 0 || accum_mode > CPT_ACCUM_F64) return CPT_ERR_INVALID_ARGUMENT;
+    const uint32_t px = width * height;
+    {
+        CPT_PROF(K_RESOLVE, stream);
+        k_resolve<<<(px + 255) / 256, 256, 0, stream>>>(accum, px, accum_mode, reinterpret_cast<float4*>(rgba));
+    }
+    CPT_LAUNCH_CHECK();
+    return CPT_OK;
+}

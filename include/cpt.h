@@ -1,0 +1,233 @@
+/* cpt — B200-native LBVH builder and progressive path tracer (C ABI).
+ *
+ * Drop-in replacement for the hot path of compix/CUDA-Path-Tracer: a triangle
+ * soup goes in; the reference's BVH arrays, compact traversal nodes and an
+ * accumulated framebuffer come out. All functions are plain C with device
+ * pointers owned by the caller (unless a function says otherwise), an explicit
+ * CUDA stream and an int status (CPT_OK = 0). Work is enqueued on the stream and
+ * returns immediately unless a flag asks for a synchronous check.
+ *
+ * Layout structs mirror the reference byte for byte:
+ *   cpt_triangle       == CUDA::Triangle       (source/application/cuda/geometry.h:20-30)
+ *   cpt_bbox           == BBox                 (source/engine/geometry/BBox.h:6-53)
+ *   cpt_triangle_info  == CUDA::TriangleInfo   (source/application/cuda/TriangleInfo.h:14-75)
+ *   cpt_dir_light      == CUDA::DirectionalLight (source/application/cuda/Lights.h:6-11)
+ *   children / parents == Node / NodeIndex     (source/application/cuda/Node.h:8-137)
+ */
+#ifndef CPT_H
+#define CPT_H
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define CPT_OK 0
+#define CPT_ERR_INVALID_ARGUMENT 1  /* null pointer, n < 2, bad key width, size overflow */
+#define CPT_ERR_CUDA 2              /* a CUDA runtime call failed */
+#define CPT_ERR_SCRATCH_TOO_SMALL 3 /* scratch_bytes below the matching *_scratch_bytes() */
+#define CPT_ERR_NONFINITE_INPUT 4   /* a vertex coordinate is NaN or infinite */
+#define CPT_ERR_DEVICE_TIMEOUT 5    /* a bounded device-side wait gave up (sort look-back) */
+#define CPT_ERR_STACK_OVERFLOW 6    /* a ray needed more than CPT_TRAVERSAL_STACK entries */
+#define CPT_ERR_CHECK_FAILED 7      /* root box volume differs from the enclosing box's */
+#define CPT_ERR_NO_DEVICE 8         /* no CUDA device / library built for another arch */
+
+/* device status-word bits (cpt_bvh.status[0], render status) */
+#define CPT_STATUS_NONFINITE 1u
+#define CPT_STATUS_TIMEOUT 2u
+#define CPT_STATUS_STACK_OVERFLOW 4u
+
+#define CPT_TRAVERSAL_STACK 64 /* MAX_TRAVERSAL_STACK_SIZE, source/engine/cuda/cuda_defs.h:21 */
+#define CPT_INVALID_INDEX 0xFFFFFFFFu
+
+/* ---- reference layouts ---- */
+typedef struct cpt_triangle { float v0[3], v1[3], v2[3]; uint32_t info_idx; } cpt_triangle; /* 40 B */
+typedef struct cpt_bbox { float min[3], max[3]; } cpt_bbox;                                  /* 24 B */
+typedef struct cpt_vertex { float color[3], uv[2], normal[3], tangent[3], bitangent[3]; } cpt_vertex; /* 56 B */
+typedef struct cpt_material {
+    float emission[3];
+    float specularity;
+    uint32_t albedo_idx;     /* texture index or CPT_INVALID_INDEX (textures: not supported, ignored) */
+    uint32_t normal_map_idx; /* idem */
+} cpt_material;                                                                   /* 24 B */
+typedef struct cpt_triangle_info { cpt_vertex vertices[3]; cpt_material material; } cpt_triangle_info; /* 192 B */
+typedef struct cpt_dir_light { float color[3], direction[3], intensity; } cpt_dir_light;               /* 28 B */
+
+/* ---- LBVH ---- */
+/* Outputs of one build. Every pointer is device memory of the stated length;
+ * cpt_bvh_bind() carves them all out of one caller allocation. */
+typedef struct cpt_bvh {
+    uint32_t n;                 /* triangles (leaves); internal nodes are n - 1 */
+    int32_t morton_bits;        /* 30 (uint32 keys) or 63 (uint64 keys) */
+    cpt_triangle* tris;         /* [n]   triangles in Morton order (reference: permuted in place) */
+    void* keys;                 /* [n]   sorted Morton keys */
+    uint32_t* children;         /* [n-1] Node words: (left << 2) | rightInternal << 1 | leftInternal */
+    uint32_t* parents_leaf;     /* [n]   parent of each leaf */
+    uint32_t* parents_internal; /* [n-1] parent of each internal node; [0] = CPT_INVALID_INDEX */
+    cpt_bbox* node_boxes;       /* [n-1] internal node boxes */
+    void* nodes;                /* [n-1] 64-B traversal nodes: left box, right box, Node word */
+    void* tri_records;          /* [n]   48-B traversal triangles: v0|info, v1-v0, v2-v0 */
+    uint32_t* status;           /* [4]   device status words (CPT_STATUS_* bits in [0]) */
+} cpt_bvh;
+
+/* Bytes of device memory cpt_bvh_bind() needs for n triangles. */
+size_t cpt_bvh_bytes(uint32_t n, int morton_bits);
+/* Lays the cpt_bvh arrays out in mem (256-B aligned pieces). */
+int cpt_bvh_bind(void* mem, size_t bytes, uint32_t n, int morton_bits, cpt_bvh* out);
+/* Scratch bytes cpt_lbvh_build() needs (keys, sort buffers, look-back, counters). */
+size_t cpt_lbvh_scratch_bytes(uint32_t n, int morton_bits);
+
+#define CPT_BUILD_CHECK 1u /* synchronize, map device status to a code, verify the root box */
+
+/* Builds the LBVH of n >= 2 triangles.
+ * Replaces CUDA::BVHBuilder::build (source/application/cuda/BVHBuilder.h:15,
+ * BVHBuilder.cu:207-269). tris_in may equal bvh->tris (in-place, as the
+ * reference). enclosing_box is a HOST pointer to (min xyz, max xyz), as the
+ * reference's DeviceSceneDescription::enclosingBBox, or NULL to compute it on
+ * the device. Outputs are bit-identical to the reference's for the same inputs. */
+int cpt_lbvh_build(const cpt_triangle* tris_in, uint32_t n, const float* enclosing_box, int morton_bits,
+                   cpt_bvh* bvh, void* scratch, size_t scratch_bytes, uint32_t flags, cudaStream_t stream);
+
+/* Reads the device status words of a build or render (synchronizes the stream)
+ * and maps them to a status code. */
+int cpt_status_check(const uint32_t* d_status, cudaStream_t stream);
+
+/* ---- traversal ---- */
+typedef struct cpt_hit { float t, u, v; uint32_t tri; } cpt_hit; /* t = FLT_MAX, tri = CPT_INVALID_INDEX on miss */
+
+/* Closest hit (any_hit = 0) or occlusion (any_hit = 1) for n rays.
+ * Replaces CUDA::trace / CUDA::shadowRay (source/application/cuda/trace.h:45-50,73-169).
+ * rays: n x 8 floats (origin xyz, unused, direction xyz, unused), device.
+ * stats (nullable, device): n x 2 uint32 — internal nodes fetched, triangle tests. */
+int cpt_trace(const cpt_bvh* bvh, const float* rays, uint32_t n, int any_hit, cpt_hit* hits, uint32_t* stats,
+              cudaStream_t stream);
+
+/* ---- path tracer ---- */
+typedef struct cpt_scene {
+    const cpt_triangle_info* infos; /* device, indexed by cpt_triangle.info_idx */
+    uint32_t info_count;
+    const cpt_dir_light* lights;    /* device */
+    uint32_t light_count;
+} cpt_scene;
+
+/* Eye and the four corner ray directions (00, 10, 11, 01) of
+ * CUDAPathTracer::setPrimaryRays/setEyePos (cuda_path_tracer.h:19-21). With
+ * jitter = 1 the corner directions are re-derived per sample from
+ * inv_view_proj (column-major) with an NDC offset of up to +-jitter_x/y, the
+ * per-frame jitter of PathTracingApp::screenToRay (PathTracingApp.cpp:217-242). */
+typedef struct cpt_camera {
+    float eye[3];
+    float dirs[4][3];
+    float inv_view_proj[16];
+    float jitter_x, jitter_y;
+    uint32_t jitter;
+} cpt_camera;
+
+#define CPT_ACCUM_KAHAN 0u /* float4 sum (w = samples) + float4 compensation per pixel */
+#define CPT_ACCUM_LERP 1u  /* reference running mean: float4 per pixel (cuda_path_tracer.cu:413-420) */
+#define CPT_ACCUM_F64 2u   /* double4 sum (w = samples) per pixel, for the RMSE reference image */
+
+typedef struct cpt_render_params {
+    uint32_t width, height;
+    uint32_t spp;              /* samples rendered by this call */
+    uint32_t frame0;           /* global sample index of the first (reference frame number) */
+    uint32_t bounces;          /* indirectBounceCount (depth - 1) */
+    float indirect_intensity;  /* indirectIntensity */
+    uint32_t stratified;       /* useStratifiedSampling */
+    uint32_t seed_lo, seed_hi; /* Philox key */
+    uint32_t accum_mode;       /* CPT_ACCUM_* */
+    uint32_t ref_grid;         /* 1: render only the reference's (W/8*8) x (H/8*8) grid */
+    uint32_t wave_paths;       /* paths in flight per wave (0: library default) */
+    uint32_t trace_stats;      /* 1: count node fetches / triangle tests of extension rays (slower) */
+} cpt_render_params;
+
+size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode);
+size_t cpt_render_scratch_bytes(const cpt_render_params* params);
+
+/* Renders params->spp samples into accum. Replaces CUDAPathTracer::raytrace
+ * (cuda_path_tracer.cu:423-464) and raytrace_kernel (:385-421).
+ * ray_counts (device, nullable): CPT_RAY_COUNTS x uint64, incremented by
+ * [0] primary, [1] extension, [2] shadow rays traced, and — with
+ * params->trace_stats — [3] internal nodes fetched and [4] triangles tested by the
+ * closest-hit (primary + extension) rays. status (device, nullable): CPT_STATUS_*
+ * bits are OR-ed in. */
+#define CPT_RAY_COUNTS 8
+int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_camera* camera, const cpt_render_params* params,
+               void* accum, void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
+               cudaStream_t stream);
+
+/* Writes the displayable image (float4 rgba per pixel, alpha 1) of an accumulator. */
+int cpt_resolve(const void* accum, uint32_t width, uint32_t height, uint32_t accum_mode, float* rgba,
+                cudaStream_t stream);
+
+/* ---- reference-facing tracer object (host buffers in, image out) ----
+ * Mirrors CUDAPathTracer (source/application/cuda/cuda_path_tracer.h:13-40):
+ * upload a HostSceneDescription, set primary rays and eye, raytrace frame by
+ * frame, reset. Owns its device memory and stream. */
+typedef struct cpt_tracer cpt_tracer;
+int cpt_tracer_create(cpt_tracer** out, int morton_bits);
+void cpt_tracer_destroy(cpt_tracer* t);
+/* CUDAPathTracer::upload + Scene::upload (cuda_path_tracer.cu:466-470, Scene.cu:28-55):
+ * host triangles / infos / lights, host enclosing box (NULL: computed). */
+int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32_t n, const cpt_triangle_info* infos,
+                      uint32_t info_count, const cpt_dir_light* lights, uint32_t light_count,
+                      const float* enclosing_box);
+int cpt_tracer_set_primary_rays(cpt_tracer* t, const float dirs[12]);
+int cpt_tracer_set_eye(cpt_tracer* t, const float eye[3]);
+int cpt_tracer_set_camera(cpt_tracer* t, const cpt_camera* cam);
+/* GI settings (PathTracingSettings.h:26-28) and the seed of the random stream. */
+int cpt_tracer_set_settings(cpt_tracer* t, uint32_t bounces, float indirect_intensity, uint32_t stratified,
+                            uint32_t seed_lo, uint32_t seed_hi, uint32_t accum_mode);
+/* Renders spp samples (frames) at width x height; the frame counter advances by spp. */
+int cpt_tracer_raytrace(cpt_tracer* t, uint32_t width, uint32_t height, uint32_t spp);
+void cpt_tracer_reset_frames(cpt_tracer* t);
+uint32_t cpt_tracer_frame(const cpt_tracer* t);
+/* Copies the resolved image (float4 per pixel) to host memory; synchronizes. */
+int cpt_tracer_read_image(cpt_tracer* t, float* rgba_host);
+/* Rays traced since upload (primary, extension, shadow); synchronizes. */
+int cpt_tracer_ray_counts(cpt_tracer* t, unsigned long long out[3]);
+cudaStream_t cpt_tracer_stream(cpt_tracer* t);
+const cpt_bvh* cpt_tracer_bvh(const cpt_tracer* t);
+
+/* ---- synthetic scenes (host memory; the benchmark workloads) ---- */
+/* Random triangles: centroids U[0,1]^3, edge lengths U(edge_min, edge_max) along
+ * random unit vectors; plus a two-triangle emitter quad (light_size square at
+ * light_y facing -y, emission light_emission) when light_size > 0.
+ * albedo: grey vertex colour. Returns the triangle count written (n_random + 2). */
+uint32_t cpt_scene_random(uint32_t n_random, uint32_t seed, float edge_min, float edge_max, float albedo,
+                          float light_y, float light_size, float light_emission, cpt_triangle* tris,
+                          cpt_triangle_info* infos);
+/* Displaced sphere (lat-long grid nu x nv quads, radius 1 + amp * fBm) plus
+ * n_hair thin random "hairball" triangles in a ball of radius hair_radius, plus
+ * an emitter quad. Returns the triangle count (2*nu*nv + n_hair + 2). */
+uint32_t cpt_scene_sphere_hairball(uint32_t nu, uint32_t nv, float amp, uint32_t n_hair, float hair_radius,
+                                   uint32_t seed, float albedo, float light_y, float light_size,
+                                   float light_emission, cpt_triangle* tris, cpt_triangle_info* infos);
+/* Enclosing box (min, max) of a host triangle soup, as the reference's caller builds it. */
+void cpt_scene_bounds(const cpt_triangle* tris, uint32_t n, float out[6]);
+/* Camera corner directions for eye/target/up, vertical fov (degrees), aspect,
+ * near/far, with NDC jitter (jx, jy) — screenToRay (PathTracingApp.cpp:217-242).
+ * Fills cam (dirs, eye, inv_view_proj; jitter fields left to the caller). */
+void cpt_camera_look_at(const float eye[3], const float target[3], const float up[3], float fov_deg, float aspect,
+                        float znear, float zfar, cpt_camera* cam);
+
+/* ---- profiling: CUDA events around every kernel launch of the library ----
+ * Between begin and end, each launch is bracketed by two events recorded on its
+ * own stream. end() synchronizes those events and adds their elapsed times to
+ * per-kernel totals, which get() reads by kernel name (e.g. "k_extend"). */
+int cpt_profile_begin(void);
+int cpt_profile_end(void);
+int cpt_profile_get(const char* kernel, double* total_ms, unsigned long long* launches);
+
+/* ---- library info ---- */
+const char* cpt_version(void);
+/* Number of kernel launches the library has issued in this process. */
+unsigned long long cpt_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,232 @@
+"""ctypes access to the CPU oracle (liboracle.so) and, when it was compiled, to the
+reference's own builder / traversal (oracle/_ref/libref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as the
+checker and by bench.py's CPU-baseline leg. Nothing in the product imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libref.so")      # reference, 30-bit keys (as shipped)
+REF64_LIB = os.path.join(HERE, "_ref", "libref64.so")  # reference, 63-bit key configuration
+
+TRIANGLE_DTYPE = np.dtype([("v0", "<f4", 3), ("v1", "<f4", 3), ("v2", "<f4", 3), ("info_idx", "<u4")])
+BBOX_DTYPE = np.dtype([("min", "<f4", 3), ("max", "<f4", 3)])
+INVALID = 0xFFFFFFFF
+FLT_MAX = np.float32(3.4028234663852886e38)
+
+
+class OCam(ctypes.Structure):
+    _fields_ = [("eye", ctypes.c_float * 3), ("dirs", (ctypes.c_float * 3) * 4), ("inv_view_proj", ctypes.c_float * 16),
+                ("jitter_x", ctypes.c_float), ("jitter_y", ctypes.c_float), ("jitter", ctypes.c_uint32)]
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+_oracle = None
+_ref = {}
+
+
+def oracle_lib() -> ctypes.CDLL:
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_LIB):
+            raise ImportError(f"{ORACLE_LIB} missing: run `make -C oracle`")
+        L = ctypes.CDLL(ORACLE_LIB)
+        P, U, I, F = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_float
+        L.orc_morton.argtypes = [P, U, P, I, P]
+        L.orc_enclosing_box.argtypes = [P, U, P]
+        L.orc_build.argtypes = [P, U, P, I, P, P, P, P, P, P]
+        L.orc_build.restype = I
+        L.orc_trace.argtypes = [P, P, P, U, P, U, I, P, P, P, P]
+        L.orc_render.argtypes = [P, P, P, U, P, P, U, U, U, U, U, U, U, U, F, I, U, U, ctypes.POINTER(OCam), P, P]
+        L.orc_render_f64.argtypes = [P, P, P, U, P, P, U, U, U, U, U, U, F, I, U, U, ctypes.POINTER(OCam), P]
+        L.orc_philox.argtypes = [P, U, U, P]
+        L.orc_sincos_turns.argtypes = [P, U, P, P]
+        L.orc_corner_dirs.argtypes = [ctypes.POINTER(OCam), U, U, U, P]
+        _oracle = L
+    return _oracle
+
+
+def ref_available(bits: int = 30) -> bool:
+    return os.path.exists(REF_LIB if bits == 30 else REF64_LIB)
+
+
+def ref_lib(bits: int = 30) -> ctypes.CDLL:
+    if bits not in _ref:
+        path = REF_LIB if bits == 30 else REF64_LIB
+        if not os.path.exists(path):
+            raise ImportError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
+        L = ctypes.CDLL(path)
+        P, U, I, F = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_float
+        L.ref_build.argtypes = [P, U, P, I, P, P, P, P, P, P]
+        L.ref_build.restype = I
+        L.ref_set_geometry.argtypes = [P, P, P, U]
+        L.ref_trace.argtypes = [P, U, P, P, P, I]
+        L.ref_render.argtypes = [P, P, U, U, U, U, U, U, U, U, F, I, U, U, P, P, P, I]
+        L.ref_render.restype = I
+        _ref[bits] = L
+    return _ref[bits]
+
+
+class BuildResult:
+    def __init__(self, n: int, bits: int):
+        self.tris = np.zeros(n, TRIANGLE_DTYPE)
+        self.keys = np.zeros(n, np.uint32 if bits == 30 else np.uint64)
+        self.children = np.zeros(n - 1, np.uint32)
+        self.parents_leaf = np.zeros(n, np.uint32)
+        self.parents_internal = np.zeros(n - 1, np.uint32)
+        self.node_boxes = np.zeros(n - 1, BBOX_DTYPE)
+
+    def arrays(self):
+        return (self.tris, self.keys, self.children, self.parents_leaf, self.parents_internal, self.node_boxes)
+
+
+def enclosing_box(tris: np.ndarray) -> np.ndarray:
+    out = np.zeros(6, np.float32)
+    oracle_lib().orc_enclosing_box(_p(tris), len(tris), _p(out))
+    return out
+
+
+def morton(tris: np.ndarray, box: np.ndarray, bits: int) -> np.ndarray:
+    keys = np.zeros(len(tris), np.uint32 if bits == 30 else np.uint64)
+    oracle_lib().orc_morton(_p(tris), len(tris), _p(np.ascontiguousarray(box, np.float32)), bits, _p(keys))
+    return keys
+
+
+def build(tris: np.ndarray, bits: int, box=None, use_ref: bool = False) -> BuildResult:
+    tris = np.ascontiguousarray(tris)
+    n = len(tris)
+    box = enclosing_box(tris) if box is None else np.ascontiguousarray(box, np.float32)
+    r = BuildResult(n, bits)
+    fn = ref_lib(bits).ref_build if use_ref else oracle_lib().orc_build
+    rc = fn(_p(tris), n, _p(box), bits, *[_p(a) for a in r.arrays()])
+    if rc != 0:
+        raise ValueError(f"build rejected its input (rc {rc})")
+    return r
+
+
+def trace(b: BuildResult, rays: np.ndarray, any_hit: bool = False, use_ref: bool = False, stats: bool = False,
+          threads: int = 0):
+    """rays: (m, 6) float32 origin+direction. Returns (t, idx, uv[, stats(m,5)])."""
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+    m = len(rays)
+    t = np.zeros(m, np.float32)
+    idx = np.zeros(m, np.uint32)
+    uv = np.zeros((m, 2), np.float32)
+    st = np.zeros((m, 5), np.uint64) if stats else None
+    if use_ref:
+        if any_hit:
+            raise ValueError("the reference has closest-hit traversal only")
+        L = ref_lib()
+        L.ref_set_geometry(_p(b.tris), _p(b.children), _p(b.node_boxes), len(b.tris))
+        L.ref_trace(_p(rays), m, _p(t), _p(idx), _p(uv), threads)
+    else:
+        oracle_lib().orc_trace(_p(b.tris), _p(b.children), _p(b.node_boxes), len(b.tris), _p(rays), m, int(any_hit),
+                               _p(t), _p(idx), _p(uv), _p(st))
+    return (t, idx, uv, st) if stats else (t, idx, uv)
+
+
+def ocam_from(eye, dirs, inv_view_proj=None, jitter=0, jitter_x=0.0, jitter_y=0.0) -> OCam:
+    c = OCam()
+    for a in range(3):
+        c.eye[a] = float(eye[a])
+    d = np.asarray(dirs, np.float32).reshape(4, 3)
+    for i in range(4):
+        for a in range(3):
+            c.dirs[i][a] = float(d[i, a])
+    if inv_view_proj is not None:
+        m = np.asarray(inv_view_proj, np.float32).reshape(16)
+        for k in range(16):
+            c.inv_view_proj[k] = float(m[k])
+    c.jitter = int(jitter)
+    c.jitter_x = float(jitter_x)
+    c.jitter_y = float(jitter_y)
+    return c
+
+
+def render(b: BuildResult, infos: np.ndarray, lights, width: int, height: int, spp: int, frame0: int, bounces: int,
+           intensity: float, stratified: bool, seed: int, cam: OCam, rows=None):
+    """Per-sample radiance (spp, rows, width, 3) float32 and ray counts (3,)."""
+    r0, r1 = (0, height) if rows is None else rows
+    rad = np.zeros((spp, r1 - r0, width, 3), np.float32)
+    counts = np.zeros(3, np.uint64)
+    nl = 0 if lights is None else len(lights)
+    oracle_lib().orc_render(_p(b.tris), _p(b.children), _p(b.node_boxes), len(b.tris), _p(infos),
+                            _p(lights) if nl else None, nl, width, height, r0, r1, spp, frame0, bounces, intensity,
+                            int(stratified), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, ctypes.byref(cam), _p(rad),
+                            _p(counts))
+    return rad, counts
+
+
+def render_f64(b: BuildResult, infos: np.ndarray, lights, width: int, height: int, spp: int, frame0: int, bounces: int,
+               intensity: float, stratified: bool, seed: int, cam: OCam) -> np.ndarray:
+    out = np.zeros((height, width, 3), np.float64)
+    nl = 0 if lights is None else len(lights)
+    oracle_lib().orc_render_f64(_p(b.tris), _p(b.children), _p(b.node_boxes), len(b.tris), _p(infos),
+                                _p(lights) if nl else None, nl, width, height, spp, frame0, bounces, intensity,
+                                int(stratified), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, ctypes.byref(cam),
+                                _p(out))
+    return out
+
+
+def ref_render(b: BuildResult, infos: np.ndarray, lights, width: int, height: int, rows, spp: int, frame0: int,
+               bounces: int, intensity: float, stratified: bool, seed: int, cam15: np.ndarray, threads: int = 0):
+    """Reference-function integrator: per-pixel f32 sum over spp for rows [r0, r1); ray counts."""
+    L = ref_lib()
+    L.ref_set_geometry(_p(b.tris), _p(b.children), _p(b.node_boxes), len(b.tris))
+    r0, r1 = rows
+    out = np.zeros((r1 - r0, width, 3), np.float32)
+    counts = np.zeros(3, np.uint64)
+    nl = 0 if lights is None else len(lights)
+    cam15 = np.ascontiguousarray(cam15, np.float32)
+    L.ref_render(_p(infos), _p(lights) if nl else None, nl, width, height, r0, r1, spp, frame0, bounces, intensity,
+                 int(stratified), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, _p(cam15), _p(out), _p(counts),
+                 threads)
+    return out, counts
+
+
+def philox(ctr, k0: int, k1: int) -> np.ndarray:
+    c = np.asarray(ctr, np.uint32)
+    out = np.zeros(4, np.uint32)
+    oracle_lib().orc_philox(_p(c), k0, k1, _p(out))
+    return out
+
+
+def sincos_turns(u: np.ndarray):
+    u = np.ascontiguousarray(u, np.float32)
+    s = np.zeros_like(u)
+    c = np.zeros_like(u)
+    oracle_lib().orc_sincos_turns(_p(u), len(u), _p(s), _p(c))
+    return s, c
+
+
+# ---------------------------------------------------------------- accumulators (numpy float32 = IEEE per op)
+def accumulate_kahan(samples: np.ndarray):
+    """samples (spp, ..., 3) in sample order -> (sum, comp, count) as the device's Kahan accumulator."""
+    s = np.zeros(samples.shape[1:], np.float32)
+    c = np.zeros(samples.shape[1:], np.float32)
+    for x in samples:
+        y = (x - c).astype(np.float32)
+        t = (s + y).astype(np.float32)
+        c = ((t - s).astype(np.float32) - y).astype(np.float32)
+        s = t
+    return s, c, np.float32(len(samples))
+
+
+def accumulate_lerp(samples: np.ndarray, frame0: int, prev=None):
+    """Reference running mean (cuda_path_tracer.cu:416-417): img = hit + t * (prev - hit), t = f / (f + 1)."""
+    img = np.zeros(samples.shape[1:], np.float32) if prev is None else prev.astype(np.float32)
+    for s, x in enumerate(samples):
+        f = np.float32(frame0 + s)
+        t = np.float32(f / np.float32(f + np.float32(1.0)))
+        img = (x + (t * (img - x).astype(np.float32)).astype(np.float32)).astype(np.float32)
+    return img

@@ -1,0 +1,147 @@
+"""The C-ABI library on the CPU: it loads, exports exactly what include/cpt.h
+declares, sizes its buffers sensibly, rejects bad arguments before touching the
+device, and its host-side scene / camera helpers behave."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import cpt
+from conftest import ROOT
+from oracle import cpu
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "cpt.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"\b(cpt_[a-z0-9_]+)\s*\(", src)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_function():
+    names = declared_functions()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(cpt.lib, n), n
+    assert set(names) == set(cpt.EXPORTED)
+
+
+def test_version_and_launch_counter():
+    assert b"sm_100a" in cpt.lib.cpt_version()
+    assert cpt.launch_count() >= 0
+
+
+def test_layouts_match_reference():
+    assert cpt.TRIANGLE_DTYPE.itemsize == cpu.oracle_lib().orc_sizeof_triangle() == 40
+    assert cpt.BBOX_DTYPE.itemsize == cpu.oracle_lib().orc_sizeof_bbox() == 24
+    assert cpt.TRIANGLE_INFO_DTYPE.itemsize == cpu.oracle_lib().orc_sizeof_triangle_info() == 192
+    if cpu.ref_available(30):
+        r = cpu.ref_lib(30)
+        assert r.ref_sizeof_triangle() == 40 and r.ref_sizeof_bbox() == 24
+        assert r.ref_sizeof_node() == 4 and r.ref_sizeof_triangle_info() == 192
+
+
+@pytest.mark.parametrize("bits", [30, 63])
+def test_buffer_sizes(bits):
+    k = 4 if bits == 30 else 8
+    for n in (2, 3, 1000, 1 << 20):
+        outputs = n * 40 + n * k + (n - 1) * 4 + n * 4 + (n - 1) * 4 + (n - 1) * 24 + (n - 1) * 64 + n * 48
+        assert outputs <= cpt.bvh_bytes(n, bits) <= outputs + 10 * 256
+        s = cpt.lbvh_scratch_bytes(n, bits)
+        assert s >= n * (k + 8)
+    assert cpt.bvh_bytes(1, bits) == 0 and cpt.lbvh_scratch_bytes(1, bits) == 0
+    assert cpt.bvh_bytes(100, 31) == 0
+
+
+def test_bind_lays_out_disjoint_aligned_arrays():
+    n = 1000
+    size = cpt.bvh_bytes(n, 63)
+    b = cpt.bvh_bind(1 << 20, size, n, 63)
+    ptrs = [b.tris, b.keys, b.children, b.parents_leaf, b.parents_internal, b.node_boxes, b.nodes, b.tri_records,
+            b.status]
+    assert all(p % 256 == 0 for p in ptrs)
+    assert ptrs == sorted(ptrs) and ptrs[-1] < (1 << 20) + size
+    with pytest.raises(cpt.CptError) as e:
+        cpt.bvh_bind(1 << 20, size - 1, n, 63)
+    assert e.value.code == cpt.ERR_SCRATCH_TOO_SMALL
+
+
+def test_build_rejects_bad_arguments_without_device_work():
+    b = cpt.bvh_bind(1 << 20, cpt.bvh_bytes(100, 30), 100, 30)
+    for args in [(0, 100, 30), (256, 1, 30), (256, 100, 31)]:
+        with pytest.raises(cpt.CptError) as e:
+            cpt.lbvh_build(args[0], args[1], args[2], b, 1 << 30, 1 << 30)
+        assert e.value.code == cpt.ERR_INVALID_ARGUMENT
+    with pytest.raises(cpt.CptError) as e:  # scratch smaller than required
+        cpt.lbvh_build(256, 100, 30, b, 1 << 30, 16)
+    assert e.value.code == cpt.ERR_SCRATCH_TOO_SMALL
+    with pytest.raises(cpt.CptError) as e:  # misaligned triangle pointer
+        cpt.lbvh_build(260, 100, 30, b, 1 << 30, 1 << 30)
+    assert e.value.code == cpt.ERR_INVALID_ARGUMENT
+
+
+def test_render_sizes_and_rejections():
+    from cpt import RenderParams
+    p = RenderParams(64, 48, 4, 0, 3, 3.0, 1, 0, 0, cpt.ACCUM_KAHAN, 0, 0)
+    s = cpt.render_scratch_bytes(p)
+    assert s >= 64 * 48 * 4 * (32 * 2 + 16 + 32)
+    assert cpt.accum_bytes(64, 48, cpt.ACCUM_KAHAN) == 64 * 48 * 32
+    assert cpt.accum_bytes(64, 48, cpt.ACCUM_LERP) == 64 * 48 * 16
+    assert cpt.accum_bytes(64, 48, cpt.ACCUM_F64) == 64 * 48 * 32
+    bad = RenderParams(0, 48, 4, 0, 3, 3.0, 1, 0, 0, 0, 0, 0)
+    assert cpt.render_scratch_bytes(bad) == 0
+    deep = RenderParams(8, 8, 1, 0, 100, 3.0, 1, 0, 0, 0, 0, 0)
+    assert cpt.render_scratch_bytes(deep) == 0
+
+
+def test_scene_random_geometry():
+    tris, infos = cpt.scene_random(5000, seed=1, edge_min=0.005, edge_max=0.02, light_y=1.25, light_size=0.5)
+    assert len(tris) == 5002
+    v = np.stack([tris["v0"], tris["v1"], tris["v2"]], 1)[:5000]
+    cen = v.mean(1)
+    assert cen.min() > -0.03 and cen.max() < 1.03
+    # vertices are centre + e_k * u_k with e_k < 0.02: pairwise distances below 0.04
+    for a, b in ((0, 1), (1, 2), (0, 2)):
+        assert np.linalg.norm(v[:, a] - v[:, b], axis=1).max() < 0.0401
+    assert np.all(tris["info_idx"] == np.arange(5002))
+    e = infos["material"]["emission"]
+    assert np.all(e[:5000] == 0) and np.all(e[5000:] == 10)
+    assert np.allclose(tris[5000:]["v0"][:, 1], 1.25)
+    again = cpt.scene_random(5000, seed=1)[0]
+    assert again.tobytes() == tris.tobytes()
+    assert cpt.scene_random(5000, seed=2)[0].tobytes() != tris.tobytes()
+
+
+def test_scene_sphere_hairball_geometry():
+    tris, infos = cpt.scene_sphere_hairball(64, 32, 2000, seed=3)
+    assert len(tris) == 2 * 64 * 32 + 2000 + 2
+    sph = np.stack([tris["v0"], tris["v1"], tris["v2"]], 1)[: 2 * 64 * 32]
+    r = np.linalg.norm(sph, axis=2)
+    assert r.min() > 0.85 and r.max() < 1.15
+    hair = np.stack([tris["v0"], tris["v1"], tris["v2"]], 1)[2 * 64 * 32: -2]
+    length = np.linalg.norm(hair[:, 1] - hair[:, 0], axis=1)
+    assert length.min() >= 0.0499 and length.max() <= 0.2001
+    assert np.linalg.norm(hair.mean(1), axis=1).max() < 1.3 + 0.11
+
+
+def test_scene_bounds_equals_oracle():
+    tris, _ = cpt.scene_random(3000, seed=9)
+    assert np.array_equal(cpt.scene_bounds(tris), cpu.enclosing_box(tris))
+
+
+def test_camera_corners_match_oracle_unjittered():
+    cam = cpt.camera_look_at((0.5, 0.5, -1.2), (0.5, 0.5, 0.0), fov_deg=45.0, aspect=1.0)
+    d = cam.as_array()[3:].reshape(4, 3)
+    assert np.allclose(np.linalg.norm(d, axis=1), 1.0, atol=1e-6)
+    # right-handed look-at along +z: screen right is world -x; 00 is bottom-left, 11 top-right
+    assert d[0][1] < 0 and d[1][1] < 0 and d[2][1] > 0 and d[3][1] > 0
+    assert d[0][0] > 0 and d[1][0] < 0 and np.isclose(d[0][0], -d[1][0], atol=1e-6)
+    t = np.tan(np.radians(22.5))
+    assert np.allclose(d[:, 2], 1.0 / np.sqrt(1.0 + 2.0 * t * t), atol=1e-6)
+    # the unjittered per-sample derivation from inv_view_proj reproduces the corners
+    o = cpu.ocam_from(cam.eye, d, np.ctypeslib.as_array(cam.inv_view_proj), jitter=1, jitter_x=0.0, jitter_y=0.0)
+    out = np.zeros((4, 3), np.float32)
+    cpu.oracle_lib().orc_corner_dirs(ctypes.byref(o), 0, 0, 0, out.ctypes.data)
+    assert np.allclose(out, d, atol=2e-6)

@@ -1,0 +1,186 @@
+"""Wavefront path tracer on the GPU against the oracle's restatement of the
+reference estimator (same Philox stream): per-pixel accumulators bit-exact for
+the Kahan, running-lerp and FP64 modes; ray counts exact; the tracer object
+(host buffers in, image out) equal to the device path."""
+import numpy as np
+import pytest
+import torch
+
+import cpt
+from cpt.device import DeviceLbvh, DeviceRenderer, DeviceScene, make_params, to_device
+from oracle import cpu
+
+pytestmark = pytest.mark.gpu
+
+W, H = 64, 48
+
+
+def scene(n=20_000, seed=5, lights=None, spec=0.0):
+    tris, infos = cpt.scene_random(n, seed=seed)
+    infos["material"]["specularity"][: len(infos) - 2] = spec
+    cam = cpt.camera_look_at((0.5, 0.5, -1.2), (0.5, 0.5, 0.0), aspect=W / H)
+    return tris, infos, lights, cam
+
+
+def dir_lights():
+    l = np.zeros(2, cpt.DIR_LIGHT_DTYPE)
+    l[0] = ((1.0, 0.9, 0.8), (0.3, -1.0, 0.2), 1.5)
+    l[1] = ((0.2, 0.3, 1.0), (-0.5, -0.7, 0.4), 0.7)
+    l["direction"] /= np.linalg.norm(l["direction"], axis=1, keepdims=True)
+    return l.astype(cpt.DIR_LIGHT_DTYPE)
+
+
+def ocam(cam, jitter=False):
+    return cpu.ocam_from(cam.eye, cam.as_array()[3:], np.ctypeslib.as_array(cam.inv_view_proj), jitter=int(jitter),
+                         jitter_x=2.0 / W, jitter_y=2.0 / H)
+
+
+def gpu_render(tris, infos, lights, cam, mode, spp=4, frame0=5, bounces=3, seed=77, bits=30, jitter=False,
+               wave_paths=0, ref_grid=False, w=W, h=H, stratified=True):
+    lb = DeviceLbvh(len(tris), bits)
+    lb.build(to_device(tris), check_root=True)
+    sc = DeviceScene(infos, lights)
+    c = cpt.Camera.from_buffer_copy(cam)
+    c.jitter, c.jitter_x, c.jitter_y = int(jitter), 2.0 / w, 2.0 / h
+    r = DeviceRenderer(make_params(w, h, spp, frame0, bounces, 3.0, stratified, seed, mode, ref_grid, wave_paths))
+    r.render(lb, sc, c)
+    torch.cuda.synchronize()
+    r.check_status()
+    return r, lb
+
+
+def oracle_samples(tris, infos, lights, cam, spp=4, frame0=5, bounces=3, seed=77, bits=30, jitter=False, w=W, h=H,
+                   stratified=True):
+    b = cpu.build(tris, bits)
+    return cpu.render(b, infos, lights, w, h, spp, frame0, bounces, 3.0, stratified, seed, ocam(cam, jitter))
+
+
+def accum_arrays(r, mode):
+    a = r.accum.cpu().numpy().view(np.uint8)
+    if mode == cpt.ACCUM_KAHAN:
+        f = a.view(np.float32).reshape(2, H, W, 4)
+        return f[0], f[1]
+    if mode == cpt.ACCUM_LERP:
+        return a.view(np.float32).reshape(H, W, 4), None
+    return a.view(np.float64).reshape(H, W, 4), None
+
+
+@pytest.mark.parametrize("bits", [30, 63])
+def test_kahan_accumulator_bit_exact(cuda, bits):
+    tris, infos, lights, cam = scene()
+    r, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_KAHAN, bits=bits)
+    rad, counts = oracle_samples(tris, infos, lights, cam, bits=bits)
+    s, c, n = cpu.accumulate_kahan(rad)
+    gs, gc = accum_arrays(r, cpt.ACCUM_KAHAN)
+    assert (rad.sum(axis=(0, 1, 2)) > 0).all(), "scene should receive light"
+    assert gs[..., :3].tobytes() == s.tobytes()
+    assert gc[..., :3].tobytes() == c.tobytes()
+    assert np.all(gs[..., 3] == n)
+    assert np.array_equal(r.counts.cpu().numpy()[:3].astype(np.uint64), counts)
+    img = r.resolve().cpu().numpy()
+    assert img[..., :3].tobytes() == (s / n).astype(np.float32).tobytes()
+
+
+def test_lerp_accumulator_matches_reference_running_mean(cuda):
+    tris, infos, lights, cam = scene()
+    r, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_LERP, frame0=0)
+    rad, _ = oracle_samples(tris, infos, lights, cam, frame0=0)
+    img, _ = accum_arrays(r, cpt.ACCUM_LERP)
+    assert img[..., :3].tobytes() == cpu.accumulate_lerp(rad, 0).tobytes()
+    assert np.all(img[..., 3] == 1.0)
+
+
+def test_f64_accumulator(cuda):
+    tris, infos, lights, cam = scene()
+    r, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_F64)
+    rad, _ = oracle_samples(tris, infos, lights, cam)
+    acc, _ = accum_arrays(r, cpt.ACCUM_F64)
+    want = np.zeros((H, W, 3), np.float64)
+    for x in rad:
+        want += x.astype(np.float64)
+    assert acc[..., :3].tobytes() == want.tobytes()
+
+
+def test_camera_jitter_per_sample(cuda):
+    tris, infos, lights, cam = scene()
+    r, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_KAHAN, jitter=True)
+    rad, _ = oracle_samples(tris, infos, lights, cam, jitter=True)
+    s, c, _ = cpu.accumulate_kahan(rad)
+    gs, _ = accum_arrays(r, cpt.ACCUM_KAHAN)
+    assert gs[..., :3].tobytes() == s.tobytes()
+
+
+def test_wave_size_does_not_change_the_image(cuda):
+    tris, infos, lights, cam = scene()
+    a, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_KAHAN, spp=6, wave_paths=W * H)
+    b, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_KAHAN, spp=6, wave_paths=4 * W * H)
+    c, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_KAHAN, spp=6)
+    assert a.accum.cpu().numpy().tobytes() == b.accum.cpu().numpy().tobytes() == c.accum.cpu().numpy().tobytes()
+
+
+def test_directional_lights_shadow_rays(cuda):
+    tris, infos, _, cam = scene()
+    lights = dir_lights()
+    r, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_KAHAN)
+    rad, counts = oracle_samples(tris, infos, lights, cam)
+    s, _, _ = cpu.accumulate_kahan(rad)
+    gs, _ = accum_arrays(r, cpt.ACCUM_KAHAN)
+    assert counts[2] > 0
+    assert gs[..., :3].tobytes() == s.tobytes()  # shininess 0: no pow() in play, bit-exact
+    assert np.array_equal(r.counts.cpu().numpy()[:3].astype(np.uint64), counts)
+
+
+def test_specular_term_within_tolerance(cuda):
+    # powf differs between CUDA and the host libm by at most a few ulp; the
+    # specular term is a colour, it does not steer rays: relative 1e-5.
+    tris, infos, _, cam = scene(spec=32.0)
+    lights = dir_lights()
+    r, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_KAHAN)
+    rad, _ = oracle_samples(tris, infos, lights, cam)
+    s, _, _ = cpu.accumulate_kahan(rad)
+    gs, _ = accum_arrays(r, cpt.ACCUM_KAHAN)
+    np.testing.assert_allclose(gs[..., :3], s, rtol=1e-5, atol=1e-6)
+
+
+def test_reference_grid_truncation(cuda):
+    w, h = 70, 50
+    tris, infos, lights, _ = scene()
+    cam = cpt.camera_look_at((0.5, 0.5, -1.2), (0.5, 0.5, 0.0), aspect=w / h)
+    lb = DeviceLbvh(len(tris), 30)
+    lb.build(to_device(tris))
+    sc = DeviceScene(infos, None)
+    r = DeviceRenderer(make_params(w, h, 2, 0, 2, 3.0, True, 1, cpt.ACCUM_KAHAN, True, 0))
+    r.render(lb, sc, cam)
+    torch.cuda.synchronize()
+    acc = r.accum.cpu().numpy().view(np.float32).reshape(2, h, w, 4)[0]
+    assert np.all(acc[:48, :64, 3] == 2) and np.all(acc[48:, :, 3] == 0) and np.all(acc[:, 64:, 3] == 0)
+    b = cpu.build(tris, 30)
+    rad, _ = cpu.render(b, infos, None, w, h, 2, 0, 2, 3.0, True, 1, cpu.ocam_from(cam.eye, cam.as_array()[3:]))
+    s, _, _ = cpu.accumulate_kahan(rad)
+    assert acc[:48, :64, :3].tobytes() == np.ascontiguousarray(s[:48, :64]).tobytes()
+
+
+def test_tracer_object_host_buffers(cuda):
+    """cpt_tracer (CUDAPathTracer): upload host soup, set rays and eye, raytrace
+    frame by frame, read the image — equals the oracle."""
+    tris, infos, _, cam = scene(n=8000)
+    t = cpt.Tracer(63)
+    t.upload(tris, infos)
+    t.set_settings(bounces=2, intensity=3.0, stratified=True, seed=123, accum_mode=cpt.ACCUM_KAHAN)
+    t.set_primary_rays(cam.as_array()[3:])
+    t.set_eye(cam.as_array()[:3])
+    t.raytrace(W, H, 1)
+    t.raytrace(W, H, 2)
+    assert t.frame == 3
+    img = t.read_image(W, H)
+    b = cpu.build(tris, 63)
+    rad, counts = cpu.render(b, infos, None, W, H, 3, 0, 2, 3.0, True, 123, cpu.ocam_from(cam.eye, cam.as_array()[3:]))
+    s, _, n = cpu.accumulate_kahan(rad)
+    assert img[..., :3].tobytes() == (s / n).astype(np.float32).tobytes()
+    assert np.array_equal(t.ray_counts(), counts)
+    t.reset_frames()
+    t.raytrace(W, H, 1)
+    img1 = t.read_image(W, H)
+    s1, _, _ = cpu.accumulate_kahan(rad[:1])
+    assert img1[..., :3].tobytes() == s1.tobytes()
+    t.close()
