@@ -366,7 +366,7 @@ def run_ours(args, w, world, rank, local):
 
     # --- end to end through the tracer object (host buffers, pinned)
     e2e = None
-    if rank == 0 or world > 1:
+    if not args.no_e2e:
         tr = cpt.Tracer(w["bits"])
         tr.set_settings(bounces=w["bounces"], intensity=3.0, stratified=True, seed=w["seed"] + 7919 * rank)
         tr.set_camera(cam)
@@ -389,7 +389,6 @@ def run_ours(args, w, world, rank, local):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         ne = max(2, min(args.steps, 5))
-        c0 = tr.ray_counts()
         w0 = time.perf_counter()
         e0.record(ts)
         for _ in range(ne):
@@ -397,9 +396,10 @@ def run_ours(args, w, world, rank, local):
         e1.record(ts)
         e1.synchronize()
         wall = time.perf_counter() - w0
-        c1 = tr.ray_counts()
+        # upload() restarts the frame counter and the ray counters: every step renders
+        # the same first frame, and the counters hold one step's rays
         e_ms = e0.elapsed_time(e1)
-        e_rays = float(c1.sum()) if c1.sum() < c0.sum() else float((c1 - c0).sum())
+        e_rays = float(tr.ray_counts().sum()) * ne
         e_ms_max = max_over_ranks(e_ms, world)
         e_rays_all = sum_over_ranks(e_rays, world)
         e2e = {"value": round(e_rays_all / (e_ms_max / 1e3) / 1e6, 3), "unit": METRIC,
@@ -438,8 +438,15 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--res", default=None, help="override resolution WxH (profiling runs)")
+    ap.add_argument("--spp", type=int, default=None, help="override samples per frame (profiling runs)")
     args = ap.parse_args()
-    w = WORKLOADS[args.workload]
+    w = dict(WORKLOADS[args.workload])
+    if args.res:
+        w["width"], w["height"] = (int(x) for x in args.res.lower().split("x"))
+    if args.spp:
+        w["spp"] = args.spp
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))

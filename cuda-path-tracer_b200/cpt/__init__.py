@@ -31,9 +31,10 @@ ERRORS = {
     6: "traversal stack overflow",
     7: "root box volume differs from the enclosing box",
     8: "no CUDA device",
+    9: "device-side index out of range (corrupt input)",
 }
 ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_SCRATCH_TOO_SMALL, ERR_NONFINITE_INPUT = 1, 2, 3, 4
-ERR_DEVICE_TIMEOUT, ERR_STACK_OVERFLOW, ERR_CHECK_FAILED, ERR_NO_DEVICE = 5, 6, 7, 8
+ERR_DEVICE_TIMEOUT, ERR_STACK_OVERFLOW, ERR_CHECK_FAILED, ERR_NO_DEVICE, ERR_BAD_INDEX = 5, 6, 7, 8, 9
 BUILD_CHECK = 1
 ACCUM_KAHAN, ACCUM_LERP, ACCUM_F64 = 0, 1, 2
 INVALID_INDEX = 0xFFFFFFFF
@@ -61,7 +62,7 @@ class Bvh(ctypes.Structure):
     _fields_ = [("n", ctypes.c_uint32), ("morton_bits", ctypes.c_int32), ("tris", ctypes.c_void_p),
                 ("keys", ctypes.c_void_p), ("children", ctypes.c_void_p), ("parents_leaf", ctypes.c_void_p),
                 ("parents_internal", ctypes.c_void_p), ("node_boxes", ctypes.c_void_p), ("nodes", ctypes.c_void_p),
-                ("tri_records", ctypes.c_void_p), ("status", ctypes.c_void_p)]
+                ("status", ctypes.c_void_p)]
 
 
 class Scene(ctypes.Structure):

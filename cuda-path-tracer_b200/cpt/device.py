@@ -71,8 +71,7 @@ class DeviceLbvh:
             "parents_leaf": get(b.parents_leaf, np.uint32, n),
             "parents_internal": get(b.parents_internal, np.uint32, n - 1),
             "node_boxes": get(b.node_boxes, BBOX_DTYPE, n - 1),
-            "nodes": get(b.nodes, np.float32, 16 * (n - 1)).reshape(n - 1, 16),
-            "tri_records": get(b.tri_records, np.float32, 12 * n).reshape(n, 12),
+            "nodes": get(b.nodes, np.float32, 24 * (n - 1)).reshape(n - 1, 24),
         }
 
     def trace(self, rays: torch.Tensor, any_hit: bool = False, stats: bool = False):

@@ -12,6 +12,7 @@
 //   k_onesweep x P     thrust::sort_by_key (BVHBuilder.cu:234) K+4 B in, K+4 B out per pass
 //   k_topology         radix_tree_construction_kernel (:107-201) keys -> Node, parents
 //   k_gather_refit     compute_internal_node_bbox_kernel (:39-98) + the triangle permutation
+//                      + the 96-B traversal nodes (child slots filled bottom-up)
 //
 // The sort is a least-significant-digit radix sort with 8-bit digits in the
 // onesweep form (one global histogram pass, then one pass per digit in which each
@@ -386,99 +387,115 @@ __global__ void __launch_bounds__(256) k_topology(const K* __restrict__ keys, ui
     else parents_leaf[s + 1] = (uint32_t)i;
     const uint32_t word = ((uint32_t)s << 2) | type;
     children[i] = word;
-    nodes[4 * (size_t)i + 3] = make_float4(__uint_as_float(word), 0.0f, 0.0f, 0.0f);
+    nodes[6 * (size_t)i + 5] = make_float4(__uint_as_float(word), 0.0f, 0.0f, 0.0f);
     counters[i] = 0;
     if (i == 0) parents_internal[0] = CPT_INVALID_INDEX;
 }
 
 // ---------------------------------------------------------------------------
 // Triangle permutation fused with the bottom-up refit. Thread i gathers sorted
-// triangle i (writing the 40-B reference record and the 48-B traversal record),
-// computes its leaf box, then walks up: at each parent it stores its child box
-// into the parent's traversal record, and the second child to arrive (atomic
-// counter) reads its sibling's box from there and forms left.unite(right).
-// Release/acquire fences order the box stores before the counter (the
-// reference's refit has no fence, BVHBuilder.cu:63-86).
+// triangle i (the 40-B reference record), computes its leaf box, then walks up.
+// At each parent it writes its child slot of the parent's 96-B traversal node
+// (the triangle for a leaf, the box for an internal node); the second child to
+// arrive (atomic counter) reads its sibling's box the way the reference does —
+// recomputed from the sibling triangle's vertices for a leaf (BVHBuilder.cu:73-80),
+// from the internal-node box array otherwise — and stores left.unite(right).
+// Release/acquire fences order those stores before the counter (the reference's
+// refit has no fence, BVHBuilder.cu:63-86).
 // ---------------------------------------------------------------------------
 struct Box { float mn[3], mx[3]; };
 
-__device__ __forceinline__ void store_slot(float* node, int side, const Box& b)
+// 40-B slot at float offset 10*side of a 96-B node; 8-B aligned float2 stores.
+__device__ __forceinline__ void store_slot(float* node, int side, const float s[10])
 {
-    if (side == 0) {
-        *reinterpret_cast<float4*>(node) = make_float4(b.mn[0], b.mn[1], b.mn[2], b.mx[0]);
-        *reinterpret_cast<float2*>(node + 4) = make_float2(b.mx[1], b.mx[2]);
-    } else {
-        *reinterpret_cast<float2*>(node + 6) = make_float2(b.mn[0], b.mn[1]);
-        *reinterpret_cast<float4*>(node + 8) = make_float4(b.mn[2], b.mx[0], b.mx[1], b.mx[2]);
-    }
+    float2* p = reinterpret_cast<float2*>(node + 10 * side);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) p[k] = make_float2(s[2 * k], s[2 * k + 1]);
 }
 
-__device__ __forceinline__ Box load_slot(const float* node, int side)
+__device__ __forceinline__ Box leaf_box(const float v[9])
 {
     Box b;
-    if (side == 0) {
-        float4 a = __ldcg(reinterpret_cast<const float4*>(node));
-        float2 c = __ldcg(reinterpret_cast<const float2*>(node + 4));
-        b.mn[0] = a.x; b.mn[1] = a.y; b.mn[2] = a.z; b.mx[0] = a.w; b.mx[1] = c.x; b.mx[2] = c.y;
-    } else {
-        float2 a = __ldcg(reinterpret_cast<const float2*>(node + 6));
-        float4 c = __ldcg(reinterpret_cast<const float4*>(node + 8));
-        b.mn[0] = a.x; b.mn[1] = a.y; b.mn[2] = c.x; b.mx[0] = c.y; b.mx[1] = c.z; b.mx[2] = c.w;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        float mn = FLT_MAX, mx = -FLT_MAX;
+#pragma unroll
+        for (int vv = 0; vv < 3; ++vv) { mn = gmin(mn, v[3 * vv + ax]); mx = gmax(mx, v[3 * vv + ax]); }
+        b.mn[ax] = mn;
+        b.mx[ax] = mx;
     }
     return b;
 }
 
 __global__ void __launch_bounds__(256) k_gather_refit(const float* __restrict__ tris_in, const uint32_t* __restrict__ order,
                                                       uint32_t n, float* __restrict__ tris_out,
-                                                      float4* __restrict__ trirec, const uint32_t* __restrict__ children,
+                                                      const uint32_t* __restrict__ children,
                                                       const uint32_t* __restrict__ parents_leaf,
                                                       const uint32_t* __restrict__ parents_internal,
                                                       int* __restrict__ counters, float* __restrict__ nodes,
-                                                      cpt_bbox* __restrict__ node_boxes)
+                                                      cpt_bbox* __restrict__ node_boxes, uint32_t* __restrict__ status)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t src = order[i];
+    uint32_t src = order[i];
+    if (src >= n) {  // only after a failed sort pass (its status is already set): stay in bounds
+        atomicOr(status, CPT_STATUS_BAD_INDEX);
+        src = n - 1;
+    }
     const float2* s2 = reinterpret_cast<const float2*>(tris_in + 10ull * src);
-    float2 a = __ldg(s2), b = __ldg(s2 + 1), c = __ldg(s2 + 2), d = __ldg(s2 + 3), e = __ldg(s2 + 4);
+    const float2 a = __ldg(s2), b = __ldg(s2 + 1), c = __ldg(s2 + 2), d = __ldg(s2 + 3), e = __ldg(s2 + 4);
     float2* o2 = reinterpret_cast<float2*>(tris_out + 10ull * i);
     o2[0] = a; o2[1] = b; o2[2] = c; o2[3] = d; o2[4] = e;
     const float v[9] = {a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x};
-    const float info = e.y;
-    trirec[3 * (size_t)i + 0] = make_float4(v[0], v[1], v[2], info);
-    trirec[3 * (size_t)i + 1] = make_float4(__fsub_rn(v[3], v[0]), __fsub_rn(v[4], v[1]), __fsub_rn(v[5], v[2]), 0.0f);
-    trirec[3 * (size_t)i + 2] = make_float4(__fsub_rn(v[6], v[0]), __fsub_rn(v[7], v[1]), __fsub_rn(v[8], v[2]), 0.0f);
-
-    // Leaf box: empty box united with v0, v1, v2 in order (BVHBuilder.cu:73-74, BBox.cpp:26-30).
-    Box box;
-#pragma unroll
-    for (int ax = 0; ax < 3; ++ax) {
-        float mn = FLT_MAX, mx = -FLT_MAX;
-#pragma unroll
-        for (int vv = 0; vv < 3; ++vv) { mn = gmin(mn, v[3 * vv + ax]); mx = gmax(mx, v[3 * vv + ax]); }
-        box.mn[ax] = mn;
-        box.mx[ax] = mx;
-    }
+    // leaf slot: v0, info, v1 - v0, v2 - v0
+    float slot[10] = {v[0], v[1], v[2], e.y,
+                      __fsub_rn(v[3], v[0]), __fsub_rn(v[4], v[1]), __fsub_rn(v[5], v[2]),
+                      __fsub_rn(v[6], v[0]), __fsub_rn(v[7], v[1]), __fsub_rn(v[8], v[2])};
+    Box box = leaf_box(v);  // BVHBuilder.cu:73-74, BBox.cpp:26-30
     uint32_t child = i;
     uint32_t p = parents_leaf[i];
     while (p != CPT_INVALID_INDEX) {
+        if (p >= n - 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
         const uint32_t word = children[p];
-        const int side = (word >> 2) == child ? 0 : 1;
-        float* node = nodes + 16 * (size_t)p;
-        store_slot(node, side, box);
+        const uint32_t left = word >> 2;
+        const int side = left == child ? 0 : 1;
+        float* node = nodes + 24 * (size_t)p;
+        store_slot(node, side, slot);
         __threadfence();
-        if (atomicAdd(&counters[p], 1) == 0) return;
+        const int arrived = atomicAdd(&counters[p], 1);
+        if (arrived == 0) return;
+        if (arrived != 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }  // a third visit: not a tree
         __threadfence();
-        Box sib = load_slot(node, 1 - side);
-        const Box& L = side == 0 ? box : sib;
-        const Box& R = side == 0 ? sib : box;
+        const uint32_t sib = left + (uint32_t)(1 - side);
+        const bool sib_internal = (word >> (1 - side)) & 1u;
+        Box sb;
+        if (sib_internal) {
+            const float2* q = reinterpret_cast<const float2*>(node_boxes + sib);
+            const float2 x0 = __ldcg(q), x1 = __ldcg(q + 1), x2 = __ldcg(q + 2);
+            sb.mn[0] = x0.x; sb.mn[1] = x0.y; sb.mn[2] = x1.x; sb.mx[0] = x1.y; sb.mx[1] = x2.x; sb.mx[2] = x2.y;
+        } else {
+            const float2* q = reinterpret_cast<const float2*>(tris_out + 10ull * sib);
+            const float2 x0 = __ldcg(q), x1 = __ldcg(q + 1), x2 = __ldcg(q + 2), x3 = __ldcg(q + 3), x4 = __ldcg(q + 4);
+            const float sv[9] = {x0.x, x0.y, x1.x, x1.y, x2.x, x2.y, x3.x, x3.y, x4.x};
+            sb = leaf_box(sv);
+        }
         Box u;
 #pragma unroll
-        for (int ax = 0; ax < 3; ++ax) { u.mn[ax] = gmin(L.mn[ax], R.mn[ax]); u.mx[ax] = gmax(L.mx[ax], R.mx[ax]); }
+        for (int ax = 0; ax < 3; ++ax) {
+            const float lmn = side == 0 ? box.mn[ax] : sb.mn[ax], rmn = side == 0 ? sb.mn[ax] : box.mn[ax];
+            const float lmx = side == 0 ? box.mx[ax] : sb.mx[ax], rmx = side == 0 ? sb.mx[ax] : box.mx[ax];
+            u.mn[ax] = gmin(lmn, rmn);
+            u.mx[ax] = gmax(lmx, rmx);
+        }
         box = u;
-        cpt_bbox out;
-        for (int ax = 0; ax < 3; ++ax) { out.min[ax] = box.mn[ax]; out.max[ax] = box.mx[ax]; }
-        node_boxes[p] = out;
+        float2* ob = reinterpret_cast<float2*>(node_boxes + p);
+        ob[0] = make_float2(box.mn[0], box.mn[1]);
+        ob[1] = make_float2(box.mn[2], box.mx[0]);
+        ob[2] = make_float2(box.mx[1], box.mx[2]);
+        // internal slot for the next level: the box, padded
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { slot[k] = box.mn[k]; slot[3 + k] = box.mx[k]; }
+        slot[6] = slot[7] = slot[8] = slot[9] = 0.0f;
         child = p;
         p = parents_internal[p];
     }
@@ -615,9 +632,9 @@ int build_impl(const cpt_triangle* tris_in, uint32_t n, const float* host_box, c
     {
         CPT_PROF(K_GATHER_REFIT, stream);
         k_gather_refit<<<(n + 255) / 256, 256, 0, stream>>>(tri_src, order, n, reinterpret_cast<float*>(bvh->tris),
-                                                             static_cast<float4*>(bvh->tri_records), bvh->children,
-                                                             bvh->parents_leaf, bvh->parents_internal, s.counters,
-                                                             static_cast<float*>(bvh->nodes), bvh->node_boxes);
+                                                             bvh->children, bvh->parents_leaf, bvh->parents_internal,
+                                                             s.counters, static_cast<float*>(bvh->nodes),
+                                                             bvh->node_boxes, bvh->status);
     }
     CPT_LAUNCH_CHECK();
     return CPT_OK;
@@ -639,8 +656,7 @@ extern "C" size_t cpt_bvh_bytes(uint32_t n, int morton_bits)
     c.take<uint32_t>(n);
     c.take<uint32_t>(n - 1);
     c.take<cpt_bbox>(n - 1);
-    c.take<float4>(4ull * (n - 1));
-    c.take<float4>(3ull * n);
+    c.take<float4>(6ull * (n - 1));
     c.take<uint32_t>(4);
     return c.used();
 }
@@ -659,8 +675,7 @@ extern "C" int cpt_bvh_bind(void* mem, size_t bytes, uint32_t n, int morton_bits
     out->parents_leaf = c.take<uint32_t>(n);
     out->parents_internal = c.take<uint32_t>(n - 1);
     out->node_boxes = c.take<cpt_bbox>(n - 1);
-    out->nodes = c.take<float4>(4ull * (n - 1));
-    out->tri_records = c.take<float4>(3ull * n);
+    out->nodes = c.take<float4>(6ull * (n - 1));
     out->status = c.take<uint32_t>(4);
     return CPT_OK;
 }
@@ -682,6 +697,7 @@ extern "C" int cpt_status_check(const uint32_t* d_status, cudaStream_t stream)
     if (h[0] & CPT_STATUS_NONFINITE) return CPT_ERR_NONFINITE_INPUT;
     if (h[0] & CPT_STATUS_TIMEOUT) return CPT_ERR_DEVICE_TIMEOUT;
     if (h[0] & CPT_STATUS_STACK_OVERFLOW) return CPT_ERR_STACK_OVERFLOW;
+    if (h[0] & CPT_STATUS_BAD_INDEX) return CPT_ERR_BAD_INDEX;
     return CPT_OK;
 }
 
@@ -691,12 +707,10 @@ extern "C" int cpt_lbvh_build(const cpt_triangle* tris_in, uint32_t n, const flo
     if (!tris_in || !bvh || !scratch || n < 2 || n > kMaxTriangles) return CPT_ERR_INVALID_ARGUMENT;
     if (morton_bits != 30 && morton_bits != 63) return CPT_ERR_INVALID_ARGUMENT;
     if (bvh->n != n || bvh->morton_bits != morton_bits || !bvh->tris || !bvh->keys || !bvh->children ||
-        !bvh->parents_leaf || !bvh->parents_internal || !bvh->node_boxes || !bvh->nodes || !bvh->tri_records ||
-        !bvh->status)
+        !bvh->parents_leaf || !bvh->parents_internal || !bvh->node_boxes || !bvh->nodes || !bvh->status)
         return CPT_ERR_INVALID_ARGUMENT;
     if ((reinterpret_cast<uintptr_t>(tris_in) & 15) || (reinterpret_cast<uintptr_t>(scratch) & 255) ||
-        (reinterpret_cast<uintptr_t>(bvh->nodes) & 15) || (reinterpret_cast<uintptr_t>(bvh->tri_records) & 15) ||
-        (reinterpret_cast<uintptr_t>(bvh->tris) & 15))
+        (reinterpret_cast<uintptr_t>(bvh->nodes) & 15) || (reinterpret_cast<uintptr_t>(bvh->tris) & 15))
         return CPT_ERR_INVALID_ARGUMENT;
     if (scratch_bytes < cpt_lbvh_scratch_bytes(n, morton_bits)) return CPT_ERR_SCRATCH_TOO_SMALL;
     int rc = morton_bits == 30 ? build_impl<uint32_t>(tris_in, n, enclosing_box, bvh, scratch, stream)

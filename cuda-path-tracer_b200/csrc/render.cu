@@ -26,6 +26,7 @@
 namespace cpt {
 
 constexpr int kExtendBlock = 128;
+constexpr int kExtendSteps = 8;
 constexpr int kShadeBlock = 128;
 constexpr int kGenBlock = 256;
 constexpr int kMaxDepth = 62;  // bounces + 1 queues; reference GUI allows 5 bounces (PathTracingSettings.h:27)
@@ -129,23 +130,19 @@ __global__ void __launch_bounds__(kGenBlock) k_generate(Wave wv, Camera cam, flo
 }
 
 template <bool kStats>
-__global__ void __launch_bounds__(kExtendBlock) k_extend(const float4* __restrict__ nodes, const float4* __restrict__ tris,
+__global__ void __launch_bounds__(kExtendBlock) k_extend(const float4* __restrict__ nodes,
                                                          const float4* __restrict__ queue,
                                                          const uint32_t* __restrict__ count, float4* __restrict__ hits,
+                                                         uint32_t* __restrict__ pool,
                                                          unsigned long long* __restrict__ ray_counts,
-                                                         uint32_t* __restrict__ status)
+                                                         uint32_t* __restrict__ status, uint32_t max_visits)
 {
-    __shared__ uint32_t s_stack[CPT_TRAVERSAL_STACK * kExtendBlock];
-    uint32_t* stack = s_stack + threadIdx.x;
+    __shared__ uint32_t s_stack[kSmemStack * kExtendBlock];
     const uint32_t n = *count;
     bool overflow = false;
     uint32_t nn = 0, nt = 0;
-    for (uint32_t i = blockIdx.x * kExtendBlock + threadIdx.x; i < n; i += gridDim.x * kExtendBlock) {
-        const float4 ro = queue[2 * (size_t)i], rd = queue[2 * (size_t)i + 1];
-        Hit h = traverse<false, kExtendBlock, kStats>(nodes, tris, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z), stack,
-                                                      overflow, nn, nt);
-        hits[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
-    }
+    persistent_trace<false, kExtendBlock, kStats, kExtendSteps>(nodes, queue, n, hits, pool, s_stack + threadIdx.x,
+                                                                overflow, nn, nt, max_visits, nullptr);
     if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
     if (kStats && ray_counts) {
         warp_count_u64(ray_counts + 3, nn);
@@ -155,9 +152,11 @@ __global__ void __launch_bounds__(kExtendBlock) k_extend(const float4* __restric
 
 struct ShadeScene {
     const float4* nodes;
-    const float4* tris;
+    const cpt_triangle* tris;  // Morton-sorted reference records (info_idx of a hit)
     const cpt_triangle_info* infos;
     const cpt_dir_light* lights;
+    uint32_t info_count;
+    uint32_t max_visits;
 };
 
 // blinnPhongBRDF (cuda_path_tracer.cu:36-50)
@@ -179,8 +178,7 @@ __device__ __forceinline__ f3 light_l(const ShadeScene& sc, f3 p, const cpt_dir_
 {
     f3 dir = mk3(l.direction[0], l.direction[1], l.direction[2]);
     f3 o = sub(p, muls(dir, 1e-3f));
-    uint32_t nn = 0, nt = 0;
-    Hit h = traverse<true, kBlock, false>(sc.nodes, sc.tris, o, neg(dir), stack, overflow, nn, nt);
+    Hit h = traverse<true, kBlock>(sc.nodes, o, neg(dir), stack, overflow, sc.max_visits);
     if (h.t < FLT_MAX) return mk3(0.f, 0.f, 0.f);
     return muls(mk3(l.color[0], l.color[1], l.color[2]), l.intensity);
 }
@@ -204,7 +202,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(ShadeScene sc, Wave wv, u
                                                        unsigned long long* __restrict__ ray_counts,
                                                        uint32_t* __restrict__ status)
 {
-    __shared__ uint32_t s_stack[kLights ? CPT_TRAVERSAL_STACK * kShadeBlock : 1];
+    __shared__ uint32_t s_stack[kLights ? kSmemStack * kShadeBlock : 1];
     uint32_t* stack = s_stack + (kLights ? threadIdx.x : 0);
     const uint32_t n = *count_in;
     bool overflow = false;
@@ -213,15 +211,17 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(ShadeScene sc, Wave wv, u
         bool emit = false;
         float4 nro = make_float4(0.f, 0.f, 0.f, 0.f), nrd = nro;
         uint32_t shadow = 0;
+        bool bad_info = false;
         if (i < n) {
             const float4 ro = queue_in[2 * (size_t)i], rd4 = queue_in[2 * (size_t)i + 1];
             const float4 hit4 = hits[i];
             const uint32_t tri = __float_as_uint(hit4.w);
             const uint32_t pid = __float_as_uint(ro.w);
-            if (tri != CPT_INVALID_INDEX) {
+            const uint32_t info_idx = tri != CPT_INVALID_INDEX ? __ldg(&sc.tris[tri].info_idx) : 0u;
+            bad_info = tri != CPT_INVALID_INDEX && info_idx >= sc.info_count;
+            if (tri != CPT_INVALID_INDEX && !bad_info) {
                 const f3 o = mk3(ro.x, ro.y, ro.z), d = mk3(rd4.x, rd4.y, rd4.z);
                 const float t = hit4.x, u = hit4.y, v = hit4.z;
-                const uint32_t info_idx = __float_as_uint(__ldg(reinterpret_cast<const float*>(sc.tris + 3 * (size_t)tri) + 3));
                 const cpt_triangle_info& in = sc.infos[info_idx];
                 const f3 hp = add(muls(d, t), o);
                 f3 albedo = normalize(bary(ld3(in.vertices[0].color), ld3(in.vertices[1].color), ld3(in.vertices[2].color), u, v));
@@ -303,6 +303,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(ShadeScene sc, Wave wv, u
             queue_out[2 * (size_t)q + 1] = nrd;
         }
         if (kLights) warp_count_u64(ray_counts ? ray_counts + 2 : nullptr, shadow);
+        if (bad_info) atomicOr(status, CPT_STATUS_BAD_INDEX);
     }
     if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
 }
@@ -413,7 +414,7 @@ size_t render_layout(const cpt_render_params* p, void* base, RenderScratch* out)
     s.queue[1] = c.take<float4>(2ull * s.capacity);
     s.hits = c.take<float4>(s.capacity);
     s.state = c.take<float4>(2ull * s.capacity);
-    s.counts = c.take<uint32_t>(kMaxDepth + 2);
+    s.counts = c.take<uint32_t>(2 * (kMaxDepth + 2));  // queue counts, then persistent-kernel ray pools
     if (out) *out = s;
     return c.used();
 }
@@ -451,7 +452,7 @@ extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_
                           unsigned long long* ray_counts, uint32_t* status, cudaStream_t stream)
 {
     if (!bvh || !scene || !camera || !accum || !scratch || !params_ok(params)) return CPT_ERR_INVALID_ARGUMENT;
-    if (!bvh->nodes || !bvh->tri_records || !scene->infos || (scene->light_count && !scene->lights))
+    if (!bvh->nodes || !bvh->tris || !scene->infos || (scene->light_count && !scene->lights))
         return CPT_ERR_INVALID_ARGUMENT;
     if (scratch_bytes < render_layout(params, nullptr, nullptr)) return CPT_ERR_SCRATCH_TOO_SMALL;
     if ((reinterpret_cast<uintptr_t>(accum) & 15) || (reinterpret_cast<uintptr_t>(scratch) & 255))
@@ -485,9 +486,11 @@ extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_
 
     ShadeScene sc;
     sc.nodes = static_cast<const float4*>(bvh->nodes);
-    sc.tris = static_cast<const float4*>(bvh->tri_records);
+    sc.tris = bvh->tris;
     sc.infos = scene->infos;
     sc.lights = scene->lights;
+    sc.info_count = scene->info_count;
+    sc.max_visits = bvh->n;
 
     const int sms = sm_count();
     const uint32_t spw_max = wave_samples(params);
@@ -495,26 +498,33 @@ extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_
         wv.s0 = s0;
         wv.spw = std::min(spw_max, params->spp - s0);
         const uint32_t paths = wv.spw * wv.pixels;
-        CPT_CUDA_TRY(cudaMemsetAsync(rs.counts, 0, sizeof(uint32_t) * (kMaxDepth + 2), stream));
+        CPT_CUDA_TRY(cudaMemsetAsync(rs.counts, 0, sizeof(uint32_t) * 2 * (kMaxDepth + 2), stream));
         {
             CPT_PROF(K_GENERATE, stream);
             k_generate<<<(int)std::min<uint32_t>((paths + kGenBlock - 1) / kGenBlock, (uint32_t)sms * 16), kGenBlock, 0,
                          stream>>>(wv, cam, rs.queue[0], rs.counts, rs.state);
         }
         CPT_LAUNCH_CHECK();
-        const int ext_blocks = std::min<int>((int)((paths + kExtendBlock - 1) / kExtendBlock), sms * 12);
+        static int ext_occ = 0;
+        if (!ext_occ) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ext_occ, k_extend<false>, kExtendBlock, 0) != cudaSuccess ||
+                ext_occ < 1)
+                ext_occ = 1;
+        }
+        const int ext_blocks = std::min<int>((int)((paths + kExtendBlock - 1) / kExtendBlock), sms * ext_occ);
         const int shade_blocks = std::min<int>((int)((paths + kShadeBlock - 1) / kShadeBlock), sms * 16);
         for (uint32_t b = 0; b <= params->bounces; ++b) {
             const float4* qin = rs.queue[b & 1];
             float4* qout = rs.queue[(b + 1) & 1];
             {
                 CPT_PROF(K_EXTEND, stream);
+                uint32_t* pool = rs.counts + kMaxDepth + 2 + b;
                 if (params->trace_stats)
-                    k_extend<true><<<ext_blocks, kExtendBlock, 0, stream>>>(sc.nodes, sc.tris, qin, rs.counts + b, rs.hits,
-                                                                            ray_counts, st);
+                    k_extend<true><<<ext_blocks, kExtendBlock, 0, stream>>>(sc.nodes, qin, rs.counts + b, rs.hits, pool,
+                                                                            ray_counts, st, sc.max_visits);
                 else
-                    k_extend<false><<<ext_blocks, kExtendBlock, 0, stream>>>(sc.nodes, sc.tris, qin, rs.counts + b,
-                                                                             rs.hits, ray_counts, st);
+                    k_extend<false><<<ext_blocks, kExtendBlock, 0, stream>>>(sc.nodes, qin, rs.counts + b, rs.hits, pool,
+                                                                             ray_counts, st, sc.max_visits);
             }
             CPT_LAUNCH_CHECK();
             {

@@ -1,5 +1,5 @@
-// Ray queries against a built LBVH (cpt_trace): one thread per ray over a
-// persistent grid, shared-memory node stack, 16-B vectorised record loads.
+// Ray queries against a built LBVH (cpt_trace): persistent warps over the ray
+// array with per-lane refill, 96-B node loads, shared-memory node stack.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include "cpt.h"
@@ -9,25 +9,37 @@
 namespace cpt {
 
 constexpr int kTraceBlock = 128;
+constexpr int kTraceSteps = 8;
 
 template <bool kAny, bool kStats>
-__global__ void __launch_bounds__(kTraceBlock) k_trace(const float4* __restrict__ nodes, const float4* __restrict__ tris,
-                                                       const float4* __restrict__ rays, uint32_t n,
-                                                       float4* __restrict__ hits, uint2* __restrict__ stats,
-                                                       uint32_t* __restrict__ status)
+__global__ void __launch_bounds__(kTraceBlock) k_trace(const float4* __restrict__ nodes, const float4* __restrict__ rays,
+                                                       uint32_t n, float4* __restrict__ hits, uint2* __restrict__ stats,
+                                                       uint32_t* __restrict__ pool, uint32_t* __restrict__ status,
+                                                       uint32_t max_visits)
 {
-    __shared__ uint32_t s_stack[CPT_TRAVERSAL_STACK * kTraceBlock];
-    uint32_t* stack = s_stack + threadIdx.x;
+    __shared__ uint32_t s_stack[kSmemStack * kTraceBlock];
     bool overflow = false;
-    for (uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x; i < n; i += gridDim.x * kTraceBlock) {
-        const float4 ro = __ldg(rays + 2 * (size_t)i), rd = __ldg(rays + 2 * (size_t)i + 1);
-        uint32_t nn = 0, nt = 0;
-        Hit h = traverse<kAny, kTraceBlock, kStats>(nodes, tris, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z), stack,
-                                                    overflow, nn, nt);
-        hits[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
-        if (kStats) stats[i] = make_uint2(nn, nt);
-    }
+    uint32_t nn = 0, nt = 0;
+    persistent_trace<kAny, kTraceBlock, kStats, kTraceSteps>(nodes, rays, n, hits, pool, s_stack + threadIdx.x, overflow,
+                                                             nn, nt, max_visits, stats);
     if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
+}
+
+template <bool kAny, bool kStats>
+int launch_trace(const float4* nd, const float4* r4, uint32_t n, float4* h4, uint2* st, uint32_t* pool,
+                 uint32_t* status, uint32_t mv, cudaStream_t stream)
+{
+    static int per_sm[2][2] = {{0, 0}, {0, 0}};
+    int& occ = per_sm[kAny][kStats];
+    if (!occ) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trace<kAny, kStats>, kTraceBlock, 0) != cudaSuccess ||
+            occ < 1)
+            occ = 1;
+    }
+    const int blocks = (int)std::min<size_t>((n + kTraceBlock - 1) / kTraceBlock, (size_t)sm_count() * occ);
+    k_trace<kAny, kStats><<<blocks, kTraceBlock, 0, stream>>>(nd, r4, n, h4, st, pool, status, mv);
+    CPT_LAUNCH_CHECK();
+    return CPT_OK;
 }
 
 }  // namespace cpt
@@ -37,25 +49,20 @@ using namespace cpt;
 extern "C" int cpt_trace(const cpt_bvh* bvh, const float* rays, uint32_t n, int any_hit, cpt_hit* hits,
                          uint32_t* stats, cudaStream_t stream)
 {
-    if (!bvh || !bvh->nodes || !bvh->tri_records || !bvh->status || (n && (!rays || !hits)))
-        return CPT_ERR_INVALID_ARGUMENT;
+    if (!bvh || !bvh->nodes || !bvh->status || (n && (!rays || !hits))) return CPT_ERR_INVALID_ARGUMENT;
     if ((reinterpret_cast<uintptr_t>(rays) & 15) || (reinterpret_cast<uintptr_t>(hits) & 15))
         return CPT_ERR_INVALID_ARGUMENT;
     if (n == 0) return CPT_OK;
-    const int blocks = (int)std::min<size_t>((n + kTraceBlock - 1) / kTraceBlock, (size_t)sm_count() * 16);
     const float4* nd = static_cast<const float4*>(bvh->nodes);
-    const float4* tr = static_cast<const float4*>(bvh->tri_records);
     const float4* r4 = reinterpret_cast<const float4*>(rays);
     float4* h4 = reinterpret_cast<float4*>(hits);
     uint2* st = reinterpret_cast<uint2*>(stats);
+    uint32_t* pool = bvh->status + 1;  // ray pool counter of the persistent kernel
+    CPT_CUDA_TRY(cudaMemsetAsync(pool, 0, sizeof(uint32_t), stream));
+    const uint32_t mv = bvh->n;  // a ray fetches each of the n - 1 internal nodes at most once
     CPT_PROF(K_TRACE, stream);
-    if (any_hit) {
-        if (stats) k_trace<true, true><<<blocks, kTraceBlock, 0, stream>>>(nd, tr, r4, n, h4, st, bvh->status);
-        else k_trace<true, false><<<blocks, kTraceBlock, 0, stream>>>(nd, tr, r4, n, h4, st, bvh->status);
-    } else {
-        if (stats) k_trace<false, true><<<blocks, kTraceBlock, 0, stream>>>(nd, tr, r4, n, h4, st, bvh->status);
-        else k_trace<false, false><<<blocks, kTraceBlock, 0, stream>>>(nd, tr, r4, n, h4, st, bvh->status);
-    }
-    CPT_LAUNCH_CHECK();
-    return CPT_OK;
+    if (any_hit) return stats ? launch_trace<true, true>(nd, r4, n, h4, st, pool, bvh->status, mv, stream)
+                              : launch_trace<true, false>(nd, r4, n, h4, st, pool, bvh->status, mv, stream);
+    return stats ? launch_trace<false, true>(nd, r4, n, h4, st, pool, bvh->status, mv, stream)
+                 : launch_trace<false, false>(nd, r4, n, h4, st, pool, bvh->status, mv, stream);
 }

@@ -8,23 +8,32 @@
 // Möller-Trumbore (intersection.h:28-59) and slab (intersection.h:106-117)
 // arithmetic in round-to-nearest intrinsics.
 //
-// What changes is the memory side:
-//  * one 64-B record per internal node holds both children's boxes and the Node
-//    word (4 x 16-B loads), instead of a 4-B Node load followed by a 24-B box
-//    load per internal child from a separate array;
-//  * one 48-B record per triangle (v0 | info, v1 - v0, v2 - v0; 3 x 16-B loads)
-//    instead of an unaligned 40-B record — the stored edges are the same
-//    subtractions the test performs, so the bits are unchanged;
-//  * 1/d is computed once per ray instead of per box (same value);
-//  * the node stack lives in shared memory, one column per thread
-//    (stack[depth * kBlock + thread]), CPT_TRAVERSAL_STACK deep like the
-//    reference's 64-entry local array; a push beyond it is dropped and reported
-//    (CPT_STATUS_STACK_OVERFLOW) instead of overrunning the array.
+// What changes is the memory side and the scheduling:
+//  * one 96-B record per internal node (six 16-B loads, three 32-B sectors) holds
+//    both children and the Node word. A child slot (10 words) is either the
+//    child's box (internal child) or the child triangle itself — v0, the info
+//    index, v1 - v0, v2 - v0 (leaf child): the reference loads a 4-B Node, then a
+//    24-B box or a 40-B triangle per child from separate arrays; here one round
+//    trip fetches everything a visit needs. The stored edges are the same
+//    subtractions the test performs, so the bits are unchanged.
+//  * 1/d is computed once per ray instead of per box (same value).
+//  * the node stack is CPT_TRAVERSAL_STACK deep like the reference's local array:
+//    the first kSmemStack entries live in shared memory, one column per thread,
+//    the rest (never reached on the test scenes) in local memory; a push beyond
+//    the capacity is dropped and reported (CPT_STATUS_STACK_OVERFLOW) instead of
+//    overrunning the array.
+//  * traversal kernels are persistent: each lane takes rays from a global pool and
+//    takes the next one as soon as its ray finishes, so a warp is not held by its
+//    slowest ray (per-ray node counts differ by 100x on hairball scenes).
 #pragma once
 #include "cpt_device.cuh"
 #include "cpt.h"
 
 namespace cpt {
+
+constexpr int kSmemStack = 32;
+constexpr int kNodeFloat4 = 6;  // 96-B node record
+constexpr int kNodeFloats = 24;
 
 struct Hit { float t, u, v; uint32_t tri; };
 
@@ -38,82 +47,198 @@ __device__ __forceinline__ float slab_test(f3 o, f3 dinv, float ax, float ay, fl
     return (n <= f && f > 0.0f) ? n : FLT_MAX;
 }
 
-__device__ __forceinline__ float tri_test(f3 o, f3 d, const float4* __restrict__ rec, float& u, float& v)
+// s: the 10-word slot, v0 = s[0..2], e1 = s[4..6], e2 = s[7..9].
+__device__ __forceinline__ float tri_test(f3 o, f3 d, const float* s, float& u, float& v)
 {
-    float4 a = __ldg(rec), b = __ldg(rec + 1), c = __ldg(rec + 2);
-    f3 p0 = mk3(a.x, a.y, a.z), e1 = mk3(b.x, b.y, b.z), e2 = mk3(c.x, c.y, c.z);
-    f3 q = cross(d, e2);
-    float det = dot(e1, q);
+    const f3 p0 = mk3(s[0], s[1], s[2]), e1 = mk3(s[4], s[5], s[6]), e2 = mk3(s[7], s[8], s[9]);
+    const f3 q = cross(d, e2);
+    const float det = dot(e1, q);
     if (det > -FLT_EPSILON && det < FLT_EPSILON) return FLT_MAX;
-    float inv = __frcp_rn(det);
-    f3 s = sub(o, p0);
-    u = __fmul_rn(inv, dot(s, q));
+    const float inv = __frcp_rn(det);
+    const f3 sv = sub(o, p0);
+    u = __fmul_rn(inv, dot(sv, q));
     if (u < 0.f) return FLT_MAX;
-    f3 r = cross(s, e1);
+    const f3 r = cross(sv, e1);
     v = __fmul_rn(inv, dot(d, r));
     if (v < 0.f || __fadd_rn(u, v) > 1.f) return FLT_MAX;
-    float t = __fmul_rn(inv, dot(e2, r));
+    const float t = __fmul_rn(inv, dot(e2, r));
     return t >= 0.0f ? t : FLT_MAX;
 }
 
-// stack: this thread's column base in shared memory (s_stack + threadIdx.x).
-template <bool kAny, int kBlock, bool kStats>
-__device__ __forceinline__ Hit traverse(const float4* __restrict__ nodes, const float4* __restrict__ tris, f3 o, f3 d,
-                                        uint32_t* stack, bool& overflow, uint32_t& n_nodes, uint32_t& n_tris)
+__device__ __forceinline__ float child_test(f3 o, f3 d, f3 dinv, bool internal, const float* s, float& u, float& v)
 {
-    const f3 dinv = mk3(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
+    if (internal) return slab_test(o, dinv, s[0], s[1], s[2], s[3], s[4], s[5]);
+    return tri_test(o, d, s, u, v);
+}
+
+// Per-ray traversal state.
+struct TraceState {
+    f3 o, d, dinv;
     Hit best;
-    best.t = FLT_MAX;
-    best.u = 0.f;
-    best.v = 0.f;
-    best.tri = CPT_INVALID_INDEX;
-    int sp = 0;
-    uint32_t cur = 0;  // the root, Node::makeInternal(0)
+    uint32_t cur;
+    int sp;
+    uint32_t visits;  // node fetches
+    uint32_t tests;   // triangle tests
+};
+
+__device__ __forceinline__ void trace_init(TraceState& s, f3 o, f3 d)
+{
+    s.o = o;
+    s.d = d;
+    s.dinv = mk3(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
+    s.best.t = FLT_MAX;
+    s.best.u = 0.f;
+    s.best.v = 0.f;
+    s.best.tri = CPT_INVALID_INDEX;
+    s.cur = 0;  // the root, Node::makeInternal(0)
+    s.sp = 0;
+    s.visits = 0;
+    s.tests = 0;
+}
+
+template <int kBlock>
+__device__ __forceinline__ void stack_push(uint32_t* smem_col, uint32_t* spill, int& sp, uint32_t v, bool& overflow)
+{
+    if (sp < kSmemStack) smem_col[sp * kBlock] = v;
+    else if (sp < CPT_TRAVERSAL_STACK) spill[sp - kSmemStack] = v;
+    else { overflow = true; return; }
+    ++sp;
+}
+
+template <int kBlock>
+__device__ __forceinline__ uint32_t stack_pop(const uint32_t* smem_col, const uint32_t* spill, int& sp)
+{
+    --sp;
+    return sp < kSmemStack ? smem_col[sp * kBlock] : spill[sp - kSmemStack];
+}
+
+// One node visit of trace.h:104-165. Returns true when the ray is finished
+// (stack empty after a pop, or — any-hit — a triangle was recorded).
+template <bool kAny, int kBlock, bool kStats>
+__device__ __forceinline__ bool trace_step(TraceState& s, const float4* __restrict__ nodes, uint32_t* smem_col,
+                                           uint32_t* spill, bool& overflow, uint32_t& n_nodes, uint32_t& n_tris,
+                                           uint32_t max_visits)
+{
+    if (++s.visits > max_visits) { overflow = true; return true; }
+    const float4* nd = nodes + kNodeFloat4 * (size_t)s.cur;
+    float w[kNodeFloats];
+#pragma unroll
+    for (int k = 0; k < kNodeFloat4; ++k) {
+        const float4 f = __ldg(nd + k);
+        w[4 * k] = f.x; w[4 * k + 1] = f.y; w[4 * k + 2] = f.z; w[4 * k + 3] = f.w;
+    }
+    const uint32_t word = __float_as_uint(w[20]);
+    if (kStats) ++n_nodes;
+    const uint32_t li = word >> 2, ri = li + 1;
+    const bool lint = word & 1u, rint = word & 2u;
+    if (kStats) {
+        const uint32_t t = (lint ? 0u : 1u) + (rint ? 0u : 1u);
+        n_tris += t;
+        s.tests += t;
+    }
+    float lu = 0.f, lv = 0.f, ru = 0.f, rv = 0.f;
+    const float hl = child_test(s.o, s.d, s.dinv, lint, w, lu, lv);
+    const float hr = child_test(s.o, s.d, s.dinv, rint, w + 10, ru, rv);
+    bool pop = false;
+    if (hl >= s.best.t && hr >= s.best.t) {
+        pop = true;
+    } else {
+        const bool sw = hr < hl;
+        const float hc = sw ? hr : hl, hf = sw ? hl : hr;
+        const uint32_t ic = sw ? ri : li, ifar = sw ? li : ri;
+        const bool cint = sw ? rint : lint, fint = sw ? lint : rint;
+        if (cint) {
+            if (hf < s.best.t) {
+                if (fint) {
+                    stack_push<kBlock>(smem_col, spill, s.sp, ifar, overflow);
+                } else {
+                    s.best.t = hf;
+                    s.best.u = sw ? lu : ru;
+                    s.best.v = sw ? lv : rv;
+                    s.best.tri = ifar;
+                    if (kAny) return true;
+                }
+            }
+            s.cur = ic;
+        } else {
+            s.best.t = hc;
+            s.best.u = sw ? ru : lu;
+            s.best.v = sw ? rv : lv;
+            s.best.tri = ic;
+            if (kAny) return true;
+            pop = true;
+        }
+    }
+    if (pop) {
+        if (s.sp == 0) return true;
+        s.cur = stack_pop<kBlock>(smem_col, spill, s.sp);
+    }
+    return false;
+}
+
+// Whole traversal of one ray by one thread (shadow rays inside the shade kernel).
+template <bool kAny, int kBlock>
+__device__ __forceinline__ Hit traverse(const float4* __restrict__ nodes, f3 o, f3 d, uint32_t* smem_col, bool& overflow,
+                                        uint32_t max_visits)
+{
+    TraceState s;
+    trace_init(s, o, d);
+    uint32_t spill[CPT_TRAVERSAL_STACK - kSmemStack];
+    uint32_t nn = 0, nt = 0;
+    while (!trace_step<kAny, kBlock, false>(s, nodes, smem_col, spill, overflow, nn, nt, max_visits)) {
+    }
+    return s.best;
+}
+
+// Persistent traversal of `n` rays: ray i is (origin, direction) = rays[2i], rays[2i+1]
+// (.w of the first holds a payload), its hit goes to hits[i]. Lanes take rays from
+// *pool in warp-sized grabs and refill as soon as their ray finishes.
+// ray_stats (nullable, with kStats): per ray (node fetches, triangle tests).
+template <bool kAny, int kBlock, bool kStats, int kSteps>
+__device__ __forceinline__ void persistent_trace(const float4* __restrict__ nodes, const float4* __restrict__ rays,
+                                                 uint32_t n, float4* __restrict__ hits, uint32_t* __restrict__ pool,
+                                                 uint32_t* smem_col, bool& overflow, uint32_t& n_nodes,
+                                                 uint32_t& n_tris, uint32_t max_visits, uint2* __restrict__ ray_stats)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    uint32_t spill[CPT_TRAVERSAL_STACK - kSmemStack];
+    TraceState s;
+    uint32_t ray = CPT_INVALID_INDEX;
+    bool drained = false;
     for (;;) {
-        for (;;) {
-            const float4* nd = nodes + 4 * (size_t)cur;
-            const float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2);
-            const uint32_t word = __float_as_uint(__ldg(reinterpret_cast<const float*>(nd + 3)));
-            if (kStats) ++n_nodes;
-            const uint32_t li = word >> 2, ri = li + 1;
-            const bool lint = word & 1u, rint = word & 2u;
-            float lu = 0.f, lv = 0.f, ru = 0.f, rv = 0.f, hl, hr;
-            if (lint) hl = slab_test(o, dinv, n0.x, n0.y, n0.z, n0.w, n1.x, n1.y);
-            else { hl = tri_test(o, d, tris + 3 * (size_t)li, lu, lv); if (kStats) ++n_tris; }
-            if (rint) hr = slab_test(o, dinv, n1.z, n1.w, n2.x, n2.y, n2.z, n2.w);
-            else { hr = tri_test(o, d, tris + 3 * (size_t)ri, ru, rv); if (kStats) ++n_tris; }
-            if (hl >= best.t && hr >= best.t) break;
-            const bool sw = hr < hl;
-            const float hc = sw ? hr : hl, hf = sw ? hl : hr;
-            const uint32_t ic = sw ? ri : li, ifar = sw ? li : ri;
-            const bool cint = sw ? rint : lint, fint = sw ? lint : rint;
-            if (cint) {
-                if (hf < best.t) {
-                    if (fint) {
-                        if (sp < CPT_TRAVERSAL_STACK) stack[(sp++) * kBlock] = ifar;
-                        else overflow = true;
-                    } else {
-                        best.t = hf;
-                        best.u = sw ? lu : ru;
-                        best.v = sw ? lv : rv;
-                        best.tri = ifar;
-                        if (kAny) return best;
+        if (!drained) {
+            const bool idle = ray == CPT_INVALID_INDEX;
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, idle);
+            if (m) {
+                const int leader = __ffs(m) - 1;
+                uint32_t base = 0;
+                if ((int)lane == leader) base = atomicAdd(pool, (uint32_t)__popc(m));
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                if (base + (uint32_t)__popc(m) >= n) drained = true;
+                if (idle) {
+                    const uint32_t r = base + (uint32_t)__popc(m & lt_mask);
+                    if (r < n) {
+                        ray = r;
+                        const float4 ro = rays[2 * (size_t)r], rd = rays[2 * (size_t)r + 1];
+                        trace_init(s, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z));
                     }
                 }
-                cur = ic;
-            } else {
-                best.t = hc;
-                best.u = sw ? ru : lu;
-                best.v = sw ? rv : lv;
-                best.tri = ic;
-                if (kAny) return best;
-                break;
             }
         }
-        if (sp == 0) break;
-        cur = stack[(--sp) * kBlock];
+        if (__ballot_sync(0xFFFFFFFFu, ray != CPT_INVALID_INDEX) == 0) break;
+        if (ray != CPT_INVALID_INDEX) {
+#pragma unroll 1
+            for (int k = 0; k < kSteps; ++k) {
+                if (trace_step<kAny, kBlock, kStats>(s, nodes, smem_col, spill, overflow, n_nodes, n_tris, max_visits)) {
+                    hits[ray] = make_float4(s.best.t, s.best.u, s.best.v, __uint_as_float(s.best.tri));
+                    if (kStats && ray_stats) ray_stats[ray] = make_uint2(s.visits, s.tests);
+                    ray = CPT_INVALID_INDEX;
+                    break;
+                }
+            }
+        }
     }
-    return best;
 }
 
 }  // namespace cpt

@@ -34,11 +34,13 @@ extern "C" {
 #define CPT_ERR_STACK_OVERFLOW 6    /* a ray needed more than CPT_TRAVERSAL_STACK entries */
 #define CPT_ERR_CHECK_FAILED 7      /* root box volume differs from the enclosing box's */
 #define CPT_ERR_NO_DEVICE 8         /* no CUDA device / library built for another arch */
+#define CPT_ERR_BAD_INDEX 9         /* a device-side index was out of range (e.g. info_idx >= info_count) */
 
 /* device status-word bits (cpt_bvh.status[0], render status) */
 #define CPT_STATUS_NONFINITE 1u
 #define CPT_STATUS_TIMEOUT 2u
 #define CPT_STATUS_STACK_OVERFLOW 4u
+#define CPT_STATUS_BAD_INDEX 8u /* an index read from device data was out of range (corrupt input) */
 
 #define CPT_TRAVERSAL_STACK 64 /* MAX_TRAVERSAL_STACK_SIZE, source/engine/cuda/cuda_defs.h:21 */
 #define CPT_INVALID_INDEX 0xFFFFFFFFu
@@ -68,8 +70,9 @@ typedef struct cpt_bvh {
     uint32_t* parents_leaf;     /* [n]   parent of each leaf */
     uint32_t* parents_internal; /* [n-1] parent of each internal node; [0] = CPT_INVALID_INDEX */
     cpt_bbox* node_boxes;       /* [n-1] internal node boxes */
-    void* nodes;                /* [n-1] 64-B traversal nodes: left box, right box, Node word */
-    void* tri_records;          /* [n]   48-B traversal triangles: v0|info, v1-v0, v2-v0 */
+    void* nodes;                /* [n-1] 96-B traversal nodes: two 40-B child slots + Node word, where a
+                                 *       slot holds the child's box (internal child) or the child
+                                 *       triangle as v0, info_idx, v1 - v0, v2 - v0 (leaf child) */
     uint32_t* status;           /* [4]   device status words (CPT_STATUS_* bits in [0]) */
 } cpt_bvh;
 
