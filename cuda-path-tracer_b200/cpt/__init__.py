@@ -102,6 +102,7 @@ _PROTOS = {
     "cpt_bvh_bind": (_I32, [_P, _SZ, _U32, _I32, ctypes.POINTER(Bvh)]),
     "cpt_lbvh_scratch_bytes": (_SZ, [_U32, _I32]),
     "cpt_lbvh_build": (_I32, [_P, _U32, _P, _I32, ctypes.POINTER(Bvh), _P, _SZ, _U32, _P]),
+    "cpt_lbvh_build_static": (_I32, [_P, _U32, _P, _I32, ctypes.POINTER(Bvh), _U32, _P]),
     "cpt_status_check": (_I32, [_P, _P]),
     "cpt_trace": (_I32, [ctypes.POINTER(Bvh), _P, _U32, _I32, _P, _P, _P]),
     "cpt_accum_bytes": (_SZ, [_U32, _U32, _U32]),

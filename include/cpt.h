@@ -94,6 +94,30 @@ size_t cpt_lbvh_scratch_bytes(uint32_t n, int morton_bits);
 int cpt_lbvh_build(const cpt_triangle* tris_in, uint32_t n, const float* enclosing_box, int morton_bits,
                    cpt_bvh* bvh, void* scratch, size_t scratch_bytes, uint32_t flags, cudaStream_t stream);
 
+/* LBVH build that allocates nothing: the same build and outputs as
+ * cpt_lbvh_build, with its scratch in a fixed array inside the library's device
+ * image instead of a caller buffer. It has no counterpart in the reference, whose
+ * builder resizes thrust vectors and cudaMallocs on every build
+ * (BVHBuilder.cu:220-242). It is for callers that cannot allocate device memory
+ * when they build: a plugin whose host application owns all device allocations,
+ * a frame loop that must not allocate (allocation can synchronize the device), a
+ * fixed memory budget. The caller still owns tris_in and every bvh output array.
+ * Limits and rules:
+ *  - n <= CPT_LBVH_STATIC_MAX_TRIANGLES (131,072); larger n returns
+ *    CPT_ERR_SCRATCH_TOO_SMALL before any device work;
+ *  - the array (CPT_LBVH_STATIC_SCRATCH_BYTES, 8 MiB) is created on every GPU
+ *    that loads the library and held until the process exits;
+ *  - the first call on a device looks up the array's device address with that
+ *    device current (cudaGetSymbolAddress) — make that first call before any
+ *    stream capture;
+ *  - all calls share the one array: calls whose work overlaps on a GPU (e.g. on
+ *    two streams) race; serialize them. Each call zeroes what must start at zero,
+ *    so leftovers of the previous call are harmless. */
+#define CPT_LBVH_STATIC_MAX_TRIANGLES 131072u
+#define CPT_LBVH_STATIC_SCRATCH_BYTES (8u << 20)
+int cpt_lbvh_build_static(const cpt_triangle* tris_in, uint32_t n, const float* enclosing_box, int morton_bits,
+                          cpt_bvh* bvh, uint32_t flags, cudaStream_t stream);
+
 /* Reads the device status words of a build or render (synchronizes the stream)
  * and maps them to a status code. */
 int cpt_status_check(const uint32_t* d_status, cudaStream_t stream);
