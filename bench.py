@@ -261,25 +261,29 @@ def run_ours(args, w, world, rank, local):
     scene = DeviceScene(infos, None, dev)
     lb = DeviceLbvh(n, w["bits"], dev)
     lb.build(d_tris, check_root=True)
-    params = make_params(W_, H_, spp, 0, w["bounces"], 3.0, True, w["seed"] + 7919 * rank, cpt.ACCUM_KAHAN)
+    params = make_params(W_, H_, spp, 0, w["bounces"], 3.0, True, w["seed"], cpt.ACCUM_KAHAN,
+                         wave_paths=args.wave_paths, ray_sort=bool(args.ray_sort))
     rend = DeviceRenderer(params, dev)
     stream = torch.cuda.current_stream()
 
     # --- one instrumented frame: node fetches and triangle tests per closest-hit ray
     rend.reset()
-    rend.render(lb, scene, cam, frame0=0, trace_stats=True)
+    rend.render(lb, scene, cam, frame0=rank * (1 << 24), trace_stats=True)
     torch.cuda.synchronize()
     rend.check_status()
     c = rend.counts.cpu().numpy()
+    depth_rays = [int(x) for x in c[8:8 + w["bounces"] + 1]]
     inst_rays_closest = int(c[0] + c[1])
     mean_nodes = c[3] / max(inst_rays_closest, 1)
     mean_tris = c[4] / max(inst_rays_closest, 1)
 
-    # --- warm-up frames
+    # --- warm-up frames (rank r renders its own slice of the sample stream)
+    from cpt.multi import rank_frame0, reduce_accumulator
+
     rend.reset()
     frame = 0
     for _ in range(args.warmup):
-        rend.render(lb, scene, cam, frame0=frame + rank * 1_000_000)
+        rend.render(lb, scene, cam, frame0=rank_frame0(frame, rank))
         frame += spp
     torch.cuda.synchronize()
     rend.counts.zero_()
@@ -297,12 +301,10 @@ def run_ours(args, w, world, rank, local):
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for k in range(args.steps):
-        rend.render(lb, scene, cam, frame0=frame + rank * 1_000_000)
+        rend.render(lb, scene, cam, frame0=rank_frame0(frame, rank))
         frame += spp
         if world > 1:  # the one exchange of the path: framebuffer reduce to rank 0 every frame
-            import torch.distributed as dist
-
-            dist.reduce(rend.accum.view(torch.float32), dst=0)
+            reduce_accumulator(rend.accum, dst=0)
     ev1.record(stream)
     torch.cuda.synchronize()
     prof = cpt.profile_end()
@@ -335,6 +337,7 @@ def run_ours(args, w, world, rank, local):
                 "traffic": traffic, "algorithmic_bytes_per_launch": round(alg_bytes / max(ext_launches, 1), 1),
                 "avg_launch_ms": round(ext_ms / max(ext_launches, 1), 4),
                 "bytes_per_ray": f"32 ray + 16 hit + 64 x {mean_nodes:.2f} nodes + 48 x {mean_tris:.2f} triangles",
+                "rays_per_depth_first_frame": depth_rays,
                 "kernel_share": {k: round(v[0] / ms_total, 4) for k, v in sorted(prof.items())}}
 
     # --- LBVH build of the same scene (device-resident triangles)
@@ -369,6 +372,7 @@ def run_ours(args, w, world, rank, local):
     if not args.no_e2e:
         tr = cpt.Tracer(w["bits"])
         tr.set_settings(bounces=w["bounces"], intensity=3.0, stratified=True, seed=w["seed"] + 7919 * rank)
+        # (the tracer object renders frame 0 of its own seed on every rank: e2e ranks are replicas)
         tr.set_camera(cam)
         h_tris = torch.empty(tris.nbytes, dtype=torch.uint8, pin_memory=True)
         h_tris.numpy()[:] = tris.view(np.uint8)
@@ -441,6 +445,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--res", default=None, help="override resolution WxH (profiling runs)")
     ap.add_argument("--spp", type=int, default=None, help="override samples per frame (profiling runs)")
+    ap.add_argument("--wave-paths", type=int, default=0, help="paths per wave (0: library default)")
+    ap.add_argument("--ray-sort", type=int, default=0, help="1: coherence-sort bounce queues")
     args = ap.parse_args()
     w = dict(WORKLOADS[args.workload])
     if args.res:

@@ -84,7 +84,7 @@ class RenderParams(ctypes.Structure):
                 ("frame0", ctypes.c_uint32), ("bounces", ctypes.c_uint32), ("indirect_intensity", ctypes.c_float),
                 ("stratified", ctypes.c_uint32), ("seed_lo", ctypes.c_uint32), ("seed_hi", ctypes.c_uint32),
                 ("accum_mode", ctypes.c_uint32), ("ref_grid", ctypes.c_uint32), ("wave_paths", ctypes.c_uint32),
-                ("trace_stats", ctypes.c_uint32)]
+                ("trace_stats", ctypes.c_uint32), ("ray_sort", ctypes.c_uint32)]
 
 
 def _load() -> ctypes.CDLL:
@@ -247,9 +247,9 @@ def launch_count() -> int:
     return int(lib.cpt_launch_count())
 
 
-RAY_COUNTS = 8
+RAY_COUNTS = 72
 KERNELS = ("k_bounds", "k_morton", "k_scan_offsets", "k_onesweep", "k_topology", "k_gather_refit", "k_trace",
-           "k_generate", "k_extend", "k_shade", "k_wave_counts", "k_accumulate", "k_resolve")
+           "k_generate", "k_extend", "k_shade", "k_wave_counts", "k_accumulate", "k_resolve", "k_ray_sort")
 
 
 def profile_begin() -> None:

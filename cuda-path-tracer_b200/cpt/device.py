@@ -96,9 +96,11 @@ class DeviceScene:
 
 
 def make_params(width, height, spp, frame0=0, bounces=3, intensity=3.0, stratified=True, seed=0,
-                accum_mode=ACCUM_KAHAN, ref_grid=False, wave_paths=0, trace_stats=False) -> RenderParams:
+                accum_mode=ACCUM_KAHAN, ref_grid=False, wave_paths=0, trace_stats=False,
+                ray_sort=False) -> RenderParams:
     return RenderParams(width, height, spp, frame0, bounces, intensity, int(stratified), seed & 0xFFFFFFFF,
-                        (seed >> 32) & 0xFFFFFFFF, accum_mode, int(ref_grid), wave_paths, int(trace_stats))
+                        (seed >> 32) & 0xFFFFFFFF, accum_mode, int(ref_grid), wave_paths, int(trace_stats),
+                        int(ray_sort))
 
 
 class DeviceRenderer:
@@ -112,7 +114,7 @@ class DeviceRenderer:
         if not self.scratch_bytes:
             raise ValueError("render parameters rejected")
         self.scratch = dev_bytes(self.scratch_bytes, device)
-        self.counts = torch.zeros(8, dtype=torch.int64, device=device or "cuda")
+        self.counts = torch.zeros(72, dtype=torch.int64, device=device or "cuda")
         self.status = torch.zeros(4, dtype=torch.int32, device=device or "cuda")
         self.image = torch.empty((params.height, params.width, 4), dtype=torch.float32, device=device or "cuda")
 

@@ -20,7 +20,7 @@ std::atomic<bool> g_profiling{false};
 
 const char* const kKernelNames[K_KERNEL_COUNT] = {
     "k_bounds", "k_morton", "k_scan_offsets", "k_onesweep", "k_topology", "k_gather_refit", "k_trace",
-    "k_generate", "k_extend", "k_shade", "k_wave_counts", "k_accumulate", "k_resolve"};
+    "k_generate", "k_extend", "k_shade", "k_wave_counts", "k_accumulate", "k_resolve", "k_ray_sort"};
 
 namespace {
 struct ProfRecord { int id; cudaEvent_t a, b; };

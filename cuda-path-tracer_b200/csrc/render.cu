@@ -22,6 +22,7 @@
 #include "cpt.h"
 #include "cpt_internal.h"
 #include "traverse.cuh"
+#include "onesweep.cuh"
 
 namespace cpt {
 
@@ -30,7 +31,7 @@ constexpr int kExtendSteps = 8;
 constexpr int kShadeBlock = 128;
 constexpr int kGenBlock = 256;
 constexpr int kMaxDepth = 62;  // bounces + 1 queues; reference GUI allows 5 bounces (PathTracingSettings.h:27)
-constexpr uint32_t kDefaultWavePaths = 1u << 23;
+constexpr uint32_t kDefaultWavePaths = 1u << 25;
 
 struct Wave {
     uint32_t width, height, pixels;
@@ -135,19 +136,73 @@ __global__ void __launch_bounds__(kExtendBlock) k_extend(const float4* __restric
                                                          const uint32_t* __restrict__ count, float4* __restrict__ hits,
                                                          uint32_t* __restrict__ pool,
                                                          unsigned long long* __restrict__ ray_counts,
-                                                         uint32_t* __restrict__ status, uint32_t max_visits)
+                                                         uint32_t* __restrict__ status, uint32_t max_visits,
+                                                         const uint32_t* __restrict__ order)
 {
     __shared__ uint32_t s_stack[kSmemStack * kExtendBlock];
     const uint32_t n = *count;
     bool overflow = false;
     uint32_t nn = 0, nt = 0;
     persistent_trace<false, kExtendBlock, kStats, kExtendSteps>(nodes, queue, n, hits, pool, s_stack + threadIdx.x,
-                                                                overflow, nn, nt, max_visits, nullptr);
+                                                                overflow, nn, nt, max_visits, nullptr, order);
     if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
     if (kStats && ray_counts) {
         warp_count_u64(ray_counts + 3, nn);
         warp_count_u64(ray_counts + 4, nt);
     }
+}
+
+// Coherence key of a queued ray: direction octant (3 bits) above a 27-bit Morton
+// code of the origin quantized to 512 cells per axis of the scene's root box.
+// Also the 4 digit histograms of the keys and zeroing of the sort's look-back.
+constexpr int kRayKeyPasses = 4;
+
+__device__ __forceinline__ uint32_t spread3_10(uint32_t x)
+{
+    x &= 0x3FFu;
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+__global__ void __launch_bounds__(256) k_ray_keys(const float4* __restrict__ queue, const uint32_t* __restrict__ count,
+                                                  const cpt_bbox* __restrict__ root, uint32_t* __restrict__ keys,
+                                                  uint32_t* __restrict__ hist, uint32_t* __restrict__ zero,
+                                                  size_t zero_words)
+{
+    __shared__ uint32_t s_hist[kRayKeyPasses * kRadix];
+    for (int i = threadIdx.x; i < kRayKeyPasses * kRadix; i += blockDim.x) s_hist[i] = 0;
+    const size_t gtid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, gsize = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = gtid; i < zero_words; i += gsize) zero[i] = 0;
+    __syncthreads();
+    const uint32_t n = *count;
+    const cpt_bbox b = *root;
+    float inv[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float ext = b.max[a] - b.min[a];
+        inv[a] = ext > 0.f ? 511.0f / ext : 0.f;
+    }
+    for (uint32_t i = (uint32_t)gtid; i < n; i += (uint32_t)gsize) {
+        const float4 o = queue[2 * (size_t)i], d = queue[2 * (size_t)i + 1];
+        const float oo[3] = {o.x, o.y, o.z};
+        uint32_t q[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float c = (oo[a] - b.min[a]) * inv[a];
+            q[a] = (uint32_t)fminf(fmaxf(c, 0.0f), 511.0f);
+        }
+        const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+        const uint32_t key = (oct << 27) | spread3_10(q[0]) | (spread3_10(q[1]) << 1) | (spread3_10(q[2]) << 2);
+        keys[i] = key;
+#pragma unroll
+        for (int p = 0; p < kRayKeyPasses; ++p) atomicAdd(&s_hist[p * kRadix + ((key >> (8 * p)) & 0xFFu)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kRayKeyPasses * kRadix; i += blockDim.x)
+        if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
 }
 
 struct ShadeScene {
@@ -317,6 +372,7 @@ __global__ void k_wave_counts(const uint32_t* __restrict__ counts, uint32_t dept
     for (uint32_t b = 1; b < depth_count; ++b) ext += counts[b];
     atomicAdd(ray_counts + 0, (unsigned long long)counts[0]);
     atomicAdd(ray_counts + 1, ext);
+    for (uint32_t b = 0; b < depth_count && b < 64; ++b) atomicAdd(ray_counts + 8 + b, (unsigned long long)counts[b]);
 }
 
 // Adds the wave's samples to the accumulator, per pixel in sample order.
@@ -392,6 +448,13 @@ struct RenderScratch {
     float4* state;
     uint32_t* counts;
     uint32_t capacity;  // paths per wave
+    // coherence sort of bounce queues
+    uint32_t* sort_keys[2];
+    uint32_t* sort_vals[2];
+    uint32_t* sort_hist;
+    uint32_t* sort_offsets;
+    uint32_t* sort_zero;  // tile counters (32 words) + look-back
+    size_t sort_zero_words;
 };
 
 inline uint32_t wave_samples(const cpt_render_params* p)
@@ -415,8 +478,68 @@ size_t render_layout(const cpt_render_params* p, void* base, RenderScratch* out)
     s.hits = c.take<float4>(s.capacity);
     s.state = c.take<float4>(2ull * s.capacity);
     s.counts = c.take<uint32_t>(2 * (kMaxDepth + 2));  // queue counts, then persistent-kernel ray pools
+    if (p->ray_sort) {
+        const size_t tiles = (s.capacity + kSortTile - 1) / kSortTile;
+        for (int k = 0; k < 2; ++k) {
+            s.sort_keys[k] = c.take<uint32_t>(s.capacity);
+            s.sort_vals[k] = c.take<uint32_t>(s.capacity);
+        }
+        s.sort_hist = c.take<uint32_t>(kRayKeyPasses * kRadix);
+        s.sort_offsets = c.take<uint32_t>(kRayKeyPasses * kRadix);
+        s.sort_zero_words = 32 + (size_t)kRayKeyPasses * tiles * kRadix;
+        s.sort_zero = c.take<uint32_t>(s.sort_zero_words);
+    } else {
+        s.sort_keys[0] = s.sort_keys[1] = s.sort_vals[0] = s.sort_vals[1] = nullptr;
+        s.sort_hist = s.sort_offsets = s.sort_zero = nullptr;
+        s.sort_zero_words = 0;
+    }
     if (out) *out = s;
     return c.used();
+}
+
+// Sorts the `*count` rays of `queue` by coherence key; the permutation ends in
+// rs.sort_vals[(kRayKeyPasses - 1) & 1]. Grids are sized for the wave capacity;
+// the kernels read the actual count on the device.
+int sort_queue(const RenderScratch& rs, const float4* queue, const uint32_t* count, const cpt_bbox* root,
+               uint32_t* status, cudaStream_t stream)
+{
+    const uint32_t tiles = (rs.capacity + kSortTile - 1) / kSortTile;
+    const int sms = sm_count();
+    CPT_CUDA_TRY(cudaMemsetAsync(rs.sort_hist, 0, sizeof(uint32_t) * kRayKeyPasses * kRadix, stream));
+    {
+        CPT_PROF(K_RAY_SORT, stream);
+        k_ray_keys<<<sms * 8, 256, 0, stream>>>(queue, count, root, rs.sort_keys[0], rs.sort_hist, rs.sort_zero,
+                                                rs.sort_zero_words);
+    }
+    CPT_LAUNCH_CHECK();
+    {
+        CPT_PROF(K_RAY_SORT, stream);
+        k_scan_offsets<<<kRayKeyPasses, kRadix, 0, stream>>>(rs.sort_hist, rs.sort_offsets);
+    }
+    CPT_LAUNCH_CHECK();
+    const size_t smem = onesweep_smem<uint32_t>();
+    CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<uint32_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<uint32_t, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    uint32_t* lookback = rs.sort_zero + 32;
+    for (int p = 0; p < kRayKeyPasses; ++p) {
+        const uint32_t* kin = rs.sort_keys[p & 1];
+        uint32_t* kout = rs.sort_keys[(p + 1) & 1];
+        const uint32_t* vin = p == 0 ? nullptr : rs.sort_vals[(p + 1) & 1];
+        uint32_t* vout = rs.sort_vals[p & 1];
+        CPT_PROF(K_RAY_SORT, stream);
+        if (p == 0)
+            k_onesweep<uint32_t, true><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, 0, count, 8 * p,
+                                                                            rs.sort_offsets + p * kRadix,
+                                                                            lookback + (size_t)p * tiles * kRadix,
+                                                                            rs.sort_zero + p, status);
+        else
+            k_onesweep<uint32_t, false><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, 0, count, 8 * p,
+                                                                             rs.sort_offsets + p * kRadix,
+                                                                             lookback + (size_t)p * tiles * kRadix,
+                                                                             rs.sort_zero + p, status);
+        CPT_LAUNCH_CHECK();
+    }
+    return CPT_OK;
 }
 
 bool params_ok(const cpt_render_params* p)
@@ -516,15 +639,21 @@ extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_
         for (uint32_t b = 0; b <= params->bounces; ++b) {
             const float4* qin = rs.queue[b & 1];
             float4* qout = rs.queue[(b + 1) & 1];
+            const uint32_t* order = nullptr;
+            if (params->ray_sort && b > 0) {
+                int rc = sort_queue(rs, qin, rs.counts + b, bvh->node_boxes, st, stream);
+                if (rc != CPT_OK) return rc;
+                order = rs.sort_vals[(kRayKeyPasses - 1) & 1];
+            }
             {
                 CPT_PROF(K_EXTEND, stream);
                 uint32_t* pool = rs.counts + kMaxDepth + 2 + b;
                 if (params->trace_stats)
                     k_extend<true><<<ext_blocks, kExtendBlock, 0, stream>>>(sc.nodes, qin, rs.counts + b, rs.hits, pool,
-                                                                            ray_counts, st, sc.max_visits);
+                                                                            ray_counts, st, sc.max_visits, order);
                 else
                     k_extend<false><<<ext_blocks, kExtendBlock, 0, stream>>>(sc.nodes, qin, rs.counts + b, rs.hits, pool,
-                                                                             ray_counts, st, sc.max_visits);
+                                                                             ray_counts, st, sc.max_visits, order);
             }
             CPT_LAUNCH_CHECK();
             {

@@ -21,7 +21,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(const float4* __restrict_
     bool overflow = false;
     uint32_t nn = 0, nt = 0;
     persistent_trace<kAny, kTraceBlock, kStats, kTraceSteps>(nodes, rays, n, hits, pool, s_stack + threadIdx.x, overflow,
-                                                             nn, nt, max_visits, stats);
+                                                             nn, nt, max_visits, stats, nullptr);
     if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
 }
 

@@ -37,43 +37,50 @@ constexpr int kNodeFloats = 24;
 
 struct Hit { float t, u, v; uint32_t tri; };
 
-__device__ __forceinline__ float slab_test(f3 o, f3 dinv, float ax, float ay, float az, float bx, float by, float bz)
+// Slab test with glm's select semantics (min(x,y) = x<y?x:y, max(x,y) = x>y?x:y).
+// When every 1/d component is finite ("finite"), no product can be NaN, and then
+// those selects and fminf/fmaxf return the same value (up to the sign of a zero,
+// which no comparison below sees), so the single-instruction forms are used.
+__device__ __forceinline__ float slab_test(f3 o, f3 dinv, bool finite, float ax, float ay, float az, float bx,
+                                           float by, float bz)
 {
-    float tx0 = __fmul_rn(__fsub_rn(ax, o.x), dinv.x), tx1 = __fmul_rn(__fsub_rn(bx, o.x), dinv.x);
-    float ty0 = __fmul_rn(__fsub_rn(ay, o.y), dinv.y), ty1 = __fmul_rn(__fsub_rn(by, o.y), dinv.y);
-    float tz0 = __fmul_rn(__fsub_rn(az, o.z), dinv.z), tz1 = __fmul_rn(__fsub_rn(bz, o.z), dinv.z);
-    float n = gmax(gmax(gmin(tx0, tx1), gmin(ty0, ty1)), gmin(tz0, tz1));
-    float f = gmin(gmin(gmax(tx0, tx1), gmax(ty0, ty1)), gmax(tz0, tz1));
+    const float tx0 = __fmul_rn(__fsub_rn(ax, o.x), dinv.x), tx1 = __fmul_rn(__fsub_rn(bx, o.x), dinv.x);
+    const float ty0 = __fmul_rn(__fsub_rn(ay, o.y), dinv.y), ty1 = __fmul_rn(__fsub_rn(by, o.y), dinv.y);
+    const float tz0 = __fmul_rn(__fsub_rn(az, o.z), dinv.z), tz1 = __fmul_rn(__fsub_rn(bz, o.z), dinv.z);
+    float n, f;
+    if (finite) {
+        n = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fminf(tz0, tz1));
+        f = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
+    } else {
+        n = gmax(gmax(gmin(tx0, tx1), gmin(ty0, ty1)), gmin(tz0, tz1));
+        f = gmin(gmin(gmax(tx0, tx1), gmax(ty0, ty1)), gmax(tz0, tz1));
+    }
     return (n <= f && f > 0.0f) ? n : FLT_MAX;
 }
 
-// s: the 10-word slot, v0 = s[0..2], e1 = s[4..6], e2 = s[7..9].
+// Möller-Trumbore on a slot (v0 = s[0..2], e1 = s[4..6], e2 = s[7..9]), without
+// early exits: every lane of a warp runs the same instructions, and u, v, t are the
+// values the reference computes; only the final predicate decides the hit.
 __device__ __forceinline__ float tri_test(f3 o, f3 d, const float* s, float& u, float& v)
 {
     const f3 p0 = mk3(s[0], s[1], s[2]), e1 = mk3(s[4], s[5], s[6]), e2 = mk3(s[7], s[8], s[9]);
     const f3 q = cross(d, e2);
     const float det = dot(e1, q);
-    if (det > -FLT_EPSILON && det < FLT_EPSILON) return FLT_MAX;
     const float inv = __frcp_rn(det);
     const f3 sv = sub(o, p0);
     u = __fmul_rn(inv, dot(sv, q));
-    if (u < 0.f) return FLT_MAX;
     const f3 r = cross(sv, e1);
     v = __fmul_rn(inv, dot(d, r));
-    if (v < 0.f || __fadd_rn(u, v) > 1.f) return FLT_MAX;
     const float t = __fmul_rn(inv, dot(e2, r));
-    return t >= 0.0f ? t : FLT_MAX;
-}
-
-__device__ __forceinline__ float child_test(f3 o, f3 d, f3 dinv, bool internal, const float* s, float& u, float& v)
-{
-    if (internal) return slab_test(o, dinv, s[0], s[1], s[2], s[3], s[4], s[5]);
-    return tri_test(o, d, s, u, v);
+    const bool hit = !(det > -FLT_EPSILON && det < FLT_EPSILON) && !(u < 0.f) && !(v < 0.f) &&
+                     !(__fadd_rn(u, v) > 1.f) && t >= 0.0f;
+    return hit ? t : FLT_MAX;
 }
 
 // Per-ray traversal state.
 struct TraceState {
     f3 o, d, dinv;
+    bool finite;  // all components of 1/d finite
     Hit best;
     uint32_t cur;
     int sp;
@@ -86,6 +93,7 @@ __device__ __forceinline__ void trace_init(TraceState& s, f3 o, f3 d)
     s.o = o;
     s.d = d;
     s.dinv = mk3(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
+    s.finite = isfinite(s.dinv.x) && isfinite(s.dinv.y) && isfinite(s.dinv.z);
     s.best.t = FLT_MAX;
     s.best.u = 0.f;
     s.best.v = 0.f;
@@ -137,8 +145,21 @@ __device__ __forceinline__ bool trace_step(TraceState& s, const float4* __restri
         s.tests += t;
     }
     float lu = 0.f, lv = 0.f, ru = 0.f, rv = 0.f;
-    const float hl = child_test(s.o, s.d, s.dinv, lint, w, lu, lv);
-    const float hr = child_test(s.o, s.d, s.dinv, rint, w + 10, ru, rv);
+    // Both slab tests run on every lane (a leaf slot's result is discarded), then
+    // one Möller-Trumbore code path serves the first leaf child, left or right,
+    // and a second one only lanes whose two children are both leaves.
+    float hl = slab_test(s.o, s.dinv, s.finite, w[0], w[1], w[2], w[3], w[4], w[5]);
+    float hr = slab_test(s.o, s.dinv, s.finite, w[10], w[11], w[12], w[13], w[14], w[15]);
+    if (!lint || !rint) {
+        float t0[10];
+#pragma unroll
+        for (int k = 0; k < 10; ++k) t0[k] = lint ? w[10 + k] : w[k];
+        float u0, v0;
+        const float h0 = tri_test(s.o, s.d, t0, u0, v0);
+        if (!lint) { hl = h0; lu = u0; lv = v0; }
+        else { hr = h0; ru = u0; rv = v0; }
+        if (!lint && !rint) hr = tri_test(s.o, s.d, w + 10, ru, rv);
+    }
     bool pop = false;
     if (hl >= s.best.t && hr >= s.best.t) {
         pop = true;
@@ -194,11 +215,14 @@ __device__ __forceinline__ Hit traverse(const float4* __restrict__ nodes, f3 o, 
 // (.w of the first holds a payload), its hit goes to hits[i]. Lanes take rays from
 // *pool in warp-sized grabs and refill as soon as their ray finishes.
 // ray_stats (nullable, with kStats): per ray (node fetches, triangle tests).
+// order (nullable): rays are taken in the order order[0], order[1], ... (a
+// permutation of 0..n-1); hits and stats stay indexed by the ray's own index.
 template <bool kAny, int kBlock, bool kStats, int kSteps>
 __device__ __forceinline__ void persistent_trace(const float4* __restrict__ nodes, const float4* __restrict__ rays,
                                                  uint32_t n, float4* __restrict__ hits, uint32_t* __restrict__ pool,
                                                  uint32_t* smem_col, bool& overflow, uint32_t& n_nodes,
-                                                 uint32_t& n_tris, uint32_t max_visits, uint2* __restrict__ ray_stats)
+                                                 uint32_t& n_tris, uint32_t max_visits, uint2* __restrict__ ray_stats,
+                                                 const uint32_t* __restrict__ order)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
@@ -219,8 +243,8 @@ __device__ __forceinline__ void persistent_trace(const float4* __restrict__ node
                 if (idle) {
                     const uint32_t r = base + (uint32_t)__popc(m & lt_mask);
                     if (r < n) {
-                        ray = r;
-                        const float4 ro = rays[2 * (size_t)r], rd = rays[2 * (size_t)r + 1];
+                        ray = order ? order[r] : r;
+                        const float4 ro = rays[2 * (size_t)ray], rd = rays[2 * (size_t)ray + 1];
                         trace_init(s, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z));
                     }
                 }

@@ -169,6 +169,8 @@ typedef struct cpt_render_params {
     uint32_t ref_grid;         /* 1: render only the reference's (W/8*8) x (H/8*8) grid */
     uint32_t wave_paths;       /* paths in flight per wave (0: library default) */
     uint32_t trace_stats;      /* 1: count node fetches / triangle tests of extension rays (slower) */
+    uint32_t ray_sort;         /* 1: sort each bounce queue by direction octant + origin Morton code
+                                *    before tracing it (coherence; results are unchanged) */
 } cpt_render_params;
 
 size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode);
@@ -177,11 +179,11 @@ size_t cpt_render_scratch_bytes(const cpt_render_params* params);
 /* Renders params->spp samples into accum. Replaces CUDAPathTracer::raytrace
  * (cuda_path_tracer.cu:423-464) and raytrace_kernel (:385-421).
  * ray_counts (device, nullable): CPT_RAY_COUNTS x uint64, incremented by
- * [0] primary, [1] extension, [2] shadow rays traced, and — with
- * params->trace_stats — [3] internal nodes fetched and [4] triangles tested by the
- * closest-hit (primary + extension) rays. status (device, nullable): CPT_STATUS_*
- * bits are OR-ed in. */
-#define CPT_RAY_COUNTS 8
+ * [0] primary, [1] extension, [2] shadow rays traced, — with params->trace_stats —
+ * [3] internal nodes fetched and [4] triangles tested by the closest-hit (primary +
+ * extension) rays, and [8 + b] closest-hit rays traced at path depth b (b < 64).
+ * status (device, nullable): CPT_STATUS_* bits are OR-ed in. */
+#define CPT_RAY_COUNTS 72
 int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_camera* camera, const cpt_render_params* params,
                void* accum, void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
                cudaStream_t stream);

@@ -36,13 +36,14 @@ def ocam(cam, jitter=False):
 
 
 def gpu_render(tris, infos, lights, cam, mode, spp=4, frame0=5, bounces=3, seed=77, bits=30, jitter=False,
-               wave_paths=0, ref_grid=False, w=W, h=H, stratified=True):
+               wave_paths=0, ref_grid=False, w=W, h=H, stratified=True, ray_sort=False):
     lb = DeviceLbvh(len(tris), bits)
     lb.build(to_device(tris), check_root=True)
     sc = DeviceScene(infos, lights)
     c = cpt.Camera.from_buffer_copy(cam)
     c.jitter, c.jitter_x, c.jitter_y = int(jitter), 2.0 / w, 2.0 / h
-    r = DeviceRenderer(make_params(w, h, spp, frame0, bounces, 3.0, stratified, seed, mode, ref_grid, wave_paths))
+    r = DeviceRenderer(make_params(w, h, spp, frame0, bounces, 3.0, stratified, seed, mode, ref_grid, wave_paths,
+                                   ray_sort=ray_sort))
     r.render(lb, sc, c)
     torch.cuda.synchronize()
     r.check_status()
@@ -116,6 +117,19 @@ def test_wave_size_does_not_change_the_image(cuda):
     b, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_KAHAN, spp=6, wave_paths=4 * W * H)
     c, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_KAHAN, spp=6)
     assert a.accum.cpu().numpy().tobytes() == b.accum.cpu().numpy().tobytes() == c.accum.cpu().numpy().tobytes()
+
+
+def test_coherence_sort_does_not_change_the_image(cuda):
+    tris, infos, _, cam = scene()
+    lights = dir_lights()
+    a, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_KAHAN, spp=3, bounces=5, ray_sort=False)
+    b, _ = gpu_render(tris, infos, lights, cam, cpt.ACCUM_KAHAN, spp=3, bounces=5, ray_sort=True)
+    assert a.accum.cpu().numpy().tobytes() == b.accum.cpu().numpy().tobytes()
+    assert np.array_equal(a.counts.cpu().numpy(), b.counts.cpu().numpy())
+    rad, _ = oracle_samples(tris, infos, lights, cam, spp=3, bounces=5)
+    s, _, _ = cpu.accumulate_kahan(rad)
+    gs, _ = accum_arrays(b, cpt.ACCUM_KAHAN)
+    assert gs[..., :3].tobytes() == s.tobytes()
 
 
 def test_directional_lights_shadow_rays(cuda):
