@@ -326,11 +326,13 @@ def run_ours(args, w, world, rank, local):
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "k_extend_traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            tj = json.load(f)
-        traffic = round(float(tj["dram_bytes_per_closest_ray"]) * rays_closest / max(ext_launches, 1), 1)
+    tp = os.path.join(ROOT, "profiles", "k_extend_c2.md")
+    if args.workload == "c2" and os.path.exists(tp):  # ncu figure of the C2 traversal (see that file)
+        import re
+
+        m = re.search(r"dram_bytes_per_closest_ray = ([0-9.]+)", open(tp).read())
+        if m:
+            traffic = round(float(m.group(1)) * rays_closest / max(ext_launches, 1), 1)
     roofline = {"bound": "hbm", "kernel": "k_extend", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6650 GB/s",
