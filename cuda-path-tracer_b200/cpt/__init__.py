@@ -127,6 +127,8 @@ _PROTOS = {
     "cpt_scene_random": (_U32, [_U32, _U32, _F, _F, _F, _F, _F, _F, _P, _P]),
     "cpt_scene_sphere_hairball": (_U32, [_U32, _U32, _F, _U32, _F, _U32, _F, _F, _F, _F, _P, _P]),
     "cpt_scene_bounds": (None, [_P, _U32, _P]),
+    "cpt_obj_load": (_I32, [ctypes.c_char_p, _F, _P, _F, _P, _P, _U32, ctypes.POINTER(_U32)]),
+    "cpt_bvh_heatmap": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Camera), _U32, _U32, _P, _P, _P, _P]),
     "cpt_camera_look_at": (None, [_P, _P, _P, _F, _F, _F, _F, ctypes.POINTER(Camera)]),
     "cpt_profile_begin": (_I32, []),
     "cpt_profile_end": (_I32, []),
@@ -175,6 +177,26 @@ def scene_sphere_hairball(nu: int, nv: int, n_hair: int, seed: int = 0, amp: flo
     n = lib.cpt_scene_sphere_hairball(nu, nv, amp, n_hair, hair_radius, seed, albedo, light_y, light_size,
                                       light_emission, _ptr(tris), _ptr(infos))
     return tris[:n], infos[:n]
+
+
+def load_obj(path: str, scale: float = 1.0, translate=(0.0, 0.0, 0.0), default_grey: float = 0.7):
+    """OBJ/MTL file -> (triangles, infos) numpy records (extractScene semantics)."""
+    n = ctypes.c_uint32()
+    tr = np.asarray(translate, np.float32)
+    check(lib.cpt_obj_load(path.encode(), scale, _ptr(tr), default_grey, None, None, 0, ctypes.byref(n)),
+          "cpt_obj_load")
+    tris = np.zeros(n.value, TRIANGLE_DTYPE)
+    infos = np.zeros(n.value, TRIANGLE_INFO_DTYPE)
+    check(lib.cpt_obj_load(path.encode(), scale, _ptr(tr), default_grey, _ptr(tris), _ptr(infos), n.value,
+                           ctypes.byref(n)), "cpt_obj_load")
+    return tris, infos
+
+
+def bvh_heatmap(bvh: "Bvh", cam: "Camera", width: int, height: int, base_color, rgba_dev: int, counts_dev: int = 0,
+                stream: int = 0) -> None:
+    bc = np.asarray(base_color, np.float32)
+    check(lib.cpt_bvh_heatmap(ctypes.byref(bvh), ctypes.byref(cam), width, height, _ptr(bc), rgba_dev,
+                              counts_dev or None, stream), "cpt_bvh_heatmap")
 
 
 def scene_bounds(tris: np.ndarray) -> np.ndarray:

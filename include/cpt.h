@@ -192,6 +192,13 @@ int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_camera* cam
 int cpt_resolve(const void* accum, uint32_t width, uint32_t height, uint32_t accum_mode, float* rgba,
                 cudaStream_t stream);
 
+/* BVH heat map: per pixel, the number of internal-node boxes the camera's primary
+ * ray hits, as base_color added once per box. Replaces CUDA::computeBVHColor
+ * (source/application/cuda/visualization.h:19-66). rgba: device float4 per pixel;
+ * node_counts (device, nullable): the counts. base_color is a host pointer. */
+int cpt_bvh_heatmap(const cpt_bvh* bvh, const cpt_camera* camera, uint32_t width, uint32_t height,
+                    const float base_color[3], float* rgba, uint32_t* node_counts, cudaStream_t stream);
+
 /* ---- reference-facing tracer object (host buffers in, image out) ----
  * Mirrors CUDAPathTracer (source/application/cuda/cuda_path_tracer.h:13-40):
  * upload a HostSceneDescription, set primary rays and eye, raytrace frame by
@@ -235,6 +242,14 @@ uint32_t cpt_scene_random(uint32_t n_random, uint32_t seed, float edge_min, floa
 uint32_t cpt_scene_sphere_hairball(uint32_t nu, uint32_t nv, float amp, uint32_t n_hair, float hair_radius,
                                    uint32_t seed, float albedo, float light_y, float light_size,
                                    float light_emission, cpt_triangle* tris, cpt_triangle_info* infos);
+/* Wavefront OBJ (+ MTL) ingest, as PathTracingApp::extractScene fills the scene
+ * (PathTracingApp.cpp:31-124): world position = file position * scale + translate
+ * (translate nullable), vertex colours or the material's Kd (default_grey without a
+ * material), normals from the file or the triangle's geometric normal, Ke as
+ * emission, Ns as specularity. With tris == NULL only counts: *n_out = triangles.
+ * Returns CPT_ERR_SCRATCH_TOO_SMALL when capacity is below the count. Host memory. */
+int cpt_obj_load(const char* path, float scale, const float* translate, float default_grey, cpt_triangle* tris,
+                 cpt_triangle_info* infos, uint32_t capacity, uint32_t* n_out);
 /* Enclosing box (min, max) of a host triangle soup, as the reference's caller builds it. */
 void cpt_scene_bounds(const cpt_triangle* tris, uint32_t n, float out[6]);
 /* Camera corner directions for eye/target/up, vertical fov (degrees), aspect,

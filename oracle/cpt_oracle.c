@@ -778,6 +778,43 @@ void orc_render_f64(const otri* sorted, const uint32_t* children, const obox* bo
     for (size_t i = 0; i < 3 * (size_t)width * height; ++i) mean_out[i] /= spp;
 }
 
+/* Heat map (visualization.h:19-66): per pixel, base added once per internal box
+ * hit, walking every hit box; stops when the 64-entry stack is full. */
+void orc_heatmap(const uint32_t* children, const obox* boxes, const ocam* cam, uint32_t width, uint32_t height,
+                 const float base[3], float* rgba, uint32_t* counts)
+{
+    v3 d00 = ld3(cam->dirs[0]), d10 = ld3(cam->dirs[1]), d11 = ld3(cam->dirs[2]), d01 = ld3(cam->dirs[3]);
+    v3 eye = ld3(cam->eye);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (long q = 0; q < (long)width * height; ++q) {
+        uint32_t x = (uint32_t)(q % width), y = (uint32_t)(q / width);
+        float tx = (float)x / (float)width, ty = (float)y / (float)height;
+        v3 dir = mix3(mix3(d00, d10, tx), mix3(d01, d11, tx), ty);
+        v3 dinv = mk(1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z);
+        uint32_t stack[STACK_CAP];
+        int top = 0, full = 0;
+        stack[top++] = 0;
+        float a[3] = {0.f, 0.f, 0.f};
+        uint32_t count = 0;
+        while (top > 0 && !full) {
+            uint32_t node = children[stack[--top]];
+            for (int side = 0; side < 2 && !full; ++side) {
+                if (!((node >> side) & 1u)) continue;
+                uint32_t c = (node >> 2) + (uint32_t)side;
+                float t;
+                if (slab_hit(eye, dinv, &boxes[c], &t)) {
+                    stack[top++] = c;
+                    for (int k = 0; k < 3; ++k) a[k] = a[k] + base[k];
+                    ++count;
+                }
+                full = top == STACK_CAP;
+            }
+        }
+        rgba[4 * q] = a[0]; rgba[4 * q + 1] = a[1]; rgba[4 * q + 2] = a[2]; rgba[4 * q + 3] = 1.0f;
+        if (counts) counts[q] = count;
+    }
+}
+
 /* Philox known-answer access for the tests. */
 void orc_philox(const uint32_t ctr[4], uint32_t k0, uint32_t k1, uint32_t out[4]) { cpt_philox4x32_10(ctr, k0, k1, out); }
 void orc_sincos_turns(const float* u, uint32_t m, float* s, float* c)

@@ -52,6 +52,7 @@ def oracle_lib() -> ctypes.CDLL:
         L.orc_philox.argtypes = [P, U, U, P]
         L.orc_sincos_turns.argtypes = [P, U, P, P]
         L.orc_corner_dirs.argtypes = [ctypes.POINTER(OCam), U, U, U, P]
+        L.orc_heatmap.argtypes = [P, P, ctypes.POINTER(OCam), U, U, P, P, P]
         _oracle = L
     return _oracle
 
@@ -192,6 +193,15 @@ def ref_render(b: BuildResult, infos: np.ndarray, lights, width: int, height: in
                  int(stratified), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, _p(cam15), _p(out), _p(counts),
                  threads)
     return out, counts
+
+
+def heatmap(b: BuildResult, cam: OCam, width: int, height: int, base):
+    rgba = np.zeros((height, width, 4), np.float32)
+    counts = np.zeros((height, width), np.uint32)
+    bc = np.asarray(base, np.float32)
+    oracle_lib().orc_heatmap(_p(b.children), _p(b.node_boxes), ctypes.byref(cam), width, height, _p(bc), _p(rgba),
+                             _p(counts))
+    return rgba, counts
 
 
 def philox(ctr, k0: int, k1: int) -> np.ndarray:
