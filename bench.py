@@ -37,6 +37,9 @@ WORKLOADS = {
                bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0),
     "c1": dict(kind="random", n=65536, bits=30, width=512, height=512, spp=1, bounces=3, eye=(0.5, 0.5, -1.2),
                target=(0.5, 0.5, 0.0), seed=0),
+    # deforming 16.8 M-triangle displaced sphere, full rebuild every frame, 8 cameras
+    "c5": dict(kind="deform", nu=4096, nv=2048, n_hair=0, bits=63, width=1280, height=720, spp=1, bounces=7,
+               eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, cameras=8, amp=0.01, omega=40.0),
 }
 METRIC = "Mrays/s"
 
@@ -49,11 +52,28 @@ def make_scene(w):
     return cpt.scene_sphere_hairball(w["nu"], w["nv"], w["n_hair"], seed=w["seed"])
 
 
+def make_cameras(w):
+    """The workload's camera(s): one, or `cameras` orbiting the target at the eye's distance."""
+    import math
+
+    import cpt
+
+    aspect = w["width"] / w["height"]
+    k = w.get("cameras", 1)
+    if k == 1:
+        return [cpt.camera_look_at(w["eye"], w["target"], fov_deg=45.0, aspect=aspect)]
+    r = math.hypot(w["eye"][0], w["eye"][2])
+    return [cpt.camera_look_at((r * math.sin(2 * math.pi * i / k), w["eye"][1], -r * math.cos(2 * math.pi * i / k)),
+                               w["target"], fov_deg=45.0, aspect=aspect) for i in range(k)]
+
+
 def workload_config(name, w, n_tris, l2_note):
-    c = {"workload": f"{name}: " + ("fBm sphere 2048x1024x2 + 1M hairball + quad light" if name == "c2"
-                                     else "65,536 random triangles + quad light"),
+    desc = {"c2": "fBm sphere 2048x1024x2 + 1M hairball + quad light",
+            "c1": "65,536 random triangles + quad light",
+            "c5": "deforming fBm sphere 4096x2048x2 + quad light, rebuild every frame, 8 cameras"}[name]
+    c = {"workload": f"{name}: {desc}",
          "triangles": int(n_tris), "morton_bits": w["bits"], "resolution": f'{w["width"]}x{w["height"]}',
-         "spp_per_step": w["spp"], "depth": w["bounces"] + 1, "l2": l2_note}
+         "spp_per_step": w["spp"], "depth": w["bounces"] + 1, "cameras": w.get("cameras", 1), "l2": l2_note}
     return c
 
 
@@ -215,7 +235,7 @@ def run_reference_arm(args, w, world, rank):
     t0 = time.perf_counter()
     tris, infos = make_scene(w)
     gen_s = time.perf_counter() - t0
-    cam = cpt.camera_look_at(w["eye"], w["target"], fov_deg=45.0, aspect=w["width"] / w["height"])
+    cam = make_cameras(w)[0]
     # size one step for ~8 s of CPU work, then warm up and time K steps of that size
     probe = cpu_reference_run(w, tris, infos, cam, w["bits"], target_s=8.0)
     rows = probe["rows"]
@@ -256,13 +276,22 @@ def run_ours(args, w, world, rank, local):
     gen_s = time.perf_counter() - t0
     n = len(tris)
     W_, H_, spp = w["width"], w["height"], w["spp"]
-    cam = cpt.camera_look_at(w["eye"], w["target"], fov_deg=45.0, aspect=W_ / H_)
+    cams = make_cameras(w)
+    cam = cams[0] if len(cams) == 1 else cams
+    deforming = w["kind"] == "deform"
     d_tris = to_device(tris, dev)
+    d_rest = to_device(tris, dev) if deforming else None
     scene = DeviceScene(infos, None, dev)
     lb = DeviceLbvh(n, w["bits"], dev)
     lb.build(d_tris, check_root=True)
     params = make_params(W_, H_, spp, 0, w["bounces"], 3.0, True, w["seed"], cpt.ACCUM_KAHAN,
-                         wave_paths=args.wave_paths, ray_sort=bool(args.ray_sort))
+                         wave_paths=args.wave_paths, ray_sort=bool(args.ray_sort), cameras=len(cams))
+
+    def deform_and_rebuild(frame_index):
+        # the deforming-mesh step: move the vertices, then a full LBVH rebuild
+        cpt.check(cpt.lib.cpt_scene_deform(d_rest.data_ptr(), d_tris.data_ptr(), n, w["amp"], w["omega"],
+                                           0.1 * frame_index, stream_handle()), "cpt_scene_deform")
+        lb.build(d_tris)
     rend = DeviceRenderer(params, dev)
     stream = torch.cuda.current_stream()
 
@@ -282,7 +311,9 @@ def run_ours(args, w, world, rank, local):
 
     rend.reset()
     frame = 0
-    for _ in range(args.warmup):
+    for i in range(args.warmup):
+        if deforming:
+            deform_and_rebuild(i)
         rend.render(lb, scene, cam, frame0=rank_frame0(frame, rank))
         frame += spp
     torch.cuda.synchronize()
@@ -301,6 +332,8 @@ def run_ours(args, w, world, rank, local):
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for k in range(args.steps):
+        if deforming:
+            deform_and_rebuild(args.warmup + k)
         rend.render(lb, scene, cam, frame0=rank_frame0(frame, rank))
         frame += spp
         if world > 1:  # the one exchange of the path: framebuffer reduce to rank 0 every frame
@@ -342,22 +375,29 @@ def run_ours(args, w, world, rank, local):
                 "rays_per_depth_first_frame": depth_rays,
                 "kernel_share": {k: round(v[0] / ms_total, 4) for k, v in sorted(prof.items())}}
 
-    # --- LBVH build of the same scene (device-resident triangles)
-    for _ in range(max(3, args.warmup)):
-        lb.build(d_tris)
-    torch.cuda.synchronize()
-    nb = max(5, args.steps)
-    cpt.profile_begin()
-    b0 = torch.cuda.Event(enable_timing=True)
-    b1 = torch.cuda.Event(enable_timing=True)
-    b0.record(stream)
-    for _ in range(nb):
-        lb.build(d_tris)
-    b1.record(stream)
-    torch.cuda.synchronize()
-    bprof = cpt.profile_end()
+    # --- LBVH build of the same scene (device-resident triangles); the deforming
+    # workload already rebuilt inside every timed step: those builds are reported
+    if deforming:
+        nb = args.steps
+        bprof = {k: v for k, v in prof.items()
+                 if k in ("k_bounds", "k_morton", "k_scan_offsets", "k_onesweep", "k_topology", "k_gather_refit")}
+        build_ms = max_over_ranks(sum(v[0] for v in bprof.values()) / nb, world)
+    else:
+        for _ in range(max(3, args.warmup)):
+            lb.build(d_tris)
+        torch.cuda.synchronize()
+        nb = max(5, args.steps)
+        cpt.profile_begin()
+        b0 = torch.cuda.Event(enable_timing=True)
+        b1 = torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        for _ in range(nb):
+            lb.build(d_tris)
+        b1.record(stream)
+        torch.cuda.synchronize()
+        bprof = cpt.profile_end()
+        build_ms = max_over_ranks(b0.elapsed_time(b1) / nb, world)
     lb.status()
-    build_ms = max_over_ranks(b0.elapsed_time(b1) / nb, world)
     key_bytes = 4 if w["bits"] == 30 else 8
     passes = 4 if w["bits"] == 30 else 8
     # algorithmic bytes per triangle: Morton 36 in + K+4 out, histogram K, sort 2P(K+4),
@@ -371,11 +411,11 @@ def run_ours(args, w, world, rank, local):
 
     # --- end to end through the tracer object (host buffers, pinned)
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and not deforming:
         tr = cpt.Tracer(w["bits"])
         tr.set_settings(bounces=w["bounces"], intensity=3.0, stratified=True, seed=w["seed"] + 7919 * rank)
         # (the tracer object renders frame 0 of its own seed on every rank: e2e ranks are replicas)
-        tr.set_camera(cam)
+        tr.set_camera(cams[0])
         h_tris = torch.empty(tris.nbytes, dtype=torch.uint8, pin_memory=True)
         h_tris.numpy()[:] = tris.view(np.uint8)
         h_infos = torch.empty(infos.nbytes, dtype=torch.uint8, pin_memory=True)
@@ -417,7 +457,7 @@ def run_ours(args, w, world, rank, local):
     # --- CPU baseline (rank 0, N = 1)
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_reference_run(w, tris, infos, cam, w["bits"], target_s=args.cpu_seconds)
+        r = cpu_reference_run(w, tris, infos, cams[0], w["bits"], target_s=args.cpu_seconds)
         cpu_base = {"value": round(r["mrays_s"], 4), "unit": METRIC, "cores": r["threads"], "kind": r["kind"],
                     "sample": r["sample"], "build_mtris_s": round(r["build_mtris_s"], 3)}
 

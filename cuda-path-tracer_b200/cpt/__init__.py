@@ -84,7 +84,7 @@ class RenderParams(ctypes.Structure):
                 ("frame0", ctypes.c_uint32), ("bounces", ctypes.c_uint32), ("indirect_intensity", ctypes.c_float),
                 ("stratified", ctypes.c_uint32), ("seed_lo", ctypes.c_uint32), ("seed_hi", ctypes.c_uint32),
                 ("accum_mode", ctypes.c_uint32), ("ref_grid", ctypes.c_uint32), ("wave_paths", ctypes.c_uint32),
-                ("trace_stats", ctypes.c_uint32), ("ray_sort", ctypes.c_uint32)]
+                ("trace_stats", ctypes.c_uint32), ("ray_sort", ctypes.c_uint32), ("cameras", ctypes.c_uint32)]
 
 
 def _load() -> ctypes.CDLL:
@@ -107,7 +107,7 @@ _PROTOS = {
     "cpt_trace": (_I32, [ctypes.POINTER(Bvh), _P, _U32, _I32, _P, _P, _P]),
     "cpt_accum_bytes": (_SZ, [_U32, _U32, _U32]),
     "cpt_render_scratch_bytes": (_SZ, [ctypes.POINTER(RenderParams)]),
-    "cpt_render": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Scene), ctypes.POINTER(Camera),
+    "cpt_render": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Scene), ctypes.c_void_p,
                           ctypes.POINTER(RenderParams), _P, _P, _SZ, _P, _P, _P]),
     "cpt_resolve": (_I32, [_P, _U32, _U32, _U32, _P, _P]),
     "cpt_tracer_create": (_I32, [ctypes.POINTER(_P), _I32]),
@@ -127,6 +127,7 @@ _PROTOS = {
     "cpt_scene_random": (_U32, [_U32, _U32, _F, _F, _F, _F, _F, _F, _P, _P]),
     "cpt_scene_sphere_hairball": (_U32, [_U32, _U32, _F, _U32, _F, _U32, _F, _F, _F, _F, _P, _P]),
     "cpt_scene_bounds": (None, [_P, _U32, _P]),
+    "cpt_scene_deform": (_I32, [_P, _P, _U32, _F, _F, _F, _P]),
     "cpt_obj_load": (_I32, [ctypes.c_char_p, _F, _P, _F, _P, _P, _U32, ctypes.POINTER(_U32)]),
     "cpt_bvh_heatmap": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Camera), _U32, _U32, _P, _P, _P, _P]),
     "cpt_camera_look_at": (None, [_P, _P, _P, _F, _F, _F, _F, ctypes.POINTER(Camera)]),
@@ -255,9 +256,10 @@ def render_scratch_bytes(params: RenderParams) -> int:
     return int(lib.cpt_render_scratch_bytes(ctypes.byref(params)))
 
 
-def render(bvh: Bvh, scene: Scene, cam: Camera, params: RenderParams, accum: int, scratch: int, scratch_bytes: int,
+def render(bvh: Bvh, scene: Scene, cam, params: RenderParams, accum: int, scratch: int, scratch_bytes: int,
            ray_counts: int = 0, status: int = 0, stream: int = 0) -> None:
-    check(lib.cpt_render(ctypes.byref(bvh), ctypes.byref(scene), ctypes.byref(cam), ctypes.byref(params), accum,
+    """cam: a Camera or a ctypes array of params.cameras Cameras."""
+    check(lib.cpt_render(ctypes.byref(bvh), ctypes.byref(scene), ctypes.addressof(cam), ctypes.byref(params), accum,
                          scratch, scratch_bytes, ray_counts or None, status or None, stream), "cpt_render")
 
 

@@ -97,10 +97,10 @@ class DeviceScene:
 
 def make_params(width, height, spp, frame0=0, bounces=3, intensity=3.0, stratified=True, seed=0,
                 accum_mode=ACCUM_KAHAN, ref_grid=False, wave_paths=0, trace_stats=False,
-                ray_sort=False) -> RenderParams:
+                ray_sort=False, cameras=1) -> RenderParams:
     return RenderParams(width, height, spp, frame0, bounces, intensity, int(stratified), seed & 0xFFFFFFFF,
                         (seed >> 32) & 0xFFFFFFFF, accum_mode, int(ref_grid), wave_paths, int(trace_stats),
-                        int(ray_sort))
+                        int(ray_sort), cameras)
 
 
 class DeviceRenderer:
@@ -108,7 +108,9 @@ class DeviceRenderer:
 
     def __init__(self, params: RenderParams, device=None):
         self.params = params
-        self.accum = dev_bytes(accum_bytes(params.width, params.height, params.accum_mode), device)
+        self.ncam = max(1, params.cameras)
+        self.accum_stride = accum_bytes(params.width, params.height, params.accum_mode)
+        self.accum = dev_bytes(self.accum_stride * self.ncam, device)
         self.accum.zero_()
         self.scratch_bytes = render_scratch_bytes(params)
         if not self.scratch_bytes:
@@ -123,8 +125,9 @@ class DeviceRenderer:
         self.counts.zero_()
         self.status.zero_()
 
-    def render(self, lbvh: DeviceLbvh, scene: DeviceScene, cam: Camera, spp: int | None = None,
+    def render(self, lbvh: DeviceLbvh, scene: DeviceScene, cam, spp: int | None = None,
                frame0: int | None = None, trace_stats: bool | None = None) -> None:
+        """cam: one Camera, or a sequence of params.cameras Cameras."""
         p = RenderParams.from_buffer_copy(self.params)
         if spp is not None:
             p.spp = spp
@@ -132,12 +135,19 @@ class DeviceRenderer:
             p.frame0 = frame0
         if trace_stats is not None:
             p.trace_stats = int(trace_stats)
-        render(lbvh.bvh, scene.scene, cam, p, self.accum.data_ptr(), self.scratch.data_ptr(), self.scratch_bytes,
+        if isinstance(cam, Camera):
+            cams = (Camera * 1)(cam)
+        else:
+            cams = (Camera * len(cam))(*cam)
+        if len(cams) != self.ncam:
+            raise ValueError(f"{len(cams)} cameras given, params.cameras = {self.ncam}")
+        render(lbvh.bvh, scene.scene, cams, p, self.accum.data_ptr(), self.scratch.data_ptr(), self.scratch_bytes,
                self.counts.data_ptr(), self.status.data_ptr(), stream_handle())
 
-    def resolve(self) -> torch.Tensor:
+    def resolve(self, camera: int = 0) -> torch.Tensor:
         p = self.params
-        resolve(self.accum.data_ptr(), p.width, p.height, p.accum_mode, self.image.data_ptr(), stream_handle())
+        resolve(self.accum.data_ptr() + camera * self.accum_stride, p.width, p.height, p.accum_mode,
+                self.image.data_ptr(), stream_handle())
         return self.image
 
     def check_status(self) -> None:

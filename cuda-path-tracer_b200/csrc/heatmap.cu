@@ -78,3 +78,38 @@ extern "C" int cpt_bvh_heatmap(const cpt_bvh* bvh, const cpt_camera* camera, uin
     CPT_LAUNCH_CHECK();
     return CPT_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Per-frame deformation of a synthetic mesh (the deforming-mesh benchmark): every
+// vertex moves along its direction from the origin, v_a += amp * sin(omega * v_a +
+// phase) * n_a, n = v / |v|. Shared vertices of the soup move identically.
+// ---------------------------------------------------------------------------
+namespace cpt {
+__global__ void __launch_bounds__(256) k_deform(const float* __restrict__ rest, float* __restrict__ out, uint32_t n,
+                                                float amp, float omega, float phase)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* s = rest + 10ull * i;
+    float* d = out + 10ull * i;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const float x = s[3 * v], y = s[3 * v + 1], z = s[3 * v + 2];
+        const float inv = rsqrtf(fmaxf(x * x + y * y + z * z, 1e-30f));
+        d[3 * v] = x + amp * __sinf(omega * x + phase) * x * inv;
+        d[3 * v + 1] = y + amp * __sinf(omega * y + phase) * y * inv;
+        d[3 * v + 2] = z + amp * __sinf(omega * z + phase) * z * inv;
+    }
+    d[9] = s[9];
+}
+}  // namespace cpt
+
+extern "C" int cpt_scene_deform(const cpt_triangle* rest, cpt_triangle* out, uint32_t n, float amplitude, float omega,
+                                float phase, cudaStream_t stream)
+{
+    if (!rest || !out || n == 0) return CPT_ERR_INVALID_ARGUMENT;
+    k_deform<<<(n + 255) / 256, 256, 0, stream>>>(reinterpret_cast<const float*>(rest), reinterpret_cast<float*>(out), n,
+                                                   amplitude, omega, phase);
+    CPT_LAUNCH_CHECK();
+    return CPT_OK;
+}

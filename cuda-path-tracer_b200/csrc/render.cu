@@ -33,10 +33,13 @@ constexpr int kGenBlock = 256;
 constexpr int kMaxDepth = 62;  // bounces + 1 queues; reference GUI allows 5 bounces (PathTracingSettings.h:27)
 constexpr uint32_t kDefaultWavePaths = 1u << 25;
 
+// A wave holds whole "image-samples": image-sample is = sample * ncam + camera, so
+// one wave can carry one sample of several cameras (or several samples of one).
 struct Wave {
     uint32_t width, height, pixels;
-    uint32_t s0;          // first sample of this wave (relative to params.frame0)
-    uint32_t spw;         // samples in this wave
+    uint32_t s0;          // first image-sample of this wave
+    uint32_t spw;         // image-samples in this wave
+    uint32_t ncam;        // cameras rendered by the call
     uint32_t frame0;
     uint32_t bounces;
     float intensity;
@@ -52,6 +55,11 @@ struct Camera {
     float m[16];
     float jx, jy;
     uint32_t jitter;
+};
+
+constexpr uint32_t kMaxCameras = 16;
+struct Cameras {
+    Camera c[kMaxCameras];
 };
 
 // Slot -> pixel: 8-row bands, column-major inside a band.
@@ -107,7 +115,7 @@ __device__ __forceinline__ void corner_dirs(const Camera& cam, uint32_t k0, uint
     }
 }
 
-__global__ void __launch_bounds__(kGenBlock) k_generate(Wave wv, Camera cam, float4* __restrict__ queue,
+__global__ void __launch_bounds__(kGenBlock) k_generate(Wave wv, Cameras cams, float4* __restrict__ queue,
                                                         uint32_t* __restrict__ counts, float4* __restrict__ state)
 {
     const uint32_t total = wv.spw * wv.pixels;
@@ -119,8 +127,10 @@ __global__ void __launch_bounds__(kGenBlock) k_generate(Wave wv, Camera cam, flo
         state[2 * (size_t)pid] = make_float4(0.f, 0.f, 0.f, 0.f);
         const uint32_t q = warp_append(&counts[0], live);
         if (!live) continue;
+        const uint32_t is = wv.s0 + sl;
+        const Camera& cam = cams.c[is % wv.ncam];
         f3 c[4];
-        corner_dirs(cam, wv.k0, wv.k1, wv.frame0 + wv.s0 + sl, c);
+        corner_dirs(cam, wv.k0, wv.k1, wv.frame0 + is / wv.ncam, c);
         // raytrace_kernel (cuda_path_tracer.cu:404-407): bilerp with (x/W, y/H), not normalised.
         float tx = __fdiv_rn(__uint2float_rn(x), __uint2float_rn(wv.width));
         float ty = __fdiv_rn(__uint2float_rn(y), __uint2float_rn(wv.height));
@@ -332,9 +342,10 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(ShadeScene sc, Wave wv, u
                     const uint32_t sl = pid / wv.pixels, slot = pid - sl * wv.pixels;
                     uint32_t x, y;
                     slot_to_pixel(slot, wv.width, wv.height, x, y);
-                    const uint32_t frame = wv.frame0 + wv.s0 + sl;
+                    const uint32_t is = wv.s0 + sl;
+                    const uint32_t frame = wv.frame0 + is / wv.ncam;
                     const f3 no = add(hp, muls(normal, 1e-5f));
-                    uint4 r = philox4x32_10(make_uint4(y * wv.width + x, frame, depth, 0u), wv.k0, wv.k1);
+                    uint4 r = philox4x32_10(make_uint4(y * wv.width + x, frame, depth, is % wv.ncam), wv.k0, wv.k1);
                     float rx = u01(r.x), ry = u01(r.y);
                     if (wv.stratified && depth == 0) {
                         uint32_t pos = frame % 64u;
@@ -375,20 +386,25 @@ __global__ void k_wave_counts(const uint32_t* __restrict__ counts, uint32_t dept
     for (uint32_t b = 0; b < depth_count && b < 64; ++b) atomicAdd(ray_counts + 8 + b, (unsigned long long)counts[b]);
 }
 
-// Adds the wave's samples to the accumulator, per pixel in sample order.
+// Adds the wave's samples to the accumulators (camera blockIdx.y, at accum +
+// camera * accum_stride bytes), per pixel in sample order.
 __global__ void __launch_bounds__(256) k_accumulate(Wave wv, uint32_t mode, const float4* __restrict__ state,
-                                                    void* __restrict__ accum)
+                                                    void* __restrict__ accum_base, size_t accum_stride)
 {
     const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x;
     if (px >= wv.pixels) return;
     const uint32_t x = px % wv.width, y = px / wv.width;
     if (x >= wv.ref_w || y >= wv.ref_h) return;
     const uint32_t slot = pixel_to_slot(x, y, wv.width, wv.height);
+    const uint32_t cam = blockIdx.y;
+    void* accum = static_cast<char*>(accum_base) + accum_stride * cam;
+    // this camera's first image-sample in the wave, then every ncam-th
+    const uint32_t first = (cam + wv.ncam - wv.s0 % wv.ncam) % wv.ncam;
     if (mode == CPT_ACCUM_KAHAN) {
         float4* sum = static_cast<float4*>(accum);
         float4* comp = sum + wv.pixels;
         float4 s = sum[px], c = comp[px];
-        for (uint32_t sl = 0; sl < wv.spw; ++sl) {
+        for (uint32_t sl = first; sl < wv.spw; sl += wv.ncam) {
             const float4 r = state[2 * ((size_t)sl * wv.pixels + slot)];
             float yx = __fsub_rn(r.x, c.x), yy = __fsub_rn(r.y, c.y), yz = __fsub_rn(r.z, c.z);
             float tx = __fadd_rn(s.x, yx), ty = __fadd_rn(s.y, yy), tz = __fadd_rn(s.z, yz);
@@ -405,9 +421,9 @@ __global__ void __launch_bounds__(256) k_accumulate(Wave wv, uint32_t mode, cons
         float4* img = static_cast<float4*>(accum);
         float4 p = img[px];
         f3 prev = mk3(p.x, p.y, p.z);
-        for (uint32_t sl = 0; sl < wv.spw; ++sl) {
+        for (uint32_t sl = first; sl < wv.spw; sl += wv.ncam) {
             const float4 r = state[2 * ((size_t)sl * wv.pixels + slot)];
-            const float f = __uint2float_rn(wv.frame0 + wv.s0 + sl);
+            const float f = __uint2float_rn(wv.frame0 + (wv.s0 + sl) / wv.ncam);
             const float tt = __fdiv_rn(f, __fadd_rn(f, 1.0f));
             prev = mix3(mk3(r.x, r.y, r.z), prev, tt);
         }
@@ -415,7 +431,7 @@ __global__ void __launch_bounds__(256) k_accumulate(Wave wv, uint32_t mode, cons
     } else {
         double4* sum = static_cast<double4*>(accum);
         double4 s = sum[px];
-        for (uint32_t sl = 0; sl < wv.spw; ++sl) {
+        for (uint32_t sl = first; sl < wv.spw; sl += wv.ncam) {
             const float4 r = state[2 * ((size_t)sl * wv.pixels + slot)];
             s.x += (double)r.x; s.y += (double)r.y; s.z += (double)r.z; s.w += 1.0;
         }
@@ -457,13 +473,17 @@ struct RenderScratch {
     size_t sort_zero_words;
 };
 
+inline uint32_t camera_count(const cpt_render_params* p) { return p->cameras ? p->cameras : 1u; }
+
+// Image-samples (sample x camera) per wave.
 inline uint32_t wave_samples(const cpt_render_params* p)
 {
     const uint64_t pixels = (uint64_t)p->width * p->height;
     const uint64_t want = p->wave_paths ? p->wave_paths : kDefaultWavePaths;
+    const uint64_t total = (uint64_t)p->spp * camera_count(p);
     uint64_t spw = want / pixels;
     if (spw < 1) spw = 1;
-    if (spw > p->spp) spw = p->spp;
+    if (spw > total) spw = total;
     return (uint32_t)spw;
 }
 
@@ -548,6 +568,7 @@ bool params_ok(const cpt_render_params* p)
     if ((uint64_t)p->width * p->height > (1ull << 31)) return false;
     if (p->bounces + 1 > (uint32_t)kMaxDepth) return false;
     if (p->accum_mode > CPT_ACCUM_F64) return false;
+    if (camera_count(p) > kMaxCameras) return false;
     return (uint64_t)p->width * p->height * wave_samples(p) < (1ull << 31);
 }
 
@@ -555,7 +576,7 @@ bool params_ok(const cpt_render_params* p)
 
 using namespace cpt;
 
-extern "C" size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode)
+extern "C" size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode)  // one camera
 {
     const size_t px = (size_t)width * height;
     if (accum_mode == CPT_ACCUM_KAHAN) return px * 2 * sizeof(float4);
@@ -584,16 +605,23 @@ extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_
     render_layout(params, scratch, &rs);
     uint32_t* st = status ? status : bvh->status;
 
-    Camera cam;
-    for (int a = 0; a < 3; ++a) cam.eye[a] = camera->eye[a];
-    for (int c = 0; c < 4; ++c)
-        for (int a = 0; a < 3; ++a) cam.dirs[c][a] = camera->dirs[c][a];
-    for (int k = 0; k < 16; ++k) cam.m[k] = camera->inv_view_proj[k];
-    cam.jx = camera->jitter_x;
-    cam.jy = camera->jitter_y;
-    cam.jitter = camera->jitter;
+    const uint32_t ncam = camera_count(params);
+    Cameras cams;
+    for (uint32_t i = 0; i < ncam; ++i) {
+        Camera& cam = cams.c[i];
+        const cpt_camera& src = camera[i];
+        for (int a = 0; a < 3; ++a) cam.eye[a] = src.eye[a];
+        for (int c = 0; c < 4; ++c)
+            for (int a = 0; a < 3; ++a) cam.dirs[c][a] = src.dirs[c][a];
+        for (int k = 0; k < 16; ++k) cam.m[k] = src.inv_view_proj[k];
+        cam.jx = src.jitter_x;
+        cam.jy = src.jitter_y;
+        cam.jitter = src.jitter;
+    }
+    const size_t accum_stride = cpt_accum_bytes(params->width, params->height, params->accum_mode);
 
     Wave wv;
+    wv.ncam = ncam;
     wv.width = params->width;
     wv.height = params->height;
     wv.pixels = params->width * params->height;
@@ -617,15 +645,16 @@ extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_
 
     const int sms = sm_count();
     const uint32_t spw_max = wave_samples(params);
-    for (uint32_t s0 = 0; s0 < params->spp; s0 += spw_max) {
+    const uint32_t total = params->spp * ncam;
+    for (uint32_t s0 = 0; s0 < total; s0 += spw_max) {
         wv.s0 = s0;
-        wv.spw = std::min(spw_max, params->spp - s0);
+        wv.spw = std::min(spw_max, total - s0);
         const uint32_t paths = wv.spw * wv.pixels;
         CPT_CUDA_TRY(cudaMemsetAsync(rs.counts, 0, sizeof(uint32_t) * 2 * (kMaxDepth + 2), stream));
         {
             CPT_PROF(K_GENERATE, stream);
             k_generate<<<(int)std::min<uint32_t>((paths + kGenBlock - 1) / kGenBlock, (uint32_t)sms * 16), kGenBlock, 0,
-                         stream>>>(wv, cam, rs.queue[0], rs.counts, rs.state);
+                         stream>>>(wv, cams, rs.queue[0], rs.counts, rs.state);
         }
         CPT_LAUNCH_CHECK();
         static int ext_occ = 0;
@@ -676,7 +705,8 @@ extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_
         }
         {
             CPT_PROF(K_ACCUMULATE, stream);
-            k_accumulate<<<(wv.pixels + 255) / 256, 256, 0, stream>>>(wv, params->accum_mode, rs.state, accum);
+            const dim3 grid((wv.pixels + 255) / 256, ncam);
+            k_accumulate<<<grid, 256, 0, stream>>>(wv, params->accum_mode, rs.state, accum, accum_stride);
         }
         CPT_LAUNCH_CHECK();
     }

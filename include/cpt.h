@@ -171,9 +171,12 @@ typedef struct cpt_render_params {
     uint32_t trace_stats;      /* 1: count node fetches / triangle tests of extension rays (slower) */
     uint32_t ray_sort;         /* 1: sort each bounce queue by direction octant + origin Morton code
                                 *    before tracing it (coherence; results are unchanged) */
+    uint32_t cameras;          /* cameras rendered in one call (0 or 1: one; at most 16): `camera` points to
+                                * that many cpt_camera, `accum` to that many consecutive accumulators of
+                                * cpt_accum_bytes() each; camera c draws from the Philox counter word 3 = c */
 } cpt_render_params;
 
-size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode);
+size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode); /* per camera */
 size_t cpt_render_scratch_bytes(const cpt_render_params* params);
 
 /* Renders params->spp samples into accum. Replaces CUDAPathTracer::raytrace
@@ -250,6 +253,10 @@ uint32_t cpt_scene_sphere_hairball(uint32_t nu, uint32_t nv, float amp, uint32_t
  * Returns CPT_ERR_SCRATCH_TOO_SMALL when capacity is below the count. Host memory. */
 int cpt_obj_load(const char* path, float scale, const float* translate, float default_grey, cpt_triangle* tris,
                  cpt_triangle_info* infos, uint32_t capacity, uint32_t* n_out);
+/* Deforming-mesh workload (device memory): out = rest with every vertex moved
+ * along its direction from the origin by amplitude * sin(omega * coord + phase). */
+int cpt_scene_deform(const cpt_triangle* rest, cpt_triangle* out, uint32_t n, float amplitude, float omega,
+                     float phase, cudaStream_t stream);
 /* Enclosing box (min, max) of a host triangle soup, as the reference's caller builds it. */
 void cpt_scene_bounds(const cpt_triangle* tris, uint32_t n, float out[6]);
 /* Camera corner directions for eye/target/up, vertical fov (degrees), aspect,

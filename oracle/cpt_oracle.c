@@ -408,6 +408,7 @@ typedef struct {
     float intensity;
     int stratified;
     uint32_t k0, k1;
+    uint32_t camera;  /* counter word 3 of the bounce stream */
 } oscene;
 
 typedef struct { uint64_t primary, extension, shadow; } ocount;
@@ -486,7 +487,7 @@ static v3 path_radiance(const oscene* sc, v3 o, v3 d, uint32_t pixel, uint32_t f
     for (uint32_t i = 0; i < sc->bounces; ++i) {
         v3 ro = add(hit, muls(normal, 1e-5f));
         float u0, u1;
-        cpt_rng_bounce_uniforms(sc->k0, sc->k1, pixel, frame, i, &u0, &u1);
+        cpt_rng_bounce_uniforms(sc->k0, sc->k1, pixel, frame, i, sc->camera, &u0, &u1);
         float rx = u0, ry = u1;
         if (sc->stratified && i == 0) {
             uint32_t pos = frame % 64u;
@@ -568,14 +569,16 @@ void orc_corner_dirs(const ocam* cam, uint32_t k0, uint32_t k1, uint32_t sample,
 
 /* Renders samples frame0 .. frame0+spp-1 of rows [row0, row1) and writes each
  * sample's radiance (3 floats) to radiance[(s * rows + (y - row0)) * width + x].
+ * camera: the camera index of a multi-camera render (random-stream word 3).
  * Pixels are indexed p = y*width + x for the random streams. counts (nullable):
  * primary, extension, shadow rays. */
 void orc_render(const otri* sorted, const uint32_t* children, const obox* boxes, uint32_t n, const oinfo* infos,
                 const olight* lights, uint32_t light_count, uint32_t width, uint32_t height, uint32_t row0,
                 uint32_t row1, uint32_t spp, uint32_t frame0, uint32_t bounces, float intensity, int stratified,
-                uint32_t k0, uint32_t k1, const ocam* cam, float* radiance, uint64_t* counts)
+                uint32_t k0, uint32_t k1, const ocam* cam, uint32_t camera, float* radiance, uint64_t* counts)
 {
-    oscene sc = {{sorted, children, boxes, n}, infos, lights, light_count, bounces, intensity, stratified, k0, k1};
+    oscene sc = {{sorted, children, boxes, n}, infos, lights, light_count, bounces, intensity, stratified, k0, k1,
+                 camera};
     uint32_t rows = row1 - row0;
     uint64_t tp = 0, te = 0, ts = 0;
     (void)height;
@@ -711,7 +714,7 @@ static d3 path_radiance_d(const oscene* sc, d3 o, d3 d, uint32_t pixel, uint32_t
     for (uint32_t i = 0; i < sc->bounces; ++i) {
         d3 ro = dadd(hit, dmuls(normal, 1e-5));
         float u0, u1;
-        cpt_rng_bounce_uniforms(sc->k0, sc->k1, pixel, frame, i, &u0, &u1);
+        cpt_rng_bounce_uniforms(sc->k0, sc->k1, pixel, frame, i, sc->camera, &u0, &u1);
         double rx = u0, ry = u1;
         if (sc->stratified && i == 0) {
             uint32_t pos = frame % 64u;
@@ -758,7 +761,8 @@ void orc_render_f64(const otri* sorted, const uint32_t* children, const obox* bo
                     uint32_t spp, uint32_t frame0, uint32_t bounces, float intensity, int stratified, uint32_t k0,
                     uint32_t k1, const ocam* cam, double* mean_out)
 {
-    oscene sc = {{sorted, children, boxes, n}, infos, lights, light_count, bounces, intensity, stratified, k0, k1};
+    oscene sc = {{sorted, children, boxes, n}, infos, lights, light_count, bounces, intensity, stratified, k0, k1,
+                 0u};
     memset(mean_out, 0, sizeof(double) * 3 * (size_t)width * height);
     for (uint32_t s = 0; s < spp; ++s) {
         float dirs[4][3];

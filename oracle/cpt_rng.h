@@ -9,7 +9,8 @@
  * this oracle draw identical numbers for the same (pixel, sample, bounce).
  *
  * Stream layout (identical in the product's device code):
- *   bounce i of pixel p, global sample f : counter (p, f, i, 0)     -> words 0,1
+ *   bounce i of pixel p, global sample f : counter (p, f, i, c)     -> words 0,1
+ *     (c = camera index of a multi-camera render, 0 otherwise)
  *   camera jitter of global sample f     : counter (~0u, f, 0, 1)   -> words 0,1
  *   uniform from a word w                : (w >> 8) * 2^-24, in [0, 1)
  *
@@ -53,9 +54,9 @@ static inline void cpt_philox4x32_10(const uint32_t ctr_in[4], uint32_t k0, uint
 static inline float cpt_u01(uint32_t w) { return (float)(w >> 8) * (1.0f / 16777216.0f); }
 
 static inline void cpt_rng_bounce_uniforms(uint32_t k0, uint32_t k1, uint32_t pixel, uint32_t sample,
-                                           uint32_t bounce, float* u0, float* u1)
+                                           uint32_t bounce, uint32_t camera, float* u0, float* u1)
 {
-    uint32_t ctr[4] = {pixel, sample, bounce, 0u}, o[4];
+    uint32_t ctr[4] = {pixel, sample, bounce, camera}, o[4];
     cpt_philox4x32_10(ctr, k0, k1, o);
     *u0 = cpt_u01(o[0]);
     *u1 = cpt_u01(o[1]);

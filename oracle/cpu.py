@@ -47,7 +47,7 @@ def oracle_lib() -> ctypes.CDLL:
         L.orc_build.argtypes = [P, U, P, I, P, P, P, P, P, P]
         L.orc_build.restype = I
         L.orc_trace.argtypes = [P, P, P, U, P, U, I, P, P, P, P]
-        L.orc_render.argtypes = [P, P, P, U, P, P, U, U, U, U, U, U, U, U, F, I, U, U, ctypes.POINTER(OCam), P, P]
+        L.orc_render.argtypes = [P, P, P, U, P, P, U, U, U, U, U, U, U, U, F, I, U, U, ctypes.POINTER(OCam), U, P, P]
         L.orc_render_f64.argtypes = [P, P, P, U, P, P, U, U, U, U, U, U, F, I, U, U, ctypes.POINTER(OCam), P]
         L.orc_philox.argtypes = [P, U, U, P]
         L.orc_sincos_turns.argtypes = [P, U, P, P]
@@ -155,7 +155,7 @@ def ocam_from(eye, dirs, inv_view_proj=None, jitter=0, jitter_x=0.0, jitter_y=0.
 
 
 def render(b: BuildResult, infos: np.ndarray, lights, width: int, height: int, spp: int, frame0: int, bounces: int,
-           intensity: float, stratified: bool, seed: int, cam: OCam, rows=None):
+           intensity: float, stratified: bool, seed: int, cam: OCam, rows=None, camera_index: int = 0):
     """Per-sample radiance (spp, rows, width, 3) float32 and ray counts (3,)."""
     r0, r1 = (0, height) if rows is None else rows
     rad = np.zeros((spp, r1 - r0, width, 3), np.float32)
@@ -163,8 +163,8 @@ def render(b: BuildResult, infos: np.ndarray, lights, width: int, height: int, s
     nl = 0 if lights is None else len(lights)
     oracle_lib().orc_render(_p(b.tris), _p(b.children), _p(b.node_boxes), len(b.tris), _p(infos),
                             _p(lights) if nl else None, nl, width, height, r0, r1, spp, frame0, bounces, intensity,
-                            int(stratified), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, ctypes.byref(cam), _p(rad),
-                            _p(counts))
+                            int(stratified), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, ctypes.byref(cam),
+                            camera_index, _p(rad), _p(counts))
     return rad, counts
 
 

@@ -202,7 +202,7 @@ glm::vec3 path_trace(const RefShadeCtx& c, const CUDA::Ray& primary, uint32_t pi
     for (uint32_t i = 0; i < c.bounces; ++i) {
         cur.origin = hitPos + normal * CUDA_EPSILON5;
         float u0, u1;
-        cpt_rng_bounce_uniforms(key0, key1, pixel, frame, i, &u0, &u1);
+        cpt_rng_bounce_uniforms(key0, key1, pixel, frame, i, 0u, &u0, &u1);
         glm::vec2 rnd(u0, u1);
         if (c.stratified && i == 0) {
             const int extent = 8;

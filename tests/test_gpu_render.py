@@ -132,6 +132,26 @@ def test_coherence_sort_does_not_change_the_image(cuda):
     assert gs[..., :3].tobytes() == s.tobytes()
 
 
+def test_several_cameras_in_one_call(cuda):
+    tris, infos, _, _ = scene()
+    cams = [cpt.camera_look_at(eye, (0.5, 0.5, 0.5), aspect=W / H)
+            for eye in ((0.5, 0.5, -1.2), (-0.8, 0.7, 0.4), (1.9, 0.3, 0.6))]
+    lb = DeviceLbvh(len(tris), 30)
+    lb.build(to_device(tris), check_root=True)
+    r = DeviceRenderer(make_params(W, H, 2, 3, 3, 3.0, True, 21, cpt.ACCUM_KAHAN, cameras=3, wave_paths=2 * W * H))
+    r.render(lb, DeviceScene(infos), cams)
+    torch.cuda.synchronize()
+    r.check_status()
+    acc = r.accum.cpu().numpy().view(np.float32).reshape(3, 2, H, W, 4)
+    b = cpu.build(tris, 30)
+    for c, cam in enumerate(cams):
+        rad, _ = cpu.render(b, infos, None, W, H, 2, 3, 3, 3.0, True, 21, cpu.ocam_from(cam.eye, cam.as_array()[3:]),
+                            camera_index=c)
+        s, _, n = cpu.accumulate_kahan(rad)
+        assert acc[c, 0, ..., :3].tobytes() == s.tobytes()
+        assert np.all(acc[c, 0, ..., 3] == n)
+
+
 def test_directional_lights_shadow_rays(cuda):
     tris, infos, _, cam = scene()
     lights = dir_lights()
