@@ -79,12 +79,21 @@ class Camera(ctypes.Structure):
         return np.array(list(self.eye) + [self.dirs[c][a] for c in range(4) for a in range(3)], np.float32)
 
 
+class View(ctypes.Structure):
+    _fields_ = [("bvh", ctypes.POINTER(Bvh)), ("scene", ctypes.POINTER(Scene)), ("camera", Camera),
+                ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("accum", ctypes.c_void_p)]
+
+
+MAX_VIEWS = 64
+
+
 class RenderParams(ctypes.Structure):
     _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("spp", ctypes.c_uint32),
                 ("frame0", ctypes.c_uint32), ("bounces", ctypes.c_uint32), ("indirect_intensity", ctypes.c_float),
                 ("stratified", ctypes.c_uint32), ("seed_lo", ctypes.c_uint32), ("seed_hi", ctypes.c_uint32),
                 ("accum_mode", ctypes.c_uint32), ("ref_grid", ctypes.c_uint32), ("wave_paths", ctypes.c_uint32),
-                ("trace_stats", ctypes.c_uint32), ("ray_sort", ctypes.c_uint32), ("cameras", ctypes.c_uint32)]
+                ("trace_stats", ctypes.c_uint32), ("ray_sort", ctypes.c_uint32), ("cameras", ctypes.c_uint32),
+                ("frame_counter", ctypes.c_void_p)]
 
 
 def _load() -> ctypes.CDLL:
@@ -110,6 +119,8 @@ _PROTOS = {
     "cpt_render": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Scene), ctypes.c_void_p,
                           ctypes.POINTER(RenderParams), _P, _P, _SZ, _P, _P, _P]),
     "cpt_resolve": (_I32, [_P, _U32, _U32, _U32, _P, _P]),
+    "cpt_render_views_scratch_bytes": (_SZ, [_P, _U32, ctypes.POINTER(RenderParams)]),
+    "cpt_render_views": (_I32, [_P, _U32, ctypes.POINTER(RenderParams), _P, _SZ, _P, _P, _P]),
     "cpt_tracer_create": (_I32, [ctypes.POINTER(_P), _I32]),
     "cpt_tracer_destroy": (None, [_P]),
     "cpt_tracer_upload": (_I32, [_P, _P, _U32, _P, _U32, _P, _U32, _P]),

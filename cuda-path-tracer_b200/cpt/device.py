@@ -9,7 +9,9 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from . import (ACCUM_KAHAN, BBOX_DTYPE, BUILD_CHECK, TRIANGLE_DTYPE, Bvh, Camera, RenderParams, Scene, accum_bytes,
+import ctypes
+
+from . import (ACCUM_KAHAN, BBOX_DTYPE, BUILD_CHECK, TRIANGLE_DTYPE, Bvh, Camera, RenderParams, Scene, View, accum_bytes,
                bvh_bind, bvh_bytes, check, lbvh_build, lbvh_scratch_bytes, lib, render, render_scratch_bytes, resolve,
                status_check, trace)
 
@@ -149,6 +151,41 @@ class DeviceRenderer:
         resolve(self.accum.data_ptr() + camera * self.accum_stride, p.width, p.height, p.accum_mode,
                 self.image.data_ptr(), stream_handle())
         return self.image
+
+    def check_status(self) -> None:
+        status_check(self.status.data_ptr(), stream_handle())
+
+
+class BatchRenderer:
+    """Several views — (BVH, shading scene, camera, resolution) — rendered in the
+    same wavefront launches; one accumulator per view."""
+
+    def __init__(self, views, params: RenderParams, device=None):
+        """views: list of (DeviceLbvh, DeviceScene, Camera, width, height)."""
+        self.params = params
+        self._keep = views
+        n = len(views)
+        self.views = (View * n)()
+        self.accums = []
+        for i, (lb, sc, cam, w, h) in enumerate(views):
+            acc = dev_bytes(accum_bytes(w, h, params.accum_mode), device)
+            acc.zero_()
+            self.accums.append(acc)
+            self.views[i] = View(ctypes.pointer(lb.bvh), ctypes.pointer(sc.scene), cam, w, h, acc.data_ptr())
+        self.scratch_bytes = int(lib.cpt_render_views_scratch_bytes(self.views, n, ctypes.byref(params)))
+        if not self.scratch_bytes:
+            raise ValueError("render parameters rejected")
+        self.scratch = dev_bytes(self.scratch_bytes, device)
+        self.counts = torch.zeros(72, dtype=torch.int64, device=device or "cuda")
+        self.status = torch.zeros(4, dtype=torch.int32, device=device or "cuda")
+
+    def render(self, frame0: int | None = None, stream: int | None = None) -> None:
+        p = RenderParams.from_buffer_copy(self.params)
+        if frame0 is not None:
+            p.frame0 = frame0
+        check(lib.cpt_render_views(self.views, len(self.accums), ctypes.byref(p), self.scratch.data_ptr(),
+                                   self.scratch_bytes, self.counts.data_ptr(), self.status.data_ptr(),
+                                   stream_handle() if stream is None else stream), "cpt_render_views")
 
     def check_status(self) -> None:
         status_check(self.status.data_ptr(), stream_handle())

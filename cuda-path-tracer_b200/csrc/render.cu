@@ -1,24 +1,29 @@
-// Wavefront path tracer for sm_100a (cpt_render, cpt_resolve).
+// Wavefront path tracer for sm_100a (cpt_render, cpt_render_views, cpt_resolve).
 //
 // The reference traces each pixel's whole path in one megakernel thread
 // (raytrace_kernel, cuda_path_tracer.cu:385-421, with blinnPhongShadingPathTrace
-// :245-333). Here a wave of paths — whole samples of the image, sample-major —
-// advances one vertex at a time:
+// :245-333). Here a wave of paths advances one vertex at a time:
 //
-//   k_generate    primary rays for every (sample, pixel) of the wave  -> queue 0
-//   k_extend      closest hit for every ray in queue b                 -> hits
+//   k_generate    primary rays for every (view, sample, pixel) of the wave -> queue 0
+//   k_extend      closest hit for every ray in queue b                      -> hits
 //   k_shade       shading of vertex b, shadow rays inline (any-hit),
-//                 next bounce direction                                 -> queue b+1
-//   k_accumulate  per pixel, the wave's samples in sample order         -> accumulator
+//                 next bounce direction                                      -> queue b+1
+//   k_accumulate  per pixel, the wave's samples in sample order              -> accumulators
 //
-// Each path's radiance is the reference's estimator evaluated in the same
-// operation order (round-to-nearest intrinsics), with the random numbers drawn
-// from the counter-based Philox stream by (pixel, sample, bounce), so the result
-// of every path is independent of queue order and wave size. The pixel order of
-// a sample walks 8-row bands column by column so that a warp's primary rays
-// cover a 4x8 pixel patch.
+// A "view" is one image: a BVH, its shading records and lights, a camera, a
+// resolution and an accumulator. One call renders up to CPT_MAX_VIEWS views —
+// several cameras of one scene, or many scenes (the batched workload) — in the
+// same waves: the view table travels as a kernel parameter (so a frame is a fixed
+// sequence of launches that a CUDA graph can capture), every ray carries its view
+// index, and the traversal reads that view's nodes. Each path's radiance is the
+// reference's estimator evaluated in the same operation order (round-to-nearest
+// intrinsics), with random numbers from the counter-based Philox stream by
+// (pixel, sample, bounce, view), so a path's result does not depend on queue order,
+// wave size or which other views share the call. Within a view, a sample walks
+// 8-row bands column by column so that a warp's primary rays cover a 4x8 patch.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <mutex>
 #include "cpt.h"
 #include "cpt_internal.h"
 #include "traverse.cuh"
@@ -33,22 +38,6 @@ constexpr int kGenBlock = 256;
 constexpr int kMaxDepth = 62;  // bounces + 1 queues; reference GUI allows 5 bounces (PathTracingSettings.h:27)
 constexpr uint32_t kDefaultWavePaths = 1u << 25;
 
-// A wave holds whole "image-samples": image-sample is = sample * ncam + camera, so
-// one wave can carry one sample of several cameras (or several samples of one).
-struct Wave {
-    uint32_t width, height, pixels;
-    uint32_t s0;          // first image-sample of this wave
-    uint32_t spw;         // image-samples in this wave
-    uint32_t ncam;        // cameras rendered by the call
-    uint32_t frame0;
-    uint32_t bounces;
-    float intensity;
-    uint32_t stratified;
-    uint32_t k0, k1;
-    uint32_t ref_w, ref_h;  // rendered extent (reference grid truncation)
-    uint32_t light_count;
-};
-
 struct Camera {
     float eye[3];
     float dirs[4][3];
@@ -57,9 +46,35 @@ struct Camera {
     uint32_t jitter;
 };
 
-constexpr uint32_t kMaxCameras = 16;
-struct Cameras {
-    Camera c[kMaxCameras];
+struct View {
+    const float4* nodes;
+    const cpt_triangle* tris;  // Morton-sorted reference records (info_idx of a hit)
+    const cpt_triangle_info* infos;
+    const cpt_dir_light* lights;
+    void* accum;
+    uint32_t info_count, light_count, max_visits;
+    uint32_t width, height, pixels, ref_w, ref_h;
+    uint32_t pixel_base;  // pixels of the views before this one
+    Camera cam;
+};
+
+struct Views {
+    View v[CPT_MAX_VIEWS];
+    uint32_t n;
+    uint32_t total_pixels;
+};
+
+// Per-wave constants. A wave holds image-samples s0 .. s0+spw-1 of every view;
+// paths are laid out view by view: view v owns paths
+// [pixel_base(v) * spw, (pixel_base(v) + pixels(v)) * spw), sample-major inside.
+struct Wave {
+    uint32_t s0, spw;
+    uint32_t frame0;
+    const uint32_t* frame_dev;  // nullable: added to frame0 on the device (CUDA-graph replays)
+    uint32_t bounces;
+    float intensity;
+    uint32_t stratified;
+    uint32_t k0, k1;
 };
 
 // Slot -> pixel: 8-row bands, column-major inside a band.
@@ -112,53 +127,6 @@ __device__ __forceinline__ void corner_dirs(const Camera& cam, uint32_t k0, uint
         f3 ps = mk3(__fdiv_rn(ws[0], ws[3]), __fdiv_rn(ws[1], ws[3]), __fdiv_rn(ws[2], ws[3]));
         f3 pe = mk3(__fdiv_rn(we[0], we[3]), __fdiv_rn(we[1], we[3]), __fdiv_rn(we[2], we[3]));
         out[c] = normalize(sub(pe, ps));
-    }
-}
-
-__global__ void __launch_bounds__(kGenBlock) k_generate(Wave wv, Cameras cams, float4* __restrict__ queue,
-                                                        uint32_t* __restrict__ counts, float4* __restrict__ state)
-{
-    const uint32_t total = wv.spw * wv.pixels;
-    for (uint32_t pid = blockIdx.x * kGenBlock + threadIdx.x; pid < total; pid += gridDim.x * kGenBlock) {
-        const uint32_t sl = pid / wv.pixels, slot = pid - sl * wv.pixels;
-        uint32_t x, y;
-        slot_to_pixel(slot, wv.width, wv.height, x, y);
-        const bool live = x < wv.ref_w && y < wv.ref_h;
-        state[2 * (size_t)pid] = make_float4(0.f, 0.f, 0.f, 0.f);
-        const uint32_t q = warp_append(&counts[0], live);
-        if (!live) continue;
-        const uint32_t is = wv.s0 + sl;
-        const Camera& cam = cams.c[is % wv.ncam];
-        f3 c[4];
-        corner_dirs(cam, wv.k0, wv.k1, wv.frame0 + is / wv.ncam, c);
-        // raytrace_kernel (cuda_path_tracer.cu:404-407): bilerp with (x/W, y/H), not normalised.
-        float tx = __fdiv_rn(__uint2float_rn(x), __uint2float_rn(wv.width));
-        float ty = __fdiv_rn(__uint2float_rn(y), __uint2float_rn(wv.height));
-        f3 d = mix3(mix3(c[0], c[1], tx), mix3(c[3], c[2], tx), ty);
-        queue[2 * (size_t)q] = make_float4(cam.eye[0], cam.eye[1], cam.eye[2], __uint_as_float(pid));
-        queue[2 * (size_t)q + 1] = make_float4(d.x, d.y, d.z, 0.f);
-    }
-}
-
-template <bool kStats>
-__global__ void __launch_bounds__(kExtendBlock) k_extend(const float4* __restrict__ nodes,
-                                                         const float4* __restrict__ queue,
-                                                         const uint32_t* __restrict__ count, float4* __restrict__ hits,
-                                                         uint32_t* __restrict__ pool,
-                                                         unsigned long long* __restrict__ ray_counts,
-                                                         uint32_t* __restrict__ status, uint32_t max_visits,
-                                                         const uint32_t* __restrict__ order)
-{
-    __shared__ uint32_t s_stack[kSmemStack * kExtendBlock];
-    const uint32_t n = *count;
-    bool overflow = false;
-    uint32_t nn = 0, nt = 0;
-    persistent_trace<false, kExtendBlock, kStats, kExtendSteps>(nodes, queue, n, hits, pool, s_stack + threadIdx.x,
-                                                                overflow, nn, nt, max_visits, nullptr, order);
-    if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
-    if (kStats && ray_counts) {
-        warp_count_u64(ray_counts + 3, nn);
-        warp_count_u64(ray_counts + 4, nt);
     }
 }
 
@@ -215,14 +183,88 @@ __global__ void __launch_bounds__(256) k_ray_keys(const float4* __restrict__ que
         if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
 }
 
-struct ShadeScene {
-    const float4* nodes;
-    const cpt_triangle* tris;  // Morton-sorted reference records (info_idx of a hit)
-    const cpt_triangle_info* infos;
-    const cpt_dir_light* lights;
-    uint32_t info_count;
-    uint32_t max_visits;
-};
+// View owning global path p (binary search on the pixel bases).
+__device__ __forceinline__ uint32_t view_of_path(const Views& vs, uint32_t p, uint32_t spw)
+{
+    uint32_t lo = 0, hi = vs.n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (vs.v[mid].pixel_base * spw <= p) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint32_t view_of_pixel(const Views& vs, uint32_t g)
+{
+    uint32_t lo = 0, hi = vs.n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (vs.v[mid].pixel_base <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint32_t wave_frame0(const Wave& wv) { return wv.frame0 + (wv.frame_dev ? *wv.frame_dev : 0u); }
+
+__global__ void __launch_bounds__(kGenBlock) k_generate(Wave wv, Views vs, float4* __restrict__ queue,
+                                                        uint32_t* __restrict__ counts, float4* __restrict__ state)
+{
+    const uint32_t total = wv.spw * vs.total_pixels;
+    const uint32_t frame0 = wave_frame0(wv);
+    for (uint32_t pid = blockIdx.x * kGenBlock + threadIdx.x; pid < total; pid += gridDim.x * kGenBlock) {
+        const uint32_t vi = view_of_path(vs, pid, wv.spw);
+        const View& v = vs.v[vi];
+        const uint32_t local = pid - v.pixel_base * wv.spw;
+        const uint32_t sl = local / v.pixels, slot = local - sl * v.pixels;
+        uint32_t x, y;
+        slot_to_pixel(slot, v.width, v.height, x, y);
+        const bool live = x < v.ref_w && y < v.ref_h;
+        state[2 * (size_t)pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+        const uint32_t q = warp_append(&counts[0], live);
+        if (!live) continue;
+        f3 c[4];
+        corner_dirs(v.cam, wv.k0, wv.k1, frame0 + wv.s0 + sl, c);
+        // raytrace_kernel (cuda_path_tracer.cu:404-407): bilerp with (x/W, y/H), not normalised.
+        const float tx = __fdiv_rn(__uint2float_rn(x), __uint2float_rn(v.width));
+        const float ty = __fdiv_rn(__uint2float_rn(y), __uint2float_rn(v.height));
+        const f3 d = mix3(mix3(c[0], c[1], tx), mix3(c[3], c[2], tx), ty);
+        queue[2 * (size_t)q] = make_float4(v.cam.eye[0], v.cam.eye[1], v.cam.eye[2], __uint_as_float(pid));
+        queue[2 * (size_t)q + 1] = make_float4(d.x, d.y, d.z, __uint_as_float(vi));
+    }
+}
+
+// kOneView: every ray traverses view 0's BVH (a single scene, e.g. several cameras of
+// it); the node array is then a kernel-wide constant instead of a per-ray value.
+template <bool kStats, bool kOneView>
+__global__ void __launch_bounds__(kExtendBlock) k_extend(Views vs, const float4* __restrict__ queue,
+                                                         const uint32_t* __restrict__ count, float4* __restrict__ hits,
+                                                         uint32_t* __restrict__ pool,
+                                                         unsigned long long* __restrict__ ray_counts,
+                                                         uint32_t* __restrict__ status, const uint32_t* __restrict__ order)
+{
+    __shared__ uint32_t s_stack[kSmemStack * kExtendBlock];
+    const uint32_t n = *count;
+    bool overflow = false;
+    uint32_t nn = 0, nt = 0;
+    // each ray's view (direction .w) selects the node array it traverses
+    const float4* nodes0 = vs.v[0].nodes;
+    const uint32_t visits0 = vs.v[0].max_visits;
+    auto view_nodes = [&](uint32_t vi, uint32_t& max_visits) -> const float4* {
+        if (kOneView) {
+            max_visits = visits0;
+            return nodes0;
+        }
+        max_visits = vs.v[vi].max_visits;
+        return vs.v[vi].nodes;
+    };
+    persistent_trace_views<false, kExtendBlock, kStats, kExtendSteps>(view_nodes, queue, n, hits, pool,
+                                                                      s_stack + threadIdx.x, overflow, nn, nt, order);
+    if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
+    if (kStats && ray_counts) {
+        warp_count_u64(ray_counts + 3, nn);
+        warp_count_u64(ray_counts + 4, nt);
+    }
+}
 
 // blinnPhongBRDF (cuda_path_tracer.cu:36-50)
 __device__ __forceinline__ f3 blinn_phong(f3 Id, f3 kd, f3 Is, f3 ks, f3 n, f3 lv, f3 h, float shininess)
@@ -235,19 +277,6 @@ __device__ __forceinline__ f3 blinn_phong(f3 Id, f3 kd, f3 Is, f3 ks, f3 n, f3 l
     return add(diffuse, spec);
 }
 
-// computeL (LightAlgorithms.h:12-20). The reference traces a full closest hit and
-// tests distance < FLT_MAX; the any-hit traversal visits nodes in the same order
-// until its first recorded triangle, so the visibility it returns is the same.
-template <int kBlock>
-__device__ __forceinline__ f3 light_l(const ShadeScene& sc, f3 p, const cpt_dir_light& l, uint32_t* stack, bool& overflow)
-{
-    f3 dir = mk3(l.direction[0], l.direction[1], l.direction[2]);
-    f3 o = sub(p, muls(dir, 1e-3f));
-    Hit h = traverse<true, kBlock>(sc.nodes, o, neg(dir), stack, overflow, sc.max_visits);
-    if (h.t < FLT_MAX) return mk3(0.f, 0.f, 0.f);
-    return muls(mk3(l.color[0], l.color[1], l.color[2]), l.intensity);
-}
-
 // toHemisphere (math_util.h:56-67)
 __device__ __forceinline__ f3 to_hemisphere(f3 v, f3 n)
 {
@@ -257,8 +286,21 @@ __device__ __forceinline__ f3 to_hemisphere(f3 v, f3 n)
     return add(add(muls(x, v.x), muls(y, v.y)), muls(n, v.z));
 }
 
+// computeL (LightAlgorithms.h:12-20). The reference traces a full closest hit and
+// tests distance < FLT_MAX; the any-hit traversal visits nodes in the same order
+// until its first recorded triangle, so the visibility it returns is the same.
+template <int kBlock>
+__device__ __forceinline__ f3 light_l(const View& v, f3 p, const cpt_dir_light& l, uint32_t* stack, bool& overflow)
+{
+    const f3 dir = mk3(l.direction[0], l.direction[1], l.direction[2]);
+    const f3 o = sub(p, muls(dir, 1e-3f));
+    const Hit h = traverse<true, kBlock>(v.nodes, o, neg(dir), stack, overflow, v.max_visits);
+    if (h.t < FLT_MAX) return mk3(0.f, 0.f, 0.f);
+    return muls(mk3(l.color[0], l.color[1], l.color[2]), l.intensity);
+}
+
 template <bool kLights>
-__global__ void __launch_bounds__(kShadeBlock) k_shade(ShadeScene sc, Wave wv, uint32_t depth,
+__global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32_t depth,
                                                        const float4* __restrict__ queue_in,
                                                        const float4* __restrict__ hits,
                                                        const uint32_t* __restrict__ count_in,
@@ -282,18 +324,20 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(ShadeScene sc, Wave wv, u
             const float4 hit4 = hits[i];
             const uint32_t tri = __float_as_uint(hit4.w);
             const uint32_t pid = __float_as_uint(ro.w);
-            const uint32_t info_idx = tri != CPT_INVALID_INDEX ? __ldg(&sc.tris[tri].info_idx) : 0u;
-            bad_info = tri != CPT_INVALID_INDEX && info_idx >= sc.info_count;
+            const uint32_t vi = __float_as_uint(rd4.w);
+            const View& v = vs.v[vi];
+            const uint32_t info_idx = tri != CPT_INVALID_INDEX ? __ldg(&v.tris[tri].info_idx) : 0u;
+            bad_info = tri != CPT_INVALID_INDEX && info_idx >= v.info_count;
             if (tri != CPT_INVALID_INDEX && !bad_info) {
                 const f3 o = mk3(ro.x, ro.y, ro.z), d = mk3(rd4.x, rd4.y, rd4.z);
-                const float t = hit4.x, u = hit4.y, v = hit4.z;
-                const cpt_triangle_info& in = sc.infos[info_idx];
+                const float t = hit4.x, u = hit4.y, w = hit4.z;
+                const cpt_triangle_info& in = v.infos[info_idx];
                 const f3 hp = add(muls(d, t), o);
-                f3 albedo = normalize(bary(ld3(in.vertices[0].color), ld3(in.vertices[1].color), ld3(in.vertices[2].color), u, v));
-                const f3 normal = normalize(bary(ld3(in.vertices[0].normal), ld3(in.vertices[1].normal), ld3(in.vertices[2].normal), u, v));
+                f3 albedo = normalize(bary(ld3(in.vertices[0].color), ld3(in.vertices[1].color), ld3(in.vertices[2].color), u, w));
+                const f3 normal = normalize(bary(ld3(in.vertices[0].normal), ld3(in.vertices[1].normal), ld3(in.vertices[2].normal), u, w));
                 const f3 e = ld3(in.material.emission);
                 const bool emissive = __fadd_rn(__fadd_rn(e.x, e.y), e.z) > 1e-7f;
-                float4 acc4 = state[2 * (size_t)pid], ab4 = state[2 * (size_t)pid + 1];
+                const float4 acc4 = state[2 * (size_t)pid], ab4 = state[2 * (size_t)pid + 1];
                 f3 acc, absorbed;
                 if (depth == 0) {
                     // blinnPhongShadingShadowTrace (cuda_path_tracer.cu:163-220)
@@ -303,12 +347,12 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(ShadeScene sc, Wave wv, u
                     } else {
                         f3 L = mk3(0.f, 0.f, 0.f), color = mk3(0.f, 0.f, 0.f);
                         if (kLights) {
-                            for (uint32_t li = 0; li < wv.light_count; ++li) {
-                                const cpt_dir_light l = sc.lights[li];
-                                L = add(L, light_l<kShadeBlock>(sc, hp, l, stack, overflow));
+                            for (uint32_t li = 0; li < v.light_count; ++li) {
+                                const cpt_dir_light l = v.lights[li];
+                                L = add(L, light_l<kShadeBlock>(v, hp, l, stack, overflow));
                                 ++shadow;
-                                f3 ldir = ld3(l.direction);
-                                f3 half = muls(sub(neg(d), ldir), 0.5f);
+                                const f3 ldir = ld3(l.direction);
+                                const f3 half = muls(sub(neg(d), ldir), 0.5f);
                                 color = add(color, blinn_phong(L, albedo, L, mk3(0.5f, 0.5f, 0.5f), normal, neg(ldir), half,
                                                                in.material.specularity));
                             }
@@ -325,9 +369,9 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(ShadeScene sc, Wave wv, u
                         L = muls(e, gmax(dot(neg(d), normal), 0.0f));
                         albedo = mk3(1.f, 1.f, 1.f);
                     } else if (kLights) {
-                        for (uint32_t li = 0; li < wv.light_count; ++li) {
-                            const cpt_dir_light l = sc.lights[li];
-                            f3 c = light_l<kShadeBlock>(sc, hp, l, stack, overflow);
+                        for (uint32_t li = 0; li < v.light_count; ++li) {
+                            const cpt_dir_light l = v.lights[li];
+                            const f3 c = light_l<kShadeBlock>(v, hp, l, stack, overflow);
                             ++shadow;
                             L = add(L, muls(c, gmax(dot(neg(ld3(l.direction)), normal), 0.0f)));
                         }
@@ -339,27 +383,27 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(ShadeScene sc, Wave wv, u
                 state[2 * (size_t)pid + 1] = make_float4(absorbed.x, absorbed.y, absorbed.z, 0.f);
                 if (depth < wv.bounces) {
                     // next direction (cuda_path_tracer.cu:269-284)
-                    const uint32_t sl = pid / wv.pixels, slot = pid - sl * wv.pixels;
+                    const uint32_t local = pid - v.pixel_base * wv.spw;
+                    const uint32_t sl = local / v.pixels, slot = local - sl * v.pixels;
                     uint32_t x, y;
-                    slot_to_pixel(slot, wv.width, wv.height, x, y);
-                    const uint32_t is = wv.s0 + sl;
-                    const uint32_t frame = wv.frame0 + is / wv.ncam;
+                    slot_to_pixel(slot, v.width, v.height, x, y);
+                    const uint32_t frame = wave_frame0(wv) + wv.s0 + sl;
                     const f3 no = add(hp, muls(normal, 1e-5f));
-                    uint4 r = philox4x32_10(make_uint4(y * wv.width + x, frame, depth, is % wv.ncam), wv.k0, wv.k1);
+                    const uint4 r = philox4x32_10(make_uint4(y * v.width + x, frame, depth, vi), wv.k0, wv.k1);
                     float rx = u01(r.x), ry = u01(r.y);
                     if (wv.stratified && depth == 0) {
-                        uint32_t pos = frame % 64u;
+                        const uint32_t pos = frame % 64u;
                         rx = __fdiv_rn(__fadd_rn((float)(int)(pos % 8u), rx), 8.0f);
                         ry = __fdiv_rn(__fadd_rn((float)(int)(pos / 8u), ry), 8.0f);
                     }
                     float sn, cs;
                     sincos_turns(ry, &sn, &cs);
-                    float rr = __fsqrt_rn(rx);
-                    f3 dl = mk3(__fmul_rn(rr, cs), __fmul_rn(rr, sn), __fsqrt_rn(__fsub_rn(1.0f, rx)));
-                    f3 nd = to_hemisphere(dl, normal);
+                    const float rr = __fsqrt_rn(rx);
+                    const f3 dl = mk3(__fmul_rn(rr, cs), __fmul_rn(rr, sn), __fsqrt_rn(__fsub_rn(1.0f, rx)));
+                    const f3 nd = to_hemisphere(dl, normal);
                     emit = true;
                     nro = make_float4(no.x, no.y, no.z, __uint_as_float(pid));
-                    nrd = make_float4(nd.x, nd.y, nd.z, 0.f);
+                    nrd = make_float4(nd.x, nd.y, nd.z, __uint_as_float(vi));
                 }
             }
         }
@@ -386,28 +430,28 @@ __global__ void k_wave_counts(const uint32_t* __restrict__ counts, uint32_t dept
     for (uint32_t b = 0; b < depth_count && b < 64; ++b) atomicAdd(ray_counts + 8 + b, (unsigned long long)counts[b]);
 }
 
-// Adds the wave's samples to the accumulators (camera blockIdx.y, at accum +
-// camera * accum_stride bytes), per pixel in sample order.
-__global__ void __launch_bounds__(256) k_accumulate(Wave wv, uint32_t mode, const float4* __restrict__ state,
-                                                    void* __restrict__ accum_base, size_t accum_stride)
+__global__ void k_advance(uint32_t* counter, uint32_t by) { *counter += by; }
+
+// Adds the wave's samples to the accumulators, per pixel in sample order; one
+// thread per pixel of every view.
+__global__ void __launch_bounds__(256) k_accumulate(Wave wv, Views vs, uint32_t mode, const float4* __restrict__ state)
 {
-    const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x;
-    if (px >= wv.pixels) return;
-    const uint32_t x = px % wv.width, y = px / wv.width;
-    if (x >= wv.ref_w || y >= wv.ref_h) return;
-    const uint32_t slot = pixel_to_slot(x, y, wv.width, wv.height);
-    const uint32_t cam = blockIdx.y;
-    void* accum = static_cast<char*>(accum_base) + accum_stride * cam;
-    // this camera's first image-sample in the wave, then every ncam-th
-    const uint32_t first = (cam + wv.ncam - wv.s0 % wv.ncam) % wv.ncam;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= vs.total_pixels) return;
+    const View& v = vs.v[view_of_pixel(vs, g)];
+    const uint32_t px = g - v.pixel_base;
+    const uint32_t x = px % v.width, y = px / v.width;
+    if (x >= v.ref_w || y >= v.ref_h) return;
+    const uint32_t slot = pixel_to_slot(x, y, v.width, v.height);
+    const size_t base = (size_t)v.pixel_base * wv.spw + slot;
     if (mode == CPT_ACCUM_KAHAN) {
-        float4* sum = static_cast<float4*>(accum);
-        float4* comp = sum + wv.pixels;
+        float4* sum = static_cast<float4*>(v.accum);
+        float4* comp = sum + v.pixels;
         float4 s = sum[px], c = comp[px];
-        for (uint32_t sl = first; sl < wv.spw; sl += wv.ncam) {
-            const float4 r = state[2 * ((size_t)sl * wv.pixels + slot)];
-            float yx = __fsub_rn(r.x, c.x), yy = __fsub_rn(r.y, c.y), yz = __fsub_rn(r.z, c.z);
-            float tx = __fadd_rn(s.x, yx), ty = __fadd_rn(s.y, yy), tz = __fadd_rn(s.z, yz);
+        for (uint32_t sl = 0; sl < wv.spw; ++sl) {
+            const float4 r = state[2 * (base + (size_t)sl * v.pixels)];
+            const float yx = __fsub_rn(r.x, c.x), yy = __fsub_rn(r.y, c.y), yz = __fsub_rn(r.z, c.z);
+            const float tx = __fadd_rn(s.x, yx), ty = __fadd_rn(s.y, yy), tz = __fadd_rn(s.z, yz);
             c.x = __fsub_rn(__fsub_rn(tx, s.x), yx);
             c.y = __fsub_rn(__fsub_rn(ty, s.y), yy);
             c.z = __fsub_rn(__fsub_rn(tz, s.z), yz);
@@ -418,21 +462,21 @@ __global__ void __launch_bounds__(256) k_accumulate(Wave wv, uint32_t mode, cons
         comp[px] = c;
     } else if (mode == CPT_ACCUM_LERP) {
         // cuda_path_tracer.cu:413-420: new = lerp(hit, prev, f / (f + 1))
-        float4* img = static_cast<float4*>(accum);
-        float4 p = img[px];
+        float4* img = static_cast<float4*>(v.accum);
+        const float4 p = img[px];
         f3 prev = mk3(p.x, p.y, p.z);
-        for (uint32_t sl = first; sl < wv.spw; sl += wv.ncam) {
-            const float4 r = state[2 * ((size_t)sl * wv.pixels + slot)];
-            const float f = __uint2float_rn(wv.frame0 + (wv.s0 + sl) / wv.ncam);
+        for (uint32_t sl = 0; sl < wv.spw; ++sl) {
+            const float4 r = state[2 * (base + (size_t)sl * v.pixels)];
+            const float f = __uint2float_rn(wave_frame0(wv) + wv.s0 + sl);
             const float tt = __fdiv_rn(f, __fadd_rn(f, 1.0f));
             prev = mix3(mk3(r.x, r.y, r.z), prev, tt);
         }
         img[px] = make_float4(prev.x, prev.y, prev.z, 1.0f);
     } else {
-        double4* sum = static_cast<double4*>(accum);
+        double4* sum = static_cast<double4*>(v.accum);
         double4 s = sum[px];
-        for (uint32_t sl = first; sl < wv.spw; sl += wv.ncam) {
-            const float4 r = state[2 * ((size_t)sl * wv.pixels + slot)];
+        for (uint32_t sl = 0; sl < wv.spw; ++sl) {
+            const float4 r = state[2 * (base + (size_t)sl * v.pixels)];
             s.x += (double)r.x; s.y += (double)r.y; s.z += (double)r.z; s.w += 1.0;
         }
         sum[px] = s;
@@ -473,26 +517,21 @@ struct RenderScratch {
     size_t sort_zero_words;
 };
 
-inline uint32_t camera_count(const cpt_render_params* p) { return p->cameras ? p->cameras : 1u; }
-
-// Image-samples (sample x camera) per wave.
-inline uint32_t wave_samples(const cpt_render_params* p)
+// Image-samples per wave for `pixels` pixels over all views.
+inline uint32_t wave_samples(const cpt_render_params* p, uint64_t pixels)
 {
-    const uint64_t pixels = (uint64_t)p->width * p->height;
     const uint64_t want = p->wave_paths ? p->wave_paths : kDefaultWavePaths;
-    const uint64_t total = (uint64_t)p->spp * camera_count(p);
     uint64_t spw = want / pixels;
     if (spw < 1) spw = 1;
-    if (spw > total) spw = total;
+    if (spw > p->spp) spw = p->spp;
     return (uint32_t)spw;
 }
 
-size_t render_layout(const cpt_render_params* p, void* base, RenderScratch* out)
+size_t render_layout(const cpt_render_params* p, uint64_t pixels, void* base, RenderScratch* out)
 {
     Carver c(base);
     RenderScratch s;
-    const uint64_t pixels = (uint64_t)p->width * p->height;
-    s.capacity = (uint32_t)(pixels * wave_samples(p));
+    s.capacity = (uint32_t)(pixels * wave_samples(p, pixels));
     s.queue[0] = c.take<float4>(2ull * s.capacity);
     s.queue[1] = c.take<float4>(2ull * s.capacity);
     s.hits = c.take<float4>(s.capacity);
@@ -562,107 +601,101 @@ int sort_queue(const RenderScratch& rs, const float4* queue, const uint32_t* cou
     return CPT_OK;
 }
 
-bool params_ok(const cpt_render_params* p)
+bool params_ok(const cpt_render_params* p, uint64_t pixels)
 {
-    if (!p || p->width == 0 || p->height == 0 || p->spp == 0) return false;
-    if ((uint64_t)p->width * p->height > (1ull << 31)) return false;
+    if (!p || p->spp == 0 || pixels == 0 || pixels > (1ull << 31)) return false;
     if (p->bounces + 1 > (uint32_t)kMaxDepth) return false;
     if (p->accum_mode > CPT_ACCUM_F64) return false;
-    if (camera_count(p) > kMaxCameras) return false;
-    return (uint64_t)p->width * p->height * wave_samples(p) < (1ull << 31);
+    return pixels * wave_samples(p, pixels) < (1ull << 31);
 }
 
-}  // namespace cpt
+inline uint32_t camera_count(const cpt_render_params* p) { return p->cameras ? p->cameras : 1u; }
 
-using namespace cpt;
-
-extern "C" size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode)  // one camera
+void to_camera(const cpt_camera& src, Camera& cam)
 {
-    const size_t px = (size_t)width * height;
-    if (accum_mode == CPT_ACCUM_KAHAN) return px * 2 * sizeof(float4);
-    if (accum_mode == CPT_ACCUM_LERP) return px * sizeof(float4);
-    if (accum_mode == CPT_ACCUM_F64) return px * sizeof(double4);
-    return 0;
+    for (int a = 0; a < 3; ++a) cam.eye[a] = src.eye[a];
+    for (int c = 0; c < 4; ++c)
+        for (int a = 0; a < 3; ++a) cam.dirs[c][a] = src.dirs[c][a];
+    for (int k = 0; k < 16; ++k) cam.m[k] = src.inv_view_proj[k];
+    cam.jx = src.jitter_x;
+    cam.jy = src.jitter_y;
+    cam.jitter = src.jitter;
 }
 
-extern "C" size_t cpt_render_scratch_bytes(const cpt_render_params* params)
+// Fills the kernel-parameter view table; returns total pixels or 0 on a bad view.
+uint64_t make_views(const cpt_view* views, uint32_t n, uint32_t ref_grid, Views& vs)
 {
-    if (!params_ok(params)) return 0;
-    return render_layout(params, nullptr, nullptr);
-}
-
-extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_camera* camera,
-                          const cpt_render_params* params, void* accum, void* scratch, size_t scratch_bytes,
-                          unsigned long long* ray_counts, uint32_t* status, cudaStream_t stream)
-{
-    if (!bvh || !scene || !camera || !accum || !scratch || !params_ok(params)) return CPT_ERR_INVALID_ARGUMENT;
-    if (!bvh->nodes || !bvh->tris || !scene->infos || (scene->light_count && !scene->lights))
-        return CPT_ERR_INVALID_ARGUMENT;
-    if (scratch_bytes < render_layout(params, nullptr, nullptr)) return CPT_ERR_SCRATCH_TOO_SMALL;
-    if ((reinterpret_cast<uintptr_t>(accum) & 15) || (reinterpret_cast<uintptr_t>(scratch) & 255))
-        return CPT_ERR_INVALID_ARGUMENT;
-    RenderScratch rs;
-    render_layout(params, scratch, &rs);
-    uint32_t* st = status ? status : bvh->status;
-
-    const uint32_t ncam = camera_count(params);
-    Cameras cams;
-    for (uint32_t i = 0; i < ncam; ++i) {
-        Camera& cam = cams.c[i];
-        const cpt_camera& src = camera[i];
-        for (int a = 0; a < 3; ++a) cam.eye[a] = src.eye[a];
-        for (int c = 0; c < 4; ++c)
-            for (int a = 0; a < 3; ++a) cam.dirs[c][a] = src.dirs[c][a];
-        for (int k = 0; k < 16; ++k) cam.m[k] = src.inv_view_proj[k];
-        cam.jx = src.jitter_x;
-        cam.jy = src.jitter_y;
-        cam.jitter = src.jitter;
+    uint64_t total = 0;
+    vs.n = n;
+    for (uint32_t i = 0; i < n; ++i) {
+        const cpt_view& s = views[i];
+        if (!s.bvh || !s.scene || !s.bvh->nodes || !s.bvh->tris || !s.scene->infos || !s.accum || s.width == 0 ||
+            s.height == 0 || (s.scene->light_count && !s.scene->lights) || (reinterpret_cast<uintptr_t>(s.accum) & 15))
+            return 0;
+        View& v = vs.v[i];
+        v.nodes = static_cast<const float4*>(s.bvh->nodes);
+        v.tris = s.bvh->tris;
+        v.infos = s.scene->infos;
+        v.lights = s.scene->lights;
+        v.accum = s.accum;
+        v.info_count = s.scene->info_count;
+        v.light_count = s.scene->light_count;
+        v.max_visits = s.bvh->n;  // a ray fetches each of the n - 1 internal nodes at most once
+        v.width = s.width;
+        v.height = s.height;
+        v.pixels = s.width * s.height;
+        v.ref_w = ref_grid ? s.width / 8u * 8u : s.width;
+        v.ref_h = ref_grid ? s.height / 8u * 8u : s.height;
+        v.pixel_base = (uint32_t)total;
+        to_camera(s.camera, v.cam);
+        total += (uint64_t)s.width * s.height;
+        if (total >= (1ull << 31)) return 0;
     }
-    const size_t accum_stride = cpt_accum_bytes(params->width, params->height, params->accum_mode);
+    vs.total_pixels = (uint32_t)total;
+    return total;
+}
+
+int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, const cpt_render_params* params,
+                 void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
+                 cudaStream_t stream)
+{
+    const uint64_t pixels = vs.total_pixels;
+    if (!params_ok(params, pixels) || !scratch || !status) return CPT_ERR_INVALID_ARGUMENT;
+    if (scratch_bytes < render_layout(params, pixels, nullptr, nullptr)) return CPT_ERR_SCRATCH_TOO_SMALL;
+    if (reinterpret_cast<uintptr_t>(scratch) & 255) return CPT_ERR_INVALID_ARGUMENT;
+    RenderScratch rs;
+    render_layout(params, pixels, scratch, &rs);
 
     Wave wv;
-    wv.ncam = ncam;
-    wv.width = params->width;
-    wv.height = params->height;
-    wv.pixels = params->width * params->height;
     wv.frame0 = params->frame0;
+    wv.frame_dev = params->frame_counter;
     wv.bounces = params->bounces;
     wv.intensity = params->indirect_intensity;
     wv.stratified = params->stratified;
     wv.k0 = params->seed_lo;
     wv.k1 = params->seed_hi;
-    wv.ref_w = params->ref_grid ? params->width / 8u * 8u : params->width;
-    wv.ref_h = params->ref_grid ? params->height / 8u * 8u : params->height;
-    wv.light_count = scene->light_count;
 
-    ShadeScene sc;
-    sc.nodes = static_cast<const float4*>(bvh->nodes);
-    sc.tris = bvh->tris;
-    sc.infos = scene->infos;
-    sc.lights = scene->lights;
-    sc.info_count = scene->info_count;
-    sc.max_visits = bvh->n;
-
+    bool one_bvh = true;
+    for (uint32_t i = 1; i < vs.n; ++i) one_bvh &= vs.v[i].nodes == vs.v[0].nodes;
     const int sms = sm_count();
-    const uint32_t spw_max = wave_samples(params);
-    const uint32_t total = params->spp * ncam;
-    for (uint32_t s0 = 0; s0 < total; s0 += spw_max) {
+    static int ext_occ = 0;
+    if (!ext_occ) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ext_occ, k_extend<false, false>, kExtendBlock, 0) != cudaSuccess ||
+            ext_occ < 1)
+            ext_occ = 1;
+    }
+    const uint32_t spw_max = wave_samples(params, pixels);
+    for (uint32_t s0 = 0; s0 < params->spp; s0 += spw_max) {
         wv.s0 = s0;
-        wv.spw = std::min(spw_max, total - s0);
-        const uint32_t paths = wv.spw * wv.pixels;
+        wv.spw = std::min(spw_max, params->spp - s0);
+        const uint32_t paths = wv.spw * vs.total_pixels;
         CPT_CUDA_TRY(cudaMemsetAsync(rs.counts, 0, sizeof(uint32_t) * 2 * (kMaxDepth + 2), stream));
         {
             CPT_PROF(K_GENERATE, stream);
             k_generate<<<(int)std::min<uint32_t>((paths + kGenBlock - 1) / kGenBlock, (uint32_t)sms * 16), kGenBlock, 0,
-                         stream>>>(wv, cams, rs.queue[0], rs.counts, rs.state);
+                         stream>>>(wv, vs, rs.queue[0], rs.counts, rs.state);
         }
         CPT_LAUNCH_CHECK();
-        static int ext_occ = 0;
-        if (!ext_occ) {
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ext_occ, k_extend<false>, kExtendBlock, 0) != cudaSuccess ||
-                ext_occ < 1)
-                ext_occ = 1;
-        }
         const int ext_blocks = std::min<int>((int)((paths + kExtendBlock - 1) / kExtendBlock), sms * ext_occ);
         const int shade_blocks = std::min<int>((int)((paths + kShadeBlock - 1) / kShadeBlock), sms * 16);
         for (uint32_t b = 0; b <= params->bounces; ++b) {
@@ -670,29 +703,33 @@ extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_
             float4* qout = rs.queue[(b + 1) & 1];
             const uint32_t* order = nullptr;
             if (params->ray_sort && b > 0) {
-                int rc = sort_queue(rs, qin, rs.counts + b, bvh->node_boxes, st, stream);
+                const int rc = sort_queue(rs, qin, rs.counts + b, sort_root, status, stream);
                 if (rc != CPT_OK) return rc;
                 order = rs.sort_vals[(kRayKeyPasses - 1) & 1];
             }
             {
                 CPT_PROF(K_EXTEND, stream);
                 uint32_t* pool = rs.counts + kMaxDepth + 2 + b;
-                if (params->trace_stats)
-                    k_extend<true><<<ext_blocks, kExtendBlock, 0, stream>>>(sc.nodes, qin, rs.counts + b, rs.hits, pool,
-                                                                            ray_counts, st, sc.max_visits, order);
-                else
-                    k_extend<false><<<ext_blocks, kExtendBlock, 0, stream>>>(sc.nodes, qin, rs.counts + b, rs.hits, pool,
-                                                                             ray_counts, st, sc.max_visits, order);
+#define CPT_EXTEND(S, O) \
+    k_extend<S, O><<<ext_blocks, kExtendBlock, 0, stream>>>(vs, qin, rs.counts + b, rs.hits, pool, ray_counts, status, order)
+                if (params->trace_stats) {
+                    if (one_bvh) CPT_EXTEND(true, true); else CPT_EXTEND(true, false);
+                } else {
+                    if (one_bvh) CPT_EXTEND(false, true); else CPT_EXTEND(false, false);
+                }
+#undef CPT_EXTEND
             }
             CPT_LAUNCH_CHECK();
             {
                 CPT_PROF(K_SHADE, stream);
-                if (scene->light_count)
-                    k_shade<true><<<shade_blocks, kShadeBlock, 0, stream>>>(sc, wv, b, qin, rs.hits, rs.counts + b, qout,
-                                                                             rs.counts + b + 1, rs.state, ray_counts, st);
+                if (any_lights)
+                    k_shade<true><<<shade_blocks, kShadeBlock, 0, stream>>>(vs, wv, b, qin, rs.hits, rs.counts + b, qout,
+                                                                             rs.counts + b + 1, rs.state, ray_counts,
+                                                                             status);
                 else
-                    k_shade<false><<<shade_blocks, kShadeBlock, 0, stream>>>(sc, wv, b, qin, rs.hits, rs.counts + b, qout,
-                                                                              rs.counts + b + 1, rs.state, ray_counts, st);
+                    k_shade<false><<<shade_blocks, kShadeBlock, 0, stream>>>(vs, wv, b, qin, rs.hits, rs.counts + b, qout,
+                                                                              rs.counts + b + 1, rs.state, ray_counts,
+                                                                              status);
             }
             CPT_LAUNCH_CHECK();
         }
@@ -705,12 +742,83 @@ extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_
         }
         {
             CPT_PROF(K_ACCUMULATE, stream);
-            const dim3 grid((wv.pixels + 255) / 256, ncam);
-            k_accumulate<<<grid, 256, 0, stream>>>(wv, params->accum_mode, rs.state, accum, accum_stride);
+            k_accumulate<<<(vs.total_pixels + 255) / 256, 256, 0, stream>>>(wv, vs, params->accum_mode, rs.state);
         }
         CPT_LAUNCH_CHECK();
     }
+    if (params->frame_counter) {
+        k_advance<<<1, 1, 0, stream>>>(params->frame_counter, params->spp);
+        CPT_LAUNCH_CHECK();
+    }
     return CPT_OK;
+}
+
+}  // namespace cpt
+
+using namespace cpt;
+
+extern "C" size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode)
+{
+    const size_t px = (size_t)width * height;
+    if (accum_mode == CPT_ACCUM_KAHAN) return px * 2 * sizeof(float4);
+    if (accum_mode == CPT_ACCUM_LERP) return px * sizeof(float4);
+    if (accum_mode == CPT_ACCUM_F64) return px * sizeof(double4);
+    return 0;
+}
+
+extern "C" size_t cpt_render_scratch_bytes(const cpt_render_params* params)
+{
+    if (!params || params->width == 0 || params->height == 0 || camera_count(params) > CPT_MAX_VIEWS) return 0;
+    const uint64_t pixels = (uint64_t)params->width * params->height * camera_count(params);
+    if (!params_ok(params, pixels)) return 0;
+    return render_layout(params, pixels, nullptr, nullptr);
+}
+
+extern "C" size_t cpt_render_views_scratch_bytes(const cpt_view* views, uint32_t n_views,
+                                                 const cpt_render_params* params)
+{
+    if (!views || n_views == 0 || n_views > CPT_MAX_VIEWS) return 0;
+    uint64_t pixels = 0;
+    for (uint32_t i = 0; i < n_views; ++i) pixels += (uint64_t)views[i].width * views[i].height;
+    if (!params_ok(params, pixels)) return 0;
+    return render_layout(params, pixels, nullptr, nullptr);
+}
+
+extern "C" int cpt_render_views(const cpt_view* views, uint32_t n_views, const cpt_render_params* params,
+                                void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
+                                cudaStream_t stream)
+{
+    if (!views || n_views == 0 || n_views > CPT_MAX_VIEWS || !params || !status) return CPT_ERR_INVALID_ARGUMENT;
+    static Views vs;  // 14 KB: built on the host, passed by value to the kernels
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!make_views(views, n_views, params->ref_grid, vs)) return CPT_ERR_INVALID_ARGUMENT;
+    bool lights = false;
+    for (uint32_t i = 0; i < n_views; ++i) lights |= views[i].scene->light_count > 0;
+    return render_views(vs, lights, views[0].bvh->node_boxes, params, scratch, scratch_bytes, ray_counts, status,
+                        stream);
+}
+
+extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_camera* camera,
+                          const cpt_render_params* params, void* accum, void* scratch, size_t scratch_bytes,
+                          unsigned long long* ray_counts, uint32_t* status, cudaStream_t stream)
+{
+    if (!bvh || !scene || !camera || !accum || !params || params->width == 0 || params->height == 0)
+        return CPT_ERR_INVALID_ARGUMENT;
+    const uint32_t ncam = camera_count(params);
+    if (ncam > CPT_MAX_VIEWS) return CPT_ERR_INVALID_ARGUMENT;
+    const size_t stride = cpt_accum_bytes(params->width, params->height, params->accum_mode);
+    cpt_view views[CPT_MAX_VIEWS];
+    for (uint32_t c = 0; c < ncam; ++c) {
+        views[c].bvh = bvh;
+        views[c].scene = scene;
+        views[c].camera = camera[c];
+        views[c].width = params->width;
+        views[c].height = params->height;
+        views[c].accum = static_cast<char*>(accum) + stride * c;
+    }
+    return cpt_render_views(views, ncam, params, scratch, scratch_bytes, ray_counts, status ? status : bvh->status,
+                            stream);
 }
 
 extern "C" int cpt_resolve(const void* accum, uint32_t width, uint32_t height, uint32_t accum_mode, float* rgba,

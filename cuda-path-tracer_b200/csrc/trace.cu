@@ -20,8 +20,12 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(const float4* __restrict_
     __shared__ uint32_t s_stack[kSmemStack * kTraceBlock];
     bool overflow = false;
     uint32_t nn = 0, nt = 0;
-    persistent_trace<kAny, kTraceBlock, kStats, kTraceSteps>(nodes, rays, n, hits, pool, s_stack + threadIdx.x, overflow,
-                                                             nn, nt, max_visits, stats, nullptr);
+    auto nodes_of = [&](uint32_t, uint32_t& mv) -> const float4* {  // one BVH for every ray
+        mv = max_visits;
+        return nodes;
+    };
+    persistent_trace_views<kAny, kTraceBlock, kStats, kTraceSteps>(nodes_of, rays, n, hits, pool, s_stack + threadIdx.x,
+                                                                   overflow, nn, nt, nullptr, stats);
     if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
 }
 

@@ -79,6 +79,8 @@ __device__ __forceinline__ float tri_test(f3 o, f3 d, const float* s, float& u, 
 
 // Per-ray traversal state.
 struct TraceState {
+    const float4* nodes;  // the node array of the ray's BVH
+    uint32_t max_visits;  // node fetches allowed (a valid tree needs at most its n - 1 internal nodes)
     f3 o, d, dinv;
     bool finite;  // all components of 1/d finite
     Hit best;
@@ -88,8 +90,10 @@ struct TraceState {
     uint32_t tests;   // triangle tests
 };
 
-__device__ __forceinline__ void trace_init(TraceState& s, f3 o, f3 d)
+__device__ __forceinline__ void trace_init(TraceState& s, const float4* nodes, uint32_t max_visits, f3 o, f3 d)
 {
+    s.nodes = nodes;
+    s.max_visits = max_visits;
     s.o = o;
     s.d = d;
     s.dinv = mk3(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
@@ -123,12 +127,11 @@ __device__ __forceinline__ uint32_t stack_pop(const uint32_t* smem_col, const ui
 // One node visit of trace.h:104-165. Returns true when the ray is finished
 // (stack empty after a pop, or — any-hit — a triangle was recorded).
 template <bool kAny, int kBlock, bool kStats>
-__device__ __forceinline__ bool trace_step(TraceState& s, const float4* __restrict__ nodes, uint32_t* smem_col,
-                                           uint32_t* spill, bool& overflow, uint32_t& n_nodes, uint32_t& n_tris,
-                                           uint32_t max_visits)
+__device__ __forceinline__ bool trace_step(TraceState& s, uint32_t* smem_col, uint32_t* spill, bool& overflow,
+                                           uint32_t& n_nodes, uint32_t& n_tris)
 {
-    if (++s.visits > max_visits) { overflow = true; return true; }
-    const float4* nd = nodes + kNodeFloat4 * (size_t)s.cur;
+    if (++s.visits > s.max_visits) { overflow = true; return true; }
+    const float4* nd = s.nodes + kNodeFloat4 * (size_t)s.cur;
     float w[kNodeFloats];
 #pragma unroll
     for (int k = 0; k < kNodeFloat4; ++k) {
@@ -203,26 +206,28 @@ __device__ __forceinline__ Hit traverse(const float4* __restrict__ nodes, f3 o, 
                                         uint32_t max_visits)
 {
     TraceState s;
-    trace_init(s, o, d);
+    trace_init(s, nodes, max_visits, o, d);
     uint32_t spill[CPT_TRAVERSAL_STACK - kSmemStack];
     uint32_t nn = 0, nt = 0;
-    while (!trace_step<kAny, kBlock, false>(s, nodes, smem_col, spill, overflow, nn, nt, max_visits)) {
+    while (!trace_step<kAny, kBlock, false>(s, smem_col, spill, overflow, nn, nt)) {
     }
     return s.best;
 }
 
-// Persistent traversal of `n` rays: ray i is (origin, direction) = rays[2i], rays[2i+1]
-// (.w of the first holds a payload), its hit goes to hits[i]. Lanes take rays from
-// *pool in warp-sized grabs and refill as soon as their ray finishes.
+// Persistent traversal of `n` rays: ray i is (origin, direction) = rays[2i], rays[2i+1];
+// its hit goes to hits[i]. nodes_of(w, max_visits) returns the node array (and the
+// visit bound) for the word w carried in the direction's .w (a view index, or
+// unused). Lanes take rays from *pool in warp-sized grabs and refill as soon as
+// their ray finishes.
 // ray_stats (nullable, with kStats): per ray (node fetches, triangle tests).
 // order (nullable): rays are taken in the order order[0], order[1], ... (a
 // permutation of 0..n-1); hits and stats stay indexed by the ray's own index.
-template <bool kAny, int kBlock, bool kStats, int kSteps>
-__device__ __forceinline__ void persistent_trace(const float4* __restrict__ nodes, const float4* __restrict__ rays,
-                                                 uint32_t n, float4* __restrict__ hits, uint32_t* __restrict__ pool,
-                                                 uint32_t* smem_col, bool& overflow, uint32_t& n_nodes,
-                                                 uint32_t& n_tris, uint32_t max_visits, uint2* __restrict__ ray_stats,
-                                                 const uint32_t* __restrict__ order)
+template <bool kAny, int kBlock, bool kStats, int kSteps, typename NodesOf>
+__device__ __forceinline__ void persistent_trace_views(NodesOf nodes_of, const float4* __restrict__ rays, uint32_t n,
+                                                       float4* __restrict__ hits, uint32_t* __restrict__ pool,
+                                                       uint32_t* smem_col, bool& overflow, uint32_t& n_nodes,
+                                                       uint32_t& n_tris, const uint32_t* __restrict__ order,
+                                                       uint2* __restrict__ ray_stats = nullptr)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
@@ -245,7 +250,9 @@ __device__ __forceinline__ void persistent_trace(const float4* __restrict__ node
                     if (r < n) {
                         ray = order ? order[r] : r;
                         const float4 ro = rays[2 * (size_t)ray], rd = rays[2 * (size_t)ray + 1];
-                        trace_init(s, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z));
+                        uint32_t mv;
+                        const float4* nodes = nodes_of(__float_as_uint(rd.w), mv);
+                        trace_init(s, nodes, mv, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z));
                     }
                 }
             }
@@ -254,7 +261,7 @@ __device__ __forceinline__ void persistent_trace(const float4* __restrict__ node
         if (ray != CPT_INVALID_INDEX) {
 #pragma unroll 1
             for (int k = 0; k < kSteps; ++k) {
-                if (trace_step<kAny, kBlock, kStats>(s, nodes, smem_col, spill, overflow, n_nodes, n_tris, max_visits)) {
+                if (trace_step<kAny, kBlock, kStats>(s, smem_col, spill, overflow, n_nodes, n_tris)) {
                     hits[ray] = make_float4(s.best.t, s.best.u, s.best.v, __uint_as_float(s.best.tri));
                     if (kStats && ray_stats) ray_stats[ray] = make_uint2(s.visits, s.tests);
                     ray = CPT_INVALID_INDEX;

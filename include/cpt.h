@@ -171,12 +171,15 @@ typedef struct cpt_render_params {
     uint32_t trace_stats;      /* 1: count node fetches / triangle tests of extension rays (slower) */
     uint32_t ray_sort;         /* 1: sort each bounce queue by direction octant + origin Morton code
                                 *    before tracing it (coherence; results are unchanged) */
-    uint32_t cameras;          /* cameras rendered in one call (0 or 1: one; at most 16): `camera` points to
-                                * that many cpt_camera, `accum` to that many consecutive accumulators of
-                                * cpt_accum_bytes() each; camera c draws from the Philox counter word 3 = c */
+    uint32_t cameras;          /* cameras rendered in one call (0 or 1: one; at most CPT_MAX_VIEWS): `camera`
+                                * points to that many cpt_camera, `accum` to that many consecutive accumulators
+                                * of cpt_accum_bytes() each; camera c draws from the Philox counter word 3 = c */
+    uint32_t* frame_counter;   /* device, nullable: when set, the call renders global samples
+                                * *frame_counter + frame0 ... and adds spp to *frame_counter at its end, so a
+                                * call captured once in a CUDA graph renders the next samples on each replay */
 } cpt_render_params;
 
-size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode); /* per camera */
+size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode); /* per camera / view */
 size_t cpt_render_scratch_bytes(const cpt_render_params* params);
 
 /* Renders params->spp samples into accum. Replaces CUDAPathTracer::raytrace
@@ -190,6 +193,25 @@ size_t cpt_render_scratch_bytes(const cpt_render_params* params);
 int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_camera* camera, const cpt_render_params* params,
                void* accum, void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
                cudaStream_t stream);
+
+/* ---- batched views: several scenes and/or cameras in the same waves ----
+ * A view is one image: a BVH, its shading inputs, a camera, a resolution and an
+ * accumulator (device, cpt_accum_bytes(width, height, params->accum_mode)).
+ * One call renders params->spp samples of up to CPT_MAX_VIEWS views; the rays of
+ * all views share every wavefront launch, and a frame is a fixed sequence of
+ * kernel launches on `stream` (capturable in a CUDA graph). View i draws from
+ * Philox counter word 3 = i. params->width/height/cameras are not used here. */
+#define CPT_MAX_VIEWS 64
+typedef struct cpt_view {
+    const cpt_bvh* bvh;
+    const cpt_scene* scene;
+    cpt_camera camera;
+    uint32_t width, height;
+    void* accum;
+} cpt_view;
+size_t cpt_render_views_scratch_bytes(const cpt_view* views, uint32_t n_views, const cpt_render_params* params);
+int cpt_render_views(const cpt_view* views, uint32_t n_views, const cpt_render_params* params, void* scratch,
+                     size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status, cudaStream_t stream);
 
 /* Writes the displayable image (float4 rgba per pixel, alpha 1) of an accumulator. */
 int cpt_resolve(const void* accum, uint32_t width, uint32_t height, uint32_t accum_mode, float* rgba,

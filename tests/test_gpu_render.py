@@ -152,6 +152,36 @@ def test_several_cameras_in_one_call(cuda):
         assert np.all(acc[c, 0, ..., 3] == n)
 
 
+def test_batched_scenes_in_one_call(cuda):
+    """Three different scenes at three resolutions in the same waves: each view's
+    accumulator equals the oracle's render of that scene alone (view i = stream word i)."""
+    from cpt.device import BatchRenderer
+
+    cube = ((0.5, 0.5, -1.2), (0.5, 0.5, 0.0))
+    specs = [(cpt.scene_random(9000, seed=3), (40, 24), cube), (cpt.scene_random(15000, seed=4), (64, 48), cube),
+             (cpt.scene_sphere_hairball(64, 32, 3000, seed=5), (32, 32), ((0.0, 0.3, -3.6), (0.0, 0.0, 0.0)))]
+    views, keep = [], []
+    for (tris, infos), (w, h), (eye, tgt) in specs:
+        lb = DeviceLbvh(len(tris), 30)
+        lb.build(to_device(tris), check_root=True)
+        sc = DeviceScene(infos)
+        cam = cpt.camera_look_at(eye, tgt, aspect=w / h)
+        views.append((lb, sc, cam, w, h))
+        keep.append((tris, infos, cam, w, h))
+    br = BatchRenderer(views, make_params(0, 0, 3, 1, 4, 3.0, True, 13, cpt.ACCUM_KAHAN, wave_paths=3000))
+    br.render()
+    torch.cuda.synchronize()
+    br.check_status()
+    for i, (tris, infos, cam, w, h) in enumerate(keep):
+        acc = br.accums[i].cpu().numpy().view(np.float32).reshape(2, h, w, 4)[0]
+        b = cpu.build(tris, 30)
+        rad, _ = cpu.render(b, infos, None, w, h, 3, 1, 4, 3.0, True, 13, cpu.ocam_from(cam.eye, cam.as_array()[3:]),
+                            camera_index=i)
+        s, _, n = cpu.accumulate_kahan(rad)
+        assert acc[..., :3].tobytes() == s.tobytes(), i
+        assert np.all(acc[..., 3] == n)
+
+
 def test_directional_lights_shadow_rays(cuda):
     tris, infos, _, cam = scene()
     lights = dir_lights()
@@ -218,3 +248,37 @@ def test_tracer_object_host_buffers(cuda):
     s1, _, _ = cpu.accumulate_kahan(rad[:1])
     assert img1[..., :3].tobytes() == s1.tobytes()
     t.close()
+
+
+def test_graph_replay_advances_the_sample_stream(cuda):
+    """One render call captured in a CUDA graph, replayed twice, equals two direct
+    calls with frame0 = 0 and spp (the device frame counter advances per replay)."""
+    tris, infos, _, cam = scene(n=8000)
+    lb = DeviceLbvh(len(tris), 30)
+    lb.build(to_device(tris), check_root=True)
+    sc = DeviceScene(infos)
+    direct = DeviceRenderer(make_params(W, H, 2, 0, 3, 3.0, True, 3, cpt.ACCUM_KAHAN))
+    direct.render(lb, sc, cam, frame0=0)
+    direct.render(lb, sc, cam, frame0=2)
+    counter = torch.zeros(1, dtype=torch.int32, device="cuda")
+    p = make_params(W, H, 2, 0, 3, 3.0, True, 3, cpt.ACCUM_KAHAN)
+    p.frame_counter = counter.data_ptr()
+    graphed = DeviceRenderer(p)
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        graphed.render(lb, sc, cam)  # warm-up outside the graph (frame 0..1)
+    torch.cuda.synchronize()
+    graphed.reset()
+    counter.zero_()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        graphed.render(lb, sc, cam)
+    torch.cuda.synchronize()
+    graphed.reset()
+    counter.zero_()
+    g.replay()
+    g.replay()
+    torch.cuda.synchronize()
+    assert int(counter.item()) == 4
+    assert graphed.accum.cpu().numpy().tobytes() == direct.accum.cpu().numpy().tobytes()
