@@ -235,8 +235,11 @@ __global__ void __launch_bounds__(kGenBlock) k_generate(Wave wv, Views vs, float
 
 // kOneView: every ray traverses view 0's BVH (a single scene, e.g. several cameras of
 // it); the node array is then a kernel-wide constant instead of a per-ray value.
+#ifndef CPT_EXTEND_MIN_BLOCKS
+#define CPT_EXTEND_MIN_BLOCKS 1
+#endif
 template <bool kStats, bool kOneView>
-__global__ void __launch_bounds__(kExtendBlock) k_extend(Views vs, const float4* __restrict__ queue,
+__global__ void __launch_bounds__(kExtendBlock, CPT_EXTEND_MIN_BLOCKS) k_extend(Views vs, const float4* __restrict__ queue,
                                                          const uint32_t* __restrict__ count, float4* __restrict__ hits,
                                                          uint32_t* __restrict__ pool,
                                                          unsigned long long* __restrict__ ray_counts,
