@@ -67,7 +67,7 @@ class Bvh(ctypes.Structure):
 
 class Scene(ctypes.Structure):
     _fields_ = [("infos", ctypes.c_void_p), ("info_count", ctypes.c_uint32), ("lights", ctypes.c_void_p),
-                ("light_count", ctypes.c_uint32)]
+                ("light_count", ctypes.c_uint32), ("textures", ctypes.c_void_p), ("texture_count", ctypes.c_uint32)]
 
 
 class Camera(ctypes.Structure):
@@ -124,6 +124,7 @@ _PROTOS = {
     "cpt_tracer_create": (_I32, [ctypes.POINTER(_P), _I32]),
     "cpt_tracer_destroy": (None, [_P]),
     "cpt_tracer_upload": (_I32, [_P, _P, _U32, _P, _U32, _P, _U32, _P]),
+    "cpt_tracer_upload_textures": (_I32, [_P, _P, _U32]),
     "cpt_tracer_set_primary_rays": (_I32, [_P, _P]),
     "cpt_tracer_set_eye": (_I32, [_P, _P]),
     "cpt_tracer_set_camera": (_I32, [_P, ctypes.POINTER(Camera)]),
@@ -139,6 +140,9 @@ _PROTOS = {
     "cpt_scene_sphere_hairball": (_U32, [_U32, _U32, _F, _U32, _F, _U32, _F, _F, _F, _F, _P, _P]),
     "cpt_scene_bounds": (None, [_P, _U32, _P]),
     "cpt_scene_deform": (_I32, [_P, _P, _U32, _F, _F, _F, _P]),
+    "cpt_texture_create": (_I32, [_P, _U32, _U32, ctypes.POINTER(ctypes.c_uint64)]),
+    "cpt_texture_destroy": (None, [ctypes.c_uint64]),
+    "cpt_texture_sample": (_I32, [ctypes.c_uint64, _P, _U32, _P, _P]),
     "cpt_obj_load": (_I32, [ctypes.c_char_p, _F, _P, _F, _P, _P, _U32, ctypes.POINTER(_U32)]),
     "cpt_bvh_heatmap": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Camera), _U32, _U32, _P, _P, _P, _P]),
     "cpt_camera_look_at": (None, [_P, _P, _P, _F, _F, _F, _F, ctypes.POINTER(Camera)]),
@@ -303,6 +307,37 @@ def profile_end() -> dict:
     return out
 
 
+class Texture:
+    """One RGBA8 image as a texture object with the reference's sampler state
+    (Scene.cu:57-81): normalized coordinates, bilinear, wrap, read as [0, 1] floats."""
+
+    def __init__(self, rgba8: np.ndarray):
+        img = np.ascontiguousarray(rgba8, np.uint8)
+        if img.ndim != 3 or img.shape[2] != 4:
+            raise ValueError("texture must be (height, width, 4) uint8")
+        self.height, self.width = int(img.shape[0]), int(img.shape[1])
+        self.texels = img
+        h = ctypes.c_uint64()
+        check(lib.cpt_texture_create(_ptr(img), self.width, self.height, ctypes.byref(h)), "cpt_texture_create")
+        self.handle = int(h.value)
+
+    def close(self) -> None:
+        if self.handle:
+            lib.cpt_texture_destroy(self.handle)
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def texture_handles(textures) -> np.ndarray:
+    """cudaTextureObject_t table (uint64) for a list of Texture."""
+    return np.array([t.handle for t in textures], np.uint64)
+
+
 class Tracer:
     """Reference-facing tracer (CUDAPathTracer): host buffers in, image out."""
 
@@ -330,6 +365,11 @@ class Tracer:
         box_arr = None if box is None else np.ascontiguousarray(box, np.float32)
         check(lib.cpt_tracer_upload(self._h, _ptr(tris), len(tris), _ptr(infos), len(infos), lp, nl,
                                     None if box_arr is None else _ptr(box_arr)), "cpt_tracer_upload")
+
+    def upload_textures(self, textures) -> None:
+        table = texture_handles(textures)
+        check(lib.cpt_tracer_upload_textures(self._h, _ptr(table) if len(table) else None, len(table)),
+              "cpt_tracer_upload_textures")
 
     def set_camera(self, cam: Camera) -> None:
         check(lib.cpt_tracer_set_camera(self._h, ctypes.byref(cam)), "cpt_tracer_set_camera")

@@ -13,7 +13,7 @@ import ctypes
 
 from . import (ACCUM_KAHAN, BBOX_DTYPE, BUILD_CHECK, TRIANGLE_DTYPE, Bvh, Camera, RenderParams, Scene, View, accum_bytes,
                bvh_bind, bvh_bytes, check, lbvh_build, lbvh_scratch_bytes, lib, render, render_scratch_bytes, resolve,
-               status_check, trace)
+               status_check, texture_handles, trace)
 
 
 def stream_handle(stream: torch.cuda.Stream | None = None) -> int:
@@ -86,15 +86,21 @@ class DeviceLbvh:
 
 
 class DeviceScene:
-    """Shading inputs (TriangleInfo records, directional lights) in device memory."""
+    """Shading inputs (TriangleInfo records, directional lights, texture table) in device memory.
 
-    def __init__(self, infos: np.ndarray, lights: np.ndarray | None = None, device=None):
+    textures: list of cpt.Texture indexed by the records' albedo_idx / normal_map_idx
+    (the caller keeps them alive while this scene renders)."""
+
+    def __init__(self, infos: np.ndarray, lights: np.ndarray | None = None, device=None, textures=None):
         self.infos = to_device(infos, device)
         self.n_infos = len(infos)
         self.n_lights = 0 if lights is None else len(lights)
         self.lights = to_device(lights, device) if self.n_lights else None
+        self.textures = list(textures or [])
+        table = texture_handles(self.textures)
+        self.texture_table = to_device(table.view(np.uint8), device) if len(table) else None
         self.scene = Scene(self.infos.data_ptr(), self.n_infos, self.lights.data_ptr() if self.n_lights else None,
-                           self.n_lights)
+                           self.n_lights, self.texture_table.data_ptr() if len(table) else None, len(table))
 
 
 def make_params(width, height, spp, frame0=0, bounces=3, intensity=3.0, stratified=True, seed=0,

@@ -437,6 +437,9 @@ struct cpt_tracer {
     size_t infos_cap = 0;
     void* d_lights = nullptr;
     size_t lights_cap = 0;
+    void* d_textures = nullptr;  // cudaTextureObject_t handles (the caller owns the textures)
+    size_t textures_cap = 0;
+    uint32_t texture_count = 0;
     cpt_bvh bvh{};
     bool ready = false;
     // frame
@@ -488,7 +491,7 @@ extern "C" void cpt_tracer_destroy(cpt_tracer* t)
 {
     if (!t) return;
     if (t->stream) cudaStreamSynchronize(t->stream);
-    void* bufs[] = {t->d_tris, t->d_bvh, t->d_build_scratch, t->d_infos, t->d_lights, t->d_accum,
+    void* bufs[] = {t->d_tris, t->d_bvh, t->d_build_scratch, t->d_infos, t->d_lights, t->d_textures, t->d_accum,
                     t->d_render_scratch, t->d_image, t->d_counts};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -525,6 +528,20 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
     t->frame = 0;  // CUDAPathTracer::upload resets the frame counter (cuda_path_tracer.cu:469)
     t->ready = true;
     CPT_CUDA_TRY(cudaMemsetAsync(t->d_counts, 0, CPT_RAY_COUNTS * sizeof(unsigned long long), t->stream));
+    return CPT_OK;
+}
+
+extern "C" int cpt_tracer_upload_textures(cpt_tracer* t, const cudaTextureObject_t* textures, uint32_t count)
+{
+    if (!t || (count && !textures)) return CPT_ERR_INVALID_ARGUMENT;
+    int rc;
+    if (count && (rc = ensure(&t->d_textures, &t->textures_cap, sizeof(cudaTextureObject_t) * (size_t)count))) return rc;
+    if (count)
+        CPT_CUDA_TRY(cudaMemcpyAsync(t->d_textures, textures, sizeof(cudaTextureObject_t) * (size_t)count,
+                                     cudaMemcpyHostToDevice, t->stream));
+    // The host copy may go away when this returns: wait for the copy.
+    CPT_CUDA_TRY(cudaStreamSynchronize(t->stream));
+    t->texture_count = count;
     return CPT_OK;
 }
 
@@ -589,7 +606,8 @@ extern "C" int cpt_tracer_raytrace(cpt_tracer* t, uint32_t width, uint32_t heigh
     t->height = height;
     if (t->frame == 0) CPT_CUDA_TRY(cudaMemsetAsync(t->d_accum, 0, ab, t->stream));
     cpt_scene sc{static_cast<const cpt_triangle_info*>(t->d_infos), t->info_count,
-                 static_cast<const cpt_dir_light*>(t->d_lights), t->light_count};
+                 static_cast<const cpt_dir_light*>(t->d_lights), t->light_count,
+                 t->texture_count ? static_cast<const cudaTextureObject_t*>(t->d_textures) : nullptr, t->texture_count};
     rc = cpt_render(&t->bvh, &sc, &t->cam, &p, t->d_accum, t->d_render_scratch, t->render_cap, t->d_counts,
                     t->bvh.status, t->stream);
     if (rc) return rc;

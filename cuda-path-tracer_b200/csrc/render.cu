@@ -51,8 +51,9 @@ struct View {
     const cpt_triangle* tris;  // Morton-sorted reference records (info_idx of a hit)
     const cpt_triangle_info* infos;
     const cpt_dir_light* lights;
+    const cudaTextureObject_t* textures;
     void* accum;
-    uint32_t info_count, light_count, max_visits;
+    uint32_t info_count, light_count, max_visits, texture_count;
     uint32_t width, height, pixels, ref_w, ref_h;
     uint32_t pixel_base;  // pixels of the views before this one
     Camera cam;
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(kGenBlock) k_generate(Wave wv, Views vs, float
 // kOneView: every ray traverses view 0's BVH (a single scene, e.g. several cameras of
 // it); the node array is then a kernel-wide constant instead of a per-ray value.
 #ifndef CPT_EXTEND_MIN_BLOCKS
-#define CPT_EXTEND_MIN_BLOCKS 1
+#define CPT_EXTEND_MIN_BLOCKS 8
 #endif
 template <bool kStats, bool kOneView>
 __global__ void __launch_bounds__(kExtendBlock, CPT_EXTEND_MIN_BLOCKS) k_extend(Views vs, const float4* __restrict__ queue,
@@ -302,6 +303,44 @@ __device__ __forceinline__ f3 light_l(const View& v, f3 p, const cpt_dir_light& 
     return muls(mk3(l.color[0], l.color[1], l.color[2]), l.intensity);
 }
 
+// extractInfo / unpackNormal (cuda_path_tracer.cu:85-138): albedo from the albedo
+// texture at the interpolated uv (as stored, not normalised) or the normalised
+// interpolated vertex colour; normal from the normal map (2 * texel - 1 in the
+// interpolated tangent frame, normalised) or the normalised interpolated normal.
+// A texture index past the view's texture table is treated as absent.
+__device__ __forceinline__ void surface(const View& v, const cpt_triangle_info& in, float u, float w, f3& albedo,
+                                        f3& normal)
+{
+    normal = normalize(bary(ld3(in.vertices[0].normal), ld3(in.vertices[1].normal), ld3(in.vertices[2].normal), u, w));
+    const uint32_t ai = in.material.albedo_idx, ni = in.material.normal_map_idx;
+    const bool tex_a = ai < v.texture_count, tex_n = ni < v.texture_count;
+    if (!tex_a && !tex_n) {
+        albedo = normalize(bary(ld3(in.vertices[0].color), ld3(in.vertices[1].color), ld3(in.vertices[2].color), u, w));
+        return;
+    }
+    // computeUV (TriangleInfo.h:71-74)
+    const float tw = __fsub_rn(__fsub_rn(1.0f, u), w);
+    const float tu = __fadd_rn(__fadd_rn(__fmul_rn(in.vertices[0].uv[0], tw), __fmul_rn(in.vertices[1].uv[0], u)),
+                               __fmul_rn(in.vertices[2].uv[0], w));
+    const float tv = __fadd_rn(__fadd_rn(__fmul_rn(in.vertices[0].uv[1], tw), __fmul_rn(in.vertices[1].uv[1], u)),
+                               __fmul_rn(in.vertices[2].uv[1], w));
+    if (tex_a) {
+        const float4 c = tex2D<float4>(v.textures[ai], tu, tv);
+        albedo = mk3(c.x, c.y, c.z);
+    } else {
+        albedo = normalize(bary(ld3(in.vertices[0].color), ld3(in.vertices[1].color), ld3(in.vertices[2].color), u, w));
+    }
+    if (tex_n) {
+        const float4 ns = tex2D<float4>(v.textures[ni], tu, tv);
+        const float nx = __fsub_rn(__fmul_rn(2.0f, ns.x), 1.0f), ny = __fsub_rn(__fmul_rn(2.0f, ns.y), 1.0f);
+        const float nz = __fsub_rn(__fmul_rn(2.0f, ns.z), 1.0f);
+        const f3 tg = normalize(bary(ld3(in.vertices[0].tangent), ld3(in.vertices[1].tangent), ld3(in.vertices[2].tangent), u, w));
+        const f3 bt = normalize(bary(ld3(in.vertices[0].bitangent), ld3(in.vertices[1].bitangent),
+                                     ld3(in.vertices[2].bitangent), u, w));
+        normal = normalize(add(add(muls(tg, nx), muls(bt, ny)), muls(normal, nz)));
+    }
+}
+
 template <bool kLights>
 __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32_t depth,
                                                        const float4* __restrict__ queue_in,
@@ -336,8 +375,8 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
                 const float t = hit4.x, u = hit4.y, w = hit4.z;
                 const cpt_triangle_info& in = v.infos[info_idx];
                 const f3 hp = add(muls(d, t), o);
-                f3 albedo = normalize(bary(ld3(in.vertices[0].color), ld3(in.vertices[1].color), ld3(in.vertices[2].color), u, w));
-                const f3 normal = normalize(bary(ld3(in.vertices[0].normal), ld3(in.vertices[1].normal), ld3(in.vertices[2].normal), u, w));
+                f3 albedo, normal;
+                surface(v, in, u, w, albedo, normal);
                 const f3 e = ld3(in.material.emission);
                 const bool emissive = __fadd_rn(__fadd_rn(e.x, e.y), e.z) > 1e-7f;
                 const float4 acc4 = state[2 * (size_t)pid], ab4 = state[2 * (size_t)pid + 1];
@@ -640,6 +679,8 @@ uint64_t make_views(const cpt_view* views, uint32_t n, uint32_t ref_grid, Views&
         v.tris = s.bvh->tris;
         v.infos = s.scene->infos;
         v.lights = s.scene->lights;
+        v.textures = s.scene->textures;
+        v.texture_count = s.scene->textures ? s.scene->texture_count : 0u;
         v.accum = s.accum;
         v.info_count = s.scene->info_count;
         v.light_count = s.scene->light_count;

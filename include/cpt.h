@@ -52,8 +52,8 @@ typedef struct cpt_vertex { float color[3], uv[2], normal[3], tangent[3], bitang
 typedef struct cpt_material {
     float emission[3];
     float specularity;
-    uint32_t albedo_idx;     /* texture index or CPT_INVALID_INDEX (textures: not supported, ignored) */
-    uint32_t normal_map_idx; /* idem */
+    uint32_t albedo_idx;     /* index into cpt_scene.textures, or CPT_INVALID_INDEX */
+    uint32_t normal_map_idx; /* idem (tangent-space normal map) */
 } cpt_material;                                                                   /* 24 B */
 typedef struct cpt_triangle_info { cpt_vertex vertices[3]; cpt_material material; } cpt_triangle_info; /* 192 B */
 typedef struct cpt_dir_light { float color[3], direction[3], intensity; } cpt_dir_light;               /* 28 B */
@@ -138,7 +138,20 @@ typedef struct cpt_scene {
     uint32_t info_count;
     const cpt_dir_light* lights;    /* device */
     uint32_t light_count;
+    const cudaTextureObject_t* textures; /* device array of texture handles (cpt_texture_create), nullable */
+    uint32_t texture_count;
 } cpt_scene;
+
+/* A 2D texture for albedo / normal maps: RGBA8 texels (host memory, row-major),
+ * sampled like the reference's textures (Scene.cu:57-81): normalized coordinates,
+ * bilinear filtering, wrap addressing, values read as floats in [0, 1]. The
+ * reference samples its mipmapped arrays with tex2D, i.e. level 0, which is what
+ * this single-level texture holds. */
+int cpt_texture_create(const uint8_t* rgba8, uint32_t width, uint32_t height, cudaTextureObject_t* out);
+void cpt_texture_destroy(cudaTextureObject_t tex);
+/* tex2D<float4>(tex, u, v) for n coordinate pairs (device uv[2n] -> device rgba_out[4n]):
+ * the sampler the shader reads, exposed for parity tests. No reference counterpart. */
+int cpt_texture_sample(cudaTextureObject_t tex, const float* uv, uint32_t n, float* rgba_out, cudaStream_t stream);
 
 /* Eye and the four corner ray directions (00, 10, 11, 01) of
  * CUDAPathTracer::setPrimaryRays/setEyePos (cuda_path_tracer.h:19-21). With
@@ -236,6 +249,10 @@ void cpt_tracer_destroy(cpt_tracer* t);
 int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32_t n, const cpt_triangle_info* infos,
                       uint32_t info_count, const cpt_dir_light* lights, uint32_t light_count,
                       const float* enclosing_box);
+/* Scene::upload(textureArrays) (Scene.cu:57-81): the texture table that
+ * albedo_idx / normal_map_idx index (handles from cpt_texture_create; the caller
+ * keeps them alive while the tracer renders). count 0 clears it. */
+int cpt_tracer_upload_textures(cpt_tracer* t, const cudaTextureObject_t* textures, uint32_t count);
 int cpt_tracer_set_primary_rays(cpt_tracer* t, const float dirs[12]);
 int cpt_tracer_set_eye(cpt_tracer* t, const float eye[3]);
 int cpt_tracer_set_camera(cpt_tracer* t, const cpt_camera* cam);

@@ -411,6 +411,81 @@ typedef struct {
     uint32_t camera;  /* counter word 3 of the bounce stream */
 } oscene;
 
+/* ---- textures: Scene::upload's sampler (Scene.cu:57-81) read by extractInfo /
+ * unpackNormal (cuda_path_tracer.cu:85-138) ---- */
+typedef struct { const uint8_t* rgba; uint32_t width, height; } otex;
+static const otex* g_textures;
+static uint32_t g_texture_count;
+
+/* The texture table later renders read (NULL clears it). */
+void orc_set_textures(const otex* textures, uint32_t count)
+{
+    g_textures = textures;
+    g_texture_count = textures ? count : 0;
+}
+
+/* tex2D<float4> with normalized coordinates, wrap addressing, bilinear filtering and
+ * normalized-float reads of RGBA8 texels, as the CUDA C Programming Guide states
+ * texture fetching ("Texture Fetching", linear filtering): wrap takes frac(u); the
+ * texel-space position is x = frac(u) * W - 0.5, i = floor(x), and the weight
+ * a = frac(x) is held in 9-bit fixed point with 8 fraction bits (rounded to
+ * nearest here; the hardware's rounding of that step is not documented, which the
+ * parity tests' tolerance covers). Texel values are byte / 255. */
+static void tex_sample(const otex* t, double u, double v, double out[4])
+{
+    double x = (u - floor(u)) * (double)t->width - 0.5, y = (v - floor(v)) * (double)t->height - 0.5;
+    double fx = floor(x), fy = floor(y);
+    double a = nearbyint((x - fx) * 256.0) / 256.0, b = nearbyint((y - fy) * 256.0) / 256.0;
+    long W = (long)t->width, H = (long)t->height;
+    long i0 = (((long)fx % W) + W) % W, j0 = (((long)fy % H) + H) % H;
+    long i1 = (i0 + 1) % W, j1 = (j0 + 1) % H;
+    const uint8_t* p00 = t->rgba + 4 * (j0 * W + i0);
+    const uint8_t* p10 = t->rgba + 4 * (j0 * W + i1);
+    const uint8_t* p01 = t->rgba + 4 * (j1 * W + i0);
+    const uint8_t* p11 = t->rgba + 4 * (j1 * W + i1);
+    for (int c = 0; c < 4; ++c)
+        out[c] = ((1.0 - a) * (1.0 - b) * p00[c] + a * (1.0 - b) * p10[c] + (1.0 - a) * b * p01[c] + a * b * p11[c]) /
+                 255.0;
+}
+
+/* tex_sample for n coordinate pairs (tests of the sampler alone). */
+void orc_tex_sample(const otex* t, const float* uv, uint32_t n, float* out)
+{
+    for (uint32_t i = 0; i < n; ++i) {
+        double s[4];
+        tex_sample(t, uv[2 * i], uv[2 * i + 1], s);
+        for (int c = 0; c < 4; ++c) out[4 * i + c] = (float)s[c];
+    }
+}
+
+/* extractInfo + unpackNormal (cuda_path_tracer.cu:85-138): albedo from the albedo
+ * texture at the interpolated uv, else the normalised interpolated colour; normal
+ * from the normal map in the interpolated tangent frame, else the normalised
+ * interpolated normal. An index past the texture table counts as absent. */
+static void surface(const oinfo* in, float u, float v, v3* albedo, v3* normal)
+{
+    *normal = normalize(bary(ld3(in->v[0].normal), ld3(in->v[1].normal), ld3(in->v[2].normal), u, v));
+    uint32_t ai = in->m.albedo_idx, ni = in->m.normal_idx;
+    int ta = ai < g_texture_count, tn = ni < g_texture_count;
+    if (!ta) *albedo = normalize(bary(ld3(in->v[0].color), ld3(in->v[1].color), ld3(in->v[2].color), u, v));
+    if (!ta && !tn) return;
+    float w = (1.0f - u) - v;
+    float tu = (in->v[0].uv[0] * w + in->v[1].uv[0] * u) + in->v[2].uv[0] * v;
+    float tv = (in->v[0].uv[1] * w + in->v[1].uv[1] * u) + in->v[2].uv[1] * v;
+    double s[4];
+    if (ta) {
+        tex_sample(&g_textures[ai], tu, tv, s);
+        *albedo = mk((float)s[0], (float)s[1], (float)s[2]);
+    }
+    if (tn) {
+        tex_sample(&g_textures[ni], tu, tv, s);
+        float nx = 2.0f * (float)s[0] - 1.0f, ny = 2.0f * (float)s[1] - 1.0f, nz = 2.0f * (float)s[2] - 1.0f;
+        v3 tg = normalize(bary(ld3(in->v[0].tangent), ld3(in->v[1].tangent), ld3(in->v[2].tangent), u, v));
+        v3 bt = normalize(bary(ld3(in->v[0].bitangent), ld3(in->v[1].bitangent), ld3(in->v[2].bitangent), u, v));
+        *normal = normalize(add(add(muls(tg, nx), muls(bt, ny)), muls(*normal, nz)));
+    }
+}
+
 typedef struct { uint64_t primary, extension, shadow; } ocount;
 
 static inline float emission_sum(const omat* m) { return m->emission[0] + m->emission[1] + m->emission[2]; }
@@ -465,8 +540,8 @@ static v3 path_radiance(const oscene* sc, v3 o, v3 d, uint32_t pixel, uint32_t f
     if (idx == INVALID_IDX) return mk(0.f, 0.f, 0.f);
     const oinfo* in = info_of(sc, idx);
     v3 hit = add(muls(d, t), o);
-    v3 albedo = normalize(bary(ld3(in->v[0].color), ld3(in->v[1].color), ld3(in->v[2].color), u, v));
-    v3 normal = normalize(bary(ld3(in->v[0].normal), ld3(in->v[1].normal), ld3(in->v[2].normal), u, v));
+    v3 albedo, normal;
+    surface(in, u, v, &albedo, &normal);
     v3 acc;
     if (emission_sum(&in->m) > 1e-7f) {
         albedo = mk(1.f, 1.f, 1.f);
@@ -504,8 +579,7 @@ static v3 path_radiance(const oscene* sc, v3 o, v3 d, uint32_t pixel, uint32_t f
         if (idx == INVALID_IDX) break;
         hit = add(muls(rd, t), ro);
         in = info_of(sc, idx);
-        albedo = normalize(bary(ld3(in->v[0].color), ld3(in->v[1].color), ld3(in->v[2].color), u, v));
-        normal = normalize(bary(ld3(in->v[0].normal), ld3(in->v[1].normal), ld3(in->v[2].normal), u, v));
+        surface(in, u, v, &albedo, &normal);
         v3 L = mk(0.f, 0.f, 0.f);
         if (emission_sum(&in->m) > 1e-7f) {
             L = muls(ld3(in->m.emission), gmax(dot(neg(rd), normal), 0.0f));
@@ -681,6 +755,30 @@ static double trace_d(const obvh* b, d3 o, d3 d, int any_hit, uint32_t* idx_out,
     return best;
 }
 
+/* surface() in double for the FP64 estimator (same sampler). */
+static void surface_d(const oinfo* in, double u, double v, d3* albedo, d3* normal)
+{
+    *normal = dnorm(dbary(dld(in->v[0].normal), dld(in->v[1].normal), dld(in->v[2].normal), u, v));
+    uint32_t ai = in->m.albedo_idx, ni = in->m.normal_idx;
+    int ta = ai < g_texture_count, tn = ni < g_texture_count;
+    if (!ta) *albedo = dnorm(dbary(dld(in->v[0].color), dld(in->v[1].color), dld(in->v[2].color), u, v));
+    if (!ta && !tn) return;
+    double w = 1.0 - u - v;
+    double tu = in->v[0].uv[0] * w + in->v[1].uv[0] * u + in->v[2].uv[0] * v;
+    double tv = in->v[0].uv[1] * w + in->v[1].uv[1] * u + in->v[2].uv[1] * v;
+    double s[4];
+    if (ta) {
+        tex_sample(&g_textures[ai], tu, tv, s);
+        *albedo = dmk(s[0], s[1], s[2]);
+    }
+    if (tn) {
+        tex_sample(&g_textures[ni], tu, tv, s);
+        d3 tg = dnorm(dbary(dld(in->v[0].tangent), dld(in->v[1].tangent), dld(in->v[2].tangent), u, v));
+        d3 bt = dnorm(dbary(dld(in->v[0].bitangent), dld(in->v[1].bitangent), dld(in->v[2].bitangent), u, v));
+        *normal = dnorm(dadd(dadd(dmuls(tg, 2 * s[0] - 1), dmuls(bt, 2 * s[1] - 1)), dmuls(*normal, 2 * s[2] - 1)));
+    }
+}
+
 static d3 path_radiance_d(const oscene* sc, d3 o, d3 d, uint32_t pixel, uint32_t frame)
 {
     uint32_t idx; double u = 0, v = 0;
@@ -688,8 +786,8 @@ static d3 path_radiance_d(const oscene* sc, d3 o, d3 d, uint32_t pixel, uint32_t
     if (idx == INVALID_IDX) return dmk(0, 0, 0);
     const oinfo* in = info_of(sc, idx);
     d3 hit = dadd(dmuls(d, t), o);
-    d3 albedo = dnorm(dbary(dld(in->v[0].color), dld(in->v[1].color), dld(in->v[2].color), u, v));
-    d3 normal = dnorm(dbary(dld(in->v[0].normal), dld(in->v[1].normal), dld(in->v[2].normal), u, v));
+    d3 albedo, normal;
+    surface_d(in, u, v, &albedo, &normal);
     d3 acc = dmk(0, 0, 0);
     if (emission_sum(&in->m) > 1e-7f) {
         albedo = dmk(1, 1, 1);
@@ -731,8 +829,7 @@ static d3 path_radiance_d(const oscene* sc, d3 o, d3 d, uint32_t pixel, uint32_t
         if (idx == INVALID_IDX) break;
         hit = dadd(dmuls(rd, t), ro);
         in = info_of(sc, idx);
-        albedo = dnorm(dbary(dld(in->v[0].color), dld(in->v[1].color), dld(in->v[2].color), u, v));
-        normal = dnorm(dbary(dld(in->v[0].normal), dld(in->v[1].normal), dld(in->v[2].normal), u, v));
+        surface_d(in, u, v, &albedo, &normal);
         d3 L = dmk(0, 0, 0);
         if (emission_sum(&in->m) > 1e-7f) {
             double c = -ddot(rd, normal);

@@ -53,6 +53,8 @@ def oracle_lib() -> ctypes.CDLL:
         L.orc_sincos_turns.argtypes = [P, U, P, P]
         L.orc_corner_dirs.argtypes = [ctypes.POINTER(OCam), U, U, U, P]
         L.orc_heatmap.argtypes = [P, P, ctypes.POINTER(OCam), U, U, P, P, P]
+        L.orc_set_textures.argtypes = [P, U]
+        L.orc_tex_sample.argtypes = [P, P, U, P]
         _oracle = L
     return _oracle
 
@@ -154,28 +156,70 @@ def ocam_from(eye, dirs, inv_view_proj=None, jitter=0, jitter_x=0.0, jitter_y=0.
     return c
 
 
+class OTex(ctypes.Structure):
+    _fields_ = [("rgba", ctypes.c_void_p), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32)]
+
+
+class _Textures:
+    """Installs a texture table (list of (H, W, 4) uint8 arrays) for one oracle call."""
+
+    def __init__(self, images):
+        self.images = [np.ascontiguousarray(im, np.uint8) for im in (images or [])]
+        self.table = (OTex * max(1, len(self.images)))()
+        for k, im in enumerate(self.images):
+            self.table[k] = OTex(im.ctypes.data, im.shape[1], im.shape[0])
+
+    def __enter__(self):
+        oracle_lib().orc_set_textures(ctypes.addressof(self.table) if self.images else None, len(self.images))
+        return self
+
+    def __exit__(self, *exc):
+        oracle_lib().orc_set_textures(None, 0)
+
+
+def tex_sample(image: np.ndarray, uv: np.ndarray) -> np.ndarray:
+    """tex2D<float4> of an (H, W, 4) uint8 image at (n, 2) float32 coordinates -> (n, 4)."""
+    image = np.ascontiguousarray(image, np.uint8)
+    uv = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    out = np.zeros((len(uv), 4), np.float32)
+    t = OTex(image.ctypes.data, image.shape[1], image.shape[0])
+    oracle_lib().orc_tex_sample(ctypes.addressof(t), _p(uv), len(uv), _p(out))
+    return out
+
+
 def render(b: BuildResult, infos: np.ndarray, lights, width: int, height: int, spp: int, frame0: int, bounces: int,
-           intensity: float, stratified: bool, seed: int, cam: OCam, rows=None, camera_index: int = 0):
-    """Per-sample radiance (spp, rows, width, 3) float32 and ray counts (3,)."""
+           intensity: float, stratified: bool, seed: int, cam: OCam, rows=None, camera_index: int = 0,
+           textures=None):
+    """Per-sample radiance (spp, rows, width, 3) float32 and ray counts (3,).
+
+    textures: list of (H, W, 4) uint8 images indexed by albedo_idx / normal_map_idx."""
     r0, r1 = (0, height) if rows is None else rows
     rad = np.zeros((spp, r1 - r0, width, 3), np.float32)
     counts = np.zeros(3, np.uint64)
     nl = 0 if lights is None else len(lights)
+    with _Textures(textures):
+        _render_call(b, infos, lights, nl, width, height, r0, r1, spp, frame0, bounces, intensity, stratified, seed,
+                     cam, camera_index, rad, counts)
+    return rad, counts
+
+
+def _render_call(b, infos, lights, nl, width, height, r0, r1, spp, frame0, bounces, intensity, stratified, seed, cam,
+                 camera_index, rad, counts):
     oracle_lib().orc_render(_p(b.tris), _p(b.children), _p(b.node_boxes), len(b.tris), _p(infos),
                             _p(lights) if nl else None, nl, width, height, r0, r1, spp, frame0, bounces, intensity,
                             int(stratified), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, ctypes.byref(cam),
                             camera_index, _p(rad), _p(counts))
-    return rad, counts
 
 
 def render_f64(b: BuildResult, infos: np.ndarray, lights, width: int, height: int, spp: int, frame0: int, bounces: int,
-               intensity: float, stratified: bool, seed: int, cam: OCam) -> np.ndarray:
+               intensity: float, stratified: bool, seed: int, cam: OCam, textures=None) -> np.ndarray:
     out = np.zeros((height, width, 3), np.float64)
     nl = 0 if lights is None else len(lights)
-    oracle_lib().orc_render_f64(_p(b.tris), _p(b.children), _p(b.node_boxes), len(b.tris), _p(infos),
-                                _p(lights) if nl else None, nl, width, height, spp, frame0, bounces, intensity,
-                                int(stratified), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, ctypes.byref(cam),
-                                _p(out))
+    with _Textures(textures):
+        oracle_lib().orc_render_f64(_p(b.tris), _p(b.children), _p(b.node_boxes), len(b.tris), _p(infos),
+                                    _p(lights) if nl else None, nl, width, height, spp, frame0, bounces, intensity,
+                                    int(stratified), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, ctypes.byref(cam),
+                                    _p(out))
     return out
 
 
