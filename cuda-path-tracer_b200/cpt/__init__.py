@@ -106,6 +106,12 @@ def _load() -> ctypes.CDLL:
 lib = _load()
 
 _P, _U32, _I32, _SZ, _F = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_size_t, ctypes.c_float
+
+
+class RcParams(ctypes.Structure):
+    _fields_ = [("learning_rate", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
+                ("epsilon", ctypes.c_float), ("ema_decay", ctypes.c_float), ("train_samples", ctypes.c_uint32),
+                ("train_steps", ctypes.c_uint32), ("seed", ctypes.c_uint32)]
 _PROTOS = {
     "cpt_bvh_bytes": (_SZ, [_U32, _I32]),
     "cpt_bvh_bind": (_I32, [_P, _SZ, _U32, _I32, ctypes.POINTER(Bvh)]),
@@ -121,6 +127,19 @@ _PROTOS = {
     "cpt_resolve": (_I32, [_P, _U32, _U32, _U32, _P, _P]),
     "cpt_render_views_scratch_bytes": (_SZ, [_P, _U32, ctypes.POINTER(RenderParams)]),
     "cpt_render_views": (_I32, [_P, _U32, ctypes.POINTER(RenderParams), _P, _SZ, _P, _P, _P]),
+    "cpt_rc_default_params": (None, [ctypes.POINTER(RcParams)]),
+    "cpt_rc_param_count": (_SZ, []),
+    "cpt_rc_create": (_I32, [ctypes.POINTER(_P), ctypes.POINTER(RcParams), _P]),
+    "cpt_rc_destroy": (None, [_P]),
+    "cpt_rc_reset": (_I32, [_P, _U32, _P]),
+    "cpt_rc_get_weights": (_I32, [_P, _P, _P]),
+    "cpt_rc_set_weights": (_I32, [_P, _P, _P]),
+    "cpt_rc_infer": (_I32, [_P, _P, _U32, _P, _P, _P]),
+    "cpt_rc_train": (_I32, [_P, _P, _U32, _P, _U32, ctypes.POINTER(_F), _P]),
+    "cpt_rc_render_scratch_bytes": (_SZ, [_P, _P, _U32, ctypes.POINTER(RenderParams)]),
+    "cpt_rc_render": (_I32, [_P, _P, _U32, ctypes.POINTER(RenderParams), _P, _SZ, _P, _P, _P]),
+    "cpt_rc_sample_count": (_I32, [_P, ctypes.POINTER(_U32), _P]),
+    "cpt_rc_samples": (_I32, [_P, ctypes.POINTER(_P)]),
     "cpt_tracer_create": (_I32, [ctypes.POINTER(_P), _I32]),
     "cpt_tracer_destroy": (None, [_P]),
     "cpt_tracer_upload": (_I32, [_P, _P, _U32, _P, _U32, _P, _U32, _P]),
@@ -288,7 +307,8 @@ def launch_count() -> int:
 
 RAY_COUNTS = 72
 KERNELS = ("k_bounds", "k_morton", "k_scan_offsets", "k_onesweep", "k_topology", "k_gather_refit", "k_trace",
-           "k_generate", "k_extend", "k_shade", "k_wave_counts", "k_accumulate", "k_resolve", "k_ray_sort")
+           "k_generate", "k_extend", "k_shade", "k_wave_counts", "k_accumulate", "k_resolve", "k_ray_sort",
+           "k_rc_infer", "k_rc_train", "k_rc_adam", "k_rc_collect")
 
 
 def profile_begin() -> None:

@@ -11,7 +11,7 @@ import torch
 
 import ctypes
 
-from . import (ACCUM_KAHAN, BBOX_DTYPE, BUILD_CHECK, TRIANGLE_DTYPE, Bvh, Camera, RenderParams, Scene, View, accum_bytes,
+from . import (ACCUM_KAHAN, BBOX_DTYPE, RcParams, BUILD_CHECK, TRIANGLE_DTYPE, Bvh, Camera, RenderParams, Scene, View, accum_bytes,
                bvh_bind, bvh_bytes, check, lbvh_build, lbvh_scratch_bytes, lib, render, render_scratch_bytes, resolve,
                status_check, texture_handles, trace)
 
@@ -195,3 +195,118 @@ class BatchRenderer:
 
     def check_status(self) -> None:
         status_check(self.status.data_ptr(), stream_handle())
+
+
+RC_LAYERS = ((96, 64), (64, 64), (64, 64), (64, 64), (64, 16))
+
+
+def rc_default_params(**kw) -> RcParams:
+    p = RcParams()
+    lib.cpt_rc_default_params(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class RadianceCache:
+    """The MLP radiance cache (cpt_rc_*): weights, Adam state and training buffers
+    on the device; cached rendering of views (list of (DeviceLbvh, DeviceScene,
+    Camera, width, height)) into per-view accumulators."""
+
+    def __init__(self, params: RcParams | None = None):
+        self.params = params or rc_default_params()
+        h = ctypes.c_void_p()
+        check(lib.cpt_rc_create(ctypes.byref(h), ctypes.byref(self.params), stream_handle()), "cpt_rc_create")
+        self._h = h
+        self.n_params = int(lib.cpt_rc_param_count())
+
+    def close(self) -> None:
+        if self._h:
+            lib.cpt_rc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reset(self, seed: int) -> None:
+        check(lib.cpt_rc_reset(self._h, seed, stream_handle()), "cpt_rc_reset")
+
+    def get_weights(self) -> list[np.ndarray]:
+        flat = np.empty(self.n_params, np.float32)
+        check(lib.cpt_rc_get_weights(self._h, flat.ctypes.data, stream_handle()), "cpt_rc_get_weights")
+        out, o = [], 0
+        for fi, fo in RC_LAYERS:
+            out.append(flat[o:o + fi * fo].reshape(fi, fo).copy())
+            o += fi * fo
+        return out
+
+    def set_weights(self, layers) -> None:
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(w, np.float32).reshape(-1) for w in layers]))
+        assert flat.size == self.n_params
+        check(lib.cpt_rc_set_weights(self._h, flat.ctypes.data, stream_handle()), "cpt_rc_set_weights")
+
+    def infer(self, samples: torch.Tensor, box) -> torch.Tensor:
+        """samples: (n, 16) float32 device tensor -> (n, 3) predictions."""
+        samples = samples.contiguous()
+        n = samples.shape[0]
+        out = torch.empty((n, 4), dtype=torch.float32, device=samples.device)
+        b = np.ascontiguousarray(box, np.float32)
+        check(lib.cpt_rc_infer(self._h, samples.data_ptr(), n, b.ctypes.data, out.data_ptr(), stream_handle()),
+              "cpt_rc_infer")
+        return out[:, :3]
+
+    def train(self, samples: torch.Tensor, box, steps: int = 1) -> float:
+        samples = samples.contiguous()
+        b = np.ascontiguousarray(box, np.float32)
+        loss = ctypes.c_float()
+        check(lib.cpt_rc_train(self._h, samples.data_ptr(), samples.shape[0], b.ctypes.data, steps,
+                               ctypes.byref(loss), stream_handle()), "cpt_rc_train")
+        return float(loss.value)
+
+    def sample_count(self) -> int:
+        n = ctypes.c_uint32()
+        check(lib.cpt_rc_sample_count(self._h, ctypes.byref(n), stream_handle()), "cpt_rc_sample_count")
+        return int(n.value)
+
+    def samples(self) -> np.ndarray:
+        """This frame's training samples (n, 16) as a host array."""
+        n = self.sample_count()
+        p = ctypes.c_void_p()
+        check(lib.cpt_rc_samples(self._h, ctypes.byref(p)), "cpt_rc_samples")
+        if n == 0:
+            return np.empty((0, 16), np.float32)
+        torch.cuda.synchronize()
+        return torch.as_tensor(_DeviceArray(p.value, (n, 16), "<f4"), device="cuda").cpu().numpy()
+
+
+class _DeviceArray:
+    """A library-owned device buffer seen through __cuda_array_interface__."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"data": (int(ptr), False), "shape": tuple(shape), "typestr": typestr,
+                                         "version": 3}
+
+
+class CachedRenderer(BatchRenderer):
+    """BatchRenderer whose frames go through the radiance cache (cpt_rc_render)."""
+
+    def __init__(self, cache: RadianceCache, views, params: RenderParams, device=None):
+        super().__init__(views, params, device)
+        self.cache = cache
+        self.rc_scratch_bytes = int(lib.cpt_rc_render_scratch_bytes(cache._h, self.views, len(self.accums),
+                                                                    ctypes.byref(params)))
+        if not self.rc_scratch_bytes:
+            raise ValueError("render parameters rejected")
+        self.rc_scratch = dev_bytes(self.rc_scratch_bytes, device)
+
+    def render(self, frame0: int | None = None, stream: int | None = None) -> None:
+        p = RenderParams.from_buffer_copy(self.params)
+        if frame0 is not None:
+            p.frame0 = frame0
+        check(lib.cpt_rc_render(self.cache._h, self.views, len(self.accums), ctypes.byref(p),
+                                self.rc_scratch.data_ptr(), self.rc_scratch_bytes, self.counts.data_ptr(),
+                                self.status.data_ptr(), stream_handle() if stream is None else stream),
+              "cpt_rc_render")

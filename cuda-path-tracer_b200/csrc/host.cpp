@@ -20,7 +20,8 @@ std::atomic<bool> g_profiling{false};
 
 const char* const kKernelNames[K_KERNEL_COUNT] = {
     "k_bounds", "k_morton", "k_scan_offsets", "k_onesweep", "k_topology", "k_gather_refit", "k_trace",
-    "k_generate", "k_extend", "k_shade", "k_wave_counts", "k_accumulate", "k_resolve", "k_ray_sort"};
+    "k_generate", "k_extend", "k_shade", "k_wave_counts", "k_accumulate", "k_resolve", "k_ray_sort",
+    "k_rc_infer", "k_rc_train", "k_rc_adam", "k_rc_collect"};
 
 namespace {
 struct ProfRecord { int id; cudaEvent_t a, b; };

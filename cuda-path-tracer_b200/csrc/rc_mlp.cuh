@@ -1,0 +1,277 @@
+// Radiance-cache network on the tensor cores: a 96 -> 64 -> 64 -> 64 -> 64 -> 16
+// ReLU MLP with BF16 weights and activations and FP32 accumulation, evaluated with
+// warp-level mma.sync m16n8k16 (one warp = 16 samples, every layer's activations
+// stay in registers between layers: the accumulator fragment of a layer is the A
+// fragment of the next after ReLU and a BF16 pack). Weights live in shared memory,
+// row-major [fan_in][fan_out] with 8 BF16 of padding per row so that ldmatrix rows
+// fall into distinct banks. The same layout serves the forward pass (B = W, loaded
+// transposed) and the backward pass (B = W^T, loaded as stored).
+//
+// The network and its encoding follow the radiance-cache workload (12-frequency
+// positional encoding, degree-4 spherical harmonics of the direction, normal,
+// albedo); the reference has no radiance cache, so there is nothing to match
+// bit for bit: the training loss and the rendered image's error against the FP64
+// estimator judge it.
+#pragma once
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace cpt {
+namespace rc {
+
+constexpr int kIn = 96;   // encoded input: 72 position + 16 SH + 3 normal + 3 albedo + 1 constant + 1 zero
+constexpr int kHid = 64;
+constexpr int kOut = 16;  // RGB, padded to two n-tiles
+constexpr int kLayers = 5;
+constexpr int kParams = kIn * kHid + 3 * kHid * kHid + kHid * kOut;  // 19456
+constexpr int kFreqs = 12;
+
+__host__ __device__ constexpr int fan_in(int l) { return l == 0 ? kIn : kHid; }
+__host__ __device__ constexpr int fan_out(int l) { return l == kLayers - 1 ? kOut : kHid; }
+__host__ __device__ constexpr int param_off(int l) { return l == 0 ? 0 : kIn * kHid + (l - 1) * kHid * kHid; }
+__host__ __device__ constexpr int w_stride(int l) { return fan_out(l) + 8; }
+__host__ __device__ constexpr int w_smem_off(int l) { return l == 0 ? 0 : kIn * (kHid + 8) + (l - 1) * kHid * (kHid + 8); }
+constexpr int kWSmem = kIn * (kHid + 8) + 3 * kHid * (kHid + 8) + kHid * (kOut + 8);  // BF16 elements
+constexpr int kXS = kIn + 8;   // row stride of encoded inputs (BF16)
+constexpr int kAS = kHid + 8;  // row stride of hidden activations / gradients
+constexpr int kZS = kOut + 8;  // row stride of output gradients
+
+// Sample layout shared by training and inference: 4 float4 =
+// (position, t.r) (direction, t.g) (normal, t.b) (albedo, unused), t = target.
+// Render records carry the same first four float4 (with the path id and the
+// path weight in the .w lanes) and a fifth.
+constexpr int kSampleF4 = 4;
+constexpr int kRecordF4 = 5;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void* p)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_addr(p)));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const void* p)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_addr(p)));
+}
+__device__ __forceinline__ void ldsm_x2_t(uint32_t (&r)[2], const void* p)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0, %1}, [%2];\n"
+                 : "=r"(r[0]), "=r"(r[1])
+                 : "r"(smem_addr(p)));
+}
+
+// D += A * B for one m16n8k16 tile, BF16 inputs, FP32 accumulators.
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ float2 unpack_bf16(uint32_t u)
+{
+    __nv_bfloat162 v = *reinterpret_cast<__nv_bfloat162*>(&u);
+    return __bfloat1622float2(v);
+}
+
+// ldmatrix addressing. Lane l supplies row (l & 7) of matrix (l >> 3).
+// A fragment of a row-major matrix S (rows r0.., cols k0..): matrices
+// (r0, k0) (r0+8, k0) (r0, k0+8) (r0+8, k0+8).
+__device__ __forceinline__ const __nv_bfloat16* frag_a(const __nv_bfloat16* s, int stride, int r0, int k0, int lane)
+{
+    const int g = lane >> 3, j = lane & 7;
+    return s + (r0 + j + (g & 1) * 8) * stride + k0 + (g >> 1) * 8;
+}
+// A fragment of S^T where S is row-major [k][m] (m0.., k0..), loaded with .trans:
+// matrices S(k0, m0) S(k0, m0+8) S(k0+8, m0) S(k0+8, m0+8).
+__device__ __forceinline__ const __nv_bfloat16* frag_at(const __nv_bfloat16* s, int stride, int m0, int k0, int lane)
+{
+    const int g = lane >> 3, j = lane & 7;
+    return s + (k0 + j + (g >> 1) * 8) * stride + m0 + (g & 1) * 8;
+}
+// B fragments of a row-major [k][n] matrix (loaded with .trans): x4 gives n-tiles
+// n0 (regs 0, 1) and n0+8 (regs 2, 3); x2 gives n-tile n0.
+__device__ __forceinline__ const __nv_bfloat16* frag_b(const __nv_bfloat16* s, int stride, int k0, int n0, int lane)
+{
+    const int g = lane >> 3, j = lane & 7;
+    return s + (k0 + j + (g & 1) * 8) * stride + n0 + (g >> 1) * 8;
+}
+// B fragments of W^T where W is row-major [n][k] (loaded as stored): x4 gives
+// n-tiles n0 (regs 0, 1) and n0+8 (regs 2, 3).
+__device__ __forceinline__ const __nv_bfloat16* frag_bt(const __nv_bfloat16* w, int stride, int k0, int n0, int lane)
+{
+    const int g = lane >> 3, j = lane & 7;
+    return w + (n0 + j + (g >> 1) * 8) * stride + k0 + (g & 1) * 8;
+}
+
+// Copies the BF16 parameters (row-major [in][out] per layer, packed) into the padded
+// shared-memory layout. All threads of the block take part.
+__device__ __forceinline__ void load_weights(const __nv_bfloat16* __restrict__ w, __nv_bfloat16* ws)
+{
+    // 8 BF16 (16 B) per chunk; every layer's rows are whole chunks.
+    constexpr int kChunks = kParams / 8;
+    for (int c = threadIdx.x; c < kChunks; c += blockDim.x) {
+        const int e = c * 8;
+        int l = 0;
+#pragma unroll
+        for (int k = 1; k < kLayers; ++k)
+            if (e >= param_off(k)) l = k;
+        const int local = e - param_off(l);
+        const int row = local / fan_out(l), col = local - row * fan_out(l);
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(w + e));
+        *reinterpret_cast<uint4*>(ws + w_smem_off(l) + row * w_stride(l) + col) = v;
+    }
+}
+
+// Real spherical harmonics, bands 0..3 (16 coefficients), of a unit vector; the
+// constants are the normalisations sqrt((2l+1)/(4 pi) (l-|m|)!/(l+|m|)!) (x sqrt 2
+// for m != 0) written out.
+__device__ __forceinline__ void sh16(float x, float y, float z, float (&o)[16])
+{
+    const float xx = x * x, yy = y * y, zz = z * z;
+    o[0] = 0.28209479177387814f;
+    o[1] = 0.4886025119029199f * y;
+    o[2] = 0.4886025119029199f * z;
+    o[3] = 0.4886025119029199f * x;
+    o[4] = 1.0925484305920792f * x * y;
+    o[5] = 1.0925484305920792f * y * z;
+    o[6] = 0.31539156525252005f * (3.0f * zz - 1.0f);
+    o[7] = 1.0925484305920792f * x * z;
+    o[8] = 0.5462742152960396f * (xx - yy);
+    o[9] = 0.5900435899266435f * y * (3.0f * xx - yy);
+    o[10] = 2.890611442640554f * x * y * z;
+    o[11] = 0.4570457994644658f * y * (5.0f * zz - 1.0f);
+    o[12] = 0.3731763325901154f * z * (5.0f * zz - 3.0f);
+    o[13] = 0.4570457994644658f * x * (5.0f * zz - 1.0f);
+    o[14] = 1.445305721320277f * z * (xx - yy);
+    o[15] = 0.5900435899266435f * x * (xx - 3.0f * yy);
+}
+
+// Writes half of one encoded row (BF16 pairs as 32-bit stores):
+//   half 0: position axes 0, 1 -> columns 0..47
+//   half 1: position axis 2 -> 48..71, SH(direction) -> 72..87, normal -> 88..90,
+//           albedo -> 91..93, constant 1 -> 94, 0 -> 95.
+// Position p = (x - box_min) / (box_max - box_min); column 24a + 2k holds
+// sin(pi 2^k p_a) and 24a + 2k + 1 its cosine. valid = false writes zeros.
+__device__ __forceinline__ void encode_half(const float4* f, bool valid, const float* bmin, const float* binv, int half,
+                                            __nv_bfloat16* row)
+{
+    uint32_t* out = reinterpret_cast<uint32_t*>(row);
+    if (!valid) {
+#pragma unroll
+        for (int k = 0; k < 24; ++k) out[half * 24 + k] = 0u;
+        return;
+    }
+    const float pos[3] = {f[0].x, f[0].y, f[0].z};
+    const int a0 = half == 0 ? 0 : 2, a1 = half == 0 ? 2 : 3;
+    for (int a = a0; a < a1; ++a) {
+        const float p = (pos[a] - bmin[a]) * binv[a];
+#pragma unroll
+        for (int k = 0; k < kFreqs; ++k) {
+            float s, c;
+            sincospif(ldexpf(p, k), &s, &c);
+            out[12 * a + k] = pack_bf16(s, c);
+        }
+    }
+    if (half == 1) {
+        float sh[16];
+        sh16(f[1].x, f[1].y, f[1].z, sh);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) out[36 + k] = pack_bf16(sh[2 * k], sh[2 * k + 1]);
+        out[44] = pack_bf16(f[2].x, f[2].y);
+        out[45] = pack_bf16(f[2].z, f[3].x);
+        out[46] = pack_bf16(f[3].y, f[3].z);
+        out[47] = pack_bf16(1.0f, 0.0f);
+    }
+}
+
+// Accumulator tiles -> A fragments of the next layer after ReLU (and the same
+// BF16 values into `store`, rows r0.. of a [rows][kAS] buffer, when non-null).
+__device__ __forceinline__ void relu_to_frags(const float (&acc)[8][4], uint32_t (&af)[4][4], __nv_bfloat16* store,
+                                              int r0, int lane)
+{
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) {
+        af[kt][0] = pack_bf16(fmaxf(acc[2 * kt][0], 0.f), fmaxf(acc[2 * kt][1], 0.f));
+        af[kt][1] = pack_bf16(fmaxf(acc[2 * kt][2], 0.f), fmaxf(acc[2 * kt][3], 0.f));
+        af[kt][2] = pack_bf16(fmaxf(acc[2 * kt + 1][0], 0.f), fmaxf(acc[2 * kt + 1][1], 0.f));
+        af[kt][3] = pack_bf16(fmaxf(acc[2 * kt + 1][2], 0.f), fmaxf(acc[2 * kt + 1][3], 0.f));
+    }
+    if (store) {
+        const int r = r0 + (lane >> 2), c = 2 * (lane & 3);
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt) {
+            *reinterpret_cast<uint32_t*>(store + r * kAS + 16 * kt + c) = af[kt][0];
+            *reinterpret_cast<uint32_t*>(store + (r + 8) * kAS + 16 * kt + c) = af[kt][1];
+            *reinterpret_cast<uint32_t*>(store + r * kAS + 16 * kt + 8 + c) = af[kt][2];
+            *reinterpret_cast<uint32_t*>(store + (r + 8) * kAS + 16 * kt + 8 + c) = af[kt][3];
+        }
+    }
+}
+
+// Forward pass of 16 rows (r0..r0+15 of the encoded input xs) through all layers.
+// acts (nullable): 4 buffers [rows][kAS] receiving the post-ReLU activations of the
+// hidden layers. y: output tiles (n-tile 0 = columns 0..7, n-tile 1 = 8..15).
+__device__ __forceinline__ void forward16(const __nv_bfloat16* ws, const __nv_bfloat16* xs, int r0,
+                                          __nv_bfloat16* const* acts, float (&y)[2][4], int lane)
+{
+    float acc[8][4];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+    const __nv_bfloat16* w0 = ws + w_smem_off(0);
+#pragma unroll
+    for (int kt = 0; kt < kIn / 16; ++kt) {
+        uint32_t a[4];
+        ldsm_x4(a, frag_a(xs, kXS, r0, 16 * kt, lane));
+#pragma unroll
+        for (int np = 0; np < 4; ++np) {
+            uint32_t b[4];
+            ldsm_x4_t(b, frag_b(w0, w_stride(0), 16 * kt, 16 * np, lane));
+            mma_bf16(acc[2 * np], a, b[0], b[1]);
+            mma_bf16(acc[2 * np + 1], a, b[2], b[3]);
+        }
+    }
+    uint32_t af[4][4];
+    relu_to_frags(acc, af, acts ? acts[0] : nullptr, r0, lane);
+#pragma unroll 1
+    for (int l = 1; l < kLayers - 1; ++l) {
+        const __nv_bfloat16* wl = ws + w_smem_off(l);
+#pragma unroll
+        for (int n = 0; n < 8; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt) {
+#pragma unroll
+            for (int np = 0; np < 4; ++np) {
+                uint32_t b[4];
+                ldsm_x4_t(b, frag_b(wl, w_stride(l), 16 * kt, 16 * np, lane));
+                mma_bf16(acc[2 * np], af[kt], b[0], b[1]);
+                mma_bf16(acc[2 * np + 1], af[kt], b[2], b[3]);
+            }
+        }
+        relu_to_frags(acc, af, acts ? acts[l] : nullptr, r0, lane);
+    }
+    const __nv_bfloat16* w4 = ws + w_smem_off(kLayers - 1);
+    y[0][0] = y[0][1] = y[0][2] = y[0][3] = 0.f;
+    y[1][0] = y[1][1] = y[1][2] = y[1][3] = 0.f;
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) {
+        uint32_t b[4];
+        ldsm_x4_t(b, frag_b(w4, w_stride(kLayers - 1), 16 * kt, 0, lane));
+        mma_bf16(y[0], af[kt], b[0], b[1]);
+        mma_bf16(y[1], af[kt], b[2], b[3]);
+    }
+}
+
+}  // namespace rc
+}  // namespace cpt

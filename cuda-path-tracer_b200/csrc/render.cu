@@ -28,6 +28,7 @@
 #include "cpt_internal.h"
 #include "traverse.cuh"
 #include "onesweep.cuh"
+#include "render_hook.h"
 
 namespace cpt {
 
@@ -76,6 +77,9 @@ struct Wave {
     float intensity;
     uint32_t stratified;
     uint32_t k0, k1;
+    float4* records;          // nullable: vertex records (RenderHook)
+    uint32_t* record_count;
+    uint32_t record_depth;
 };
 
 // Slot -> pixel: 8-row bands, column-major inside a band.
@@ -341,7 +345,7 @@ __device__ __forceinline__ void surface(const View& v, const cpt_triangle_info& 
     }
 }
 
-template <bool kLights>
+template <bool kLights, bool kRecord>
 __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32_t depth,
                                                        const float4* __restrict__ queue_in,
                                                        const float4* __restrict__ hits,
@@ -361,6 +365,8 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
         float4 nro = make_float4(0.f, 0.f, 0.f, 0.f), nrd = nro;
         uint32_t shadow = 0;
         bool bad_info = false;
+        bool rec = false;
+        float4 rec0, rec1, rec2, rec3, rec4;
         if (i < n) {
             const float4 ro = queue_in[2 * (size_t)i], rd4 = queue_in[2 * (size_t)i + 1];
             const float4 hit4 = hits[i];
@@ -423,6 +429,14 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
                 }
                 state[2 * (size_t)pid] = make_float4(acc.x, acc.y, acc.z, 0.f);
                 state[2 * (size_t)pid + 1] = make_float4(absorbed.x, absorbed.y, absorbed.z, 0.f);
+                if (kRecord && depth == wv.record_depth) {
+                    rec = true;
+                    rec0 = make_float4(hp.x, hp.y, hp.z, __uint_as_float(pid));
+                    rec1 = make_float4(d.x, d.y, d.z, __fmul_rn(absorbed.x, wv.intensity));
+                    rec2 = make_float4(normal.x, normal.y, normal.z, __fmul_rn(absorbed.y, wv.intensity));
+                    rec3 = make_float4(albedo.x, albedo.y, albedo.z, __fmul_rn(absorbed.z, wv.intensity));
+                    rec4 = make_float4(acc.x, acc.y, acc.z, 0.f);
+                }
                 if (depth < wv.bounces) {
                     // next direction (cuda_path_tracer.cu:269-284)
                     const uint32_t local = pid - v.pixel_base * wv.spw;
@@ -453,6 +467,17 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
         if (emit) {
             queue_out[2 * (size_t)q] = nro;
             queue_out[2 * (size_t)q + 1] = nrd;
+        }
+        if (kRecord) {
+            const uint32_t rq = warp_append(wv.record_count, rec);
+            if (rec) {
+                float4* r = wv.records + 5 * (size_t)rq;
+                r[0] = rec0;
+                r[1] = rec1;
+                r[2] = rec2;
+                r[3] = rec3;
+                r[4] = rec4;
+            }
         }
         if (kLights) warp_count_u64(ray_counts ? ray_counts + 2 : nullptr, shadow);
         if (bad_info) atomicOr(status, CPT_STATUS_BAD_INDEX);
@@ -544,6 +569,9 @@ __global__ void __launch_bounds__(256) k_resolve(const void* __restrict__ accum,
     }
 }
 
+constexpr int kCountWords = 2 * (kMaxDepth + 2) + 1;
+constexpr int kRecordCountWord = 2 * (kMaxDepth + 2);
+
 struct RenderScratch {
     float4* queue[2];
     float4* hits;
@@ -578,7 +606,7 @@ size_t render_layout(const cpt_render_params* p, uint64_t pixels, void* base, Re
     s.queue[1] = c.take<float4>(2ull * s.capacity);
     s.hits = c.take<float4>(s.capacity);
     s.state = c.take<float4>(2ull * s.capacity);
-    s.counts = c.take<uint32_t>(2 * (kMaxDepth + 2));  // queue counts, then persistent-kernel ray pools
+    s.counts = c.take<uint32_t>(kCountWords);  // queue counts, persistent-kernel ray pools, record count
     if (p->ray_sort) {
         const size_t tiles = (s.capacity + kSortTile - 1) / kSortTile;
         for (int k = 0; k < 2; ++k) {
@@ -701,7 +729,7 @@ uint64_t make_views(const cpt_view* views, uint32_t n, uint32_t ref_grid, Views&
 
 int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, const cpt_render_params* params,
                  void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
-                 cudaStream_t stream)
+                 const RenderHook* hook, cudaStream_t stream)
 {
     const uint64_t pixels = vs.total_pixels;
     if (!params_ok(params, pixels) || !scratch || !status) return CPT_ERR_INVALID_ARGUMENT;
@@ -718,6 +746,12 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
     wv.stratified = params->stratified;
     wv.k0 = params->seed_lo;
     wv.k1 = params->seed_hi;
+    const bool record = hook && hook->records;
+    if (record && hook->capacity < rs.capacity) return CPT_ERR_SCRATCH_TOO_SMALL;
+    wv.records = record ? hook->records : nullptr;
+    wv.record_count = rs.counts + kRecordCountWord;
+    wv.record_depth = hook ? hook->record_depth : 0u;
+    const bool image = !hook || hook->image_pass;
 
     bool one_bvh = true;
     for (uint32_t i = 1; i < vs.n; ++i) one_bvh &= vs.v[i].nodes == vs.v[0].nodes;
@@ -733,7 +767,7 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
         wv.s0 = s0;
         wv.spw = std::min(spw_max, params->spp - s0);
         const uint32_t paths = wv.spw * vs.total_pixels;
-        CPT_CUDA_TRY(cudaMemsetAsync(rs.counts, 0, sizeof(uint32_t) * 2 * (kMaxDepth + 2), stream));
+        CPT_CUDA_TRY(cudaMemsetAsync(rs.counts, 0, sizeof(uint32_t) * kCountWords, stream));
         {
             CPT_PROF(K_GENERATE, stream);
             k_generate<<<(int)std::min<uint32_t>((paths + kGenBlock - 1) / kGenBlock, (uint32_t)sms * 16), kGenBlock, 0,
@@ -766,14 +800,16 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
             CPT_LAUNCH_CHECK();
             {
                 CPT_PROF(K_SHADE, stream);
-                if (any_lights)
-                    k_shade<true><<<shade_blocks, kShadeBlock, 0, stream>>>(vs, wv, b, qin, rs.hits, rs.counts + b, qout,
-                                                                             rs.counts + b + 1, rs.state, ray_counts,
-                                                                             status);
-                else
-                    k_shade<false><<<shade_blocks, kShadeBlock, 0, stream>>>(vs, wv, b, qin, rs.hits, rs.counts + b, qout,
-                                                                              rs.counts + b + 1, rs.state, ray_counts,
-                                                                              status);
+#define CPT_SHADE(L, R)                                                                                          \
+    k_shade<L, R><<<shade_blocks, kShadeBlock, 0, stream>>>(vs, wv, b, qin, rs.hits, rs.counts + b, qout,        \
+                                                            rs.counts + b + 1, rs.state, ray_counts, status)
+                const bool rec_here = record && b == wv.record_depth;
+                if (any_lights) {
+                    if (rec_here) CPT_SHADE(true, true); else CPT_SHADE(true, false);
+                } else {
+                    if (rec_here) CPT_SHADE(false, true); else CPT_SHADE(false, false);
+                }
+#undef CPT_SHADE
             }
             CPT_LAUNCH_CHECK();
         }
@@ -784,13 +820,18 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
             }
             CPT_LAUNCH_CHECK();
         }
+        if (hook && hook->after_wave) {
+            const int rc = hook->after_wave(hook->ctx, hook->records, wv.record_count, hook->capacity, rs.state, stream);
+            if (rc != CPT_OK) return rc;
+        }
+        if (!image) continue;
         {
             CPT_PROF(K_ACCUMULATE, stream);
             k_accumulate<<<(vs.total_pixels + 255) / 256, 256, 0, stream>>>(wv, vs, params->accum_mode, rs.state);
         }
         CPT_LAUNCH_CHECK();
     }
-    if (params->frame_counter) {
+    if (params->frame_counter && image) {
         k_advance<<<1, 1, 0, stream>>>(params->frame_counter, params->spp);
         CPT_LAUNCH_CHECK();
     }
@@ -828,9 +869,29 @@ extern "C" size_t cpt_render_views_scratch_bytes(const cpt_view* views, uint32_t
     return render_layout(params, pixels, nullptr, nullptr);
 }
 
+size_t cpt::render_hook_layout(const cpt_view* views, uint32_t n_views, const cpt_render_params* params, void*,
+                               uint32_t* capacity)
+{
+    if (!views || n_views == 0 || n_views > CPT_MAX_VIEWS || !params) return 0;
+    uint64_t pixels = 0;
+    for (uint32_t i = 0; i < n_views; ++i) pixels += (uint64_t)views[i].width * views[i].height;
+    if (!params_ok(params, pixels)) return 0;
+    const uint64_t cap = pixels * wave_samples(params, pixels);
+    if (capacity) *capacity = std::max<uint32_t>(*capacity, (uint32_t)cap);
+    return align_up((size_t)cap * 5 * sizeof(float4), 256);
+}
+
 extern "C" int cpt_render_views(const cpt_view* views, uint32_t n_views, const cpt_render_params* params,
                                 void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
                                 cudaStream_t stream)
+{
+    return cpt::cpt_render_views_hooked(views, n_views, params, scratch, scratch_bytes, ray_counts, status, nullptr,
+                                        stream);
+}
+
+int cpt::cpt_render_views_hooked(const cpt_view* views, uint32_t n_views, const cpt_render_params* params,
+                                 void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
+                                 const RenderHook* hook, cudaStream_t stream)
 {
     if (!views || n_views == 0 || n_views > CPT_MAX_VIEWS || !params || !status) return CPT_ERR_INVALID_ARGUMENT;
     static Views vs;  // 14 KB: built on the host, passed by value to the kernels
@@ -839,7 +900,7 @@ extern "C" int cpt_render_views(const cpt_view* views, uint32_t n_views, const c
     if (!make_views(views, n_views, params->ref_grid, vs)) return CPT_ERR_INVALID_ARGUMENT;
     bool lights = false;
     for (uint32_t i = 0; i < n_views; ++i) lights |= views[i].scene->light_count > 0;
-    return render_views(vs, lights, views[0].bvh->node_boxes, params, scratch, scratch_bytes, ray_counts, status,
+    return render_views(vs, lights, views[0].bvh->node_boxes, params, scratch, scratch_bytes, ray_counts, status, hook,
                         stream);
 }
 

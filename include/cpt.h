@@ -304,6 +304,55 @@ void cpt_scene_bounds(const cpt_triangle* tris, uint32_t n, float out[6]);
 void cpt_camera_look_at(const float eye[3], const float target[3], const float up[3], float fov_deg, float aspect,
                         float znear, float zfar, cpt_camera* cam);
 
+/* ---- radiance cache (no reference counterpart: an extension judged by image
+ * error against the FP64 estimator, with plain path tracing as fallback) ----
+ * A 96 -> 4 x 64 (ReLU) -> 16 MLP (BF16 weights, FP32 accumulation) over the
+ * encoded secondary vertex: 12-frequency sin/cos encoding of the position in the
+ * scene box, real spherical harmonics bands 0-3 of the ray direction, normal,
+ * albedo. It predicts the radiance that the rest of a path (vertices 2 and on)
+ * brings to vertex 1, per unit throughput there; trained online with relative-L2
+ * loss and Adam on full-depth training paths of the same renderer.
+ * Samples (training and cpt_rc_infer) are 16 floats: position, target r,
+ * direction, target g, normal, target b, albedo, 0. Weights (cpt_rc_get/set) are
+ * FP32, per layer row-major [fan_in][fan_out], layers packed in order. */
+typedef struct cpt_rc cpt_rc;
+typedef struct cpt_rc_params {
+    float learning_rate;     /* 1e-2 */
+    float beta1, beta2;      /* 0.9, 0.99 */
+    float epsilon;           /* 1e-15 */
+    float ema_decay;         /* inference weights: 0 = the trained weights, else their moving average */
+    uint32_t train_samples;  /* training paths per frame, 65536 */
+    uint32_t train_steps;    /* optimizer steps per frame; the samples are split between them */
+    uint32_t seed;           /* weight initialisation */
+} cpt_rc_params;
+void cpt_rc_default_params(cpt_rc_params* p);
+size_t cpt_rc_param_count(void);
+int cpt_rc_create(cpt_rc** out, const cpt_rc_params* params /* nullable: defaults */, cudaStream_t stream);
+void cpt_rc_destroy(cpt_rc* rc);
+/* New random weights, optimizer state cleared. */
+int cpt_rc_reset(cpt_rc* rc, uint32_t seed, cudaStream_t stream);
+int cpt_rc_get_weights(cpt_rc* rc, float* host_out, cudaStream_t stream);
+int cpt_rc_set_weights(cpt_rc* rc, const float* host_in, cudaStream_t stream);
+/* Predictions for n device samples (16 floats each) -> out: n x (r, g, b, 0) on the device.
+ * box: host (min xyz, max xyz) normalising positions. Synchronizes the stream. */
+int cpt_rc_infer(cpt_rc* rc, const float* samples, uint32_t n, const float box[6], float* out, cudaStream_t stream);
+/* `steps` optimizer steps over n device samples split into equal batches; *loss_out
+ * (nullable) = mean relative L2 over the samples before their step. Synchronizes. */
+int cpt_rc_train(cpt_rc* rc, const float* samples, uint32_t n, const float box[6], uint32_t steps, float* loss_out,
+                 cudaStream_t stream);
+/* One cached frame of the views (as cpt_render_views): trains on this frame's
+ * training paths (train_samples full-depth paths over reduced copies of the views,
+ * an independent random stream), then renders vertices 0 and 1 exactly and the
+ * rest of each path from the cache. bounces < 2 renders plain paths. The position
+ * box is views[0].bvh's root box. */
+size_t cpt_rc_render_scratch_bytes(const cpt_rc* rc, const cpt_view* views, uint32_t n_views,
+                                   const cpt_render_params* params);
+int cpt_rc_render(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_render_params* params, void* scratch,
+                  size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status, cudaStream_t stream);
+/* Training samples collected by the last cpt_rc_render (device pointer, count). */
+int cpt_rc_sample_count(cpt_rc* rc, uint32_t* out, cudaStream_t stream);
+int cpt_rc_samples(cpt_rc* rc, const float** samples_dev);
+
 /* ---- profiling: CUDA events around every kernel launch of the library ----
  * Between begin and end, each launch is bracketed by two events recorded on its
  * own stream. end() synchronizes those events and adds their elapsed times to
