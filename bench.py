@@ -40,6 +40,10 @@ WORKLOADS = {
     # 64 scenes, 10k-2M triangles (log-uniform, alternating generators), 256^2-1024^2, one graph launch per frame
     "c3": dict(kind="batch", scenes=64, tri_min=10_000, tri_max=2_000_000, res_min=256, res_max=1024, spp=4,
                bounces=5, bits=63, seed=0, width=0, height=0),
+    # radiance cache on the C2 scene: 1 spp frames through the cache vs plain 16 spp, RMSE vs an FP64 image
+    "c4": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
+               bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, plain_spp=64, ref_spp=4096,
+               ref_div=4, warm_updates=4, max_spp=256),
     # deforming 16.8 M-triangle displaced sphere, full rebuild every frame, 8 cameras
     "c5": dict(kind="deform", nu=4096, nv=2048, n_hair=0, bits=63, width=1280, height=720, spp=1, bounces=7,
                eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, cameras=8, amp=0.01, omega=40.0),
@@ -72,6 +76,8 @@ def make_cameras(w):
 
 def workload_config(name, w, n_tris, l2_note):
     desc = {"c2": "fBm sphere 2048x1024x2 + 1M hairball + quad light",
+            "c4": "fBm sphere 2048x1024x2 + 1M hairball + quad light, radiance cache (96-64x4-16 BF16 MLP, 2^16 "
+                  "training paths/frame, Adam 1e-2) vs plain path tracing",
             "c1": "65,536 random triangles + quad light",
             "c5": "deforming fBm sphere 4096x2048x2 + quad light, rebuild every frame, 8 cameras",
             "c3": "64 scenes 10k-2M triangles (random / sphere+hairball alternating), 256^2-1024^2, 4 spp, "
@@ -642,6 +648,135 @@ def run_ours(args, w, world, rank, local):
     return 0
 
 
+def run_cache(args, w, world, rank, local):
+    """Time-to-equal-RMSE. The plain tracer renders plain_spp samples per pixel
+    (frames of 16 samples; time T_plain, error RMSE_plain against an
+    FP64-accumulated image of ref_spp samples). The cached tracer starts from
+    untrained weights: warm_updates training-only frames (cpt_rc_update), then
+    frames of `spp` samples (training + image) until its error reaches RMSE_plain
+    (time T_cache, warm-up included). value = T_cache / T_plain. The error is taken
+    on every ref_div-th pixel in x and y: the FP64 image is rendered at
+    (W / ref_div) x (H / ref_div), whose primary rays are exactly those of that
+    pixel subgrid (the ray through pixel x of W is the bilinear blend at x / W).
+    Both tracers use the reference's first-bounce stratification (8 x 8 strata
+    cycling over 64 samples); the same comparison without it is reported beside.
+    Frames are timed with CUDA events; the error checks between them are not."""
+    import torch
+
+    import cpt
+    from cpt.device import (BatchRenderer, CachedRenderer, DeviceLbvh, DeviceScene, RadianceCache, make_params,
+                            rc_default_params, to_device)
+
+    dev = torch.device("cuda", local if world > 1 else 0)
+    tris, infos = make_scene(w)
+    n = len(tris)
+    W_, H_ = w["width"], w["height"]
+    cam = make_cameras(w)[0]
+    lb = DeviceLbvh(n, w["bits"], dev)
+    lb.build(to_device(tris, dev), check_root=True)
+    scene = DeviceScene(infos, None, dev)
+    stream = torch.cuda.current_stream()
+    rdiv = w["ref_div"]
+    rw, rh = W_ // rdiv, H_ // rdiv
+    spf = w["spp"]
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    def experiment(stratified):
+        t0 = time.perf_counter()
+        refp = make_params(rw, rh, w["ref_spp"], 0, w["bounces"], 3.0, stratified, w["seed"] + 99991, cpt.ACCUM_F64)
+        ref = BatchRenderer([(lb, scene, cam, rw, rh)], refp, dev)
+        ref.render()
+        torch.cuda.synchronize()
+        ref.check_status()
+        ri = ref.accums[0].view(torch.float64).view(rh, rw, 4)
+        ref_img = ri[..., :3] / ri[..., 3:4].clamp(min=1)
+        ref_s = time.perf_counter() - t0
+        del ref
+
+        def rmse(acc):
+            a = acc.view(torch.float32).view(2, H_, W_, 4)[0]
+            img = (a[..., :3] / a[..., 3:4].clamp(min=1)).double()[::rdiv, ::rdiv][:rh, :rw]
+            return float(torch.sqrt(((img - ref_img) ** 2).mean()))
+
+        pp = make_params(W_, H_, 16, 0, w["bounces"], 3.0, stratified, w["seed"], cpt.ACCUM_KAHAN)
+        plain = BatchRenderer([(lb, scene, cam, W_, H_)], pp, dev)
+        for i in range(max(1, args.warmup)):
+            plain.render(frame0=100000 + 16 * i)
+        torch.cuda.synchronize()
+        plain.accums[0].zero_()
+        plain.counts.zero_()
+        t_plain = 0.0
+        for f in range(w["plain_spp"] // 16):
+            t_plain += timed(lambda: plain.render(frame0=16 * f))
+        plain.check_status()
+        rmse_plain = rmse(plain.accums[0])
+        plain_rays = int(plain.counts[:3].sum())
+        del plain
+
+        rc = RadianceCache(rc_default_params())
+        cp = make_params(W_, H_, spf, 0, w["bounces"], 3.0, stratified, w["seed"], cpt.ACCUM_KAHAN)
+        cr = CachedRenderer(rc, [(lb, scene, cam, W_, H_)], cp, dev)
+        cr.render(frame0=200000)  # warm the kernels on a throwaway network
+        torch.cuda.synchronize()
+        rc.reset(1337)
+        cr.accums[0].zero_()
+        cr.counts.zero_()
+        cpt.profile_begin()
+        launches0 = cpt.launch_count()
+        t_cache = 0.0
+        for u in range(w["warm_updates"]):
+            t_cache += timed(lambda: cr.update(frame0=300000 + u))
+        t_warm = t_cache
+        spp, curve, reached = 0, [], False
+        while spp < w["max_spp"]:
+            t_cache += timed(lambda: cr.render(frame0=spp))
+            spp += spf
+            e = rmse(cr.accums[0])
+            curve.append((spp, round(t_cache, 1), round(e, 6)))
+            if e <= rmse_plain:
+                reached = True
+                break
+        prof = cpt.profile_end()
+        launches = cpt.launch_count() - launches0
+        cr.check_status()
+        cache_rays = int(cr.counts[:3].sum())
+        rc.close()
+        return {"stratified": stratified, "ratio": round(t_cache / t_plain, 4) if reached else None,
+                "plain": {"spp": w["plain_spp"], "ms": round(t_plain, 2), "rmse": round(rmse_plain, 6),
+                          "mrays_s": round(plain_rays / t_plain / 1e3, 3)},
+                "cache": {"spp": spp, "spp_per_frame": spf, "warm_updates": w["warm_updates"],
+                          "warm_ms": round(t_warm, 2), "ms": round(t_cache, 2), "reached": reached,
+                          "rmse_curve": curve, "mrays_s": round(cache_rays / t_cache / 1e3, 3),
+                          "kernel_ms": {k: round(v[0], 3) for k, v in sorted(prof.items())}},
+                "reference": {"resolution": f"{rw}x{rh} (every {rdiv}th pixel of {W_}x{H_})",
+                              "spp": w["ref_spp"], "accum": "f64", "s": round(ref_s, 2)},
+                "launches": int(launches)}
+
+    main_run = experiment(True)
+    alt = experiment(False)
+    if rank == 0:
+        rc_p = rc_default_params()
+        line = {"metric": "time-to-equal-RMSE (cache / plain, vs FP64 image)", "value": main_run["ratio"],
+                "unit": "x", "n_gpus": world, "steps": main_run["cache"]["spp"] // spf, "warmup": args.warmup,
+                "ms_per_step": round(main_run["cache"]["ms"] / max(1, main_run["cache"]["spp"] // spf), 3),
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 tracing, bf16 MLP (f32 accumulate)", "data": "synthetic (seeded host generator)",
+                "config": workload_config("c4", w, n, "scene arrays 1.4 GB > 126 MB L2, no flush needed"),
+                "stratified": main_run, "unstratified": alt,
+                "rc_params": {"train_samples": rc_p.train_samples, "train_steps": rc_p.train_steps,
+                              "learning_rate": rc_p.learning_rate, "beta2": rc_p.beta2},
+                "gpu_launches": main_run["launches"]}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -670,6 +805,8 @@ def main():
     try:
         if w["kind"] == "batch":
             return run_batch(args, w, world, rank, local)
+        if args.workload == "c4":
+            return run_cache(args, w, world, rank, local)
         return run_ours(args, w, world, rank, local)
     finally:
         if world > 1:

@@ -138,6 +138,7 @@ _PROTOS = {
     "cpt_rc_train": (_I32, [_P, _P, _U32, _P, _U32, ctypes.POINTER(_F), _P]),
     "cpt_rc_render_scratch_bytes": (_SZ, [_P, _P, _U32, ctypes.POINTER(RenderParams)]),
     "cpt_rc_render": (_I32, [_P, _P, _U32, ctypes.POINTER(RenderParams), _P, _SZ, _P, _P, _P]),
+    "cpt_rc_update": (_I32, [_P, _P, _U32, ctypes.POINTER(RenderParams), _P, _SZ, _P, _P, _P]),
     "cpt_rc_sample_count": (_I32, [_P, ctypes.POINTER(_U32), _P]),
     "cpt_rc_samples": (_I32, [_P, ctypes.POINTER(_P)]),
     "cpt_tracer_create": (_I32, [ctypes.POINTER(_P), _I32]),

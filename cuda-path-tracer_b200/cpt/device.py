@@ -310,3 +310,13 @@ class CachedRenderer(BatchRenderer):
                                 self.rc_scratch.data_ptr(), self.rc_scratch_bytes, self.counts.data_ptr(),
                                 self.status.data_ptr(), stream_handle() if stream is None else stream),
               "cpt_rc_render")
+
+    def update(self, frame0: int | None = None, stream: int | None = None) -> None:
+        """Training paths and optimizer steps only (no image)."""
+        p = RenderParams.from_buffer_copy(self.params)
+        if frame0 is not None:
+            p.frame0 = frame0
+        check(lib.cpt_rc_update(self.cache._h, self.views, len(self.accums), ctypes.byref(p),
+                                self.rc_scratch.data_ptr(), self.rc_scratch_bytes, self.counts.data_ptr(),
+                                self.status.data_ptr(), stream_handle() if stream is None else stream),
+              "cpt_rc_update")

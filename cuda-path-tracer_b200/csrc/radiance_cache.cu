@@ -691,9 +691,10 @@ extern "C" size_t cpt_rc_render_scratch_bytes(const cpt_rc* rc, const cpt_view* 
     return std::max(a, b) + std::max(ra, rb);
 }
 
-extern "C" int cpt_rc_render(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_render_params* params,
-                             void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
-                             cudaStream_t stream)
+namespace {
+
+int rc_frame(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_render_params* params, void* scratch,
+             size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status, bool image, cudaStream_t stream)
 {
     if (!rc || !views || n_views == 0 || n_views > CPT_MAX_VIEWS || !params || !scratch || !status)
         return CPT_ERR_INVALID_ARGUMENT;
@@ -735,6 +736,7 @@ extern "C" int cpt_rc_render(cpt_rc* rc, const cpt_view* views, uint32_t n_views
             if (r) return r;
         }
     }
+    if (!image) return CPT_OK;
     // 3. the image: vertices 0 and 1 traced, the cache for the rest
     Ctx cr{rc, box, false};
     RenderHook h{};
@@ -745,6 +747,22 @@ extern "C" int cpt_rc_render(cpt_rc* rc, const cpt_view* views, uint32_t n_views
     h.after_wave = params->bounces >= 2 ? after_wave : nullptr;
     h.ctx = &cr;
     return cpt_render_views_hooked(views, n_views, &pr, scratch, render_part, ray_counts, status, &h, stream);
+}
+
+}  // namespace
+
+extern "C" int cpt_rc_render(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_render_params* params,
+                             void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
+                             cudaStream_t stream)
+{
+    return rc_frame(rc, views, n_views, params, scratch, scratch_bytes, ray_counts, status, true, stream);
+}
+
+extern "C" int cpt_rc_update(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_render_params* params,
+                             void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
+                             cudaStream_t stream)
+{
+    return rc_frame(rc, views, n_views, params, scratch, scratch_bytes, ray_counts, status, false, stream);
 }
 
 extern "C" int cpt_rc_sample_count(cpt_rc* rc, uint32_t* out, cudaStream_t stream)

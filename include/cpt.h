@@ -349,6 +349,10 @@ size_t cpt_rc_render_scratch_bytes(const cpt_rc* rc, const cpt_view* views, uint
                                    const cpt_render_params* params);
 int cpt_rc_render(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_render_params* params, void* scratch,
                   size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status, cudaStream_t stream);
+/* The training half of cpt_rc_render alone (training paths + optimizer steps, no
+ * image): warming a cache up, or following a scene change, without rendering. */
+int cpt_rc_update(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_render_params* params, void* scratch,
+                  size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status, cudaStream_t stream);
 /* Training samples collected by the last cpt_rc_render (device pointer, count). */
 int cpt_rc_sample_count(cpt_rc* rc, uint32_t* out, cudaStream_t stream);
 int cpt_rc_samples(cpt_rc* rc, const float** samples_dev);
