@@ -34,7 +34,7 @@ sys.path.insert(0, os.path.join(ROOT, "cuda-path-tracer_b200"))
 
 WORKLOADS = {
     "c2": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
-               bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0),
+               bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, split=1.0),
     "c1": dict(kind="random", n=65536, bits=30, width=512, height=512, spp=1, bounces=3, eye=(0.5, 0.5, -1.2),
                target=(0.5, 0.5, 0.0), seed=0),
     # 64 scenes, 10k-2M triangles (log-uniform, alternating generators), 256^2-1024^2, one graph launch per frame
@@ -43,10 +43,10 @@ WORKLOADS = {
     # radiance cache on the C2 scene: 1 spp frames through the cache vs plain 16 spp, RMSE vs an FP64 image
     "c4": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
                bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, plain_spp=64, ref_spp=4096,
-               ref_div=4, warm_updates=4, max_spp=256),
+               ref_div=4, warm_updates=4, max_spp=256, split=1.0),
     # deforming 16.8 M-triangle displaced sphere, full rebuild every frame, 8 cameras
     "c5": dict(kind="deform", nu=4096, nv=2048, n_hair=0, bits=63, width=1280, height=720, spp=1, bounces=7,
-               eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, cameras=8, amp=0.01, omega=40.0),
+               eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, cameras=8, amp=0.01, omega=40.0, cache=True),
 }
 METRIC = "Mrays/s"
 
@@ -79,7 +79,8 @@ def workload_config(name, w, n_tris, l2_note):
             "c4": "fBm sphere 2048x1024x2 + 1M hairball + quad light, radiance cache (96-64x4-16 BF16 MLP, 2^16 "
                   "training paths/frame, Adam 1e-2) vs plain path tracing",
             "c1": "65,536 random triangles + quad light",
-            "c5": "deforming fBm sphere 4096x2048x2 + quad light, rebuild every frame, 8 cameras",
+            "c5": "deforming fBm sphere 4096x2048x2 + quad light, rebuild every frame, 8 cameras, radiance cache "
+                  "(trained across the deforming frames)",
             "c3": "64 scenes 10k-2M triangles (random / sphere+hairball alternating), 256^2-1024^2, 4 spp, "
                   "depth 6, one CUDA-graph launch per frame, autotuned wave"}[name]
     c = {"workload": f"{name}: {desc}",
@@ -457,6 +458,9 @@ def run_ours(args, w, world, rank, local):
     scene = DeviceScene(infos, None, dev)
     lb = DeviceLbvh(n, w["bits"], dev)
     lb.build(d_tris, check_root=True)
+    split = w.get("split", 0.0) if args.split is None else args.split
+    if split > 0:
+        lb.split(split, keep_scratch=True)
     params = make_params(W_, H_, spp, 0, w["bounces"], 3.0, True, w["seed"], cpt.ACCUM_KAHAN,
                          wave_paths=args.wave_paths, ray_sort=bool(args.ray_sort), cameras=len(cams))
 
@@ -465,8 +469,19 @@ def run_ours(args, w, world, rank, local):
         cpt.check(cpt.lib.cpt_scene_deform(d_rest.data_ptr(), d_tris.data_ptr(), n, w["amp"], w["omega"],
                                            0.1 * frame_index, stream_handle()), "cpt_scene_deform")
         lb.build(d_tris)
+        if split > 0:
+            lb.split(split, keep_scratch=True)
     rend = DeviceRenderer(params, dev)
     stream = torch.cuda.current_stream()
+    cached = None
+    if w.get("cache"):
+        # every camera is a view of the same BVH; the cache trains on all of them
+        from cpt.device import CachedRenderer, RadianceCache
+
+        rcache = RadianceCache()
+        cparams = make_params(W_, H_, spp, 0, w["bounces"], 3.0, True, w["seed"], cpt.ACCUM_KAHAN,
+                              wave_paths=args.wave_paths)
+        cached = CachedRenderer(rcache, [(lb, scene, c_, W_, H_) for c_ in cams], cparams, dev)
 
     # --- one instrumented frame: node fetches and triangle tests per closest-hit ray
     rend.reset()
@@ -484,13 +499,22 @@ def run_ours(args, w, world, rank, local):
 
     rend.reset()
     frame = 0
+
+    def frame_step(f0):
+        if cached is not None:
+            cached.render(frame0=f0)
+        else:
+            rend.render(lb, scene, cam, frame0=f0)
+
     for i in range(args.warmup):
         if deforming:
             deform_and_rebuild(i)
-        rend.render(lb, scene, cam, frame0=rank_frame0(frame, rank))
+        frame_step(rank_frame0(frame, rank))
         frame += spp
     torch.cuda.synchronize()
     rend.counts.zero_()
+    if cached is not None:
+        cached.counts.zero_()
 
     # --- timed frames
     sampler = ClockSampler(local if world > 1 else 0) if rank == 0 else None
@@ -507,10 +531,11 @@ def run_ours(args, w, world, rank, local):
     for k in range(args.steps):
         if deforming:
             deform_and_rebuild(args.warmup + k)
-        rend.render(lb, scene, cam, frame0=rank_frame0(frame, rank))
+        frame_step(rank_frame0(frame, rank))
         frame += spp
         if world > 1:  # the one exchange of the path: framebuffer reduce to rank 0 every frame
-            reduce_accumulator(rend.accum, dst=0)
+            for acc in (cached.accums if cached is not None else [rend.accum]):
+                reduce_accumulator(acc, dst=0)
     ev1.record(stream)
     torch.cuda.synchronize()
     prof = cpt.profile_end()
@@ -518,8 +543,10 @@ def run_ours(args, w, world, rank, local):
     launches = cpt.launch_count() - launches0
     clocks = sampler.stop() if sampler else None
     rend.check_status()
+    if cached is not None:
+        cached.check_status()
     ms_total = ev0.elapsed_time(ev1)
-    counts = rend.counts.cpu().numpy()
+    counts = (cached.counts if cached is not None else rend.counts).cpu().numpy()
     rays_local = int(counts[0] + counts[1] + counts[2])
     ms_max = max_over_ranks(ms_total, world)
     rays_all = sum_over_ranks(rays_local, world)
@@ -536,7 +563,8 @@ def run_ours(args, w, world, rank, local):
     if args.workload == "c2" and os.path.exists(tp):  # ncu figure of the C2 traversal (see that file)
         import re
 
-        m = re.search(r"dram_bytes_per_closest_ray = ([0-9.]+)", open(tp).read())
+        key = "dram_bytes_per_closest_ray_split" if split > 0 else "dram_bytes_per_closest_ray"
+        m = re.search(key + r" = ([0-9.]+)", open(tp).read())
         if m:
             traffic = round(float(m.group(1)) * rays_closest / max(ext_launches, 1), 1)
     roofline = {"bound": "hbm", "kernel": "k_extend", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -547,6 +575,31 @@ def run_ours(args, w, world, rank, local):
                 "bytes_per_ray": f"32 ray + 16 hit + 64 x {mean_nodes:.2f} nodes + 48 x {mean_tris:.2f} triangles",
                 "rays_per_depth_first_frame": depth_rays,
                 "kernel_share": {k: round(v[0] / ms_total, 4) for k, v in sorted(prof.items())}}
+
+    # --- the same frame over the LBVH itself (no split BVH), for comparison
+    lbvh_topology = None
+    if split > 0 and not deforming and cached is None:
+        lb.unsplit()
+        rend.render(lb, scene, cam, frame0=rank_frame0(frame, rank))
+        torch.cuda.synchronize()
+        rend.counts.zero_()
+        u0, u1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        u0.record(stream)
+        rend.render(lb, scene, cam, frame0=rank_frame0(frame + spp, rank))
+        u1.record(stream)
+        torch.cuda.synchronize()
+        u_ms = max_over_ranks(u0.elapsed_time(u1), world)
+        u_rays = sum_over_ranks(int(rend.counts[:3].sum()), world)
+        lbvh_topology = {"mrays_s": round(u_rays / (u_ms / 1e3) / 1e6, 3), "ms_per_step": round(u_ms, 3),
+                         "note": "one frame traversing the reference-topology LBVH instead of the split BVH"}
+        lb.split(split, keep_scratch=True)
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        lb.split(split, keep_scratch=True)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        lbvh_topology["split_build_ms"] = round(s0.elapsed_time(s1), 3)
 
     # --- LBVH build of the same scene (device-resident triangles); the deforming
     # workload already rebuilt inside every timed step: those builds are reported
@@ -586,6 +639,7 @@ def run_ours(args, w, world, rank, local):
     e2e = None
     if not args.no_e2e and not deforming:
         tr = cpt.Tracer(w["bits"])
+        tr.set_split(split)
         tr.set_settings(bounces=w["bounces"], intensity=3.0, stratified=True, seed=w["seed"] + 7919 * rank)
         # (the tracer object renders frame 0 of its own seed on every rank: e2e ranks are replicas)
         tr.set_camera(cams[0])
@@ -624,7 +678,9 @@ def run_ours(args, w, world, rank, local):
         e2e = {"value": round(e_rays_all / (e_ms_max / 1e3) / 1e6, 3), "unit": METRIC,
                "h2d_bytes_per_step": int(tris.nbytes + infos.nbytes), "d2h_bytes_per_step": int(W_ * H_ * 16),
                "ms_per_step": round(e_ms_max / ne, 3), "wall_ms_per_step": round(1e3 * wall / ne, 3),
-               "steps": ne, "includes": "H2D soup+shading records (pinned), LBVH build, 16-spp frame, D2H image"}
+               "steps": ne, "includes": "H2D soup+shading records (pinned), LBVH build"
+                                        + (f", split BVH build (extra {split})" if split > 0 else "")
+                                        + ", 16-spp frame, D2H image"}
         tr.close()
 
     # --- CPU baseline (rank 0, N = 1)
@@ -640,6 +696,8 @@ def run_ours(args, w, world, rank, local):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded host generator)",
                 "config": workload_config(args.workload, w, n, "scene arrays 1.4 GB > 126 MB L2, no flush needed"),
                 "rays_per_step": int(rays_all / args.steps), "roofline": roofline, "lbvh": lbvh,
+                "traversal_bvh": (f"split BVH (cpt_lbvh_split, extra pieces {split} x n)" if split > 0
+                                  else "LBVH (reference topology)"), "lbvh_topology": lbvh_topology,
                 "cpu_baseline": cpu_base, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
                 "parallelism": f"replicas x{world}: own BVH per GPU, disjoint sample streams, "
                                f"framebuffer reduce to rank 0 per frame" if world > 1 else "1 GPU",
@@ -674,6 +732,9 @@ def run_cache(args, w, world, rank, local):
     cam = make_cameras(w)[0]
     lb = DeviceLbvh(n, w["bits"], dev)
     lb.build(to_device(tris, dev), check_root=True)
+    split = w.get("split", 0.0) if args.split is None else args.split
+    if split > 0:
+        lb.split(split)
     scene = DeviceScene(infos, None, dev)
     stream = torch.cuda.current_stream()
     rdiv = w["ref_div"]
@@ -791,6 +852,8 @@ def main():
     ap.add_argument("--spp", type=int, default=None, help="override samples per frame (profiling runs)")
     ap.add_argument("--wave-paths", type=int, default=0, help="paths per wave (0: library default)")
     ap.add_argument("--ray-sort", type=int, default=0, help="1: coherence-sort bounce queues")
+    ap.add_argument("--split", type=float, default=None,
+                    help="split traversal BVH extra-piece ratio (0: traverse the LBVH; default per workload)")
     args = ap.parse_args()
     w = dict(WORKLOADS[args.workload])
     if args.res:

@@ -62,7 +62,7 @@ class Bvh(ctypes.Structure):
     _fields_ = [("n", ctypes.c_uint32), ("morton_bits", ctypes.c_int32), ("tris", ctypes.c_void_p),
                 ("keys", ctypes.c_void_p), ("children", ctypes.c_void_p), ("parents_leaf", ctypes.c_void_p),
                 ("parents_internal", ctypes.c_void_p), ("node_boxes", ctypes.c_void_p), ("nodes", ctypes.c_void_p),
-                ("status", ctypes.c_void_p)]
+                ("status", ctypes.c_void_p), ("split_nodes", ctypes.c_void_p), ("split_capacity", ctypes.c_uint32)]
 
 
 class Scene(ctypes.Structure):
@@ -145,6 +145,7 @@ _PROTOS = {
     "cpt_tracer_destroy": (None, [_P]),
     "cpt_tracer_upload": (_I32, [_P, _P, _U32, _P, _U32, _P, _U32, _P]),
     "cpt_tracer_upload_textures": (_I32, [_P, _P, _U32]),
+    "cpt_tracer_set_split": (_I32, [_P, _F]),
     "cpt_tracer_set_primary_rays": (_I32, [_P, _P]),
     "cpt_tracer_set_eye": (_I32, [_P, _P]),
     "cpt_tracer_set_camera": (_I32, [_P, ctypes.POINTER(Camera)]),
@@ -163,6 +164,8 @@ _PROTOS = {
     "cpt_texture_create": (_I32, [_P, _U32, _U32, ctypes.POINTER(ctypes.c_uint64)]),
     "cpt_texture_destroy": (None, [ctypes.c_uint64]),
     "cpt_texture_sample": (_I32, [ctypes.c_uint64, _P, _U32, _P, _P]),
+    "cpt_lbvh_split_bytes": (_SZ, [_U32, _I32, _F, ctypes.POINTER(_SZ)]),
+    "cpt_lbvh_split": (_I32, [ctypes.POINTER(Bvh), _F, _P, _SZ, _P, _SZ, _P]),
     "cpt_obj_load": (_I32, [ctypes.c_char_p, _F, _P, _F, _P, _P, _U32, ctypes.POINTER(_U32)]),
     "cpt_bvh_heatmap": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Camera), _U32, _U32, _P, _P, _P, _P]),
     "cpt_camera_look_at": (None, [_P, _P, _P, _F, _F, _F, _F, ctypes.POINTER(Camera)]),
@@ -386,6 +389,9 @@ class Tracer:
         box_arr = None if box is None else np.ascontiguousarray(box, np.float32)
         check(lib.cpt_tracer_upload(self._h, _ptr(tris), len(tris), _ptr(infos), len(infos), lp, nl,
                                     None if box_arr is None else _ptr(box_arr)), "cpt_tracer_upload")
+
+    def set_split(self, extra_ratio: float) -> None:
+        check(lib.cpt_tracer_set_split(self._h, float(extra_ratio)), "cpt_tracer_set_split")
 
     def upload_textures(self, textures) -> None:
         table = texture_handles(textures)

@@ -438,6 +438,11 @@ struct cpt_tracer {
     size_t infos_cap = 0;
     void* d_lights = nullptr;
     size_t lights_cap = 0;
+    void* d_split_nodes = nullptr;  // split traversal BVH (cpt_tracer_set_split)
+    size_t split_nodes_cap = 0;
+    void* d_split_scratch = nullptr;
+    size_t split_scratch_cap = 0;
+    float split_ratio = 0.f;  // 0: traverse the LBVH itself
     void* d_textures = nullptr;  // cudaTextureObject_t handles (the caller owns the textures)
     size_t textures_cap = 0;
     uint32_t texture_count = 0;
@@ -493,7 +498,7 @@ extern "C" void cpt_tracer_destroy(cpt_tracer* t)
     if (!t) return;
     if (t->stream) cudaStreamSynchronize(t->stream);
     void* bufs[] = {t->d_tris, t->d_bvh, t->d_build_scratch, t->d_infos, t->d_lights, t->d_textures, t->d_accum,
-                    t->d_render_scratch, t->d_image, t->d_counts};
+                    t->d_render_scratch, t->d_image, t->d_counts, t->d_split_nodes, t->d_split_scratch};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (t->stream) cudaStreamDestroy(t->stream);
@@ -523,12 +528,29 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
     rc = cpt_lbvh_build(static_cast<const cpt_triangle*>(t->d_tris), n, enclosing_box, t->bits, &t->bvh,
                         t->d_build_scratch, t->build_cap, 0, t->stream);
     if (rc) return rc;
+    if (t->split_ratio > 0.f) {
+        size_t nb = 0;
+        const size_t sb = cpt_lbvh_split_bytes(n, t->bits, t->split_ratio, &nb);
+        if (!sb) return CPT_ERR_INVALID_ARGUMENT;
+        if ((rc = ensure(&t->d_split_nodes, &t->split_nodes_cap, nb))) return rc;
+        if ((rc = ensure(&t->d_split_scratch, &t->split_scratch_cap, sb))) return rc;
+        rc = cpt_lbvh_split(&t->bvh, t->split_ratio, t->d_split_nodes, t->split_nodes_cap, t->d_split_scratch,
+                            t->split_scratch_cap, t->stream);
+        if (rc) return rc;
+    }
     t->n = n;
     t->info_count = info_count;
     t->light_count = light_count;
     t->frame = 0;  // CUDAPathTracer::upload resets the frame counter (cuda_path_tracer.cu:469)
     t->ready = true;
     CPT_CUDA_TRY(cudaMemsetAsync(t->d_counts, 0, CPT_RAY_COUNTS * sizeof(unsigned long long), t->stream));
+    return CPT_OK;
+}
+
+extern "C" int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio)
+{
+    if (!t || !(extra_ratio >= 0.f) || !(extra_ratio <= 64.f)) return CPT_ERR_INVALID_ARGUMENT;
+    t->split_ratio = extra_ratio;
     return CPT_OK;
 }
 

@@ -29,39 +29,13 @@
 #include "cpt_device.cuh"
 #include "cpt_internal.h"
 #include "onesweep.cuh"
+#include "lbvh_common.cuh"
 
 namespace cpt {
 
 constexpr int kMortonBlock = 256;
 constexpr int kBoundsBlock = 256;
 constexpr int kBoundsBlocks = 1024;
-
-template <typename K> struct KeyTraits;
-template <> struct KeyTraits<uint32_t> { static constexpr int passes = 4, order = 10, total_bits = 32; };
-template <> struct KeyTraits<uint64_t> { static constexpr int passes = 8, order = 21, total_bits = 64; };
-
-// Bit spreading for the 3-D interleave (x -> bit 3i, y -> 3i+1, z -> 3i+2, the
-// layout of morton.h:63-102): the standard shift-and-mask "part 1 by 2" sequence
-// on 64 bits, valid for inputs of up to 21 bits.
-__device__ __forceinline__ uint64_t spread3(uint32_t v)
-{
-    uint64_t x = v & 0x1FFFFFull;
-    x = (x | (x << 32)) & 0x001F00000000FFFFull;
-    x = (x | (x << 16)) & 0x001F0000FF0000FFull;
-    x = (x | (x << 8)) & 0x100F00F00F00F00Full;
-    x = (x | (x << 4)) & 0x10C30C30C30C30C3ull;
-    x = (x | (x << 2)) & 0x1249249249249249ull;
-    return x;
-}
-
-// quantize (math_util.h:10-13): clamp(int(x * n), 0, n - 1); cvt.rzi saturates and maps NaN to 0.
-__device__ __forceinline__ uint32_t quantize(float x, uint32_t n)
-{
-    int32_t q = __float2int_rz(__fmul_rn(x, (float)n));
-    int32_t hi = (int32_t)(n - 1);
-    q = q < hi ? q : hi;
-    return (uint32_t)(q > 0 ? q : 0);
-}
 
 struct BoxArg {
     float mn[3];
@@ -171,60 +145,7 @@ __global__ void __launch_bounds__(kMortonBlock) k_morton(const float* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// Karras radix tree over the sorted keys (BVHBuilder.cu:107-201). Also writes
-// the Node word into the traversal record, zeroes the refit counters and marks
-// the root's parent.
-// ---------------------------------------------------------------------------
-template <typename K>
-__device__ __forceinline__ int key_delta(const K* __restrict__ keys, K ki, int n, int i, int j)
-{
-    if (j < 0 || j >= n) return -1;
-    K kj = __ldg(keys + j);
-    if (ki == kj) return __clz(i ^ j) + KeyTraits<K>::total_bits;
-    if (sizeof(K) == 8) return __clzll((long long)(ki ^ kj));
-    return __clz((int)(ki ^ kj));
-}
-
-template <typename K>
-__global__ void __launch_bounds__(256) k_topology(const K* __restrict__ keys, uint32_t n, uint32_t* __restrict__ children,
-                                                  uint32_t* __restrict__ parents_leaf,
-                                                  uint32_t* __restrict__ parents_internal, int* __restrict__ counters,
-                                                  float4* __restrict__ nodes)
-{
-    const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    const int nn = (int)n;
-    if (i >= nn - 1) return;
-    const K ki = keys[i];
-    int dd = key_delta(keys, ki, nn, i, i + 1) - key_delta(keys, ki, nn, i, i - 1);
-    int d = (dd > 0) - (dd < 0);
-    int dmin = key_delta(keys, ki, nn, i, i - d);
-    int lmax = 2;
-    while (key_delta(keys, ki, nn, i, i + lmax * d) > dmin) lmax *= 2;
-    int l = 0;
-    while (lmax > 1) {
-        lmax /= 2;
-        if (key_delta(keys, ki, nn, i, i + (l + lmax) * d) > dmin) l += lmax;
-    }
-    const int j = i + l * d;
-    const int dnode = key_delta(keys, ki, nn, i, j);
-    int s = 0;
-    while (l > 1) {
-        l = (l + 1) / 2;
-        if (key_delta(keys, ki, nn, i, i + (s + l) * d) > dnode) s += l;
-    }
-    s = i + s * d + (d < 0 ? d : 0);
-    uint32_t type = 0;
-    if (min(i, j) != s) { type |= 1u; parents_internal[s] = (uint32_t)i; }
-    else parents_leaf[s] = (uint32_t)i;
-    if (max(i, j) != s + 1) { type |= 2u; parents_internal[s + 1] = (uint32_t)i; }
-    else parents_leaf[s + 1] = (uint32_t)i;
-    const uint32_t word = ((uint32_t)s << 2) | type;
-    children[i] = word;
-    nodes[6 * (size_t)i + 5] = make_float4(__uint_as_float(word), 0.0f, 0.0f, 0.0f);
-    counters[i] = 0;
-    if (i == 0) parents_internal[0] = CPT_INVALID_INDEX;
-}
-
+// Karras radix tree: k_topology (lbvh_common.cuh).
 // ---------------------------------------------------------------------------
 // Triangle permutation fused with the bottom-up refit. Thread i gathers sorted
 // triangle i (the 40-B reference record), computes its leaf box, then walks up.
@@ -236,30 +157,6 @@ __global__ void __launch_bounds__(256) k_topology(const K* __restrict__ keys, ui
 // Release/acquire fences order those stores before the counter (the reference's
 // refit has no fence, BVHBuilder.cu:63-86).
 // ---------------------------------------------------------------------------
-struct Box { float mn[3], mx[3]; };
-
-// 40-B slot at float offset 10*side of a 96-B node; 8-B aligned float2 stores.
-__device__ __forceinline__ void store_slot(float* node, int side, const float s[10])
-{
-    float2* p = reinterpret_cast<float2*>(node + 10 * side);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) p[k] = make_float2(s[2 * k], s[2 * k + 1]);
-}
-
-__device__ __forceinline__ Box leaf_box(const float v[9])
-{
-    Box b;
-#pragma unroll
-    for (int ax = 0; ax < 3; ++ax) {
-        float mn = FLT_MAX, mx = -FLT_MAX;
-#pragma unroll
-        for (int vv = 0; vv < 3; ++vv) { mn = gmin(mn, v[3 * vv + ax]); mx = gmax(mx, v[3 * vv + ax]); }
-        b.mn[ax] = mn;
-        b.mx[ax] = mx;
-    }
-    return b;
-}
-
 __global__ void __launch_bounds__(256) k_gather_refit(const float* __restrict__ tris_in, const uint32_t* __restrict__ order,
                                                       uint32_t n, float* __restrict__ tris_out,
                                                       const uint32_t* __restrict__ children,
@@ -280,8 +177,8 @@ __global__ void __launch_bounds__(256) k_gather_refit(const float* __restrict__ 
     float2* o2 = reinterpret_cast<float2*>(tris_out + 10ull * i);
     o2[0] = a; o2[1] = b; o2[2] = c; o2[3] = d; o2[4] = e;
     const float v[9] = {a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x};
-    // leaf slot: v0, info, v1 - v0, v2 - v0
-    float slot[10] = {v[0], v[1], v[2], e.y,
+    // leaf slot: v0, the leaf's index (the triangle a hit reports), v1 - v0, v2 - v0
+    float slot[10] = {v[0], v[1], v[2], __uint_as_float(i),
                       __fsub_rn(v[3], v[0]), __fsub_rn(v[4], v[1]), __fsub_rn(v[5], v[2]),
                       __fsub_rn(v[6], v[0]), __fsub_rn(v[7], v[1]), __fsub_rn(v[8], v[2])};
     Box box = leaf_box(v);  // BVHBuilder.cu:73-74, BBox.cpp:26-30
@@ -459,7 +356,7 @@ int build_impl(const cpt_triangle* tris_in, uint32_t n, const float* host_box, c
     const uint32_t inner = n - 1;
     {
         CPT_PROF(K_TOPOLOGY, stream);
-        k_topology<K><<<(inner + 255) / 256, 256, 0, stream>>>(keys, n, bvh->children, bvh->parents_leaf,
+        k_topology<K><<<(inner + 255) / 256, 256, 0, stream>>>(keys, n, nullptr, bvh->children, bvh->parents_leaf,
                                                                 bvh->parents_internal, s.counters,
                                                                 static_cast<float4*>(bvh->nodes));
     }
@@ -512,6 +409,8 @@ extern "C" int cpt_bvh_bind(void* mem, size_t bytes, uint32_t n, int morton_bits
     out->node_boxes = c.take<cpt_bbox>(n - 1);
     out->nodes = c.take<float4>(6ull * (n - 1));
     out->status = c.take<uint32_t>(4);
+    out->split_nodes = nullptr;
+    out->split_capacity = 0;
     return CPT_OK;
 }
 

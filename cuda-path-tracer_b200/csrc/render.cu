@@ -703,7 +703,7 @@ uint64_t make_views(const cpt_view* views, uint32_t n, uint32_t ref_grid, Views&
             s.height == 0 || (s.scene->light_count && !s.scene->lights) || (reinterpret_cast<uintptr_t>(s.accum) & 15))
             return 0;
         View& v = vs.v[i];
-        v.nodes = static_cast<const float4*>(s.bvh->nodes);
+        v.nodes = static_cast<const float4*>(s.bvh->split_nodes ? s.bvh->split_nodes : s.bvh->nodes);
         v.tris = s.bvh->tris;
         v.infos = s.scene->infos;
         v.lights = s.scene->lights;
@@ -712,7 +712,8 @@ uint64_t make_views(const cpt_view* views, uint32_t n, uint32_t ref_grid, Views&
         v.accum = s.accum;
         v.info_count = s.scene->info_count;
         v.light_count = s.scene->light_count;
-        v.max_visits = s.bvh->n;  // a ray fetches each of the n - 1 internal nodes at most once
+        // a ray fetches each internal node at most once
+        v.max_visits = s.bvh->split_nodes ? s.bvh->split_capacity : s.bvh->n;
         v.width = s.width;
         v.height = s.height;
         v.pixels = s.width * s.height;

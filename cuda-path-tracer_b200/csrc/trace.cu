@@ -57,13 +57,15 @@ extern "C" int cpt_trace(const cpt_bvh* bvh, const float* rays, uint32_t n, int 
     if ((reinterpret_cast<uintptr_t>(rays) & 15) || (reinterpret_cast<uintptr_t>(hits) & 15))
         return CPT_ERR_INVALID_ARGUMENT;
     if (n == 0) return CPT_OK;
-    const float4* nd = static_cast<const float4*>(bvh->nodes);
+    // the split BVH when one was built (same hits, fewer node visits)
+    const float4* nd = static_cast<const float4*>(bvh->split_nodes ? bvh->split_nodes : bvh->nodes);
     const float4* r4 = reinterpret_cast<const float4*>(rays);
     float4* h4 = reinterpret_cast<float4*>(hits);
     uint2* st = reinterpret_cast<uint2*>(stats);
     uint32_t* pool = bvh->status + 1;  // ray pool counter of the persistent kernel
     CPT_CUDA_TRY(cudaMemsetAsync(pool, 0, sizeof(uint32_t), stream));
-    const uint32_t mv = bvh->n;  // a ray fetches each of the n - 1 internal nodes at most once
+    // a ray fetches each internal node at most once
+    const uint32_t mv = bvh->split_nodes ? bvh->split_capacity : bvh->n;
     CPT_PROF(K_TRACE, stream);
     if (any_hit) return stats ? launch_trace<true, true>(nd, r4, n, h4, st, pool, bvh->status, mv, stream)
                               : launch_trace<true, false>(nd, r4, n, h4, st, pool, bvh->status, mv, stream);

@@ -11,8 +11,8 @@
 // What changes is the memory side and the scheduling:
 //  * one 96-B record per internal node (six 16-B loads, three 32-B sectors) holds
 //    both children and the Node word. A child slot (10 words) is either the
-//    child's box (internal child) or the child triangle itself — v0, the info
-//    index, v1 - v0, v2 - v0 (leaf child): the reference loads a 4-B Node, then a
+//    child's box (internal child) or the child triangle itself — v0, the
+//    triangle's index in the sorted array, v1 - v0, v2 - v0 (leaf child): the reference loads a 4-B Node, then a
 //    24-B box or a 40-B triangle per child from separate arrays; here one round
 //    trip fetches everything a visit needs. The stored edges are the same
 //    subtractions the test performs, so the bits are unchanged.
@@ -142,6 +142,9 @@ __device__ __forceinline__ bool trace_step(TraceState& s, uint32_t* smem_col, ui
     if (kStats) ++n_nodes;
     const uint32_t li = word >> 2, ri = li + 1;
     const bool lint = word & 1u, rint = word & 2u;
+    // the triangle a leaf child stands for: its slot's index word (the leaf position
+    // in an LBVH over the triangles, the piece's triangle in a split BVH)
+    const uint32_t tl = __float_as_uint(w[3]), tr = __float_as_uint(w[13]);
     if (kStats) {
         const uint32_t t = (lint ? 0u : 1u) + (rint ? 0u : 1u);
         n_tris += t;
@@ -179,7 +182,7 @@ __device__ __forceinline__ bool trace_step(TraceState& s, uint32_t* smem_col, ui
                     s.best.t = hf;
                     s.best.u = sw ? lu : ru;
                     s.best.v = sw ? lv : rv;
-                    s.best.tri = ifar;
+                    s.best.tri = sw ? tl : tr;
                     if (kAny) return true;
                 }
             }
@@ -188,7 +191,7 @@ __device__ __forceinline__ bool trace_step(TraceState& s, uint32_t* smem_col, ui
             s.best.t = hc;
             s.best.u = sw ? ru : lu;
             s.best.v = sw ? rv : lv;
-            s.best.tri = ic;
+            s.best.tri = sw ? tr : tl;
             if (kAny) return true;
             pop = true;
         }

@@ -72,8 +72,11 @@ typedef struct cpt_bvh {
     cpt_bbox* node_boxes;       /* [n-1] internal node boxes */
     void* nodes;                /* [n-1] 96-B traversal nodes: two 40-B child slots + Node word, where a
                                  *       slot holds the child's box (internal child) or the child
-                                 *       triangle as v0, info_idx, v1 - v0, v2 - v0 (leaf child) */
+                                 *       triangle as v0, its index in tris, v1 - v0, v2 - v0 (leaf child) */
     uint32_t* status;           /* [4]   device status words (CPT_STATUS_* bits in [0]) */
+    void* split_nodes;          /* nullable: traversal nodes of the split BVH (cpt_lbvh_split); when set,
+                                 *       tracing and rendering traverse them instead of `nodes` */
+    uint32_t split_capacity;    /* pieces the split nodes were built for (0 when none) */
 } cpt_bvh;
 
 /* Bytes of device memory cpt_bvh_bind() needs for n triangles. */
@@ -117,6 +120,24 @@ int cpt_lbvh_build(const cpt_triangle* tris_in, uint32_t n, const float* enclosi
 #define CPT_LBVH_STATIC_SCRATCH_BYTES (8u << 20)
 int cpt_lbvh_build_static(const cpt_triangle* tris_in, uint32_t n, const float* enclosing_box, int morton_bits,
                           cpt_bvh* bvh, uint32_t flags, cudaStream_t stream);
+
+/* Split traversal BVH (no reference counterpart; an optional traversal accelerator).
+ * Built from an LBVH's Morton-sorted triangles: triangles whose box is large for
+ * their area (long thin ones) are cut into up to 64 pieces along their longest box
+ * axis, each piece keeping the box of the triangle clipped to its slab (widened by
+ * 2^-20 of the coordinates so rounding cannot lose a hit); the pieces get their
+ * own LBVH (Morton keys of the piece box centres in the root box, the same sort,
+ * topology and refit kernels). The extra pieces are shared out in proportion to
+ * sqrt(box area - 2 x triangle area), at most extra_ratio x n of them. Leaves hold
+ * the whole triangle and its sorted index, so tracing reports the same triangles
+ * (t, u, v and index) as over `nodes`, except that of two triangles hit at exactly
+ * the same t either may be reported. The reference-format outputs are not touched.
+ * Sets bvh->split_nodes = nodes and bvh->split_capacity. node_bytes / scratch bytes
+ * from cpt_lbvh_split_bytes (0 on bad arguments); scratch is free after the stream
+ * passes the call. */
+size_t cpt_lbvh_split_bytes(uint32_t n, int morton_bits, float extra_ratio, size_t* node_bytes);
+int cpt_lbvh_split(cpt_bvh* bvh, float extra_ratio, void* nodes, size_t node_bytes, void* scratch, size_t scratch_bytes,
+                   cudaStream_t stream);
 
 /* Reads the device status words of a build or render (synchronizes the stream)
  * and maps them to a status code. */
@@ -253,6 +274,9 @@ int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32_t n, const
  * albedo_idx / normal_map_idx index (handles from cpt_texture_create; the caller
  * keeps them alive while the tracer renders). count 0 clears it. */
 int cpt_tracer_upload_textures(cpt_tracer* t, const cudaTextureObject_t* textures, uint32_t count);
+/* extra_ratio > 0: every later upload also builds the split traversal BVH
+ * (cpt_lbvh_split) and renders through it; 0 (default) renders over the LBVH. */
+int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio);
 int cpt_tracer_set_primary_rays(cpt_tracer* t, const float dirs[12]);
 int cpt_tracer_set_eye(cpt_tracer* t, const float eye[3]);
 int cpt_tracer_set_camera(cpt_tracer* t, const cpt_camera* cam);

@@ -50,7 +50,7 @@ def leaf_boxes(tris):
 
 def assert_records_consistent(out):
     """96-B node = [left slot | right slot | Node word | pad]; a slot is the child's
-    box padded with zeros (internal child) or the child triangle as v0, info_idx,
+    box padded with zeros (internal child) or the child triangle as v0, its index,
     v1 - v0, v2 - v0 (leaf child)."""
     n = len(out["tris"])
     nodes, ch = out["nodes"], out["children"]
@@ -59,7 +59,7 @@ def assert_records_consistent(out):
     t = out["tris"]
     tri_slot = np.zeros((n, 10), np.float32)
     tri_slot[:, 0:3] = t["v0"]
-    tri_slot[:, 3] = t["info_idx"].view(np.float32)
+    tri_slot[:, 3] = np.arange(len(t), dtype=np.uint32).view(np.float32)
     tri_slot[:, 4:7] = (t["v1"] - t["v0"]).astype(np.float32)
     tri_slot[:, 7:10] = (t["v2"] - t["v0"]).astype(np.float32)
     box_slot = np.zeros((n - 1, 10), np.float32)

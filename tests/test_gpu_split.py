@@ -1,0 +1,125 @@
+"""Split traversal BVH (cpt_lbvh_split) on the GPU: the same closest hits as the
+LBVH it is built from (the oracle's restatement of the reference traversal) —
+identical (t, u, v, triangle) except where two triangles are hit at exactly the
+same t — fewer node visits on long thin triangles, bit-identical images on the
+test scenes, and the reference-format outputs left untouched."""
+import numpy as np
+import pytest
+import torch
+
+import cpt
+from cpt.device import BatchRenderer, DeviceLbvh, DeviceScene, make_params, to_device
+from oracle import cpu
+
+pytestmark = pytest.mark.gpu
+
+
+def hairball(n_hair=20_000, nu=64, nv=32, seed=3):
+    return cpt.scene_sphere_hairball(nu, nv, n_hair, seed=seed, hair_radius=1.3)
+
+
+def random_rays(m, seed=1, inside=False):
+    g = np.random.default_rng(seed)
+    if inside:
+        o = g.uniform(-1.2, 1.2, (m, 3))
+    else:
+        d0 = g.normal(size=(m, 3))
+        o = 3.0 * d0 / np.linalg.norm(d0, axis=1, keepdims=True)
+    tgt = g.uniform(-1.0, 1.0, (m, 3))
+    d = tgt - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.zeros((m, 8), np.float32)
+    r[:, 0:3] = o
+    r[:, 4:7] = d
+    return r
+
+
+def tie_or_equal(h_split, h_ref, ulps=1):
+    """Same hit, or hits whose t agree within `ulps` units in the last place: the
+    closest of two triangles whose distances are that close depends on the order in
+    which the trees visit them (the box entry distance and a triangle's computed t
+    differ by rounding)."""
+    same = h_split.view(np.uint32) == h_ref.view(np.uint32)
+    all_same = same.all(axis=1)
+    tr = h_ref[:, 0].astype(np.float64)
+    near = np.abs(h_split[:, 0].astype(np.float64) - tr) <= ulps * np.spacing(np.abs(h_ref[:, 0])).astype(np.float64)
+    return all_same | near, all_same
+
+
+@pytest.mark.parametrize("bits", [30, 63])
+@pytest.mark.parametrize("ratio", [0.5, 2.0])
+def test_split_hits_match_oracle(cuda, bits, ratio):
+    tris, _ = hairball()
+    lb = DeviceLbvh(len(tris), bits)
+    lb.build(to_device(tris), check_root=True)
+    before = lb.download()
+    rays = np.concatenate([random_rays(20_000, 1), random_rays(10_000, 2, inside=True)])
+    d_rays = torch.from_numpy(rays).cuda()
+    base_hits, base_stats = lb.trace(d_rays, stats=True)
+    lb.split(ratio)
+    split_hits, split_stats = lb.trace(d_rays, stats=True)
+    torch.cuda.synchronize()
+    lb.status()
+    hs, hb = split_hits.cpu().numpy(), base_hits.cpu().numpy()
+    ok, exact = tie_or_equal(hs, hb)
+    assert ok.all()
+    assert exact.mean() > 0.999
+    # the oracle's restatement of the reference traversal agrees with the LBVH path
+    b = cpu.build(tris, bits)
+    t, idx, uv = cpu.trace(b, rays[:, [0, 1, 2, 4, 5, 6]])
+    ok2, _ = tie_or_equal(hs, np.stack([t, uv[:, 0], uv[:, 1], idx.view(np.float32)], 1))
+    assert ok2.all()
+    # any-hit agrees on occlusion
+    a_split, _ = lb.trace(d_rays, any_hit=True)
+    lb.unsplit()
+    a_base, _ = lb.trace(d_rays, any_hit=True)
+    assert np.array_equal(a_split.cpu().numpy()[:, 0] < 3e38, a_base.cpu().numpy()[:, 0] < 3e38)
+    # fewer visits on the hairball; reference-format outputs untouched
+    v_split, v_base = split_stats.cpu().numpy()[:, 0].mean(), base_stats.cpu().numpy()[:, 0].mean()
+    assert v_split < (0.95 if ratio >= 2.0 else 1.0) * v_base, (v_split, v_base)
+    after = lb.download()
+    for k in ("tris", "keys", "children", "parents_leaf", "parents_internal", "node_boxes", "nodes"):
+        assert after[k].tobytes() == before[k].tobytes(), k
+
+
+def test_split_render_matches_plain(cuda):
+    tris, infos = hairball(n_hair=30_000)
+    cam = cpt.camera_look_at((0.0, 0.35, -3.6), (0.0, 0.0, 0.0), aspect=64 / 48)
+    lb = DeviceLbvh(len(tris), 63)
+    lb.build(to_device(tris), check_root=True)
+    sc = DeviceScene(infos)
+    p = make_params(64, 48, 8, 3, 5, 3.0, True, 17, cpt.ACCUM_KAHAN)
+    r0 = BatchRenderer([(lb, sc, cam, 64, 48)], p)
+    r0.render()
+    lb.split(1.0)
+    r1 = BatchRenderer([(lb, sc, cam, 64, 48)], p)
+    r1.render()
+    torch.cuda.synchronize()
+    r1.check_status()
+    a0 = r0.accums[0].cpu().numpy().view(np.float32)
+    a1 = r1.accums[0].cpu().numpy().view(np.float32)
+    differ = (a0.view(np.uint32) != a1.view(np.uint32)).reshape(2, 48, 64, 4)[0].any(-1)
+    assert differ.mean() < 0.002   # only pixels whose path met an exact tie may differ
+    assert np.array_equal(r0.counts.cpu().numpy()[:3] > 0, r1.counts.cpu().numpy()[:3] > 0)
+
+
+def test_split_degenerate_and_zero_budget(cuda):
+    # ratio 0: one piece per triangle; a flat scene (zero extent on an axis) where every
+    # hit is a near-tie between coplanar triangles
+    tris, _ = cpt.scene_random(5000, seed=9)
+    tris["v0"][:, 2] = tris["v1"][:, 2] = tris["v2"][:, 2] = 0.5
+    lb = DeviceLbvh(len(tris), 30)
+    lb.build(to_device(tris))
+    rays = random_rays(5000, 4)
+    rays[:, 4:7] = np.array([0.1, 0.2, 1.0]) / np.linalg.norm([0.1, 0.2, 1.0])
+    rays[:, 0:3] = np.random.default_rng(5).uniform(0, 1, (5000, 3)) - np.array([0, 0, 1.0])
+    d_rays = torch.from_numpy(rays.astype(np.float32)).cuda()
+    h0, _ = lb.trace(d_rays)
+    lb.split(0.0)
+    h1, _ = lb.trace(d_rays)
+    torch.cuda.synchronize()
+    lb.status()
+    a, b = h1.cpu().numpy(), h0.cpu().numpy()
+    ok, _ = tie_or_equal(a, b, ulps=4)
+    assert ok.all()
+    assert np.array_equal(a[:, 0] < 3e38, b[:, 0] < 3e38)
