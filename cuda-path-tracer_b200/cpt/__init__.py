@@ -32,12 +32,14 @@ ERRORS = {
     7: "root box volume differs from the enclosing box",
     8: "no CUDA device",
     9: "device-side index out of range (corrupt input)",
+    10: "tree taller than the traversal stack (split BVH not built)",
 }
 ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_SCRATCH_TOO_SMALL, ERR_NONFINITE_INPUT = 1, 2, 3, 4
 ERR_DEVICE_TIMEOUT, ERR_STACK_OVERFLOW, ERR_CHECK_FAILED, ERR_NO_DEVICE, ERR_BAD_INDEX = 5, 6, 7, 8, 9
 BUILD_CHECK = 1
 ACCUM_KAHAN, ACCUM_LERP, ACCUM_F64 = 0, 1, 2
 INVALID_INDEX = 0xFFFFFFFF
+SPLIT_PLOC = 1
 TRAVERSAL_STACK = 64
 
 TRIANGLE_DTYPE = np.dtype([("v0", "<f4", 3), ("v1", "<f4", 3), ("v2", "<f4", 3), ("info_idx", "<u4")])
@@ -145,7 +147,7 @@ _PROTOS = {
     "cpt_tracer_destroy": (None, [_P]),
     "cpt_tracer_upload": (_I32, [_P, _P, _U32, _P, _U32, _P, _U32, _P]),
     "cpt_tracer_upload_textures": (_I32, [_P, _P, _U32]),
-    "cpt_tracer_set_split": (_I32, [_P, _F]),
+    "cpt_tracer_set_split": (_I32, [_P, _F, _U32]),
     "cpt_tracer_set_primary_rays": (_I32, [_P, _P]),
     "cpt_tracer_set_eye": (_I32, [_P, _P]),
     "cpt_tracer_set_camera": (_I32, [_P, ctypes.POINTER(Camera)]),
@@ -164,8 +166,8 @@ _PROTOS = {
     "cpt_texture_create": (_I32, [_P, _U32, _U32, ctypes.POINTER(ctypes.c_uint64)]),
     "cpt_texture_destroy": (None, [ctypes.c_uint64]),
     "cpt_texture_sample": (_I32, [ctypes.c_uint64, _P, _U32, _P, _P]),
-    "cpt_lbvh_split_bytes": (_SZ, [_U32, _I32, _F, ctypes.POINTER(_SZ)]),
-    "cpt_lbvh_split": (_I32, [ctypes.POINTER(Bvh), _F, _P, _SZ, _P, _SZ, _P]),
+    "cpt_lbvh_split_bytes": (_SZ, [_U32, _I32, _F, _U32, ctypes.POINTER(_SZ)]),
+    "cpt_lbvh_split": (_I32, [ctypes.POINTER(Bvh), _F, _U32, _P, _SZ, _P, _SZ, _P]),
     "cpt_obj_load": (_I32, [ctypes.c_char_p, _F, _P, _F, _P, _P, _U32, ctypes.POINTER(_U32)]),
     "cpt_bvh_heatmap": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Camera), _U32, _U32, _P, _P, _P, _P]),
     "cpt_camera_look_at": (None, [_P, _P, _P, _F, _F, _F, _F, ctypes.POINTER(Camera)]),
@@ -390,8 +392,8 @@ class Tracer:
         check(lib.cpt_tracer_upload(self._h, _ptr(tris), len(tris), _ptr(infos), len(infos), lp, nl,
                                     None if box_arr is None else _ptr(box_arr)), "cpt_tracer_upload")
 
-    def set_split(self, extra_ratio: float) -> None:
-        check(lib.cpt_tracer_set_split(self._h, float(extra_ratio)), "cpt_tracer_set_split")
+    def set_split(self, extra_ratio: float, flags: int = 0) -> None:
+        check(lib.cpt_tracer_set_split(self._h, float(extra_ratio), int(flags)), "cpt_tracer_set_split")
 
     def upload_textures(self, textures) -> None:
         table = texture_handles(textures)

@@ -56,11 +56,12 @@ class DeviceLbvh:
     def status(self, stream: int | None = None) -> None:
         status_check(self.bvh.status, stream_handle() if stream is None else stream)
 
-    def split(self, extra_ratio: float = 1.0, stream: int | None = None, keep_scratch: bool = False) -> None:
+    def split(self, extra_ratio: float = 1.0, stream: int | None = None, keep_scratch: bool = False,
+              flags: int = 0) -> None:
         """Builds the split traversal BVH (cpt_lbvh_split) over the built tree; tracing
         and rendering then traverse it. Call again after every build."""
         nb = ctypes.c_size_t()
-        sb = int(lib.cpt_lbvh_split_bytes(self.n, self.bits, float(extra_ratio), ctypes.byref(nb)))
+        sb = int(lib.cpt_lbvh_split_bytes(self.n, self.bits, float(extra_ratio), int(flags), ctypes.byref(nb)))
         if not sb:
             raise ValueError("split BVH parameters rejected")
         dev = self.mem.device
@@ -68,7 +69,7 @@ class DeviceLbvh:
             self.split_nodes = dev_bytes(nb.value, dev)
         if getattr(self, "split_scratch", None) is None or self.split_scratch.numel() < sb:
             self.split_scratch = dev_bytes(sb, dev)
-        check(lib.cpt_lbvh_split(ctypes.byref(self.bvh), float(extra_ratio), self.split_nodes.data_ptr(),
+        check(lib.cpt_lbvh_split(ctypes.byref(self.bvh), float(extra_ratio), int(flags), self.split_nodes.data_ptr(),
                                  self.split_nodes.numel(), self.split_scratch.data_ptr(), self.split_scratch.numel(),
                                  stream_handle() if stream is None else stream), "cpt_lbvh_split")
         if not keep_scratch:

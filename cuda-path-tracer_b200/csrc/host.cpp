@@ -443,6 +443,7 @@ struct cpt_tracer {
     void* d_split_scratch = nullptr;
     size_t split_scratch_cap = 0;
     float split_ratio = 0.f;  // 0: traverse the LBVH itself
+    uint32_t split_flags = 0;
     void* d_textures = nullptr;  // cudaTextureObject_t handles (the caller owns the textures)
     size_t textures_cap = 0;
     uint32_t texture_count = 0;
@@ -530,11 +531,12 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
     if (rc) return rc;
     if (t->split_ratio > 0.f) {
         size_t nb = 0;
-        const size_t sb = cpt_lbvh_split_bytes(n, t->bits, t->split_ratio, &nb);
+        const size_t sb = cpt_lbvh_split_bytes(n, t->bits, t->split_ratio, t->split_flags, &nb);
         if (!sb) return CPT_ERR_INVALID_ARGUMENT;
         if ((rc = ensure(&t->d_split_nodes, &t->split_nodes_cap, nb))) return rc;
         if ((rc = ensure(&t->d_split_scratch, &t->split_scratch_cap, sb))) return rc;
-        rc = cpt_lbvh_split(&t->bvh, t->split_ratio, t->d_split_nodes, t->split_nodes_cap, t->d_split_scratch,
+        rc = cpt_lbvh_split(&t->bvh, t->split_ratio, t->split_flags, t->d_split_nodes, t->split_nodes_cap,
+                            t->d_split_scratch,
                             t->split_scratch_cap, t->stream);
         if (rc) return rc;
     }
@@ -547,10 +549,11 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
     return CPT_OK;
 }
 
-extern "C" int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio)
+extern "C" int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio, uint32_t flags)
 {
     if (!t || !(extra_ratio >= 0.f) || !(extra_ratio <= 64.f)) return CPT_ERR_INVALID_ARGUMENT;
     t->split_ratio = extra_ratio;
+    t->split_flags = flags;
     return CPT_OK;
 }
 

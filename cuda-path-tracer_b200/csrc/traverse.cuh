@@ -140,7 +140,7 @@ __device__ __forceinline__ bool trace_step(TraceState& s, uint32_t* smem_col, ui
     }
     const uint32_t word = __float_as_uint(w[20]);
     if (kStats) ++n_nodes;
-    const uint32_t li = word >> 2, ri = li + 1;
+    const uint32_t li = word >> 2, ri = __float_as_uint(w[21]);
     const bool lint = word & 1u, rint = word & 2u;
     // the triangle a leaf child stands for: its slot's index word (the leaf position
     // in an LBVH over the triangles, the piece's triangle in a split BVH)

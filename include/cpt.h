@@ -35,6 +35,7 @@ extern "C" {
 #define CPT_ERR_CHECK_FAILED 7      /* root box volume differs from the enclosing box's */
 #define CPT_ERR_NO_DEVICE 8         /* no CUDA device / library built for another arch */
 #define CPT_ERR_BAD_INDEX 9         /* a device-side index was out of range (e.g. info_idx >= info_count) */
+#define CPT_ERR_TREE_TOO_DEEP 10    /* a built tree is taller than CPT_TRAVERSAL_STACK (split BVH not used) */
 
 /* device status-word bits (cpt_bvh.status[0], render status) */
 #define CPT_STATUS_NONFINITE 1u
@@ -70,9 +71,10 @@ typedef struct cpt_bvh {
     uint32_t* parents_leaf;     /* [n]   parent of each leaf */
     uint32_t* parents_internal; /* [n-1] parent of each internal node; [0] = CPT_INVALID_INDEX */
     cpt_bbox* node_boxes;       /* [n-1] internal node boxes */
-    void* nodes;                /* [n-1] 96-B traversal nodes: two 40-B child slots + Node word, where a
-                                 *       slot holds the child's box (internal child) or the child
-                                 *       triangle as v0, its index in tris, v1 - v0, v2 - v0 (leaf child) */
+    void* nodes;                /* [n-1] 96-B traversal nodes: two 40-B child slots, the Node word and the
+                                 *       right child's index (left + 1 here), where a slot holds the
+                                 *       child's box (internal child) or the child triangle as v0, its
+                                 *       index in tris, v1 - v0, v2 - v0 (leaf child) */
     uint32_t* status;           /* [4]   device status words (CPT_STATUS_* bits in [0]) */
     void* split_nodes;          /* nullable: traversal nodes of the split BVH (cpt_lbvh_split); when set,
                                  *       tracing and rendering traverse them instead of `nodes` */
@@ -135,9 +137,11 @@ int cpt_lbvh_build_static(const cpt_triangle* tris_in, uint32_t n, const float* 
  * Sets bvh->split_nodes = nodes and bvh->split_capacity. node_bytes / scratch bytes
  * from cpt_lbvh_split_bytes (0 on bad arguments); scratch is free after the stream
  * passes the call. */
-size_t cpt_lbvh_split_bytes(uint32_t n, int morton_bits, float extra_ratio, size_t* node_bytes);
-int cpt_lbvh_split(cpt_bvh* bvh, float extra_ratio, void* nodes, size_t node_bytes, void* scratch, size_t scratch_bytes,
-                   cudaStream_t stream);
+#define CPT_SPLIT_PLOC 1u /* pieces clustered by surface area (locally-ordered clustering, search radius 16
+                             * in Morton order) instead of the Karras topology: fewer node visits, longer build */
+size_t cpt_lbvh_split_bytes(uint32_t n, int morton_bits, float extra_ratio, uint32_t flags, size_t* node_bytes);
+int cpt_lbvh_split(cpt_bvh* bvh, float extra_ratio, uint32_t flags, void* nodes, size_t node_bytes, void* scratch,
+                   size_t scratch_bytes, cudaStream_t stream);
 
 /* Reads the device status words of a build or render (synchronizes the stream)
  * and maps them to a status code. */
@@ -275,8 +279,8 @@ int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32_t n, const
  * keeps them alive while the tracer renders). count 0 clears it. */
 int cpt_tracer_upload_textures(cpt_tracer* t, const cudaTextureObject_t* textures, uint32_t count);
 /* extra_ratio > 0: every later upload also builds the split traversal BVH
- * (cpt_lbvh_split) and renders through it; 0 (default) renders over the LBVH. */
-int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio);
+ * (cpt_lbvh_split with `flags`) and renders through it; 0 (default) renders over the LBVH. */
+int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio, uint32_t flags);
 int cpt_tracer_set_primary_rays(cpt_tracer* t, const float dirs[12]);
 int cpt_tracer_set_eye(cpt_tracer* t, const float eye[3]);
 int cpt_tracer_set_camera(cpt_tracer* t, const cpt_camera* cam);

@@ -49,13 +49,14 @@ def leaf_boxes(tris):
 
 
 def assert_records_consistent(out):
-    """96-B node = [left slot | right slot | Node word | pad]; a slot is the child's
-    box padded with zeros (internal child) or the child triangle as v0, its index,
-    v1 - v0, v2 - v0 (leaf child)."""
+    """96-B node = [left slot | right slot | Node word | right index | pad]; a slot is
+    the child's box padded with zeros (internal child) or the child triangle as v0,
+    its index, v1 - v0, v2 - v0 (leaf child)."""
     n = len(out["tris"])
     nodes, ch = out["nodes"], out["children"]
     assert nodes.shape == (n - 1, 24)
     assert same_bits(nodes[:, 20].view(np.uint32), ch)
+    assert same_bits(nodes[:, 21].view(np.uint32), (ch >> 2) + 1)
     t = out["tris"]
     tri_slot = np.zeros((n, 10), np.float32)
     tri_slot[:, 0:3] = t["v0"]
