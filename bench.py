@@ -559,7 +559,7 @@ def run_ours(args, w, world, rank, local):
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "k_extend_c2.md")
+    tp = os.path.join(ROOT, "profiles", "k_extend_c2_split.md" if split > 0 else "k_extend_c2.md")
     if args.workload == "c2" and os.path.exists(tp):  # ncu figure of the C2 traversal (see that file)
         import re
 
