@@ -39,7 +39,7 @@ WORKLOADS = {
                target=(0.5, 0.5, 0.0), seed=0),
     # 64 scenes, 10k-2M triangles (log-uniform, alternating generators), 256^2-1024^2, one graph launch per frame
     "c3": dict(kind="batch", scenes=64, tri_min=10_000, tri_max=2_000_000, res_min=256, res_max=1024, spp=4,
-               bounces=5, bits=63, seed=0, width=0, height=0),
+               bounces=5, bits=63, seed=0, width=0, height=0, split=1.0),
     # radiance cache on the C2 scene: 1 spp frames through the cache vs plain 16 spp, RMSE vs an FP64 image
     "c4": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
                bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, plain_spp=64, ref_spp=4096,
@@ -81,7 +81,7 @@ def workload_config(name, w, n_tris, l2_note):
             "c1": "65,536 random triangles + quad light",
             "c5": "deforming fBm sphere 4096x2048x2 + quad light, rebuild every frame, 8 cameras, radiance cache "
                   "(trained across the deforming frames)",
-            "c3": "64 scenes 10k-2M triangles (random / sphere+hairball alternating), 256^2-1024^2, 4 spp, "
+            "c3": "64 scenes 10k-2M triangles (random / sphere+hairball alternating; split BVH for the hairball scenes), 256^2-1024^2, 4 spp, "
                   "depth 6, one CUDA-graph launch per frame, autotuned wave"}[name]
     c = {"workload": f"{name}: {desc}",
          "triangles": int(n_tris), "morton_bits": w["bits"], "resolution": f'{w["width"]}x{w["height"]}',
@@ -269,12 +269,15 @@ def run_batch(args, w, world, rank, local):
     dev = torch.device("cuda", local if world > 1 else 0)
     t0 = time.perf_counter()
     specs = batch_specs(w)
+    split = w.get("split", 0.0) if args.split is None else args.split
     views, keep, n_tris, pixels = [], [], 0, 0
     for i, (kind, ntri, side) in enumerate(specs):
         tris, infos = batch_scene(kind, ntri, w["seed"] + i)
         lb = DeviceLbvh(len(tris), w["bits"], dev)
         d = to_device(tris, dev)
         lb.build(d, check_root=True)
+        if kind != "random" and split > 0:  # the hairball scenes traverse a split BVH
+            lb.split(split)
         sc = DeviceScene(infos, None, dev)
         eye, tgt = ((0.5, 0.5, -1.2), (0.5, 0.5, 0.0)) if kind == "random" else ((0.0, 0.35, -3.6), (0.0, 0.0, 0.0))
         cam = cpt.camera_look_at(eye, tgt, fov_deg=45.0, aspect=1.0)
