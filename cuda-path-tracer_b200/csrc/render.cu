@@ -33,7 +33,10 @@
 namespace cpt {
 
 constexpr int kExtendBlock = 128;
-constexpr int kExtendSteps = 8;
+#ifndef CPT_EXTEND_STEPS
+#define CPT_EXTEND_STEPS 1024
+#endif
+constexpr int kExtendSteps = CPT_EXTEND_STEPS;  // most node visits between two refills of a warp
 constexpr int kShadeBlock = 128;
 constexpr int kGenBlock = 256;
 constexpr int kMaxDepth = 62;  // bounces + 1 queues; reference GUI allows 5 bounces (PathTracingSettings.h:27)

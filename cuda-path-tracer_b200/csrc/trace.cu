@@ -9,7 +9,7 @@
 namespace cpt {
 
 constexpr int kTraceBlock = 128;
-constexpr int kTraceSteps = 8;
+constexpr int kTraceSteps = 1024;
 
 template <bool kAny, bool kStats>
 __global__ void __launch_bounds__(kTraceBlock) k_trace(const float4* __restrict__ nodes, const float4* __restrict__ rays,
