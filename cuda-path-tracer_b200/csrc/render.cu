@@ -716,7 +716,7 @@ uint64_t make_views(const cpt_view* views, uint32_t n, uint32_t ref_grid, Views&
         v.info_count = s.scene->info_count;
         v.light_count = s.scene->light_count;
         // a ray fetches each internal node at most once
-        v.max_visits = s.bvh->split_nodes ? s.bvh->split_capacity : s.bvh->n;
+        v.max_visits = s.bvh->split_nodes ? (s.bvh->split_capacity | kFastSlabBit) : s.bvh->n;
         v.width = s.width;
         v.height = s.height;
         v.pixels = s.width * s.height;

@@ -65,7 +65,7 @@ extern "C" int cpt_trace(const cpt_bvh* bvh, const float* rays, uint32_t n, int 
     uint32_t* pool = bvh->status + 1;  // ray pool counter of the persistent kernel
     CPT_CUDA_TRY(cudaMemsetAsync(pool, 0, sizeof(uint32_t), stream));
     // a ray fetches each internal node at most once
-    const uint32_t mv = bvh->split_nodes ? bvh->split_capacity : bvh->n;
+    const uint32_t mv = bvh->split_nodes ? (bvh->split_capacity | kFastSlabBit) : bvh->n;
     CPT_PROF(K_TRACE, stream);
     if (any_hit) return stats ? launch_trace<true, true>(nd, r4, n, h4, st, pool, bvh->status, mv, stream)
                               : launch_trace<true, false>(nd, r4, n, h4, st, pool, bvh->status, mv, stream);

@@ -62,6 +62,20 @@ __device__ __forceinline__ float slab_test(f3 o, f3 dinv, bool finite, float ax,
     return (n <= f && f > 0.0f) ? n : FLT_MAX;
 }
 
+// Slab test for trees whose box distances only steer pruning (the split BVH):
+// t = b * (1/d) - o * (1/d) in one fused multiply-add per plane. Valid when every
+// 1/d component is finite (no inf * 0).
+__device__ __forceinline__ float slab_test_fma(f3 odinv, f3 dinv, float ax, float ay, float az, float bx, float by,
+                                               float bz)
+{
+    const float tx0 = fmaf(ax, dinv.x, -odinv.x), tx1 = fmaf(bx, dinv.x, -odinv.x);
+    const float ty0 = fmaf(ay, dinv.y, -odinv.y), ty1 = fmaf(by, dinv.y, -odinv.y);
+    const float tz0 = fmaf(az, dinv.z, -odinv.z), tz1 = fmaf(bz, dinv.z, -odinv.z);
+    const float n = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fminf(tz0, tz1));
+    const float f = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
+    return (n <= f && f > 0.0f) ? n : FLT_MAX;
+}
+
 // Möller-Trumbore on a slot (v0 = s[0..2], e1 = s[4..6], e2 = s[7..9]), without
 // early exits: every lane of a warp runs the same instructions, and u, v, t are the
 // values the reference computes; only the final predicate decides the hit.
@@ -92,16 +106,24 @@ struct TraceState {
     int sp;
     uint32_t visits;  // node fetches
     uint32_t tests;   // triangle tests
+    bool fast;        // fused slab test (split BVH and finite 1/d)
+    f3 odinv;         // o * (1/d), for the fused slab test
 };
+
+// Visit bound word: bit 31 set = a tree whose box distances only steer pruning
+// (the split BVH), which may use the fused slab test.
+constexpr uint32_t kFastSlabBit = 0x80000000u;
 
 __device__ __forceinline__ void trace_init(TraceState& s, const float4* nodes, uint32_t max_visits, f3 o, f3 d)
 {
     s.nodes = nodes;
-    s.max_visits = max_visits;
+    s.max_visits = max_visits & ~kFastSlabBit;
     s.o = o;
     s.d = d;
     s.dinv = mk3(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
     s.finite = isfinite(s.dinv.x) && isfinite(s.dinv.y) && isfinite(s.dinv.z);
+    s.fast = (max_visits & kFastSlabBit) && s.finite;
+    s.odinv = mk3(o.x * s.dinv.x, o.y * s.dinv.y, o.z * s.dinv.z);
     s.best.t = FLT_MAX;
     s.best.u = 0.f;
     s.best.v = 0.f;
@@ -158,8 +180,14 @@ __device__ __forceinline__ bool trace_step(TraceState& s, uint32_t* smem_col, ui
     // Both slab tests run on every lane (a leaf slot's result is discarded), then
     // one Möller-Trumbore code path serves the first leaf child, left or right,
     // and a second one only lanes whose two children are both leaves.
-    float hl = slab_test(s.o, s.dinv, s.finite, w[0], w[1], w[2], w[3], w[4], w[5]);
-    float hr = slab_test(s.o, s.dinv, s.finite, w[10], w[11], w[12], w[13], w[14], w[15]);
+    float hl, hr;
+    if (s.fast) {
+        hl = slab_test_fma(s.odinv, s.dinv, w[0], w[1], w[2], w[3], w[4], w[5]);
+        hr = slab_test_fma(s.odinv, s.dinv, w[10], w[11], w[12], w[13], w[14], w[15]);
+    } else {
+        hl = slab_test(s.o, s.dinv, s.finite, w[0], w[1], w[2], w[3], w[4], w[5]);
+        hr = slab_test(s.o, s.dinv, s.finite, w[10], w[11], w[12], w[13], w[14], w[15]);
+    }
     if (!lint || !rint) {
         float t0[10];
 #pragma unroll
