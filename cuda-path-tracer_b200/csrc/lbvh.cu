@@ -438,6 +438,10 @@ extern "C" int cpt_status_check(const uint32_t* d_status, cudaStream_t stream)
 extern "C" int cpt_lbvh_build(const cpt_triangle* tris_in, uint32_t n, const float* enclosing_box, int morton_bits,
                               cpt_bvh* bvh, void* scratch, size_t scratch_bytes, uint32_t flags, cudaStream_t stream)
 {
+    if (bvh) {  // a split tree of the previous build is stale
+        bvh->split_nodes = nullptr;
+        bvh->split_capacity = 0;
+    }
     if (!tris_in || !bvh || !scratch || n < 2 || n > kMaxTriangles) return CPT_ERR_INVALID_ARGUMENT;
     if (morton_bits != 30 && morton_bits != 63) return CPT_ERR_INVALID_ARGUMENT;
     if (bvh->n != n || bvh->morton_bits != morton_bits || !bvh->tris || !bvh->keys || !bvh->children ||

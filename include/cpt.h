@@ -77,7 +77,8 @@ typedef struct cpt_bvh {
                                  *       index in tris, v1 - v0, v2 - v0 (leaf child) */
     uint32_t* status;           /* [4]   device status words (CPT_STATUS_* bits in [0]) */
     void* split_nodes;          /* nullable: traversal nodes of the split BVH (cpt_lbvh_split); when set,
-                                 *       tracing and rendering traverse them instead of `nodes` */
+                                 *       tracing and rendering traverse them instead of `nodes`.
+                                 *       cpt_lbvh_build clears it (the split tree is of the old triangles) */
     uint32_t split_capacity;    /* pieces the split nodes were built for (0 when none) */
 } cpt_bvh;
 

@@ -104,6 +104,9 @@ def test_split_render_matches_plain(cuda, flags):
     differ = (a0.view(np.uint32) != a1.view(np.uint32)).reshape(2, 48, 64, 4)[0].any(-1)
     assert differ.mean() < 0.002   # only pixels whose path met an exact tie may differ
     assert np.array_equal(r0.counts.cpu().numpy()[:3] > 0, r1.counts.cpu().numpy()[:3] > 0)
+    # a new build drops the split tree of the old triangles
+    lb.build(to_device(tris))
+    assert not lb.bvh.split_nodes and lb.bvh.split_capacity == 0
 
 
 @pytest.mark.parametrize("flags", [0, cpt.SPLIT_PLOC])
