@@ -34,16 +34,16 @@ sys.path.insert(0, os.path.join(ROOT, "cuda-path-tracer_b200"))
 
 WORKLOADS = {
     "c2": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
-               bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, split=1.0),
+               bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, split=1.25),
     "c1": dict(kind="random", n=65536, bits=30, width=512, height=512, spp=1, bounces=3, eye=(0.5, 0.5, -1.2),
                target=(0.5, 0.5, 0.0), seed=0),
     # 64 scenes, 10k-2M triangles (log-uniform, alternating generators), 256^2-1024^2, one graph launch per frame
     "c3": dict(kind="batch", scenes=64, tri_min=10_000, tri_max=2_000_000, res_min=256, res_max=1024, spp=4,
-               bounces=5, bits=63, seed=0, width=0, height=0, split=1.0),
+               bounces=5, bits=63, seed=0, width=0, height=0, split=1.25),
     # radiance cache on the C2 scene: 1 spp frames through the cache vs plain 16 spp, RMSE vs an FP64 image
     "c4": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
                bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, plain_spp=64, ref_spp=4096,
-               ref_div=4, warm_updates=4, max_spp=256, split=1.0),
+               ref_div=4, warm_updates=4, max_spp=256, split=1.25),
     # deforming 16.8 M-triangle displaced sphere, full rebuild every frame, 8 cameras
     "c5": dict(kind="deform", nu=4096, nv=2048, n_hair=0, bits=63, width=1280, height=720, spp=1, bounces=7,
                eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, cameras=8, amp=0.01, omega=40.0, cache=True),
