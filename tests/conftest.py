@@ -16,6 +16,9 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a); runs the library's kernels")
+    # temporary files of the tests stay inside the checkout (ignored by git)
+    if not config.option.basetemp:
+        config.option.basetemp = os.path.join(ROOT, ".pytest_tmp")
 
 
 @pytest.fixture(scope="session")

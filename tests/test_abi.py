@@ -144,3 +144,14 @@ def test_camera_corners_match_oracle_unjittered():
     out = np.zeros((4, 3), np.float32)
     cpu.oracle_lib().orc_corner_dirs(ctypes.byref(o), 0, 0, 0, out.ctypes.data)
     assert np.allclose(out, d, atol=2e-6)
+
+
+def test_cpp_header_compiles():
+    """include/cpt.hpp (the C++ mirror classes) compiles as C++17 against cpt.h."""
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I", os.path.join(root, "include"),
+                        "-I", "/usr/local/cuda/include", os.path.join(root, "tests", "cpp", "cpp_api_test.cpp")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
