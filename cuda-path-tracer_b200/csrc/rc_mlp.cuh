@@ -10,8 +10,8 @@
 // The network and its encoding follow the radiance-cache workload (12-frequency
 // positional encoding, degree-4 spherical harmonics of the direction, normal,
 // albedo); the reference has no radiance cache, so there is nothing to match
-// bit for bit: the training loss and the rendered image's error against the FP64
-// estimator judge it.
+// bit for bit: its quality is measured by the training loss and by the rendered
+// image's error against the FP64 estimator.
 #pragma once
 #include <cuda_bf16.h>
 #include <stdint.h>

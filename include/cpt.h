@@ -333,7 +333,7 @@ void cpt_scene_bounds(const cpt_triangle* tris, uint32_t n, float out[6]);
 void cpt_camera_look_at(const float eye[3], const float target[3], const float up[3], float fov_deg, float aspect,
                         float znear, float zfar, cpt_camera* cam);
 
-/* ---- radiance cache (no reference counterpart: an extension judged by image
+/* ---- radiance cache (no reference counterpart: an extension measured by image
  * error against the FP64 estimator, with plain path tracing as fallback) ----
  * A 96 -> 4 x 64 (ReLU) -> 16 MLP (BF16 weights, FP32 accumulation) over the
  * encoded secondary vertex: 12-frequency sin/cos encoding of the position in the
