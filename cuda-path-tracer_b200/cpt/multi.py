@@ -7,6 +7,9 @@ one reduction to rank 0 — the single exchange step of the path (NCCL over
 NVLink between GPUs; gloo on CPU in the tests). Kahan accumulators reduce by
 channel-wise sum: the sums and sample counts add up; the compensation channel is
 summed too and stays a (small) correction term.
+
+Batches of independent scenes shard by scene instead: `assign_by_cost` gives each
+rank a set of whole scenes (its own BVHs, images and accumulators, no exchange).
 """
 from __future__ import annotations
 
@@ -27,3 +30,31 @@ def reduce_accumulator(accum, dst: int = 0, group=None) -> None:
 
     t = accum if accum.dtype == torch.float32 else accum.view(torch.float32)
     dist.reduce(t, dst=dst, op=dist.ReduceOp.SUM, group=group)
+
+
+def assign_by_cost(costs, world: int) -> list[list[int]]:
+    """Scenes -> ranks, longest processing time first: scenes in decreasing cost
+    (ties: lower index first) each go to the rank with the least total so far (ties:
+    lower rank). Deterministic, so every rank computes the same assignment; the
+    largest rank total is within one scene's cost of the best possible."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-float(costs[i]), i))
+    load = [0.0] * world
+    out: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += float(costs[i])
+    for lst in out:
+        lst.sort()
+    return out
+
+
+def scene_cost(pixels: int, triangles: int, hairball: bool) -> float:
+    """Relative render cost of one scene of a batch: rays (pixels) times the depth
+    of its tree (log2 triangles), four times more for the long-triangle hairball
+    scenes (their rays visit several times more nodes)."""
+    import math
+
+    return float(pixels) * max(1.0, math.log2(max(triangles, 2))) * (4.0 if hairball else 1.0)

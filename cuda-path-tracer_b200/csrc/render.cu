@@ -32,7 +32,10 @@
 
 namespace cpt {
 
-constexpr int kExtendBlock = 128;
+#ifndef CPT_EXTEND_BLOCK
+#define CPT_EXTEND_BLOCK 128
+#endif
+constexpr int kExtendBlock = CPT_EXTEND_BLOCK;
 #ifndef CPT_EXTEND_STEPS
 #define CPT_EXTEND_STEPS 1024
 #endif
@@ -244,7 +247,7 @@ __global__ void __launch_bounds__(kGenBlock) k_generate(Wave wv, Views vs, float
 // kOneView: every ray traverses view 0's BVH (a single scene, e.g. several cameras of
 // it); the node array is then a kernel-wide constant instead of a per-ray value.
 #ifndef CPT_EXTEND_MIN_BLOCKS
-#define CPT_EXTEND_MIN_BLOCKS 8
+#define CPT_EXTEND_MIN_BLOCKS (1024 / CPT_EXTEND_BLOCK)  // 32 warps per SM: 64 registers
 #endif
 template <bool kStats, bool kOneView>
 __global__ void __launch_bounds__(kExtendBlock, CPT_EXTEND_MIN_BLOCKS) k_extend(Views vs, const float4* __restrict__ queue,
