@@ -154,8 +154,9 @@ __global__ void __launch_bounds__(kMortonBlock) k_morton(const float* __restrict
 // arrive (atomic counter) reads its sibling's box the way the reference does —
 // recomputed from the sibling triangle's vertices for a leaf (BVHBuilder.cu:73-80),
 // from the internal-node box array otherwise — and stores left.unite(right).
-// Release/acquire fences order those stores before the counter (the reference's
-// refit has no fence, BVHBuilder.cu:63-86).
+// The counter increment is an acquire-release atomic: it publishes this thread's
+// slot and box stores and makes the sibling's visible to the second arriver (the
+// reference's refit has no ordering between them, BVHBuilder.cu:63-86).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_gather_refit(const float* __restrict__ tris_in, const uint32_t* __restrict__ order,
                                                       uint32_t n, float* __restrict__ tris_out,
@@ -191,11 +192,9 @@ __global__ void __launch_bounds__(256) k_gather_refit(const float* __restrict__ 
         const int side = left == child ? 0 : 1;
         float* node = nodes + 24 * (size_t)p;
         store_slot(node, side, slot);
-        __threadfence();
-        const int arrived = atomicAdd(&counters[p], 1);
+        const int arrived = arrive_acq_rel(&counters[p]);
         if (arrived == 0) return;
         if (arrived != 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }  // a third visit: not a tree
-        __threadfence();
         const uint32_t sib = left + (uint32_t)(1 - side);
         const bool sib_internal = (word >> (1 - side)) & 1u;
         Box sb;

@@ -120,4 +120,21 @@ __device__ __forceinline__ Box leaf_box(const float v[9])
 }
 
 
+// Refit arrival counter: one atomic increment that releases this thread's earlier
+// stores (its child slot and box) and acquires those of the thread that came before
+// it at the same parent (the sibling's box), device-wide.
+__device__ __forceinline__ int arrive_acq_rel(int* counter)
+{
+#ifdef CPT_REFIT_FENCES
+    __threadfence();
+    const int r = atomicAdd(counter, 1);
+    __threadfence();
+    return r;
+#else
+    int r;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(r) : "l"(counter) : "memory");
+    return r;
+#endif
+}
+
 }  // namespace cpt

@@ -366,8 +366,7 @@ __global__ void __launch_bounds__(256) k_split_refit(const cpt_triangle* __restr
     float slot[10] = {t.v0[0], t.v0[1], t.v0[2], __uint_as_float(tri),
                       __fsub_rn(t.v1[0], t.v0[0]), __fsub_rn(t.v1[1], t.v0[1]), __fsub_rn(t.v1[2], t.v0[2]),
                       __fsub_rn(t.v2[0], t.v0[0]), __fsub_rn(t.v2[1], t.v0[1]), __fsub_rn(t.v2[2], t.v0[2])};
-    __threadfence();
-    uint32_t child = i;
+    uint32_t child = i;  // (the leaf box is published by the first arrival's release)
     uint32_t p = parents_leaf[i];
     while (p != CPT_INVALID_INDEX) {
         if (p >= n - 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
@@ -376,11 +375,9 @@ __global__ void __launch_bounds__(256) k_split_refit(const cpt_triangle* __restr
         const int side = left == child ? 0 : 1;
         float* node = nodes + 24 * (size_t)p;
         store_slot(node, side, slot);
-        __threadfence();
-        const int arrived = atomicAdd(&counters[p], 1);
+        const int arrived = arrive_acq_rel(&counters[p]);
         if (arrived == 0) return;
         if (arrived != 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
-        __threadfence();
         const uint32_t sib = left + (uint32_t)(1 - side);
         const bool sib_internal = (word >> (1 - side)) & 1u;
         Box sb;

@@ -1,5 +1,6 @@
-// Ray queries against a built LBVH (cpt_trace): persistent warps over the ray
-// array with per-lane refill, 96-B node loads, shared-memory node stack.
+// Ray queries against a built LBVH or its split tree (cpt_trace): persistent warps
+// over the ray array that refill their idle lanes from a shared pool, 96-B node
+// loads, shared-memory node stack.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include "cpt.h"

@@ -22,9 +22,10 @@
 //    the rest (never reached on the test scenes) in local memory; a push beyond
 //    the capacity is dropped and reported (CPT_STATUS_STACK_OVERFLOW) instead of
 //    overrunning the array.
-//  * traversal kernels are persistent: each lane takes rays from a global pool and
-//    takes the next one as soon as its ray finishes, so a warp is not held by its
-//    slowest ray (per-ray node counts differ by 100x on hairball scenes).
+//  * traversal kernels are persistent: lanes take rays from a global pool, and a
+//    warp takes new rays for its idle lanes once fewer than half of them still
+//    trace, so a warp is not held by its slowest ray (per-ray node counts differ
+//    by 100x on hairball scenes).
 #pragma once
 #include "cpt_device.cuh"
 #include "cpt.h"
