@@ -77,7 +77,7 @@ def make_cameras(w):
 def workload_config(name, w, n_tris, l2_note):
     desc = {"c2": "fBm sphere 2048x1024x2 + 1M hairball + quad light",
             "c4": "fBm sphere 2048x1024x2 + 1M hairball + quad light, radiance cache (96-64x4-16 BF16 MLP, 2^16 "
-                  "training paths/frame, Adam 1e-2) vs plain path tracing",
+                  "training paths per 1-spp frame, Adam 1e-2) vs plain path tracing",
             "c1": "65,536 random triangles + quad light",
             "c5": "deforming fBm sphere 4096x2048x2 + quad light, rebuild every frame, 8 cameras, radiance cache "
                   "(trained across the deforming frames)",
@@ -799,6 +799,7 @@ def run_cache(args, w, world, rank, local):
     if split > 0:
         lb.split(split)
     scene = DeviceScene(infos, None, dev)
+    scene.build_emitters(lb)
     stream = torch.cuda.current_stream()
     rdiv = w["ref_div"]
     rw, rh = W_ // rdiv, H_ // rdiv
@@ -812,9 +813,22 @@ def run_cache(args, w, world, rank, local):
         e1.synchronize()
         return e0.elapsed_time(e1)
 
-    def experiment(stratified):
+    def rc_params():
+        """2^16 training suffixes and 4 optimiser steps per image sample (one
+        call renders `spf` samples, so it trains on spf * 2^16 suffixes), or — with
+        --rc-per-call — per call."""
+        p = rc_default_params()
+        if not args.rc_per_call:
+            p.train_samples *= spf
+            p.train_steps *= spf
+        return p
+
+    def experiment(stratified, nee=False, reach=None):
+        """reach (with nee): the reference estimator's RMSE; also measures how long the
+        next-event plain tracer takes to get there, in frames of 1 sample."""
         t0 = time.perf_counter()
-        refp = make_params(rw, rh, w["ref_spp"], 0, w["bounces"], 3.0, stratified, w["seed"] + 99991, cpt.ACCUM_F64)
+        refp = make_params(rw, rh, w["ref_spp"], 0, w["bounces"], 3.0, stratified, w["seed"] + 99991, cpt.ACCUM_F64,
+                           nee=nee)
         ref = BatchRenderer([(lb, scene, cam, rw, rh)], refp, dev)
         ref.render()
         torch.cuda.synchronize()
@@ -829,7 +843,7 @@ def run_cache(args, w, world, rank, local):
             img = (a[..., :3] / a[..., 3:4].clamp(min=1)).double()[::rdiv, ::rdiv][:rh, :rw]
             return float(torch.sqrt(((img - ref_img) ** 2).mean()))
 
-        pp = make_params(W_, H_, 16, 0, w["bounces"], 3.0, stratified, w["seed"], cpt.ACCUM_KAHAN)
+        pp = make_params(W_, H_, 16, 0, w["bounces"], 3.0, stratified, w["seed"], cpt.ACCUM_KAHAN, nee=nee)
         plain = BatchRenderer([(lb, scene, cam, W_, H_)], pp, dev)
         for i in range(max(1, args.warmup)):
             plain.render(frame0=100000 + 16 * i)
@@ -842,10 +856,23 @@ def run_cache(args, w, world, rank, local):
         plain.check_status()
         rmse_plain = rmse(plain.accums[0])
         plain_rays = int(plain.counts[:3].sum())
+        reach_out = None
+        if reach is not None:
+            plain.accums[0].zero_()
+            t_r, k, got = 0.0, 0, None
+            while k < w["plain_spp"]:
+                t_r += timed(lambda: plain.render(frame0=k, spp=1))
+                k += 1
+                e = rmse(plain.accums[0])
+                if e <= reach:
+                    got = e
+                    break
+            reach_out = {"target_rmse": round(reach, 6), "spp": k, "ms": round(t_r, 2),
+                         "rmse": None if got is None else round(got, 6)}
         del plain
 
-        rc = RadianceCache(rc_default_params())
-        cp = make_params(W_, H_, spf, 0, w["bounces"], 3.0, stratified, w["seed"], cpt.ACCUM_KAHAN)
+        rc = RadianceCache(rc_params())
+        cp = make_params(W_, H_, spf, 0, w["bounces"], 3.0, stratified, w["seed"], cpt.ACCUM_KAHAN, nee=nee)
         cr = CachedRenderer(rc, [(lb, scene, cam, W_, H_)], cp, dev)
         cr.render(frame0=200000)  # warm the kernels on a throwaway network
         torch.cuda.synchronize()
@@ -872,7 +899,8 @@ def run_cache(args, w, world, rank, local):
         cr.check_status()
         cache_rays = int(cr.counts[:3].sum())
         rc.close()
-        return {"stratified": stratified, "ratio": round(t_cache / t_plain, 4) if reached else None,
+        return {"stratified": stratified, "nee": nee, "ratio": round(t_cache / t_plain, 4) if reached else None,
+                "t_cache_ms": round(t_cache, 2), "cache_curve": curve, "plain_to_reference_rmse": reach_out,
                 "plain": {"spp": w["plain_spp"], "ms": round(t_plain, 2), "rmse": round(rmse_plain, 6),
                           "mrays_s": round(plain_rays / t_plain / 1e3, 3)},
                 "cache": {"spp": spp, "spp_per_frame": spf, "warm_updates": w["warm_updates"],
@@ -885,8 +913,23 @@ def run_cache(args, w, world, rank, local):
 
     main_run = experiment(True)
     alt = experiment(False)
+    nee_runs = ([experiment(True, True, main_run["plain"]["rmse"]), experiment(False, True, alt["plain"]["rmse"])]
+                if args.nee else [])
+
+    def nee_summary(ref_run, nee_run):
+        """Next-event estimation against the reference estimator's plain 64-sample
+        RMSE: the plain tracer with it, and the cached tracer with it."""
+        target, t_ref = ref_run["plain"]["rmse"], ref_run["plain"]["ms"]
+        r = nee_run["plain_to_reference_rmse"]
+        first = next((c for c in nee_run["cache_curve"] if c[2] <= target), None)
+        return {"target_rmse": target, "reference_plain_ms": t_ref,
+                "plain_nee_ratio": round(r["ms"] / t_ref, 4) if r and r["rmse"] is not None else None,
+                "plain_nee": r,
+                "cache_nee_ratio": round(first[1] / t_ref, 4) if first else None,
+                "cache_nee": {"spp": first[0], "ms": first[1], "rmse": first[2]} if first else None,
+                "cache_vs_plain_both_nee": nee_run["ratio"]}
     if rank == 0:
-        rc_p = rc_default_params()
+        rc_p = rc_params()
         line = {"metric": "time-to-equal-RMSE (cache / plain, vs FP64 image)", "value": main_run["ratio"],
                 "unit": "x", "n_gpus": world, "steps": main_run["cache"]["spp"] // spf, "warmup": args.warmup,
                 "ms_per_step": round(main_run["cache"]["ms"] / max(1, main_run["cache"]["spp"] // spf), 3),
@@ -894,6 +937,10 @@ def run_cache(args, w, world, rank, local):
                 "dtype": "f32 tracing, bf16 MLP (f32 accumulate)", "data": "synthetic (seeded host generator)",
                 "config": workload_config("c4", w, n, "scene arrays 1.4 GB > 126 MB L2, no flush needed"),
                 "stratified": main_run, "unstratified": alt,
+                "next_event": ({"stratified": nee_summary(main_run, nee_runs[0]),
+                                "unstratified": nee_summary(alt, nee_runs[1]),
+                                "runs": {"stratified": nee_runs[0], "unstratified": nee_runs[1]}}
+                               if nee_runs else None),
                 "rc_params": {"train_samples": rc_p.train_samples, "train_steps": rc_p.train_steps,
                               "learning_rate": rc_p.learning_rate, "beta2": rc_p.beta2},
                 "gpu_launches": main_run["launches"]}
@@ -915,6 +962,10 @@ def main():
     ap.add_argument("--spp", type=int, default=None, help="override samples per frame (profiling runs)")
     ap.add_argument("--wave-paths", type=int, default=0, help="paths per wave (0: library default)")
     ap.add_argument("--ray-sort", type=int, default=0, help="1: coherence-sort bounce queues")
+    ap.add_argument("--rc-per-call", action="store_true",
+                    help="c4: 2^16 training suffixes per render call instead of per image sample")
+    ap.add_argument("--nee", type=int, default=1,
+                    help="c4: also compare with next-event estimation in both tracers (1) or not (0)")
     ap.add_argument("--split", type=float, default=None,
                     help="split traversal BVH extra-piece ratio (0: traverse the LBVH; default per workload)")
     args = ap.parse_args()

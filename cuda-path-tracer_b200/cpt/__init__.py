@@ -69,7 +69,8 @@ class Bvh(ctypes.Structure):
 
 class Scene(ctypes.Structure):
     _fields_ = [("infos", ctypes.c_void_p), ("info_count", ctypes.c_uint32), ("lights", ctypes.c_void_p),
-                ("light_count", ctypes.c_uint32), ("textures", ctypes.c_void_p), ("texture_count", ctypes.c_uint32)]
+                ("light_count", ctypes.c_uint32), ("textures", ctypes.c_void_p), ("texture_count", ctypes.c_uint32),
+                ("emitters", ctypes.c_void_p)]
 
 
 class Camera(ctypes.Structure):
@@ -95,7 +96,7 @@ class RenderParams(ctypes.Structure):
                 ("stratified", ctypes.c_uint32), ("seed_lo", ctypes.c_uint32), ("seed_hi", ctypes.c_uint32),
                 ("accum_mode", ctypes.c_uint32), ("ref_grid", ctypes.c_uint32), ("wave_paths", ctypes.c_uint32),
                 ("trace_stats", ctypes.c_uint32), ("ray_sort", ctypes.c_uint32), ("cameras", ctypes.c_uint32),
-                ("frame_counter", ctypes.c_void_p)]
+                ("frame_counter", ctypes.c_void_p), ("nee", ctypes.c_uint32)]
 
 
 def _load() -> ctypes.CDLL:
@@ -127,6 +128,9 @@ _PROTOS = {
     "cpt_render": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Scene), ctypes.c_void_p,
                           ctypes.POINTER(RenderParams), _P, _P, _SZ, _P, _P, _P]),
     "cpt_resolve": (_I32, [_P, _U32, _U32, _U32, _P, _P]),
+    "cpt_emitters_bytes": (_SZ, [_U32, _U32]),
+    "cpt_emitters_build": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Scene), _U32, _P, _SZ,
+                                  ctypes.POINTER(_U32), _P]),
     "cpt_render_views_scratch_bytes": (_SZ, [_P, _U32, ctypes.POINTER(RenderParams)]),
     "cpt_render_views": (_I32, [_P, _U32, ctypes.POINTER(RenderParams), _P, _SZ, _P, _P, _P]),
     "cpt_rc_default_params": (None, [ctypes.POINTER(RcParams)]),
@@ -148,6 +152,7 @@ _PROTOS = {
     "cpt_tracer_upload": (_I32, [_P, _P, _U32, _P, _U32, _P, _U32, _P]),
     "cpt_tracer_upload_textures": (_I32, [_P, _P, _U32]),
     "cpt_tracer_set_split": (_I32, [_P, _F, _U32]),
+    "cpt_tracer_set_nee": (_I32, [_P, _U32]),
     "cpt_tracer_set_primary_rays": (_I32, [_P, _P]),
     "cpt_tracer_set_eye": (_I32, [_P, _P]),
     "cpt_tracer_set_camera": (_I32, [_P, ctypes.POINTER(Camera)]),
@@ -303,6 +308,20 @@ def render(bvh: Bvh, scene: Scene, cam, params: RenderParams, accum: int, scratc
                          scratch, scratch_bytes, ray_counts or None, status or None, stream), "cpt_render")
 
 
+def emitters_bytes(n: int, max_emitters: int) -> int:
+    return int(lib.cpt_emitters_bytes(n, max_emitters))
+
+
+def emitters_build(bvh: Bvh, scene: Scene, max_emitters: int, table: int, table_bytes: int, stream: int = 0,
+                   sync: bool = True) -> int | None:
+    """Emitter table of bvh's emissive triangles (next-event estimation). With sync,
+    returns the number of emitters (raises if more than max_emitters)."""
+    count = _U32(0)
+    check(lib.cpt_emitters_build(ctypes.byref(bvh), ctypes.byref(scene), max_emitters, table, table_bytes,
+                                 ctypes.byref(count) if sync else None, stream), "cpt_emitters_build")
+    return int(count.value) if sync else None
+
+
 def resolve(accum: int, width: int, height: int, mode: int, rgba: int, stream: int = 0) -> None:
     check(lib.cpt_resolve(accum, width, height, mode, rgba, stream), "cpt_resolve")
 
@@ -314,7 +333,7 @@ def launch_count() -> int:
 RAY_COUNTS = 72
 KERNELS = ("k_bounds", "k_morton", "k_scan_offsets", "k_onesweep", "k_topology", "k_gather_refit", "k_trace",
            "k_generate", "k_extend", "k_shade", "k_wave_counts", "k_accumulate", "k_resolve", "k_ray_sort",
-           "k_rc_infer", "k_rc_train", "k_rc_adam", "k_rc_collect")
+           "k_rc_infer", "k_rc_train", "k_rc_adam", "k_rc_collect", "k_occlude")
 
 
 def profile_begin() -> None:
@@ -394,6 +413,10 @@ class Tracer:
 
     def set_split(self, extra_ratio: float, flags: int = 0) -> None:
         check(lib.cpt_tracer_set_split(self._h, float(extra_ratio), int(flags)), "cpt_tracer_set_split")
+
+    def set_nee(self, on: bool) -> None:
+        """Next-event estimation on / off (restarts the accumulation when it changes)."""
+        check(lib.cpt_tracer_set_nee(self._h, int(bool(on))), "cpt_tracer_set_nee")
 
     def upload_textures(self, textures) -> None:
         table = texture_handles(textures)

@@ -12,7 +12,7 @@ import torch
 import ctypes
 
 from . import (ACCUM_KAHAN, BBOX_DTYPE, RcParams, BUILD_CHECK, TRIANGLE_DTYPE, Bvh, Camera, RenderParams, Scene, View, accum_bytes,
-               bvh_bind, bvh_bytes, check, lbvh_build, lbvh_scratch_bytes, lib, render, render_scratch_bytes, resolve,
+               bvh_bind, bvh_bytes, check, emitters_build, emitters_bytes, lbvh_build, lbvh_scratch_bytes, lib, render, render_scratch_bytes, resolve,
                status_check, texture_handles, trace)
 
 
@@ -126,14 +126,28 @@ class DeviceScene:
         self.texture_table = to_device(table.view(np.uint8), device) if len(table) else None
         self.scene = Scene(self.infos.data_ptr(), self.n_infos, self.lights.data_ptr() if self.n_lights else None,
                            self.n_lights, self.texture_table.data_ptr() if len(table) else None, len(table))
+        self.emitters = None
+        self.emitter_count = None
+
+    def build_emitters(self, lbvh: "DeviceLbvh", max_emitters: int = 1 << 16, stream: int | None = None,
+                       sync: bool = True) -> int | None:
+        """(Re)builds the emitter table of lbvh's triangles for next-event estimation
+        and attaches it to this scene. Call again after every rebuild of lbvh."""
+        nbytes = emitters_bytes(lbvh.n, max_emitters)
+        if self.emitters is None or self.emitters.numel() < nbytes:
+            self.emitters = dev_bytes(nbytes, self.infos.device)
+        self.scene.emitters = self.emitters.data_ptr()
+        self.emitter_count = emitters_build(lbvh.bvh, self.scene, max_emitters, self.emitters.data_ptr(), nbytes,
+                                            stream_handle() if stream is None else stream, sync)
+        return self.emitter_count
 
 
 def make_params(width, height, spp, frame0=0, bounces=3, intensity=3.0, stratified=True, seed=0,
                 accum_mode=ACCUM_KAHAN, ref_grid=False, wave_paths=0, trace_stats=False,
-                ray_sort=False, cameras=1) -> RenderParams:
+                ray_sort=False, cameras=1, nee=False) -> RenderParams:
     return RenderParams(width, height, spp, frame0, bounces, intensity, int(stratified), seed & 0xFFFFFFFF,
                         (seed >> 32) & 0xFFFFFFFF, accum_mode, int(ref_grid), wave_paths, int(trace_stats),
-                        int(ray_sort), cameras)
+                        int(ray_sort), cameras, None, int(nee))
 
 
 class DeviceRenderer:
@@ -210,10 +224,14 @@ class BatchRenderer:
         self.counts = torch.zeros(72, dtype=torch.int64, device=device or "cuda")
         self.status = torch.zeros(4, dtype=torch.int32, device=device or "cuda")
 
-    def render(self, frame0: int | None = None, stream: int | None = None) -> None:
+    def render(self, frame0: int | None = None, stream: int | None = None, spp: int | None = None) -> None:
         p = RenderParams.from_buffer_copy(self.params)
         if frame0 is not None:
             p.frame0 = frame0
+        if spp is not None:
+            if spp > self.params.spp:
+                raise ValueError("spp above the scratch's sizing")
+            p.spp = spp
         check(lib.cpt_render_views(self.views, len(self.accums), ctypes.byref(p), self.scratch.data_ptr(),
                                    self.scratch_bytes, self.counts.data_ptr(), self.status.data_ptr(),
                                    stream_handle() if stream is None else stream), "cpt_render_views")

@@ -39,7 +39,7 @@ int sm_count();
 enum KernelId {
     K_BOUNDS, K_MORTON, K_SCAN, K_ONESWEEP, K_TOPOLOGY, K_GATHER_REFIT, K_TRACE,
     K_GENERATE, K_EXTEND, K_SHADE, K_WAVE_COUNTS, K_ACCUMULATE, K_RESOLVE, K_RAY_SORT,
-    K_RC_INFER, K_RC_TRAIN, K_RC_ADAM, K_RC_COLLECT, K_KERNEL_COUNT
+    K_RC_INFER, K_RC_TRAIN, K_RC_ADAM, K_RC_COLLECT, K_OCCLUDE, K_KERNEL_COUNT
 };
 extern const char* const kKernelNames[K_KERNEL_COUNT];
 extern std::atomic<bool> g_profiling;

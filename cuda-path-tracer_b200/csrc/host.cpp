@@ -21,7 +21,7 @@ std::atomic<bool> g_profiling{false};
 const char* const kKernelNames[K_KERNEL_COUNT] = {
     "k_bounds", "k_morton", "k_scan_offsets", "k_onesweep", "k_topology", "k_gather_refit", "k_trace",
     "k_generate", "k_extend", "k_shade", "k_wave_counts", "k_accumulate", "k_resolve", "k_ray_sort",
-    "k_rc_infer", "k_rc_train", "k_rc_adam", "k_rc_collect"};
+    "k_rc_infer", "k_rc_train", "k_rc_adam", "k_rc_collect", "k_occlude"};
 
 namespace {
 struct ProfRecord { int id; cudaEvent_t a, b; };
@@ -447,6 +447,9 @@ struct cpt_tracer {
     void* d_textures = nullptr;  // cudaTextureObject_t handles (the caller owns the textures)
     size_t textures_cap = 0;
     uint32_t texture_count = 0;
+    void* d_emitters = nullptr;  // emitter table (cpt_tracer_set_nee)
+    size_t emitters_cap = 0;
+    bool nee = false, emitters_ready = false;
     cpt_bvh bvh{};
     bool ready = false;
     // frame
@@ -499,7 +502,8 @@ extern "C" void cpt_tracer_destroy(cpt_tracer* t)
     if (!t) return;
     if (t->stream) cudaStreamSynchronize(t->stream);
     void* bufs[] = {t->d_tris, t->d_bvh, t->d_build_scratch, t->d_infos, t->d_lights, t->d_textures, t->d_accum,
-                    t->d_render_scratch, t->d_image, t->d_counts, t->d_split_nodes, t->d_split_scratch};
+                    t->d_render_scratch, t->d_image, t->d_counts, t->d_split_nodes, t->d_split_scratch,
+                    t->d_emitters};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (t->stream) cudaStreamDestroy(t->stream);
@@ -545,6 +549,7 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
     t->light_count = light_count;
     t->frame = 0;  // CUDAPathTracer::upload resets the frame counter (cuda_path_tracer.cu:469)
     t->ready = true;
+    t->emitters_ready = false;
     CPT_CUDA_TRY(cudaMemsetAsync(t->d_counts, 0, CPT_RAY_COUNTS * sizeof(unsigned long long), t->stream));
     return CPT_OK;
 }
@@ -555,6 +560,33 @@ extern "C" int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio, uint32_t f
     t->split_ratio = extra_ratio;
     t->split_flags = flags;
     return CPT_OK;
+}
+
+extern "C" int cpt_tracer_set_nee(cpt_tracer* t, uint32_t on)
+{
+    if (!t || on > 1) return CPT_ERR_INVALID_ARGUMENT;
+    if ((on != 0) != t->nee) t->frame = 0;  // another estimator: start the accumulation again
+    t->nee = on != 0;
+    return CPT_OK;
+}
+
+// The emitter table of the uploaded scene, sized by a first count (synchronizes once per upload).
+static int tracer_emitters(cpt_tracer* t, const cpt_scene& sc)
+{
+    if (t->emitters_ready) return CPT_OK;
+    uint32_t cap = 1024, found = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        int rc = ensure(&t->d_emitters, &t->emitters_cap, cpt_emitters_bytes(t->n, cap));
+        if (rc) return rc;
+        rc = cpt_emitters_build(&t->bvh, &sc, cap, t->d_emitters, t->emitters_cap, &found, t->stream);
+        if (rc == CPT_OK) {
+            t->emitters_ready = true;
+            return CPT_OK;
+        }
+        if (rc != CPT_ERR_SCRATCH_TOO_SMALL) return rc;
+        cap = found;
+    }
+    return CPT_ERR_SCRATCH_TOO_SMALL;
 }
 
 extern "C" int cpt_tracer_upload_textures(cpt_tracer* t, const cudaTextureObject_t* textures, uint32_t count)
@@ -622,6 +654,7 @@ extern "C" int cpt_tracer_raytrace(cpt_tracer* t, uint32_t width, uint32_t heigh
     p.seed_lo = t->seed_lo;
     p.seed_hi = t->seed_hi;
     p.accum_mode = t->accum_mode;
+    p.nee = t->nee ? 1u : 0u;
     int rc;
     const size_t ab = cpt_accum_bytes(width, height, t->accum_mode), sb = cpt_render_scratch_bytes(&p);
     if (!sb) return CPT_ERR_INVALID_ARGUMENT;
@@ -633,7 +666,12 @@ extern "C" int cpt_tracer_raytrace(cpt_tracer* t, uint32_t width, uint32_t heigh
     if (t->frame == 0) CPT_CUDA_TRY(cudaMemsetAsync(t->d_accum, 0, ab, t->stream));
     cpt_scene sc{static_cast<const cpt_triangle_info*>(t->d_infos), t->info_count,
                  static_cast<const cpt_dir_light*>(t->d_lights), t->light_count,
-                 t->texture_count ? static_cast<const cudaTextureObject_t*>(t->d_textures) : nullptr, t->texture_count};
+                 t->texture_count ? static_cast<const cudaTextureObject_t*>(t->d_textures) : nullptr, t->texture_count,
+                 nullptr};
+    if (t->nee) {
+        if ((rc = tracer_emitters(t, sc))) return rc;
+        sc.emitters = t->d_emitters;
+    }
     rc = cpt_render(&t->bvh, &sc, &t->cam, &p, t->d_accum, t->d_render_scratch, t->render_cap, t->d_counts,
                     t->bvh.status, t->stream);
     if (rc) return rc;

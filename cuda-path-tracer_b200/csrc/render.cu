@@ -8,6 +8,10 @@
 //   k_extend      closest hit for every ray in queue b                      -> hits
 //   k_shade       shading of vertex b, shadow rays inline (any-hit),
 //                 next bounce direction                                      -> queue b+1
+//                 with next-event estimation: one shadow ray toward a point
+//                 on the emitters and its weighted emission                  -> shadow queue
+//   k_occlude     any-hit for every shadow ray; unoccluded ones add their
+//                 emission to the path's radiance                            -> path state
 //   k_accumulate  per pixel, the wave's samples in sample order              -> accumulators
 //
 // A "view" is one image: a BVH, its shading records and lights, a camera, a
@@ -59,6 +63,7 @@ struct View {
     const cpt_triangle_info* infos;
     const cpt_dir_light* lights;
     const cudaTextureObject_t* textures;
+    const float4* emitters;  // emitter table (next-event estimation), nullable
     void* accum;
     uint32_t info_count, light_count, max_visits, texture_count;
     uint32_t width, height, pixels, ref_w, ref_h;
@@ -351,7 +356,71 @@ __device__ __forceinline__ void surface(const View& v, const cpt_triangle_info& 
     }
 }
 
-template <bool kLights, bool kRecord>
+constexpr uint32_t kNeeCounter = 0x10000u;  // Philox counter word 2 of the emitter draws: this + depth
+constexpr float kPi = 3.14159265358979f;
+
+// Next-event estimate at a vertex that bounces (position hp, shading normal n, ray
+// origin of its bounce no = hp + n * 1e-5, path weight absorbed). The bounce it
+// stands beside samples w with density max(n . w, 0) / pi and, where it hits an
+// emitter, adds intensity * absorbed * e * max(-w . n_e, 0) (cuda_path_tracer.cu:
+// 269-284, 303-312). Here a point y is drawn on the emitters with density 1 / A
+// (a triangle by area, then uniformly on it), and the same integral over the
+// emitters' area is estimated as
+//     intensity * absorbed * e * max(-w . n_e, 0) * (n . w / pi) * |n_g . w| / r^2 * A,
+// w = (y - no) / r, n_e the emitter's shading normal at y (the reference's
+// `normal` of that hit), n_g its geometric normal. Returns false when the estimate
+// is zero; otherwise the shadow ray (origin no, far limit 0.9999 r, direction w)
+// and the emission it carries when unoccluded.
+__device__ __forceinline__ bool nee_sample(const View& v, f3 no, f3 n, f3 absorbed, float intensity, uint32_t pixel,
+                                           uint32_t frame, uint32_t depth, uint32_t vi, uint32_t k0, uint32_t k1,
+                                           float4& ro, float4& rd, f3& c, bool& bad)
+{
+    const float4 hdr = __ldg(v.emitters);
+    const uint32_t count = __float_as_uint(hdr.x);
+    const float total = hdr.y;
+    if (__float_as_uint(hdr.w)) bad = true;  // the table overflowed
+    if (count == 0 || !(total > 0.0f)) return false;
+    const uint4 r = philox4x32_10(make_uint4(pixel, frame, kNeeCounter + depth, vi), k0, k1);
+    const float up = u01(r.x), s1 = u01(r.y), s2 = u01(r.z);
+    const float4* rec = v.emitters + 1;
+    uint32_t lo = 0, hi = count - 1;  // the first emitter with up < cdf
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (up < __ldg(&rec[3 * (size_t)mid].w)) hi = mid;
+        else lo = mid + 1;
+    }
+    const float4 a = __ldg(rec + 3 * (size_t)lo), b = __ldg(rec + 3 * (size_t)lo + 1), e = __ldg(rec + 3 * (size_t)lo + 2);
+    const f3 v0 = xyz(a), e1 = xyz(b), e2 = xyz(e);
+    const float sq = __fsqrt_rn(s1);
+    const float bu = __fmul_rn(sq, __fsub_rn(1.0f, s2)), bw = __fmul_rn(sq, s2);
+    const f3 y = add(add(v0, muls(e1, bu)), muls(e2, bw));
+    const f3 dv = sub(y, no);
+    const float r2 = dot(dv, dv);
+    if (!(r2 > 0.0f)) return false;
+    const float dist = __fsqrt_rn(r2);
+    const f3 w = muls(dv, __frcp_rn(dist));
+    const float cos_x = dot(n, w);
+    if (!(cos_x > 0.0f)) return false;
+    const uint32_t tri = __float_as_uint(e.w);
+    const uint32_t info_idx = __ldg(&v.tris[tri].info_idx);
+    if (info_idx >= v.info_count) { bad = true; return false; }
+    const cpt_triangle_info& in = v.infos[info_idx];
+    f3 albedo_e, n_e;
+    surface(v, in, bu, bw, albedo_e, n_e);
+    const float cos_e = gmax(dot(neg(w), n_e), 0.0f);
+    if (!(cos_e > 0.0f)) return false;
+    const float cos_g = fabsf(dot(normalize(cross(e1, e2)), w));
+    const float g = __fdiv_rn(__fmul_rn(__fmul_rn(__fmul_rn(cos_x, cos_e), cos_g), total), __fmul_rn(r2, kPi));
+    c = muls(mul(absorbed, ld3(in.material.emission)), __fmul_rn(g, intensity));
+    ro = make_float4(no.x, no.y, no.z, __fmul_rn(dist, 0.9999f));
+    rd = make_float4(w.x, w.y, w.z, __uint_as_float(vi));
+    return true;
+}
+
+// kNee: next-event estimation (cpt_render_params.nee): emission hit by a bounce ray
+// is left out, and every vertex that bounces queues one shadow ray toward the
+// emitters (nee_sample) for k_occlude.
+template <bool kLights, bool kRecord, bool kNee>
 __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32_t depth,
                                                        const float4* __restrict__ queue_in,
                                                        const float4* __restrict__ hits,
@@ -359,7 +428,10 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
                                                        float4* __restrict__ queue_out, uint32_t* __restrict__ count_out,
                                                        float4* __restrict__ state,
                                                        unsigned long long* __restrict__ ray_counts,
-                                                       uint32_t* __restrict__ status)
+                                                       uint32_t* __restrict__ status,
+                                                       float4* __restrict__ shadow_rays,
+                                                       float4* __restrict__ shadow_emission,
+                                                       uint32_t* __restrict__ shadow_count)
 {
     __shared__ uint32_t s_stack[kLights ? kSmemStack * kShadeBlock : 1];
     uint32_t* stack = s_stack + (kLights ? threadIdx.x : 0);
@@ -373,6 +445,9 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
         bool bad_info = false;
         bool rec = false;
         float4 rec0, rec1, rec2, rec3, rec4;
+        bool nee = false;
+        float4 sro, srd;
+        f3 sc;
         if (i < n) {
             const float4 ro = queue_in[2 * (size_t)i], rd4 = queue_in[2 * (size_t)i + 1];
             const float4 hit4 = hits[i];
@@ -420,7 +495,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
                     absorbed = mk3(ab4.x, ab4.y, ab4.z);
                     f3 L = mk3(0.f, 0.f, 0.f);
                     if (emissive) {
-                        L = muls(e, gmax(dot(neg(d), normal), 0.0f));
+                        if (!kNee) L = muls(e, gmax(dot(neg(d), normal), 0.0f));
                         albedo = mk3(1.f, 1.f, 1.f);
                     } else if (kLights) {
                         for (uint32_t li = 0; li < v.light_count; ++li) {
@@ -466,6 +541,9 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
                     emit = true;
                     nro = make_float4(no.x, no.y, no.z, __uint_as_float(pid));
                     nrd = make_float4(nd.x, nd.y, nd.z, __uint_as_float(vi));
+                    if (kNee)
+                        nee = nee_sample(v, no, normal, absorbed, wv.intensity, y * v.width + x, frame, depth, vi,
+                                         wv.k0, wv.k1, sro, srd, sc, bad_info);
                 }
             }
         }
@@ -485,9 +563,54 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
                 r[4] = rec4;
             }
         }
-        if (kLights) warp_count_u64(ray_counts ? ray_counts + 2 : nullptr, shadow);
+        if (kNee) {
+            const uint32_t sq = warp_append(shadow_count, nee);
+            if (nee) {
+                shadow_rays[2 * (size_t)sq] = sro;
+                shadow_rays[2 * (size_t)sq + 1] = srd;
+                shadow_emission[sq] = make_float4(sc.x, sc.y, sc.z, __uint_as_float(__float_as_uint(nro.w)));
+                ++shadow;
+            }
+        }
+        if (kLights || kNee) warp_count_u64(ray_counts ? ray_counts + 2 : nullptr, shadow);
         if (bad_info) atomicOr(status, CPT_STATUS_BAD_INDEX);
     }
+    if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
+}
+
+// Shadow rays of next-event estimation: any-hit up to each ray's far limit; an
+// unoccluded ray adds its emission to its path's radiance (one shadow ray per
+// path and vertex, so no two threads add to the same path).
+template <bool kOneView>
+__global__ void __launch_bounds__(kExtendBlock, CPT_EXTEND_MIN_BLOCKS) k_occlude(Views vs, const float4* __restrict__ rays,
+                                                          const float4* __restrict__ emission,
+                                                          const uint32_t* __restrict__ count,
+                                                          uint32_t* __restrict__ pool, float4* __restrict__ state,
+                                                          uint32_t* __restrict__ status)
+{
+    __shared__ uint32_t s_stack[kSmemStack * kExtendBlock];
+    const uint32_t n = *count;
+    bool overflow = false;
+    uint32_t nn = 0, nt = 0;
+    const float4* nodes0 = vs.v[0].nodes;
+    const uint32_t visits0 = vs.v[0].max_visits;
+    auto view_nodes = [&](uint32_t vi, uint32_t& max_visits) -> const float4* {
+        if (kOneView) {
+            max_visits = visits0;
+            return nodes0;
+        }
+        max_visits = vs.v[vi].max_visits;
+        return vs.v[vi].nodes;
+    };
+    persistent_trace<true, kExtendBlock, false, kExtendSteps, true>(
+        view_nodes, rays, n, pool, s_stack + threadIdx.x, overflow, nn, nt, nullptr,
+        [&](uint32_t ray, const TraceState& s) {
+            if (s.best.tri != CPT_INVALID_INDEX) return;
+            const float4 c = emission[ray];
+            float4* st = state + 2 * (size_t)__float_as_uint(c.w);
+            const float4 a = *st;
+            *st = make_float4(__fadd_rn(a.x, c.x), __fadd_rn(a.y, c.y), __fadd_rn(a.z, c.z), a.w);
+        });
     if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
 }
 
@@ -575,8 +698,12 @@ __global__ void __launch_bounds__(256) k_resolve(const void* __restrict__ accum,
     }
 }
 
-constexpr int kCountWords = 2 * (kMaxDepth + 2) + 1;
-constexpr int kRecordCountWord = 2 * (kMaxDepth + 2);
+// Count words: queue counts, extension-ray pools, shadow-queue counts, shadow-ray
+// pools (kMaxDepth + 2 each), then the record count.
+constexpr int kCountWords = 4 * (kMaxDepth + 2) + 1;
+constexpr int kShadowCountWord = 2 * (kMaxDepth + 2);
+constexpr int kShadowPoolWord = 3 * (kMaxDepth + 2);
+constexpr int kRecordCountWord = 4 * (kMaxDepth + 2);
 
 struct RenderScratch {
     float4* queue[2];
@@ -584,6 +711,8 @@ struct RenderScratch {
     float4* state;
     uint32_t* counts;
     uint32_t capacity;  // paths per wave
+    float4* shadow_rays;      // next-event estimation: 2 float4 per shadow ray
+    float4* shadow_emission;  // and its emission | path id
     // coherence sort of bounce queues
     uint32_t* sort_keys[2];
     uint32_t* sort_vals[2];
@@ -613,6 +742,12 @@ size_t render_layout(const cpt_render_params* p, uint64_t pixels, void* base, Re
     s.hits = c.take<float4>(s.capacity);
     s.state = c.take<float4>(2ull * s.capacity);
     s.counts = c.take<uint32_t>(kCountWords);  // queue counts, persistent-kernel ray pools, record count
+    if (p->nee) {
+        s.shadow_rays = c.take<float4>(2ull * s.capacity);
+        s.shadow_emission = c.take<float4>(s.capacity);
+    } else {
+        s.shadow_rays = s.shadow_emission = nullptr;
+    }
     if (p->ray_sort) {
         const size_t tiles = (s.capacity + kSortTile - 1) / kSortTile;
         for (int k = 0; k < 2; ++k) {
@@ -681,7 +816,7 @@ bool params_ok(const cpt_render_params* p, uint64_t pixels)
 {
     if (!p || p->spp == 0 || pixels == 0 || pixels > (1ull << 31)) return false;
     if (p->bounces + 1 > (uint32_t)kMaxDepth) return false;
-    if (p->accum_mode > CPT_ACCUM_F64) return false;
+    if (p->accum_mode > CPT_ACCUM_F64 || p->nee > 1) return false;
     return pixels * wave_samples(p, pixels) < (1ull << 31);
 }
 
@@ -699,14 +834,15 @@ void to_camera(const cpt_camera& src, Camera& cam)
 }
 
 // Fills the kernel-parameter view table; returns total pixels or 0 on a bad view.
-uint64_t make_views(const cpt_view* views, uint32_t n, uint32_t ref_grid, Views& vs)
+uint64_t make_views(const cpt_view* views, uint32_t n, uint32_t ref_grid, bool nee, Views& vs)
 {
     uint64_t total = 0;
     vs.n = n;
     for (uint32_t i = 0; i < n; ++i) {
         const cpt_view& s = views[i];
         if (!s.bvh || !s.scene || !s.bvh->nodes || !s.bvh->tris || !s.scene->infos || !s.accum || s.width == 0 ||
-            s.height == 0 || (s.scene->light_count && !s.scene->lights) || (reinterpret_cast<uintptr_t>(s.accum) & 15))
+            s.height == 0 || (s.scene->light_count && !s.scene->lights) || (reinterpret_cast<uintptr_t>(s.accum) & 15) ||
+            (nee && (!s.scene->emitters || (reinterpret_cast<uintptr_t>(s.scene->emitters) & 15))))
             return 0;
         View& v = vs.v[i];
         v.nodes = static_cast<const float4*>(s.bvh->split_nodes ? s.bvh->split_nodes : s.bvh->nodes);
@@ -714,6 +850,7 @@ uint64_t make_views(const cpt_view* views, uint32_t n, uint32_t ref_grid, Views&
         v.infos = s.scene->infos;
         v.lights = s.scene->lights;
         v.textures = s.scene->textures;
+        v.emitters = nee ? static_cast<const float4*>(s.scene->emitters) : nullptr;
         v.texture_count = s.scene->textures ? s.scene->texture_count : 0u;
         v.accum = s.accum;
         v.info_count = s.scene->info_count;
@@ -805,20 +942,43 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
 #undef CPT_EXTEND
             }
             CPT_LAUNCH_CHECK();
+            const bool nee_here = params->nee && b < params->bounces;
             {
                 CPT_PROF(K_SHADE, stream);
-#define CPT_SHADE(L, R)                                                                                          \
-    k_shade<L, R><<<shade_blocks, kShadeBlock, 0, stream>>>(vs, wv, b, qin, rs.hits, rs.counts + b, qout,        \
-                                                            rs.counts + b + 1, rs.state, ray_counts, status)
+#define CPT_SHADE(L, R, N)                                                                                          \
+    k_shade<L, R, N><<<shade_blocks, kShadeBlock, 0, stream>>>(vs, wv, b, qin, rs.hits, rs.counts + b, qout,        \
+                                                               rs.counts + b + 1, rs.state, ray_counts, status,    \
+                                                               rs.shadow_rays, rs.shadow_emission,                 \
+                                                               rs.counts + kShadowCountWord + b)
                 const bool rec_here = record && b == wv.record_depth;
-                if (any_lights) {
-                    if (rec_here) CPT_SHADE(true, true); else CPT_SHADE(true, false);
+                if (params->nee) {  // (the last vertex queues no shadow ray: it does not bounce)
+                    if (any_lights) {
+                        if (rec_here) CPT_SHADE(true, true, true); else CPT_SHADE(true, false, true);
+                    } else {
+                        if (rec_here) CPT_SHADE(false, true, true); else CPT_SHADE(false, false, true);
+                    }
                 } else {
-                    if (rec_here) CPT_SHADE(false, true); else CPT_SHADE(false, false);
+                    if (any_lights) {
+                        if (rec_here) CPT_SHADE(true, true, false); else CPT_SHADE(true, false, false);
+                    } else {
+                        if (rec_here) CPT_SHADE(false, true, false); else CPT_SHADE(false, false, false);
+                    }
                 }
 #undef CPT_SHADE
             }
             CPT_LAUNCH_CHECK();
+            if (nee_here) {
+                CPT_PROF(K_OCCLUDE, stream);
+                uint32_t* spool = rs.counts + kShadowPoolWord + b;
+                const uint32_t* scount = rs.counts + kShadowCountWord + b;
+                if (one_bvh)
+                    k_occlude<true><<<ext_blocks, kExtendBlock, 0, stream>>>(vs, rs.shadow_rays, rs.shadow_emission,
+                                                                            scount, spool, rs.state, status);
+                else
+                    k_occlude<false><<<ext_blocks, kExtendBlock, 0, stream>>>(vs, rs.shadow_rays, rs.shadow_emission,
+                                                                             scount, spool, rs.state, status);
+                CPT_LAUNCH_CHECK();
+            }
         }
         if (ray_counts) {
             {
@@ -904,7 +1064,7 @@ int cpt::cpt_render_views_hooked(const cpt_view* views, uint32_t n_views, const 
     static Views vs;  // 14 KB: built on the host, passed by value to the kernels
     static std::mutex mu;
     std::lock_guard<std::mutex> lk(mu);
-    if (!make_views(views, n_views, params->ref_grid, vs)) return CPT_ERR_INVALID_ARGUMENT;
+    if (!make_views(views, n_views, params->ref_grid, params->nee != 0, vs)) return CPT_ERR_INVALID_ARGUMENT;
     bool lights = false;
     for (uint32_t i = 0; i < n_views; ++i) lights |= views[i].scene->light_count > 0;
     return render_views(vs, lights, views[0].bvh->node_boxes, params, scratch, scratch_bytes, ray_counts, status, hook,

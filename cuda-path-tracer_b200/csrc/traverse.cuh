@@ -250,22 +250,22 @@ __device__ __forceinline__ Hit traverse(const float4* __restrict__ nodes, f3 o, 
     return s.best;
 }
 
-// Persistent traversal of `n` rays: ray i is (origin, direction) = rays[2i], rays[2i+1];
-// its hit goes to hits[i]. nodes_of(w, max_visits) returns the node array (and the
-// visit bound) for the word w carried in the direction's .w (a view index, or
-// unused). Idle lanes take rays from *pool in warp-sized grabs (one atomic per
-// warp) whenever fewer than kRefillLanes lanes of the warp still trace (at most
-// kSteps node visits apart): refilling at every finished ray costs more in
+// Persistent traversal of `n` rays: ray i is (origin, direction) = rays[2i], rays[2i+1].
+// nodes_of(w, max_visits) returns the node array (and the visit bound) for the word
+// w carried in the direction's .w (a view index, or unused). kTmax: the origin's .w
+// is the ray's far limit (a triangle at t >= it is not a hit; shadow rays toward a
+// point); otherwise the ray is unbounded. done(i, state) is called once per ray when
+// its traversal ends. Idle lanes take rays from *pool in warp-sized grabs (one
+// atomic per warp) whenever fewer than kRefillLanes lanes of the warp still trace
+// (at most kSteps node visits apart): refilling at every finished ray costs more in
 // bookkeeping than the idle lanes do (C2: 16 lanes, 228 vs 194 Mrays/s).
-// ray_stats (nullable, with kStats): per ray (node fetches, triangle tests).
 // order (nullable): rays are taken in the order order[0], order[1], ... (a
-// permutation of 0..n-1); hits and stats stay indexed by the ray's own index.
-template <bool kAny, int kBlock, bool kStats, int kSteps, typename NodesOf>
-__device__ __forceinline__ void persistent_trace_views(NodesOf nodes_of, const float4* __restrict__ rays, uint32_t n,
-                                                       float4* __restrict__ hits, uint32_t* __restrict__ pool,
-                                                       uint32_t* smem_col, bool& overflow, uint32_t& n_nodes,
-                                                       uint32_t& n_tris, const uint32_t* __restrict__ order,
-                                                       uint2* __restrict__ ray_stats = nullptr)
+// permutation of 0..n-1); done() still receives the ray's own index.
+template <bool kAny, int kBlock, bool kStats, int kSteps, bool kTmax, typename NodesOf, typename Done>
+__device__ __forceinline__ void persistent_trace(NodesOf nodes_of, const float4* __restrict__ rays, uint32_t n,
+                                                 uint32_t* __restrict__ pool, uint32_t* smem_col, bool& overflow,
+                                                 uint32_t& n_nodes, uint32_t& n_tris, const uint32_t* __restrict__ order,
+                                                 Done done)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
@@ -291,6 +291,7 @@ __device__ __forceinline__ void persistent_trace_views(NodesOf nodes_of, const f
                         uint32_t mv;
                         const float4* nodes = nodes_of(__float_as_uint(rd.w), mv);
                         trace_init(s, nodes, mv, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z));
+                        if (kTmax) s.best.t = ro.w;
                     }
                 }
             }
@@ -302,8 +303,7 @@ __device__ __forceinline__ void persistent_trace_views(NodesOf nodes_of, const f
         for (int k = 1;; ++k) {
             if (ray != CPT_INVALID_INDEX &&
                 trace_step<kAny, kBlock, kStats>(s, smem_col, spill, overflow, n_nodes, n_tris)) {
-                hits[ray] = make_float4(s.best.t, s.best.u, s.best.v, __uint_as_float(s.best.tri));
-                if (kStats && ray_stats) ray_stats[ray] = make_uint2(s.visits, s.tests);
+                done(ray, s);
                 ray = CPT_INVALID_INDEX;
             }
             const unsigned live = __ballot_sync(0xFFFFFFFFu, ray != CPT_INVALID_INDEX);
@@ -311,6 +311,23 @@ __device__ __forceinline__ void persistent_trace_views(NodesOf nodes_of, const f
             if (!drained && (__popc(live) < kRefillLanes || k >= kSteps)) break;
         }
     }
+}
+
+// persistent_trace of unbounded rays whose hit goes to hits[i] = (t, u, v, triangle).
+// ray_stats (nullable, with kStats): per ray (node fetches, triangle tests).
+template <bool kAny, int kBlock, bool kStats, int kSteps, typename NodesOf>
+__device__ __forceinline__ void persistent_trace_views(NodesOf nodes_of, const float4* __restrict__ rays, uint32_t n,
+                                                       float4* __restrict__ hits, uint32_t* __restrict__ pool,
+                                                       uint32_t* smem_col, bool& overflow, uint32_t& n_nodes,
+                                                       uint32_t& n_tris, const uint32_t* __restrict__ order,
+                                                       uint2* __restrict__ ray_stats = nullptr)
+{
+    persistent_trace<kAny, kBlock, kStats, kSteps, false>(
+        nodes_of, rays, n, pool, smem_col, overflow, n_nodes, n_tris, order,
+        [&](uint32_t ray, const TraceState& s) {
+            hits[ray] = make_float4(s.best.t, s.best.u, s.best.v, __uint_as_float(s.best.tri));
+            if (kStats && ray_stats) ray_stats[ray] = make_uint2(s.visits, s.tests);
+        });
 }
 
 }  // namespace cpt

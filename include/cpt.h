@@ -166,6 +166,8 @@ typedef struct cpt_scene {
     uint32_t light_count;
     const cudaTextureObject_t* textures; /* device array of texture handles (cpt_texture_create), nullable */
     uint32_t texture_count;
+    const void* emitters;           /* device, nullable: emitter table (cpt_emitters_build) of this scene's
+                                     * BVH, read when cpt_render_params.nee is set */
 } cpt_scene;
 
 /* A 2D texture for albedo / normal maps: RGBA8 texels (host memory, row-major),
@@ -216,6 +218,8 @@ typedef struct cpt_render_params {
     uint32_t* frame_counter;   /* device, nullable: when set, the call renders global samples
                                 * *frame_counter + frame0 ... and adds spp to *frame_counter at its end, so a
                                 * call captured once in a CUDA graph renders the next samples on each replay */
+    uint32_t nee;              /* 1: next-event estimation (see cpt_emitters_build); every view's scene needs
+                                * an emitter table. 0: the reference's estimator */
 } cpt_render_params;
 
 size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode); /* per camera / view */
@@ -252,6 +256,32 @@ size_t cpt_render_views_scratch_bytes(const cpt_view* views, uint32_t n_views, c
 int cpt_render_views(const cpt_view* views, uint32_t n_views, const cpt_render_params* params, void* scratch,
                      size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status, cudaStream_t stream);
 
+/* ---- next-event estimation (an extension; no reference counterpart) ----
+ * The reference gathers emitted light only where a bounce ray happens to hit an
+ * emissive triangle (blinnPhongShadingPathTrace, cuda_path_tracer.cu:303-312), so a
+ * small light makes every sample a lottery. With cpt_render_params.nee = 1, every
+ * vertex that bounces also draws one point on the scene's emitters (a triangle by
+ * area, then a uniform point on it) and traces a shadow ray to it; emission hit by a
+ * bounce ray is then left out (the camera ray still sees it). The estimate has the
+ * expectation of the reference's estimator: the light the bounce would have picked
+ * up by chance, e * max(-w . n_e, 0) per hit, is integrated over the emitters'
+ * area instead, weighted by the cosine-sampling density cos(theta) / pi of the
+ * bounce it replaces.
+ *
+ * The emitter table lists the emissive triangles (emission r + g + b > 1e-7, the
+ * renderer's test) of a built BVH in sorted-triangle order:
+ *   16-B header: emitter count (u32), total area (f32), emitters found (u32),
+ *                1 when they did not fit (u32; the count is then 0)
+ *   48 B per emitter: (v0, cdf) (v1 - v0, area) (v2 - v0, sorted triangle index)
+ * It describes the triangles' current positions: build it again after every
+ * cpt_lbvh_build of the scene (the sorted order and the vertices change). */
+size_t cpt_emitters_bytes(uint32_t n, uint32_t max_emitters); /* n = bvh->n */
+/* count_out (host, nullable): when set, the call synchronizes the stream, stores
+ * the number of emissive triangles and returns CPT_ERR_SCRATCH_TOO_SMALL if they
+ * are more than max_emitters. */
+int cpt_emitters_build(const cpt_bvh* bvh, const cpt_scene* scene, uint32_t max_emitters, void* table,
+                       size_t table_bytes, uint32_t* count_out, cudaStream_t stream);
+
 /* Writes the displayable image (float4 rgba per pixel, alpha 1) of an accumulator. */
 int cpt_resolve(const void* accum, uint32_t width, uint32_t height, uint32_t accum_mode, float* rgba,
                 cudaStream_t stream);
@@ -282,6 +312,10 @@ int cpt_tracer_upload_textures(cpt_tracer* t, const cudaTextureObject_t* texture
 /* extra_ratio > 0: every later upload also builds the split traversal BVH
  * (cpt_lbvh_split with `flags`) and renders through it; 0 (default) renders over the LBVH. */
 int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio, uint32_t flags);
+/* on = 1: render with next-event estimation (cpt_render_params.nee); the tracer
+ * builds the uploaded scene's emitter table on the next raytrace. Switching
+ * restarts the accumulation (frame 0). Default 0: the reference's estimator. */
+int cpt_tracer_set_nee(cpt_tracer* t, uint32_t on);
 int cpt_tracer_set_primary_rays(cpt_tracer* t, const float dirs[12]);
 int cpt_tracer_set_eye(cpt_tracer* t, const float eye[3]);
 int cpt_tracer_set_camera(cpt_tracer* t, const cpt_camera* cam);

@@ -325,14 +325,14 @@ static inline float child_hit(const obvh* b, v3 o, v3 d, v3 dinv, uint32_t idx, 
 
 /* Closest hit (any_hit = 0) or first hit (any_hit = 1; same visiting order, stops
  * at the first recorded triangle, so its hit/miss equals the closest-hit's). */
-static float trace_ray(const obvh* b, v3 o, v3 d, int any_hit, uint32_t* idx_out, float* u_out, float* v_out,
-                       ostats* st)
+static float trace_ray_lim(const obvh* b, v3 o, v3 d, int any_hit, float tmax, uint32_t* idx_out, float* u_out,
+                           float* v_out, ostats* st)
 {
     v3 dinv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     uint32_t stack[STACK_CAP];
     int top = 0;
     stack[top++] = 0u; /* Node::makeInternal(0): the root */
-    float best = FLT_MAX;
+    float best = tmax; /* FLT_MAX: unbounded; otherwise a hit must lie nearer than tmax */
     uint32_t best_idx = INVALID_IDX;
     float bu = 0.f, bv = 0.f;
     while (top > 0) {
@@ -373,6 +373,12 @@ done:
     *u_out = bu;
     *v_out = bv;
     return best;
+}
+
+static float trace_ray(const obvh* b, v3 o, v3 d, int any_hit, uint32_t* idx_out, float* u_out, float* v_out,
+                       ostats* st)
+{
+    return trace_ray_lim(b, o, d, any_hit, FLT_MAX, idx_out, u_out, v_out, st);
 }
 
 /* rays: m x 6 floats (origin, direction). Outputs per ray: t (FLT_MAX on miss),
@@ -530,6 +536,112 @@ static inline const oinfo* info_of(const oscene* sc, uint32_t sorted_idx)
     return &sc->infos[sc->bvh.tris[sorted_idx].info];
 }
 
+/* ---- next-event estimation (an extension of the renderer, no reference counterpart) ----
+ * Emitter table, restated from the product's layout: a 16-B header (count, total
+ * area, emitters found, overflow flag) and 48 B per emitter, (v0, cdf)
+ * (v1 - v0, area) (v2 - v0, sorted triangle index), the emissive triangles
+ * (emission r + g + b > 1e-7) in sorted order; area = 0.5 |e1 x e2|; cdf summed
+ * in segments of 256 emitters (partial sums in each segment, then the segment
+ * totals in order), cdf_j = (segment offset + partial sum) / total.
+ * Returns the number of emitters found; the table holds them when <= cap. */
+#define NEE_SEG 256u
+uint32_t orc_emitters(const otri* sorted, uint32_t n, const oinfo* infos, uint32_t info_count, uint32_t cap,
+                      float* table)
+{
+    uint32_t found = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t ii = sorted[i].info;
+        if (ii < info_count && emission_sum(&infos[ii].m) > 1e-7f) ++found;
+    }
+    uint32_t count = found <= cap ? found : 0u, overflow = found <= cap ? 0u : 1u;
+    float* rec = table + 4;
+    uint32_t j = 0;
+    for (uint32_t i = 0; i < n && count; ++i) {
+        uint32_t ii = sorted[i].info;
+        if (!(ii < info_count && emission_sum(&infos[ii].m) > 1e-7f)) continue;
+        v3 v0 = ld3(sorted[i].v0), e1 = sub(ld3(sorted[i].v1), v0), e2 = sub(ld3(sorted[i].v2), v0);
+        v3 c = cross(e1, e2);
+        float* r = rec + 12 * (size_t)j++;
+        r[0] = v0.x; r[1] = v0.y; r[2] = v0.z; r[3] = 0.f;
+        r[4] = e1.x; r[5] = e1.y; r[6] = e1.z; r[7] = 0.5f * sqrtf(dot(c, c));
+        r[8] = e2.x; r[9] = e2.y; r[10] = e2.z; memcpy(&r[11], &i, 4);
+    }
+    float total = 0.f;
+    uint32_t segs = (count + NEE_SEG - 1) / NEE_SEG;
+    for (uint32_t sgi = 0; sgi < segs; ++sgi) {
+        float seg = 0.f;
+        for (uint32_t k = sgi * NEE_SEG; k < count && k < (sgi + 1) * NEE_SEG; ++k) seg += rec[12 * (size_t)k + 7];
+        total += seg;
+    }
+    float off = 0.f;
+    for (uint32_t sgi = 0; sgi < segs; ++sgi) {
+        float sum = 0.f;
+        for (uint32_t k = sgi * NEE_SEG; k < count && k < (sgi + 1) * NEE_SEG; ++k) {
+            sum += rec[12 * (size_t)k + 7];
+            rec[12 * (size_t)k + 3] = total > 0.f ? (off + sum) / total : 0.f;
+        }
+        off += sum;
+    }
+    memcpy(&table[0], &count, 4);
+    table[1] = total;
+    memcpy(&table[2], &found, 4);
+    memcpy(&table[3], &overflow, 4);
+    return found;
+}
+
+/* The emitter table later renders estimate direct light with (NULL: the
+ * reference's estimator). */
+static const float* g_nee;
+void orc_set_nee(const float* table) { g_nee = table; }
+
+/* One emitter draw at a vertex that bounces (origin no of its bounce, shading
+ * normal n, path weight absorbed): a point y drawn with density 1 / A, the
+ * estimate intensity * absorbed * e * max(-w . n_e, 0) * (n . w / pi) *
+ * |n_g . w| / r^2 * A of the emission the bounce would pick up, and the shadow
+ * ray toward y (direction w, far limit 0.9999 r). Returns 0 when the estimate is 0. */
+static int nee_sample(const oscene* sc, v3 no, v3 n, v3 absorbed, uint32_t pixel, uint32_t frame, uint32_t depth,
+                      v3* c_out, v3* w_out, float* tmax)
+{
+    uint32_t count;
+    memcpy(&count, g_nee, 4);
+    float total = g_nee[1];
+    if (count == 0 || !(total > 0.0f)) return 0;
+    float up, s1, s2;
+    cpt_rng_nee_uniforms(sc->k0, sc->k1, pixel, frame, depth, sc->camera, &up, &s1, &s2);
+    const float* rec = g_nee + 4;
+    uint32_t lo = 0, hi = count - 1;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (up < rec[12 * (size_t)mid + 3]) hi = mid;
+        else lo = mid + 1;
+    }
+    const float* r = rec + 12 * (size_t)lo;
+    v3 v0 = ld3(r), e1 = ld3(r + 4), e2 = ld3(r + 8);
+    uint32_t tri;
+    memcpy(&tri, &r[11], 4);
+    float sq = sqrtf(s1);
+    float bu = sq * (1.0f - s2), bw = sq * s2;
+    v3 y = add(add(v0, muls(e1, bu)), muls(e2, bw));
+    v3 dv = sub(y, no);
+    float r2 = dot(dv, dv);
+    if (!(r2 > 0.0f)) return 0;
+    float dist = sqrtf(r2);
+    v3 w = muls(dv, 1.0f / dist);
+    float cos_x = dot(n, w);
+    if (!(cos_x > 0.0f)) return 0;
+    const oinfo* in = info_of(sc, tri);
+    v3 ae, ne;
+    surface(in, bu, bw, &ae, &ne);
+    float cos_e = gmax(dot(neg(w), ne), 0.0f);
+    if (!(cos_e > 0.0f)) return 0;
+    float cos_g = fabsf(dot(normalize(cross(e1, e2)), w));
+    float g = (((cos_x * cos_e) * cos_g) * total) / (r2 * 3.14159265358979f);
+    *c_out = muls(mul(absorbed, ld3(in->m.emission)), g * sc->intensity);
+    *w_out = w;
+    *tmax = dist * 0.9999f;
+    return 1;
+}
+
 /* One path (blinnPhongShadingPathTrace, cuda_path_tracer.cu:245-333). */
 static v3 path_radiance(const oscene* sc, v3 o, v3 d, uint32_t pixel, uint32_t frame, ocount* cnt)
 {
@@ -561,6 +673,17 @@ static v3 path_radiance(const oscene* sc, v3 o, v3 d, uint32_t pixel, uint32_t f
     v3 absorbed = albedo;
     for (uint32_t i = 0; i < sc->bounces; ++i) {
         v3 ro = add(hit, muls(normal, 1e-5f));
+        if (g_nee) {
+            v3 c, w;
+            float tmax;
+            if (nee_sample(sc, ro, normal, absorbed, pixel, frame, i, &c, &w, &tmax)) {
+                uint32_t si;
+                float su, sv;
+                trace_ray_lim(&sc->bvh, ro, w, 1, tmax, &si, &su, &sv, &st);
+                cnt->shadow++;
+                if (si == INVALID_IDX) acc = add(acc, c);
+            }
+        }
         float u0, u1;
         cpt_rng_bounce_uniforms(sc->k0, sc->k1, pixel, frame, i, sc->camera, &u0, &u1);
         float rx = u0, ry = u1;
@@ -582,7 +705,7 @@ static v3 path_radiance(const oscene* sc, v3 o, v3 d, uint32_t pixel, uint32_t f
         surface(in, u, v, &albedo, &normal);
         v3 L = mk(0.f, 0.f, 0.f);
         if (emission_sum(&in->m) > 1e-7f) {
-            L = muls(ld3(in->m.emission), gmax(dot(neg(rd), normal), 0.0f));
+            if (!g_nee) L = muls(ld3(in->m.emission), gmax(dot(neg(rd), normal), 0.0f));
             albedo = mk(1.f, 1.f, 1.f);
         } else {
             for (uint32_t l = 0; l < sc->light_count; ++l) {

@@ -12,6 +12,8 @@
  *   bounce i of pixel p, global sample f : counter (p, f, i, c)     -> words 0,1
  *     (c = camera index of a multi-camera render, 0 otherwise)
  *   camera jitter of global sample f     : counter (~0u, f, 0, 1)   -> words 0,1
+ *   emitter draw at vertex i (next-event estimation, an extension)
+ *                                        : counter (p, f, 0x10000 + i, c) -> words 0,1,2
  *   uniform from a word w                : (w >> 8) * 2^-24, in [0, 1)
  *
  * cpt_sincos_turns(u) returns sin(2*pi*u) and cos(2*pi*u). It replaces the
@@ -60,6 +62,18 @@ static inline void cpt_rng_bounce_uniforms(uint32_t k0, uint32_t k1, uint32_t pi
     cpt_philox4x32_10(ctr, k0, k1, o);
     *u0 = cpt_u01(o[0]);
     *u1 = cpt_u01(o[1]);
+}
+
+/* Next-event estimation at vertex `bounce`: counter (p, f, 0x10000 + bounce, c) ->
+ * words 0 (emitter), 1, 2 (point on it). */
+static inline void cpt_rng_nee_uniforms(uint32_t k0, uint32_t k1, uint32_t pixel, uint32_t sample, uint32_t bounce,
+                                        uint32_t camera, float* u0, float* u1, float* u2)
+{
+    uint32_t ctr[4] = {pixel, sample, 0x10000u + bounce, camera}, o[4];
+    cpt_philox4x32_10(ctr, k0, k1, o);
+    *u0 = cpt_u01(o[0]);
+    *u1 = cpt_u01(o[1]);
+    *u2 = cpt_u01(o[2]);
 }
 
 static inline void cpt_rng_jitter_uniforms(uint32_t k0, uint32_t k1, uint32_t sample, float* u0, float* u1)

@@ -55,6 +55,9 @@ def oracle_lib() -> ctypes.CDLL:
         L.orc_heatmap.argtypes = [P, P, ctypes.POINTER(OCam), U, U, P, P, P]
         L.orc_set_textures.argtypes = [P, U]
         L.orc_tex_sample.argtypes = [P, P, U, P]
+        L.orc_emitters.argtypes = [P, U, P, U, U, P]
+        L.orc_emitters.restype = U
+        L.orc_set_nee.argtypes = [P]
         _oracle = L
     return _oracle
 
@@ -187,19 +190,34 @@ def tex_sample(image: np.ndarray, uv: np.ndarray) -> np.ndarray:
     return out
 
 
+def emitters(b: BuildResult, infos: np.ndarray, cap: int) -> tuple[np.ndarray, int]:
+    """Emitter table (next-event estimation) of a build: (float32 array of
+    4 + 12 * cap words, emitters found)."""
+    table = np.zeros(4 + 12 * cap, np.float32)
+    infos = np.ascontiguousarray(infos)
+    found = oracle_lib().orc_emitters(_p(b.tris), len(b.tris), _p(infos), len(infos), cap, _p(table))
+    return table, int(found)
+
+
 def render(b: BuildResult, infos: np.ndarray, lights, width: int, height: int, spp: int, frame0: int, bounces: int,
            intensity: float, stratified: bool, seed: int, cam: OCam, rows=None, camera_index: int = 0,
-           textures=None):
+           textures=None, nee_table: np.ndarray | None = None):
     """Per-sample radiance (spp, rows, width, 3) float32 and ray counts (3,).
 
-    textures: list of (H, W, 4) uint8 images indexed by albedo_idx / normal_map_idx."""
+    textures: list of (H, W, 4) uint8 images indexed by albedo_idx / normal_map_idx.
+    nee_table: an emitter table (emitters()) to render with next-event estimation."""
     r0, r1 = (0, height) if rows is None else rows
     rad = np.zeros((spp, r1 - r0, width, 3), np.float32)
     counts = np.zeros(3, np.uint64)
     nl = 0 if lights is None else len(lights)
+    table = None if nee_table is None else np.ascontiguousarray(nee_table, np.float32)
     with _Textures(textures):
-        _render_call(b, infos, lights, nl, width, height, r0, r1, spp, frame0, bounces, intensity, stratified, seed,
-                     cam, camera_index, rad, counts)
+        oracle_lib().orc_set_nee(_p(table))
+        try:
+            _render_call(b, infos, lights, nl, width, height, r0, r1, spp, frame0, bounces, intensity, stratified,
+                         seed, cam, camera_index, rad, counts)
+        finally:
+            oracle_lib().orc_set_nee(None)
     return rad, counts
 
 
