@@ -524,6 +524,8 @@ def run_ours(args, w, world, rank, local):
     split = w.get("split", 0.0) if args.split is None else args.split
     if split > 0:
         lb.split(split, keep_scratch=True)
+    if args.wide:
+        lb.wide(keep_scratch=True)
     params = make_params(W_, H_, spp, 0, w["bounces"], 3.0, True, w["seed"], cpt.ACCUM_KAHAN,
                          wave_paths=args.wave_paths, ray_sort=bool(args.ray_sort), cameras=len(cams))
 
@@ -534,6 +536,8 @@ def run_ours(args, w, world, rank, local):
         lb.build(d_tris)
         if split > 0:
             lb.split(split, keep_scratch=True)
+        if args.wide:
+            lb.wide(keep_scratch=True)
     rend = DeviceRenderer(params, dev)
     stream = torch.cuda.current_stream()
     cached = None
@@ -618,7 +622,8 @@ def run_ours(args, w, world, rank, local):
     # --- roofline of the dominant kernel (closest-hit traversal, k_extend)
     ext_ms, ext_launches = prof.get("k_extend", (0.0, 0))
     rays_closest = int(counts[0] + counts[1])
-    alg_bytes = rays_closest * (32 + 16) + rays_closest * (64.0 * mean_nodes + 48.0 * mean_tris)
+    node_b = 80.0 if args.wide else 64.0  # a wide node record, or the compact two-child node
+    alg_bytes = rays_closest * (32 + 16) + rays_closest * (node_b * mean_nodes + 48.0 * mean_tris)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
     traffic = None
@@ -635,7 +640,7 @@ def run_ours(args, w, world, rank, local):
                 if peak_kind == "measured" else "fallback 6650 GB/s",
                 "traffic": traffic, "algorithmic_bytes_per_launch": round(alg_bytes / max(ext_launches, 1), 1),
                 "avg_launch_ms": round(ext_ms / max(ext_launches, 1), 4),
-                "bytes_per_ray": f"32 ray + 16 hit + 64 x {mean_nodes:.2f} nodes + 48 x {mean_tris:.2f} triangles",
+                "bytes_per_ray": f"32 ray + 16 hit + {node_b:.0f} x {mean_nodes:.2f} nodes + 48 x {mean_tris:.2f} triangles",
                 "rays_per_depth_first_frame": depth_rays,
                 "kernel_share": {k: round(v[0] / ms_total, 4) for k, v in sorted(prof.items())}}
 
@@ -663,6 +668,14 @@ def run_ours(args, w, world, rank, local):
         s1.record(stream)
         torch.cuda.synchronize()
         lbvh_topology["split_build_ms"] = round(s0.elapsed_time(s1), 3)
+        if args.wide:
+            lb.wide(keep_scratch=True)
+            torch.cuda.synchronize()
+            s0.record(stream)
+            lb.wide(keep_scratch=True)
+            s1.record(stream)
+            torch.cuda.synchronize()
+            lbvh_topology["wide_build_ms"] = round(s0.elapsed_time(s1), 3)
 
     # --- LBVH build of the same scene (device-resident triangles); the deforming
     # workload already rebuilt inside every timed step: those builds are reported
@@ -962,6 +975,8 @@ def main():
     ap.add_argument("--spp", type=int, default=None, help="override samples per frame (profiling runs)")
     ap.add_argument("--wave-paths", type=int, default=0, help="paths per wave (0: library default)")
     ap.add_argument("--ray-sort", type=int, default=0, help="1: coherence-sort bounce queues")
+    ap.add_argument("--wide", type=int, default=0,
+                    help="1: traverse the compressed 8-wide tree built from the (split) binary tree")
     ap.add_argument("--rc-per-call", action="store_true",
                     help="c4: 2^16 training suffixes per render call instead of per image sample")
     ap.add_argument("--nee", type=int, default=1,

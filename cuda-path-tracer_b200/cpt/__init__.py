@@ -64,7 +64,8 @@ class Bvh(ctypes.Structure):
     _fields_ = [("n", ctypes.c_uint32), ("morton_bits", ctypes.c_int32), ("tris", ctypes.c_void_p),
                 ("keys", ctypes.c_void_p), ("children", ctypes.c_void_p), ("parents_leaf", ctypes.c_void_p),
                 ("parents_internal", ctypes.c_void_p), ("node_boxes", ctypes.c_void_p), ("nodes", ctypes.c_void_p),
-                ("status", ctypes.c_void_p), ("split_nodes", ctypes.c_void_p), ("split_capacity", ctypes.c_uint32)]
+                ("status", ctypes.c_void_p), ("split_nodes", ctypes.c_void_p), ("split_capacity", ctypes.c_uint32),
+                ("wide_nodes", ctypes.c_void_p), ("wide_tris", ctypes.c_void_p), ("wide_capacity", ctypes.c_uint32)]
 
 
 class Scene(ctypes.Structure):
@@ -128,6 +129,8 @@ _PROTOS = {
     "cpt_render": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Scene), ctypes.c_void_p,
                           ctypes.POINTER(RenderParams), _P, _P, _SZ, _P, _P, _P]),
     "cpt_resolve": (_I32, [_P, _U32, _U32, _U32, _P, _P]),
+    "cpt_lbvh_wide_bytes": (_SZ, [_U32, ctypes.POINTER(_SZ), ctypes.POINTER(_SZ)]),
+    "cpt_lbvh_wide": (_I32, [ctypes.POINTER(Bvh), _P, _SZ, _P, _SZ, _P, _SZ, _P]),
     "cpt_emitters_bytes": (_SZ, [_U32, _U32]),
     "cpt_emitters_build": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Scene), _U32, _P, _SZ,
                                   ctypes.POINTER(_U32), _P]),

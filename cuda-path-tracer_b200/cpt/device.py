@@ -56,6 +56,42 @@ class DeviceLbvh:
     def status(self, stream: int | None = None) -> None:
         status_check(self.bvh.status, stream_handle() if stream is None else stream)
 
+    def status_words(self) -> np.ndarray:
+        """The four device status words (synchronizes): status bits, trace pool,
+        wide node count, wide triangle record count."""
+        torch.cuda.synchronize(self.mem.device)
+        off = self.bvh.status - self.mem.data_ptr()
+        return self.mem[off:off + 16].cpu().numpy().view(np.uint32).copy()
+
+    def wide(self, stream: int | None = None, keep_scratch: bool = False) -> None:
+        """Builds the compressed 8-wide traversal tree (cpt_lbvh_wide) from the binary
+        tree in use (the split tree when one was built); tracing and rendering then
+        traverse it. Call again after every build or split."""
+        leaves = self.bvh.split_capacity if self.bvh.split_nodes else self.n
+        nb, tb = ctypes.c_size_t(), ctypes.c_size_t()
+        sb = int(lib.cpt_lbvh_wide_bytes(leaves, ctypes.byref(nb), ctypes.byref(tb)))
+        if not sb:
+            raise ValueError("wide BVH parameters rejected")
+        dev = self.mem.device
+        if getattr(self, "wide_nodes", None) is None or self.wide_nodes.numel() < nb.value:
+            self.wide_nodes = dev_bytes(nb.value, dev)
+        if getattr(self, "wide_tris", None) is None or self.wide_tris.numel() < tb.value:
+            self.wide_tris = dev_bytes(tb.value, dev)
+        if getattr(self, "wide_scratch", None) is None or self.wide_scratch.numel() < sb:
+            self.wide_scratch = dev_bytes(sb, dev)
+        check(lib.cpt_lbvh_wide(ctypes.byref(self.bvh), self.wide_nodes.data_ptr(), self.wide_nodes.numel(),
+                                self.wide_tris.data_ptr(), self.wide_tris.numel(), self.wide_scratch.data_ptr(),
+                                self.wide_scratch.numel(), stream_handle() if stream is None else stream),
+              "cpt_lbvh_wide")
+        if not keep_scratch:
+            self.wide_scratch = None
+
+    def unwide(self) -> None:
+        """Back to the binary tree for tracing and rendering."""
+        self.bvh.wide_nodes = None
+        self.bvh.wide_tris = None
+        self.bvh.wide_capacity = 0
+
     def split(self, extra_ratio: float = 1.0, stream: int | None = None, keep_scratch: bool = False,
               flags: int = 0) -> None:
         """Builds the split traversal BVH (cpt_lbvh_split) over the built tree; tracing
@@ -77,9 +113,10 @@ class DeviceLbvh:
             self.split_scratch = None
 
     def unsplit(self) -> None:
-        """Back to traversing the LBVH itself."""
+        """Back to traversing the LBVH itself (a wide tree built from the split tree goes too)."""
         self.bvh.split_nodes = None
         self.bvh.split_capacity = 0
+        self.unwide()
 
     def download(self) -> dict:
         """Reference-format arrays plus the compact records, as numpy."""

@@ -410,6 +410,9 @@ extern "C" int cpt_bvh_bind(void* mem, size_t bytes, uint32_t n, int morton_bits
     out->status = c.take<uint32_t>(4);
     out->split_nodes = nullptr;
     out->split_capacity = 0;
+    out->wide_nodes = nullptr;
+    out->wide_tris = nullptr;
+    out->wide_capacity = 0;
     return CPT_OK;
 }
 
@@ -437,9 +440,12 @@ extern "C" int cpt_status_check(const uint32_t* d_status, cudaStream_t stream)
 extern "C" int cpt_lbvh_build(const cpt_triangle* tris_in, uint32_t n, const float* enclosing_box, int morton_bits,
                               cpt_bvh* bvh, void* scratch, size_t scratch_bytes, uint32_t flags, cudaStream_t stream)
 {
-    if (bvh) {  // a split tree of the previous build is stale
+    if (bvh) {  // split and wide trees of the previous build are stale
         bvh->split_nodes = nullptr;
         bvh->split_capacity = 0;
+        bvh->wide_nodes = nullptr;
+        bvh->wide_tris = nullptr;
+        bvh->wide_capacity = 0;
     }
     if (!tris_in || !bvh || !scratch || n < 2 || n > kMaxTriangles) return CPT_ERR_INVALID_ARGUMENT;
     if (morton_bits != 30 && morton_bits != 63) return CPT_ERR_INVALID_ARGUMENT;

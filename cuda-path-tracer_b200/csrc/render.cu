@@ -59,6 +59,9 @@ struct Camera {
 
 struct View {
     const float4* nodes;
+    const float4* wide_nodes;  // compressed wide tree (cpt_lbvh_wide), nullable
+    const float4* wide_tris;
+    uint32_t wide_cap;         // its node capacity
     const cpt_triangle* tris;  // Morton-sorted reference records (info_idx of a hit)
     const cpt_triangle_info* infos;
     const cpt_dir_light* lights;
@@ -254,17 +257,45 @@ __global__ void __launch_bounds__(kGenBlock) k_generate(Wave wv, Views vs, float
 #ifndef CPT_EXTEND_MIN_BLOCKS
 #define CPT_EXTEND_MIN_BLOCKS (1024 / CPT_EXTEND_BLOCK)  // 32 warps per SM: 64 registers
 #endif
-template <bool kStats, bool kOneView>
+// kWide: every view's wide tree (cpt_lbvh_wide) instead of its binary nodes.
+static_assert(kWideSmemStack * 2 == kSmemStack, "wide and binary stacks share the shared-memory buffer");
+template <bool kStats, bool kOneView, bool kWide>
 __global__ void __launch_bounds__(kExtendBlock, CPT_EXTEND_MIN_BLOCKS) k_extend(Views vs, const float4* __restrict__ queue,
                                                          const uint32_t* __restrict__ count, float4* __restrict__ hits,
                                                          uint32_t* __restrict__ pool,
                                                          unsigned long long* __restrict__ ray_counts,
                                                          uint32_t* __restrict__ status, const uint32_t* __restrict__ order)
 {
-    __shared__ uint32_t s_stack[kSmemStack * kExtendBlock];
+    __shared__ __align__(16) uint32_t s_stack[kSmemStack * kExtendBlock];
     const uint32_t n = *count;
     bool overflow = false;
     uint32_t nn = 0, nt = 0;
+    if constexpr (kWide) {
+        const float4* wn0 = vs.v[0].wide_nodes;
+        const float4* wt0 = vs.v[0].wide_tris;
+        const uint32_t cap0 = vs.v[0].wide_cap;
+        auto wide_of = [&](uint32_t vi, uint32_t& mv, const float4*& tr) -> const float4* {
+            if (kOneView) {
+                mv = cap0;
+                tr = wt0;
+                return wn0;
+            }
+            mv = vs.v[vi].wide_cap;
+            tr = vs.v[vi].wide_tris;
+            return vs.v[vi].wide_nodes;
+        };
+        persistent_trace_wide<false, kExtendBlock, kStats, kExtendSteps, false>(
+            wide_of, queue, n, pool, reinterpret_cast<uint2*>(s_stack) + threadIdx.x, overflow, nn, nt, order,
+            [&](uint32_t ray, const WideState& s) {
+                hits[ray] = make_float4(s.best.t, s.best.u, s.best.v, __uint_as_float(s.best.tri));
+            });
+        if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
+        if (kStats && ray_counts) {
+            warp_count_u64(ray_counts + 3, nn);
+            warp_count_u64(ray_counts + 4, nt);
+        }
+        return;
+    }
     // each ray's view (direction .w) selects the node array it traverses
     const float4* nodes0 = vs.v[0].nodes;
     const uint32_t visits0 = vs.v[0].max_visits;
@@ -581,17 +612,37 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
 // Shadow rays of next-event estimation: any-hit up to each ray's far limit; an
 // unoccluded ray adds its emission to its path's radiance (one shadow ray per
 // path and vertex, so no two threads add to the same path).
-template <bool kOneView>
+template <bool kOneView, bool kWide>
 __global__ void __launch_bounds__(kExtendBlock, CPT_EXTEND_MIN_BLOCKS) k_occlude(Views vs, const float4* __restrict__ rays,
                                                           const float4* __restrict__ emission,
                                                           const uint32_t* __restrict__ count,
                                                           uint32_t* __restrict__ pool, float4* __restrict__ state,
                                                           uint32_t* __restrict__ status)
 {
-    __shared__ uint32_t s_stack[kSmemStack * kExtendBlock];
+    __shared__ __align__(16) uint32_t s_stack[kSmemStack * kExtendBlock];
     const uint32_t n = *count;
     bool overflow = false;
     uint32_t nn = 0, nt = 0;
+    auto add_unoccluded = [&](uint32_t ray, const Hit& best) {
+        if (best.tri != CPT_INVALID_INDEX) return;
+        const float4 c = emission[ray];
+        float4* st = state + 2 * (size_t)__float_as_uint(c.w);
+        const float4 a = *st;
+        *st = make_float4(__fadd_rn(a.x, c.x), __fadd_rn(a.y, c.y), __fadd_rn(a.z, c.z), a.w);
+    };
+    if constexpr (kWide) {
+        auto wide_of = [&](uint32_t vi, uint32_t& mv, const float4*& tr) -> const float4* {
+            const uint32_t v = kOneView ? 0u : vi;
+            mv = vs.v[v].wide_cap;
+            tr = vs.v[v].wide_tris;
+            return vs.v[v].wide_nodes;
+        };
+        persistent_trace_wide<true, kExtendBlock, false, kExtendSteps, true>(
+            wide_of, rays, n, pool, reinterpret_cast<uint2*>(s_stack) + threadIdx.x, overflow, nn, nt, nullptr,
+            [&](uint32_t ray, const WideState& s) { add_unoccluded(ray, s.best); });
+        if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
+        return;
+    }
     const float4* nodes0 = vs.v[0].nodes;
     const uint32_t visits0 = vs.v[0].max_visits;
     auto view_nodes = [&](uint32_t vi, uint32_t& max_visits) -> const float4* {
@@ -604,13 +655,7 @@ __global__ void __launch_bounds__(kExtendBlock, CPT_EXTEND_MIN_BLOCKS) k_occlude
     };
     persistent_trace<true, kExtendBlock, false, kExtendSteps, true>(
         view_nodes, rays, n, pool, s_stack + threadIdx.x, overflow, nn, nt, nullptr,
-        [&](uint32_t ray, const TraceState& s) {
-            if (s.best.tri != CPT_INVALID_INDEX) return;
-            const float4 c = emission[ray];
-            float4* st = state + 2 * (size_t)__float_as_uint(c.w);
-            const float4 a = *st;
-            *st = make_float4(__fadd_rn(a.x, c.x), __fadd_rn(a.y, c.y), __fadd_rn(a.z, c.z), a.w);
-        });
+        [&](uint32_t ray, const TraceState& s) { add_unoccluded(ray, s.best); });
     if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
 }
 
@@ -846,6 +891,9 @@ uint64_t make_views(const cpt_view* views, uint32_t n, uint32_t ref_grid, bool n
             return 0;
         View& v = vs.v[i];
         v.nodes = static_cast<const float4*>(s.bvh->split_nodes ? s.bvh->split_nodes : s.bvh->nodes);
+        v.wide_nodes = static_cast<const float4*>(s.bvh->wide_nodes);
+        v.wide_tris = static_cast<const float4*>(s.bvh->wide_tris);
+        v.wide_cap = s.bvh->wide_nodes ? s.bvh->wide_capacity - 1 : 0u;
         v.tris = s.bvh->tris;
         v.infos = s.scene->infos;
         v.lights = s.scene->lights;
@@ -897,12 +945,13 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
     wv.record_depth = hook ? hook->record_depth : 0u;
     const bool image = !hook || hook->image_pass;
 
-    bool one_bvh = true;
+    bool one_bvh = true, wide = true;
     for (uint32_t i = 1; i < vs.n; ++i) one_bvh &= vs.v[i].nodes == vs.v[0].nodes;
+    for (uint32_t i = 0; i < vs.n; ++i) wide &= vs.v[i].wide_nodes != nullptr;  // else every view's binary tree
     const int sms = sm_count();
     static int ext_occ = 0;
     if (!ext_occ) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ext_occ, k_extend<false, false>, kExtendBlock, 0) != cudaSuccess ||
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ext_occ, k_extend<false, false, false>, kExtendBlock, 0) != cudaSuccess ||
             ext_occ < 1)
             ext_occ = 1;
     }
@@ -932,12 +981,18 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
             {
                 CPT_PROF(K_EXTEND, stream);
                 uint32_t* pool = rs.counts + kMaxDepth + 2 + b;
-#define CPT_EXTEND(S, O) \
-    k_extend<S, O><<<ext_blocks, kExtendBlock, 0, stream>>>(vs, qin, rs.counts + b, rs.hits, pool, ray_counts, status, order)
-                if (params->trace_stats) {
-                    if (one_bvh) CPT_EXTEND(true, true); else CPT_EXTEND(true, false);
+#define CPT_EXTEND(S, O, W) \
+    k_extend<S, O, W><<<ext_blocks, kExtendBlock, 0, stream>>>(vs, qin, rs.counts + b, rs.hits, pool, ray_counts, status, order)
+                if (wide) {
+                    if (params->trace_stats) {
+                        if (one_bvh) CPT_EXTEND(true, true, true); else CPT_EXTEND(true, false, true);
+                    } else {
+                        if (one_bvh) CPT_EXTEND(false, true, true); else CPT_EXTEND(false, false, true);
+                    }
+                } else if (params->trace_stats) {
+                    if (one_bvh) CPT_EXTEND(true, true, false); else CPT_EXTEND(true, false, false);
                 } else {
-                    if (one_bvh) CPT_EXTEND(false, true); else CPT_EXTEND(false, false);
+                    if (one_bvh) CPT_EXTEND(false, true, false); else CPT_EXTEND(false, false, false);
                 }
 #undef CPT_EXTEND
             }
@@ -971,12 +1026,15 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
                 CPT_PROF(K_OCCLUDE, stream);
                 uint32_t* spool = rs.counts + kShadowPoolWord + b;
                 const uint32_t* scount = rs.counts + kShadowCountWord + b;
-                if (one_bvh)
-                    k_occlude<true><<<ext_blocks, kExtendBlock, 0, stream>>>(vs, rs.shadow_rays, rs.shadow_emission,
-                                                                            scount, spool, rs.state, status);
-                else
-                    k_occlude<false><<<ext_blocks, kExtendBlock, 0, stream>>>(vs, rs.shadow_rays, rs.shadow_emission,
-                                                                             scount, spool, rs.state, status);
+#define CPT_OCCLUDE(O, W)                                                                                   \
+    k_occlude<O, W><<<ext_blocks, kExtendBlock, 0, stream>>>(vs, rs.shadow_rays, rs.shadow_emission, scount, spool, \
+                                                             rs.state, status)
+                if (wide) {
+                    if (one_bvh) CPT_OCCLUDE(true, true); else CPT_OCCLUDE(false, true);
+                } else {
+                    if (one_bvh) CPT_OCCLUDE(true, false); else CPT_OCCLUDE(false, false);
+                }
+#undef CPT_OCCLUDE
                 CPT_LAUNCH_CHECK();
             }
         }

@@ -923,5 +923,8 @@ extern "C" int cpt_lbvh_split(cpt_bvh* bvh, float extra_ratio, uint32_t flags, v
     if (rc) return rc;
     bvh->split_nodes = nodes;
     bvh->split_capacity = cap;
+    bvh->wide_nodes = nullptr;  // a wide tree of the previous binary tree is stale
+    bvh->wide_tris = nullptr;
+    bvh->wide_capacity = 0;
     return CPT_OK;
 }

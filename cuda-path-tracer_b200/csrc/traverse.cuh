@@ -250,6 +250,192 @@ __device__ __forceinline__ Hit traverse(const float4* __restrict__ nodes, f3 o, 
     return s.best;
 }
 
+// ---------------------------------------------------------------------------
+// Compressed 8-wide BVH (cpt_lbvh_wide). A wide node is five float4: origin p and
+// per-axis exponents e (child box planes p + q * 2^e, q one byte), the masks of its
+// internal and leaf slots, the index of its first internal child and of its first
+// triangle record, and the 48 quantized planes. The ray carries a node group — the
+// hit internal slots of one node still to visit, in the order k ^ octant(ray) — and
+// a triangle group — the hit leaf slots of the node just visited. A step tests one
+// triangle of the triangle group, or else visits the next node of the node group
+// (the rest of the group goes on the stack), or else pops a group. The triangle test
+// is tri_test on the binary leaf slot's words, so a hit's t, u, v are unchanged.
+constexpr int kWideSmemStack = 16;  // stack entries (2 words) per thread in shared memory
+// The wide traversal refills as soon as one lane of the warp is idle: its steps are
+// long (8 child boxes), so an idle lane costs more than the refill's ballot and
+// atomic (C2: 313 Mrays/s at 32, 302 at 28, 283 at 24, 242 at 16, 196 at 8).
+#ifndef CPT_WIDE_REFILL_LANES
+#define CPT_WIDE_REFILL_LANES 32
+#endif
+constexpr int kWideRefillLanes = CPT_WIDE_REFILL_LANES;
+constexpr float kWideFarInv = 1099511627776.0f;  // 2^40: 1/d of a zero direction component
+
+struct WideState {
+    const float4* nodes;
+    const float4* tris;
+    uint32_t max_visits;  // wide node fetches allowed (the wide tree's node capacity)
+    uint32_t tri_cap;     // triangle records
+    f3 o, d, dinv;
+    uint32_t oct;         // direction sign bits (x: 1, y: 2, z: 4)
+    Hit best;
+    uint32_t cbase, gbits;  // node group: first child; bits 0-7 hit slots in visit order, 8-15 internal mask
+    uint32_t tbase, tbits;  // triangle group: first record; bits 0-7 hit leaf slots, 8-15 leaf mask
+    int sp;
+    uint32_t visits, tests;
+};
+
+__device__ __forceinline__ void wide_init(WideState& s, const float4* nodes, const float4* tris, uint32_t max_visits,
+                                          f3 o, f3 d)
+{
+    s.nodes = nodes;
+    s.tris = tris;
+    s.max_visits = max_visits;
+    s.tri_cap = max_visits + 1;
+    s.o = o;
+    s.d = d;
+    const float ix = __frcp_rn(d.x), iy = __frcp_rn(d.y), iz = __frcp_rn(d.z);
+    s.dinv = mk3(isfinite(ix) ? ix : copysignf(kWideFarInv, d.x), isfinite(iy) ? iy : copysignf(kWideFarInv, d.y),
+                 isfinite(iz) ? iz : copysignf(kWideFarInv, d.z));
+    s.oct = (s.dinv.x < 0.f ? 1u : 0u) | (s.dinv.y < 0.f ? 2u : 0u) | (s.dinv.z < 0.f ? 4u : 0u);
+    s.best.t = FLT_MAX;
+    s.best.u = 0.f;
+    s.best.v = 0.f;
+    s.best.tri = CPT_INVALID_INDEX;
+    s.cbase = 0;  // the root, wide node 0: the one internal slot (0) of a virtual parent, visited first
+    s.gbits = (1u << s.oct) | (1u << 8);
+    s.tbase = 0;
+    s.tbits = 0;
+    s.sp = 0;
+    s.visits = 0;
+    s.tests = 0;
+}
+
+// byte i of w plus 2^23, as a float: 0x4B0000qq is exactly 2^23 + q
+__device__ __forceinline__ float qbyte(uint32_t w, uint32_t sel)
+{
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, sel));
+}
+
+__device__ __forceinline__ float fmax3(float a, float b, float c)
+{
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+__device__ __forceinline__ float fmin3(float a, float b, float c)
+{
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// bit k of the result = bit (k ^ oct) of x (8-bit masks)
+__device__ __forceinline__ uint32_t xor_permute8(uint32_t x, uint32_t oct)
+{
+    x = (oct & 1u) ? (((x & 0x55u) << 1) | ((x >> 1) & 0x55u)) : x;
+    x = (oct & 2u) ? (((x & 0x33u) << 2) | ((x >> 2) & 0x33u)) : x;
+    x = (oct & 4u) ? (((x & 0x0Fu) << 4) | ((x >> 4) & 0x0Fu)) : x;
+    return x;
+}
+
+template <int kBlock>
+__device__ __forceinline__ void wide_push(uint2* smem_col, uint2* spill, int& sp, uint2 v, bool& overflow)
+{
+    if (sp < kWideSmemStack) smem_col[sp * kBlock] = v;
+    else if (sp < CPT_TRAVERSAL_STACK) spill[sp - kWideSmemStack] = v;
+    else { overflow = true; return; }
+    ++sp;
+}
+
+template <int kBlock>
+__device__ __forceinline__ uint2 wide_pop(const uint2* smem_col, const uint2* spill, int& sp)
+{
+    --sp;
+    return sp < kWideSmemStack ? smem_col[sp * kBlock] : spill[sp - kWideSmemStack];
+}
+
+// One step; returns true when the ray is finished.
+template <bool kAny, int kBlock, bool kStats>
+__device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* spill, bool& overflow,
+                                          uint32_t& n_nodes, uint32_t& n_tris)
+{
+    if (s.tbits & 0xFFu) {
+        const uint32_t slot = __ffs(s.tbits & 0xFFu) - 1;
+        s.tbits &= ~(1u << slot);
+        const uint32_t idx = s.tbase + __popc((s.tbits >> 8) & ((1u << slot) - 1u));
+        if (idx >= s.tri_cap) { overflow = true; return true; }
+        const float4 a = __ldg(s.tris + 3 * (size_t)idx), b = __ldg(s.tris + 3 * (size_t)idx + 1),
+                     c = __ldg(s.tris + 3 * (size_t)idx + 2);
+        const float w[10] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, c.x, c.y, c.z};
+        float u, v;
+        const float t = tri_test(s.o, s.d, w, u, v);
+        if (kStats) { ++n_tris; ++s.tests; }
+        if (t < s.best.t) {
+            s.best.t = t;
+            s.best.u = u;
+            s.best.v = v;
+            s.best.tri = __float_as_uint(a.w);
+            if (kAny) return true;
+        }
+        if (s.tbits & 0xFFu) return false;  // more triangles of this group: next step
+    }
+    if (!(s.gbits & 0xFFu)) {
+        if (s.sp == 0) return true;
+        const uint2 g = wide_pop<kBlock>(smem_col, spill, s.sp);
+        s.cbase = g.x;
+        s.gbits = g.y;
+    }
+    const uint32_t k = __ffs(s.gbits & 0xFFu) - 1;
+    s.gbits &= ~(1u << k);
+    const uint32_t slot = k ^ s.oct;
+    const uint32_t child = s.cbase + __popc((s.gbits >> 8) & ((1u << slot) - 1u));
+    if (s.gbits & 0xFFu) wide_push<kBlock>(smem_col, spill, s.sp, make_uint2(s.cbase, s.gbits), overflow);
+    if (++s.visits > s.max_visits || child >= s.max_visits) { overflow = true; return true; }
+    if (kStats) ++n_nodes;
+    const float4* nd = s.nodes + 5 * (size_t)child;
+    const float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3), n4 = __ldg(nd + 4);
+    const uint32_t ew = __float_as_uint(n0.w);
+    const uint32_t imask = ew >> 24, lmask = __float_as_uint(n1.z);
+    // plane t = q * (2^e / d) + (p - o) / d, evaluated as (2^23 + q) * a + (b - 2^23 * a): the
+    // folded offset costs at most half a quantum, and the build leaves one quantum of slack
+    const float sx = __uint_as_float((ew & 0xFFu) << 23), sy = __uint_as_float(((ew >> 8) & 0xFFu) << 23),
+                sz = __uint_as_float(((ew >> 16) & 0xFFu) << 23);
+    const float adx = sx * s.dinv.x, ady = sy * s.dinv.y, adz = sz * s.dinv.z;
+    const float bdx = fmaf(-8388608.0f, adx, (n0.x - s.o.x) * s.dinv.x);
+    const float bdy = fmaf(-8388608.0f, ady, (n0.y - s.o.y) * s.dinv.y);
+    const float bdz = fmaf(-8388608.0f, adz, (n0.z - s.o.z) * s.dinv.z);
+    // near / far planes per axis: lo and hi, swapped for a negative direction
+    const uint32_t lx0 = __float_as_uint(n2.x), lx1 = __float_as_uint(n2.y), ly0 = __float_as_uint(n2.z),
+                   ly1 = __float_as_uint(n2.w), lz0 = __float_as_uint(n3.x), lz1 = __float_as_uint(n3.y);
+    const uint32_t hx0 = __float_as_uint(n3.z), hx1 = __float_as_uint(n3.w), hy0 = __float_as_uint(n4.x),
+                   hy1 = __float_as_uint(n4.y), hz0 = __float_as_uint(n4.z), hz1 = __float_as_uint(n4.w);
+    const bool fx = s.oct & 1u, fy = s.oct & 2u, fz = s.oct & 4u;
+    const uint32_t nx0 = fx ? hx0 : lx0, nx1 = fx ? hx1 : lx1, fx0 = fx ? lx0 : hx0, fx1 = fx ? lx1 : hx1;
+    const uint32_t ny0 = fy ? hy0 : ly0, ny1 = fy ? hy1 : ly1, fy0 = fy ? ly0 : hy0, fy1 = fy ? ly1 : hy1;
+    const uint32_t nz0 = fz ? hz0 : lz0, nz1 = fz ? hz1 : lz1, fz0 = fz ? lz0 : hz0, fz1 = fz ? lz1 : hz1;
+    uint32_t hm = 0;
+    const float tlim = s.best.t;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t sel = 0x7440u | (uint32_t)(i & 3);
+        const float tnx = fmaf(qbyte(i < 4 ? nx0 : nx1, sel), adx, bdx);
+        const float tny = fmaf(qbyte(i < 4 ? ny0 : ny1, sel), ady, bdy);
+        const float tnz = fmaf(qbyte(i < 4 ? nz0 : nz1, sel), adz, bdz);
+        const float tfx = fmaf(qbyte(i < 4 ? fx0 : fx1, sel), adx, bdx);
+        const float tfy = fmaf(qbyte(i < 4 ? fy0 : fy1, sel), ady, bdy);
+        const float tfz = fmaf(qbyte(i < 4 ? fz0 : fz1, sel), adz, bdz);
+        // [max(tn, 0), min(tf, best)] non-empty (a superset of the binary test's hits on the boundary)
+        const float tn = fmaxf(fmax3(tnx, tny, tnz), 0.0f), tf = fminf(fmin3(tfx, tfy, tfz), tlim);
+        hm |= (tn <= tf ? 1u : 0u) << i;
+    }
+    s.cbase = __float_as_uint(n1.x);
+    s.gbits = xor_permute8(hm & imask, s.oct) | (imask << 8);
+    s.tbase = __float_as_uint(n1.y);
+    s.tbits = (hm & lmask) | (lmask << 8);
+    return false;
+}
+
 // Persistent traversal of `n` rays: ray i is (origin, direction) = rays[2i], rays[2i+1].
 // nodes_of(w, max_visits) returns the node array (and the visit bound) for the word
 // w carried in the direction's .w (a view index, or unused). kTmax: the origin's .w
@@ -309,6 +495,59 @@ __device__ __forceinline__ void persistent_trace(NodesOf nodes_of, const float4*
             const unsigned live = __ballot_sync(0xFFFFFFFFu, ray != CPT_INVALID_INDEX);
             if (live == 0) break;
             if (!drained && (__popc(live) < kRefillLanes || k >= kSteps)) break;
+        }
+    }
+}
+
+// persistent_trace over wide BVHs: wide_of(w, max_visits, tris) returns the wide
+// node array, its node capacity and its triangle records for the word w of the
+// direction's .w. Same refill rule and far-limit convention as persistent_trace.
+template <bool kAny, int kBlock, bool kStats, int kSteps, bool kTmax, typename WideOf, typename Done>
+__device__ __forceinline__ void persistent_trace_wide(WideOf wide_of, const float4* __restrict__ rays, uint32_t n,
+                                                      uint32_t* __restrict__ pool, uint2* smem_col, bool& overflow,
+                                                      uint32_t& n_nodes, uint32_t& n_tris,
+                                                      const uint32_t* __restrict__ order, Done done)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    uint2 spill[CPT_TRAVERSAL_STACK - kWideSmemStack];
+    WideState s;
+    uint32_t ray = CPT_INVALID_INDEX;
+    bool drained = false;
+    for (;;) {
+        if (!drained) {
+            const bool idle = ray == CPT_INVALID_INDEX;
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, idle);
+            if (m) {
+                const int leader = __ffs(m) - 1;
+                uint32_t base = 0;
+                if ((int)lane == leader) base = atomicAdd(pool, (uint32_t)__popc(m));
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                if (base + (uint32_t)__popc(m) >= n) drained = true;
+                if (idle) {
+                    const uint32_t r = base + (uint32_t)__popc(m & lt_mask);
+                    if (r < n) {
+                        ray = order ? order[r] : r;
+                        const float4 ro = rays[2 * (size_t)ray], rd = rays[2 * (size_t)ray + 1];
+                        uint32_t mv;
+                        const float4* tris;
+                        const float4* nodes = wide_of(__float_as_uint(rd.w), mv, tris);
+                        wide_init(s, nodes, tris, mv, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z));
+                        if (kTmax) s.best.t = ro.w;
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(0xFFFFFFFFu, ray != CPT_INVALID_INDEX) == 0) break;
+#pragma unroll 1
+        for (int k = 1;; ++k) {
+            if (ray != CPT_INVALID_INDEX && wide_step<kAny, kBlock, kStats>(s, smem_col, spill, overflow, n_nodes, n_tris)) {
+                done(ray, s);
+                ray = CPT_INVALID_INDEX;
+            }
+            const unsigned live = __ballot_sync(0xFFFFFFFFu, ray != CPT_INVALID_INDEX);
+            if (live == 0) break;
+            if (!drained && (__popc(live) < kWideRefillLanes || k >= kSteps)) break;
         }
     }
 }

@@ -1,0 +1,363 @@
+// Compressed 8-wide traversal BVH (cpt_lbvh_wide): an extension with no reference
+// counterpart, built from the binary traversal tree in use (the split tree when one
+// was built, else the LBVH's nodes). Hits are those of the binary tree up to the order
+// in which exactly equal distances are found: every triangle keeps its arithmetic
+// (the leaf record holds the binary leaf slot's words), only the culling boxes change.
+//
+// Collapse: top-down, one launch per level of the wide tree. A wide node starts from
+// its binary node's two children and repeatedly opens the internal child of largest
+// surface area until it has 8 children or only leaves. Its children go to slots by
+// direction (Ylitie, Karras, Laine, "Efficient Incoherent Ray Traversal on GPUs
+// Through Compressed Wide BVHs", HPG 2017): slot s is meant to be met first by rays
+// whose direction has sign pattern s, so that visiting the slots in the order
+// k ^ octant(ray), k = 0..7, is near-to-far; children are assigned greedily by the
+// smallest projection of their centre on the octant's diagonal. Internal children are
+// allocated consecutively (one atomic per node) and queued for the next level;
+// leaf children's triangle records likewise.
+//
+// Quantization: the node box, widened by a margin m, gives a per-axis power-of-two
+// scale 2^e with (hi - lo + 2m) <= 253 * 2^e and the origin p = lo - m - 2^e (rounded
+// down); a child box, widened by the same m, is stored as qlo = floor((lo - m - p) /
+// 2^e) - 1, qhi = ceil((hi + m - p) / 2^e) + 1. The traversal evaluates a plane as
+// fma(2^23 + q, 2^e / d, (p - o) / d - 2^23 * 2^e / d), whose folded offset errs by at
+// most half a quantum (the spare quantum on each side covers it); m = 2^-20 x
+// (largest root-box coordinate magnitude + root-box diagonal) keeps the children's
+// boxes conservative under that rounding for ray origins within a few scene sizes.
+// A leaf child's box is its triangle's box intersected with its binary parent's box
+// (the binary parent of a split piece is bounded by the pieces, the triangle is not).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+#include <algorithm>
+#include "cpt.h"
+#include "cpt_device.cuh"
+#include "cpt_internal.h"
+#include "lbvh_common.cuh"
+#include "traverse.cuh"
+
+namespace cpt {
+namespace {
+
+constexpr int kWideBlock = 128;
+constexpr int kWideLevels = 96;
+constexpr uint32_t kLeafRef = 0x80000000u;
+constexpr int kCtrWords = 4 + kWideLevels + 2;  // alloc nodes, alloc tris, done blocks, margin | level bounds
+
+struct WideScratch {
+    float4* queue;  // per wide node: (box lo, binary node) (box hi, 0)
+    uint32_t* ctr;
+};
+
+size_t wide_scratch_layout(uint32_t leaves, void* base, WideScratch* out)
+{
+    Carver c(base);
+    WideScratch s;
+    s.queue = c.take<float4>(2ull * std::max<uint32_t>(leaves - 1, 1u));
+    s.ctr = c.take<uint32_t>(kCtrWords);
+    if (out) *out = s;
+    return c.used();
+}
+
+__device__ __forceinline__ void read_record(const float4* __restrict__ bin, uint32_t b, float w[24])
+{
+    const float4* p = bin + 6 * (size_t)b;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const float4 f = p[k];
+        w[4 * k] = f.x; w[4 * k + 1] = f.y; w[4 * k + 2] = f.z; w[4 * k + 3] = f.w;
+    }
+}
+
+__device__ __forceinline__ float box_area(const float* b)
+{
+    const float dx = b[3] - b[0], dy = b[4] - b[1], dz = b[5] - b[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// Child `side` of the binary node whose record is w and whose box is pb: its box and
+// reference (internal: its binary index; leaf: parent * 2 + side | kLeafRef).
+__device__ __forceinline__ void child_of(const float w[24], uint32_t parent, const float pb[6], int side, float box[6],
+                                         uint32_t& ref)
+{
+    const uint32_t word = __float_as_uint(w[20]);
+    const bool internal = side ? (word & 2u) : (word & 1u);
+    const float* s = w + 10 * side;
+    if (internal) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) box[k] = s[k];
+        ref = side ? __float_as_uint(w[21]) : (word >> 2);
+    } else {
+        const float v0[3] = {s[0], s[1], s[2]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float v1 = v0[a] + s[4 + a], v2 = v0[a] + s[7 + a];
+            box[a] = fmaxf(fminf(fminf(v0[a], v1), v2), pb[a]);
+            box[3 + a] = fminf(fmaxf(fmaxf(v0[a], v1), v2), pb[3 + a]);
+            if (box[a] > box[3 + a]) box[a] = box[3 + a] = 0.5f * (box[a] + box[3 + a]);  // rounding: keep it a box
+        }
+        ref = (2u * parent + (uint32_t)side) | kLeafRef;
+    }
+}
+
+__global__ void k_wide_init(const float4* __restrict__ bin, float4* __restrict__ queue, uint32_t* __restrict__ ctr)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    float w[24];
+    read_record(bin, 0, w);
+    const uint32_t word = __float_as_uint(w[20]);
+    float lo[3], hi[3], mag = 0.f;
+    const float inf[6] = {-FLT_MAX, -FLT_MAX, -FLT_MAX, FLT_MAX, FLT_MAX, FLT_MAX};
+    for (int a = 0; a < 3; ++a) { lo[a] = FLT_MAX; hi[a] = -FLT_MAX; }
+    for (int side = 0; side < 2; ++side) {
+        float b[6];
+        uint32_t ref;
+        child_of(w, 0, inf, side, b, ref);
+        for (int a = 0; a < 3; ++a) { lo[a] = fminf(lo[a], b[a]); hi[a] = fmaxf(hi[a], b[3 + a]); }
+    }
+    (void)word;
+    float diag2 = 0.f;
+    for (int a = 0; a < 3; ++a) {
+        mag = fmaxf(mag, fmaxf(fabsf(lo[a]), fabsf(hi[a])));
+        diag2 += (hi[a] - lo[a]) * (hi[a] - lo[a]);
+    }
+    const float margin = ldexpf(mag + sqrtf(diag2), -20);
+    queue[0] = make_float4(lo[0], lo[1], lo[2], __uint_as_float(0u));
+    queue[1] = make_float4(hi[0], hi[1], hi[2], 0.f);
+    ctr[0] = 1;  // wide nodes allocated: the root
+    ctr[1] = 0;  // triangle records allocated
+    ctr[2] = 0;  // blocks done in the current level
+    ctr[3] = __float_as_uint(margin);
+    for (int l = 0; l < kWideLevels + 2; ++l) ctr[4 + l] = l == 0 ? 0u : 1u;  // bounds[0] = 0, bounds[1] = 1
+}
+
+// Smallest e with ext <= 253 * 2^e (e in [-126, 127]): the 255 quanta of a byte less
+// one quantum of slack on each side.
+__device__ __forceinline__ int scale_exp(double ext)
+{
+    if (!(ext > 0.0)) return -126;
+    int k;
+    const double f = frexp(ext / 253.0, &k);  // ext / 253 = f * 2^k, f in [0.5, 1)
+    int e = f > 0.5 ? k : k - 1;
+    while (ldexp(253.0, e) < ext) ++e;
+    return max(-126, min(127, e));
+}
+
+__global__ void __launch_bounds__(kWideBlock) k_wide_level(const float4* __restrict__ bin, float4* __restrict__ wide,
+                                                           float4* __restrict__ tris, float4* __restrict__ queue,
+                                                           uint32_t* __restrict__ ctr, int level, uint32_t node_cap,
+                                                           uint32_t tri_cap, uint32_t bin_internal,
+                                                           uint32_t* __restrict__ status)
+{
+    __shared__ float s_box[8 * 6][kWideBlock];
+    __shared__ uint32_t s_ref[8][kWideBlock];
+    const uint32_t start = ctr[4 + level], end = ctr[4 + level + 1];
+    const float m = __uint_as_float(ctr[3]);
+    const int t = threadIdx.x;
+    for (uint32_t wi = start + blockIdx.x * kWideBlock + t; wi < end; wi += gridDim.x * kWideBlock) {
+        const float4 q0 = queue[2 * (size_t)wi], q1 = queue[2 * (size_t)wi + 1];
+        const uint32_t b = __float_as_uint(q0.w);
+        const float nb[6] = {q0.x, q0.y, q0.z, q1.x, q1.y, q1.z};
+        if (b >= bin_internal) { atomicOr(status, CPT_STATUS_BAD_INDEX); continue; }
+        // frontier: the binary node's children, then open the largest internal one
+        int count = 0;
+        {
+            float w[24];
+            read_record(bin, b, w);
+            for (int side = 0; side < 2; ++side) {
+                float bx[6];
+                uint32_t ref;
+                child_of(w, b, nb, side, bx, ref);
+                for (int k = 0; k < 6; ++k) s_box[6 * count + k][t] = bx[k];
+                s_ref[count][t] = ref;
+                ++count;
+            }
+        }
+        while (count < 8) {
+            int best = -1;
+            float best_area = -1.f;
+            for (int i = 0; i < count; ++i) {
+                if (s_ref[i][t] & kLeafRef) continue;
+                float bx[6];
+                for (int k = 0; k < 6; ++k) bx[k] = s_box[6 * i + k][t];
+                const float a = box_area(bx);
+                if (a > best_area) { best_area = a; best = i; }
+            }
+            if (best < 0) break;
+            const uint32_t c = s_ref[best][t];
+            if (c >= bin_internal) { atomicOr(status, CPT_STATUS_BAD_INDEX); break; }
+            float pb[6];
+            for (int k = 0; k < 6; ++k) pb[k] = s_box[6 * best + k][t];
+            float w[24];
+            read_record(bin, c, w);
+            for (int side = 0; side < 2; ++side) {
+                float bx[6];
+                uint32_t ref;
+                child_of(w, c, pb, side, bx, ref);
+                const int slot = side == 0 ? best : count++;
+                for (int k = 0; k < 6; ++k) s_box[6 * slot + k][t] = bx[k];
+                s_ref[slot][t] = ref;
+            }
+        }
+        // quantization frame
+        float p[3];
+        int e[3];
+        double sc[3];
+        float ctr_b[3];
+        for (int a = 0; a < 3; ++a) {
+            const double lo = (double)nb[a] - (double)m, hi = (double)nb[3 + a] + (double)m;
+            e[a] = scale_exp((hi - lo) * (1.0 + 1e-6));
+            sc[a] = ldexp(1.0, e[a]);
+            // p one quantum below the widened box, rounded down to a float
+            const double pd = lo - sc[a];
+            float pf = (float)pd;
+            if ((double)pf > pd) pf = nextafterf(pf, -FLT_MAX);
+            p[a] = pf;
+            ctr_b[a] = 0.5f * (nb[a] + nb[3 + a]);
+        }
+        // slots by direction: greedy smallest projection on the octant diagonal
+        int slot_of[8];
+        uint32_t used = 0, placed = 0;
+        for (int i = 0; i < count; ++i) slot_of[i] = -1;
+        for (int r = 0; r < count; ++r) {
+            float best_c = FLT_MAX;
+            int bi = 0, bs = 0;
+            for (int i = 0; i < count; ++i) {
+                if (placed >> i & 1u) continue;
+                float c[3];
+                for (int a = 0; a < 3; ++a) c[a] = 0.5f * (s_box[6 * i + a][t] + s_box[6 * i + 3 + a][t]) - ctr_b[a];
+                for (int s = 0; s < 8; ++s) {
+                    if (used >> s & 1u) continue;
+                    const float cost = ((s & 1) ? -c[0] : c[0]) + ((s & 2) ? -c[1] : c[1]) + ((s & 4) ? -c[2] : c[2]);
+                    if (cost < best_c) { best_c = cost; bi = i; bs = s; }
+                }
+            }
+            slot_of[bi] = bs;
+            placed |= 1u << bi;
+            used |= 1u << bs;
+        }
+        uint32_t imask = 0, lmask = 0;
+        for (int i = 0; i < count; ++i) {
+            if (s_ref[i][t] & kLeafRef) lmask |= 1u << slot_of[i];
+            else imask |= 1u << slot_of[i];
+        }
+        const uint32_t n_int = __popc(imask), n_leaf = __popc(lmask);
+        const uint32_t child_base = n_int ? atomicAdd(&ctr[0], n_int) : 0u;
+        const uint32_t tri_base = n_leaf ? atomicAdd(&ctr[1], n_leaf) : 0u;
+        if (child_base + n_int > node_cap || tri_base + n_leaf > tri_cap) {
+            atomicOr(status, CPT_STATUS_BAD_INDEX);
+            continue;
+        }
+        uint32_t qlo[3][2] = {{0xFFFFFFFFu, 0xFFFFFFFFu}, {0xFFFFFFFFu, 0xFFFFFFFFu}, {0xFFFFFFFFu, 0xFFFFFFFFu}};
+        uint32_t qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+        for (int i = 0; i < count; ++i) {
+            const int s = slot_of[i];
+            const uint32_t ref = s_ref[i][t];
+            float bx[6];
+            for (int k = 0; k < 6; ++k) bx[k] = s_box[6 * i + k][t];
+            for (int a = 0; a < 3; ++a) {
+                // one quantum of slack each side for the traversal's folded plane offset
+                const double lo = (double)bx[a] - (double)m, hi = (double)bx[3 + a] + (double)m;
+                const int ql = (int)fmin(fmax(floor((lo - (double)p[a]) / sc[a]) - 1.0, 0.0), 255.0);
+                const int qh = (int)fmin(fmax(ceil((hi - (double)p[a]) / sc[a]) + 1.0, 0.0), 255.0);
+                const int sh = 8 * (s & 3);
+                qlo[a][s >> 2] = (qlo[a][s >> 2] & ~(0xFFu << sh)) | ((uint32_t)ql << sh);
+                qhi[a][s >> 2] = (qhi[a][s >> 2] & ~(0xFFu << sh)) | ((uint32_t)qh << sh);
+            }
+            const uint32_t below = (1u << s) - 1u;
+            if (ref & kLeafRef) {
+                const uint32_t parent = (ref & ~kLeafRef) >> 1, side = ref & 1u;
+                const float4* pr = bin + 6 * (size_t)parent;
+                const float2* sl = reinterpret_cast<const float2*>(pr) + 5 * side;
+                const float2 a0 = sl[0], a1 = sl[1], a2 = sl[2], a3 = sl[3], a4 = sl[4];
+                float4* tr = tris + 3 * (size_t)(tri_base + __popc(lmask & below));
+                tr[0] = make_float4(a0.x, a0.y, a1.x, a1.y);  // v0, triangle index
+                tr[1] = make_float4(a2.x, a2.y, a3.x, 0.f);   // v1 - v0
+                tr[2] = make_float4(a3.y, a4.x, a4.y, 0.f);   // v2 - v0
+            } else {
+                float4* qd = queue + 2 * (size_t)(child_base + __popc(imask & below));
+                qd[0] = make_float4(bx[0], bx[1], bx[2], __uint_as_float(ref));
+                qd[1] = make_float4(bx[3], bx[4], bx[5], 0.f);
+            }
+        }
+        const uint32_t ew = (uint32_t)(e[0] + 127) | ((uint32_t)(e[1] + 127) << 8) | ((uint32_t)(e[2] + 127) << 16) |
+                            (imask << 24);
+        float4* o = wide + 5 * (size_t)wi;
+        o[0] = make_float4(p[0], p[1], p[2], __uint_as_float(ew));
+        o[1] = make_float4(__uint_as_float(child_base), __uint_as_float(tri_base), __uint_as_float(lmask), 0.f);
+        o[2] = make_float4(__uint_as_float(qlo[0][0]), __uint_as_float(qlo[0][1]), __uint_as_float(qlo[1][0]),
+                           __uint_as_float(qlo[1][1]));
+        o[3] = make_float4(__uint_as_float(qlo[2][0]), __uint_as_float(qlo[2][1]), __uint_as_float(qhi[0][0]),
+                           __uint_as_float(qhi[0][1]));
+        o[4] = make_float4(__uint_as_float(qhi[1][0]), __uint_as_float(qhi[1][1]), __uint_as_float(qhi[2][0]),
+                           __uint_as_float(qhi[2][1]));
+    }
+    // the last block of the level closes it: the next level is what this one allocated
+    __syncthreads();
+    if (t == 0) {
+        __threadfence();
+        const uint32_t done = atomicAdd(&ctr[2], 1u);
+        if (done == gridDim.x - 1) {
+            __threadfence();
+            ctr[4 + level + 2] = atomicAdd(&ctr[0], 0u);
+            ctr[2] = 0;
+        }
+    }
+}
+
+__global__ void k_wide_check(const uint32_t* __restrict__ ctr, uint32_t* __restrict__ status,
+                             uint32_t* __restrict__ counts_out)
+{
+    if (threadIdx.x != 0) return;
+    // nodes allocated by the last level were never filled: the tree was too tall
+    if (ctr[4 + kWideLevels + 1] != ctr[4 + kWideLevels]) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
+    if (counts_out) { counts_out[0] = ctr[0]; counts_out[1] = ctr[1]; }
+}
+
+}  // namespace
+}  // namespace cpt
+
+using namespace cpt;
+
+extern "C" size_t cpt_lbvh_wide_bytes(uint32_t leaves, size_t* node_bytes, size_t* tri_bytes)
+{
+    if (leaves < 2 || leaves >= (1u << 31)) return 0;
+    if (node_bytes) *node_bytes = align_up((size_t)(leaves - 1) * 80, 256);
+    if (tri_bytes) *tri_bytes = align_up((size_t)leaves * 48, 256);
+    return wide_scratch_layout(leaves, nullptr, nullptr);
+}
+
+extern "C" int cpt_lbvh_wide(cpt_bvh* bvh, void* nodes, size_t node_bytes, void* tris, size_t tri_bytes, void* scratch,
+                             size_t scratch_bytes, cudaStream_t stream)
+{
+    if (!bvh || !bvh->nodes || !bvh->status || !nodes || !tris || !scratch) return CPT_ERR_INVALID_ARGUMENT;
+    const bool split = bvh->split_nodes != nullptr;
+    const uint32_t leaves = split ? bvh->split_capacity : bvh->n;
+    size_t nb = 0, tb = 0;
+    const size_t need = cpt_lbvh_wide_bytes(leaves, &nb, &tb);
+    if (!need) return CPT_ERR_INVALID_ARGUMENT;
+    if (scratch_bytes < need || node_bytes < nb || tri_bytes < tb) return CPT_ERR_SCRATCH_TOO_SMALL;
+    if ((reinterpret_cast<uintptr_t>(nodes) & 15) || (reinterpret_cast<uintptr_t>(tris) & 15) ||
+        (reinterpret_cast<uintptr_t>(scratch) & 255))
+        return CPT_ERR_INVALID_ARGUMENT;
+    bvh->wide_nodes = nullptr;
+    bvh->wide_tris = nullptr;
+    bvh->wide_capacity = 0;
+    WideScratch ws;
+    wide_scratch_layout(leaves, scratch, &ws);
+    const float4* bin = static_cast<const float4*>(split ? bvh->split_nodes : bvh->nodes);
+    k_wide_init<<<1, 32, 0, stream>>>(bin, ws.queue, ws.ctr);
+    CPT_LAUNCH_CHECK();
+    const int blocks = sm_count() * 8;
+    for (int l = 0; l < kWideLevels; ++l) {
+        k_wide_level<<<blocks, kWideBlock, 0, stream>>>(bin, static_cast<float4*>(nodes), static_cast<float4*>(tris),
+                                                        ws.queue, ws.ctr, l, leaves - 1, leaves, leaves - 1,
+                                                        bvh->status);
+        CPT_LAUNCH_CHECK();
+    }
+    k_wide_check<<<1, 32, 0, stream>>>(ws.ctr, bvh->status, bvh->status + 2);
+    CPT_LAUNCH_CHECK();
+    bvh->wide_nodes = nodes;
+    bvh->wide_tris = tris;
+    bvh->wide_capacity = leaves;
+    return CPT_OK;
+}

@@ -80,6 +80,10 @@ typedef struct cpt_bvh {
                                  *       tracing and rendering traverse them instead of `nodes`.
                                  *       cpt_lbvh_build clears it (the split tree is of the old triangles) */
     uint32_t split_capacity;    /* pieces the split nodes were built for (0 when none) */
+    void* wide_nodes;           /* nullable: compressed 8-wide nodes (cpt_lbvh_wide); when set, tracing and
+                                 *       rendering traverse them. cpt_lbvh_build and cpt_lbvh_split clear it */
+    void* wide_tris;            /*       and their 48-B triangle records */
+    uint32_t wide_capacity;     /* leaves of the binary tree the wide tree was built from (0 when none) */
 } cpt_bvh;
 
 /* Bytes of device memory cpt_bvh_bind() needs for n triangles. */
@@ -255,6 +259,19 @@ typedef struct cpt_view {
 size_t cpt_render_views_scratch_bytes(const cpt_view* views, uint32_t n_views, const cpt_render_params* params);
 int cpt_render_views(const cpt_view* views, uint32_t n_views, const cpt_render_params* params, void* scratch,
                      size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status, cudaStream_t stream);
+
+/* ---- compressed 8-wide traversal BVH (an extension; no reference counterpart) ----
+ * Collapses the binary traversal tree in use (the split tree when one was built,
+ * else the LBVH's nodes) into 8-wide nodes of 80 B with 8-bit child boxes and
+ * direction-ordered slots, and copies the leaf triangles into 48-B records in
+ * visiting order. Tracing and rendering then traverse it. Hits are those of the
+ * binary tree (same triangle arithmetic) up to which of several exactly equal
+ * distances is reported. `leaves` for the sizes: bvh->n, or bvh->split_capacity
+ * after cpt_lbvh_split. status[2] / status[3] receive the wide node and triangle
+ * record counts. */
+size_t cpt_lbvh_wide_bytes(uint32_t leaves, size_t* node_bytes, size_t* tri_bytes); /* returns scratch bytes */
+int cpt_lbvh_wide(cpt_bvh* bvh, void* nodes, size_t node_bytes, void* tris, size_t tri_bytes, void* scratch,
+                  size_t scratch_bytes, cudaStream_t stream);
 
 /* ---- next-event estimation (an extension; no reference counterpart) ----
  * The reference gathers emitted light only where a bounce ray happens to hit an

@@ -1,0 +1,108 @@
+"""Compressed 8-wide traversal BVH (cpt_lbvh_wide) on the GPU: the closest hits of
+the binary tree it collapses (the LBVH — the oracle's restatement of the reference
+traversal — or the split tree), identical (t, u, v, triangle) except where two
+triangles are hit at exactly the same t; the same occlusion for any-hit and far-limited
+rays; images equal to the binary tree's up to such ties; counts of the tree written
+to the status words; a rebuild or split drops the stale wide tree."""
+import numpy as np
+import pytest
+import torch
+
+import cpt
+from cpt.device import BatchRenderer, DeviceLbvh, DeviceScene, make_params, to_device
+from oracle import cpu
+from test_gpu_split import hairball, random_rays, tie_or_equal
+
+pytestmark = pytest.mark.gpu
+
+
+def trace_pair(lb, d_rays):
+    h, st = lb.trace(d_rays, stats=True)
+    a, _ = lb.trace(d_rays, any_hit=True)
+    torch.cuda.synchronize()
+    lb.status()
+    return h.cpu().numpy(), st.cpu().numpy(), a.cpu().numpy()
+
+
+@pytest.mark.parametrize("bits", [30, 63])
+@pytest.mark.parametrize("split", [0.0, 1.25])
+def test_wide_hits_match_binary(cuda, bits, split):
+    tris, _ = hairball()
+    lb = DeviceLbvh(len(tris), bits)
+    lb.build(to_device(tris), check_root=True)
+    if split:
+        lb.split(split)
+    rays = np.concatenate([random_rays(20_000, 1), random_rays(10_000, 2, inside=True)])
+    d_rays = torch.from_numpy(rays).cuda()
+    hb, sb, ab = trace_pair(lb, d_rays)
+    lb.wide()
+    hw, sw, aw = trace_pair(lb, d_rays)
+    ok, exact = tie_or_equal(hw, hb)
+    assert ok.all()
+    assert exact.mean() > 0.999
+    assert np.array_equal(aw[:, 0] < 3e38, ab[:, 0] < 3e38)
+    # against the oracle's reference traversal as well
+    b = cpu.build(tris, bits)
+    t, idx, uv = cpu.trace(b, rays[:, [0, 1, 2, 4, 5, 6]])
+    ok2, _ = tie_or_equal(hw, np.stack([t, uv[:, 0], uv[:, 1], idx.view(np.float32)], 1))
+    assert ok2.all()
+    # fewer node fetches than the binary tree; the counts in the status words
+    assert sw[:, 0].mean() < 0.6 * sb[:, 0].mean(), (sw[:, 0].mean(), sb[:, 0].mean())
+    leaves = lb.bvh.split_capacity if split else lb.n
+    assert lb.bvh.wide_capacity == leaves
+    counts = lb.status_words()
+    assert 1 <= counts[2] <= leaves - 1 and counts[3] >= 1
+
+
+def test_wide_far_limit_and_zero_direction(cuda):
+    """Rays along the axes (zero direction components) and occlusion tests with a far
+    limit (the renderer's shadow rays) agree with the binary tree."""
+    tris, _ = cpt.scene_random(20_000, seed=4)
+    lb = DeviceLbvh(len(tris), 30)
+    lb.build(to_device(tris))
+    g = np.random.default_rng(8)
+    m = 6000
+    rays = np.zeros((m, 8), np.float32)
+    rays[:, 0:3] = g.uniform(-0.2, 1.2, (m, 3))
+    axis = g.integers(0, 3, m)
+    sign = np.where(g.random(m) < 0.5, -1.0, 1.0)
+    rays[np.arange(m), 4 + axis] = sign
+    d_rays = torch.from_numpy(rays).cuda()
+    hb, _, ab = trace_pair(lb, d_rays)
+    lb.wide()
+    hw, _, aw = trace_pair(lb, d_rays)
+    ok, _ = tie_or_equal(hw, hb)
+    assert ok.all()
+    assert np.array_equal(aw[:, 0] < 3e38, ab[:, 0] < 3e38)
+    assert (hb[:, 0] < 3e38).mean() > 0.1
+
+
+@pytest.mark.parametrize("nee", [False, True])
+def test_wide_render_matches_binary(cuda, nee):
+    tris, infos = hairball(n_hair=30_000)
+    cam = cpt.camera_look_at((0.0, 0.35, -3.6), (0.0, 0.0, 0.0), aspect=64 / 48)
+    lb = DeviceLbvh(len(tris), 63)
+    lb.build(to_device(tris), check_root=True)
+    lb.split(1.25)
+    sc = DeviceScene(infos)
+    if nee:
+        sc.build_emitters(lb)
+    p = make_params(64, 48, 8, 3, 5, 3.0, True, 17, cpt.ACCUM_KAHAN, nee=nee)
+    r0 = BatchRenderer([(lb, sc, cam, 64, 48)], p)
+    r0.render()
+    lb.wide()
+    r1 = BatchRenderer([(lb, sc, cam, 64, 48)], p)
+    r1.render()
+    torch.cuda.synchronize()
+    r1.check_status()
+    a0 = r0.accums[0].cpu().numpy().view(np.uint32).reshape(2, 48, 64, 4)[0]
+    a1 = r1.accums[0].cpu().numpy().view(np.uint32).reshape(2, 48, 64, 4)[0]
+    differ = (a0 != a1).any(-1)
+    assert differ.mean() < 0.002  # only pixels whose path met an exact tie may differ
+    assert np.array_equal(r0.counts.cpu().numpy()[:3], r1.counts.cpu().numpy()[:3]) or differ.any()
+    # a new split or build drops the wide tree of the old binary tree
+    lb.split(1.25)
+    assert not lb.bvh.wide_nodes and lb.bvh.wide_capacity == 0
+    lb.wide()
+    lb.build(to_device(tris))
+    assert not lb.bvh.wide_nodes and not lb.bvh.split_nodes
