@@ -34,16 +34,16 @@ sys.path.insert(0, os.path.join(ROOT, "cuda-path-tracer_b200"))
 
 WORKLOADS = {
     "c2": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
-               bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, split=1.25),
+               bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, split=4.0, wide=1),
     "c1": dict(kind="random", n=65536, bits=30, width=512, height=512, spp=1, bounces=3, eye=(0.5, 0.5, -1.2),
                target=(0.5, 0.5, 0.0), seed=0),
     # 64 scenes, 10k-2M triangles (log-uniform, alternating generators), 256^2-1024^2, one graph launch per frame
     "c3": dict(kind="batch", scenes=64, tri_min=10_000, tri_max=2_000_000, res_min=256, res_max=1024, spp=4,
-               bounces=5, bits=63, seed=0, width=0, height=0, split=1.25),
+               bounces=5, bits=63, seed=0, width=0, height=0, split=1.25, wide=1),
     # radiance cache on the C2 scene: 1 spp frames through the cache vs plain 16 spp, RMSE vs an FP64 image
     "c4": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
                bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, plain_spp=64, ref_spp=4096,
-               ref_div=4, warm_updates=4, max_spp=256, split=1.25),
+               ref_div=4, warm_updates=4, max_spp=256, split=4.0, wide=1),
     # deforming 16.8 M-triangle displaced sphere, full rebuild every frame, 8 cameras
     "c5": dict(kind="deform", nu=4096, nv=2048, n_hair=0, bits=63, width=1280, height=720, spp=1, bounces=7,
                eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, cameras=8, amp=0.01, omega=40.0, cache=True),
@@ -285,6 +285,8 @@ def run_batch(args, w, world, rank, local):
         lb.build(d, check_root=True)
         if kind != "random" and split > 0:  # the hairball scenes traverse a split BVH
             lb.split(split)
+        if args.wide:
+            lb.wide(keep_scratch=True)
         sc = DeviceScene(infos, None, dev)
         eye, tgt = ((0.5, 0.5, -1.2), (0.5, 0.5, 0.0)) if kind == "random" else ((0.0, 0.35, -3.6), (0.0, 0.0, 0.0))
         cam = cpt.camera_look_at(eye, tgt, fov_deg=45.0, aspect=1.0)
@@ -369,7 +371,8 @@ def run_batch(args, w, world, rank, local):
     prof = cpt.profile_end()
     ext_ms, ext_n = prof.get("k_extend", (0.0, 0))
     closest_frame = float(counts[0] + counts[1]) / args.steps
-    alg = closest_frame * (48 + 64.0 * mean_nodes + 48.0 * mean_tris)
+    node_b = 80.0 if args.wide else 64.0  # a wide node record, or the compact two-child node
+    alg = closest_frame * (48 + node_b * mean_nodes + 48.0 * mean_tris)
     peak, peak_kind = measured_peaks()
     ach = alg / (ext_ms / 1e3) / 1e9 if ext_ms else 0.0
     frame_ms = sum(v[0] for v in prof.values())
@@ -380,6 +383,8 @@ def run_batch(args, w, world, rank, local):
     for (lb, _, _, _, _), h in zip(views, hair):
         if h:
             lb.split(split, keep_scratch=True)  # scratch stays allocated for the captured rebuilds
+        if args.wide:
+            lb.wide(keep_scratch=True)
     torch.cuda.synchronize()
 
     def rebuild_all():
@@ -387,6 +392,8 @@ def run_batch(args, w, world, rank, local):
             lb.build(d)
             if h:
                 lb.split(split, keep_scratch=True)
+            if args.wide:
+                lb.wide(keep_scratch=True)
 
     counter2 = torch.zeros(1, dtype=torch.int32, device=dev)
     p2 = params(best["wave_paths"], best["ray_sort"])
@@ -447,7 +454,7 @@ def run_batch(args, w, world, rank, local):
                 "rays_per_step": int(rays / args.steps),
                 "roofline": {"bound": "hbm", "kernel": "k_extend", "achieved": round(ach, 1), "peak": peak,
                              "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
-                             "bytes_per_ray": f"48 + 64 x {mean_nodes:.2f} nodes + 48 x {mean_tris:.2f} triangles",
+                             "bytes_per_ray": f"48 + {node_b:.0f} x {mean_nodes:.2f} nodes + 48 x {mean_tris:.2f} triangles",
                              "kernel_share": {k: round(v[0] / frame_ms, 4) for k, v in sorted(prof.items())}},
                 "lbvh": {"mtris_s": round(n_tris / build_ms / 1e3, 2), "ms": round(build_ms, 3),
                          "note": "each rank's scenes built back to back (max over ranks)"},
@@ -627,11 +634,13 @@ def run_ours(args, w, world, rank, local):
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "k_extend_c2_split.md" if split > 0 else "k_extend_c2.md")
+    prof_name, key = (("k_extend_c2_wide.md", "dram_bytes_per_closest_ray_wide") if args.wide else
+                      ("k_extend_c2_split.md", "dram_bytes_per_closest_ray_split") if split > 0 else
+                      ("k_extend_c2.md", "dram_bytes_per_closest_ray"))
+    tp = os.path.join(ROOT, "profiles", prof_name)
     if args.workload == "c2" and os.path.exists(tp):  # ncu figure of the C2 traversal (see that file)
         import re
 
-        key = "dram_bytes_per_closest_ray_split" if split > 0 else "dram_bytes_per_closest_ray"
         m = re.search(key + r" = ([0-9.]+)", open(tp).read())
         if m:
             traffic = round(float(m.group(1)) * rays_closest / max(ext_launches, 1), 1)
@@ -716,6 +725,7 @@ def run_ours(args, w, world, rank, local):
     if not args.no_e2e and not deforming:
         tr = cpt.Tracer(w["bits"])
         tr.set_split(split)
+        tr.set_wide(bool(args.wide))
         tr.set_settings(bounces=w["bounces"], intensity=3.0, stratified=True, seed=w["seed"] + 7919 * rank)
         # (the tracer object renders frame 0 of its own seed on every rank: e2e ranks are replicas)
         tr.set_camera(cams[0])
@@ -811,6 +821,8 @@ def run_cache(args, w, world, rank, local):
     split = w.get("split", 0.0) if args.split is None else args.split
     if split > 0:
         lb.split(split)
+    if args.wide:
+        lb.wide()
     scene = DeviceScene(infos, None, dev)
     scene.build_emitters(lb)
     stream = torch.cuda.current_stream()
@@ -975,8 +987,9 @@ def main():
     ap.add_argument("--spp", type=int, default=None, help="override samples per frame (profiling runs)")
     ap.add_argument("--wave-paths", type=int, default=0, help="paths per wave (0: library default)")
     ap.add_argument("--ray-sort", type=int, default=0, help="1: coherence-sort bounce queues")
-    ap.add_argument("--wide", type=int, default=0,
-                    help="1: traverse the compressed 8-wide tree built from the (split) binary tree")
+    ap.add_argument("--wide", type=int, default=None,
+                    help="1: traverse the compressed 8-wide tree built from the (split) binary tree, 0: the binary "
+                         "tree (default per workload)")
     ap.add_argument("--rc-per-call", action="store_true",
                     help="c4: 2^16 training suffixes per render call instead of per image sample")
     ap.add_argument("--nee", type=int, default=1,
@@ -985,6 +998,8 @@ def main():
                     help="split traversal BVH extra-piece ratio (0: traverse the LBVH; default per workload)")
     args = ap.parse_args()
     w = dict(WORKLOADS[args.workload])
+    if args.wide is None:
+        args.wide = int(w.get("wide", 0))
     if args.res:
         w["width"], w["height"] = (int(x) for x in args.res.lower().split("x"))
     if args.spp:

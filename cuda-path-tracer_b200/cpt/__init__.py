@@ -156,6 +156,7 @@ _PROTOS = {
     "cpt_tracer_upload_textures": (_I32, [_P, _P, _U32]),
     "cpt_tracer_set_split": (_I32, [_P, _F, _U32]),
     "cpt_tracer_set_nee": (_I32, [_P, _U32]),
+    "cpt_tracer_set_wide": (_I32, [_P, _U32]),
     "cpt_tracer_set_primary_rays": (_I32, [_P, _P]),
     "cpt_tracer_set_eye": (_I32, [_P, _P]),
     "cpt_tracer_set_camera": (_I32, [_P, ctypes.POINTER(Camera)]),
@@ -416,6 +417,10 @@ class Tracer:
 
     def set_split(self, extra_ratio: float, flags: int = 0) -> None:
         check(lib.cpt_tracer_set_split(self._h, float(extra_ratio), int(flags)), "cpt_tracer_set_split")
+
+    def set_wide(self, on: bool) -> None:
+        """Every later upload also builds the compressed wide tree and renders through it."""
+        check(lib.cpt_tracer_set_wide(self._h, int(bool(on))), "cpt_tracer_set_wide")
 
     def set_nee(self, on: bool) -> None:
         """Next-event estimation on / off (restarts the accumulation when it changes)."""

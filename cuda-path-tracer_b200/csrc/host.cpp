@@ -447,6 +447,13 @@ struct cpt_tracer {
     void* d_textures = nullptr;  // cudaTextureObject_t handles (the caller owns the textures)
     size_t textures_cap = 0;
     uint32_t texture_count = 0;
+    void* d_wide_nodes = nullptr;  // compressed wide tree (cpt_tracer_set_wide)
+    size_t wide_nodes_cap = 0;
+    void* d_wide_tris = nullptr;
+    size_t wide_tris_cap = 0;
+    void* d_wide_scratch = nullptr;
+    size_t wide_scratch_cap = 0;
+    bool wide = false;
     void* d_emitters = nullptr;  // emitter table (cpt_tracer_set_nee)
     size_t emitters_cap = 0;
     bool nee = false, emitters_ready = false;
@@ -503,7 +510,7 @@ extern "C" void cpt_tracer_destroy(cpt_tracer* t)
     if (t->stream) cudaStreamSynchronize(t->stream);
     void* bufs[] = {t->d_tris, t->d_bvh, t->d_build_scratch, t->d_infos, t->d_lights, t->d_textures, t->d_accum,
                     t->d_render_scratch, t->d_image, t->d_counts, t->d_split_nodes, t->d_split_scratch,
-                    t->d_emitters};
+                    t->d_emitters, t->d_wide_nodes, t->d_wide_tris, t->d_wide_scratch};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (t->stream) cudaStreamDestroy(t->stream);
@@ -544,6 +551,18 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
                             t->split_scratch_cap, t->stream);
         if (rc) return rc;
     }
+    if (t->wide) {
+        const uint32_t leaves = t->bvh.split_nodes ? t->bvh.split_capacity : n;
+        size_t nb = 0, tb = 0;
+        const size_t sb = cpt_lbvh_wide_bytes(leaves, &nb, &tb);
+        if (!sb) return CPT_ERR_INVALID_ARGUMENT;
+        if ((rc = ensure(&t->d_wide_nodes, &t->wide_nodes_cap, nb))) return rc;
+        if ((rc = ensure(&t->d_wide_tris, &t->wide_tris_cap, tb))) return rc;
+        if ((rc = ensure(&t->d_wide_scratch, &t->wide_scratch_cap, sb))) return rc;
+        rc = cpt_lbvh_wide(&t->bvh, t->d_wide_nodes, t->wide_nodes_cap, t->d_wide_tris, t->wide_tris_cap,
+                           t->d_wide_scratch, t->wide_scratch_cap, t->stream);
+        if (rc) return rc;
+    }
     t->n = n;
     t->info_count = info_count;
     t->light_count = light_count;
@@ -559,6 +578,13 @@ extern "C" int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio, uint32_t f
     if (!t || !(extra_ratio >= 0.f) || !(extra_ratio <= 64.f)) return CPT_ERR_INVALID_ARGUMENT;
     t->split_ratio = extra_ratio;
     t->split_flags = flags;
+    return CPT_OK;
+}
+
+extern "C" int cpt_tracer_set_wide(cpt_tracer* t, uint32_t on)
+{
+    if (!t || on > 1) return CPT_ERR_INVALID_ARGUMENT;
+    t->wide = on != 0;
     return CPT_OK;
 }
 

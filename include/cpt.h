@@ -329,6 +329,9 @@ int cpt_tracer_upload_textures(cpt_tracer* t, const cudaTextureObject_t* texture
 /* extra_ratio > 0: every later upload also builds the split traversal BVH
  * (cpt_lbvh_split with `flags`) and renders through it; 0 (default) renders over the LBVH. */
 int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio, uint32_t flags);
+/* on = 1: every later upload also builds the compressed wide tree (cpt_lbvh_wide) of
+ * the traversal tree (after the split tree, when one is set) and renders through it. */
+int cpt_tracer_set_wide(cpt_tracer* t, uint32_t on);
 /* on = 1: render with next-event estimation (cpt_render_params.nee); the tracer
  * builds the uploaded scene's emitter table on the next raytrace. Switching
  * restarts the accumulation (frame 0). Default 0: the reference's estimator. */

@@ -277,12 +277,13 @@ public:
                                       uint32_t(seed), uint32_t(seed >> 32), accumMode),
               "CUDAPathTracer::setSettings");
     }
-    // extensions without a reference counterpart: next-event estimation, split traversal BVH
+    // extensions without a reference counterpart: next-event estimation, split and wide traversal trees
     void setNextEventEstimation(bool on) { check(cpt_tracer_set_nee(m_t, on ? 1u : 0u), "CUDAPathTracer::setNextEventEstimation"); }
     void setSplit(float extraRatio, uint32_t flags = 0)
     {
         check(cpt_tracer_set_split(m_t, extraRatio, flags), "CUDAPathTracer::setSplit");
     }
+    void setWide(bool on) { check(cpt_tracer_set_wide(m_t, on ? 1u : 0u), "CUDAPathTracer::setWide"); }
     // the accumulated image, width x height RGBA32F (replaces the GL surface)
     std::vector<float> readImage(int screenWidth, int screenHeight)
     {

@@ -106,3 +106,25 @@ def test_wide_render_matches_binary(cuda, nee):
     lb.wide()
     lb.build(to_device(tris))
     assert not lb.bvh.wide_nodes and not lb.bvh.split_nodes
+
+
+def test_tracer_object_with_wide_tree(cuda):
+    """cpt_tracer_set_wide: the tracer builds the wide tree on upload (after the split
+    tree) and its image equals the binary tree's up to exact ties."""
+    tris, infos = hairball(n_hair=10_000)
+    cam = cpt.camera_look_at((0.0, 0.35, -3.6), (0.0, 0.0, 0.0), aspect=64 / 48)
+    imgs = []
+    for wide in (False, True):
+        t = cpt.Tracer(63)
+        t.set_split(2.0)
+        t.set_wide(wide)
+        t.upload(tris, infos)
+        t.set_settings(bounces=3, intensity=3.0, stratified=True, seed=5, accum_mode=cpt.ACCUM_KAHAN)
+        t.set_camera(cam)
+        t.raytrace(64, 48, 4)
+        imgs.append(t.read_image(64, 48))
+        b = t.bvh()
+        assert b.wide_capacity == (b.split_capacity if wide else 0)
+        t.close()
+    differ = (imgs[0].view(np.uint32) != imgs[1].view(np.uint32)).any(-1)
+    assert differ.mean() < 0.002
