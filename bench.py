@@ -77,7 +77,7 @@ def make_cameras(w):
 def workload_config(name, w, n_tris, l2_note):
     desc = {"c2": "fBm sphere 2048x1024x2 + 1M hairball + quad light",
             "c4": "fBm sphere 2048x1024x2 + 1M hairball + quad light, radiance cache (96-64x4-16 BF16 MLP, 2^16 "
-                  "training paths per 1-spp frame, Adam 1e-2) vs plain path tracing",
+                  "training paths per frame, Adam 1e-2) vs plain path tracing",
             "c1": "65,536 random triangles + quad light",
             "c5": "deforming fBm sphere 4096x2048x2 + quad light, rebuild every frame, 8 cameras, radiance cache "
                   "(trained across the deforming frames)",
@@ -839,11 +839,11 @@ def run_cache(args, w, world, rank, local):
         return e0.elapsed_time(e1)
 
     def rc_params():
-        """2^16 training suffixes and 4 optimiser steps per image sample (one
-        call renders `spf` samples, so it trains on spf * 2^16 suffixes), or — with
-        --rc-per-call — per call."""
+        """2^16 training suffixes and 4 optimiser steps per frame (one render call of
+        `spf` samples), or — with --rc-per-sample — per image sample (spf * 2^16
+        suffixes per call)."""
         p = rc_default_params()
-        if not args.rc_per_call:
+        if args.rc_per_sample:
             p.train_samples *= spf
             p.train_steps *= spf
         return p
@@ -990,8 +990,8 @@ def main():
     ap.add_argument("--wide", type=int, default=None,
                     help="1: traverse the compressed 8-wide tree built from the (split) binary tree, 0: the binary "
                          "tree (default per workload)")
-    ap.add_argument("--rc-per-call", action="store_true",
-                    help="c4: 2^16 training suffixes per render call instead of per image sample")
+    ap.add_argument("--rc-per-sample", action="store_true",
+                    help="c4: 2^16 training suffixes per image sample instead of per render call (frame)")
     ap.add_argument("--nee", type=int, default=1,
                     help="c4: also compare with next-event estimation in both tracers (1) or not (0)")
     ap.add_argument("--split", type=float, default=None,
