@@ -88,9 +88,10 @@ __global__ void __launch_bounds__(256) k_topology(const K* __restrict__ keys, ui
     else parents_leaf[s + 1] = (uint32_t)i;
     const uint32_t word = ((uint32_t)s << 2) | type;
     children[i] = word;
-    // Node word, then the right child's index (s + 1 here; any index in trees whose
-    // siblings are not adjacent)
-    nodes[6 * (size_t)i + 5] = make_float4(__uint_as_float(word), __uint_as_float((uint32_t)s + 1u), 0.0f, 0.0f);
+    // Node word, the right child's index (s + 1 here; any index in trees whose siblings
+    // are not adjacent), and j, the other end of the node's leaf range [min(i, j), max(i, j)]
+    nodes[6 * (size_t)i + 5] = make_float4(__uint_as_float(word), __uint_as_float((uint32_t)s + 1u),
+                                           __uint_as_float((uint32_t)j), 0.0f);
     counters[i] = 0;
     if (i == 0) parents_internal[0] = CPT_INVALID_INDEX;
 }

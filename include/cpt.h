@@ -71,8 +71,9 @@ typedef struct cpt_bvh {
     uint32_t* parents_leaf;     /* [n]   parent of each leaf */
     uint32_t* parents_internal; /* [n-1] parent of each internal node; [0] = CPT_INVALID_INDEX */
     cpt_bbox* node_boxes;       /* [n-1] internal node boxes */
-    void* nodes;                /* [n-1] 96-B traversal nodes: two 40-B child slots, the Node word and the
-                                 *       right child's index (left + 1 here), where a slot holds the
+    void* nodes;                /* [n-1] 96-B traversal nodes: two 40-B child slots, the Node word, the
+                                 *       right child's index (left + 1 here) and the far end j of the
+                                 *       node's leaf range [min(i, j), max(i, j)], where a slot holds the
                                  *       child's box (internal child) or the child triangle as v0, its
                                  *       index in tris, v1 - v0, v2 - v0 (leaf child) */
     uint32_t* status;           /* [4]   device status words (CPT_STATUS_* bits in [0]) */
