@@ -261,6 +261,7 @@ __device__ __forceinline__ Hit traverse(const float4* __restrict__ nodes, f3 o, 
 // (the rest of the group goes on the stack), or else pops a group. The triangle test
 // is tri_test on the binary leaf slot's words, so a hit's t, u, v are unchanged.
 constexpr int kWideSmemStack = 16;  // stack entries (2 words) per thread in shared memory
+constexpr float kWideGrow = 1.0f + 1.0f / 262144.0f;  // relative slack of a wide child's box test
 // The wide traversal refills as soon as one lane of the warp is idle: its steps are
 // long (8 child boxes), so an idle lane costs more than the refill's ballot and
 // atomic (C2: 313 Mrays/s at 32, 302 at 28, 283 at 24, 242 at 16, 196 at 8).
@@ -425,8 +426,9 @@ __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* 
         const float tfx = fmaf(qbyte(i < 4 ? fx0 : fx1, sel), adx, bdx);
         const float tfy = fmaf(qbyte(i < 4 ? fy0 : fy1, sel), ady, bdy);
         const float tfz = fmaf(qbyte(i < 4 ? fz0 : fz1, sel), adz, bdz);
-        // [max(tn, 0), min(tf, best)] non-empty (a superset of the binary test's hits on the boundary)
-        const float tn = fmaxf(fmax3(tnx, tny, tnz), 0.0f), tf = fminf(fmin3(tfx, tfy, tfz), tlim);
+        // [max(tn, 0), min(tf, best) * (1 + 2^-18)] non-empty: the far end grows by a relative
+        // 2^-18, which covers the rounding of (p - o) / d for ray origins at any distance
+        const float tn = fmaxf(fmax3(tnx, tny, tnz), 0.0f), tf = fminf(fmin3(tfx, tfy, tfz), tlim) * kWideGrow;
         hm |= (tn <= tf ? 1u : 0u) << i;
     }
     s.cbase = __float_as_uint(n1.x);

@@ -21,8 +21,10 @@
 // 2^e) - 1, qhi = ceil((hi + m - p) / 2^e) + 1. The traversal evaluates a plane as
 // fma(2^23 + q, 2^e / d, (p - o) / d - 2^23 * 2^e / d), whose folded offset errs by at
 // most half a quantum (the spare quantum on each side covers it); m = 2^-20 x
-// (largest root-box coordinate magnitude + root-box diagonal) keeps the children's
-// boxes conservative under that rounding for ray origins within a few scene sizes.
+// (largest root-box coordinate magnitude + root-box diagonal) covers the rounding of
+// the quantized planes at the scene's scale, and the traversal's relative slack of
+// 2^-18 on the far end of each interval covers the rounding of (p - o) / d, which
+// grows with the distance of the ray origin.
 // A leaf child's box is its triangle's box intersected with its binary parent's box
 // (the binary parent of a split piece is bounded by the pieces, the triangle is not).
 #include <cuda_runtime.h>

@@ -128,3 +128,65 @@ def test_tracer_object_with_wide_tree(cuda):
         t.close()
     differ = (imgs[0].view(np.uint32) != imgs[1].view(np.uint32)).any(-1)
     assert differ.mean() < 0.002
+
+
+def _closest_brute(tris, rays):
+    """Closest Moller-Trumbore hit distance of every ray over every triangle, with the
+    product's float32 operation order (each operation rounded); inf on a miss."""
+    v0 = tris["v0"].astype(np.float32)
+    e1 = (tris["v1"] - tris["v0"]).astype(np.float32)
+    e2 = (tris["v2"] - tris["v0"]).astype(np.float32)
+
+    def cross(a, b):
+        return np.stack([a[..., 1] * b[..., 2] - b[..., 1] * a[..., 2], a[..., 2] * b[..., 0] - b[..., 2] * a[..., 0],
+                         a[..., 0] * b[..., 1] - b[..., 0] * a[..., 1]], -1)
+
+    def dot(a, b):
+        return (a[..., 0] * b[..., 0] + a[..., 1] * b[..., 1]) + a[..., 2] * b[..., 2]
+
+    out = np.full(len(rays), np.inf, np.float32)
+    eps = np.float32(np.finfo(np.float32).eps)
+    with np.errstate(all="ignore"):
+        for k in range(len(rays)):
+            o, d = rays[k, 0:3], rays[k, 4:7]
+            q = cross(np.broadcast_to(d, e2.shape), e2)
+            det = dot(e1, q)
+            inv = np.float32(1.0) / det
+            sv = o - v0
+            u = inv * dot(sv, q)
+            r = cross(sv, e1)
+            v = inv * dot(np.broadcast_to(d, r.shape), r)
+            t = inv * dot(e2, r)
+            hit = ~((det > -eps) & (det < eps)) & ~(u < 0) & ~(v < 0) & ~((u + v) > 1) & (t >= 0)
+            if hit.any():
+                out[k] = t[hit].min()
+    return out
+
+
+@pytest.mark.parametrize("distance", [3.0, 1000.0])
+def test_wide_far_camera_finds_every_closest_hit(cuda, distance):
+    """Rays from far away (the plane distances (p - o) / d round at the scale of the
+    distance, not of the scene): the wide tree still returns the brute-force closest
+    hit of every ray."""
+    tris, _ = cpt.scene_random(20_000, seed=12)
+    lb = DeviceLbvh(len(tris), 30)
+    lb.build(to_device(tris))
+    lb.wide()
+    g = np.random.default_rng(21)
+    m = 1000
+    d0 = g.normal(size=(m, 3))
+    o = 0.5 + distance * d0 / np.linalg.norm(d0, axis=1, keepdims=True)
+    tgt = g.uniform(0.0, 1.0, (m, 3))
+    dirs = tgt - o
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    rays = np.zeros((m, 8), np.float32)
+    rays[:, 0:3] = o
+    rays[:, 4:7] = dirs
+    h, _ = lb.trace(torch.from_numpy(rays).cuda())
+    torch.cuda.synchronize()
+    lb.status()
+    got = h.cpu().numpy()[:, 0]
+    want = _closest_brute(tris, rays)
+    assert (want < np.inf).mean() > 0.2
+    got = np.where(got >= 3e38, np.inf, got)
+    assert np.array_equal(got, want)
