@@ -190,3 +190,30 @@ def test_wide_far_camera_finds_every_closest_hit(cuda, distance):
     assert (want < np.inf).mean() > 0.2
     got = np.where(got >= 3e38, np.inf, got)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("distance", [3.0, 1000.0])
+def test_split_far_camera_finds_every_closest_hit(cuda, distance):
+    """The same far-camera check for the binary split tree (pieces of long triangles,
+    fused slab test)."""
+    tris, _ = hairball(n_hair=8000, nu=32, nv=16, seed=6)
+    lb = DeviceLbvh(len(tris), 63)
+    lb.build(to_device(tris))
+    lb.split(2.0)
+    g = np.random.default_rng(22)
+    m = 1000
+    d0 = g.normal(size=(m, 3))
+    o = distance * d0 / np.linalg.norm(d0, axis=1, keepdims=True)
+    tgt = g.uniform(-1.0, 1.0, (m, 3))
+    dirs = tgt - o
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    rays = np.zeros((m, 8), np.float32)
+    rays[:, 0:3] = o
+    rays[:, 4:7] = dirs
+    h, _ = lb.trace(torch.from_numpy(rays).cuda())
+    torch.cuda.synchronize()
+    lb.status()
+    got = np.where(h.cpu().numpy()[:, 0] >= 3e38, np.inf, h.cpu().numpy()[:, 0])
+    want = _closest_brute(tris, rays)
+    assert (want < np.inf).mean() > 0.2
+    assert np.array_equal(got, want)
