@@ -336,7 +336,12 @@ __device__ __forceinline__ Box piece_box(const float4* pieces, uint32_t r, bool 
 // Leaf i (sorted piece order[i]): its slot is the whole triangle, its box the
 // piece's; then the bottom-up walk of k_gather_refit with the sibling leaf's box
 // read from the leaf box array.
-__global__ void __launch_bounds__(256) k_split_refit(const cpt_triangle* __restrict__ tris, const float4* __restrict__ pieces,
+// Leaves per block of k_split_refit: nodes whose leaf range (word 22 of the record,
+// written by k_topology) lies inside the block complete in shared memory, as in the
+// LBVH refit; the rest through the global acquire-release counters.
+constexpr int kSplitRefitBlock = 64;
+
+__global__ void __launch_bounds__(kSplitRefitBlock) k_split_refit(const cpt_triangle* __restrict__ tris, const float4* __restrict__ pieces,
                                                      const uint32_t* __restrict__ order,
                                                      const uint32_t* __restrict__ n_pieces,
                                                      const uint32_t* __restrict__ children,
@@ -346,9 +351,15 @@ __global__ void __launch_bounds__(256) k_split_refit(const cpt_triangle* __restr
                                                      cpt_bbox* __restrict__ node_boxes, float4* __restrict__ leaf_boxes,
                                                      uint32_t n_tris, uint32_t* __restrict__ status)
 {
+    __shared__ int s_count[kSplitRefitBlock];
+    __shared__ float s_box[2 * kSplitRefitBlock][6];  // [2 * (p - base) + side]: the first arriver's box
+    const uint32_t base = blockIdx.x * kSplitRefitBlock;
+    s_count[threadIdx.x] = 0;
+    __syncthreads();
     const uint32_t n = *n_pieces;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = base + threadIdx.x;
     if (i >= n || n < 2) return;
+    const uint32_t block_end = min(n, base + (uint32_t)kSplitRefitBlock);
     uint32_t src = order[i];
     if (src >= n) {
         atomicOr(status, CPT_STATUS_BAD_INDEX);
@@ -370,23 +381,41 @@ __global__ void __launch_bounds__(256) k_split_refit(const cpt_triangle* __restr
     uint32_t p = parents_leaf[i];
     while (p != CPT_INVALID_INDEX) {
         if (p >= n - 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
-        const uint32_t word = children[p];
+        float* node = nodes + 24 * (size_t)p;
+        const float4 meta = *reinterpret_cast<const float4*>(node + 20);  // Node word, right child, range end
+        const uint32_t word = __float_as_uint(meta.x);
         const uint32_t left = word >> 2;
         const int side = left == child ? 0 : 1;
-        float* node = nodes + 24 * (size_t)p;
+        const uint32_t j = __float_as_uint(meta.z);
+        const bool local = min(p, j) >= base && max(p, j) < block_end;
         store_slot(node, side, slot);
-        const int arrived = arrive_acq_rel(&counters[p]);
-        if (arrived == 0) return;
-        if (arrived != 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
         const uint32_t sib = left + (uint32_t)(1 - side);
-        const bool sib_internal = (word >> (1 - side)) & 1u;
         Box sb;
-        if (sib_internal) {
-            const float2* q = reinterpret_cast<const float2*>(node_boxes + sib);
-            const float2 x0 = __ldcg(q), x1 = __ldcg(q + 1), x2 = __ldcg(q + 2);
-            sb.mn[0] = x0.x; sb.mn[1] = x0.y; sb.mn[2] = x1.x; sb.mx[0] = x1.y; sb.mx[1] = x2.x; sb.mx[2] = x2.y;
+        if (local) {
+            const uint32_t k = p - base;
+            float* mine = s_box[2 * k + side];
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) { mine[ax] = box.mn[ax]; mine[3 + ax] = box.mx[ax]; }
+            __threadfence_block();
+            const int arrived = atomicAdd(&s_count[k], 1);
+            if (arrived == 0) return;
+            if (arrived != 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
+            __threadfence_block();
+            const volatile float* other = s_box[2 * k + (1 - side)];
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) { sb.mn[ax] = other[ax]; sb.mx[ax] = other[3 + ax]; }
         } else {
-            sb = piece_box(leaf_boxes, sib, true);
+            const int arrived = arrive_acq_rel(&counters[p]);
+            if (arrived == 0) return;
+            if (arrived != 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
+            const bool sib_internal = (word >> (1 - side)) & 1u;
+            if (sib_internal) {
+                const float2* q = reinterpret_cast<const float2*>(node_boxes + sib);
+                const float2 x0 = __ldcg(q), x1 = __ldcg(q + 1), x2 = __ldcg(q + 2);
+                sb.mn[0] = x0.x; sb.mn[1] = x0.y; sb.mn[2] = x1.x; sb.mx[0] = x1.y; sb.mx[1] = x2.x; sb.mx[2] = x2.y;
+            } else {
+                sb = piece_box(leaf_boxes, sib, true);
+            }
         }
 #pragma unroll
         for (int ax = 0; ax < 3; ++ax) {
@@ -880,7 +909,8 @@ int split_impl(cpt_bvh* bvh, uint32_t cap, bool ploc, void* nodes, void* scratch
     k_topology<K><<<(cap + 255) / 256, 256, 0, stream>>>(keys, 0, s.n_pieces, s.children, s.parents_leaf,
                                                           s.parents_internal, s.counters, static_cast<float4*>(nodes));
     CPT_LAUNCH_CHECK();
-    k_split_refit<<<(cap + 255) / 256, 256, 0, stream>>>(bvh->tris, s.pieces, order, s.n_pieces, s.children,
+    k_split_refit<<<(cap + kSplitRefitBlock - 1) / kSplitRefitBlock, kSplitRefitBlock, 0, stream>>>(
+        bvh->tris, s.pieces, order, s.n_pieces, s.children,
                                                           s.parents_leaf, s.parents_internal, s.counters,
                                                           static_cast<float*>(nodes), s.node_boxes, s.leaf_boxes, n,
                                                           bvh->status);
