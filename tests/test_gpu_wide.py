@@ -217,3 +217,42 @@ def test_split_far_camera_finds_every_closest_hit(cuda, distance):
     want = _closest_brute(tris, rays)
     assert (want < np.inf).mean() > 0.2
     assert np.array_equal(got, want)
+
+
+def test_wide_batched_views_match_binary(cuda):
+    """Several scenes in one call (the per-ray view lookup of the wide kernels): each
+    view's image equals its binary-tree image up to exact ties, with and without
+    next-event estimation; a call mixing wide and binary views traverses the binary
+    trees of all."""
+    specs = [(hairball(n_hair=6000, nu=32, nv=16, seed=s), s) for s in (1, 2)]
+    views, lbs, scs = [], [], []
+    cam = cpt.camera_look_at((0.0, 0.35, -3.6), (0.0, 0.0, 0.0), aspect=1.0)
+    for (tris, infos), s in specs:
+        lb = DeviceLbvh(len(tris), 63)
+        lb.build(to_device(tris))
+        lb.split(1.0)
+        sc = DeviceScene(infos)
+        sc.build_emitters(lb)
+        lbs.append(lb)
+        scs.append(sc)
+        views.append((lb, sc, cam, 40, 40))
+    for nee in (False, True):
+        p = make_params(0, 0, 4, 0, 4, 3.0, True, 9, cpt.ACCUM_KAHAN, nee=nee)
+        for lb in lbs:
+            lb.unwide()
+        r0 = BatchRenderer(views, p)
+        r0.render()
+        lbs[0].wide()
+        rm = BatchRenderer(views, p)  # mixed: every view traverses its binary tree
+        rm.render()
+        lbs[1].wide()
+        r1 = BatchRenderer(views, p)
+        r1.render()
+        torch.cuda.synchronize()
+        r1.check_status()
+        for k in range(2):
+            a0 = r0.accums[k].cpu().numpy().view(np.uint32)
+            assert a0.tobytes() == rm.accums[k].cpu().numpy().tobytes()
+            a1 = r1.accums[k].cpu().numpy().view(np.uint32)
+            differ = (a0.reshape(2, 40, 40, 4)[0] != a1.reshape(2, 40, 40, 4)[0]).any(-1)
+            assert differ.mean() < 0.003
