@@ -766,6 +766,7 @@ def run_ours(args, w, world, rank, local):
                "ms_per_step": round(e_ms_max / ne, 3), "wall_ms_per_step": round(1e3 * wall / ne, 3),
                "steps": ne, "includes": "H2D soup+shading records (pinned), LBVH build"
                                         + (f", split BVH build (extra {split})" if split > 0 else "")
+                                        + (", wide tree build" if args.wide else "")
                                         + ", 16-spp frame, D2H image"}
         tr.close()
 

@@ -425,6 +425,8 @@ extern "C" void cpt_camera_look_at(const float eye[3], const float target[3], co
 struct cpt_tracer {
     int bits = 63;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // shading-record uploads, overlapped with the builds
+    cudaEvent_t ev_upload = nullptr, ev_copied = nullptr;
     int device = 0;
     // scene
     uint32_t n = 0, info_count = 0, light_count = 0;
@@ -495,6 +497,9 @@ extern "C" int cpt_tracer_create(cpt_tracer** out, int morton_bits)
     t->bits = morton_bits;
     cudaGetDevice(&t->device);
     if (cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&t->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&t->ev_upload, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&t->ev_copied, cudaEventDisableTiming) != cudaSuccess ||
         cudaMalloc(reinterpret_cast<void**>(&t->d_counts), CPT_RAY_COUNTS * sizeof(unsigned long long)) != cudaSuccess) {
         cpt_tracer_destroy(t);
         return CPT_ERR_CUDA;
@@ -513,6 +518,10 @@ extern "C" void cpt_tracer_destroy(cpt_tracer* t)
                     t->d_emitters, t->d_wide_nodes, t->d_wide_tris, t->d_wide_scratch};
     for (void* b : bufs)
         if (b) cudaFree(b);
+    if (t->copy_stream) cudaStreamSynchronize(t->copy_stream);
+    if (t->ev_upload) cudaEventDestroy(t->ev_upload);
+    if (t->ev_copied) cudaEventDestroy(t->ev_copied);
+    if (t->copy_stream) cudaStreamDestroy(t->copy_stream);
     if (t->stream) cudaStreamDestroy(t->stream);
     delete t;
 }
@@ -524,6 +533,7 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
     if (!t || !tris || !infos || n < 2 || n > kMaxTriangles || info_count == 0 || (light_count && !lights))
         return CPT_ERR_INVALID_ARGUMENT;
     int rc;
+    t->ready = false;  // until this upload has completed its builds
     if ((rc = ensure(&t->d_tris, &t->tris_cap, sizeof(cpt_triangle) * (size_t)n))) return rc;
     const size_t bvh_bytes = cpt_bvh_bytes(n, t->bits), scr = cpt_lbvh_scratch_bytes(n, t->bits);
     if ((rc = ensure(&t->d_bvh, &t->bvh_cap, bvh_bytes))) return rc;
@@ -531,12 +541,19 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
     if ((rc = ensure(&t->d_infos, &t->infos_cap, sizeof(cpt_triangle_info) * (size_t)info_count))) return rc;
     if (light_count && (rc = ensure(&t->d_lights, &t->lights_cap, sizeof(cpt_dir_light) * (size_t)light_count))) return rc;
     if ((rc = cpt_bvh_bind(t->d_bvh, t->bvh_cap, n, t->bits, &t->bvh))) return rc;
+    // The triangles go first on the tracer's stream (the builds read them); the shading
+    // records and lights, which only the renderer reads, go on a second stream that
+    // starts after everything already queued on the tracer's stream (an earlier frame
+    // may still read them) and overlaps the builds; the next render waits for them.
+    CPT_CUDA_TRY(cudaEventRecord(t->ev_upload, t->stream));
+    CPT_CUDA_TRY(cudaStreamWaitEvent(t->copy_stream, t->ev_upload, 0));
     CPT_CUDA_TRY(cudaMemcpyAsync(t->d_tris, tris, sizeof(cpt_triangle) * (size_t)n, cudaMemcpyHostToDevice, t->stream));
     CPT_CUDA_TRY(cudaMemcpyAsync(t->d_infos, infos, sizeof(cpt_triangle_info) * (size_t)info_count, cudaMemcpyHostToDevice,
-                                 t->stream));
+                                 t->copy_stream));
     if (light_count)
         CPT_CUDA_TRY(cudaMemcpyAsync(t->d_lights, lights, sizeof(cpt_dir_light) * (size_t)light_count,
-                                     cudaMemcpyHostToDevice, t->stream));
+                                     cudaMemcpyHostToDevice, t->copy_stream));
+    CPT_CUDA_TRY(cudaEventRecord(t->ev_copied, t->copy_stream));
     rc = cpt_lbvh_build(static_cast<const cpt_triangle*>(t->d_tris), n, enclosing_box, t->bits, &t->bvh,
                         t->d_build_scratch, t->build_cap, 0, t->stream);
     if (rc) return rc;
@@ -563,6 +580,7 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
                            t->d_wide_scratch, t->wide_scratch_cap, t->stream);
         if (rc) return rc;
     }
+    CPT_CUDA_TRY(cudaStreamWaitEvent(t->stream, t->ev_copied, 0));
     t->n = n;
     t->info_count = info_count;
     t->light_count = light_count;
