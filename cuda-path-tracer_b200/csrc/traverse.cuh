@@ -356,6 +356,47 @@ __device__ __forceinline__ uint2 wide_pop(const uint2* smem_col, const uint2* sp
     return sp < kWideSmemStack ? smem_col[sp * kBlock] : spill[sp - kWideSmemStack];
 }
 
+// The children of a wide node (five float4 n0..n4) whose boxes the ray's interval
+// [0, best] meets: bit i for slot i.
+__device__ __forceinline__ uint32_t wide_child_hits(const WideState& s, float4 n0, float4 n2, float4 n3, float4 n4)
+{
+    const uint32_t ew = __float_as_uint(n0.w);
+    // plane t = q * (2^e / d) + (p - o) / d, evaluated as (2^23 + q) * a + (b - 2^23 * a): the
+    // folded offset costs at most half a quantum, and the build leaves one quantum of slack
+    const float sx = __uint_as_float((ew & 0xFFu) << 23), sy = __uint_as_float(((ew >> 8) & 0xFFu) << 23),
+                sz = __uint_as_float(((ew >> 16) & 0xFFu) << 23);
+    const float adx = sx * s.dinv.x, ady = sy * s.dinv.y, adz = sz * s.dinv.z;
+    const float bdx = fmaf(-8388608.0f, adx, (n0.x - s.o.x) * s.dinv.x);
+    const float bdy = fmaf(-8388608.0f, ady, (n0.y - s.o.y) * s.dinv.y);
+    const float bdz = fmaf(-8388608.0f, adz, (n0.z - s.o.z) * s.dinv.z);
+    // near / far planes per axis: lo and hi, swapped for a negative direction
+    const uint32_t lx0 = __float_as_uint(n2.x), lx1 = __float_as_uint(n2.y), ly0 = __float_as_uint(n2.z),
+                   ly1 = __float_as_uint(n2.w), lz0 = __float_as_uint(n3.x), lz1 = __float_as_uint(n3.y);
+    const uint32_t hx0 = __float_as_uint(n3.z), hx1 = __float_as_uint(n3.w), hy0 = __float_as_uint(n4.x),
+                   hy1 = __float_as_uint(n4.y), hz0 = __float_as_uint(n4.z), hz1 = __float_as_uint(n4.w);
+    const bool fx = s.oct & 1u, fy = s.oct & 2u, fz = s.oct & 4u;
+    const uint32_t nx0 = fx ? hx0 : lx0, nx1 = fx ? hx1 : lx1, fx0 = fx ? lx0 : hx0, fx1 = fx ? lx1 : hx1;
+    const uint32_t ny0 = fy ? hy0 : ly0, ny1 = fy ? hy1 : ly1, fy0 = fy ? ly0 : hy0, fy1 = fy ? ly1 : hy1;
+    const uint32_t nz0 = fz ? hz0 : lz0, nz1 = fz ? hz1 : lz1, fz0 = fz ? lz0 : hz0, fz1 = fz ? lz1 : hz1;
+    uint32_t hm = 0;
+    const float tlim = s.best.t;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t sel = 0x7440u | (uint32_t)(i & 3);
+        const float tnx = fmaf(qbyte(i < 4 ? nx0 : nx1, sel), adx, bdx);
+        const float tny = fmaf(qbyte(i < 4 ? ny0 : ny1, sel), ady, bdy);
+        const float tnz = fmaf(qbyte(i < 4 ? nz0 : nz1, sel), adz, bdz);
+        const float tfx = fmaf(qbyte(i < 4 ? fx0 : fx1, sel), adx, bdx);
+        const float tfy = fmaf(qbyte(i < 4 ? fy0 : fy1, sel), ady, bdy);
+        const float tfz = fmaf(qbyte(i < 4 ? fz0 : fz1, sel), adz, bdz);
+        // [max(tn, 0), min(tf, best) * (1 + 2^-18)] non-empty: the far end grows by a relative
+        // 2^-18, which covers the rounding of (p - o) / d for ray origins at any distance
+        const float tn = fmaxf(fmax3(tnx, tny, tnz), 0.0f), tf = fminf(fmin3(tfx, tfy, tfz), tlim) * kWideGrow;
+        hm |= (tn <= tf ? 1u : 0u) << i;
+    }
+    return hm;
+}
+
 // One step; returns true when the ray is finished.
 template <bool kAny, int kBlock, bool kStats>
 __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* spill, bool& overflow,
@@ -396,41 +437,8 @@ __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* 
     if (kStats) ++n_nodes;
     const float4* nd = s.nodes + 5 * (size_t)child;
     const float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3), n4 = __ldg(nd + 4);
-    const uint32_t ew = __float_as_uint(n0.w);
-    const uint32_t imask = ew >> 24, lmask = __float_as_uint(n1.z);
-    // plane t = q * (2^e / d) + (p - o) / d, evaluated as (2^23 + q) * a + (b - 2^23 * a): the
-    // folded offset costs at most half a quantum, and the build leaves one quantum of slack
-    const float sx = __uint_as_float((ew & 0xFFu) << 23), sy = __uint_as_float(((ew >> 8) & 0xFFu) << 23),
-                sz = __uint_as_float(((ew >> 16) & 0xFFu) << 23);
-    const float adx = sx * s.dinv.x, ady = sy * s.dinv.y, adz = sz * s.dinv.z;
-    const float bdx = fmaf(-8388608.0f, adx, (n0.x - s.o.x) * s.dinv.x);
-    const float bdy = fmaf(-8388608.0f, ady, (n0.y - s.o.y) * s.dinv.y);
-    const float bdz = fmaf(-8388608.0f, adz, (n0.z - s.o.z) * s.dinv.z);
-    // near / far planes per axis: lo and hi, swapped for a negative direction
-    const uint32_t lx0 = __float_as_uint(n2.x), lx1 = __float_as_uint(n2.y), ly0 = __float_as_uint(n2.z),
-                   ly1 = __float_as_uint(n2.w), lz0 = __float_as_uint(n3.x), lz1 = __float_as_uint(n3.y);
-    const uint32_t hx0 = __float_as_uint(n3.z), hx1 = __float_as_uint(n3.w), hy0 = __float_as_uint(n4.x),
-                   hy1 = __float_as_uint(n4.y), hz0 = __float_as_uint(n4.z), hz1 = __float_as_uint(n4.w);
-    const bool fx = s.oct & 1u, fy = s.oct & 2u, fz = s.oct & 4u;
-    const uint32_t nx0 = fx ? hx0 : lx0, nx1 = fx ? hx1 : lx1, fx0 = fx ? lx0 : hx0, fx1 = fx ? lx1 : hx1;
-    const uint32_t ny0 = fy ? hy0 : ly0, ny1 = fy ? hy1 : ly1, fy0 = fy ? ly0 : hy0, fy1 = fy ? ly1 : hy1;
-    const uint32_t nz0 = fz ? hz0 : lz0, nz1 = fz ? hz1 : lz1, fz0 = fz ? lz0 : hz0, fz1 = fz ? lz1 : hz1;
-    uint32_t hm = 0;
-    const float tlim = s.best.t;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const uint32_t sel = 0x7440u | (uint32_t)(i & 3);
-        const float tnx = fmaf(qbyte(i < 4 ? nx0 : nx1, sel), adx, bdx);
-        const float tny = fmaf(qbyte(i < 4 ? ny0 : ny1, sel), ady, bdy);
-        const float tnz = fmaf(qbyte(i < 4 ? nz0 : nz1, sel), adz, bdz);
-        const float tfx = fmaf(qbyte(i < 4 ? fx0 : fx1, sel), adx, bdx);
-        const float tfy = fmaf(qbyte(i < 4 ? fy0 : fy1, sel), ady, bdy);
-        const float tfz = fmaf(qbyte(i < 4 ? fz0 : fz1, sel), adz, bdz);
-        // [max(tn, 0), min(tf, best) * (1 + 2^-18)] non-empty: the far end grows by a relative
-        // 2^-18, which covers the rounding of (p - o) / d for ray origins at any distance
-        const float tn = fmaxf(fmax3(tnx, tny, tnz), 0.0f), tf = fminf(fmin3(tfx, tfy, tfz), tlim) * kWideGrow;
-        hm |= (tn <= tf ? 1u : 0u) << i;
-    }
+    const uint32_t imask = __float_as_uint(n0.w) >> 24, lmask = __float_as_uint(n1.z);
+    const uint32_t hm = wide_child_hits(s, n0, n2, n3, n4);
     s.cbase = __float_as_uint(n1.x);
     s.gbits = xor_permute8(hm & imask, s.oct) | (imask << 8);
     s.tbase = __float_as_uint(n1.y);
