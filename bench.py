@@ -781,10 +781,12 @@ def run_ours(args, w, world, rank, local):
         line = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded host generator)",
-                "config": workload_config(args.workload, w, n, "scene arrays 1.4 GB > 126 MB L2, no flush needed"),
+                "config": workload_config(args.workload, w, n, "scene arrays (LBVH 1.4 GB, traversal trees more) > "
+                                                               "126 MB L2, no flush needed"),
                 "rays_per_step": int(rays_all / args.steps), "roofline": roofline, "lbvh": lbvh,
-                "traversal_bvh": (f"split BVH (cpt_lbvh_split, extra pieces {split} x n)" if split > 0
-                                  else "LBVH (reference topology)"), "lbvh_topology": lbvh_topology,
+                "traversal_bvh": (("compressed 8-wide tree (cpt_lbvh_wide) over the " if args.wide else "")
+                                  + (f"split BVH (cpt_lbvh_split, extra pieces {split} x n)" if split > 0
+                                     else "LBVH (reference topology)")), "lbvh_topology": lbvh_topology,
                 "cpu_baseline": cpu_base, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
                 "parallelism": f"replicas x{world}: own BVH per GPU, disjoint sample streams, "
                                f"framebuffer reduce to rank 0 per frame" if world > 1 else "1 GPU",
@@ -961,7 +963,8 @@ def run_cache(args, w, world, rank, local):
                 "ms_per_step": round(main_run["cache"]["ms"] / max(1, main_run["cache"]["spp"] // spf), 3),
                 "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32 tracing, bf16 MLP (f32 accumulate)", "data": "synthetic (seeded host generator)",
-                "config": workload_config("c4", w, n, "scene arrays 1.4 GB > 126 MB L2, no flush needed"),
+                "config": workload_config("c4", w, n, "scene arrays (LBVH 1.4 GB, traversal trees more) > 126 MB L2, "
+                                                "no flush needed"),
                 "stratified": main_run, "unstratified": alt,
                 "next_event": ({"stratified": nee_summary(main_run, nee_runs[0]),
                                 "unstratified": nee_summary(alt, nee_runs[1]),
