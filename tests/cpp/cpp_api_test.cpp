@@ -74,6 +74,19 @@ int main(int argc, char** argv)
     if (!write(out + "/image.bin", tracer.readImage(48, 32))) return 1;
     std::printf("frames %u\n", tracer.frame());
 
+    // the extensions: split and wide traversal trees, next-event estimation
+    cpt::CUDAPathTracer fast(30);
+    fast.setSettings(3, 3.0f, true, 7);
+    fast.setSplit(2.0f);
+    fast.setWide(true);
+    fast.setNextEventEstimation(true);
+    fast.upload(scene);
+    fast.setPrimaryRays(ray(0), ray(1), ray(2), ray(3));
+    fast.setEyePos({cam.eye[0], cam.eye[1], cam.eye[2]});
+    fast.raytrace(48, 32);
+    if (cpt::last_error() != CPT_OK) return 1;
+    if (!write(out + "/image_ext.bin", fast.readImage(48, 32))) return 1;
+
     // error behaviour: reported and kept, the tracer stays usable
     tracer.raytrace(0, 32);
     if (cpt::last_error() != CPT_ERR_INVALID_ARGUMENT) return 1;

@@ -49,3 +49,18 @@ def test_cpp_classes_build_and_render(cuda, tmp_path):
     assert img.tobytes() == ref.tobytes()
     assert np.isfinite(img).all() and img[..., :3].max() > 0
     t.close()
+    # setSplit / setWide / setNextEventEstimation against the same calls through the C ABI
+    t = cpt.Tracer(30)
+    t.set_settings(bounces=3, intensity=3.0, stratified=True, seed=7)
+    t.set_split(2.0)
+    t.set_wide(True)
+    t.set_nee(True)
+    t.upload(tris, infos, None, box)
+    t.set_primary_rays(cam.as_array()[3:])
+    t.set_eye(cam.eye)
+    t.raytrace(48, 32)
+    ref = t.read_image(48, 32)
+    img = np.fromfile(tmp_path / "image_ext.bin", np.float32).reshape(32, 48, 4)
+    assert img.tobytes() == ref.tobytes()
+    assert t.bvh().wide_capacity == t.bvh().split_capacity > 0
+    t.close()
