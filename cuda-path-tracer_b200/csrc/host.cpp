@@ -12,6 +12,7 @@
 #include <vector>
 #include "cpt.h"
 #include "cpt_internal.h"
+#include "render_hook.h"
 
 namespace cpt {
 
@@ -580,7 +581,6 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
                            t->d_wide_scratch, t->wide_scratch_cap, t->stream);
         if (rc) return rc;
     }
-    CPT_CUDA_TRY(cudaStreamWaitEvent(t->stream, t->ev_copied, 0));
     t->n = n;
     t->info_count = info_count;
     t->light_count = light_count;
@@ -713,11 +713,24 @@ extern "C" int cpt_tracer_raytrace(cpt_tracer* t, uint32_t width, uint32_t heigh
                  t->texture_count ? static_cast<const cudaTextureObject_t*>(t->d_textures) : nullptr, t->texture_count,
                  nullptr};
     if (t->nee) {
+        CPT_CUDA_TRY(cudaStreamWaitEvent(t->stream, t->ev_copied, 0));  // the table reads the shading records
         if ((rc = tracer_emitters(t, sc))) return rc;
         sc.emitters = t->d_emitters;
     }
-    rc = cpt_render(&t->bvh, &sc, &t->cam, &p, t->d_accum, t->d_render_scratch, t->render_cap, t->d_counts,
-                    t->bvh.status, t->stream);
+    // the shading records of the last upload may still be copying: the frame's first
+    // shading launch waits for them, the primary traversal does not
+    cpt_view view{};
+    view.bvh = &t->bvh;
+    view.scene = &sc;
+    view.camera = t->cam;
+    view.width = width;
+    view.height = height;
+    view.accum = t->d_accum;
+    RenderHook hook{};
+    hook.image_pass = true;
+    hook.shade_after = t->ev_copied;
+    rc = cpt_render_views_hooked(&view, 1, &p, t->d_render_scratch, t->render_cap, t->d_counts, t->bvh.status, &hook,
+                                 t->stream);
     if (rc) return rc;
     t->frame += spp;
     return CPT_OK;

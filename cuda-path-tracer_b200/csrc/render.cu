@@ -998,6 +998,8 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
             }
             CPT_LAUNCH_CHECK();
             const bool nee_here = params->nee && b < params->bounces;
+            if (hook && hook->shade_after && s0 == 0 && b == 0)
+                CPT_CUDA_TRY(cudaStreamWaitEvent(stream, hook->shade_after, 0));
             {
                 CPT_PROF(K_SHADE, stream);
 #define CPT_SHADE(L, R, N)                                                                                          \

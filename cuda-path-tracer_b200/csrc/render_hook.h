@@ -1,4 +1,4 @@
-// Wavefront-render extension points used by the radiance cache.
+// Wavefront-render extension points used by the radiance cache and the tracer object.
 #pragma once
 #include <cuda_runtime.h>
 #include <stddef.h>
@@ -23,6 +23,10 @@ struct RenderHook {
     int (*after_wave)(void* ctx, const float4* records, const uint32_t* record_count, uint32_t capacity,
                       float4* state, cudaStream_t stream);
     void* ctx;
+    // nullable: the first shading launch waits for this event (the shading records or
+    // lights may still be on their way to the device; the traversal before it does not
+    // read them)
+    cudaEvent_t shade_after;
 };
 
 // Bytes of a record buffer for this render (0 on bad arguments); *capacity gets

@@ -20,7 +20,9 @@
 //   k_split_weight/total  w_i = sqrt(max(0, area(box_i) - 2 area(tri_i))), sum in fixed order
 //   k_split_count         pieces s_i = 1 + min(63, floor(extra * w_i / sum w)) -> sum s_i <= n + extra
 //   k_split_scan_tiles    piece offsets of each 4096-triangle tile, total piece count
-//   k_split_emit          pieces: clipped boxes, Morton keys of their centres in the root box,
+//   k_split_first         each triangle's first piece (exclusive offsets, in place of the counts)
+//   k_split_emit          pieces, 64 per thread (balanced however the triangles are cut):
+//                         clipped boxes, Morton keys of their centres in the root box,
 //                         digit histograms, zeroed look-back state
 //   k_scan_offsets, k_onesweep x P, k_topology   as the main build, on the device count
 //   k_split_refit         leaf slots + bottom-up boxes into the 96-B traversal nodes
@@ -248,14 +250,45 @@ __device__ __forceinline__ void clip_box(const cpt_triangle& t, int axis, float 
     bmx[axis] = fminf(hi_s, thi[axis]);
 }
 
+// Piece counts -> exclusive per-triangle piece offsets, in place (tile offsets from
+// k_split_scan_tiles, a block scan inside the tile).
+__global__ void __launch_bounds__(kSplitBlock) k_split_first(uint32_t n, uint32_t* __restrict__ counts,
+                                                             const uint32_t* __restrict__ tile_offsets)
+{
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    uint32_t c[kScanItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t i = base + k;
+        c[k] = i < n ? counts[i] : 0u;
+        sum += c[k];
+    }
+    uint32_t block_total;
+    uint32_t off = tile_offsets[blockIdx.x] + block_exclusive_scan(sum, &block_total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t i = base + k;
+        if (i < n) counts[i] = off;
+        off += c[k];
+    }
+}
+
+// Pieces of the triangles, kEmitPieces consecutive pieces per thread whatever the
+// triangles they come from (a long hairball triangle is cut into up to 64 pieces):
+// piece j belongs to the triangle i with first[i] <= j < first[i + 1], found once per
+// thread by binary search. Writes the piece box, its Morton key and all the digit
+// histograms of the sort, and zeroes the sort's look-back state.
+constexpr int kEmitPieces = 64;
+
 template <typename K>
 __global__ void __launch_bounds__(kSplitBlock) k_split_emit(const cpt_triangle* __restrict__ tris, uint32_t n,
-                                                            const uint32_t* __restrict__ counts,
-                                                            const uint32_t* __restrict__ tile_offsets,
-                                                            const cpt_bbox* __restrict__ root, uint32_t capacity,
+                                                            const uint32_t* __restrict__ first,
+                                                            const uint32_t* __restrict__ n_pieces,
+                                                            const cpt_bbox* __restrict__ root,
                                                             float4* __restrict__ pieces, K* __restrict__ keys,
                                                             uint32_t* __restrict__ hist, uint32_t* __restrict__ zero,
-                                                            size_t zero_words, uint32_t* __restrict__ status)
+                                                            size_t zero_words)
 {
     constexpr int P = KeyTraits<K>::passes;
     constexpr int order = KeyTraits<K>::order;
@@ -265,6 +298,7 @@ __global__ void __launch_bounds__(kSplitBlock) k_split_emit(const cpt_triangle* 
         const size_t gtid = (size_t)blockIdx.x * kSplitBlock + threadIdx.x, gsize = (size_t)gridDim.x * kSplitBlock;
         for (size_t i = gtid; i < zero_words; i += gsize) zero[i] = 0;
     }
+    __syncthreads();
     float rmn[3], rinv[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -272,28 +306,40 @@ __global__ void __launch_bounds__(kSplitBlock) k_split_emit(const cpt_triangle* 
         rinv[a] = __frcp_rn(__fsub_rn(root->max[a], root->min[a]));
     }
     const uint32_t cells = 1u << order;
-    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-    uint32_t sum = 0;
-    for (int k = 0; k < kScanItems; ++k) {
-        const uint32_t i = base + k;
-        if (i < n) sum += counts[i];
-    }
-    uint32_t block_total;
-    uint32_t off = tile_offsets[blockIdx.x] + block_exclusive_scan(sum, &block_total);
-    bool overflow = false;
-    for (int k = 0; k < kScanItems; ++k) {
-        const uint32_t i = base + k;
-        if (i >= n) break;
-        const cpt_triangle t = tris[i];
-        const uint32_t s = counts[i];
+    const uint32_t np = *n_pieces;
+    const uint64_t j0 = ((uint64_t)blockIdx.x * kSplitBlock + threadIdx.x) * kEmitPieces;
+    if (j0 < np) {
+        uint32_t lo = 0, hi = n - 1;  // the last triangle whose first piece is at or before j0
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (first[mid] <= j0) lo = mid;
+            else hi = mid - 1;
+        }
+        uint32_t i = lo;
+        uint32_t fi = first[i];
+        uint32_t ei = i + 1 < n ? first[i + 1] : np;
+        cpt_triangle t = tris[i];
         float tlo[3], thi[3];
-        tri_box(t, tlo, thi);
         int axis = 0;
-        float ext = thi[0] - tlo[0];
-        if (thi[1] - tlo[1] > ext) { axis = 1; ext = thi[1] - tlo[1]; }
-        if (thi[2] - tlo[2] > ext) { axis = 2; ext = thi[2] - tlo[2]; }
-        for (uint32_t p = 0; p < s; ++p, ++off) {
-            if (off >= capacity) { overflow = true; break; }
+        float ext = 0.f;
+        auto setup = [&]() {
+            tri_box(t, tlo, thi);
+            axis = 0;
+            ext = thi[0] - tlo[0];
+            if (thi[1] - tlo[1] > ext) { axis = 1; ext = thi[1] - tlo[1]; }
+            if (thi[2] - tlo[2] > ext) { axis = 2; ext = thi[2] - tlo[2]; }
+        };
+        setup();
+        const uint32_t jend = j0 + kEmitPieces < (uint64_t)np ? (uint32_t)(j0 + kEmitPieces) : np;
+        for (uint32_t j = (uint32_t)j0; j < jend; ++j) {
+            while (j >= ei && i + 1 < n) {  // the next triangle with pieces
+                ++i;
+                fi = ei;
+                ei = i + 1 < n ? first[i + 1] : np;
+                t = tris[i];
+                setup();
+            }
+            const uint32_t s = ei - fi, p = j - fi;
             float bmn[3], bmx[3];
             if (s == 1) {
 #pragma unroll
@@ -303,8 +349,8 @@ __global__ void __launch_bounds__(kSplitBlock) k_split_emit(const cpt_triangle* 
                 const float hi_s = p + 1 == s ? thi[axis] : tlo[axis] + ext * ((float)(p + 1) / (float)s);
                 clip_box(t, axis, lo_s, hi_s, tlo, thi, bmn, bmx);
             }
-            pieces[2 * (size_t)off] = make_float4(bmn[0], bmn[1], bmn[2], __uint_as_float(i));
-            pieces[2 * (size_t)off + 1] = make_float4(bmx[0], bmx[1], bmx[2], 0.f);
+            pieces[2 * (size_t)j] = make_float4(bmn[0], bmn[1], bmn[2], __uint_as_float(i));
+            pieces[2 * (size_t)j + 1] = make_float4(bmx[0], bmx[1], bmx[2], 0.f);
             uint32_t q[3];
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
@@ -312,12 +358,11 @@ __global__ void __launch_bounds__(kSplitBlock) k_split_emit(const cpt_triangle* 
                 q[a] = quantize(__fmul_rn(__fsub_rn(c, rmn[a]), rinv[a]), cells);
             }
             const uint64_t key = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
-            keys[off] = (K)key;
+            keys[j] = (K)key;
 #pragma unroll
             for (int pp = 0; pp < P; ++pp) atomicAdd(&s_hist[pp * kRadix + (uint32_t)((key >> (8 * pp)) & 0xFF)], 1u);
         }
     }
-    if (overflow) atomicOr(status, CPT_STATUS_BAD_INDEX);
     __syncthreads();
     for (int i = threadIdx.x; i < P * kRadix; i += kSplitBlock)
         if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
@@ -875,9 +920,12 @@ int split_impl(cpt_bvh* bvh, uint32_t cap, bool ploc, void* nodes, void* scratch
     CPT_LAUNCH_CHECK();
     k_split_scan_tiles<<<1, 1024, 0, stream>>>(s.tile_sums, ctiles, cap, s.n_pieces, bvh->status);
     CPT_LAUNCH_CHECK();
-    k_split_emit<K><<<ctiles, kSplitBlock, 0, stream>>>(bvh->tris, n, s.counts, s.tile_sums, bvh->node_boxes, cap,
-                                                        s.pieces, s.keys[0], s.hist, s.zero, s.zero_words,
-                                                        bvh->status);
+    k_split_first<<<ctiles, kSplitBlock, 0, stream>>>(n, s.counts, s.tile_sums);
+    CPT_LAUNCH_CHECK();
+    const uint32_t eblocks = (uint32_t)(((uint64_t)cap + (uint64_t)kSplitBlock * kEmitPieces - 1) /
+                                        ((uint64_t)kSplitBlock * kEmitPieces));
+    k_split_emit<K><<<eblocks, kSplitBlock, 0, stream>>>(bvh->tris, n, s.counts, s.n_pieces, bvh->node_boxes,
+                                                         s.pieces, s.keys[0], s.hist, s.zero, s.zero_words);
     CPT_LAUNCH_CHECK();
     k_scan_offsets<<<P, kRadix, 0, stream>>>(s.hist, s.offsets);
     CPT_LAUNCH_CHECK();
