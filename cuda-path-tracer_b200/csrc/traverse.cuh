@@ -1,4 +1,4 @@
-// Closest-hit / any-hit traversal over the compact LBVH records.
+// Closest-hit / any-hit traversal over the compact LBVH records and over the wide tree.
 //
 // Follows CUDA::trace (source/application/cuda/trace.h:73-169) decision for
 // decision — both children tested (left first), both-farther-than-best pruning,
@@ -26,6 +26,10 @@
 //    warp takes new rays for its idle lanes once fewer than half of them still
 //    trace, so a warp is not held by its slowest ray (per-ray node counts differ
 //    by 100x on hairball scenes).
+//
+// The second half of the file traverses the compressed 8-wide tree (cpt_lbvh_wide)
+// built over a binary tree: 80-B nodes with 8-bit child planes, the same triangle
+// test on the binary leaf slot's words, and a refill as soon as one lane is idle.
 #pragma once
 #include "cpt_device.cuh"
 #include "cpt.h"
