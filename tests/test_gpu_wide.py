@@ -256,3 +256,34 @@ def test_wide_batched_views_match_binary(cuda):
             a1 = r1.accums[k].cpu().numpy().view(np.uint32)
             differ = (a0.reshape(2, 40, 40, 4)[0] != a1.reshape(2, 40, 40, 4)[0]).any(-1)
             assert differ.mean() < 0.003
+
+
+def test_wide_build_rejects_bad_arguments(cuda):
+    """Buffers below cpt_lbvh_wide_bytes, misaligned or missing pointers: an error code
+    and no wide tree attached."""
+    import ctypes
+
+    tris, _ = cpt.scene_random(3000, seed=2)
+    lb = DeviceLbvh(len(tris), 30)
+    lb.build(to_device(tris))
+    nb, tb = ctypes.c_size_t(), ctypes.c_size_t()
+    sb = int(cpt.lib.cpt_lbvh_wide_bytes(lb.n, ctypes.byref(nb), ctypes.byref(tb)))
+    assert sb > 0 and nb.value >= (lb.n - 1) * 80 and tb.value >= lb.n * 48
+    assert cpt.lib.cpt_lbvh_wide_bytes(1, None, None) == 0
+    nodes = torch.empty(nb.value, dtype=torch.uint8, device="cuda")
+    trs = torch.empty(tb.value, dtype=torch.uint8, device="cuda")
+    scr = torch.empty(sb, dtype=torch.uint8, device="cuda")
+    b = ctypes.byref(lb.bvh)
+    assert cpt.lib.cpt_lbvh_wide(b, nodes.data_ptr(), nb.value - 16, trs.data_ptr(), tb.value, scr.data_ptr(), sb,
+                                 0) == cpt.ERR_SCRATCH_TOO_SMALL
+    assert cpt.lib.cpt_lbvh_wide(b, nodes.data_ptr(), nb.value, trs.data_ptr(), tb.value, scr.data_ptr(), sb - 1,
+                                 0) == cpt.ERR_SCRATCH_TOO_SMALL
+    assert cpt.lib.cpt_lbvh_wide(b, nodes.data_ptr() + 4, nb.value, trs.data_ptr(), tb.value, scr.data_ptr(), sb,
+                                 0) == cpt.ERR_INVALID_ARGUMENT
+    assert cpt.lib.cpt_lbvh_wide(b, None, nb.value, trs.data_ptr(), tb.value, scr.data_ptr(), sb,
+                                 0) == cpt.ERR_INVALID_ARGUMENT
+    assert not lb.bvh.wide_nodes
+    assert cpt.lib.cpt_lbvh_wide(b, nodes.data_ptr(), nb.value, trs.data_ptr(), tb.value, scr.data_ptr(), sb, 0) == 0
+    torch.cuda.synchronize()
+    lb.status()
+    assert lb.bvh.wide_nodes == nodes.data_ptr() and lb.bvh.wide_capacity == lb.n
