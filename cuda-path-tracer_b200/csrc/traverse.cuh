@@ -273,6 +273,11 @@ constexpr float kWideGrow = 1.0f + 1.0f / 262144.0f;  // relative slack of a wid
 #define CPT_WIDE_REFILL_LANES 32
 #endif
 constexpr int kWideRefillLanes = CPT_WIDE_REFILL_LANES;
+// A lane with triangles still to test may visit its next node in the same step, the
+// node's triangle group queuing behind the first (at most two groups pending).
+#ifndef CPT_WIDE_DUAL
+#define CPT_WIDE_DUAL 1
+#endif
 constexpr float kWideFarInv = 1099511627776.0f;  // 2^40: 1/d of a zero direction component
 
 struct WideState {
@@ -285,6 +290,7 @@ struct WideState {
     Hit best;
     uint32_t cbase, gbits;  // node group: first child; bits 0-7 hit slots in visit order, 8-15 internal mask
     uint32_t tbase, tbits;  // triangle group: first record; bits 0-7 hit leaf slots, 8-15 leaf mask
+    uint32_t tbase2, tbits2;  // a second triangle group, queued behind the first (CPT_WIDE_DUAL)
     int sp;
     uint32_t visits, tests;
 };
@@ -310,6 +316,8 @@ __device__ __forceinline__ void wide_init(WideState& s, const float4* nodes, con
     s.gbits = (1u << s.oct) | (1u << 8);
     s.tbase = 0;
     s.tbits = 0;
+    s.tbase2 = 0;
+    s.tbits2 = 0;
     s.sp = 0;
     s.visits = 0;
     s.tests = 0;
@@ -424,10 +432,23 @@ __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* 
             s.best.tri = __float_as_uint(a.w);
             if (kAny) return true;
         }
+#if CPT_WIDE_DUAL
+        if (!(s.tbits & 0xFFu) && (s.tbits2 & 0xFFu)) {  // the queued group moves up
+            s.tbase = s.tbase2;
+            s.tbits = s.tbits2;
+            s.tbits2 = 0;
+        }
+        if (s.tbits2 & 0xFFu) return false;  // both groups pending: no node visit this step
+#else
         if (s.tbits & 0xFFu) return false;  // more triangles of this group: next step
+#endif
     }
     if (!(s.gbits & 0xFFu)) {
+#if CPT_WIDE_DUAL
+        if (s.sp == 0) return !(s.tbits & 0xFFu);  // done once the last triangles are tested
+#else
         if (s.sp == 0) return true;
+#endif
         const uint2 g = wide_pop<kBlock>(smem_col, spill, s.sp);
         s.cbase = g.x;
         s.gbits = g.y;
@@ -445,6 +466,13 @@ __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* 
     const uint32_t hm = wide_child_hits(s, n0, n2, n3, n4);
     s.cbase = __float_as_uint(n1.x);
     s.gbits = xor_permute8(hm & imask, s.oct) | (imask << 8);
+#if CPT_WIDE_DUAL
+    if (s.tbits & 0xFFu) {  // triangles still pending: the new group queues behind them
+        s.tbase2 = __float_as_uint(n1.y);
+        s.tbits2 = (hm & lmask) | (lmask << 8);
+        return false;
+    }
+#endif
     s.tbase = __float_as_uint(n1.y);
     s.tbits = (hm & lmask) | (lmask << 8);
     return false;
