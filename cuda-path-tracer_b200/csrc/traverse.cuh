@@ -259,10 +259,11 @@ __device__ __forceinline__ Hit traverse(const float4* __restrict__ nodes, f3 o, 
 // per-axis exponents e (child box planes p + q * 2^e, q one byte), the masks of its
 // internal and leaf slots, the index of its first internal child and of its first
 // triangle record, and the 48 quantized planes. The ray carries a node group — the
-// hit internal slots of one node still to visit, in the order k ^ octant(ray) — and
-// a triangle group — the hit leaf slots of the node just visited. A step tests one
-// triangle of the triangle group, or else visits the next node of the node group
-// (the rest of the group goes on the stack), or else pops a group. The triangle test
+// hit internal slots of one node still to visit, in the order k ^ octant(ray) — and up
+// to three triangle groups — the hit leaf slots of nodes visited, in visiting order. A
+// step tests one triangle of the first triangle group and, unless every group slot is
+// taken, visits the next node of the node group (the rest of the group goes on the
+// stack; the node's triangle group queues behind), or pops a group. The triangle test
 // is tri_test on the binary leaf slot's words, so a hit's t, u, v are unchanged.
 constexpr int kWideSmemStack = 16;  // stack entries (2 words) per thread in shared memory
 constexpr float kWideGrow = 1.0f + 1.0f / 262144.0f;  // relative slack of a wide child's box test
