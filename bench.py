@@ -284,7 +284,7 @@ def run_batch(args, w, world, rank, local):
         d = to_device(tris, dev)
         lb.build(d, check_root=True)
         if kind != "random" and split > 0:  # the hairball scenes traverse a split BVH
-            lb.split(split)
+            lb.split(split, flags=split_flags(args))
         if args.wide:
             lb.wide(keep_scratch=True)
         sc = DeviceScene(infos, None, dev)
@@ -382,7 +382,7 @@ def run_batch(args, w, world, rank, local):
     hair = [specs[i][0] != "random" and split > 0 for i in mine]
     for (lb, _, _, _, _), h in zip(views, hair):
         if h:
-            lb.split(split, keep_scratch=True)  # scratch stays allocated for the captured rebuilds
+            lb.split(split, keep_scratch=True, flags=split_flags(args))  # scratch stays allocated for the captured rebuilds
         if args.wide:
             lb.wide(keep_scratch=True)
     torch.cuda.synchronize()
@@ -391,7 +391,7 @@ def run_batch(args, w, world, rank, local):
         for (lb, _, _, _, _), d, h in zip(views, keep, hair):
             lb.build(d)
             if h:
-                lb.split(split, keep_scratch=True)
+                lb.split(split, keep_scratch=True, flags=split_flags(args))
             if args.wide:
                 lb.wide(keep_scratch=True)
 
@@ -530,7 +530,7 @@ def run_ours(args, w, world, rank, local):
     lb.build(d_tris, check_root=True)
     split = w.get("split", 0.0) if args.split is None else args.split
     if split > 0:
-        lb.split(split, keep_scratch=True)
+        lb.split(split, keep_scratch=True, flags=split_flags(args))
     if args.wide:
         lb.wide(keep_scratch=True)
     params = make_params(W_, H_, spp, 0, w["bounces"], 3.0, True, w["seed"], cpt.ACCUM_KAHAN,
@@ -542,7 +542,7 @@ def run_ours(args, w, world, rank, local):
                                            0.1 * frame_index, stream_handle()), "cpt_scene_deform")
         lb.build(d_tris)
         if split > 0:
-            lb.split(split, keep_scratch=True)
+            lb.split(split, keep_scratch=True, flags=split_flags(args))
         if args.wide:
             lb.wide(keep_scratch=True)
     rend = DeviceRenderer(params, dev)
@@ -669,11 +669,11 @@ def run_ours(args, w, world, rank, local):
         u_rays = sum_over_ranks(int(rend.counts[:3].sum()), world)
         lbvh_topology = {"mrays_s": round(u_rays / (u_ms / 1e3) / 1e6, 3), "ms_per_step": round(u_ms, 3),
                          "note": "one frame traversing the reference-topology LBVH instead of the split BVH"}
-        lb.split(split, keep_scratch=True)
+        lb.split(split, keep_scratch=True, flags=split_flags(args))
         torch.cuda.synchronize()
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s0.record(stream)
-        lb.split(split, keep_scratch=True)
+        lb.split(split, keep_scratch=True, flags=split_flags(args))
         s1.record(stream)
         torch.cuda.synchronize()
         lbvh_topology["split_build_ms"] = round(s0.elapsed_time(s1), 3)
@@ -785,7 +785,8 @@ def run_ours(args, w, world, rank, local):
                                                                "126 MB L2, no flush needed"),
                 "rays_per_step": int(rays_all / args.steps), "roofline": roofline, "lbvh": lbvh,
                 "traversal_bvh": (("compressed 8-wide tree (cpt_lbvh_wide) over the " if args.wide else "")
-                                  + (f"split BVH (cpt_lbvh_split, extra pieces {split} x n)" if split > 0
+                                  + (f"split BVH (cpt_lbvh_split, extra pieces {split} x n"
+                                     + (", treelet-restructured" if args.treelet else "") + ")" if split > 0
                                      else "LBVH (reference topology)")), "lbvh_topology": lbvh_topology,
                 "cpu_baseline": cpu_base, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
                 "parallelism": f"replicas x{world}: own BVH per GPU, disjoint sample streams, "
@@ -823,7 +824,7 @@ def run_cache(args, w, world, rank, local):
     lb.build(to_device(tris, dev), check_root=True)
     split = w.get("split", 0.0) if args.split is None else args.split
     if split > 0:
-        lb.split(split)
+        lb.split(split, flags=split_flags(args))
     if args.wide:
         lb.wide()
     scene = DeviceScene(infos, None, dev)
@@ -977,6 +978,13 @@ def run_cache(args, w, world, rank, local):
     return 0
 
 
+def split_flags(args) -> int:
+    """cpt_lbvh_split flags of the run: treelet restructuring on request."""
+    import cpt
+
+    return cpt.SPLIT_TREELET if args.treelet else 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1000,10 +1008,15 @@ def main():
                     help="c4: also compare with next-event estimation in both tracers (1) or not (0)")
     ap.add_argument("--split", type=float, default=None,
                     help="split traversal BVH extra-piece ratio (0: traverse the LBVH; default per workload)")
+    ap.add_argument("--treelet", type=int, default=None,
+                    help="1: treelet restructuring of the split BVH's topology (CPT_SPLIT_TREELET), 0: the Karras "
+                         "topology (default per workload)")
     args = ap.parse_args()
     w = dict(WORKLOADS[args.workload])
     if args.wide is None:
         args.wide = int(w.get("wide", 0))
+    if args.treelet is None:
+        args.treelet = int(w.get("treelet", 0))
     if args.res:
         w["width"], w["height"] = (int(x) for x in args.res.lower().split("x"))
     if args.spp:

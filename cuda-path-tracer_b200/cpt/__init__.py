@@ -40,6 +40,7 @@ BUILD_CHECK = 1
 ACCUM_KAHAN, ACCUM_LERP, ACCUM_F64 = 0, 1, 2
 INVALID_INDEX = 0xFFFFFFFF
 SPLIT_PLOC = 1
+SPLIT_TREELET = 2
 TRAVERSAL_STACK = 64
 
 TRIANGLE_DTYPE = np.dtype([("v0", "<f4", 3), ("v1", "<f4", 3), ("v2", "<f4", 3), ("info_idx", "<u4")])

@@ -594,6 +594,8 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
 extern "C" int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio, uint32_t flags)
 {
     if (!t || !(extra_ratio >= 0.f) || !(extra_ratio <= 64.f)) return CPT_ERR_INVALID_ARGUMENT;
+    if ((flags & ~(CPT_SPLIT_PLOC | CPT_SPLIT_TREELET)) || (flags & CPT_SPLIT_PLOC && flags & CPT_SPLIT_TREELET))
+        return CPT_ERR_INVALID_ARGUMENT;
     t->split_ratio = extra_ratio;
     t->split_flags = flags;
     return CPT_OK;

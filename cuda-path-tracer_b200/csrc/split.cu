@@ -26,6 +26,7 @@
 //                         digit histograms, zeroed look-back state
 //   k_scan_offsets, k_onesweep x P, k_topology   as the main build, on the device count
 //   k_split_refit         leaf slots + bottom-up boxes into the 96-B traversal nodes
+//   k_treelet x 3         (CPT_SPLIT_TREELET) treelet restructuring of the Karras topology
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -480,6 +481,368 @@ __global__ void __launch_bounds__(kSplitRefitBlock) k_split_refit(const cpt_tria
 }
 
 // ---------------------------------------------------------------------------
+// Treelet restructuring (CPT_SPLIT_TREELET; Karras and Aila, "Fast Parallel
+// Construction of High-Quality Bounding Volume Hierarchies", HPG 2013), applied to
+// the split tree after its refit. The cost of a tree is the sum of the surface
+// areas of its internal nodes (the surface-area heuristic with the leaves fixed:
+// every piece stays one leaf). A bottom-up walk with the refit's arrival counters
+// reaches a node once both its subtrees are final; where the node has at least
+// gamma leaves, its warp forms a treelet — the node's two children, then, up to 7
+// leaves, the internal treelet leaf of largest area replaced by its two children —
+// and finds the least-cost topology over those leaves by dynamic programming over
+// their subsets, c(S) = area(S) + min over splits S = P + (S \ P) of c(P) + c(S \ P)
+// (one leaf: 0), the lanes sharing out the 966 (subset, split) pairs of 7 leaves.
+// A cheaper topology that is no taller than the old one replaces it in the same
+// nodes (the treelet root keeps its index, box and parent). The result does not
+// depend on timing: a treelet sees only its finished subtree, areas and sums are
+// rounded without contraction, and equal costs go to the smallest split mask.
+// Rounds with gamma = 7, 14, 28. Since no treelet grows taller, the tree is never
+// taller than the Karras tree it starts from.
+// ---------------------------------------------------------------------------
+constexpr int kTreeletBlock = 128;
+constexpr int kTreeletWarps = kTreeletBlock / 32;
+constexpr int kTreeletLeaves = 7;
+constexpr int kTreeletSubsets = 1 << kTreeletLeaves;
+constexpr int kTreeletPairs = 966;  // sum over k = 2..7 of C(7, k) (2^(k-1) - 1)
+constexpr int kTreeletRounds = 3;
+constexpr int kTreeletGamma = 7;
+constexpr int kTreeletMaxLevels = 1024;
+
+// Index of the first (subset, split) pair of the subsets of k leaves (k = 2..7;
+// k = 8 gives the total).
+__device__ __forceinline__ int treelet_class_start(int k)
+{
+    switch (k) {
+    case 2: return 0;
+    case 3: return 21;
+    case 4: return 126;
+    case 5: return 371;
+    case 6: return 686;
+    case 7: return 903;
+    default: return kTreeletPairs;
+    }
+}
+
+// Half the surface area of a box (lo xyz, hi xyz), rounded alike on every run.
+__device__ __forceinline__ float half_area(const float* b)
+{
+    const float dx = __fsub_rn(b[3], b[0]), dy = __fsub_rn(b[4], b[1]), dz = __fsub_rn(b[5], b[2]);
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dy), __fmul_rn(dy, dz)), __fmul_rn(dz, dx));
+}
+
+struct TreeletWarp {
+    unsigned long long best[kTreeletSubsets];  // (cost bits << 32) | split mask, reduced by atomicMin
+    float c[kTreeletSubsets];                  // least cost over a subset (its area until its size class)
+    float box[kTreeletLeaves][6];
+    float slot[kTreeletLeaves][10];            // the leaf's 40-B child slot as its parent held it
+    float area[kTreeletLeaves];
+    uint32_t id[kTreeletLeaves];               // internal node index, or piece position for a leaf
+    uint32_t height[kTreeletLeaves];
+    uint32_t size[kTreeletLeaves];
+    uint32_t inode[kTreeletLeaves - 1];        // the treelet's internal nodes, [0] = its root
+    uint32_t internal_mask;                    // bit k: treelet leaf k is an internal node
+    uint32_t m;                                // treelet leaves (0: bad index met)
+    float old_cost;
+    uint8_t split[kTreeletSubsets];
+};
+
+// Treelet leaves k0 and k1 := the two children of internal node q. False on an out-of-range index.
+__device__ bool treelet_take_children(const float* __restrict__ nodes, const float4* __restrict__ leaf_boxes,
+                                      const uint2* __restrict__ info, uint32_t n, uint32_t q, int k0, int k1,
+                                      TreeletWarp& w)
+{
+    const float* rec = nodes + 24 * (size_t)q;
+    const float4 meta = __ldcg(reinterpret_cast<const float4*>(rec + 20));
+    const uint32_t word = __float_as_uint(meta.x);
+    const uint32_t ids[2] = {word >> 2, __float_as_uint(meta.y)};
+    for (int side = 0; side < 2; ++side) {
+        const int k = side ? k1 : k0;
+        const bool internal = (word >> side) & 1u;
+        const uint32_t id = ids[side];
+        if (internal ? id >= n - 1 : id >= n) return false;
+        const float2* sp = reinterpret_cast<const float2*>(rec + 10 * side);
+        for (int j = 0; j < 5; ++j) {
+            const float2 v = __ldcg(sp + j);
+            w.slot[k][2 * j] = v.x;
+            w.slot[k][2 * j + 1] = v.y;
+        }
+        if (internal) {  // an internal child's slot starts with its box
+            for (int a = 0; a < 6; ++a) w.box[k][a] = w.slot[k][a];
+            const uint2 f = __ldcg(info + id);
+            w.size[k] = f.x;
+            w.height[k] = f.y;
+            w.internal_mask |= 1u << k;
+        } else {
+            const float4 lo = leaf_boxes[2 * (size_t)id], hi = leaf_boxes[2 * (size_t)id + 1];
+            w.box[k][0] = lo.x; w.box[k][1] = lo.y; w.box[k][2] = lo.z;
+            w.box[k][3] = hi.x; w.box[k][4] = hi.y; w.box[k][5] = hi.z;
+            w.size[k] = 1;
+            w.height[k] = 0;
+            w.internal_mask &= ~(1u << k);
+        }
+        w.id[k] = id;
+        w.area[k] = half_area(w.box[k]);
+    }
+    return true;
+}
+
+// Restructures the treelet rooted at internal node r, whose subtree is h_before
+// tall; called by the whole warp.
+__device__ void treelet_restructure(float* __restrict__ nodes, const float4* __restrict__ leaf_boxes,
+                                    uint32_t* __restrict__ parents_leaf, uint32_t* __restrict__ parents_internal,
+                                    uint2* __restrict__ info, uint32_t n, uint32_t r, uint32_t h_before,
+                                    const uint16_t* __restrict__ pairs, TreeletWarp& w, uint32_t* __restrict__ status)
+{
+    const int lane = threadIdx.x & 31;
+    __syncwarp();  // every lane is done with the previous treelet's shared state
+    if (lane == 0) {  // formation
+        w.internal_mask = 0;
+        w.inode[0] = r;
+        bool ok = treelet_take_children(nodes, leaf_boxes, info, n, r, 0, 1, w);
+        uint32_t m = 2, ni = 1;
+        float old = 0.f;
+        if (ok) {
+            float rb[6];
+            for (int a = 0; a < 3; ++a) {
+                rb[a] = fminf(w.box[0][a], w.box[1][a]);
+                rb[3 + a] = fmaxf(w.box[0][3 + a], w.box[1][3 + a]);
+            }
+            old = half_area(rb);
+        }
+        while (ok && m < (uint32_t)kTreeletLeaves) {
+            int b = -1;
+            float ba = -1.f;
+            for (uint32_t k = 0; k < m; ++k)
+                if (((w.internal_mask >> k) & 1u) && w.area[k] > ba) { ba = w.area[k]; b = (int)k; }
+            if (b < 0) break;
+            const uint32_t q = w.id[b];
+            w.inode[ni++] = q;
+            old = __fadd_rn(old, w.area[b]);
+            ok = treelet_take_children(nodes, leaf_boxes, info, n, q, b, (int)m, w);
+            ++m;
+        }
+        if (!ok) atomicOr(status, CPT_STATUS_BAD_INDEX);
+        w.m = ok ? m : 0u;
+        w.old_cost = old;
+    }
+    __syncwarp();
+    const uint32_t m = w.m;
+    if (m < 3) return;
+    const uint32_t full = (1u << m) - 1u;
+    for (uint32_t S = (uint32_t)lane + 1u; S <= full; S += 32u) {
+        if (__popc(S) == 1) { w.c[S] = 0.f; continue; }
+        float b[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+#pragma unroll
+        for (int k = 0; k < kTreeletLeaves; ++k)
+            if ((S >> k) & 1u)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    b[a] = fminf(b[a], w.box[k][a]);
+                    b[3 + a] = fmaxf(b[3 + a], w.box[k][3 + a]);
+                }
+        w.c[S] = half_area(b);
+        w.best[S] = ~0ull;
+    }
+    __syncwarp();
+    for (int k = 2; k <= (int)m; ++k) {
+        const int p1 = treelet_class_start(k + 1);
+        for (int t = treelet_class_start(k) + lane; t < p1; t += 32) {
+            const uint32_t e = pairs[t];
+            const uint32_t S = e & 127u, P = e >> 7;
+            if (S & ~full) continue;
+            const float v = __fadd_rn(w.c[P], w.c[S ^ P]);
+            atomicMin(&w.best[S], ((unsigned long long)__float_as_uint(v) << 32) | P);
+        }
+        __syncwarp();
+        for (uint32_t S = (uint32_t)lane + 1u; S <= full; S += 32u)
+            if (__popc(S) == k) {
+                const unsigned long long b = w.best[S];
+                w.c[S] = __fadd_rn(w.c[S], __uint_as_float((uint32_t)(b >> 32)));
+                w.split[S] = (uint8_t)(b & 127u);
+            }
+        __syncwarp();
+    }
+    if (lane == 0 && w.c[full] < __fmul_rn(w.old_cost, 0.999999f)) {
+        // the new topology, top-down: node j covers subset sub[j]; a child reference
+        // is a treelet leaf k (< 8) or node 8 + j
+        uint32_t sub[kTreeletLeaves - 1], ck[kTreeletLeaves - 1][2];
+        uint32_t cnt = 1;
+        sub[0] = full;
+        bool ok = true;
+        for (uint32_t j = 0; j < cnt && ok; ++j) {
+            const uint32_t S = sub[j], P = w.split[S];
+            const uint32_t X[2] = {P, S ^ P};
+            for (int side = 0; side < 2; ++side) {
+                if (X[side] == 0u || (X[side] & ~S)) { ok = false; break; }
+                if (__popc(X[side]) == 1) {
+                    ck[j][side] = (uint32_t)(__ffs(X[side]) - 1);
+                } else {
+                    if (cnt >= m - 1) { ok = false; break; }
+                    sub[cnt] = X[side];
+                    ck[j][side] = 8u + cnt;
+                    ++cnt;
+                }
+            }
+        }
+        if (!ok || cnt != m - 1) {
+            atomicOr(status, CPT_STATUS_BAD_INDEX);
+        } else {
+            uint32_t h[kTreeletLeaves - 1], sz[kTreeletLeaves - 1];
+            for (int j = (int)cnt - 1; j >= 0; --j) {
+                uint32_t hh = 0, ss = 0;
+                for (int side = 0; side < 2; ++side) {
+                    const uint32_t c = ck[j][side];
+                    hh = max(hh, c < 8u ? w.height[c] : h[c - 8u]);
+                    ss += c < 8u ? w.size[c] : sz[c - 8u];
+                }
+                h[j] = hh + 1u;
+                sz[j] = ss;
+            }
+            if (h[0] <= h_before) {
+                for (uint32_t j = 0; j < cnt; ++j) {
+                    const uint32_t nd = w.inode[j];
+                    float* rec = nodes + 24 * (size_t)nd;
+                    uint32_t ids[2], word = 0;
+                    for (int side = 0; side < 2; ++side) {
+                        const uint32_t c = ck[j][side];
+                        float slot[10];
+                        if (c < 8u) {
+                            ids[side] = w.id[c];
+                            for (int a = 0; a < 10; ++a) slot[a] = w.slot[c][a];
+                            if ((w.internal_mask >> c) & 1u) {
+                                word |= 1u << side;
+                                parents_internal[ids[side]] = nd;
+                            } else {
+                                parents_leaf[ids[side]] = nd;
+                            }
+                        } else {
+                            const uint32_t x = c - 8u, X = sub[x];
+                            ids[side] = w.inode[x];
+                            word |= 1u << side;
+                            for (int a = 0; a < 3; ++a) { slot[a] = FLT_MAX; slot[3 + a] = -FLT_MAX; }
+                            for (uint32_t k = 0; k < m; ++k)
+                                if ((X >> k) & 1u)
+                                    for (int a = 0; a < 3; ++a) {
+                                        slot[a] = fminf(slot[a], w.box[k][a]);
+                                        slot[3 + a] = fmaxf(slot[3 + a], w.box[k][3 + a]);
+                                    }
+                            slot[6] = slot[7] = slot[8] = slot[9] = 0.0f;
+                            parents_internal[ids[side]] = nd;
+                        }
+                        store_slot(rec, side, slot);
+                    }
+                    word |= ids[0] << 2;
+                    reinterpret_cast<float4*>(rec)[5] =
+                        make_float4(__uint_as_float(word), __uint_as_float(ids[1]), 0.f, 0.f);
+                    info[nd] = make_uint2(sz[j], h[j]);
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncwarp();
+}
+
+// One round of treelet restructuring over the split tree: every piece's walker goes
+// up; the second arrival at a node records its size and height and, at gamma or
+// more leaves, has its warp restructure the node's treelet.
+__global__ void __launch_bounds__(kTreeletBlock) k_treelet(const uint32_t* __restrict__ n_pieces,
+                                                          float* __restrict__ nodes,
+                                                          const float4* __restrict__ leaf_boxes,
+                                                          uint32_t* __restrict__ parents_leaf,
+                                                          uint32_t* __restrict__ parents_internal,
+                                                          int* __restrict__ counters, uint2* __restrict__ info,
+                                                          uint32_t gamma, uint32_t* __restrict__ status)
+{
+    // (subset, split) pairs by subset size: a subset S of k >= 2 leaves lists its
+    // 2^(k-1) - 1 splits P (P holds S's lowest leaf, P != S) from
+    // treelet_class_start(k) + rank of S among the k-leaf subsets x (2^(k-1) - 1).
+    __shared__ uint16_t s_pairs[kTreeletPairs];
+    __shared__ TreeletWarp s_warp[kTreeletWarps];
+    if (threadIdx.x < kTreeletSubsets) {
+        const uint32_t S = threadIdx.x;
+        const int k = __popc(S);
+        if (k >= 2) {
+            uint32_t rank = 0;
+            for (uint32_t x = 1; x < S; ++x) rank += __popc(x) == k ? 1u : 0u;
+            const uint32_t np = (1u << (k - 1)) - 1u, low = S & (0u - S), rest = S ^ low;
+            uint16_t* out = s_pairs + treelet_class_start(k) + rank * np;
+            for (uint32_t j = 0; j < np; ++j) {
+                uint32_t P = low, bits = rest, jj = j;
+                while (bits) {
+                    const uint32_t b = bits & (0u - bits);
+                    if (jj & 1u) P |= b;
+                    jj >>= 1;
+                    bits ^= b;
+                }
+                out[j] = (uint16_t)(S | (P << 7));
+            }
+        }
+    }
+    __syncthreads();
+    const uint32_t n = *n_pieces;
+    if (n < 3) return;
+    TreeletWarp& w = s_warp[threadIdx.x >> 5];
+    const uint32_t i = blockIdx.x * kTreeletBlock + threadIdx.x;
+    bool active = i < n;
+    uint32_t node = active ? parents_leaf[i] : CPT_INVALID_INDEX;
+    uint32_t height = 0;
+    for (int level = 0; __any_sync(0xFFFFFFFFu, active); ++level) {
+        bool process = false;
+        if (active) {
+            if (node == CPT_INVALID_INDEX) {
+                active = false;  // passed the root
+            } else if (node >= n - 1 || level >= kTreeletMaxLevels) {
+                atomicOr(status, CPT_STATUS_BAD_INDEX);
+                active = false;
+            } else {
+                const int arrived = arrive_acq_rel(&counters[node]);
+                if (arrived != 1) {
+                    if (arrived != 0) atomicOr(status, CPT_STATUS_BAD_INDEX);
+                    active = false;
+                } else {
+                    const float4 meta = __ldcg(reinterpret_cast<const float4*>(nodes + 24 * (size_t)node + 20));
+                    const uint32_t word = __float_as_uint(meta.x);
+                    const uint32_t ids[2] = {word >> 2, __float_as_uint(meta.y)};
+                    uint32_t size = 0;
+                    bool ok = true;
+                    height = 0;
+                    for (int side = 0; side < 2; ++side) {
+                        if ((word >> side) & 1u) {
+                            if (ids[side] >= n - 1) { ok = false; continue; }
+                            const uint2 f = __ldcg(info + ids[side]);
+                            size += f.x;
+                            height = max(height, f.y);
+                        } else {
+                            if (ids[side] >= n) ok = false;
+                            size += 1u;
+                        }
+                    }
+                    if (!ok) {
+                        atomicOr(status, CPT_STATUS_BAD_INDEX);
+                        active = false;
+                    } else {
+                        height += 1u;
+                        info[node] = make_uint2(size, height);
+                        process = size >= gamma;
+                    }
+                }
+            }
+        }
+        uint32_t todo = __ballot_sync(0xFFFFFFFFu, process);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1u;
+            const uint32_t r = __shfl_sync(0xFFFFFFFFu, node, src);
+            const uint32_t hr = __shfl_sync(0xFFFFFFFFu, height, src);
+            treelet_restructure(nodes, leaf_boxes, parents_leaf, parents_internal, info, n, r, hr, s_pairs, w,
+                                status);
+        }
+        if (active) node = __ldcg(parents_internal + node);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Locally-ordered clustering (PLOC; Meister and Bittner, "Parallel Locally-Ordered
 // Clustering for Bounding Volume Hierarchy Construction", TVCG 2018), as an
 // alternative to the Karras topology for the split BVH. Clusters start as the
@@ -780,6 +1143,7 @@ struct SplitScratch {
     int* counters;
     cpt_bbox* node_boxes;
     float4* leaf_boxes;
+    uint2* info;  // treelet restructuring: per internal node (leaves, height)
     // clustering (CPT_SPLIT_PLOC)
     float4* nbox;
     uint32_t* clusters[2];
@@ -793,7 +1157,7 @@ struct SplitScratch {
 };
 
 template <typename K>
-size_t split_layout(uint32_t n, uint32_t cap, bool ploc, void* base, SplitScratch<K>* out)
+size_t split_layout(uint32_t n, uint32_t cap, bool ploc, bool treelet, void* base, SplitScratch<K>* out)
 {
     constexpr int P = KeyTraits<K>::passes;
     Carver c(base);
@@ -822,6 +1186,7 @@ size_t split_layout(uint32_t n, uint32_t cap, bool ploc, void* base, SplitScratc
         const size_t ptiles = (cap + kScanTile - 1) / kScanTile;
         s.node_boxes = nullptr;
         s.leaf_boxes = nullptr;
+        s.info = nullptr;
         s.nbox = c.take<float4>(4ull * cap);
         s.clusters[0] = c.take<uint32_t>(cap);
         s.clusters[1] = c.take<uint32_t>(cap);
@@ -835,6 +1200,7 @@ size_t split_layout(uint32_t n, uint32_t cap, bool ploc, void* base, SplitScratc
     } else {
         s.node_boxes = c.take<cpt_bbox>(cap);
         s.leaf_boxes = c.take<float4>(2ull * cap);
+        s.info = treelet ? c.take<uint2>(cap) : nullptr;
         s.nbox = nullptr;
         s.clusters[0] = s.clusters[1] = s.nn = s.leaf_tri = s.tile_create = s.tile_keep = nullptr;
         s.kids = nullptr;
@@ -903,12 +1269,13 @@ int ploc_impl(cpt_bvh* bvh, uint32_t cap, const float4* pieces, const uint32_t* 
 }
 
 template <typename K>
-int split_impl(cpt_bvh* bvh, uint32_t cap, bool ploc, void* nodes, void* scratch, cudaStream_t stream)
+int split_impl(cpt_bvh* bvh, uint32_t cap, bool ploc, bool treelet, void* nodes, void* scratch,
+               cudaStream_t stream)
 {
     constexpr int P = KeyTraits<K>::passes;
     const uint32_t n = bvh->n;
     SplitScratch<K> s;
-    split_layout<K>(n, cap, ploc, scratch, &s);
+    split_layout<K>(n, cap, ploc, treelet, scratch, &s);
     const uint32_t ctiles = (n + kScanTile - 1) / kScanTile;
     const double extra = (double)(cap - n);
     CPT_CUDA_TRY(cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * P * kRadix, stream));
@@ -963,6 +1330,15 @@ int split_impl(cpt_bvh* bvh, uint32_t cap, bool ploc, void* nodes, void* scratch
                                                           static_cast<float*>(nodes), s.node_boxes, s.leaf_boxes, n,
                                                           bvh->status);
     CPT_LAUNCH_CHECK();
+    if (treelet) {
+        for (int round = 0; round < kTreeletRounds; ++round) {
+            CPT_CUDA_TRY(cudaMemsetAsync(s.counters, 0, sizeof(int) * (size_t)cap, stream));
+            k_treelet<<<(cap + kTreeletBlock - 1) / kTreeletBlock, kTreeletBlock, 0, stream>>>(
+                s.n_pieces, static_cast<float*>(nodes), s.leaf_boxes, s.parents_leaf, s.parents_internal, s.counters,
+                s.info, (uint32_t)kTreeletGamma << round, bvh->status);
+            CPT_LAUNCH_CHECK();
+        }
+    }
     return CPT_OK;
 }
 
@@ -975,12 +1351,13 @@ extern "C" size_t cpt_lbvh_split_bytes(uint32_t n, int morton_bits, float extra_
                                        size_t* node_bytes)
 {
     if (n < 2 || (morton_bits != 30 && morton_bits != 63)) return 0;
-    const bool ploc = flags & CPT_SPLIT_PLOC;
+    const bool ploc = flags & CPT_SPLIT_PLOC, treelet = flags & CPT_SPLIT_TREELET;
+    if ((flags & ~(CPT_SPLIT_PLOC | CPT_SPLIT_TREELET)) || (ploc && treelet)) return 0;
     const uint64_t cap = split_capacity(n, extra_ratio);
     if (cap >= (1ull << 31)) return 0;
     if (node_bytes) *node_bytes = align_up((size_t)(cap - 1) * 96, 256);
-    return morton_bits == 30 ? split_layout<uint32_t>(n, (uint32_t)cap, ploc, nullptr, nullptr)
-                             : split_layout<uint64_t>(n, (uint32_t)cap, ploc, nullptr, nullptr);
+    return morton_bits == 30 ? split_layout<uint32_t>(n, (uint32_t)cap, ploc, treelet, nullptr, nullptr)
+                             : split_layout<uint64_t>(n, (uint32_t)cap, ploc, treelet, nullptr, nullptr);
 }
 
 extern "C" int cpt_lbvh_split(cpt_bvh* bvh, float extra_ratio, uint32_t flags, void* nodes, size_t node_bytes,
@@ -995,9 +1372,9 @@ extern "C" int cpt_lbvh_split(cpt_bvh* bvh, float extra_ratio, uint32_t flags, v
     if ((reinterpret_cast<uintptr_t>(nodes) & 15) || (reinterpret_cast<uintptr_t>(scratch) & 255))
         return CPT_ERR_INVALID_ARGUMENT;
     const uint32_t cap = (uint32_t)split_capacity(bvh->n, extra_ratio);
-    const bool ploc = flags & CPT_SPLIT_PLOC;
-    const int rc = bvh->morton_bits == 30 ? split_impl<uint32_t>(bvh, cap, ploc, nodes, scratch, stream)
-                                          : split_impl<uint64_t>(bvh, cap, ploc, nodes, scratch, stream);
+    const bool ploc = flags & CPT_SPLIT_PLOC, treelet = flags & CPT_SPLIT_TREELET;
+    const int rc = bvh->morton_bits == 30 ? split_impl<uint32_t>(bvh, cap, ploc, treelet, nodes, scratch, stream)
+                                          : split_impl<uint64_t>(bvh, cap, ploc, treelet, nodes, scratch, stream);
     if (rc) return rc;
     bvh->split_nodes = nodes;
     bvh->split_capacity = cap;

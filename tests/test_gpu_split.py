@@ -50,7 +50,7 @@ def tie_or_equal(h_split, h_ref, ulps=1):
 
 @pytest.mark.parametrize("bits", [30, 63])
 @pytest.mark.parametrize("ratio", [0.5, 2.0])
-@pytest.mark.parametrize("flags", [0, cpt.SPLIT_PLOC])
+@pytest.mark.parametrize("flags", [0, cpt.SPLIT_PLOC, cpt.SPLIT_TREELET])
 def test_split_hits_match_oracle(cuda, bits, ratio, flags):
     tris, _ = hairball()
     lb = DeviceLbvh(len(tris), bits)
@@ -79,14 +79,14 @@ def test_split_hits_match_oracle(cuda, bits, ratio, flags):
     assert np.array_equal(a_split.cpu().numpy()[:, 0] < 3e38, a_base.cpu().numpy()[:, 0] < 3e38)
     # fewer visits on the hairball; reference-format outputs untouched
     v_split, v_base = split_stats.cpu().numpy()[:, 0].mean(), base_stats.cpu().numpy()[:, 0].mean()
-    if flags == 0:  # (the clustered tree's visit counts depend on the scene; parity is what is tested)
+    if flags != cpt.SPLIT_PLOC:  # (the clustered tree's visit counts depend on the scene; parity is what is tested)
         assert v_split < (0.95 if ratio >= 2.0 else 1.0) * v_base, (v_split, v_base)
     after = lb.download()
     for k in ("tris", "keys", "children", "parents_leaf", "parents_internal", "node_boxes", "nodes"):
         assert after[k].tobytes() == before[k].tobytes(), k
 
 
-@pytest.mark.parametrize("flags", [0, cpt.SPLIT_PLOC])
+@pytest.mark.parametrize("flags", [0, cpt.SPLIT_PLOC, cpt.SPLIT_TREELET])
 def test_split_render_matches_plain(cuda, flags):
     tris, infos = hairball(n_hair=30_000)
     cam = cpt.camera_look_at((0.0, 0.35, -3.6), (0.0, 0.0, 0.0), aspect=64 / 48)
@@ -111,7 +111,7 @@ def test_split_render_matches_plain(cuda, flags):
     assert not lb.bvh.split_nodes and lb.bvh.split_capacity == 0
 
 
-@pytest.mark.parametrize("flags", [0, cpt.SPLIT_PLOC])
+@pytest.mark.parametrize("flags", [0, cpt.SPLIT_PLOC, cpt.SPLIT_TREELET])
 def test_split_degenerate_and_zero_budget(cuda, flags):
     # ratio 0: one piece per triangle; a flat scene (zero extent on an axis) where every
     # hit is a near-tie between coplanar triangles
@@ -155,3 +155,97 @@ def test_ploc_on_identical_boxes(cuda):
     lb.status()
     a, b = h1.cpu().numpy(), h0.cpu().numpy()
     assert np.array_equal(a[:, 0], b[:, 0])  # same t; any of the identical triangles may be reported
+
+
+def split_tree(lb):
+    """Walks the split tree's 96-B records from the root, level by level: returns the
+    reached internal node indices, the leaf triangles (with multiplicity), the height,
+    the summed half surface area of the internal child boxes, and whether every
+    internal child's box lies inside its parent's and every leaf triangle's box meets
+    its parent's."""
+    raw = lb.split_nodes.cpu().numpy()
+    rec = raw[: (raw.size // 96) * 96].view(np.float32).reshape(-1, 24)
+    words = rec[:, 20].view(np.uint32)
+    right = rec[:, 21].view(np.uint32)
+    frontier = np.array([0], np.int64)
+    pbox = np.array([[-np.inf] * 3 + [np.inf] * 3], np.float32)
+    reached, leaves, height, area, contained = [], [], 0, 0.0, True
+    while frontier.size:
+        reached.append(frontier)
+        height += 1
+        w = words[frontier]
+        nxt, nbox = [], []
+        for side in (0, 1):
+            internal = ((w >> side) & 1).astype(bool)
+            idx = (w >> 2) if side == 0 else right[frontier]
+            slot = rec[frontier, 10 * side:10 * side + 10]
+            b = slot[internal, :6]
+            pb = pbox[internal]
+            contained &= bool(np.all(b[:, :3] >= pb[:, :3]) and np.all(b[:, 3:] <= pb[:, 3:]))
+            ext = b[:, 3:].astype(np.float64) - b[:, :3]
+            area += float((ext[:, 0] * ext[:, 1] + ext[:, 1] * ext[:, 2] + ext[:, 2] * ext[:, 0]).sum())
+            nxt.append(idx[internal].astype(np.int64))
+            nbox.append(b)
+            lf = slot[~internal]
+            v0 = lf[:, 0:3]
+            tri = np.stack([v0, v0 + lf[:, 4:7], v0 + lf[:, 7:10]], 1)
+            lo, hi, pl = tri.min(1), tri.max(1), pbox[~internal]
+            contained &= bool(np.all(lo <= pl[:, 3:] + 1e-6) and np.all(hi >= pl[:, :3] - 1e-6))
+            leaves.append(lf[:, 3].view(np.uint32))
+        frontier = np.concatenate(nxt)
+        pbox = np.concatenate(nbox) if frontier.size else pbox[:0]
+    return np.concatenate(reached), np.sort(np.concatenate(leaves)), height, area, contained
+
+
+@pytest.mark.parametrize("bits,ratio", [(63, 1.0), (30, 0.0)])
+def test_treelet_tree_structure(cuda, bits, ratio):
+    # restructuring keeps every piece exactly once, every node reachable once, boxes
+    # nested, never a taller tree, and lowers the summed node surface area; and its
+    # result does not depend on timing (two builds are byte-identical)
+    tris, _ = hairball(n_hair=20_000)
+    lb = DeviceLbvh(len(tris), bits)
+    lb.build(to_device(tris), check_root=True)
+    lb.split(ratio)
+    torch.cuda.synchronize()
+    lb.status()
+    r0, l0, h0, a0, c0 = split_tree(lb)
+    lb.split(ratio, flags=cpt.SPLIT_TREELET)
+    torch.cuda.synchronize()
+    lb.status()
+    raw1 = lb.split_nodes.cpu().numpy().copy()
+    r1, l1, h1, a1, c1 = split_tree(lb)
+    assert c0 and c1
+    assert np.array_equal(l0, l1)
+    assert r1.size == l1.size - 1 and np.unique(r1).size == r1.size
+    assert np.array_equal(np.sort(r1), np.arange(r1.size))
+    assert h1 <= h0
+    assert a1 < 0.99 * a0, (a1, a0)
+    lb.split(ratio, flags=cpt.SPLIT_TREELET)
+    torch.cuda.synchronize()
+    raw2 = lb.split_nodes.cpu().numpy()
+    used = r1.size * 96
+    assert raw2[:used].tobytes() == raw1[:used].tobytes()
+
+
+def test_treelet_flag_checks(cuda):
+    tris, _ = hairball(n_hair=2_000, nu=16, nv=8)
+    lb = DeviceLbvh(len(tris), 30)
+    lb.build(to_device(tris))
+    with pytest.raises(ValueError):
+        lb.split(1.0, flags=cpt.SPLIT_TREELET | cpt.SPLIT_PLOC)
+    with pytest.raises(ValueError):
+        lb.split(1.0, flags=8)
+    # two and three triangles: no treelet of 3 leaves or fewer to improve; hits still match
+    for count in (2, 3):
+        small = tris[:count].copy()
+        lb2 = DeviceLbvh(count, 30)
+        lb2.build(to_device(small))
+        rays = random_rays(2000, 7)
+        d_rays = torch.from_numpy(rays).cuda()
+        h0, _ = lb2.trace(d_rays)
+        lb2.split(2.0, flags=cpt.SPLIT_TREELET)
+        h1, _ = lb2.trace(d_rays)
+        torch.cuda.synchronize()
+        lb2.status()
+        ok, _ = tie_or_equal(h1.cpu().numpy(), h0.cpu().numpy())
+        assert ok.all()

@@ -25,13 +25,13 @@ def trace_pair(lb, d_rays):
 
 
 @pytest.mark.parametrize("bits", [30, 63])
-@pytest.mark.parametrize("split", [0.0, 1.25])
-def test_wide_hits_match_binary(cuda, bits, split):
+@pytest.mark.parametrize("split,flags", [(0.0, 0), (1.25, 0), (1.25, cpt.SPLIT_TREELET)])
+def test_wide_hits_match_binary(cuda, bits, split, flags):
     tris, _ = hairball()
     lb = DeviceLbvh(len(tris), bits)
     lb.build(to_device(tris), check_root=True)
     if split:
-        lb.split(split)
+        lb.split(split, flags=flags)
     rays = np.concatenate([random_rays(20_000, 1), random_rays(10_000, 2, inside=True)])
     d_rays = torch.from_numpy(rays).cuda()
     hb, sb, ab = trace_pair(lb, d_rays)
@@ -193,13 +193,14 @@ def test_wide_far_camera_finds_every_closest_hit(cuda, distance):
 
 
 @pytest.mark.parametrize("distance", [3.0, 1000.0])
-def test_split_far_camera_finds_every_closest_hit(cuda, distance):
+@pytest.mark.parametrize("flags", [0, cpt.SPLIT_TREELET])
+def test_split_far_camera_finds_every_closest_hit(cuda, distance, flags):
     """The same far-camera check for the binary split tree (pieces of long triangles,
-    fused slab test)."""
+    fused slab test), with the Karras and the treelet-restructured topology."""
     tris, _ = hairball(n_hair=8000, nu=32, nv=16, seed=6)
     lb = DeviceLbvh(len(tris), 63)
     lb.build(to_device(tris))
-    lb.split(2.0)
+    lb.split(2.0, flags=flags)
     g = np.random.default_rng(22)
     m = 1000
     d0 = g.normal(size=(m, 3))
