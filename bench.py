@@ -34,7 +34,7 @@ sys.path.insert(0, os.path.join(ROOT, "cuda-path-tracer_b200"))
 
 WORKLOADS = {
     "c2": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
-               bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, split=4.0, wide=1),
+               bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, split=8.0, wide=1, treelet=1),
     "c1": dict(kind="random", n=65536, bits=30, width=512, height=512, spp=1, bounces=3, eye=(0.5, 0.5, -1.2),
                target=(0.5, 0.5, 0.0), seed=0),
     # 64 scenes, 10k-2M triangles (log-uniform, alternating generators), 256^2-1024^2, one graph launch per frame

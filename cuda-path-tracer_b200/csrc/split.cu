@@ -26,7 +26,7 @@
 //                         digit histograms, zeroed look-back state
 //   k_scan_offsets, k_onesweep x P, k_topology   as the main build, on the device count
 //   k_split_refit         leaf slots + bottom-up boxes into the 96-B traversal nodes
-//   k_treelet x 3         (CPT_SPLIT_TREELET) treelet restructuring of the Karras topology
+//   k_treelet             (CPT_SPLIT_TREELET) treelet restructuring of the Karras topology
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -496,16 +496,28 @@ __global__ void __launch_bounds__(kSplitRefitBlock) k_split_refit(const cpt_tria
 // nodes (the treelet root keeps its index, box and parent). The result does not
 // depend on timing: a treelet sees only its finished subtree, areas and sums are
 // rounded without contraction, and equal costs go to the smallest split mask.
-// Rounds with gamma = 7, 14, 28. Since no treelet grows taller, the tree is never
-// taller than the Karras tree it starts from.
+// One round with gamma = 4 (treelets of 4 to 6 leaves where a subtree has fewer
+// than 7): on the C2 scene more rounds (gamma doubling) lower the binary tree's cost
+// a little further but raise the node visits of the 8-wide tree collapsed from it.
+// Since no treelet grows taller, the tree is never taller than the Karras tree it
+// starts from.
 // ---------------------------------------------------------------------------
 constexpr int kTreeletBlock = 128;
 constexpr int kTreeletWarps = kTreeletBlock / 32;
 constexpr int kTreeletLeaves = 7;
 constexpr int kTreeletSubsets = 1 << kTreeletLeaves;
 constexpr int kTreeletPairs = 966;  // sum over k = 2..7 of C(7, k) (2^(k-1) - 1)
-constexpr int kTreeletRounds = 3;
-constexpr int kTreeletGamma = 7;
+#ifndef CPT_TREELET_ROUNDS
+#define CPT_TREELET_ROUNDS 1
+#endif
+#ifndef CPT_TREELET_GAMMA
+#define CPT_TREELET_GAMMA 4
+#endif
+#ifndef CPT_TREELET_GAMMA_SHIFT
+#define CPT_TREELET_GAMMA_SHIFT 1  // gamma doubles every round
+#endif
+constexpr int kTreeletRounds = CPT_TREELET_ROUNDS;
+constexpr int kTreeletGamma = CPT_TREELET_GAMMA;
 constexpr int kTreeletMaxLevels = 1024;
 
 // Index of the first (subset, split) pair of the subsets of k leaves (k = 2..7;
@@ -743,7 +755,7 @@ __device__ void treelet_restructure(float* __restrict__ nodes, const float4* __r
     __syncwarp();
 }
 
-// One round of treelet restructuring over the split tree: every piece's walker goes
+// A round of treelet restructuring over the split tree: every piece's walker goes
 // up; the second arrival at a node records its size and height and, at gamma or
 // more leaves, has its warp restructure the node's treelet.
 __global__ void __launch_bounds__(kTreeletBlock) k_treelet(const uint32_t* __restrict__ n_pieces,
@@ -1335,7 +1347,7 @@ int split_impl(cpt_bvh* bvh, uint32_t cap, bool ploc, bool treelet, void* nodes,
             CPT_CUDA_TRY(cudaMemsetAsync(s.counters, 0, sizeof(int) * (size_t)cap, stream));
             k_treelet<<<(cap + kTreeletBlock - 1) / kTreeletBlock, kTreeletBlock, 0, stream>>>(
                 s.n_pieces, static_cast<float*>(nodes), s.leaf_boxes, s.parents_leaf, s.parents_internal, s.counters,
-                s.info, (uint32_t)kTreeletGamma << round, bvh->status);
+                s.info, (uint32_t)kTreeletGamma << (CPT_TREELET_GAMMA_SHIFT * round), bvh->status);
             CPT_LAUNCH_CHECK();
         }
     }

@@ -143,9 +143,9 @@ int cpt_lbvh_build_static(const cpt_triangle* tris_in, uint32_t n, const float* 
  * Sets bvh->split_nodes = nodes and bvh->split_capacity. node_bytes / scratch bytes
  * from cpt_lbvh_split_bytes (0 on bad arguments); scratch is free after the stream
  * passes the call. */
-#define CPT_SPLIT_TREELET 2u /* treelet restructuring of the Karras topology (7-leaf treelets, least total
-                               * node surface area, never taller; Karras and Aila 2013 — the optimisation the
-                               * reference's README cites): fewer node visits, longer build. Not with PLOC */
+#define CPT_SPLIT_TREELET 2u /* treelet restructuring of the Karras topology (treelets of up to 7 leaves, least
+                               * total node surface area, never taller; Karras and Aila 2013 — the optimisation
+                               * the reference's README cites): fewer node visits, longer build. Not with PLOC */
 #define CPT_SPLIT_PLOC 1u /* pieces clustered by surface area (locally-ordered clustering, search radius 16
                              * in Morton order) instead of the Karras topology: fewer node visits, longer build */
 size_t cpt_lbvh_split_bytes(uint32_t n, int morton_bits, float extra_ratio, uint32_t flags, size_t* node_bytes);
