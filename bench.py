@@ -34,7 +34,9 @@ sys.path.insert(0, os.path.join(ROOT, "cuda-path-tracer_b200"))
 
 WORKLOADS = {
     "c2": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
-               bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, split=8.0, wide=1, treelet=1),
+               bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, split=8.0, wide=1, treelet=1,
+               # every e2e step rebuilds the trees inside its timed region: there the cheaper build wins
+               e2e_split=4.0, e2e_treelet=0),
     "c1": dict(kind="random", n=65536, bits=30, width=512, height=512, spp=1, bounces=3, eye=(0.5, 0.5, -1.2),
                target=(0.5, 0.5, 0.0), seed=0),
     # 64 scenes, 10k-2M triangles (log-uniform, alternating generators), 256^2-1024^2, one graph launch per frame
@@ -724,7 +726,9 @@ def run_ours(args, w, world, rank, local):
     e2e = None
     if not args.no_e2e and not deforming:
         tr = cpt.Tracer(w["bits"])
-        tr.set_split(split)
+        e2e_split = w.get("e2e_split", split) if args.split is None else split
+        e2e_treelet = w.get("e2e_treelet", args.treelet) if args.treelet_given is None else args.treelet
+        tr.set_split(e2e_split, cpt.SPLIT_TREELET if e2e_treelet and e2e_split > 0 else 0)
         tr.set_wide(bool(args.wide))
         tr.set_settings(bounces=w["bounces"], intensity=3.0, stratified=True, seed=w["seed"] + 7919 * rank)
         # (the tracer object renders frame 0 of its own seed on every rank: e2e ranks are replicas)
@@ -765,7 +769,9 @@ def run_ours(args, w, world, rank, local):
                "h2d_bytes_per_step": int(tris.nbytes + infos.nbytes), "d2h_bytes_per_step": int(W_ * H_ * 16),
                "ms_per_step": round(e_ms_max / ne, 3), "wall_ms_per_step": round(1e3 * wall / ne, 3),
                "steps": ne, "includes": "H2D soup+shading records (pinned), LBVH build"
-                                        + (f", split BVH build (extra {split})" if split > 0 else "")
+                                        + (f", split BVH build (extra {e2e_split}"
+                                           + (", treelet-restructured" if e2e_treelet else ", Karras topology")
+                                           + ")" if e2e_split > 0 else "")
                                         + (", wide tree build" if args.wide else "")
                                         + ", 16-spp frame, D2H image"}
         tr.close()
@@ -1015,6 +1021,7 @@ def main():
     w = dict(WORKLOADS[args.workload])
     if args.wide is None:
         args.wide = int(w.get("wide", 0))
+    args.treelet_given = args.treelet
     if args.treelet is None:
         args.treelet = int(w.get("treelet", 0))
     if args.res:

@@ -542,26 +542,30 @@ __device__ __forceinline__ float half_area(const float* b)
     return __fadd_rn(__fadd_rn(__fmul_rn(dx, dy), __fmul_rn(dy, dz)), __fmul_rn(dz, dx));
 }
 
-struct TreeletWarp {
-    unsigned long long best[kTreeletSubsets];  // (cost bits << 32) | split mask, reduced by atomicMin
-    float c[kTreeletSubsets];                  // least cost over a subset (its area until its size class)
+// A treelet as formed: its leaves and internal nodes.
+struct TreeletForm {
     float box[kTreeletLeaves][6];
-    float slot[kTreeletLeaves][10];            // the leaf's 40-B child slot as its parent held it
-    float area[kTreeletLeaves];
-    uint32_t id[kTreeletLeaves];               // internal node index, or piece position for a leaf
+    uint32_t id[kTreeletLeaves];      // internal node index, or piece position for a leaf
     uint32_t height[kTreeletLeaves];
     uint32_t size[kTreeletLeaves];
-    uint32_t inode[kTreeletLeaves - 1];        // the treelet's internal nodes, [0] = its root
-    uint32_t internal_mask;                    // bit k: treelet leaf k is an internal node
-    uint32_t m;                                // treelet leaves (0: bad index met)
-    float old_cost;
+    uint32_t from[kTreeletLeaves];    // parent * 2 + side: the record slot holding the leaf
+    uint32_t inode[kTreeletLeaves - 1];  // the treelet's internal nodes, [0] = its root
+    uint32_t internal_mask;           // bit k: treelet leaf k is an internal node
+    uint32_t m;                       // treelet leaves (0: bad index met)
+    float old_cost;                   // summed area of the treelet's internal nodes
+};
+
+struct TreeletWarp {
+    TreeletForm form;
+    float c[kTreeletSubsets];         // least cost over a subset (its area until its size class is done)
+    float slot[kTreeletLeaves][10];   // the leaves' 40-B child slots, read before any rewrite
     uint8_t split[kTreeletSubsets];
 };
 
 // Treelet leaves k0 and k1 := the two children of internal node q. False on an out-of-range index.
 __device__ bool treelet_take_children(const float* __restrict__ nodes, const float4* __restrict__ leaf_boxes,
                                       const uint2* __restrict__ info, uint32_t n, uint32_t q, int k0, int k1,
-                                      TreeletWarp& w)
+                                      TreeletForm& f)
 {
     const float* rec = nodes + 24 * (size_t)q;
     const float4 meta = __ldcg(reinterpret_cast<const float4*>(rec + 20));
@@ -572,75 +576,90 @@ __device__ bool treelet_take_children(const float* __restrict__ nodes, const flo
         const bool internal = (word >> side) & 1u;
         const uint32_t id = ids[side];
         if (internal ? id >= n - 1 : id >= n) return false;
-        const float2* sp = reinterpret_cast<const float2*>(rec + 10 * side);
-        for (int j = 0; j < 5; ++j) {
-            const float2 v = __ldcg(sp + j);
-            w.slot[k][2 * j] = v.x;
-            w.slot[k][2 * j + 1] = v.y;
-        }
         if (internal) {  // an internal child's slot starts with its box
-            for (int a = 0; a < 6; ++a) w.box[k][a] = w.slot[k][a];
-            const uint2 f = __ldcg(info + id);
-            w.size[k] = f.x;
-            w.height[k] = f.y;
-            w.internal_mask |= 1u << k;
+            const float2* sp = reinterpret_cast<const float2*>(rec + 10 * side);
+            const float2 a = __ldcg(sp), b = __ldcg(sp + 1), c = __ldcg(sp + 2);
+            f.box[k][0] = a.x; f.box[k][1] = a.y; f.box[k][2] = b.x;
+            f.box[k][3] = b.y; f.box[k][4] = c.x; f.box[k][5] = c.y;
+            const uint2 g = __ldcg(info + id);
+            f.size[k] = g.x;
+            f.height[k] = g.y;
+            f.internal_mask |= 1u << k;
         } else {
             const float4 lo = leaf_boxes[2 * (size_t)id], hi = leaf_boxes[2 * (size_t)id + 1];
-            w.box[k][0] = lo.x; w.box[k][1] = lo.y; w.box[k][2] = lo.z;
-            w.box[k][3] = hi.x; w.box[k][4] = hi.y; w.box[k][5] = hi.z;
-            w.size[k] = 1;
-            w.height[k] = 0;
-            w.internal_mask &= ~(1u << k);
+            f.box[k][0] = lo.x; f.box[k][1] = lo.y; f.box[k][2] = lo.z;
+            f.box[k][3] = hi.x; f.box[k][4] = hi.y; f.box[k][5] = hi.z;
+            f.size[k] = 1;
+            f.height[k] = 0;
+            f.internal_mask &= ~(1u << k);
         }
-        w.id[k] = id;
-        w.area[k] = half_area(w.box[k]);
+        f.id[k] = id;
+        f.from[k] = 2u * q + (uint32_t)side;
     }
     return true;
 }
 
-// Restructures the treelet rooted at internal node r, whose subtree is h_before
-// tall; called by the whole warp.
-__device__ void treelet_restructure(float* __restrict__ nodes, const float4* __restrict__ leaf_boxes,
-                                    uint32_t* __restrict__ parents_leaf, uint32_t* __restrict__ parents_internal,
-                                    uint2* __restrict__ info, uint32_t n, uint32_t r, uint32_t h_before,
-                                    const uint16_t* __restrict__ pairs, TreeletWarp& w, uint32_t* __restrict__ status)
+// Forms the treelet rooted at internal node r (one lane).
+__device__ void treelet_form(const float* __restrict__ nodes, const float4* __restrict__ leaf_boxes,
+                             const uint2* __restrict__ info, uint32_t n, uint32_t r, TreeletForm& f,
+                             uint32_t* __restrict__ status)
+{
+    f.internal_mask = 0;
+    f.inode[0] = r;
+    bool ok = treelet_take_children(nodes, leaf_boxes, info, n, r, 0, 1, f);
+    uint32_t m = 2, ni = 1;
+    float old = 0.f;
+    if (ok) {
+        float rb[6];
+        for (int a = 0; a < 3; ++a) {
+            rb[a] = fminf(f.box[0][a], f.box[1][a]);
+            rb[3 + a] = fmaxf(f.box[0][3 + a], f.box[1][3 + a]);
+        }
+        old = half_area(rb);
+    }
+    while (ok && m < (uint32_t)kTreeletLeaves) {
+        int b = -1;
+        float ba = -1.f;
+        for (uint32_t k = 0; k < m; ++k)
+            if ((f.internal_mask >> k) & 1u) {
+                const float a = half_area(f.box[k]);
+                if (a > ba) { ba = a; b = (int)k; }
+            }
+        if (b < 0) break;
+        f.inode[ni++] = f.id[b];
+        old = __fadd_rn(old, ba);
+        ok = treelet_take_children(nodes, leaf_boxes, info, n, f.id[b], b, (int)m, f);
+        ++m;
+    }
+    if (!ok) atomicOr(status, CPT_STATUS_BAD_INDEX);
+    f.m = ok ? m : 0u;
+    f.old_cost = old;
+}
+
+// Solves the warp's formed treelet (rooted at a node whose subtree is h_before tall)
+// and rewrites it if cheaper and no taller; called by the whole warp.
+__device__ void treelet_solve(float* __restrict__ nodes, uint32_t* __restrict__ parents_leaf,
+                              uint32_t* __restrict__ parents_internal, uint2* __restrict__ info,
+                              uint32_t h_before, const uint16_t* __restrict__ pairs, TreeletWarp& w)
 {
     const int lane = threadIdx.x & 31;
-    __syncwarp();  // every lane is done with the previous treelet's shared state
-    if (lane == 0) {  // formation
-        w.internal_mask = 0;
-        w.inode[0] = r;
-        bool ok = treelet_take_children(nodes, leaf_boxes, info, n, r, 0, 1, w);
-        uint32_t m = 2, ni = 1;
-        float old = 0.f;
-        if (ok) {
-            float rb[6];
-            for (int a = 0; a < 3; ++a) {
-                rb[a] = fminf(w.box[0][a], w.box[1][a]);
-                rb[3 + a] = fmaxf(w.box[0][3 + a], w.box[1][3 + a]);
-            }
-            old = half_area(rb);
-        }
-        while (ok && m < (uint32_t)kTreeletLeaves) {
-            int b = -1;
-            float ba = -1.f;
-            for (uint32_t k = 0; k < m; ++k)
-                if (((w.internal_mask >> k) & 1u) && w.area[k] > ba) { ba = w.area[k]; b = (int)k; }
-            if (b < 0) break;
-            const uint32_t q = w.id[b];
-            w.inode[ni++] = q;
-            old = __fadd_rn(old, w.area[b]);
-            ok = treelet_take_children(nodes, leaf_boxes, info, n, q, b, (int)m, w);
-            ++m;
-        }
-        if (!ok) atomicOr(status, CPT_STATUS_BAD_INDEX);
-        w.m = ok ? m : 0u;
-        w.old_cost = old;
+    __syncwarp();  // the form is written
+    const TreeletForm& f = w.form;
+    const uint32_t m = f.m;
+    if (m < 3) {
+        __syncwarp();  // every lane has read m before the next form is written
+        return;
     }
-    __syncwarp();
-    const uint32_t m = w.m;
-    if (m < 3) return;
     const uint32_t full = (1u << m) - 1u;
+    if ((uint32_t)lane < m) {
+        const uint32_t from = f.from[lane];
+        const float2* sp = reinterpret_cast<const float2*>(nodes + 24 * (size_t)(from >> 1) + 10 * (from & 1u));
+        for (int j = 0; j < 5; ++j) {
+            const float2 v = __ldcg(sp + j);
+            w.slot[lane][2 * j] = v.x;
+            w.slot[lane][2 * j + 1] = v.y;
+        }
+    }
     for (uint32_t S = (uint32_t)lane + 1u; S <= full; S += 32u) {
         if (__popc(S) == 1) { w.c[S] = 0.f; continue; }
         float b[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
@@ -649,32 +668,47 @@ __device__ void treelet_restructure(float* __restrict__ nodes, const float4* __r
             if ((S >> k) & 1u)
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {
-                    b[a] = fminf(b[a], w.box[k][a]);
-                    b[3 + a] = fmaxf(b[3 + a], w.box[k][3 + a]);
+                    b[a] = fminf(b[a], f.box[k][a]);
+                    b[3 + a] = fmaxf(b[3 + a], f.box[k][3 + a]);
                 }
         w.c[S] = half_area(b);
-        w.best[S] = ~0ull;
     }
     __syncwarp();
+    // size class k: C(7, k) subsets of 2^(k-1) - 1 splits each; a lane takes a subset,
+    // or (k = 6, 7) a group of g lanes shares a subset's splits and reduces by shuffles.
+    // The least (cost bits, split mask) wins.
     for (int k = 2; k <= (int)m; ++k) {
-        const int p1 = treelet_class_start(k + 1);
-        for (int t = treelet_class_start(k) + lane; t < p1; t += 32) {
-            const uint32_t e = pairs[t];
-            const uint32_t S = e & 127u, P = e >> 7;
-            if (S & ~full) continue;
-            const float v = __fadd_rn(w.c[P], w.c[S ^ P]);
-            atomicMin(&w.best[S], ((unsigned long long)__float_as_uint(v) << 32) | P);
+        const int subsets = k == 2 ? 21 : k == 3 ? 35 : k == 4 ? 35 : k == 5 ? 21 : k == 6 ? 7 : 1;
+        const int g = k == 6 ? 4 : k == 7 ? 32 : 1;
+        const int np = (1 << (k - 1)) - 1;
+        const uint16_t* cls = pairs + treelet_class_start(k);
+        for (int i0 = 0; i0 < subsets * g; i0 += 32) {
+            const int idx = i0 + lane, rho = idx / g, q = idx % g;
+            unsigned long long key = ~0ull;
+            uint32_t S = 0;
+            if (rho < subsets) {
+                const uint16_t* ps = cls + rho * np;
+                S = ps[0] & 127u;
+                if (!(S & ~full))
+                    for (int j = q; j < np; j += g) {
+                        const uint32_t P = (uint32_t)ps[j] >> 7;
+                        const float v = __fadd_rn(w.c[P], w.c[S ^ P]);
+                        const unsigned long long kk = ((unsigned long long)__float_as_uint(v) << 32) | P;
+                        key = kk < key ? kk : key;
+                    }
+            }
+            for (int o = 1; o < g; o <<= 1) {
+                const unsigned long long other = __shfl_xor_sync(0xFFFFFFFFu, key, o);
+                key = other < key ? other : key;
+            }
+            if (rho < subsets && q == 0 && !(S & ~full)) {
+                w.c[S] = __fadd_rn(w.c[S], __uint_as_float((uint32_t)(key >> 32)));
+                w.split[S] = (uint8_t)(key & 127u);
+            }
         }
         __syncwarp();
-        for (uint32_t S = (uint32_t)lane + 1u; S <= full; S += 32u)
-            if (__popc(S) == k) {
-                const unsigned long long b = w.best[S];
-                w.c[S] = __fadd_rn(w.c[S], __uint_as_float((uint32_t)(b >> 32)));
-                w.split[S] = (uint8_t)(b & 127u);
-            }
-        __syncwarp();
     }
-    if (lane == 0 && w.c[full] < __fmul_rn(w.old_cost, 0.999999f)) {
+    if (lane == 0 && w.c[full] < __fmul_rn(f.old_cost, 0.999999f)) {
         // the new topology, top-down: node j covers subset sub[j]; a child reference
         // is a treelet leaf k (< 8) or node 8 + j
         uint32_t sub[kTreeletLeaves - 1], ck[kTreeletLeaves - 1][2];
@@ -696,32 +730,30 @@ __device__ void treelet_restructure(float* __restrict__ nodes, const float4* __r
                 }
             }
         }
-        if (!ok || cnt != m - 1) {
-            atomicOr(status, CPT_STATUS_BAD_INDEX);
-        } else {
+        if (ok && cnt == m - 1) {
             uint32_t h[kTreeletLeaves - 1], sz[kTreeletLeaves - 1];
             for (int j = (int)cnt - 1; j >= 0; --j) {
                 uint32_t hh = 0, ss = 0;
                 for (int side = 0; side < 2; ++side) {
                     const uint32_t c = ck[j][side];
-                    hh = max(hh, c < 8u ? w.height[c] : h[c - 8u]);
-                    ss += c < 8u ? w.size[c] : sz[c - 8u];
+                    hh = max(hh, c < 8u ? f.height[c] : h[c - 8u]);
+                    ss += c < 8u ? f.size[c] : sz[c - 8u];
                 }
                 h[j] = hh + 1u;
                 sz[j] = ss;
             }
             if (h[0] <= h_before) {
                 for (uint32_t j = 0; j < cnt; ++j) {
-                    const uint32_t nd = w.inode[j];
+                    const uint32_t nd = f.inode[j];
                     float* rec = nodes + 24 * (size_t)nd;
                     uint32_t ids[2], word = 0;
                     for (int side = 0; side < 2; ++side) {
                         const uint32_t c = ck[j][side];
                         float slot[10];
                         if (c < 8u) {
-                            ids[side] = w.id[c];
+                            ids[side] = f.id[c];
                             for (int a = 0; a < 10; ++a) slot[a] = w.slot[c][a];
-                            if ((w.internal_mask >> c) & 1u) {
+                            if ((f.internal_mask >> c) & 1u) {
                                 word |= 1u << side;
                                 parents_internal[ids[side]] = nd;
                             } else {
@@ -729,14 +761,14 @@ __device__ void treelet_restructure(float* __restrict__ nodes, const float4* __r
                             }
                         } else {
                             const uint32_t x = c - 8u, X = sub[x];
-                            ids[side] = w.inode[x];
+                            ids[side] = f.inode[x];
                             word |= 1u << side;
                             for (int a = 0; a < 3; ++a) { slot[a] = FLT_MAX; slot[3 + a] = -FLT_MAX; }
                             for (uint32_t k = 0; k < m; ++k)
                                 if ((X >> k) & 1u)
                                     for (int a = 0; a < 3; ++a) {
-                                        slot[a] = fminf(slot[a], w.box[k][a]);
-                                        slot[3 + a] = fmaxf(slot[3 + a], w.box[k][3 + a]);
+                                        slot[a] = fminf(slot[a], f.box[k][a]);
+                                        slot[3 + a] = fmaxf(slot[3 + a], f.box[k][3 + a]);
                                     }
                             slot[6] = slot[7] = slot[8] = slot[9] = 0.0f;
                             parents_internal[ids[side]] = nd;
@@ -757,7 +789,7 @@ __device__ void treelet_restructure(float* __restrict__ nodes, const float4* __r
 
 // A round of treelet restructuring over the split tree: every piece's walker goes
 // up; the second arrival at a node records its size and height and, at gamma or
-// more leaves, has its warp restructure the node's treelet.
+// more leaves, has its warp form and solve the node's treelet.
 __global__ void __launch_bounds__(kTreeletBlock) k_treelet(const uint32_t* __restrict__ n_pieces,
                                                           float* __restrict__ nodes,
                                                           const float4* __restrict__ leaf_boxes,
@@ -794,6 +826,7 @@ __global__ void __launch_bounds__(kTreeletBlock) k_treelet(const uint32_t* __res
     __syncthreads();
     const uint32_t n = *n_pieces;
     if (n < 3) return;
+    const int lane = threadIdx.x & 31;
     TreeletWarp& w = s_warp[threadIdx.x >> 5];
     const uint32_t i = blockIdx.x * kTreeletBlock + threadIdx.x;
     bool active = i < n;
@@ -822,9 +855,9 @@ __global__ void __launch_bounds__(kTreeletBlock) k_treelet(const uint32_t* __res
                     for (int side = 0; side < 2; ++side) {
                         if ((word >> side) & 1u) {
                             if (ids[side] >= n - 1) { ok = false; continue; }
-                            const uint2 f = __ldcg(info + ids[side]);
-                            size += f.x;
-                            height = max(height, f.y);
+                            const uint2 g = __ldcg(info + ids[side]);
+                            size += g.x;
+                            height = max(height, g.y);
                         } else {
                             if (ids[side] >= n) ok = false;
                             size += 1u;
@@ -847,8 +880,8 @@ __global__ void __launch_bounds__(kTreeletBlock) k_treelet(const uint32_t* __res
             todo &= todo - 1u;
             const uint32_t r = __shfl_sync(0xFFFFFFFFu, node, src);
             const uint32_t hr = __shfl_sync(0xFFFFFFFFu, height, src);
-            treelet_restructure(nodes, leaf_boxes, parents_leaf, parents_internal, info, n, r, hr, s_pairs, w,
-                                status);
+            if (lane == 0) treelet_form(nodes, leaf_boxes, info, n, r, w.form, status);
+            treelet_solve(nodes, parents_leaf, parents_internal, info, hr, s_pairs, w);
         }
         if (active) node = __ldcg(parents_internal + node);
     }
