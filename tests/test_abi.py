@@ -81,6 +81,28 @@ def test_build_rejects_bad_arguments_without_device_work():
     assert e.value.code == cpt.ERR_INVALID_ARGUMENT
 
 
+@pytest.mark.parametrize("bits", [30, 63])
+def test_split_sizes_and_flags(bits):
+    # split tree sizing (host-only): records for the pieces, scratch per piece, 8 B more
+    # per piece with treelet restructuring; unknown flags and PLOC + treelets refused
+    def sizes(n, ratio, flags):
+        nb = ctypes.c_size_t()
+        sb = cpt.lib.cpt_lbvh_split_bytes(n, bits, ctypes.c_float(ratio), flags, ctypes.byref(nb))
+        return int(sb), nb.value
+
+    n = 100_000
+    for ratio in (0.0, 1.0, 8.0):
+        cap = n + int(np.floor(ratio * n))
+        s0, nb0 = sizes(n, ratio, 0)
+        s1, nb1 = sizes(n, ratio, cpt.SPLIT_TREELET)
+        sp, nbp = sizes(n, ratio, cpt.SPLIT_PLOC)
+        assert nb0 == nb1 == nbp >= (cap - 1) * 96
+        assert s0 > 0 and s1 - s0 >= 8 * cap and sp > 0
+    assert sizes(n, 1.0, cpt.SPLIT_TREELET | cpt.SPLIT_PLOC)[0] == 0
+    assert sizes(n, 1.0, 4)[0] == 0
+    assert sizes(1, 1.0, 0)[0] == 0
+
+
 def test_render_sizes_and_rejections():
     from cpt import RenderParams
     p = RenderParams(64, 48, 4, 0, 3, 3.0, 1, 0, 0, cpt.ACCUM_KAHAN, 0, 0)
