@@ -77,7 +77,8 @@ def make_cameras(w):
 
 
 def workload_config(name, w, n_tris, l2_note):
-    desc = {"c2": "fBm sphere 2048x1024x2 + 1M hairball + quad light",
+    hair = f'{w["n_hair"] >> 20}M' if w.get("n_hair", 0) and w["n_hair"] % (1 << 20) == 0 else str(w.get("n_hair"))
+    desc = {"c2": f'fBm sphere {w.get("nu")}x{w.get("nv")}x2 + {hair} hairball + quad light',
             "c4": "fBm sphere 2048x1024x2 + 1M hairball + quad light, radiance cache (96-64x4-16 BF16 MLP, 2^16 "
                   "training paths per frame, Adam 1e-2) vs plain path tracing",
             "c1": "65,536 random triangles + quad light",
@@ -1003,6 +1004,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--res", default=None, help="override resolution WxH (profiling runs)")
     ap.add_argument("--spp", type=int, default=None, help="override samples per frame (profiling runs)")
+    ap.add_argument("--sphere", default=None, help="override the sphere's grid NUxNV (profiling runs)")
+    ap.add_argument("--hair", type=int, default=None, help="override the hairball's triangle count (profiling runs)")
     ap.add_argument("--wave-paths", type=int, default=0, help="paths per wave (0: library default)")
     ap.add_argument("--ray-sort", type=int, default=0, help="1: coherence-sort bounce queues")
     ap.add_argument("--wide", type=int, default=None,
@@ -1028,6 +1031,10 @@ def main():
         w["width"], w["height"] = (int(x) for x in args.res.lower().split("x"))
     if args.spp:
         w["spp"] = args.spp
+    if args.sphere:
+        w["nu"], w["nv"] = (int(x) for x in args.sphere.lower().split("x"))
+    if args.hair is not None:
+        w["n_hair"] = args.hair
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))
