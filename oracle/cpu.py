@@ -58,6 +58,8 @@ def oracle_lib() -> ctypes.CDLL:
         L.orc_emitters.argtypes = [P, U, P, U, U, P]
         L.orc_emitters.restype = U
         L.orc_set_nee.argtypes = [P]
+        L.orc_treelet.argtypes = [P, U, P, U]
+        L.orc_treelet.restype = I
         _oracle = L
     return _oracle
 
@@ -118,6 +120,42 @@ def build(tris: np.ndarray, bits: int, box=None, use_ref: bool = False) -> Build
     if rc != 0:
         raise ValueError(f"build rejected its input (rc {rc})")
     return r
+
+
+def treelet(records: np.ndarray, n: int, leaf_boxes: np.ndarray, gamma: int = 4) -> np.ndarray:
+    """One round of the split tree's treelet restructuring (cpt_treelet.c) over a copy
+    of the 96-B records ((n - 1) x 24 float32); leaf_boxes: (n, 6) lo xyz, hi xyz."""
+    out = np.ascontiguousarray(records, np.float32).reshape(-1, 24)[: n - 1].copy()
+    lb = np.ascontiguousarray(leaf_boxes, np.float32).reshape(n, 6)
+    if oracle_lib().orc_treelet(_p(out), n, _p(lb), gamma) != 0:
+        raise ValueError("treelet restructuring met a malformed tree")
+    return out
+
+
+def records_of(b: BuildResult) -> tuple[np.ndarray, np.ndarray]:
+    """The LBVH as 96-B traversal records (internal child slot: its box; leaf child slot:
+    v0, the leaf index, v1 - v0, v2 - v0; the Node word; right = left + 1) and the
+    leaves' triangle boxes."""
+    n = b.tris.size
+    v0, v1, v2 = (b.tris[k].astype(np.float32) for k in ("v0", "v1", "v2"))
+    leaf_boxes = np.concatenate([np.minimum(np.minimum(v0, v1), v2), np.maximum(np.maximum(v0, v1), v2)], 1)
+    boxes = np.concatenate([b.node_boxes["min"], b.node_boxes["max"]], 1).astype(np.float32)
+    rec = np.zeros((n - 1, 24), np.float32)
+    words = b.children
+    for side in (0, 1):
+        idx = (words >> 2) + side
+        internal = ((words >> side) & 1).astype(bool)
+        slot = np.zeros((n - 1, 10), np.float32)
+        slot[internal, :6] = boxes[idx[internal]]
+        li = idx[~internal]
+        slot[~internal, 0:3] = v0[li]
+        slot[~internal, 3] = li.astype(np.uint32).view(np.float32)
+        slot[~internal, 4:7] = v1[li] - v0[li]
+        slot[~internal, 7:10] = v2[li] - v0[li]
+        rec[:, 10 * side:10 * side + 10] = slot
+    rec[:, 20] = words.view(np.float32)
+    rec[:, 21] = ((words >> 2) + 1).astype(np.uint32).view(np.float32)
+    return rec, leaf_boxes
 
 
 def trace(b: BuildResult, rays: np.ndarray, any_hit: bool = False, use_ref: bool = False, stats: bool = False,

@@ -249,3 +249,38 @@ def test_treelet_flag_checks(cuda):
         lb2.status()
         ok, _ = tie_or_equal(h1.cpu().numpy(), h0.cpu().numpy())
         assert ok.all()
+
+
+@pytest.mark.parametrize("bits", [30, 63])
+def test_treelet_matches_oracle(cuda, bits):
+    # one piece per triangle (ratio 0): the leaves' boxes are their triangles' boxes, so
+    # the oracle's restatement (oracle/cpt_treelet.c) can restructure the GPU's Karras
+    # split tree and must reproduce the GPU's restructured records: the same words, and
+    # the same box and triangle floats (as values: the sign of a zero may differ)
+    tris, _ = hairball(n_hair=20_000)
+    n = len(tris)
+    lb = DeviceLbvh(n, bits)
+    lb.build(to_device(tris), check_root=True)
+    lb.split(0.0)
+    torch.cuda.synchronize()
+    lb.status()
+    rec0 = lb.split_nodes.cpu().numpy()[: (n - 1) * 96].view(np.float32).reshape(n - 1, 24).copy()
+    lb.split(0.0, flags=cpt.SPLIT_TREELET)
+    torch.cuda.synchronize()
+    lb.status()
+    rec1 = lb.split_nodes.cpu().numpy()[: (n - 1) * 96].view(np.float32).reshape(n - 1, 24).copy()
+    srt = lb.download()["tris"]
+    lo = np.minimum(np.minimum(srt["v0"], srt["v1"]), srt["v2"])
+    hi = np.maximum(np.maximum(srt["v0"], srt["v1"]), srt["v2"])
+    words, right = rec0[:, 20].view(np.uint32), rec0[:, 21].view(np.uint32)
+    leaf_boxes = np.full((n, 6), np.nan, np.float32)
+    for side in (0, 1):
+        leaf = ((words >> side) & 1) == 0
+        ids = ((words >> 2) if side == 0 else right)[leaf]
+        tri = rec0[leaf, 10 * side + 3].view(np.uint32)
+        leaf_boxes[ids] = np.concatenate([lo[tri], hi[tri]], 1)
+    assert not np.isnan(leaf_boxes).any()
+    want = cpu.treelet(rec0, n, leaf_boxes, 4)
+    assert (want.view(np.uint32) != rec0.view(np.uint32)).any()  # the restructuring changed something
+    assert np.array_equal(rec1[:, 20:24].view(np.uint32), want[:, 20:24].view(np.uint32))
+    assert np.array_equal(rec1[:, :20], want[:, :20])
