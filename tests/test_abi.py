@@ -81,6 +81,22 @@ def test_build_rejects_bad_arguments_without_device_work():
     assert e.value.code == cpt.ERR_INVALID_ARGUMENT
 
 
+def test_static_build_limits_without_device_work():
+    # the no-allocation build: its fixed scratch covers every accepted size for both key
+    # widths; sizes above the limit, n < 2 and bad key widths are refused on the host
+    # before the library looks for a device
+    max_n, scratch = 131072, 8 << 20
+    for bits in (30, 63):
+        assert cpt.lbvh_scratch_bytes(max_n, bits) <= scratch
+        assert cpt.lbvh_scratch_bytes(2, bits) <= scratch
+    b = cpt.bvh_bind(1 << 20, cpt.bvh_bytes(100, 30), 100, 30)
+    call = cpt.lib.cpt_lbvh_build_static
+    for n in (max_n + 1, 1 << 24, 0xFFFFFFFF):
+        assert call(256, n, None, 30, ctypes.byref(b), 0, None) == cpt.ERR_SCRATCH_TOO_SMALL
+    for n, bits in ((0, 30), (1, 63), (100, 31), (100, 64)):
+        assert call(256, n, None, bits, ctypes.byref(b), 0, None) == cpt.ERR_INVALID_ARGUMENT
+
+
 @pytest.mark.parametrize("bits", [30, 63])
 def test_split_sizes_and_flags(bits):
     # split tree sizing (host-only): records for the pieces, scratch per piece, 8 B more
