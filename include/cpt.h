@@ -317,7 +317,14 @@ int cpt_bvh_heatmap(const cpt_bvh* bvh, const cpt_camera* camera, uint32_t width
 /* ---- reference-facing tracer object (host buffers in, image out) ----
  * Mirrors CUDAPathTracer (source/application/cuda/cuda_path_tracer.h:13-40):
  * upload a HostSceneDescription, set primary rays and eye, raytrace frame by
- * frame, reset. Owns its device memory and stream. */
+ * frame, reset. Owns its device memory and stream.
+ * Device: the tracer belongs to the device current at cpt_tracer_create and does not
+ * switch devices itself; make that device current before each call on it (one tracer
+ * per GPU, as the reference's single-device application has one).
+ * Host buffers: cpt_tracer_upload copies asynchronously. Pageable host memory may be
+ * reused when the call returns. Page-locked (pinned) memory — which lets the copies
+ * overlap the builds — must stay unchanged until the copies have run: until the next
+ * cpt_tracer_read_image or cpt_tracer_ray_counts returns after a cpt_tracer_raytrace. */
 typedef struct cpt_tracer cpt_tracer;
 int cpt_tracer_create(cpt_tracer** out, int morton_bits);
 void cpt_tracer_destroy(cpt_tracer* t);
