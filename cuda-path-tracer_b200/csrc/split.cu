@@ -1395,7 +1395,8 @@ using namespace cpt;
 extern "C" size_t cpt_lbvh_split_bytes(uint32_t n, int morton_bits, float extra_ratio, uint32_t flags,
                                        size_t* node_bytes)
 {
-    if (n < 2 || (morton_bits != 30 && morton_bits != 63)) return 0;
+    if (n < 2 || n > kMaxTriangles || (morton_bits != 30 && morton_bits != 63)) return 0;
+    if (!(extra_ratio >= 0.f) || !(extra_ratio <= 64.f)) return 0;  // the range cpt_lbvh_split accepts
     const bool ploc = flags & CPT_SPLIT_PLOC, treelet = flags & CPT_SPLIT_TREELET;
     if ((flags & ~(CPT_SPLIT_PLOC | CPT_SPLIT_TREELET)) || (ploc && treelet)) return 0;
     const uint64_t cap = split_capacity(n, extra_ratio);

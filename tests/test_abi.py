@@ -117,6 +117,10 @@ def test_split_sizes_and_flags(bits):
     assert sizes(n, 1.0, cpt.SPLIT_TREELET | cpt.SPLIT_PLOC)[0] == 0
     assert sizes(n, 1.0, 4)[0] == 0
     assert sizes(1, 1.0, 0)[0] == 0
+    # ratios cpt_lbvh_split refuses get no size either (0..64, not NaN or infinite)
+    assert sizes(n, 64.0, 0)[0] > 0
+    for ratio in (64.5, -0.5, float("nan"), float("inf")):
+        assert sizes(n, ratio, 0)[0] == 0, ratio
 
 
 def test_render_sizes_and_rejections():
