@@ -320,16 +320,18 @@ def sincos_turns(u: np.ndarray):
 
 
 # ---------------------------------------------------------------- accumulators (numpy float32 = IEEE per op)
-def accumulate_kahan(samples: np.ndarray):
-    """samples (spp, ..., 3) in sample order -> (sum, comp, count) as the device's Kahan accumulator."""
-    s = np.zeros(samples.shape[1:], np.float32)
-    c = np.zeros(samples.shape[1:], np.float32)
+def accumulate_kahan(samples: np.ndarray, init=None):
+    """samples (spp, ..., 3) in sample order -> (sum, comp, count) as the device's Kahan accumulator;
+    init: a (sum, comp, count) to continue from."""
+    if init is None:
+        init = (np.zeros(samples.shape[1:], np.float32), np.zeros(samples.shape[1:], np.float32), 0)
+    s, c = np.array(init[0], np.float32), np.array(init[1], np.float32)
     for x in samples:
         y = (x - c).astype(np.float32)
         t = (s + y).astype(np.float32)
         c = ((t - s).astype(np.float32) - y).astype(np.float32)
         s = t
-    return s, c, np.float32(len(samples))
+    return s, c, np.float32(init[2] + len(samples))
 
 
 def accumulate_lerp(samples: np.ndarray, frame0: int, prev=None):

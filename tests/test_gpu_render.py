@@ -282,3 +282,32 @@ def test_graph_replay_advances_the_sample_stream(cuda):
     torch.cuda.synchronize()
     assert int(counter.item()) == 4
     assert graphed.accum.cpu().numpy().tobytes() == direct.accum.cpu().numpy().tobytes()
+
+
+def test_checkpoint_resume_matches_one_accumulation(cuda, tmp_path):
+    """Frames [0, 2) rendered, saved to a file (cpt/progress.py), loaded into a fresh
+    renderer's accumulator and frames [2, 4) rendered there: the same accumulator bytes
+    as both calls on one accumulator."""
+    from cpt import progress
+
+    tris, infos, _, cam = scene(n=8000)
+    lb = DeviceLbvh(len(tris), 30)
+    lb.build(to_device(tris), check_root=True)
+    sc = DeviceScene(infos)
+    p = make_params(W, H, 2, 0, 3, 3.0, True, 3, cpt.ACCUM_KAHAN)
+    direct = DeviceRenderer(p)
+    direct.render(lb, sc, cam, frame0=0)
+    direct.render(lb, sc, cam, frame0=2)
+    first = DeviceRenderer(p)
+    first.render(lb, sc, cam, frame0=0)
+    torch.cuda.synchronize()
+    path = str(tmp_path / "progress.npz")
+    progress.save(path, first.accum, p, next_frame=2)
+    second = DeviceRenderer(p)
+    frame0 = progress.resume(second, path)
+    assert frame0 == 2
+    second.render(lb, sc, cam, frame0=frame0)
+    torch.cuda.synchronize()
+    direct.check_status()
+    second.check_status()
+    assert second.accum.cpu().numpy().tobytes() == direct.accum.cpu().numpy().tobytes()
