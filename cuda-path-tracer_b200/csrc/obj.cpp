@@ -10,7 +10,10 @@
 //     not supported by this library's shader (indices stay CPT_INVALID_INDEX).
 // The reference imports through assimp (a Windows binary here); this parser follows
 // the OBJ format itself: polygons are fanned (v0, vk, vk+1), negative indices count
-// back from the last vertex, trailing comments are ignored.
+// back from the last vertex, trailing comments are ignored, lines may be of any
+// length, and an `mtllib` line may name several files. A face index (position, uv or
+// normal) of 0 or outside the elements read so far makes the call fail with
+// CPT_ERR_INVALID_ARGUMENT, as a missing file does.
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -30,14 +33,27 @@ struct Mtl {
     float ns = 0.f;
 };
 
-constexpr int kAbsent = -2147483647 - 1;  // no uv / normal index on this face vertex
-
-struct FaceVert { int v = 0, t = kAbsent, n = kAbsent; };
+struct FaceVert {
+    int v = 0, t = -1, n = -1;        // 0-based after resolve(); t, n = -1: not given
+    bool has_t = false, has_n = false;
+};
 
 std::string dir_of(const std::string& p)
 {
     const size_t k = p.find_last_of('/');
     return k == std::string::npos ? std::string() : p.substr(0, k + 1);
+}
+
+// Next line of f without its terminator; false at the end of the file.
+bool read_line(FILE* f, std::string& line)
+{
+    line.clear();
+    char buf[4096];
+    while (fgets(buf, sizeof(buf), f)) {
+        line += buf;
+        if (!line.empty() && line.back() == '\n') return true;
+    }
+    return !line.empty();
 }
 
 std::string strip_comment(const std::string& s)
@@ -50,10 +66,9 @@ void load_mtl(const std::string& path, std::map<std::string, Mtl>& out)
 {
     FILE* f = fopen(path.c_str(), "r");
     if (!f) return;
-    char buf[4096];
-    std::string cur;
-    while (fgets(buf, sizeof(buf), f)) {
-        std::istringstream ss(strip_comment(buf));
+    std::string line, cur;
+    while (read_line(f, line)) {
+        std::istringstream ss(strip_comment(line));
         std::string tag;
         if (!(ss >> tag)) continue;
         if (tag == "newmtl") { ss >> cur; out[cur] = Mtl(); }
@@ -88,9 +103,9 @@ extern "C" int cpt_obj_load(const char* path, float scale, const float* translat
     const std::string base = dir_of(path);
     uint32_t n = 0;
     int rc = CPT_OK;
-    char buf[8192];
-    while (fgets(buf, sizeof(buf), f)) {
-        std::istringstream ss(strip_comment(buf));
+    std::string line;
+    while (read_line(f, line)) {
+        std::istringstream ss(strip_comment(line));
         std::string tag;
         if (!(ss >> tag)) continue;
         if (tag == "v") {
@@ -112,8 +127,7 @@ extern "C" int cpt_obj_load(const char* path, float scale, const float* translat
             nrm.push_back(x); nrm.push_back(y); nrm.push_back(z);
         } else if (tag == "mtllib") {
             std::string name;
-            ss >> name;
-            load_mtl(base + name, mtls);
+            while (ss >> name) load_mtl(base + name, mtls);
         } else if (tag == "usemtl") {
             std::string name;
             ss >> name;
@@ -126,19 +140,19 @@ extern "C" int cpt_obj_load(const char* path, float scale, const float* translat
             while (ss >> tok) {
                 FaceVert v;
                 int a = 0, b = 0, c = 0;
-                if (sscanf(tok.c_str(), "%d/%d/%d", &a, &b, &c) == 3) { v.v = a; v.t = b; v.n = c; }
-                else if (sscanf(tok.c_str(), "%d//%d", &a, &c) == 2) { v.v = a; v.n = c; }
-                else if (sscanf(tok.c_str(), "%d/%d", &a, &b) == 2) { v.v = a; v.t = b; }
-                else if (sscanf(tok.c_str(), "%d", &a) == 1) { v.v = a; }
-                else continue;
-                v.v = resolve(v.v, pos.size() / 3);
-                v.t = v.t == kAbsent ? -1 : resolve(v.t, uvs.size() / 2);
-                v.n = v.n == kAbsent ? -1 : resolve(v.n, nrm.size() / 3);
-                if ((v.t >= 0 && (size_t)v.t >= uvs.size() / 2) || (v.n >= 0 && (size_t)v.n >= nrm.size() / 3)) {
+                if (sscanf(tok.c_str(), "%d/%d/%d", &a, &b, &c) == 3) { v.has_t = v.has_n = true; }
+                else if (sscanf(tok.c_str(), "%d//%d", &a, &c) == 2) { v.has_n = true; }
+                else if (sscanf(tok.c_str(), "%d/%d", &a, &b) == 2) { v.has_t = true; }
+                else if (sscanf(tok.c_str(), "%d", &a) != 1) continue;
+                v.v = resolve(a, pos.size() / 3);
+                if (v.has_t) v.t = resolve(b, uvs.size() / 2);
+                if (v.has_n) v.n = resolve(c, nrm.size() / 3);
+                if (v.v < 0 || (size_t)v.v >= pos.size() / 3 ||
+                    (v.has_t && (v.t < 0 || (size_t)v.t >= uvs.size() / 2)) ||
+                    (v.has_n && (v.n < 0 || (size_t)v.n >= nrm.size() / 3))) {
                     rc = CPT_ERR_INVALID_ARGUMENT;
                     break;
                 }
-                if (v.v < 0 || (size_t)v.v >= pos.size() / 3) { rc = CPT_ERR_INVALID_ARGUMENT; break; }
                 fv.push_back(v);
             }
             if (rc != CPT_OK) break;

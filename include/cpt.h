@@ -383,7 +383,9 @@ uint32_t cpt_scene_sphere_hairball(uint32_t nu, uint32_t nv, float amp, uint32_t
  * (translate nullable), vertex colours or the material's Kd (default_grey without a
  * material), normals from the file or the triangle's geometric normal, Ke as
  * emission, Ns as specularity. With tris == NULL only counts: *n_out = triangles.
- * Returns CPT_ERR_SCRATCH_TOO_SMALL when capacity is below the count. Host memory. */
+ * Returns CPT_ERR_SCRATCH_TOO_SMALL when capacity is below the count, and
+ * CPT_ERR_INVALID_ARGUMENT for a missing file or a face whose position, uv or normal
+ * index is 0 or outside the elements read so far. Host memory. */
 int cpt_obj_load(const char* path, float scale, const float* translate, float default_grey, cpt_triangle* tris,
                  cpt_triangle_info* infos, uint32_t capacity, uint32_t* n_out);
 /* Deforming-mesh workload (device memory): out = rest with every vertex moved

@@ -74,3 +74,52 @@ def test_reference_fixture_meshes():
     tris, infos = cpt.load_obj(os.path.join(REF_MESHES, "cornell-box", "CornellBox-Original.obj"), scale=5.0)
     assert len(tris) == 36
     assert (infos["material"]["emission"].sum(1) > 0).sum() == 2
+
+
+def _write(tmp_path, name, text):
+    p = tmp_path / name
+    p.write_text(text)
+    return str(p)
+
+
+def _count(path):
+    import ctypes
+
+    n = ctypes.c_uint32()
+    rc = cpt.lib.cpt_obj_load(path.encode(), 1.0, None, 0.7, None, None, 0, ctypes.byref(n))
+    return rc, n.value
+
+
+def test_invalid_uv_and_normal_indices_are_errors(tmp_path):
+    head = "v 0 0 0\nv 1 0 0\nv 0 1 0\nvt 0 0\nvn 0 0 1\n"
+    assert _count(_write(tmp_path, "ok.obj", head + "f 1/1/1 2/1/1 3/-1/-1\n")) == (cpt.OK, 1)
+    for face in ("f 1/0/1 2/1/1 3/1/1",      # uv index 0
+                 "f 1/2/1 2/1/1 3/1/1",      # uv index past the uvs read
+                 "f 1/1/-2 2/1/1 3/1/1",     # negative normal index before the first normal
+                 "f 1//5 2//1 3//1",         # normal index past the normals read
+                 "f 1/-2147483648/1 2/1/1 3/1/1",
+                 "f 0 2 3", "f 1 2 4", "f -4 2 3"):
+        assert _count(_write(tmp_path, "bad.obj", head + face + "\n"))[0] == cpt.ERR_INVALID_ARGUMENT, face
+
+
+def test_long_lines_keep_every_vertex(tmp_path):
+    # a 3000-gon on one line (about 14 KB): fanned into 2998 triangles, none dropped
+    k = 3000
+    ang = np.arange(k) * (2 * np.pi / k)
+    verts = "".join(f"v {np.cos(a):.6f} {np.sin(a):.6f} 0\n" for a in ang)
+    face = "f " + " ".join(str(i + 1) for i in range(k)) + "\n"
+    assert len(face) > 8192
+    tris, _ = cpt.load_obj(_write(tmp_path, "ngon.obj", verts + face + "v 0 0 1\nf 1 2 3001\n"))
+    assert len(tris) == k - 2 + 1
+    assert np.allclose(tris[-2]["v2"], (np.cos(ang[-1]), np.sin(ang[-1]), 0), atol=1e-6)
+    assert np.allclose(tris[-1]["v2"], (0, 0, 1))
+
+
+def test_several_material_libraries_on_one_line(tmp_path):
+    _write(tmp_path, "a.mtl", "newmtl red\nKd 1 0 0\n")
+    _write(tmp_path, "b.mtl", "newmtl lamp\nKd 1 1 1\nKe 5 5 5\n")
+    obj = _write(tmp_path, "two.obj", "mtllib a.mtl b.mtl\nv 0 0 0\nv 1 0 0\nv 0 1 0\n"
+                                      "usemtl red\nf 1 2 3\nusemtl lamp\nf 1 3 2\n")
+    tris, infos = cpt.load_obj(obj)
+    assert np.allclose(infos["vertices"]["color"][0], (1, 0, 0))
+    assert np.allclose(infos["material"]["emission"][1], (5, 5, 5))
