@@ -3,10 +3,21 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
+#include <nvtx3/nvToolsExt.h>
 #include <atomic>
 #include "cpt.h"
 
 namespace cpt {
+
+// An NVTX range named after the entry point, open for the call's host-side duration,
+// so that profilers (Nsight Systems, Nsight Compute's --nvtx filters) group the kernels
+// a call launches under it. Without a profiler attached NVTX calls do nothing.
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
+};
 
 // Count of kernel launches issued by this library (reported by cpt_launch_count).
 extern std::atomic<unsigned long long> g_launches;
@@ -60,6 +71,7 @@ constexpr uint32_t kMaxTriangles = (1u << 30) - 1;  // 30-bit node indices (Node
 #define CPT_PROF_CAT2(a, b) a##b
 #define CPT_PROF_CAT(a, b) CPT_PROF_CAT2(a, b)
 #define CPT_PROF(id, stream) ::cpt::ProfScope CPT_PROF_CAT(prof_scope_, __LINE__)((id), (stream))
+#define CPT_RANGE(name) ::cpt::Range CPT_PROF_CAT(nvtx_range_, __LINE__)(name)
 
 #define CPT_LAUNCH_CHECK()                                          \
     do {                                                            \

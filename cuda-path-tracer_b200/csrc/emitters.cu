@@ -226,6 +226,7 @@ extern "C" size_t cpt_emitters_bytes(uint32_t n, uint32_t max_emitters)
 extern "C" int cpt_emitters_build(const cpt_bvh* bvh, const cpt_scene* scene, uint32_t max_emitters, void* table,
                                   size_t table_bytes, uint32_t* count_out, cudaStream_t stream)
 {
+    CPT_RANGE("cpt_emitters_build");
     if (!bvh || !scene || !table || !bvh->tris || bvh->n == 0 || !scene->infos) return CPT_ERR_INVALID_ARGUMENT;
     if (reinterpret_cast<uintptr_t>(table) & 255) return CPT_ERR_INVALID_ARGUMENT;
     if (table_bytes < cpt_emitters_bytes(bvh->n, max_emitters)) return CPT_ERR_SCRATCH_TOO_SMALL;

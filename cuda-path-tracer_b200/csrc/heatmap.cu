@@ -65,6 +65,7 @@ using namespace cpt;
 extern "C" int cpt_bvh_heatmap(const cpt_bvh* bvh, const cpt_camera* camera, uint32_t width, uint32_t height,
                                const float base_color[3], float* rgba, uint32_t* node_counts, cudaStream_t stream)
 {
+    CPT_RANGE("cpt_bvh_heatmap");
     if (!bvh || !bvh->nodes || !camera || !base_color || !rgba || width == 0 || height == 0) return CPT_ERR_INVALID_ARGUMENT;
     if ((uint64_t)width * height >= (1ull << 31) || (reinterpret_cast<uintptr_t>(rgba) & 15)) return CPT_ERR_INVALID_ARGUMENT;
     HeatCam hc;
@@ -107,6 +108,7 @@ __global__ void __launch_bounds__(256) k_deform(const float* __restrict__ rest, 
 extern "C" int cpt_scene_deform(const cpt_triangle* rest, cpt_triangle* out, uint32_t n, float amplitude, float omega,
                                 float phase, cudaStream_t stream)
 {
+    CPT_RANGE("cpt_scene_deform");
     if (!rest || !out || n == 0) return CPT_ERR_INVALID_ARGUMENT;
     k_deform<<<(n + 255) / 256, 256, 0, stream>>>(reinterpret_cast<const float*>(rest), reinterpret_cast<float*>(out), n,
                                                    amplitude, omega, phase);

@@ -531,6 +531,7 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
                                  uint32_t info_count, const cpt_dir_light* lights, uint32_t light_count,
                                  const float* enclosing_box)
 {
+    CPT_RANGE("cpt_tracer_upload");
     if (!t || !tris || !infos || n < 2 || n > kMaxTriangles || info_count == 0 || (light_count && !lights))
         return CPT_ERR_INVALID_ARGUMENT;
     int rc;
@@ -688,6 +689,7 @@ extern "C" int cpt_tracer_set_settings(cpt_tracer* t, uint32_t bounces, float in
 
 extern "C" int cpt_tracer_raytrace(cpt_tracer* t, uint32_t width, uint32_t height, uint32_t spp)
 {
+    CPT_RANGE("cpt_tracer_raytrace");
     if (!t || !t->ready || width == 0 || height == 0 || spp == 0) return CPT_ERR_INVALID_ARGUMENT;
     cpt_render_params p{};
     p.width = width;
@@ -747,6 +749,7 @@ extern "C" uint32_t cpt_tracer_frame(const cpt_tracer* t) { return t ? t->frame 
 
 extern "C" int cpt_tracer_read_image(cpt_tracer* t, float* rgba_host)
 {
+    CPT_RANGE("cpt_tracer_read_image");
     if (!t || !rgba_host || !t->d_accum || !t->width) return CPT_ERR_INVALID_ARGUMENT;
     int rc;
     const size_t bytes = sizeof(float) * 4 * (size_t)t->width * t->height;

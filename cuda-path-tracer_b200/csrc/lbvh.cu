@@ -479,6 +479,7 @@ extern "C" int cpt_status_check(const uint32_t* d_status, cudaStream_t stream)
 extern "C" int cpt_lbvh_build(const cpt_triangle* tris_in, uint32_t n, const float* enclosing_box, int morton_bits,
                               cpt_bvh* bvh, void* scratch, size_t scratch_bytes, uint32_t flags, cudaStream_t stream)
 {
+    CPT_RANGE("cpt_lbvh_build");
     if (bvh) {  // split and wide trees of the previous build are stale
         bvh->split_nodes = nullptr;
         bvh->split_capacity = 0;

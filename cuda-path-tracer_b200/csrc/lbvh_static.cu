@@ -49,6 +49,7 @@ int scratch_address(void** out)
 extern "C" int cpt_lbvh_build_static(const cpt_triangle* tris_in, uint32_t n, const float* enclosing_box,
                                      int morton_bits, cpt_bvh* bvh, uint32_t flags, cudaStream_t stream)
 {
+    CPT_RANGE("cpt_lbvh_build_static");
     if (n > kStaticMaxTriangles) return CPT_ERR_SCRATCH_TOO_SMALL;
     if (n < 2 || (morton_bits != 30 && morton_bits != 63)) return CPT_ERR_INVALID_ARGUMENT;
     if (cpt_lbvh_scratch_bytes(n, morton_bits) > kStaticScratchBytes) return CPT_ERR_SCRATCH_TOO_SMALL;

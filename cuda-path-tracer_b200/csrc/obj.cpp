@@ -24,6 +24,7 @@
 #include <string>
 #include <vector>
 #include "cpt.h"
+#include "cpt_internal.h"
 
 namespace {
 
@@ -92,6 +93,7 @@ int resolve(int idx, size_t count)
 extern "C" int cpt_obj_load(const char* path, float scale, const float* translate, float default_grey,
                             cpt_triangle* tris, cpt_triangle_info* infos, uint32_t capacity, uint32_t* n_out)
 {
+    CPT_RANGE("cpt_obj_load");
     if (!path || !n_out) return CPT_ERR_INVALID_ARGUMENT;
     FILE* f = fopen(path, "r");
     if (!f) return CPT_ERR_INVALID_ARGUMENT;

@@ -640,6 +640,7 @@ extern "C" int cpt_rc_set_weights(cpt_rc* rc, const float* host_in, cudaStream_t
 extern "C" int cpt_rc_infer(cpt_rc* rc, const float* samples, uint32_t n, const float box[6], float* out,
                             cudaStream_t stream)
 {
+    CPT_RANGE("cpt_rc_infer");
     if (!rc || !box || (n && (!samples || !out))) return CPT_ERR_INVALID_ARGUMENT;
     if (!n) return CPT_OK;
     CPT_CUDA_TRY(cudaMemcpyAsync(rc->box, box, 6 * sizeof(float), cudaMemcpyHostToDevice, stream));
@@ -657,6 +658,7 @@ extern "C" int cpt_rc_infer(cpt_rc* rc, const float* samples, uint32_t n, const 
 extern "C" int cpt_rc_train(cpt_rc* rc, const float* samples, uint32_t n, const float box[6], uint32_t steps,
                             float* loss_out, cudaStream_t stream)
 {
+    CPT_RANGE("cpt_rc_train");
     if (!rc || !box || !samples || n == 0 || steps == 0) return CPT_ERR_INVALID_ARGUMENT;
     CPT_CUDA_TRY(cudaMemcpyAsync(rc->box, box, 6 * sizeof(float), cudaMemcpyHostToDevice, stream));
     CPT_CUDA_TRY(cudaMemsetAsync(rc->loss, 0, 2 * sizeof(float), stream));
@@ -755,6 +757,7 @@ extern "C" int cpt_rc_render(cpt_rc* rc, const cpt_view* views, uint32_t n_views
                              void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
                              cudaStream_t stream)
 {
+    CPT_RANGE("cpt_rc_render");
     return rc_frame(rc, views, n_views, params, scratch, scratch_bytes, ray_counts, status, true, stream);
 }
 
@@ -762,6 +765,7 @@ extern "C" int cpt_rc_update(cpt_rc* rc, const cpt_view* views, uint32_t n_views
                              void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
                              cudaStream_t stream)
 {
+    CPT_RANGE("cpt_rc_update");
     return rc_frame(rc, views, n_views, params, scratch, scratch_bytes, ray_counts, status, false, stream);
 }
 

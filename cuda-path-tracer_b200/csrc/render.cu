@@ -1112,6 +1112,7 @@ extern "C" int cpt_render_views(const cpt_view* views, uint32_t n_views, const c
                                 void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
                                 cudaStream_t stream)
 {
+    CPT_RANGE("cpt_render_views");
     return cpt::cpt_render_views_hooked(views, n_views, params, scratch, scratch_bytes, ray_counts, status, nullptr,
                                         stream);
 }
@@ -1135,6 +1136,7 @@ extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_
                           const cpt_render_params* params, void* accum, void* scratch, size_t scratch_bytes,
                           unsigned long long* ray_counts, uint32_t* status, cudaStream_t stream)
 {
+    CPT_RANGE("cpt_render");
     if (!bvh || !scene || !camera || !accum || !params || params->width == 0 || params->height == 0)
         return CPT_ERR_INVALID_ARGUMENT;
     const uint32_t ncam = camera_count(params);
@@ -1156,6 +1158,7 @@ extern "C" int cpt_render(const cpt_bvh* bvh, const cpt_scene* scene, const cpt_
 extern "C" int cpt_resolve(const void* accum, uint32_t width, uint32_t height, uint32_t accum_mode, float* rgba,
                            cudaStream_t stream)
 {
+    CPT_RANGE("cpt_resolve");
     if (!accum || !rgba || width == 0 || height == 0 || accum_mode > CPT_ACCUM_F64) return CPT_ERR_INVALID_ARGUMENT;
     const uint32_t px = width * height;
     {

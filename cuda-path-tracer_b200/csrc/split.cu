@@ -1409,6 +1409,7 @@ extern "C" size_t cpt_lbvh_split_bytes(uint32_t n, int morton_bits, float extra_
 extern "C" int cpt_lbvh_split(cpt_bvh* bvh, float extra_ratio, uint32_t flags, void* nodes, size_t node_bytes,
                               void* scratch, size_t scratch_bytes, cudaStream_t stream)
 {
+    CPT_RANGE("cpt_lbvh_split");
     if (!bvh || !bvh->tris || !bvh->node_boxes || !bvh->status || !nodes || !scratch) return CPT_ERR_INVALID_ARGUMENT;
     if (!(extra_ratio >= 0.f) || !(extra_ratio <= 64.f)) return CPT_ERR_INVALID_ARGUMENT;
     size_t nb = 0;

@@ -10,6 +10,7 @@
 // RGBA8 array, which is what tex2D reads from the reference's mipmapped arrays.
 extern "C" int cpt_texture_create(const uint8_t* rgba8, uint32_t width, uint32_t height, cudaTextureObject_t* out)
 {
+    CPT_RANGE("cpt_texture_create");
     if (!rgba8 || !out || width == 0 || height == 0) return CPT_ERR_INVALID_ARGUMENT;
     *out = 0;
     const cudaChannelFormatDesc fmt = cudaCreateChannelDesc<uchar4>();

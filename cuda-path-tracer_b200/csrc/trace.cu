@@ -98,6 +98,7 @@ using namespace cpt;
 extern "C" int cpt_trace(const cpt_bvh* bvh, const float* rays, uint32_t n, int any_hit, cpt_hit* hits,
                          uint32_t* stats, cudaStream_t stream)
 {
+    CPT_RANGE("cpt_trace");
     if (!bvh || !bvh->nodes || !bvh->status || (n && (!rays || !hits))) return CPT_ERR_INVALID_ARGUMENT;
     if ((reinterpret_cast<uintptr_t>(rays) & 15) || (reinterpret_cast<uintptr_t>(hits) & 15))
         return CPT_ERR_INVALID_ARGUMENT;

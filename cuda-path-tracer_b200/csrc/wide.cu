@@ -331,6 +331,7 @@ extern "C" size_t cpt_lbvh_wide_bytes(uint32_t leaves, size_t* node_bytes, size_
 extern "C" int cpt_lbvh_wide(cpt_bvh* bvh, void* nodes, size_t node_bytes, void* tris, size_t tri_bytes, void* scratch,
                              size_t scratch_bytes, cudaStream_t stream)
 {
+    CPT_RANGE("cpt_lbvh_wide");
     if (!bvh || !bvh->nodes || !bvh->status || !nodes || !tris || !scratch) return CPT_ERR_INVALID_ARGUMENT;
     const bool split = bvh->split_nodes != nullptr;
     const uint32_t leaves = split ? bvh->split_capacity : bvh->n;
