@@ -163,7 +163,7 @@ typedef struct cpt_hit { float t, u, v; uint32_t tri; } cpt_hit; /* t = FLT_MAX,
  * Replaces CUDA::trace / CUDA::shadowRay (source/application/cuda/trace.h:45-50,73-169).
  * rays: n x 8 floats (origin xyz, unused, direction xyz, unused), device. As in the
  * reference there is no ray interval: a hit counts at any t >= 0, with no far limit
- * (intersection.h:57); the unused words are ignored.
+ * (intersection.h:58); the unused words are ignored.
  * stats (nullable, device): n x 2 uint32 — internal nodes fetched, triangle tests. */
 int cpt_trace(const cpt_bvh* bvh, const float* rays, uint32_t n, int any_hit, cpt_hit* hits, uint32_t* stats,
               cudaStream_t stream);
