@@ -166,6 +166,7 @@ _PROTOS = {
     "cpt_tracer_reset_frames": (None, [_P]),
     "cpt_tracer_frame": (_U32, [_P]),
     "cpt_tracer_read_image": (_I32, [_P, _P]),
+    "cpt_tracer_resolve": (_I32, [_P, _P]),
     "cpt_tracer_ray_counts": (_I32, [_P, _P]),
     "cpt_tracer_stream": (_P, [_P]),
     "cpt_tracer_bvh": (ctypes.POINTER(Bvh), [_P]),
@@ -463,6 +464,10 @@ class Tracer:
             out = np.empty((height, width, 4), np.float32)
         check(lib.cpt_tracer_read_image(self._h, _ptr(out)), "cpt_tracer_read_image")
         return out
+
+    def resolve(self, rgba_dev: int) -> None:
+        """Writes the image into device memory (float4 per pixel) on the tracer's stream."""
+        check(lib.cpt_tracer_resolve(self._h, rgba_dev), "cpt_tracer_resolve")
 
     def ray_counts(self) -> np.ndarray:
         out = np.zeros(3, np.uint64)

@@ -760,6 +760,14 @@ extern "C" int cpt_tracer_read_image(cpt_tracer* t, float* rgba_host)
     return cpt_status_check(t->bvh.status, t->stream);
 }
 
+extern "C" int cpt_tracer_resolve(cpt_tracer* t, float* rgba_dev)
+{
+    CPT_RANGE("cpt_tracer_resolve");
+    if (!t || !rgba_dev || !t->d_accum || !t->width || (reinterpret_cast<uintptr_t>(rgba_dev) & 15))
+        return CPT_ERR_INVALID_ARGUMENT;
+    return cpt_resolve(t->d_accum, t->width, t->height, t->accum_mode, rgba_dev, t->stream);
+}
+
 extern "C" int cpt_tracer_ray_counts(cpt_tracer* t, unsigned long long out[3])
 {
     if (!t || !out) return CPT_ERR_INVALID_ARGUMENT;

@@ -361,6 +361,12 @@ void cpt_tracer_reset_frames(cpt_tracer* t);
 uint32_t cpt_tracer_frame(const cpt_tracer* t);
 /* Copies the resolved image (float4 per pixel) to host memory; synchronizes. */
 int cpt_tracer_read_image(cpt_tracer* t, float* rgba_host);
+/* The same resolved image written to device memory (float4 per pixel, width x height
+ * of the last raytrace, 16-B aligned) on the tracer's stream, without synchronizing:
+ * for a caller that displays from device memory, as the reference's raytrace_kernel
+ * writes its screen surface (cuda_path_tracer.cu:416-420) — e.g. followed by a
+ * cudaMemcpy2DToArrayAsync into a graphics-interop array on cpt_tracer_stream(t). */
+int cpt_tracer_resolve(cpt_tracer* t, float* rgba_dev);
 /* Rays traced since upload (primary, extension, shadow); synchronizes. */
 int cpt_tracer_ray_counts(cpt_tracer* t, unsigned long long out[3]);
 cudaStream_t cpt_tracer_stream(cpt_tracer* t);

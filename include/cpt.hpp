@@ -255,8 +255,22 @@ public:
             check(CPT_ERR_INVALID_ARGUMENT, "CUDAPathTracer::raytrace");
             return;
         }
-        check(cpt_tracer_raytrace(m_t, uint32_t(screenWidth), uint32_t(screenHeight), 1), "CUDAPathTracer::raytrace");
+        if (!check(cpt_tracer_raytrace(m_t, uint32_t(screenWidth), uint32_t(screenHeight), 1), "CUDAPathTracer::raytrace"))
+            return;
+        if (!m_screen) return;
+        // the reference's raytrace_kernel writes every pixel's running value into the screen
+        // surface (cuda_path_tracer.cu:416-420); here the resolved image goes into the array
+        const size_t row = size_t(screenWidth) * 4 * sizeof(float);
+        m_image.resize(size_t(screenWidth) * size_t(screenHeight) * 4);
+        if (!m_image.data() || !check(cpt_tracer_resolve(m_t, m_image.data()), "CUDAPathTracer::raytrace")) return;
+        check_cuda(cudaMemcpy2DToArrayAsync(m_screen, 0, 0, m_image.data(), row, row, size_t(screenHeight),
+                                            cudaMemcpyDeviceToDevice, cpt_tracer_stream(m_t)),
+                   "CUDAPathTracer::raytrace");
     }
+    // CUDAPathTracer::setScreenTexture (cuda_path_tracer.h:18): a float4 (RGBA32F) array of
+    // the screen size, e.g. a mapped OpenGL texture, that every raytrace() updates with the
+    // accumulated image on the tracer's stream. nullptr: no screen array.
+    void setScreenTexture(const cudaArray_t* screenArray) { m_screen = screenArray ? *screenArray : nullptr; }
     void upload(const HostSceneDescription& sceneDesc)
     {
         const cpt_bbox& b = sceneDesc.enclosingBBox;
@@ -296,6 +310,8 @@ public:
 
 private:
     cpt_tracer* m_t = nullptr;
+    cudaArray_t m_screen = nullptr;
+    DeviceVector<float> m_image;  // the resolved image on its way into m_screen
 };
 
 }  // namespace cpt

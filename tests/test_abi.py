@@ -137,6 +137,13 @@ def test_render_sizes_and_rejections():
     assert cpt.render_scratch_bytes(deep) == 0
 
 
+def test_tracer_calls_refuse_a_null_tracer():
+    # no tracer exists without a device; the calls still refuse a null handle on the host
+    assert cpt.lib.cpt_tracer_resolve(None, 256) == cpt.ERR_INVALID_ARGUMENT
+    assert cpt.lib.cpt_tracer_read_image(None, 256) == cpt.ERR_INVALID_ARGUMENT
+    assert cpt.lib.cpt_tracer_raytrace(None, 8, 8, 1) == cpt.ERR_INVALID_ARGUMENT
+
+
 def test_scene_random_geometry():
     tris, infos = cpt.scene_random(5000, seed=1, edge_min=0.005, edge_max=0.02, light_y=1.25, light_size=0.5)
     assert len(tris) == 5002

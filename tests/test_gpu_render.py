@@ -250,6 +250,25 @@ def test_tracer_object_host_buffers(cuda):
     t.close()
 
 
+def test_tracer_resolve_writes_the_image_on_the_device(cuda):
+    """cpt_tracer_resolve (the device-side image the C++ mirror's setScreenTexture copies
+    into its array) gives the bytes cpt_tracer_read_image gives."""
+    tris, infos, _, cam = scene(n=8000)
+    t = cpt.Tracer(63)
+    t.upload(tris, infos)
+    t.set_settings(bounces=2, intensity=3.0, stratified=True, seed=123, accum_mode=cpt.ACCUM_KAHAN)
+    t.set_primary_rays(cam.as_array()[3:])
+    t.set_eye(cam.as_array()[:3])
+    t.raytrace(W, H, 2)
+    img = t.read_image(W, H)
+    out = torch.full((H, W, 4), -1.0, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    t.resolve(out.data_ptr())
+    torch.cuda.synchronize()
+    assert out.cpu().numpy().tobytes() == img.tobytes()
+    t.close()
+
+
 def test_graph_replay_advances_the_sample_stream(cuda):
     """One render call captured in a CUDA graph, replayed twice, equals two direct
     calls with frame0 = 0 and spp (the device frame counter advances per replay)."""
