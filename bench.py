@@ -266,6 +266,7 @@ def run_batch(args, w, world, rank, local):
     import torch
 
     import cpt
+    from cpt import autotune
     from cpt.device import BatchRenderer, DeviceLbvh, DeviceScene, make_params, stream_handle, to_device
     from cpt.multi import assign_by_cost, scene_cost
 
@@ -305,9 +306,8 @@ def run_batch(args, w, world, rank, local):
         return make_params(0, 0, w["spp"], 0, w["bounces"], 3.0, True, w["seed"],
                            cpt.ACCUM_KAHAN, wave_paths=wave, ray_sort=sort, trace_stats=stats)
 
-    # --- autotuner: one warm + one timed frame per candidate, keep the fastest
-    tune = []
-    for wave, sort in ((1 << 24, 0), (1 << 25, 0), (1 << 26, 0), (1 << 25, 1)):
+    # --- autotuner (cpt/autotune.py): one warm + one timed frame per candidate, keep the fastest
+    def time_frame(wave, sort):
         br = BatchRenderer(views, params(wave, sort), dev)
         br.render()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -315,10 +315,13 @@ def run_batch(args, w, world, rank, local):
         br.render()
         e1.record(stream)
         torch.cuda.synchronize()
-        tune.append({"wave_paths": wave, "ray_sort": sort, "ms": round(e0.elapsed_time(e1), 3)})
         del br
         torch.cuda.empty_cache()
-    best = min(tune, key=lambda r: r["ms"])
+        return e0.elapsed_time(e1)
+
+    tuned = autotune.tune(time_frame, ((1 << 24, 0), (1 << 25, 0), (1 << 26, 0), (1 << 25, 1)))
+    tune = tuned.table
+    best = {"wave_paths": tuned.wave_paths, "ray_sort": tuned.ray_sort, "ms": tuned.ms}
 
     # --- instrumented frame: node visits per closest-hit ray
     br = BatchRenderer(views, params(best["wave_paths"], best["ray_sort"], stats=True), dev)
