@@ -51,7 +51,7 @@ extern "C" int cpt_lbvh_build_static(const cpt_triangle* tris_in, uint32_t n, co
 {
     CPT_RANGE("cpt_lbvh_build_static");
     if (n > kStaticMaxTriangles) return CPT_ERR_SCRATCH_TOO_SMALL;
-    if (n < 2 || (morton_bits != 30 && morton_bits != 63)) return CPT_ERR_INVALID_ARGUMENT;
+    if (n < 2 || (morton_bits != 30 && morton_bits != 63) || !tris_in || !bvh) return CPT_ERR_INVALID_ARGUMENT;
     if (cpt_lbvh_scratch_bytes(n, morton_bits) > kStaticScratchBytes) return CPT_ERR_SCRATCH_TOO_SMALL;
     void* scratch = nullptr;
     const int rc = scratch_address(&scratch);

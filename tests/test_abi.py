@@ -137,6 +137,54 @@ def test_render_sizes_and_rejections():
     assert cpt.render_scratch_bytes(deep) == 0
 
 
+def test_every_entry_point_refuses_null_arguments():
+    # null handles and buffers are refused on the host with CPT_ERR_INVALID_ARGUMENT,
+    # before any device call, and never dereferenced
+    L = cpt.lib
+    calls = {
+        "cpt_lbvh_build_static": lambda: L.cpt_lbvh_build_static(None, 10, None, 30, None, 0, None),
+        "cpt_bvh_bind": lambda: L.cpt_bvh_bind(None, 0, 10, 30, None),
+        "cpt_status_check": lambda: L.cpt_status_check(None, None),
+        "cpt_lbvh_wide": lambda: L.cpt_lbvh_wide(None, None, 0, None, 0, None, 0, None),
+        "cpt_emitters_build": lambda: L.cpt_emitters_build(None, None, 4, None, 0, None, None),
+        "cpt_render": lambda: L.cpt_render(None, None, None, None, None, None, 0, None, None, None),
+        "cpt_render_views": lambda: L.cpt_render_views(None, 0, None, None, 0, None, None, None),
+        "cpt_resolve": lambda: L.cpt_resolve(None, 8, 8, 0, None, None),
+        "cpt_bvh_heatmap": lambda: L.cpt_bvh_heatmap(None, None, 8, 8, None, None, None, None),
+        "cpt_scene_deform": lambda: L.cpt_scene_deform(None, None, 10, 1.0, 1.0, 0.0, None),
+        "cpt_texture_create": lambda: L.cpt_texture_create(None, 4, 4, None),
+        "cpt_texture_sample": lambda: L.cpt_texture_sample(0, None, 4, None, None),
+        "cpt_rc_create": lambda: L.cpt_rc_create(None, None, None),
+        "cpt_rc_reset": lambda: L.cpt_rc_reset(None, 1, None),
+        "cpt_rc_get_weights": lambda: L.cpt_rc_get_weights(None, None, None),
+        "cpt_rc_set_weights": lambda: L.cpt_rc_set_weights(None, None, None),
+        "cpt_rc_infer": lambda: L.cpt_rc_infer(None, None, 4, None, None, None),
+        "cpt_rc_train": lambda: L.cpt_rc_train(None, None, 4, None, 1, None, None),
+        "cpt_rc_render": lambda: L.cpt_rc_render(None, None, 0, None, None, 0, None, None, None),
+        "cpt_rc_update": lambda: L.cpt_rc_update(None, None, 0, None, None, 0, None, None, None),
+        "cpt_rc_sample_count": lambda: L.cpt_rc_sample_count(None, None, None),
+        "cpt_rc_samples": lambda: L.cpt_rc_samples(None, None),
+        "cpt_tracer_create": lambda: L.cpt_tracer_create(None, 30),
+        "cpt_tracer_upload": lambda: L.cpt_tracer_upload(None, None, 10, None, 1, None, 0, None),
+        "cpt_tracer_upload_textures": lambda: L.cpt_tracer_upload_textures(None, None, 0),
+        "cpt_tracer_set_split": lambda: L.cpt_tracer_set_split(None, 1.0, 0),
+        "cpt_tracer_set_wide": lambda: L.cpt_tracer_set_wide(None, 1),
+        "cpt_tracer_set_nee": lambda: L.cpt_tracer_set_nee(None, 1),
+        "cpt_tracer_set_primary_rays": lambda: L.cpt_tracer_set_primary_rays(None, None),
+        "cpt_tracer_set_eye": lambda: L.cpt_tracer_set_eye(None, None),
+        "cpt_tracer_set_camera": lambda: L.cpt_tracer_set_camera(None, None),
+        "cpt_tracer_set_settings": lambda: L.cpt_tracer_set_settings(None, 1, 3.0, 1, 0, 0, 0),
+        "cpt_tracer_ray_counts": lambda: L.cpt_tracer_ray_counts(None, None),
+    }
+    for name, call in calls.items():
+        assert call() == cpt.ERR_INVALID_ARGUMENT, name
+    # calls without a status accept a null handle
+    L.cpt_tracer_destroy(None)
+    L.cpt_rc_destroy(None)
+    L.cpt_tracer_reset_frames(None)
+    assert L.cpt_tracer_frame(None) == 0 and not L.cpt_tracer_stream(None) and not L.cpt_tracer_bvh(None)
+
+
 def test_tracer_calls_refuse_a_null_tracer():
     # no tracer exists without a device; the calls still refuse a null handle on the host
     assert cpt.lib.cpt_tracer_resolve(None, 256) == cpt.ERR_INVALID_ARGUMENT
