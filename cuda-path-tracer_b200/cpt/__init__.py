@@ -167,6 +167,8 @@ _PROTOS = {
     "cpt_tracer_frame": (_U32, [_P]),
     "cpt_tracer_read_image": (_I32, [_P, _P]),
     "cpt_tracer_resolve": (_I32, [_P, _P]),
+    "cpt_tracer_get_progress": (_I32, [_P, _P, _SZ, ctypes.POINTER(_U32)]),
+    "cpt_tracer_set_progress": (_I32, [_P, _P, _SZ, _U32, _U32, _U32]),
     "cpt_tracer_ray_counts": (_I32, [_P, _P]),
     "cpt_tracer_stream": (_P, [_P]),
     "cpt_tracer_bvh": (ctypes.POINTER(Bvh), [_P]),
@@ -464,6 +466,19 @@ class Tracer:
             out = np.empty((height, width, 4), np.float32)
         check(lib.cpt_tracer_read_image(self._h, _ptr(out)), "cpt_tracer_read_image")
         return out
+
+    def get_progress(self, width: int, height: int, accum_mode: int) -> tuple[np.ndarray, int]:
+        """(accumulator bytes, next frame) of the last raytrace at width x height."""
+        out = np.empty(accum_bytes(width, height, accum_mode), np.uint8)
+        frame = ctypes.c_uint32()
+        check(lib.cpt_tracer_get_progress(self._h, _ptr(out), out.nbytes, ctypes.byref(frame)),
+              "cpt_tracer_get_progress")
+        return out, frame.value
+
+    def set_progress(self, accum: np.ndarray, width: int, height: int, frame: int) -> None:
+        a = np.ascontiguousarray(accum).reshape(-1).view(np.uint8)
+        check(lib.cpt_tracer_set_progress(self._h, _ptr(a), a.nbytes, width, height, frame),
+              "cpt_tracer_set_progress")
 
     def resolve(self, rgba_dev: int) -> None:
         """Writes the image into device memory (float4 per pixel) on the tracer's stream."""

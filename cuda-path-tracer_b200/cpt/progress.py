@@ -16,11 +16,13 @@ File format: a NumPy .npz holding `accum` (uint8, the accumulator bytes) and `me
 fields in STREAM_FIELDS). Written to a temporary name and renamed, so a crash while
 saving leaves the previous checkpoint intact.
 
+The `cpt_tracer` object keeps its accumulator inside; `Tracer.get_progress` /
+`Tracer.set_progress` (cpt_tracer_get_progress / cpt_tracer_set_progress) move it and
+the frame counter, and `save` / `load` store them like any other accumulator.
+
 What is not covered: a radiance cache's optimizer state (its weights can be read and
 set with cpt_rc_get_weights / cpt_rc_set_weights, its Adam moments cannot), so a
-cached render resumes with the same weights but not bit-identically; and the
-`cpt_tracer` object, whose accumulator is internal (render through `cpt_render` or
-`cpt_render_views` with a caller-owned accumulator to checkpoint).
+cached render resumes with the same weights but not bit-identically.
 """
 from __future__ import annotations
 

@@ -768,6 +768,32 @@ extern "C" int cpt_tracer_resolve(cpt_tracer* t, float* rgba_dev)
     return cpt_resolve(t->d_accum, t->width, t->height, t->accum_mode, rgba_dev, t->stream);
 }
 
+extern "C" int cpt_tracer_get_progress(cpt_tracer* t, void* accum_host, size_t bytes, uint32_t* frame)
+{
+    if (!t || !accum_host || !frame || !t->d_accum || !t->width) return CPT_ERR_INVALID_ARGUMENT;
+    if (bytes != cpt_accum_bytes(t->width, t->height, t->accum_mode)) return CPT_ERR_INVALID_ARGUMENT;
+    CPT_CUDA_TRY(cudaMemcpyAsync(accum_host, t->d_accum, bytes, cudaMemcpyDeviceToHost, t->stream));
+    CPT_CUDA_TRY(cudaStreamSynchronize(t->stream));
+    *frame = t->frame;
+    return CPT_OK;
+}
+
+extern "C" int cpt_tracer_set_progress(cpt_tracer* t, const void* accum_host, size_t bytes, uint32_t width,
+                                       uint32_t height, uint32_t frame)
+{
+    if (!t || !accum_host || width == 0 || height == 0) return CPT_ERR_INVALID_ARGUMENT;
+    const size_t need = cpt_accum_bytes(width, height, t->accum_mode);
+    if (!need || bytes != need) return CPT_ERR_INVALID_ARGUMENT;
+    int rc;
+    if ((rc = ensure(&t->d_accum, &t->accum_cap, need))) return rc;
+    CPT_CUDA_TRY(cudaMemcpyAsync(t->d_accum, accum_host, bytes, cudaMemcpyHostToDevice, t->stream));
+    CPT_CUDA_TRY(cudaStreamSynchronize(t->stream));  // the host copy may go away
+    t->width = width;
+    t->height = height;
+    t->frame = frame;
+    return CPT_OK;
+}
+
 extern "C" int cpt_tracer_ray_counts(cpt_tracer* t, unsigned long long out[3])
 {
     if (!t || !out) return CPT_ERR_INVALID_ARGUMENT;

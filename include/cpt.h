@@ -367,6 +367,18 @@ int cpt_tracer_read_image(cpt_tracer* t, float* rgba_host);
  * writes its screen surface (cuda_path_tracer.cu:416-420) — e.g. followed by a
  * cudaMemcpy2DToArrayAsync into a graphics-interop array on cpt_tracer_stream(t). */
 int cpt_tracer_resolve(cpt_tracer* t, float* rgba_dev);
+/* Checkpoint / resume of the progressive image (the reference loses it on exit).
+ * get: copies the accumulator of the last raytrace (cpt_accum_bytes(width, height,
+ * accum_mode) bytes, the layout of the tracer's accum mode) and the frame counter to
+ * host memory; synchronizes. set: restores them for a width x height image, so that the
+ * next cpt_tracer_raytrace at that size continues from frame `frame`; synchronizes.
+ * Resuming gives the same image as an uninterrupted run when the scene, camera and
+ * settings (cpt_tracer_set_settings, cpt_tracer_set_nee) are those of the saved run;
+ * apply the settings before set, which reads the accumulator in the current accum mode
+ * (the Kahan and FP64 layouts have the same size, so a mode mismatch is not detected). */
+int cpt_tracer_get_progress(cpt_tracer* t, void* accum_host, size_t bytes, uint32_t* frame);
+int cpt_tracer_set_progress(cpt_tracer* t, const void* accum_host, size_t bytes, uint32_t width, uint32_t height,
+                            uint32_t frame);
 /* Rays traced since upload (primary, extension, shadow); synchronizes. */
 int cpt_tracer_ray_counts(cpt_tracer* t, unsigned long long out[3]);
 cudaStream_t cpt_tracer_stream(cpt_tracer* t);

@@ -175,6 +175,9 @@ def test_every_entry_point_refuses_null_arguments():
         "cpt_tracer_set_camera": lambda: L.cpt_tracer_set_camera(None, None),
         "cpt_tracer_set_settings": lambda: L.cpt_tracer_set_settings(None, 1, 3.0, 1, 0, 0, 0),
         "cpt_tracer_ray_counts": lambda: L.cpt_tracer_ray_counts(None, None),
+        "cpt_tracer_get_progress": lambda: L.cpt_tracer_get_progress(None, None, 0, None),
+        "cpt_tracer_set_progress": lambda: L.cpt_tracer_set_progress(None, None, 0, 8, 8, 1),
+        "cpt_tracer_resolve": lambda: L.cpt_tracer_resolve(None, None),
     }
     for name, call in calls.items():
         assert call() == cpt.ERR_INVALID_ARGUMENT, name

@@ -269,6 +269,36 @@ def test_tracer_resolve_writes_the_image_on_the_device(cuda):
     t.close()
 
 
+def test_tracer_progress_resume_matches_one_run(cuda):
+    """cpt_tracer_get_progress / cpt_tracer_set_progress: frames [0, 2) by one tracer,
+    restored into a second tracer with the same scene, camera and settings that renders
+    frame 2, give the image of one tracer rendering frames [0, 3)."""
+    tris, infos, _, cam = scene(n=8000)
+
+    def tracer():
+        t = cpt.Tracer(63)
+        t.upload(tris, infos)
+        t.set_settings(bounces=2, intensity=3.0, stratified=True, seed=123, accum_mode=cpt.ACCUM_KAHAN)
+        t.set_primary_rays(cam.as_array()[3:])
+        t.set_eye(cam.as_array()[:3])
+        return t
+
+    straight = tracer()
+    straight.raytrace(W, H, 3)
+    want = straight.read_image(W, H)
+    first = tracer()
+    first.raytrace(W, H, 2)
+    acc, frame = first.get_progress(W, H, cpt.ACCUM_KAHAN)
+    assert frame == 2 and acc.nbytes == cpt.accum_bytes(W, H, cpt.ACCUM_KAHAN)
+    second = tracer()
+    second.set_progress(acc, W, H, frame)
+    second.raytrace(W, H, 1)
+    assert second.frame == 3
+    assert second.read_image(W, H).tobytes() == want.tobytes()
+    for t in (straight, first, second):
+        t.close()
+
+
 def test_graph_replay_advances_the_sample_stream(cuda):
     """One render call captured in a CUDA graph, replayed twice, equals two direct
     calls with frame0 = 0 and spp (the device frame counter advances per replay)."""
