@@ -513,13 +513,14 @@ extern "C" int cpt_tracer_create(cpt_tracer** out, int morton_bits)
 extern "C" void cpt_tracer_destroy(cpt_tracer* t)
 {
     if (!t) return;
+    // both streams may still use the buffers (the copy stream uploads shading records)
     if (t->stream) cudaStreamSynchronize(t->stream);
+    if (t->copy_stream) cudaStreamSynchronize(t->copy_stream);
     void* bufs[] = {t->d_tris, t->d_bvh, t->d_build_scratch, t->d_infos, t->d_lights, t->d_textures, t->d_accum,
                     t->d_render_scratch, t->d_image, t->d_counts, t->d_split_nodes, t->d_split_scratch,
                     t->d_emitters, t->d_wide_nodes, t->d_wide_tris, t->d_wide_scratch};
     for (void* b : bufs)
         if (b) cudaFree(b);
-    if (t->copy_stream) cudaStreamSynchronize(t->copy_stream);
     if (t->ev_upload) cudaEventDestroy(t->ev_upload);
     if (t->ev_copied) cudaEventDestroy(t->ev_copied);
     if (t->copy_stream) cudaStreamDestroy(t->copy_stream);
