@@ -204,10 +204,20 @@ def sum_over_ranks(x, world):
 
 
 # --------------------------------------------------------------------------- CPU baseline
-def cpu_reference_run(w, tris, infos, cam, bits, target_s=12.0, rows_hint=None):
+def sample_rows(height, stride):
+    """Every stride-th row of the frame, starting half a stride in: a sample spread
+    evenly over the whole image (sky, sphere and hairball rows in their proportions)."""
+    return np.arange(stride // 2, height, stride, dtype=np.uint32)
+
+
+def cpu_reference_run(w, tris, infos, cam, bits, target_s=12.0, stride=None):
     """The reference's own builder (oracle/_ref, OpenMP over all host threads) on the
-    full scene, then its trace functions inside the restated integrator on a band
-    of rows, sized for ~target_s seconds. Falls back to the oracle port."""
+    full scene, then the restated integrator over the reference's trace functions on
+    every `stride`-th row of frame 0 (samples 0 .. spp-1 of the workload's seed), with
+    the stride chosen for ~target_s seconds of CPU work. The frame's rate is taken to
+    be the sampled rows' rate (the rows are spread over the whole frame). Per-pixel
+    float64 sums of the rows come back for the parity check against the GPU's frame 0.
+    Falls back to the oracle port when the reference library was not built."""
     from oracle import cpu
 
     threads = os.cpu_count() or 1
@@ -216,30 +226,41 @@ def cpu_reference_run(w, tris, infos, cam, bits, target_s=12.0, rows_hint=None):
     b = cpu.build(tris, bits, use_ref=(kind == "reference"))
     build_s = time.perf_counter() - t0
     width, height, spp = w["width"], w["height"], w["spp"]
-    mid = height // 2
     cam15 = cam.as_array()
 
     def run(rows):
-        r0 = max(0, mid - rows // 2)
-        r1 = min(height, r0 + rows)
         t1 = time.perf_counter()
         if kind == "reference":
-            _, cnt = cpu.ref_render(b, infos, None, width, height, (r0, r1), spp, 0, w["bounces"], 3.0, True,
-                                    w["seed"], cam15, threads)
+            sums, cnt = cpu.ref_render_rows(b, infos, None, width, height, rows, spp, 0, w["bounces"], 3.0, True,
+                                            w["seed"], cam15, threads)
         else:
-            _, cnt = cpu.render(b, infos, None, width, height, spp, 0, w["bounces"], 3.0, True, w["seed"],
-                                cpu.ocam_from(cam.eye, cam15[3:]), rows=(r0, r1))
-        return time.perf_counter() - t1, int(cnt.sum()), r1 - r0
+            sums, cnt = cpu.render_rows(b, infos, width, height, rows, spp, 0, w["bounces"], 3.0, True, w["seed"],
+                                        cpu.ocam_from(cam.eye, cam15[3:]))
+        return time.perf_counter() - t1, int(cnt.sum()), sums
 
-    rows = rows_hint
-    if rows is None:
-        dt, _, _ = run(1)
-        rows = int(max(1, min(height, target_s / max(dt, 1e-3))))
-    dt, rays, rows = run(rows)
+    if stride is None:  # probe 8 rows spread over the frame, then size the sample
+        probe = sample_rows(height, max(1, height // 8))
+        dt, _, _ = run(probe)
+        rows_needed = max(1.0, target_s / max(dt / len(probe), 1e-4))
+        stride = int(min(height, max(1, round(height / rows_needed))))
+    rows = sample_rows(height, stride)
+    dt, rays, sums = run(rows)
     return {"kind": kind, "threads": threads, "build_s": build_s, "build_mtris_s": len(tris) / build_s / 1e6,
-            "render_s": dt, "rays": rays, "rows": rows, "mrays_s": rays / dt / 1e6,
-            "sample": f"{rows} of {height} rows (centre band) x {width} px x {spp} spp, depth {w['bounces'] + 1}; "
-                      f"build of all {len(tris)} triangles"}
+            "render_s": dt, "rays": rays, "rows": rows, "stride": stride, "sums": sums,
+            "mrays_s": rays / dt / 1e6,
+            "sample": f"one row in {stride} of frame 0 ({len(rows)} of {height} rows, from row {stride // 2}) x "
+                      f"{width} px x {spp} spp, depth {w['bounces'] + 1}; the frame's rate is taken as the sampled "
+                      f"rows' rate; build of all {len(tris)} triangles"}
+
+
+def frame_parity(gpu_sums, cpu_sums, spp):
+    """GPU frame-0 rows (FP64 accumulator) against the reference's rows (float64 sums
+    of the same float samples in the same order): pixels whose three sums differ in
+    any bit, and the largest difference of the per-pixel mean."""
+    differ = (gpu_sums != cpu_sums).any(axis=-1)
+    diff = np.abs(gpu_sums - cpu_sums).max() / spp if gpu_sums.size else 0.0
+    return {"rows": int(gpu_sums.shape[0]), "pixels": int(differ.size), "mismatched_pixels": int(differ.sum()),
+            "max_abs_diff": float(diff), "exact": bool(not differ.any())}
 
 
 # --------------------------------------------------------------------------- batched scenes (c3)
@@ -488,14 +509,14 @@ def run_reference_arm(args, w, world, rank):
     cam = make_cameras(w)[0]
     # size one step for ~8 s of CPU work, then warm up and time K steps of that size
     probe = cpu_reference_run(w, tris, infos, cam, w["bits"], target_s=8.0)
-    rows = probe["rows"]
+    stride = probe["stride"]
     for _ in range(max(0, args.warmup - 1)):
-        cpu_reference_run(w, tris, infos, cam, w["bits"], rows_hint=rows)
+        cpu_reference_run(w, tris, infos, cam, w["bits"], stride=stride)
     rays = 0
     secs = 0.0
     last = probe
     for _ in range(args.steps):
-        last = cpu_reference_run(w, tris, infos, cam, w["bits"], rows_hint=rows)
+        last = cpu_reference_run(w, tris, infos, cam, w["bits"], stride=stride)
         rays += last["rays"]
         secs += last["render_s"]
     value = rays / secs / 1e6
@@ -597,6 +618,8 @@ def run_ours(args, w, world, rank, local):
         cached.counts.zero_()
 
     # --- timed frames
+    my_accums = cached.accums if cached is not None else [rend.accum]
+    display = [torch.empty_like(a) for a in my_accums] if world > 1 else []  # rank 0's reduced images
     sampler = ClockSampler(local if world > 1 else 0) if rank == 0 else None
     if sampler:
         sampler.start()
@@ -614,8 +637,8 @@ def run_ours(args, w, world, rank, local):
         frame_step(rank_frame0(frame, rank))
         frame += spp
         if world > 1:  # the one exchange of the path: framebuffer reduce to rank 0 every frame
-            for acc in (cached.accums if cached is not None else [rend.accum]):
-                reduce_accumulator(acc, dst=0)
+            for acc, disp in zip(my_accums, display):
+                reduce_accumulator(acc, disp, dst=0, mode=cpt.ACCUM_KAHAN)
     ev1.record(stream)
     torch.cuda.synchronize()
     prof = cpt.profile_end()
@@ -639,21 +662,14 @@ def run_ours(args, w, world, rank, local):
     alg_bytes = rays_closest * (32 + 16) + rays_closest * (node_b * mean_nodes + 48.0 * mean_tris)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
-    traffic = None
-    prof_name, key = (("k_extend_c2_wide.md", "dram_bytes_per_closest_ray_wide") if args.wide else
-                      ("k_extend_c2_split.md", "dram_bytes_per_closest_ray_split") if split > 0 else
-                      ("k_extend_c2.md", "dram_bytes_per_closest_ray"))
-    tp = os.path.join(ROOT, "profiles", prof_name)
-    if args.workload == "c2" and os.path.exists(tp):  # ncu figure of the C2 traversal (see that file)
-        import re
-
-        m = re.search(key + r" = ([0-9.]+)", open(tp).read())
-        if m:
-            traffic = round(float(m.group(1)) * rays_closest / max(ext_launches, 1), 1)
+    # DRAM traffic needs ncu, which this run does not use: the per-ray figure of the
+    # traversal's capture is in the profile named here, not re-read by the benchmark
+    prof_name = ("k_extend_c2_wide.md" if args.wide else "k_extend_c2_split.md" if split > 0 else "k_extend_c2.md")
     roofline = {"bound": "hbm", "kernel": "k_extend", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6650 GB/s",
-                "traffic": traffic, "algorithmic_bytes_per_launch": round(alg_bytes / max(ext_launches, 1), 1),
+                "traffic": None, "traffic_note": f"not measured in this run (no ncu); see profiles/{prof_name}",
+                "algorithmic_bytes_per_launch": round(alg_bytes / max(ext_launches, 1), 1),
                 "avg_launch_ms": round(ext_ms / max(ext_launches, 1), 4),
                 "bytes_per_ray": f"32 ray + 16 hit + {node_b:.0f} x {mean_nodes:.2f} nodes + 48 x {mean_tris:.2f} triangles",
                 "rays_per_depth_first_frame": depth_rays,
@@ -780,12 +796,28 @@ def run_ours(args, w, world, rank, local):
                                         + ", 16-spp frame, D2H image"}
         tr.close()
 
-    # --- CPU baseline (rank 0, N = 1)
-    cpu_base = None
+    # --- CPU baseline (rank 0, N = 1): the reference's code on every k-th row of frame 0,
+    # and the parity of the GPU's frame 0 (FP64 accumulator, same traversal tree as the
+    # timed frames) on those rows
+    cpu_base, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference_run(w, tris, infos, cams[0], w["bits"], target_s=args.cpu_seconds)
         cpu_base = {"value": round(r["mrays_s"], 4), "unit": METRIC, "cores": r["threads"], "kind": r["kind"],
                     "sample": r["sample"], "build_mtris_s": round(r["build_mtris_s"], 3)}
+        if not deforming and cached is None:
+            pr = DeviceRenderer(make_params(W_, H_, spp, 0, w["bounces"], 3.0, True, w["seed"], cpt.ACCUM_F64,
+                                            wave_paths=args.wave_paths), dev)
+            pr.render(lb, scene, cams[0], frame0=0)
+            torch.cuda.synchronize()
+            pr.check_status()
+            acc = pr.accum.view(torch.float64).view(H_, W_, 4)
+            gpu_rows = acc[torch.as_tensor(r["rows"].astype(np.int64), device=dev), :, :3].cpu().numpy()
+            parity = frame_parity(gpu_rows, r["sums"], spp)
+            frame_rays = float(pr.counts[:3].sum())
+            parity["against"] = f"{r['kind']} ({'oracle/_ref: the reference compiled from source' if r['kind'] == 'reference' else 'oracle port'}) on the LBVH"
+            cpu_base["sample_rays_share"] = round(r["rays"] / max(frame_rays, 1.0), 5)
+            cpu_base["sample_rows_share"] = round(len(r["rows"]) / H_, 5)
+            del pr
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -798,7 +830,8 @@ def run_ours(args, w, world, rank, local):
                                   + (f"split BVH (cpt_lbvh_split, extra pieces {split} x n"
                                      + (", treelet-restructured" if args.treelet else "") + ")" if split > 0
                                      else "LBVH (reference topology)")), "lbvh_topology": lbvh_topology,
-                "cpu_baseline": cpu_base, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+                "cpu_baseline": cpu_base, "parity": parity, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clocks,
                 "parallelism": f"replicas x{world}: own BVH per GPU, disjoint sample streams, "
                                f"framebuffer reduce to rank 0 per frame" if world > 1 else "1 GPU",
                 "scene_gen_s": round(gen_s, 2)}

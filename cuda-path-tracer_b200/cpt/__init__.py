@@ -37,9 +37,16 @@ ERRORS = {
 ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_SCRATCH_TOO_SMALL, ERR_NONFINITE_INPUT = 1, 2, 3, 4
 ERR_DEVICE_TIMEOUT, ERR_STACK_OVERFLOW, ERR_CHECK_FAILED, ERR_NO_DEVICE, ERR_BAD_INDEX = 5, 6, 7, 8, 9
 BUILD_CHECK = 1
+BUILD_TEST_WITHHOLD = 2  # test of the bounded sort wait: tile 0 of the first pass never publishes
+
+
+def build_lookback_limit(log2_polls: int) -> int:
+    """cpt_lbvh_build flag bits: a look-back poll limit of 2^log2_polls per tile."""
+    return (int(log2_polls) & 31) << 8
+
+
 ACCUM_KAHAN, ACCUM_LERP, ACCUM_F64 = 0, 1, 2
 INVALID_INDEX = 0xFFFFFFFF
-SPLIT_PLOC = 1
 SPLIT_TREELET = 2
 TRAVERSAL_STACK = 64
 
@@ -167,8 +174,8 @@ _PROTOS = {
     "cpt_tracer_frame": (_U32, [_P]),
     "cpt_tracer_read_image": (_I32, [_P, _P]),
     "cpt_tracer_resolve": (_I32, [_P, _P]),
-    "cpt_tracer_get_progress": (_I32, [_P, _P, _SZ, ctypes.POINTER(_U32)]),
-    "cpt_tracer_set_progress": (_I32, [_P, _P, _SZ, _U32, _U32, _U32]),
+    "cpt_tracer_get_progress": (_I32, [_P, _P, _SZ, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "cpt_tracer_set_progress": (_I32, [_P, _P, _SZ, _U32, _U32, _U32, _U32]),
     "cpt_tracer_ray_counts": (_I32, [_P, _P]),
     "cpt_tracer_stream": (_P, [_P]),
     "cpt_tracer_bvh": (ctypes.POINTER(Bvh), [_P]),
@@ -468,16 +475,19 @@ class Tracer:
         return out
 
     def get_progress(self, width: int, height: int, accum_mode: int) -> tuple[np.ndarray, int]:
-        """(accumulator bytes, next frame) of the last raytrace at width x height."""
+        """(accumulator bytes, next frame) of the last raytrace at width x height, whose
+        accumulator mode must be accum_mode (the tracer reports its own; a mismatch raises)."""
         out = np.empty(accum_bytes(width, height, accum_mode), np.uint8)
-        frame = ctypes.c_uint32()
-        check(lib.cpt_tracer_get_progress(self._h, _ptr(out), out.nbytes, ctypes.byref(frame)),
+        frame, mode = ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib.cpt_tracer_get_progress(self._h, _ptr(out), out.nbytes, ctypes.byref(frame), ctypes.byref(mode)),
               "cpt_tracer_get_progress")
+        if mode.value != accum_mode:
+            raise CptError(ERR_INVALID_ARGUMENT, f"cpt_tracer_get_progress: tracer accumulates in mode {mode.value}")
         return out, frame.value
 
-    def set_progress(self, accum: np.ndarray, width: int, height: int, frame: int) -> None:
+    def set_progress(self, accum: np.ndarray, width: int, height: int, frame: int, accum_mode: int) -> None:
         a = np.ascontiguousarray(accum).reshape(-1).view(np.uint8)
-        check(lib.cpt_tracer_set_progress(self._h, _ptr(a), a.nbytes, width, height, frame),
+        check(lib.cpt_tracer_set_progress(self._h, _ptr(a), a.nbytes, width, height, frame, accum_mode),
               "cpt_tracer_set_progress")
 
     def resolve(self, rgba_dev: int) -> None:

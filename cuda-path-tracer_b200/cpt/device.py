@@ -48,10 +48,14 @@ class DeviceLbvh:
         self.scratch = dev_bytes(self.scratch_bytes, device)
         self.bvh: Bvh = bvh_bind(self.mem.data_ptr(), self.mem.numel(), self.n, self.bits)
 
-    def build(self, tris: torch.Tensor | int, box=None, check_root: bool = False, stream: int | None = None) -> None:
+    def build(self, tris: torch.Tensor | int, box=None, check_root: bool = False, stream: int | None = None,
+              flags: int = 0) -> None:
+        """cpt_lbvh_build into this object's arrays; `flags` adds cpt_lbvh_build flag
+        bits (the look-back limit and its test hook) to the check flag."""
         ptr = tris if isinstance(tris, int) else tris.data_ptr()
         lbvh_build(ptr, self.n, self.bits, self.bvh, self.scratch.data_ptr(), self.scratch_bytes, box=box,
-                   flags=BUILD_CHECK if check_root else 0, stream=stream_handle() if stream is None else stream)
+                   flags=(BUILD_CHECK if check_root else 0) | int(flags),
+                   stream=stream_handle() if stream is None else stream)
 
     def status(self, stream: int | None = None) -> None:
         status_check(self.bvh.status, stream_handle() if stream is None else stream)

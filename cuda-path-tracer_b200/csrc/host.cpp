@@ -596,8 +596,7 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
 extern "C" int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio, uint32_t flags)
 {
     if (!t || !(extra_ratio >= 0.f) || !(extra_ratio <= 64.f)) return CPT_ERR_INVALID_ARGUMENT;
-    if ((flags & ~(CPT_SPLIT_PLOC | CPT_SPLIT_TREELET)) || (flags & CPT_SPLIT_PLOC && flags & CPT_SPLIT_TREELET))
-        return CPT_ERR_INVALID_ARGUMENT;
+    if (flags & ~CPT_SPLIT_TREELET) return CPT_ERR_INVALID_ARGUMENT;
     t->split_ratio = extra_ratio;
     t->split_flags = flags;
     return CPT_OK;
@@ -708,8 +707,13 @@ extern "C" int cpt_tracer_raytrace(cpt_tracer* t, uint32_t width, uint32_t heigh
     const size_t ab = cpt_accum_bytes(width, height, t->accum_mode), sb = cpt_render_scratch_bytes(&p);
     if (!sb) return CPT_ERR_INVALID_ARGUMENT;
     if (width != t->width || height != t->height) t->frame = p.frame0 = 0;
-    if ((rc = ensure(&t->d_accum, &t->accum_cap, ab))) return rc;
-    if ((rc = ensure(&t->d_render_scratch, &t->render_cap, sb))) return rc;
+    // A failed allocation (ensure frees the old buffer first) leaves no image: the
+    // next raytrace then starts from frame 0 on a zeroed accumulator.
+    if ((rc = ensure(&t->d_accum, &t->accum_cap, ab)) || (rc = ensure(&t->d_render_scratch, &t->render_cap, sb))) {
+        t->frame = 0;
+        t->width = t->height = 0;
+        return rc;
+    }
     t->width = width;
     t->height = height;
     if (t->frame == 0) CPT_CUDA_TRY(cudaMemsetAsync(t->d_accum, 0, ab, t->stream));
@@ -769,22 +773,30 @@ extern "C" int cpt_tracer_resolve(cpt_tracer* t, float* rgba_dev)
     return cpt_resolve(t->d_accum, t->width, t->height, t->accum_mode, rgba_dev, t->stream);
 }
 
-extern "C" int cpt_tracer_get_progress(cpt_tracer* t, void* accum_host, size_t bytes, uint32_t* frame)
+extern "C" int cpt_tracer_get_progress(cpt_tracer* t, void* accum_host, size_t bytes, uint32_t* frame,
+                                       uint32_t* accum_mode)
 {
-    if (!t || !accum_host || !frame || !t->d_accum || !t->width) return CPT_ERR_INVALID_ARGUMENT;
+    if (!t || !accum_host || !frame || !accum_mode || !t->d_accum || !t->width) return CPT_ERR_INVALID_ARGUMENT;
     if (bytes != cpt_accum_bytes(t->width, t->height, t->accum_mode)) return CPT_ERR_INVALID_ARGUMENT;
     CPT_CUDA_TRY(cudaMemcpyAsync(accum_host, t->d_accum, bytes, cudaMemcpyDeviceToHost, t->stream));
     CPT_CUDA_TRY(cudaStreamSynchronize(t->stream));
     *frame = t->frame;
+    *accum_mode = t->accum_mode;
     return CPT_OK;
 }
 
 extern "C" int cpt_tracer_set_progress(cpt_tracer* t, const void* accum_host, size_t bytes, uint32_t width,
-                                       uint32_t height, uint32_t frame)
+                                       uint32_t height, uint32_t frame, uint32_t accum_mode)
 {
     if (!t || !accum_host || width == 0 || height == 0) return CPT_ERR_INVALID_ARGUMENT;
+    // the Kahan and FP64 layouts have the same size: the mode is checked, not guessed
+    if (accum_mode != t->accum_mode) return CPT_ERR_INVALID_ARGUMENT;
     const size_t need = cpt_accum_bytes(width, height, t->accum_mode);
     if (!need || bytes != need) return CPT_ERR_INVALID_ARGUMENT;
+    // Until the copy has landed the tracer holds no image: any failure below leaves it
+    // to start from frame 0 on a zeroed accumulator at its next raytrace.
+    t->frame = 0;
+    t->width = t->height = 0;
     int rc;
     if ((rc = ensure(&t->d_accum, &t->accum_cap, need))) return rc;
     CPT_CUDA_TRY(cudaMemcpyAsync(t->d_accum, accum_host, bytes, cudaMemcpyHostToDevice, t->stream));

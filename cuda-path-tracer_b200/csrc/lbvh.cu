@@ -19,8 +19,10 @@
 // tile ranks its keys with warp-level match/popc scans and finds its output base
 // by decoupled look-back over the preceding tiles). LSD radix sorting is stable,
 // which reproduces thrust's stable sort_by_key order for equal keys. The
-// look-back wait is bounded: after kLookbackPolls polls it records
-// CPT_STATUS_TIMEOUT and proceeds, so no launch can hang.
+// look-back wait is bounded: after its poll limit (kLookbackPolls, or the
+// caller's CPT_BUILD_LOOKBACK_LIMIT) it records CPT_STATUS_TIMEOUT and proceeds,
+// so no launch can hang; topology and refit then return at once, and the parent
+// walk of the refit is bounded by n - 1 steps.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <math.h>
@@ -188,6 +190,7 @@ __global__ void __launch_bounds__(kRefitBlock) k_gather_refit(const float* __res
     __syncthreads();
     const uint32_t i = base + threadIdx.x;
     if (i >= n) return;
+    if (sort_timed_out(status)) return;  // the order is not a sort: nothing to gather or refit
     const uint32_t block_end = min(n, base + (uint32_t)kRefitBlock);  // leaves [base, block_end)
     uint32_t src = order[i];
     if (src >= n) {  // only after a failed sort pass (its status is already set): stay in bounds
@@ -206,8 +209,11 @@ __global__ void __launch_bounds__(kRefitBlock) k_gather_refit(const float* __res
     Box box = leaf_box(v);  // BVHBuilder.cu:73-74, BBox.cpp:26-30
     uint32_t child = i;
     uint32_t p = parents_leaf[i];
-    while (p != CPT_INVALID_INDEX) {
-        if (p >= n - 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
+    // A node lets at most one arriver continue (the second; a third is refused), so
+    // a walk passes at most n - 1 nodes even on a corrupt topology; the step count
+    // makes that bound explicit.
+    for (uint32_t steps = 0; p != CPT_INVALID_INDEX; ++steps) {
+        if (p >= n - 1 || steps >= n - 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
         float* node = nodes + 24 * (size_t)p;
         const float4 meta = *reinterpret_cast<const float4*>(node + 20);  // Node word, right child, range end
         const uint32_t word = __float_as_uint(meta.x);
@@ -315,7 +321,7 @@ size_t scratch_layout(uint32_t n, void* base, SortScratch<K>* s)
 
 template <typename K>
 int build_impl(const cpt_triangle* tris_in, uint32_t n, const float* host_box, cpt_bvh* bvh, void* scratch,
-               cudaStream_t stream)
+               SortWait wait, cudaStream_t stream)
 {
     constexpr int P = KeyTraits<K>::passes;
     SortScratch<K> s;
@@ -381,11 +387,14 @@ int build_impl(const cpt_triangle* tris_in, uint32_t n, const float* host_box, c
         if (p == 0)
             k_onesweep<K, true><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, n, nullptr, 8 * p,
                                                                      s.offsets + p * kRadix,
-                                                                     lb, s.tile_counters + p, bvh->status);
-        else
+                                                                     lb, s.tile_counters + p, bvh->status, wait);
+        else {
+            SortWait later = wait;
+            later.withhold_tile0 = 0;  // (the test hook stalls the first pass only)
             k_onesweep<K, false><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, n, nullptr, 8 * p,
                                                                       s.offsets + p * kRadix,
-                                                                      lb, s.tile_counters + p, bvh->status);
+                                                                      lb, s.tile_counters + p, bvh->status, later);
+        }
         CPT_LAUNCH_CHECK();
     }
     // P is even: keys end in bvh->keys, values in vals[(P - 1) & 1].
@@ -396,7 +405,7 @@ int build_impl(const cpt_triangle* tris_in, uint32_t n, const float* host_box, c
         CPT_PROF(K_TOPOLOGY, stream);
         k_topology<K><<<(inner + 255) / 256, 256, 0, stream>>>(keys, n, nullptr, bvh->children, bvh->parents_leaf,
                                                                 bvh->parents_internal, s.counters,
-                                                                static_cast<float4*>(bvh->nodes));
+                                                                static_cast<float4*>(bvh->nodes), bvh->status);
     }
     CPT_LAUNCH_CHECK();
     {
@@ -496,8 +505,18 @@ extern "C" int cpt_lbvh_build(const cpt_triangle* tris_in, uint32_t n, const flo
         (reinterpret_cast<uintptr_t>(bvh->nodes) & 15) || (reinterpret_cast<uintptr_t>(bvh->tris) & 15))
         return CPT_ERR_INVALID_ARGUMENT;
     if (scratch_bytes < cpt_lbvh_scratch_bytes(n, morton_bits)) return CPT_ERR_SCRATCH_TOO_SMALL;
-    int rc = morton_bits == 30 ? build_impl<uint32_t>(tris_in, n, enclosing_box, bvh, scratch, stream)
-                               : build_impl<uint64_t>(tris_in, n, enclosing_box, bvh, scratch, stream);
+    if (flags & ~(CPT_BUILD_CHECK | CPT_BUILD_TEST_WITHHOLD | CPT_BUILD_LOOKBACK_LIMIT(31)))
+        return CPT_ERR_INVALID_ARGUMENT;
+    SortWait wait;
+    const uint32_t log2_polls = (flags >> 8) & 31u;
+    if (log2_polls) wait.poll_limit = 1u << log2_polls;
+    if (flags & CPT_BUILD_TEST_WITHHOLD) {
+        // the stalled wait must be short: an explicit limit of at most 2^16 polls
+        if (log2_polls == 0 || log2_polls > 16) return CPT_ERR_INVALID_ARGUMENT;
+        wait.withhold_tile0 = 1;
+    }
+    int rc = morton_bits == 30 ? build_impl<uint32_t>(tris_in, n, enclosing_box, bvh, scratch, wait, stream)
+                               : build_impl<uint64_t>(tris_in, n, enclosing_box, bvh, scratch, wait, stream);
     if (rc != CPT_OK || !(flags & CPT_BUILD_CHECK)) return rc;
     rc = cpt_status_check(bvh->status, stream);
     if (rc != CPT_OK) return rc;

@@ -36,6 +36,17 @@ __device__ __forceinline__ uint32_t quantize(float x, uint32_t n)
     return (uint32_t)(q > 0 ? q : 0);
 }
 
+struct Box { float mn[3], mx[3]; };
+
+// True when a sort pass of this build gave up a look-back wait (CPT_STATUS_TIMEOUT):
+// the kernels after the sort then return at once, leaving their outputs unwritten,
+// and the build reports CPT_ERR_DEVICE_TIMEOUT. The status word is only read here,
+// in kernels launched after the sort, so the kernel boundary orders it.
+__device__ __forceinline__ bool sort_timed_out(const uint32_t* status)
+{
+    return (__ldcg(status) & CPT_STATUS_TIMEOUT) != 0u;
+}
+
 // ---------------------------------------------------------------------------
 // Karras radix tree over the sorted keys (BVHBuilder.cu:107-201). Also writes
 // the Node word into the traversal record, zeroes the refit counters and marks
@@ -57,11 +68,12 @@ __global__ void __launch_bounds__(256) k_topology(const K* __restrict__ keys, ui
                                                   const uint32_t* __restrict__ n_ptr, uint32_t* __restrict__ children,
                                                   uint32_t* __restrict__ parents_leaf,
                                                   uint32_t* __restrict__ parents_internal, int* __restrict__ counters,
-                                                  float4* __restrict__ nodes)
+                                                  float4* __restrict__ nodes, const uint32_t* __restrict__ status)
 {
     const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int nn = (int)(n_ptr ? *n_ptr : n_arg);
     if (i >= nn - 1) return;
+    if (sort_timed_out(status)) return;  // the keys are not sorted: build nothing from them
     const K ki = keys[i];
     int dd = key_delta(keys, ki, nn, i, i + 1) - key_delta(keys, ki, nn, i, i - 1);
     int d = (dd > 0) - (dd < 0);
@@ -96,7 +108,6 @@ __global__ void __launch_bounds__(256) k_topology(const K* __restrict__ keys, ui
     if (i == 0) parents_internal[0] = CPT_INVALID_INDEX;
 }
 
-struct Box { float mn[3], mx[3]; };
 
 // 40-B slot at float offset 10*side of a 96-B node; 8-B aligned float2 stores.
 __device__ __forceinline__ void store_slot(float* node, int side, const float s[10])

@@ -28,7 +28,10 @@ std::mutex g_setup_mu;
 void* g_scratch_addr[kMaxDevices] = {nullptr};
 
 // Device address of the scratch array on the current device; looked up once per
-// device (with that device current) and cached.
+// device (with that device current) and cached for the life of the process, so the
+// lookup never runs inside a stream capture after the first call. A device reset
+// (cudaDeviceReset, or a destroyed and recreated primary context) reloads the device
+// image and leaves the cached address stale; the header tells callers so.
 int scratch_address(void** out)
 {
     int dev = -1;

@@ -16,7 +16,15 @@ constexpr int kSortWarps = kSortBlock / 32;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortBlock * kSortItems;  // 4096 keys per tile
 constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kValueMask = (1u << 30) - 1;
-constexpr uint32_t kLookbackPolls = 1u << 22;
+constexpr uint32_t kLookbackPolls = 1u << 22;  // default poll limit of one tile's look-back
+
+// Look-back wait settings of one digit pass: the poll limit, and (a test of the
+// failure path only) whether the pass's tile 0 withholds its published counts, so
+// that every look-back reaching it waits out the limit and reports a timeout.
+struct SortWait {
+    uint32_t poll_limit = kLookbackPolls;
+    uint32_t withhold_tile0 = 0;
+};
 
 // Exclusive prefix of each pass's 256 digit counts (one block per pass).
 static __global__ void __launch_bounds__(kRadix) k_scan_offsets(const uint32_t* __restrict__ hist,
@@ -57,7 +65,10 @@ constexpr size_t onesweep_smem() { return (size_t)kSortTile * sizeof(K) + (size_
 // One digit pass. Tiles are claimed in launch order through tile_counter, so a
 // tile only ever waits on tiles already owned by running blocks (which publish
 // their own counts before they wait): the look-back always completes; the poll
-// bound is a guard, not a scheduling assumption.
+// bound (wait.poll_limit polls of one tile, then CPT_STATUS_TIMEOUT and the tile
+// goes on with the prefix it has) is a guard, not a scheduling assumption. Output
+// positions stay inside [0, n) whatever prefix a timed-out tile uses, because a
+// prefix read from the look-back never exceeds the true one.
 template <typename K, bool kFirst>
 #ifndef CPT_SORT_MIN_BLOCKS
 #define CPT_SORT_MIN_BLOCKS 3  // 80 registers: three 4096-key tiles per SM (0.63 vs 0.67 ms per 5.2 M-key sort)
@@ -68,7 +79,7 @@ __global__ void __launch_bounds__(kSortBlock, CPT_SORT_MIN_BLOCKS) k_onesweep(co
                                                          int shift, const uint32_t* __restrict__ offsets,
                                                          uint32_t* __restrict__ lookback,
                                                          uint32_t* __restrict__ tile_counter,
-                                                         uint32_t* __restrict__ status)
+                                                         uint32_t* __restrict__ status, SortWait wait = SortWait())
 {
     extern __shared__ __align__(16) unsigned char smem[];
     K* s_keys = reinterpret_cast<K*>(smem);
@@ -123,7 +134,8 @@ __global__ void __launch_bounds__(kSortBlock, CPT_SORT_MIN_BLOCKS) k_onesweep(co
         count += c;
     }
     // Publish this tile's count as early as possible.
-    st_volatile(&lookback[(size_t)tile * kRadix + tid], (tile == 0 ? kFlagInc : kFlagAgg) | count);
+    if (tile != 0 || !wait.withhold_tile0)
+        st_volatile(&lookback[(size_t)tile * kRadix + tid], (tile == 0 ? kFlagInc : kFlagAgg) | count);
 
     // Tile-local exclusive scan of the digit counts (warp shuffles + warp totals).
     uint32_t x = count;
@@ -149,7 +161,7 @@ __global__ void __launch_bounds__(kSortBlock, CPT_SORT_MIN_BLOCKS) k_onesweep(co
             uint32_t v = ld_volatile(&lookback[(size_t)j * kRadix + tid]);
             uint32_t f = v & ~kValueMask;
             if (f == 0) {
-                if (++polls > kLookbackPolls) { timed_out = true; break; }
+                if (++polls > wait.poll_limit) { timed_out = true; break; }
                 if (polls > 32) __nanosleep(100);
                 continue;
             }

@@ -405,6 +405,7 @@ __global__ void __launch_bounds__(kSplitRefitBlock) k_split_refit(const cpt_tria
     const uint32_t n = *n_pieces;
     const uint32_t i = base + threadIdx.x;
     if (i >= n || n < 2) return;
+    if (sort_timed_out(status)) return;  // the pieces are not sorted: no tree to refit
     const uint32_t block_end = min(n, base + (uint32_t)kSplitRefitBlock);
     uint32_t src = order[i];
     if (src >= n) {
@@ -425,8 +426,9 @@ __global__ void __launch_bounds__(kSplitRefitBlock) k_split_refit(const cpt_tria
                       __fsub_rn(t.v2[0], t.v0[0]), __fsub_rn(t.v2[1], t.v0[1]), __fsub_rn(t.v2[2], t.v0[2])};
     uint32_t child = i;  // (the leaf box is published by the first arrival's release)
     uint32_t p = parents_leaf[i];
-    while (p != CPT_INVALID_INDEX) {
-        if (p >= n - 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
+    // at most n - 1 nodes on any walk (each node lets one arriver continue)
+    for (uint32_t steps = 0; p != CPT_INVALID_INDEX; ++steps) {
+        if (p >= n - 1 || steps >= n - 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
         float* node = nodes + 24 * (size_t)p;
         const float4 meta = *reinterpret_cast<const float4*>(node + 20);  // Node word, right child, range end
         const uint32_t word = __float_as_uint(meta.x);
@@ -826,6 +828,7 @@ __global__ void __launch_bounds__(kTreeletBlock) k_treelet(const uint32_t* __res
     __syncthreads();
     const uint32_t n = *n_pieces;
     if (n < 3) return;
+    if (sort_timed_out(status)) return;  // (uniform over the launch: set before it started)
     const int lane = threadIdx.x & 31;
     TreeletWarp& w = s_warp[threadIdx.x >> 5];
     const uint32_t i = blockIdx.x * kTreeletBlock + threadIdx.x;
@@ -887,287 +890,6 @@ __global__ void __launch_bounds__(kTreeletBlock) k_treelet(const uint32_t* __res
     }
 }
 
-// ---------------------------------------------------------------------------
-// Locally-ordered clustering (PLOC; Meister and Bittner, "Parallel Locally-Ordered
-// Clustering for Bounding Volume Hierarchy Construction", TVCG 2018), as an
-// alternative to the Karras topology for the split BVH. Clusters start as the
-// Morton-sorted pieces; every round, each cluster finds the neighbour within
-// kPlocRadius positions whose union box has the smallest surface area (ties: the
-// smaller pair hash; non-finite areas count as infinite); mutual nearest neighbours
-// merge into a new node that takes the lower position, the rest keep theirs, and
-// a compaction keeps the Morton order. The globally closest pair of any round is
-// mutual, so every round merges at least one pair.
-// Node ids: leaves 0..N-1, internal nodes N.. in creation order; the root is the
-// last one created. Traversal index of internal node N + k is (N - 2) - k, so the
-// root is 0.
-// ---------------------------------------------------------------------------
-constexpr int kPlocRadius = 16;
-
-__device__ __forceinline__ float union_area(float4 amn, float4 amx, float4 bmn, float4 bmx)
-{
-    const float dx = fmaxf(amx.x, bmx.x) - fminf(amn.x, bmn.x);
-    const float dy = fmaxf(amx.y, bmx.y) - fminf(amn.y, bmn.y);
-    const float dz = fmaxf(amx.z, bmx.z) - fminf(amn.z, bmn.z);
-    const float a = dx * dy + dy * dz + dz * dx;
-    return isfinite(a) ? a : INFINITY;
-}
-
-// Order of pairs with equal areas: a hash of the pair, the same from both ends, so
-// the order over pairs stays total (mutual pairs exist) and equal boxes pair up
-// like a random matching instead of chaining.
-__device__ __forceinline__ uint32_t pair_hash(uint32_t a, uint32_t b)
-{
-    uint32_t h = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u + (a << 6) + (a >> 2));
-    h ^= h >> 16;
-    h *= 0x85EBCA6Bu;
-    h ^= h >> 13;
-    h *= 0xC2B2AE35u;
-    h ^= h >> 16;
-    return h;
-}
-
-__global__ void __launch_bounds__(256) k_ploc_init(const float4* __restrict__ pieces, const uint32_t* __restrict__ order,
-                                                   const uint32_t* __restrict__ n_pieces, float4* __restrict__ nbox,
-                                                   uint32_t* __restrict__ clusters, uint32_t* __restrict__ leaf_tri,
-                                                   uint32_t* __restrict__ n_cur, uint32_t* __restrict__ status)
-{
-    const uint32_t n = *n_pieces;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) *n_cur = n;
-    if (i >= n) return;
-    uint32_t src = order[i];
-    if (src >= n) {
-        atomicOr(status, CPT_STATUS_BAD_INDEX);
-        src = n - 1;
-    }
-    const float4 a = pieces[2 * (size_t)src], b = pieces[2 * (size_t)src + 1];
-    nbox[2 * (size_t)i] = make_float4(a.x, a.y, a.z, 0.f);
-    nbox[2 * (size_t)i + 1] = make_float4(b.x, b.y, b.z, 0.f);
-    leaf_tri[i] = __float_as_uint(a.w);
-    clusters[i] = i;
-}
-
-__global__ void __launch_bounds__(kSplitBlock) k_ploc_nn(const uint32_t* __restrict__ clusters,
-                                                         const float4* __restrict__ nbox,
-                                                         const uint32_t* __restrict__ n_ptr, uint32_t* __restrict__ nn)
-{
-    __shared__ float4 s_mn[kSplitBlock + 2 * kPlocRadius], s_mx[kSplitBlock + 2 * kPlocRadius];
-    const int n = (int)*n_ptr;
-    const int base = (int)(blockIdx.x * kSplitBlock);
-    if (n <= 1 || base >= n) return;
-    for (int k = threadIdx.x; k < kSplitBlock + 2 * kPlocRadius; k += kSplitBlock) {
-        const int g = base - kPlocRadius + k;
-        if (g >= 0 && g < n) {
-            const uint32_t id = clusters[g];
-            s_mn[k] = nbox[2 * (size_t)id];
-            s_mx[k] = nbox[2 * (size_t)id + 1];
-        }
-    }
-    __syncthreads();
-    const int i = base + (int)threadIdx.x;
-    if (i >= n) return;
-    const int li = (int)threadIdx.x + kPlocRadius;
-    const float4 amn = s_mn[li], amx = s_mx[li];
-    float best = 0.f;
-    uint32_t bh = 0;
-    int bj = -1;
-#pragma unroll 4
-    for (int o = -kPlocRadius; o <= kPlocRadius; ++o) {
-        const int j = i + o;
-        if (o == 0 || j < 0 || j >= n) continue;
-        const float d = union_area(amn, amx, s_mn[li + o], s_mx[li + o]);
-        const uint32_t h = pair_hash((uint32_t)min(i, j), (uint32_t)max(i, j));
-        if (bj < 0 || d < best || (d == best && h < bh)) {
-            best = d;
-            bh = h;
-            bj = j;
-        }
-    }
-    nn[i] = (uint32_t)bj;
-}
-
-// Per 4096-cluster tile: merges created (mutual pairs, lower position) and clusters kept.
-__device__ __forceinline__ void ploc_flags(const uint32_t* nn, uint32_t i, bool& create, bool& keep)
-{
-    const uint32_t j = nn[i];
-    const bool mutual = nn[j] == i;
-    create = mutual && i < j;
-    keep = !(mutual && i > j);
-}
-
-__global__ void __launch_bounds__(kSplitBlock) k_ploc_count(const uint32_t* __restrict__ nn,
-                                                            const uint32_t* __restrict__ n_ptr,
-                                                            uint32_t* __restrict__ tile_create,
-                                                            uint32_t* __restrict__ tile_keep)
-{
-    const uint32_t n = *n_ptr;
-    if (n <= 1 || blockIdx.x * (uint32_t)kScanTile >= n) return;
-    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-    uint32_t packed = 0;
-    for (int k = 0; k < kScanItems; ++k) {
-        const uint32_t i = base + k;
-        if (i >= n) break;
-        bool c, kp;
-        ploc_flags(nn, i, c, kp);
-        packed += (c ? 1u << 16 : 0u) + (kp ? 1u : 0u);
-    }
-    uint32_t total;
-    block_exclusive_scan(packed, &total);
-    if (threadIdx.x == 0) {
-        tile_create[blockIdx.x] = total >> 16;
-        tile_keep[blockIdx.x] = total & 0xFFFFu;
-    }
-}
-
-// Exclusive scans of both tile arrays (one block); the create offsets continue the
-// running internal-node count. Writes the next round's cluster count.
-__global__ void __launch_bounds__(1024) k_ploc_scan(uint32_t* __restrict__ tile_create, uint32_t* __restrict__ tile_keep,
-                                                    const uint32_t* __restrict__ n_ptr, uint32_t* __restrict__ n_next,
-                                                    uint32_t* __restrict__ internal_count)
-{
-    __shared__ uint32_t s_c[1024], s_k[1024];
-    const uint32_t n = *n_ptr;
-    if (n <= 1) {
-        if (threadIdx.x == 0) *n_next = n;
-        return;
-    }
-    const uint32_t tiles = (n + kScanTile - 1) / kScanTile;
-    const uint32_t per = (tiles + 1023) / 1024;
-    const uint32_t created_before = *internal_count;
-    uint32_t lc = 0, lk = 0;
-    for (uint32_t k = 0; k < per; ++k) {
-        const uint32_t t = threadIdx.x * per + k;
-        if (t < tiles) { lc += tile_create[t]; lk += tile_keep[t]; }
-    }
-    s_c[threadIdx.x] = lc;
-    s_k[threadIdx.x] = lk;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t rc = 0, rk = 0;
-        for (int k = 0; k < 1024; ++k) {
-            const uint32_t c = s_c[k], kk = s_k[k];
-            s_c[k] = rc;
-            s_k[k] = rk;
-            rc += c;
-            rk += kk;
-        }
-        *n_next = rk;
-        *internal_count = created_before + rc;
-    }
-    __syncthreads();
-    uint32_t rc = created_before + s_c[threadIdx.x], rk = s_k[threadIdx.x];
-    for (uint32_t k = 0; k < per; ++k) {
-        const uint32_t t = threadIdx.x * per + k;
-        if (t < tiles) {
-            const uint32_t c = tile_create[t], kk = tile_keep[t];
-            tile_create[t] = rc;
-            tile_keep[t] = rk;
-            rc += c;
-            rk += kk;
-        }
-    }
-}
-
-__global__ void __launch_bounds__(kSplitBlock) k_ploc_merge(const uint32_t* __restrict__ clusters,
-                                                            const uint32_t* __restrict__ nn,
-                                                            const uint32_t* __restrict__ n_ptr,
-                                                            const uint32_t* __restrict__ tile_create,
-                                                            const uint32_t* __restrict__ tile_keep,
-                                                            float4* __restrict__ nbox, uint2* __restrict__ kids,
-                                                            uint32_t n_leaves_cap, const uint32_t* __restrict__ n_leaves,
-                                                            uint32_t* __restrict__ out, uint32_t* __restrict__ status)
-{
-    const uint32_t n = *n_ptr;
-    if (n <= 1 || blockIdx.x * (uint32_t)kScanTile >= n) return;
-    const uint32_t nl = *n_leaves;
-    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-    uint32_t packed = 0;
-    for (int k = 0; k < kScanItems; ++k) {
-        const uint32_t i = base + k;
-        if (i >= n) break;
-        bool c, kp;
-        ploc_flags(nn, i, c, kp);
-        packed += (c ? 1u << 16 : 0u) + (kp ? 1u : 0u);
-    }
-    uint32_t total;
-    const uint32_t ex = block_exclusive_scan(packed, &total);
-    uint32_t coff = tile_create[blockIdx.x] + (ex >> 16);
-    uint32_t koff = tile_keep[blockIdx.x] + (ex & 0xFFFFu);
-    for (int k = 0; k < kScanItems; ++k) {
-        const uint32_t i = base + k;
-        if (i >= n) break;
-        bool c, kp;
-        ploc_flags(nn, i, c, kp);
-        if (c) {
-            const uint32_t a = clusters[i], b = clusters[nn[i]];
-            const uint32_t id = nl + coff++;
-            if (coff > nl - 1 || nl > n_leaves_cap) {  // more merges than a binary tree has: impossible
-                atomicOr(status, CPT_STATUS_BAD_INDEX);
-                return;
-            }
-            const float4 amn = nbox[2 * (size_t)a], amx = nbox[2 * (size_t)a + 1];
-            const float4 bmn = nbox[2 * (size_t)b], bmx = nbox[2 * (size_t)b + 1];
-            // .w of the min corner: the subtree's height (leaves 0)
-            const float height = fmaxf(amn.w, bmn.w) + 1.0f;
-            nbox[2 * (size_t)id] = make_float4(fminf(amn.x, bmn.x), fminf(amn.y, bmn.y), fminf(amn.z, bmn.z), height);
-            nbox[2 * (size_t)id + 1] = make_float4(fmaxf(amx.x, bmx.x), fmaxf(amx.y, bmx.y), fmaxf(amx.z, bmx.z), 0.f);
-            kids[id - nl] = make_uint2(a, b);
-            out[koff++] = id;
-        } else if (kp) {
-            out[koff++] = clusters[i];
-        }
-    }
-}
-
-// The 96-B traversal nodes of the clustered tree.
-__global__ void __launch_bounds__(256) k_ploc_emit(const uint2* __restrict__ kids, const float4* __restrict__ nbox,
-                                                   const uint32_t* __restrict__ leaf_tri,
-                                                   const cpt_triangle* __restrict__ tris, uint32_t n_tris,
-                                                   const uint32_t* __restrict__ n_leaves, float* __restrict__ nodes,
-                                                   uint32_t* __restrict__ status)
-{
-    const uint32_t nl = *n_leaves;
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (nl < 2 || k >= nl - 1) return;
-    const uint2 ab = kids[k];
-    const uint32_t c[2] = {ab.x, ab.y};
-    uint32_t idx[2] = {0u, 0u};
-    bool internal[2];
-    float* node = nodes + 24 * (size_t)((nl - 2) - k);
-#pragma unroll
-    for (int side = 0; side < 2; ++side) {
-        float slot[10];
-        internal[side] = c[side] >= nl;
-        if (c[side] >= 2 * nl - 1) {
-            atomicOr(status, CPT_STATUS_BAD_INDEX);
-            return;
-        }
-        if (internal[side]) {
-            const float4 mn = nbox[2 * (size_t)c[side]], mx = nbox[2 * (size_t)c[side] + 1];
-            slot[0] = mn.x; slot[1] = mn.y; slot[2] = mn.z;
-            slot[3] = mx.x; slot[4] = mx.y; slot[5] = mx.z;
-            slot[6] = slot[7] = slot[8] = slot[9] = 0.f;
-            idx[side] = (nl - 2) - (c[side] - nl);
-        } else {
-            uint32_t tri = leaf_tri[c[side]];
-            if (tri >= n_tris) {
-                atomicOr(status, CPT_STATUS_BAD_INDEX);
-                tri = n_tris - 1;
-            }
-            const cpt_triangle t = tris[tri];
-            slot[0] = t.v0[0]; slot[1] = t.v0[1]; slot[2] = t.v0[2];
-            slot[3] = __uint_as_float(tri);
-            slot[4] = __fsub_rn(t.v1[0], t.v0[0]); slot[5] = __fsub_rn(t.v1[1], t.v0[1]);
-            slot[6] = __fsub_rn(t.v1[2], t.v0[2]);
-            slot[7] = __fsub_rn(t.v2[0], t.v0[0]); slot[8] = __fsub_rn(t.v2[1], t.v0[1]);
-            slot[9] = __fsub_rn(t.v2[2], t.v0[2]);
-        }
-        store_slot(node, side, slot);
-    }
-    const uint32_t word = (idx[0] << 2) | (internal[1] ? 2u : 0u) | (internal[0] ? 1u : 0u);
-    reinterpret_cast<float4*>(node)[5] = make_float4(__uint_as_float(word), __uint_as_float(idx[1]), 0.f, 0.f);
-}
-
 template <typename K>
 struct SplitScratch {
     double* partial;
@@ -1189,20 +911,10 @@ struct SplitScratch {
     cpt_bbox* node_boxes;
     float4* leaf_boxes;
     uint2* info;  // treelet restructuring: per internal node (leaves, height)
-    // clustering (CPT_SPLIT_PLOC)
-    float4* nbox;
-    uint32_t* clusters[2];
-    uint32_t* nn;
-    uint2* kids;
-    uint32_t* leaf_tri;
-    uint32_t* tile_create;
-    uint32_t* tile_keep;
-    uint32_t* n_round;  // [2] cluster counts, ping-pong
-    uint32_t* internal_count;
 };
 
 template <typename K>
-size_t split_layout(uint32_t n, uint32_t cap, bool ploc, bool treelet, void* base, SplitScratch<K>* out)
+size_t split_layout(uint32_t n, uint32_t cap, bool treelet, void* base, SplitScratch<K>* out)
 {
     constexpr int P = KeyTraits<K>::passes;
     Carver c(base);
@@ -1227,30 +939,9 @@ size_t split_layout(uint32_t n, uint32_t cap, bool ploc, bool treelet, void* bas
     s.parents_leaf = c.take<uint32_t>(cap);
     s.parents_internal = c.take<uint32_t>(cap);
     s.counters = c.take<int>(cap);
-    if (ploc) {
-        const size_t ptiles = (cap + kScanTile - 1) / kScanTile;
-        s.node_boxes = nullptr;
-        s.leaf_boxes = nullptr;
-        s.info = nullptr;
-        s.nbox = c.take<float4>(4ull * cap);
-        s.clusters[0] = c.take<uint32_t>(cap);
-        s.clusters[1] = c.take<uint32_t>(cap);
-        s.nn = c.take<uint32_t>(cap);
-        s.kids = c.take<uint2>(cap);
-        s.leaf_tri = c.take<uint32_t>(cap);
-        s.tile_create = c.take<uint32_t>(ptiles);
-        s.tile_keep = c.take<uint32_t>(ptiles);
-        s.n_round = c.take<uint32_t>(2);
-        s.internal_count = c.take<uint32_t>(1);
-    } else {
-        s.node_boxes = c.take<cpt_bbox>(cap);
-        s.leaf_boxes = c.take<float4>(2ull * cap);
-        s.info = treelet ? c.take<uint2>(cap) : nullptr;
-        s.nbox = nullptr;
-        s.clusters[0] = s.clusters[1] = s.nn = s.leaf_tri = s.tile_create = s.tile_keep = nullptr;
-        s.kids = nullptr;
-        s.n_round = s.internal_count = nullptr;
-    }
+    s.node_boxes = c.take<cpt_bbox>(cap);
+    s.leaf_boxes = c.take<float4>(2ull * cap);
+    s.info = treelet ? c.take<uint2>(cap) : nullptr;
     if (out) *out = s;
     return c.used();
 }
@@ -1261,66 +952,14 @@ inline uint64_t split_capacity(uint32_t n, float extra_ratio)
     return (uint64_t)n + (uint64_t)floor(r * (double)n);
 }
 
-int ploc_impl(cpt_bvh* bvh, uint32_t cap, const float4* pieces, const uint32_t* order, const uint32_t* n_pieces,
-              float4* nbox, uint32_t* const clusters[2], uint32_t* nn, uint2* kids, uint32_t* leaf_tri,
-              uint32_t* tile_create, uint32_t* tile_keep, uint32_t* n_round, uint32_t* internal_count, void* nodes,
-              cudaStream_t stream)
-{
-    const uint32_t blocks256 = (cap + 255) / 256, tiles = (cap + kScanTile - 1) / kScanTile;
-    CPT_CUDA_TRY(cudaMemsetAsync(internal_count, 0, sizeof(uint32_t), stream));
-    k_ploc_init<<<blocks256, 256, 0, stream>>>(pieces, order, n_pieces, nbox, clusters[0], leaf_tri, n_round,
-                                               bvh->status);
-    CPT_LAUNCH_CHECK();
-    // Rounds run in batches; a round on a single cluster does nothing, so a batch
-    // may overrun the end. The count is checked on the host between batches.
-    constexpr int kBatch = 6;
-    constexpr int kMaxRounds = 1 << 16;  // a round merges at least one pair: n - 1 rounds at most
-    int round = 0;
-    uint32_t left = 2;
-    while (left > 1) {
-        for (int b = 0; b < kBatch; ++b, ++round) {
-            const uint32_t* cin = clusters[round & 1];
-            uint32_t* cout = clusters[(round + 1) & 1];
-            const uint32_t* ncur = n_round + (round & 1);
-            uint32_t* nnext = n_round + ((round + 1) & 1);
-            k_ploc_nn<<<blocks256, kSplitBlock, 0, stream>>>(cin, nbox, ncur, nn);
-            CPT_LAUNCH_CHECK();
-            k_ploc_count<<<tiles, kSplitBlock, 0, stream>>>(nn, ncur, tile_create, tile_keep);
-            CPT_LAUNCH_CHECK();
-            k_ploc_scan<<<1, 1024, 0, stream>>>(tile_create, tile_keep, ncur, nnext, internal_count);
-            CPT_LAUNCH_CHECK();
-            k_ploc_merge<<<tiles, kSplitBlock, 0, stream>>>(cin, nn, ncur, tile_create, tile_keep, nbox, kids, cap,
-                                                            n_pieces, cout, bvh->status);
-            CPT_LAUNCH_CHECK();
-        }
-        CPT_CUDA_TRY(cudaMemcpyAsync(&left, n_round + (round & 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-        CPT_CUDA_TRY(cudaStreamSynchronize(stream));
-        if (round > kMaxRounds) return CPT_ERR_CUDA;
-    }
-    // Traversal keeps at most one pending node per level: a tree taller than the
-    // stack is refused (the caller keeps traversing the LBVH).
-    float root_min[4];
-    CPT_CUDA_TRY(cudaMemcpyAsync(&left, n_pieces, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-    CPT_CUDA_TRY(cudaStreamSynchronize(stream));
-    if (left < 2) return CPT_ERR_INVALID_ARGUMENT;
-    CPT_CUDA_TRY(cudaMemcpyAsync(root_min, nbox + 2 * (size_t)(2 * left - 2), sizeof(root_min), cudaMemcpyDeviceToHost,
-                                 stream));
-    CPT_CUDA_TRY(cudaStreamSynchronize(stream));
-    if (!(root_min[3] <= (float)CPT_TRAVERSAL_STACK)) return CPT_ERR_TREE_TOO_DEEP;
-    k_ploc_emit<<<blocks256, 256, 0, stream>>>(kids, nbox, leaf_tri, bvh->tris, bvh->n, n_pieces,
-                                               static_cast<float*>(nodes), bvh->status);
-    CPT_LAUNCH_CHECK();
-    return CPT_OK;
-}
-
 template <typename K>
-int split_impl(cpt_bvh* bvh, uint32_t cap, bool ploc, bool treelet, void* nodes, void* scratch,
+int split_impl(cpt_bvh* bvh, uint32_t cap, bool treelet, void* nodes, void* scratch,
                cudaStream_t stream)
 {
     constexpr int P = KeyTraits<K>::passes;
     const uint32_t n = bvh->n;
     SplitScratch<K> s;
-    split_layout<K>(n, cap, ploc, treelet, scratch, &s);
+    split_layout<K>(n, cap, treelet, scratch, &s);
     const uint32_t ctiles = (n + kScanTile - 1) / kScanTile;
     const double extra = (double)(cap - n);
     CPT_CUDA_TRY(cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * P * kRadix, stream));
@@ -1364,10 +1003,9 @@ int split_impl(cpt_bvh* bvh, uint32_t cap, bool ploc, bool treelet, void* nodes,
     }
     const uint32_t* order = s.vals[(P - 1) & 1];
     const K* keys = s.keys[P & 1];
-    if (ploc) return ploc_impl(bvh, cap, s.pieces, order, s.n_pieces, s.nbox, s.clusters, s.nn, s.kids, s.leaf_tri,
-                               s.tile_create, s.tile_keep, s.n_round, s.internal_count, nodes, stream);
     k_topology<K><<<(cap + 255) / 256, 256, 0, stream>>>(keys, 0, s.n_pieces, s.children, s.parents_leaf,
-                                                          s.parents_internal, s.counters, static_cast<float4*>(nodes));
+                                                          s.parents_internal, s.counters, static_cast<float4*>(nodes),
+                                                          bvh->status);
     CPT_LAUNCH_CHECK();
     k_split_refit<<<(cap + kSplitRefitBlock - 1) / kSplitRefitBlock, kSplitRefitBlock, 0, stream>>>(
         bvh->tris, s.pieces, order, s.n_pieces, s.children,
@@ -1397,13 +1035,13 @@ extern "C" size_t cpt_lbvh_split_bytes(uint32_t n, int morton_bits, float extra_
 {
     if (n < 2 || n > kMaxTriangles || (morton_bits != 30 && morton_bits != 63)) return 0;
     if (!(extra_ratio >= 0.f) || !(extra_ratio <= 64.f)) return 0;  // the range cpt_lbvh_split accepts
-    const bool ploc = flags & CPT_SPLIT_PLOC, treelet = flags & CPT_SPLIT_TREELET;
-    if ((flags & ~(CPT_SPLIT_PLOC | CPT_SPLIT_TREELET)) || (ploc && treelet)) return 0;
+    const bool treelet = flags & CPT_SPLIT_TREELET;
+    if (flags & ~CPT_SPLIT_TREELET) return 0;
     const uint64_t cap = split_capacity(n, extra_ratio);
     if (cap >= (1ull << 31)) return 0;
     if (node_bytes) *node_bytes = align_up((size_t)(cap - 1) * 96, 256);
-    return morton_bits == 30 ? split_layout<uint32_t>(n, (uint32_t)cap, ploc, treelet, nullptr, nullptr)
-                             : split_layout<uint64_t>(n, (uint32_t)cap, ploc, treelet, nullptr, nullptr);
+    return morton_bits == 30 ? split_layout<uint32_t>(n, (uint32_t)cap, treelet, nullptr, nullptr)
+                             : split_layout<uint64_t>(n, (uint32_t)cap, treelet, nullptr, nullptr);
 }
 
 extern "C" int cpt_lbvh_split(cpt_bvh* bvh, float extra_ratio, uint32_t flags, void* nodes, size_t node_bytes,
@@ -1419,9 +1057,9 @@ extern "C" int cpt_lbvh_split(cpt_bvh* bvh, float extra_ratio, uint32_t flags, v
     if ((reinterpret_cast<uintptr_t>(nodes) & 15) || (reinterpret_cast<uintptr_t>(scratch) & 255))
         return CPT_ERR_INVALID_ARGUMENT;
     const uint32_t cap = (uint32_t)split_capacity(bvh->n, extra_ratio);
-    const bool ploc = flags & CPT_SPLIT_PLOC, treelet = flags & CPT_SPLIT_TREELET;
-    const int rc = bvh->morton_bits == 30 ? split_impl<uint32_t>(bvh, cap, ploc, treelet, nodes, scratch, stream)
-                                          : split_impl<uint64_t>(bvh, cap, ploc, treelet, nodes, scratch, stream);
+    const bool treelet = flags & CPT_SPLIT_TREELET;
+    const int rc = bvh->morton_bits == 30 ? split_impl<uint32_t>(bvh, cap, treelet, nodes, scratch, stream)
+                                          : split_impl<uint64_t>(bvh, cap, treelet, nodes, scratch, stream);
     if (rc) return rc;
     bvh->split_nodes = nodes;
     bvh->split_capacity = cap;

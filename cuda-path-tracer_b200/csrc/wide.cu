@@ -152,6 +152,10 @@ __global__ void __launch_bounds__(kWideBlock) k_wide_level(const float4* __restr
 {
     __shared__ float s_box[8 * 6][kWideBlock];
     __shared__ uint32_t s_ref[8][kWideBlock];
+    // A sort of the build (or of the split tree) gave up a look-back wait: the binary
+    // tree is not one. Every block leaves (the word was set before this launch), so
+    // the level counters keep their initial values and no node is written.
+    if (__ldcg(status) & CPT_STATUS_TIMEOUT) return;
     const uint32_t start = ctr[4 + level], end = ctr[4 + level + 1];
     const float m = __uint_as_float(ctr[3]);
     const int t = threadIdx.x;

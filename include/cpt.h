@@ -95,6 +95,17 @@ int cpt_bvh_bind(void* mem, size_t bytes, uint32_t n, int morton_bits, cpt_bvh* 
 size_t cpt_lbvh_scratch_bytes(uint32_t n, int morton_bits);
 
 #define CPT_BUILD_CHECK 1u /* synchronize, map device status to a code, verify the root box */
+/* The sort's decoupled look-back is the build's only device-side wait; it gives up
+ * after a poll limit per tile, records CPT_STATUS_TIMEOUT, and the build's later
+ * kernels then return at once (the call, or cpt_status_check, reports
+ * CPT_ERR_DEVICE_TIMEOUT). CPT_BUILD_LOOKBACK_LIMIT(k), k in 1..31, sets the limit to
+ * 2^k polls (default 2^22, k = 0). CPT_BUILD_TEST_WITHHOLD exercises that failure
+ * path without a fault: the first sort pass's first tile never publishes its digit
+ * counts, so every look-back that reaches it waits out the limit; it requires an
+ * explicit limit of at most 2^16 polls (else CPT_ERR_INVALID_ARGUMENT). Other flag
+ * bits are refused. */
+#define CPT_BUILD_TEST_WITHHOLD 2u
+#define CPT_BUILD_LOOKBACK_LIMIT(k) (((uint32_t)(k) & 31u) << 8)
 
 /* Builds the LBVH of n >= 2 triangles.
  * Replaces CUDA::BVHBuilder::build (source/application/cuda/BVHBuilder.h:15,
@@ -120,7 +131,10 @@ int cpt_lbvh_build(const cpt_triangle* tris_in, uint32_t n, const float* enclosi
  *    that loads the library and held until the process exits;
  *  - the first call on a device looks up the array's device address with that
  *    device current (cudaGetSymbolAddress) — make that first call before any
- *    stream capture;
+ *    stream capture. The address is kept for the life of the process: after a
+ *    cudaDeviceReset (or anything else that destroys and recreates the device's
+ *    primary context) the library's device image is loaded anew and the kept
+ *    address is stale, so do not call this entry point on that device again;
  *  - all calls share the one array: calls whose work overlaps on a GPU (e.g. on
  *    two streams) race; serialize them. Each call zeroes what must start at zero,
  *    so leftovers of the previous call are harmless. */
@@ -145,9 +159,8 @@ int cpt_lbvh_build_static(const cpt_triangle* tris_in, uint32_t n, const float* 
  * passes the call. */
 #define CPT_SPLIT_TREELET 2u /* treelet restructuring of the Karras topology (treelets of up to 7 leaves, least
                                * total node surface area, never taller; Karras and Aila 2013 — the optimisation
-                               * the reference's README cites): fewer node visits, longer build. Not with PLOC */
-#define CPT_SPLIT_PLOC 1u /* pieces clustered by surface area (locally-ordered clustering, search radius 16
-                             * in Morton order) instead of the Karras topology: fewer node visits, longer build */
+                               * the reference's README cites): fewer node visits, longer build. Other flag
+                               * bits are refused (CPT_ERR_INVALID_ARGUMENT; 0 from cpt_lbvh_split_bytes) */
 size_t cpt_lbvh_split_bytes(uint32_t n, int morton_bits, float extra_ratio, uint32_t flags, size_t* node_bytes);
 int cpt_lbvh_split(cpt_bvh* bvh, float extra_ratio, uint32_t flags, void* nodes, size_t node_bytes, void* scratch,
                    size_t scratch_bytes, cudaStream_t stream);
@@ -369,16 +382,18 @@ int cpt_tracer_read_image(cpt_tracer* t, float* rgba_host);
 int cpt_tracer_resolve(cpt_tracer* t, float* rgba_dev);
 /* Checkpoint / resume of the progressive image (the reference loses it on exit).
  * get: copies the accumulator of the last raytrace (cpt_accum_bytes(width, height,
- * accum_mode) bytes, the layout of the tracer's accum mode) and the frame counter to
- * host memory; synchronizes. set: restores them for a width x height image, so that the
- * next cpt_tracer_raytrace at that size continues from frame `frame`; synchronizes.
- * Resuming gives the same image as an uninterrupted run when the scene, camera and
- * settings (cpt_tracer_set_settings, cpt_tracer_set_nee) are those of the saved run;
- * apply the settings before set, which reads the accumulator in the current accum mode
- * (the Kahan and FP64 layouts have the same size, so a mode mismatch is not detected). */
-int cpt_tracer_get_progress(cpt_tracer* t, void* accum_host, size_t bytes, uint32_t* frame);
+ * accum_mode) bytes, the layout of the tracer's accum mode), the frame counter and
+ * that accum mode (CPT_ACCUM_*) to host memory; synchronizes. set: restores them for a
+ * width x height image, so that the next cpt_tracer_raytrace at that size continues
+ * from frame `frame`; synchronizes. set refuses (CPT_ERR_INVALID_ARGUMENT) an
+ * accum_mode other than the tracer's current one: the Kahan and FP64 layouts have the
+ * same size, so the mode is checked rather than inferred. Resuming gives the same image
+ * as an uninterrupted run when the scene, camera and settings (cpt_tracer_set_settings,
+ * cpt_tracer_set_nee) are those of the saved run; apply the settings before set. A set
+ * that fails leaves the tracer without an image (its next raytrace starts at frame 0). */
+int cpt_tracer_get_progress(cpt_tracer* t, void* accum_host, size_t bytes, uint32_t* frame, uint32_t* accum_mode);
 int cpt_tracer_set_progress(cpt_tracer* t, const void* accum_host, size_t bytes, uint32_t width, uint32_t height,
-                            uint32_t frame);
+                            uint32_t frame, uint32_t accum_mode);
 /* Rays traced since upload (primary, extension, shadow); synchronizes. */
 int cpt_tracer_ray_counts(cpt_tracer* t, unsigned long long out[3]);
 cudaStream_t cpt_tracer_stream(cpt_tracer* t);

@@ -81,6 +81,8 @@ def ref_lib(bits: int = 30) -> ctypes.CDLL:
         L.ref_trace.argtypes = [P, U, P, P, P, I]
         L.ref_render.argtypes = [P, P, U, U, U, U, U, U, U, U, F, I, U, U, P, P, P, I]
         L.ref_render.restype = I
+        L.ref_render_rows.argtypes = [P, P, U, U, U, P, U, U, U, U, F, I, U, U, P, P, P, I]
+        L.ref_render_rows.restype = I
         _ref[bits] = L
     return _ref[bits]
 
@@ -292,6 +294,41 @@ def ref_render(b: BuildResult, infos: np.ndarray, lights, width: int, height: in
     L.ref_render(_p(infos), _p(lights) if nl else None, nl, width, height, r0, r1, spp, frame0, bounces, intensity,
                  int(stratified), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, _p(cam15), _p(out), _p(counts),
                  threads)
+    return out, counts
+
+
+def ref_render_rows(b: BuildResult, infos: np.ndarray, lights, width: int, height: int, rows, spp: int, frame0: int,
+                    bounces: int, intensity: float, stratified: bool, seed: int, cam15: np.ndarray, threads: int = 0,
+                    bits: int = 30):
+    """Reference-function integrator over a list of rows: per-pixel float64 sums of
+    the spp samples (sample order), shape (len(rows), width, 3); ray counts."""
+    L = ref_lib(bits)
+    L.ref_set_geometry(_p(b.tris), _p(b.children), _p(b.node_boxes), len(b.tris))
+    rows = np.ascontiguousarray(rows, np.uint32)
+    out = np.zeros((len(rows), width, 3), np.float64)
+    counts = np.zeros(3, np.uint64)
+    nl = 0 if lights is None else len(lights)
+    cam15 = np.ascontiguousarray(cam15, np.float32)
+    rc = L.ref_render_rows(_p(infos), _p(lights) if nl else None, nl, width, height, _p(rows), len(rows), spp, frame0,
+                           bounces, intensity, int(stratified), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, _p(cam15),
+                           _p(out), _p(counts), threads)
+    if rc != 0:
+        raise ValueError("ref_render_rows: a row index is outside the image")
+    return out, counts
+
+
+def render_rows(b: BuildResult, infos: np.ndarray, width: int, height: int, rows, spp: int, frame0: int, bounces: int,
+                intensity: float, stratified: bool, seed: int, cam: OCam):
+    """The oracle's integrator over a list of rows, float64 per-pixel sums (as
+    ref_render_rows); ray counts."""
+    out = np.zeros((len(rows), width, 3), np.float64)
+    counts = np.zeros(3, np.uint64)
+    for k, y in enumerate(rows):
+        rad, cnt = render(b, infos, None, width, height, spp, frame0, bounces, intensity, stratified, seed, cam,
+                          rows=(int(y), int(y) + 1))
+        for x in rad:  # sample order
+            out[k] += x[0].astype(np.float64)
+        counts += cnt
     return out, counts
 
 

@@ -288,4 +288,54 @@ int ref_render(const void* infos, const void* lights, uint32_t light_count,
     return 0;
 }
 
+// The same integrator over an arbitrary list of rows (e.g. every k-th row of the
+// frame, a sample spread over the whole image), each pixel's samples summed in
+// sample order in float64 (the device's FP64 accumulator adds the same float
+// radiance values in the same order). sum_out: 3 doubles per pixel, rows in list
+// order. Returns -1 for a row outside the image. Needs ref_set_geometry first.
+int ref_render_rows(const void* infos, const void* lights, uint32_t light_count,
+                    uint32_t width, uint32_t height, const uint32_t* rows, uint32_t row_count,
+                    uint32_t spp, uint32_t frame0, uint32_t bounces, float intensity, int stratified,
+                    uint32_t key0, uint32_t key1, const float* cam, double* sum_out,
+                    uint64_t* ray_counts, int threads)
+{
+    if (!rows || !sum_out) return -1;
+    for (uint32_t r = 0; r < row_count; ++r)
+        if (rows[r] >= height) return -1;
+    if (threads > 0) omp_set_num_threads(threads);
+    RefShadeCtx c{static_cast<const CUDA::TriangleInfo*>(infos),
+                  static_cast<const CUDA::DirectionalLight*>(lights), light_count, bounces, intensity,
+                  stratified != 0};
+    glm::vec3 eye(cam[0], cam[1], cam[2]);
+    glm::vec3 d00(cam[3], cam[4], cam[5]), d10(cam[6], cam[7], cam[8]);
+    glm::vec3 d11(cam[9], cam[10], cam[11]), d01(cam[12], cam[13], cam[14]);
+    uint64_t tot[3] = {0, 0, 0};
+    const long total = (long)row_count * width;
+#pragma omp parallel
+    {
+        uint64_t local[3] = {0, 0, 0};
+#pragma omp for schedule(dynamic, 16)
+        for (long q = 0; q < total; ++q) {
+            uint32_t x = (uint32_t)(q % width), y = rows[q / width];
+            long p = (long)y * width + x;
+            double sum[3] = {0.0, 0.0, 0.0};
+            for (uint32_t s = 0; s < spp; ++s) {
+                // cuda_path_tracer.cu:404-407 with lerpDirection :376-379
+                glm::vec2 tc(x / (float)width, y / (float)height);
+                CUDA::Ray ray;
+                ray.direction = glm::lerp(glm::lerp(d00, d10, tc.x), glm::lerp(d01, d11, tc.x), tc.y);
+                ray.origin = eye;
+                glm::vec3 v = path_trace(c, ray, (uint32_t)p, frame0 + s, key0, key1, local);
+                sum[0] += (double)v.x; sum[1] += (double)v.y; sum[2] += (double)v.z;
+            }
+            double* o = sum_out + 3 * q;
+            o[0] = sum[0]; o[1] = sum[1]; o[2] = sum[2];
+        }
+#pragma omp critical
+        { tot[0] += local[0]; tot[1] += local[1]; tot[2] += local[2]; }
+    }
+    if (ray_counts) { ray_counts[0] = tot[0]; ray_counts[1] = tot[1]; ray_counts[2] = tot[2]; }
+    return 0;
+}
+
 }  // extern "C"

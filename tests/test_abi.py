@@ -79,6 +79,12 @@ def test_build_rejects_bad_arguments_without_device_work():
     with pytest.raises(cpt.CptError) as e:  # misaligned triangle pointer
         cpt.lbvh_build(260, 100, 30, b, 1 << 30, 1 << 30)
     assert e.value.code == cpt.ERR_INVALID_ARGUMENT
+    # flag bits: unknown ones, and the look-back test hook without a short explicit
+    # poll limit (none, or above 2^16 polls), are refused before any device work
+    for flags in (4, 1 << 16, cpt.BUILD_TEST_WITHHOLD, cpt.BUILD_TEST_WITHHOLD | cpt.build_lookback_limit(17)):
+        with pytest.raises(cpt.CptError) as e:
+            cpt.lbvh_build(256, 100, 30, b, 1 << 30, 1 << 30, flags=flags)
+        assert e.value.code == cpt.ERR_INVALID_ARGUMENT, flags
 
 
 def test_static_build_limits_without_device_work():
@@ -100,7 +106,8 @@ def test_static_build_limits_without_device_work():
 @pytest.mark.parametrize("bits", [30, 63])
 def test_split_sizes_and_flags(bits):
     # split tree sizing (host-only): records for the pieces, scratch per piece, 8 B more
-    # per piece with treelet restructuring; unknown flags and PLOC + treelets refused
+    # per piece with treelet restructuring; unknown flags (bit 0 once chose a clustered
+    # topology, since removed) refused
     def sizes(n, ratio, flags):
         nb = ctypes.c_size_t()
         sb = cpt.lib.cpt_lbvh_split_bytes(n, bits, ctypes.c_float(ratio), flags, ctypes.byref(nb))
@@ -111,10 +118,10 @@ def test_split_sizes_and_flags(bits):
         cap = n + int(np.floor(ratio * n))
         s0, nb0 = sizes(n, ratio, 0)
         s1, nb1 = sizes(n, ratio, cpt.SPLIT_TREELET)
-        sp, nbp = sizes(n, ratio, cpt.SPLIT_PLOC)
-        assert nb0 == nb1 == nbp >= (cap - 1) * 96
-        assert s0 > 0 and s1 - s0 >= 8 * cap and sp > 0
-    assert sizes(n, 1.0, cpt.SPLIT_TREELET | cpt.SPLIT_PLOC)[0] == 0
+        assert nb0 == nb1 >= (cap - 1) * 96
+        assert s0 > 0 and s1 - s0 >= 8 * cap
+    assert sizes(n, 1.0, 1)[0] == 0
+    assert sizes(n, 1.0, cpt.SPLIT_TREELET | 1)[0] == 0
     assert sizes(n, 1.0, 4)[0] == 0
     assert sizes(1, 1.0, 0)[0] == 0
     # ratios cpt_lbvh_split refuses get no size either (0..64, not NaN or infinite)
@@ -175,8 +182,8 @@ def test_every_entry_point_refuses_null_arguments():
         "cpt_tracer_set_camera": lambda: L.cpt_tracer_set_camera(None, None),
         "cpt_tracer_set_settings": lambda: L.cpt_tracer_set_settings(None, 1, 3.0, 1, 0, 0, 0),
         "cpt_tracer_ray_counts": lambda: L.cpt_tracer_ray_counts(None, None),
-        "cpt_tracer_get_progress": lambda: L.cpt_tracer_get_progress(None, None, 0, None),
-        "cpt_tracer_set_progress": lambda: L.cpt_tracer_set_progress(None, None, 0, 8, 8, 1),
+        "cpt_tracer_get_progress": lambda: L.cpt_tracer_get_progress(None, None, 0, None, None),
+        "cpt_tracer_set_progress": lambda: L.cpt_tracer_set_progress(None, None, 0, 8, 8, 1, 0),
         "cpt_tracer_resolve": lambda: L.cpt_tracer_resolve(None, None),
     }
     for name, call in calls.items():

@@ -1,0 +1,158 @@
+"""Parity at the benchmark's own configurations and on the benchmark's traversal.
+
+* The small plain-method configuration exactly as the benchmark runs it: 65,536
+  random triangles + the 2-triangle emitter quad, 30-bit keys, 512 x 512, 1 sample,
+  depth 4, seed 0. Keys, sorted order, topology and boxes bit-exact against the
+  oracle; the image (Kahan accumulator), its compensation plane and the ray counts
+  bit-exact against the oracle's restatement of the integrator, and against the
+  same loop over the reference's own trace functions (oracle/_ref) where built.
+* The large configuration's traversal (a treelet-restructured split BVH at 8.0
+  extra pieces per triangle under the compressed 8-wide tree) over a 1.31 M-triangle
+  sphere + hairball: the closest-hit triangle equals the oracle's reference
+  traversal except for rays whose two nearest hits lie within 1 ulp of each other
+  (counted, required rare, and each alternative checked to be a real hit there).
+* The deforming-mesh step (cpt_scene_deform) against a float64 host restatement,
+  and the rebuild of the deformed mesh bit-exact against the oracle.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import cpt
+from cpt.device import DeviceLbvh, DeviceRenderer, DeviceScene, make_params, stream_handle, to_device
+from oracle import cpu
+from test_gpu_build import assert_same_as
+from test_gpu_split import tie_or_equal
+
+pytestmark = pytest.mark.gpu
+
+
+def test_c1_as_configured_is_bit_exact(cuda):
+    W = H = 512
+    tris, infos = cpt.scene_random(65536, seed=0)
+    assert len(tris) == 65538
+    lb = DeviceLbvh(len(tris), 30)
+    lb.build(to_device(tris), check_root=True)
+    ob = cpu.build(tris, 30)
+    assert_same_as(lb.download(), ob)
+
+    cam = cpt.camera_look_at((0.5, 0.5, -1.2), (0.5, 0.5, 0.0), fov_deg=45.0, aspect=1.0)
+    r = DeviceRenderer(make_params(W, H, 1, 0, 3, 3.0, True, 0, cpt.ACCUM_KAHAN))
+    r.render(lb, DeviceScene(infos), cam)
+    torch.cuda.synchronize()
+    r.check_status()
+    acc = r.accum.cpu().numpy().view(np.float32).reshape(2, H, W, 4)
+    rad, counts = cpu.render(ob, infos, None, W, H, 1, 0, 3, 3.0, True, 0, cpu.ocam_from(cam.eye, cam.as_array()[3:]))
+    s, c, n = cpu.accumulate_kahan(rad)
+    assert (s > 0).any(), "the image should receive light"
+    assert acc[0, ..., :3].tobytes() == s.tobytes()
+    assert acc[1, ..., :3].tobytes() == c.tobytes()
+    assert np.all(acc[0, ..., 3] == n)
+    assert np.array_equal(r.counts.cpu().numpy()[:3].astype(np.uint64), counts)
+    if cpu.ref_available(30):  # the reference's own CUDA::trace / computeL / TriangleInfo code, compiled here
+        rs, rc = cpu.ref_render(ob, infos, None, W, H, (0, H), 1, 0, 3, 3.0, True, 0, cam.as_array())
+        assert acc[0, ..., :3].tobytes() == rs.tobytes()  # one sample: the Kahan sum is the sample itself
+        assert np.array_equal(r.counts.cpu().numpy()[:3].astype(np.uint64), rc)
+
+
+def primary_rays(cam, width, height, m, seed):
+    """m primary rays of the camera through random pixels, as the renderer forms them
+    (bilinear blend of the corner directions at x / W, y / H)."""
+    g = np.random.default_rng(seed)
+    x = g.integers(0, width, m).astype(np.float32) / np.float32(width)
+    y = g.integers(0, height, m).astype(np.float32) / np.float32(height)
+    d = cam.as_array()[3:].reshape(4, 3)  # 00, 10, 11, 01
+    top = d[0] + (d[1] - d[0]) * x[:, None]
+    bot = d[3] + (d[2] - d[3]) * x[:, None]
+    r = np.zeros((m, 8), np.float32)
+    r[:, 0:3] = cam.as_array()[:3]
+    r[:, 4:7] = top + (bot - top) * y[:, None]
+    return r
+
+
+def scattered_rays(m, seed):
+    g = np.random.default_rng(seed)
+    o = g.uniform(-1.3, 1.3, (m, 3))
+    d = g.normal(size=(m, 3))
+    r = np.zeros((m, 8), np.float32)
+    r[:, 0:3] = o
+    r[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    return r
+
+
+def mt_hit64(tri, o, d):
+    """Moller-Trumbore in float64 (intersection.h:28-59): (t, u, v) per ray."""
+    p0, p1, p2 = (tri[k].astype(np.float64) for k in ("v0", "v1", "v2"))
+    e1, e2 = p1 - p0, p2 - p0
+    q = np.cross(d, e2)
+    det = (e1 * q).sum(1)
+    inv = 1.0 / det
+    s = o - p0
+    u = inv * (s * q).sum(1)
+    rr = np.cross(s, e1)
+    v = inv * (d * rr).sum(1)
+    t = inv * (e2 * rr).sum(1)
+    return t, u, v
+
+
+def test_benchmark_traversal_matches_reference_hits_at_scale(cuda):
+    tris = cpt.scene_sphere_hairball(1024, 512, 1 << 18, seed=0)[0]
+    n = len(tris)
+    assert n >= 1_300_000
+    lb = DeviceLbvh(n, 63)
+    lb.build(to_device(tris), check_root=True)
+    lb.split(8.0, flags=cpt.SPLIT_TREELET)
+    lb.wide()
+    cam = cpt.camera_look_at((0.0, 0.35, -3.6), (0.0, 0.0, 0.0), fov_deg=45.0, aspect=1920 / 1080)
+    rays = np.concatenate([primary_rays(cam, 1920, 1080, 150_000, 1), scattered_rays(100_000, 2)])
+    h, _ = lb.trace(torch.from_numpy(rays).cuda())
+    torch.cuda.synchronize()
+    lb.status()
+    hg = h.cpu().numpy()
+    ob = cpu.build(tris, 63)
+    t, idx, uv = cpu.trace(ob, rays[:, [0, 1, 2, 4, 5, 6]])
+    ho = np.stack([t, uv[:, 0], uv[:, 1], idx.view(np.float32)], 1)
+    ok, exact = tie_or_equal(hg, ho, ulps=1)
+    assert ok.all(), f"{int((~ok).sum())} rays differ beyond a 1-ulp tie"
+    hit = idx != cpu.INVALID
+    assert hit.mean() > 0.25
+    ties = ~exact
+    assert ties.mean() < 1e-3, ties.sum()
+    same_tri = hg[:, 3].view(np.uint32) == idx
+    assert same_tri[~ties].all()
+    if ties.any():  # each alternative triangle is really hit at that distance
+        alt = ob.tris[hg[ties, 3].view(np.uint32)]
+        o = rays[ties, 0:3].astype(np.float64)
+        d = rays[ties, 4:7].astype(np.float64)
+        tt, u, v = mt_hit64(alt, o, d)
+        assert np.all(np.abs(tt - hg[ties, 0]) <= 1e-5 * np.maximum(1.0, np.abs(tt)))
+        assert np.all((u >= -1e-6) & (v >= -1e-6) & (u + v <= 1 + 1e-6))
+
+
+def test_deform_matches_host_restatement_and_rebuild_is_exact(cuda):
+    rest, _ = cpt.scene_sphere_hairball(256, 128, 2000, seed=4)
+    n = len(rest)
+    amp, omega, phase = 0.01, 40.0, 0.3
+    d_rest, d_out = to_device(rest), to_device(rest)
+    cpt.check(cpt.lib.cpt_scene_deform(d_rest.data_ptr(), d_out.data_ptr(), n, ctypes.c_float(amp),
+                                       ctypes.c_float(omega), ctypes.c_float(phase), stream_handle()),
+              "cpt_scene_deform")
+    torch.cuda.synchronize()
+    got = d_out.cpu().numpy().view(cpt.TRIANGLE_DTYPE)
+    for k in ("v0", "v1", "v2"):
+        v = rest[k].astype(np.float64)
+        nrm = v / np.sqrt(np.maximum((v * v).sum(1, keepdims=True), 1e-30))
+        want = v + amp * np.sin(omega * v + phase) * nrm
+        # __sinf on |omega x + phase| <= 53 and the fast reciprocal square root: the
+        # displacement (amplitude 0.01) is off by well under 1e-6; the sum rounds to fp32
+        assert np.abs(got[k] - want).max() < 2e-6, k
+    assert np.array_equal(got["info_idx"], rest["info_idx"])
+    assert not np.array_equal(got["v0"], rest["v0"])
+    lb = DeviceLbvh(n, 63)
+    lb.build(d_out, check_root=True)
+    assert_same_as(lb.download(), cpu.build(got, 63))
+    assert cpt.lib.cpt_scene_deform(d_rest.data_ptr(), d_out.data_ptr(), 0, ctypes.c_float(amp),
+                                    ctypes.c_float(omega), ctypes.c_float(phase), stream_handle()) == \
+        cpt.ERR_INVALID_ARGUMENT

@@ -50,7 +50,7 @@ def tie_or_equal(h_split, h_ref, ulps=1):
 
 @pytest.mark.parametrize("bits", [30, 63])
 @pytest.mark.parametrize("ratio", [0.5, 2.0])
-@pytest.mark.parametrize("flags", [0, cpt.SPLIT_PLOC, cpt.SPLIT_TREELET])
+@pytest.mark.parametrize("flags", [0, cpt.SPLIT_TREELET])
 def test_split_hits_match_oracle(cuda, bits, ratio, flags):
     tris, _ = hairball()
     lb = DeviceLbvh(len(tris), bits)
@@ -79,14 +79,13 @@ def test_split_hits_match_oracle(cuda, bits, ratio, flags):
     assert np.array_equal(a_split.cpu().numpy()[:, 0] < 3e38, a_base.cpu().numpy()[:, 0] < 3e38)
     # fewer visits on the hairball; reference-format outputs untouched
     v_split, v_base = split_stats.cpu().numpy()[:, 0].mean(), base_stats.cpu().numpy()[:, 0].mean()
-    if flags != cpt.SPLIT_PLOC:  # (the clustered tree's visit counts depend on the scene; parity is what is tested)
-        assert v_split < (0.95 if ratio >= 2.0 else 1.0) * v_base, (v_split, v_base)
+    assert v_split < (0.95 if ratio >= 2.0 else 1.0) * v_base, (v_split, v_base)
     after = lb.download()
     for k in ("tris", "keys", "children", "parents_leaf", "parents_internal", "node_boxes", "nodes"):
         assert after[k].tobytes() == before[k].tobytes(), k
 
 
-@pytest.mark.parametrize("flags", [0, cpt.SPLIT_PLOC, cpt.SPLIT_TREELET])
+@pytest.mark.parametrize("flags", [0, cpt.SPLIT_TREELET])
 def test_split_render_matches_plain(cuda, flags):
     tris, infos = hairball(n_hair=30_000)
     cam = cpt.camera_look_at((0.0, 0.35, -3.6), (0.0, 0.0, 0.0), aspect=64 / 48)
@@ -111,7 +110,7 @@ def test_split_render_matches_plain(cuda, flags):
     assert not lb.bvh.split_nodes and lb.bvh.split_capacity == 0
 
 
-@pytest.mark.parametrize("flags", [0, cpt.SPLIT_PLOC, cpt.SPLIT_TREELET])
+@pytest.mark.parametrize("flags", [0, cpt.SPLIT_TREELET])
 def test_split_degenerate_and_zero_budget(cuda, flags):
     # ratio 0: one piece per triangle; a flat scene (zero extent on an axis) where every
     # hit is a near-tie between coplanar triangles
@@ -134,9 +133,10 @@ def test_split_degenerate_and_zero_budget(cuda, flags):
     assert np.array_equal(a[:, 0] < 3e38, b[:, 0] < 3e38)
 
 
-def test_ploc_on_identical_boxes(cuda):
-    # every piece the same box: all union areas tie, the pair hash decides, and
-    # clustering still ends in one tree whose hits are those of the LBVH
+@pytest.mark.parametrize("flags", [0, cpt.SPLIT_TREELET])
+def test_split_on_identical_boxes(cuda, flags):
+    # every piece the same box (all Morton keys equal, every treelet cost a tie): the
+    # split tree's hits are those of the LBVH
     tri = np.zeros(1, cpt.TRIANGLE_DTYPE)
     tri["v0"], tri["v1"], tri["v2"] = (0.0, 0.0, 0.0), (1.0, 0.0, 0.0), (0.0, 1.0, 0.0)
     tris = np.repeat(tri, 3000)
@@ -149,7 +149,7 @@ def test_ploc_on_identical_boxes(cuda):
     rays[:, 6] = 1.0
     d_rays = torch.from_numpy(rays).cuda()
     h0, _ = lb.trace(d_rays)
-    lb.split(0.0, flags=cpt.SPLIT_PLOC)
+    lb.split(0.0, flags=flags)
     h1, _ = lb.trace(d_rays)
     torch.cuda.synchronize()
     lb.status()
@@ -232,7 +232,7 @@ def test_treelet_flag_checks(cuda):
     lb = DeviceLbvh(len(tris), 30)
     lb.build(to_device(tris))
     with pytest.raises(ValueError):
-        lb.split(1.0, flags=cpt.SPLIT_TREELET | cpt.SPLIT_PLOC)
+        lb.split(1.0, flags=cpt.SPLIT_TREELET | 1)
     with pytest.raises(ValueError):
         lb.split(1.0, flags=8)
     # two and three triangles: no treelet of 3 leaves or fewer to improve; hits still match

@@ -57,12 +57,14 @@ def worker(rank, world, port, outdir, die_rank):
     if rank == die_rank:
         os._exit(0)  # leaves between steps, without joining the reduction
     t = torch.from_numpy(acc.copy())
+    out = torch.zeros_like(t)
     try:
-        reduce_accumulator(t, dst=0)
+        reduce_accumulator(t, out, dst=0)
         status = "ok"
     except Exception as e:  # the peer is gone: the collective must fail, not hang
         status = "error: " + type(e).__name__
-    np.save(os.path.join(outdir, f"reduced{rank}.npy"), t.numpy())
+    np.save(os.path.join(outdir, f"reduced{rank}.npy"), out.numpy())
+    np.save(os.path.join(outdir, f"after{rank}.npy"), t.numpy())
     with open(os.path.join(outdir, f"status{rank}.txt"), "w") as f:
         f.write(status)
     try:
@@ -89,9 +91,15 @@ def test_two_rank_sample_sharding_and_reduce(tmp_path):
     a0 = np.load(tmp_path / "local0.npy")
     a1 = np.load(tmp_path / "local1.npy")
     got = np.load(tmp_path / "reduced0.npy")
-    assert got.tobytes() == (a0 + a1).astype(np.float32).tobytes()
+    # each rank's compensated sum (sum - compensation), added across ranks; counts add up
+    want = ((a0[0] - a0[1]).astype(np.float32) + (a1[0] - a1[1]).astype(np.float32)).astype(np.float32)
+    assert got[0].tobytes() == want.tobytes()
+    assert not got[1].any()
     assert np.all(got[0, ..., 3] == 2 * SPP)
     assert not np.array_equal(a0[0], a1[0]), "ranks must render different samples"
+    # the ranks' own accumulators are untouched (they keep accumulating their frames)
+    for r, a in ((0, a0), (1, a1)):
+        assert np.load(tmp_path / f"after{r}.npy").tobytes() == a.tobytes()
 
 
 def test_rank_frame0_ranges_are_disjoint():

@@ -8,7 +8,8 @@ import pytest
 import cpt
 from scene_files import write_box
 
-REF_MESHES = "/root/reference/assets/meshes"
+# the reference checkout's fixture meshes, when a checkout is present (CPT_REFERENCE_ROOT)
+REF_MESHES = os.path.join(os.environ.get("CPT_REFERENCE_ROOT", "/root/reference"), "assets", "meshes")
 
 
 def test_box_counts_materials_and_emitter(tmp_path):

@@ -150,3 +150,23 @@ def test_morton_known_answers():
 def test_build_rejects_fewer_than_two():
     with pytest.raises(ValueError):
         cpu.build(np.zeros(1, cpu.TRIANGLE_DTYPE), 30, box=np.array([0, 0, 0, 1, 1, 1], np.float32))
+
+
+def test_row_sample_renders_match_reference_functions():
+    """The benchmark's CPU leg renders a stride of rows with float64 per-pixel sums:
+    the reference-function loop (ref_render_rows) and the oracle's integrator give
+    the same bits and ray counts on the same rows; rows outside the image are refused."""
+    if not cpu.ref_available(30):
+        pytest.skip("reference not compiled in this checkout (make -C oracle ref)")
+    tris, infos = cpt.scene_random(4000, seed=6)
+    b = cpu.build(tris, 30)
+    w, h = 32, 24
+    cam = cpt.camera_look_at((0.5, 0.5, -1.2), (0.5, 0.5, 0.0), aspect=w / h)
+    rows = np.array([1, 6, 11, 16, 21], np.uint32)
+    ref, rc = cpu.ref_render_rows(b, infos, None, w, h, rows, 3, 2, 3, 3.0, True, 8, cam.as_array())
+    orc, oc = cpu.render_rows(b, infos, w, h, rows, 3, 2, 3, 3.0, True, 8, cpu.ocam_from(cam.eye, cam.as_array()[3:]))
+    assert ref.tobytes() == orc.tobytes()
+    assert np.array_equal(rc, oc) and rc[0] == len(rows) * w * 3
+    assert (ref > 0).any()
+    with pytest.raises(ValueError):
+        cpu.ref_render_rows(b, infos, None, w, h, np.array([h], np.uint32), 1, 0, 3, 3.0, True, 8, cam.as_array())

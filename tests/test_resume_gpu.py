@@ -63,7 +63,11 @@ def test_tracer_progress_resume_matches_one_run(cuda):
     acc, frame = first.get_progress(W, H, cpt.ACCUM_KAHAN)
     assert frame == 2 and acc.nbytes == cpt.accum_bytes(W, H, cpt.ACCUM_KAHAN)
     second = tracer()
-    second.set_progress(acc, W, H, frame)
+    # the checkpoint's accumulator mode is checked: the FP64 layout has the same size
+    with pytest.raises(cpt.CptError) as e:
+        second.set_progress(acc, W, H, frame, cpt.ACCUM_F64)
+    assert e.value.code == cpt.ERR_INVALID_ARGUMENT
+    second.set_progress(acc, W, H, frame, cpt.ACCUM_KAHAN)
     second.raytrace(W, H, 1)
     assert second.frame == 3
     assert second.read_image(W, H).tobytes() == want.tobytes()

@@ -22,20 +22,32 @@ pytestmark = pytest.mark.gpu
 MAX_TRIANGLES = 131072
 
 
-def static_build(tris, bits, check=True):
+def in_place_source(lb, tris):
+    """The triangles copied into the output's own sorted-triangle array, which the
+    build then permutes in place (as the reference permutes its scene's triangles)."""
+    src = to_device(tris)
+    torch.cuda.synchronize()
+    lb.mem[: src.numel()].copy_(src)  # bvh.tris is the first array of the allocation
+    assert lb.bvh.tris == lb.mem.data_ptr()
+    return lb.bvh.tris
+
+
+def static_build(tris, bits, check=True, in_place=False):
     lb = DeviceLbvh(len(tris), bits)  # outputs owned by the caller (torch memory); no scratch used
     src = to_device(tris)
+    ptr = in_place_source(lb, tris) if in_place else src.data_ptr()
     box = cpt.scene_bounds(tris)
-    rc = cpt.lib.cpt_lbvh_build_static(src.data_ptr(), len(tris), box.ctypes.data, bits, ctypes.byref(lb.bvh),
+    rc = cpt.lib.cpt_lbvh_build_static(ptr, len(tris), box.ctypes.data, bits, ctypes.byref(lb.bvh),
                                        cpt.BUILD_CHECK if check else 0, torch.cuda.current_stream().cuda_stream)
     cpt.check(rc, "cpt_lbvh_build_static")
     torch.cuda.synchronize()
     return lb.download()
 
 
-def allocating_build(tris, bits):
+def allocating_build(tris, bits, in_place=False):
     lb = DeviceLbvh(len(tris), bits)
-    lb.build(to_device(tris), box=cpt.scene_bounds(tris), check_root=True)
+    src = to_device(tris)
+    lb.build(in_place_source(lb, tris) if in_place else src, box=cpt.scene_bounds(tris), check_root=True)
     torch.cuda.synchronize()
     return lb.download()
 
@@ -53,6 +65,16 @@ def test_static_build_equals_allocating_build_twice(cuda, bits):
         assert_identical(static_build(tris, bits), allocating_build(tris, bits))
     # and the first scene again after the second: nothing left over changes the result
     assert_identical(static_build(first, bits), allocating_build(first, bits))
+
+
+@pytest.mark.parametrize("bits", [30, 63])
+def test_static_build_in_place_at_the_limit(cuda, bits):
+    """An in-place build (input = the output's triangle array) gathers from a copy of
+    the triangles held in the fixed scratch, its largest piece (40 B per triangle):
+    at the maximum size it must equal the allocating in-place build, twice."""
+    tris = cpt.scene_random(MAX_TRIANGLES - 2, seed=33)[0]
+    for _ in range(2):
+        assert_identical(static_build(tris, bits, in_place=True), allocating_build(tris, bits, in_place=True))
 
 
 def test_static_build_rejects_more_than_the_limit(cuda):
