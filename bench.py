@@ -43,9 +43,9 @@ WORKLOADS = {
     "c3": dict(kind="batch", scenes=64, tri_min=10_000, tri_max=2_000_000, res_min=256, res_max=1024, spp=4,
                bounces=5, bits=63, seed=0, width=0, height=0, split=1.25, wide=1),
     # radiance cache on the C2 scene: 1 spp frames through the cache vs plain 16 spp, RMSE vs an FP64 image
-    "c4": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
+    "c4": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=1,
                bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, plain_spp=64, ref_spp=4096,
-               ref_div=4, warm_updates=4, max_spp=256, split=4.0, wide=1),
+               ref_div=4, warm_updates=4, max_spp=256, split=8.0, wide=1, treelet=1),
     # deforming 16.8 M-triangle displaced sphere, full rebuild every frame, 8 cameras
     "c5": dict(kind="deform", nu=4096, nv=2048, n_hair=0, bits=63, width=1280, height=720, spp=1, bounces=7,
                eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, cameras=8, amp=0.01, omega=40.0, cache=True),
@@ -251,6 +251,42 @@ def cpu_reference_run(w, tris, infos, cam, bits, target_s=12.0, stride=None):
             "sample": f"one row in {stride} of frame 0 ({len(rows)} of {height} rows, from row {stride // 2}) x "
                       f"{width} px x {spp} spp, depth {w['bounces'] + 1}; the frame's rate is taken as the sampled "
                       f"rows' rate; build of all {len(tris)} triangles"}
+
+
+def reference_gpu_build(tris, dev, reps=5):
+    """The reference's own GPU LBVH build (oracle/_ref/librefgpu.so: BVHBuilder::build
+    compiled from its sources for sm_100a, 30-bit keys as shipped) on this GPU, beside
+    this library's build of the same triangles at the same key width; None when that
+    library was not built."""
+    import torch
+
+    from oracle import cpu
+    from cpt.device import DeviceLbvh, to_device
+
+    if not cpu.refgpu_available():
+        return None
+    n = len(tris)
+    ref, _ = cpu.refgpu_build(tris, reps=reps)
+    lb = DeviceLbvh(n, 30, dev)
+    d = to_device(tris, dev)
+    lb.build(d, check_root=True)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        lb.build(d)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    lb.status()
+    ours = e0.elapsed_time(e1) / reps
+    del lb, d
+    return {"what": "the reference's CUDA::BVHBuilder::build (thrust + its kernels, BVHBuilder.cu:207-269) compiled "
+                    "from source for sm_100a, on this GPU; ours = cpt_lbvh_build at the same 30-bit key width on the "
+                    "same triangles", "triangles": n, "morton_bits": 30, "builds": reps,
+            "reference_ms": round(ref["ms_mean"], 3), "reference_ms_min": round(ref["ms_min"], 3),
+            "reference_wall_ms": round(ref["wall_ms_mean"], 3),
+            "reference_mtris_s": round(n / ref["ms_mean"] / 1e3, 2), "ours_ms": round(ours, 4),
+            "ours_mtris_s": round(n / ours / 1e3, 2), "speedup": round(ref["ms_mean"] / ours, 2)}
 
 
 def frame_parity(gpu_sums, cpu_sums, spp):
@@ -796,10 +832,36 @@ def run_ours(args, w, world, rank, local):
                                         + ", 16-spp frame, D2H image"}
         tr.close()
 
+    # the LBVH timing above rebuilt the tree (dropping the split and wide trees): the
+    # measurements below use the benchmark's own traversal tree again
+    if not deforming:
+        lb.build(d_tris)
+        if split > 0:
+            lb.split(split, keep_scratch=True, flags=split_flags(args))
+        if args.wide:
+            lb.wide(keep_scratch=True)
+        torch.cuda.synchronize()
+
+    # --- radiance cache (the C4 configuration on this scene and tree): time to reach the
+    # plain tracer's 64-sample error against an FP64 image, 1-sample cached frames
+    cache_c4 = None
+    if rank == 0 and world == 1 and args.workload == "c2" and not args.no_cache_ratio:
+        wc = dict(WORKLOADS["c4"])
+        wc.update(width=W_, height=H_)
+        from cpt.device import rc_default_params
+
+        r4 = cache_experiment(wc, lb, scene, cams[0], dev, True, args.warmup, wc["spp"], rc_default_params())
+        cache_c4 = {"metric": "time-to-equal-RMSE (cache / plain, vs FP64 image), stratified first bounce",
+                    "value": r4["ratio"], "unit": "x", "higher_is_better": False,
+                    "plain": r4["plain"], "cache": {k: r4["cache"][k] for k in
+                                                    ("spp", "spp_per_frame", "ms", "warm_ms", "reached", "mrays_s",
+                                                     "training_samples_last_frame", "training")},
+                    "reference": r4["reference"], "curve_tail": r4["cache_curve"][-4:]}
+
     # --- CPU baseline (rank 0, N = 1): the reference's code on every k-th row of frame 0,
     # and the parity of the GPU's frame 0 (FP64 accumulator, same traversal tree as the
     # timed frames) on those rows
-    cpu_base, parity = None, None
+    cpu_base, parity, ref_gpu = None, None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference_run(w, tris, infos, cams[0], w["bits"], target_s=args.cpu_seconds)
         cpu_base = {"value": round(r["mrays_s"], 4), "unit": METRIC, "cores": r["threads"], "kind": r["kind"],
@@ -818,6 +880,7 @@ def run_ours(args, w, world, rank, local):
             cpu_base["sample_rays_share"] = round(r["rays"] / max(frame_rays, 1.0), 5)
             cpu_base["sample_rows_share"] = round(len(r["rows"]) / H_, 5)
             del pr
+        ref_gpu = reference_gpu_build(tris, dev)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -830,7 +893,9 @@ def run_ours(args, w, world, rank, local):
                                   + (f"split BVH (cpt_lbvh_split, extra pieces {split} x n"
                                      + (", treelet-restructured" if args.treelet else "") + ")" if split > 0
                                      else "LBVH (reference topology)")), "lbvh_topology": lbvh_topology,
-                "cpu_baseline": cpu_base, "parity": parity, "e2e": e2e, "gpu_launches": int(launches),
+                "cpu_baseline": cpu_base, "parity": parity, "reference_gpu_lbvh": ref_gpu,
+                "radiance_cache_c4": cache_c4, "e2e": e2e,
+                "gpu_launches": int(launches),
                 "clocks": clocks,
                 "parallelism": f"replicas x{world}: own BVH per GPU, disjoint sample streams, "
                                f"framebuffer reduce to rank 0 per frame" if world > 1 else "1 GPU",
@@ -839,29 +904,151 @@ def run_ours(args, w, world, rank, local):
     return 0
 
 
-def run_cache(args, w, world, rank, local):
-    """Time-to-equal-RMSE. The plain tracer renders plain_spp samples per pixel
-    (frames of 16 samples; time T_plain, error RMSE_plain against an
-    FP64-accumulated image of ref_spp samples). The cached tracer starts from
-    untrained weights: warm_updates training-only frames (cpt_rc_update), then
-    frames of `spp` samples (training + image) until its error reaches RMSE_plain
-    (time T_cache, warm-up included). value = T_cache / T_plain. The error is taken
-    on every ref_div-th pixel in x and y: the FP64 image is rendered at
-    (W / ref_div) x (H / ref_div), whose primary rays are exactly those of that
-    pixel subgrid (the ray through pixel x of W is the bilinear blend at x / W).
-    Both tracers use the reference's first-bounce stratification (8 x 8 strata
-    cycling over 64 samples); the same comparison without it is reported beside.
-    Frames are timed with CUDA events; the error checks between them are not."""
+def cache_experiment(w, lb, scene, cam, dev, stratified, warmup, spf, rc_params, nee=False, reach=None):
+    """Time-to-equal-RMSE of the radiance cache against the plain tracer on one scene.
+
+    The plain tracer renders plain_spp samples per pixel in frames of 16 samples (time
+    T_plain, error RMSE_plain against an FP64-accumulated image of ref_spp samples). The
+    cached tracer starts from untrained weights: warm_updates training-only frames
+    (cpt_rc_update), then frames of `spf` samples (each trains on the frame's own
+    training paths and renders the image) until its error reaches RMSE_plain (time
+    T_cache, warm-up included); ratio = T_cache / T_plain. The error is taken on every
+    ref_div-th pixel in x and y: the FP64 image is rendered at (W / ref_div) x (H /
+    ref_div), whose primary rays are exactly those of that pixel subgrid (the ray through
+    pixel x of W is the bilinear blend at x / W). Frames are timed with CUDA events; the
+    error checks between them are not. With nee and reach (an RMSE), also measures how
+    long the next-event plain tracer takes to reach it, in frames of 1 sample."""
     import torch
 
     import cpt
-    from cpt.device import (BatchRenderer, CachedRenderer, DeviceLbvh, DeviceScene, RadianceCache, make_params,
-                            rc_default_params, to_device)
+    from cpt.device import BatchRenderer, CachedRenderer, RadianceCache, make_params
+
+    W_, H_ = w["width"], w["height"]
+    rdiv = w["ref_div"]
+    rw, rh = W_ // rdiv, H_ // rdiv
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    t0 = time.perf_counter()
+    refp = make_params(rw, rh, w["ref_spp"], 0, w["bounces"], 3.0, stratified, w["seed"] + 99991, cpt.ACCUM_F64,
+                       nee=nee)
+    ref = BatchRenderer([(lb, scene, cam, rw, rh)], refp, dev)
+    ref.render()
+    torch.cuda.synchronize()
+    ref.check_status()
+    ri = ref.accums[0].view(torch.float64).view(rh, rw, 4)
+    ref_img = ri[..., :3] / ri[..., 3:4].clamp(min=1)
+    ref_s = time.perf_counter() - t0
+    del ref
+
+    def rmse(acc):
+        a = acc.view(torch.float32).view(2, H_, W_, 4)[0]
+        img = (a[..., :3] / a[..., 3:4].clamp(min=1)).double()[::rdiv, ::rdiv][:rh, :rw]
+        return float(torch.sqrt(((img - ref_img) ** 2).mean()))
+
+    pp = make_params(W_, H_, 16, 0, w["bounces"], 3.0, stratified, w["seed"], cpt.ACCUM_KAHAN, nee=nee)
+    plain = BatchRenderer([(lb, scene, cam, W_, H_)], pp, dev)
+    for i in range(max(1, warmup)):
+        plain.render(frame0=100000 + 16 * i)
+    torch.cuda.synchronize()
+    plain.accums[0].zero_()
+    plain.counts.zero_()
+    t_plain = 0.0
+    for f in range(w["plain_spp"] // 16):
+        t_plain += timed(lambda: plain.render(frame0=16 * f))
+    plain.check_status()
+    rmse_plain = rmse(plain.accums[0])
+    plain_rays = int(plain.counts[:3].sum())
+    reach_out = None
+    if reach is not None:
+        plain.accums[0].zero_()
+        t_r, k, got = 0.0, 0, None
+        while k < w["plain_spp"]:
+            t_r += timed(lambda: plain.render(frame0=k, spp=1))
+            k += 1
+            e = rmse(plain.accums[0])
+            if e <= reach:
+                got = e
+                break
+        reach_out = {"target_rmse": round(reach, 6), "spp": k, "ms": round(t_r, 2),
+                     "rmse": None if got is None else round(got, 6)}
+    del plain
+
+    rc = RadianceCache(rc_params)
+    cp = make_params(W_, H_, spf, 0, w["bounces"], 3.0, stratified, w["seed"], cpt.ACCUM_KAHAN, nee=nee)
+    cr = CachedRenderer(rc, [(lb, scene, cam, W_, H_)], cp, dev)
+    cr.render(frame0=200000)  # warm the kernels on a throwaway network
+    torch.cuda.synchronize()
+    rc.reset(1337)
+    cr.accums[0].zero_()
+    cr.counts.zero_()
+    cpt.profile_begin()
+    launches0 = cpt.launch_count()
+    t_cache = 0.0
+    for u in range(w["warm_updates"]):
+        t_cache += timed(lambda: cr.update(frame0=300000 + u))
+    t_warm = t_cache
+    spp, curve, reached = 0, [], False
+    while spp < w["max_spp"]:
+        t_cache += timed(lambda: cr.render(frame0=spp))
+        spp += spf
+        e = rmse(cr.accums[0])
+        curve.append((spp, round(t_cache, 1), round(e, 6)))
+        if e <= rmse_plain:
+            reached = True
+            break
+    prof = cpt.profile_end()
+    launches = cpt.launch_count() - launches0
+    cr.check_status()
+    cache_rays = int(cr.counts[:3].sum())
+    samples_last = rc.sample_count()
+    rc.close()
+    # the curve at the plain tracer's sample count, for the record
+    return {"stratified": stratified, "nee": nee, "ratio": round(t_cache / t_plain, 4) if reached else None,
+            "t_cache_ms": round(t_cache, 2), "cache_curve": curve if len(curve) <= 80 else curve[::4] + curve[-1:],
+            "plain_to_reference_rmse": reach_out,
+            "plain": {"spp": w["plain_spp"], "frames_spp": 16, "ms": round(t_plain, 2), "rmse": round(rmse_plain, 6),
+                      "mrays_s": round(plain_rays / t_plain / 1e3, 3)},
+            "cache": {"spp": spp, "spp_per_frame": spf, "warm_updates": w["warm_updates"],
+                      "warm_ms": round(t_warm, 2), "ms": round(t_cache, 2), "reached": reached,
+                      "mrays_s": round(cache_rays / t_cache / 1e3, 3), "training_samples_last_frame": samples_last,
+                      "training": "about train_samples of each frame's own paths, traced to full depth",
+                      "kernel_ms": {k: round(v[0], 3) for k, v in sorted(prof.items())}},
+            "reference": {"resolution": f"{rw}x{rh} (every {rdiv}th pixel of {W_}x{H_})",
+                          "spp": w["ref_spp"], "accum": "f64", "s": round(ref_s, 2)},
+            "launches": int(launches)}
+
+
+def rc_params_for(args, spf):
+    """2^16 training paths and 4 optimiser steps per frame (one render call of `spf`
+    samples), or — with --rc-per-sample — per image sample."""
+    from cpt.device import rc_default_params
+
+    p = rc_default_params()
+    if args.rc_per_sample:
+        p.train_samples *= spf
+        p.train_steps *= spf
+    return p
+
+
+def run_cache(args, w, world, rank, local):
+    """The radiance-cache workload (cache_experiment) on the C2 scene, stratified and
+    independent first bounces, and with next-event estimation in both tracers."""
+    import torch
+
+    import cpt
+    from cpt.device import DeviceLbvh, DeviceScene, to_device
 
     dev = torch.device("cuda", local if world > 1 else 0)
     tris, infos = make_scene(w)
     n = len(tris)
-    W_, H_ = w["width"], w["height"]
     cam = make_cameras(w)[0]
     lb = DeviceLbvh(n, w["bits"], dev)
     lb.build(to_device(tris, dev), check_root=True)
@@ -872,116 +1059,11 @@ def run_cache(args, w, world, rank, local):
         lb.wide()
     scene = DeviceScene(infos, None, dev)
     scene.build_emitters(lb)
-    stream = torch.cuda.current_stream()
-    rdiv = w["ref_div"]
-    rw, rh = W_ // rdiv, H_ // rdiv
     spf = w["spp"]
-
-    def timed(fn):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        fn()
-        e1.record(stream)
-        e1.synchronize()
-        return e0.elapsed_time(e1)
-
-    def rc_params():
-        """2^16 training suffixes and 4 optimiser steps per frame (one render call of
-        `spf` samples), or — with --rc-per-sample — per image sample (spf * 2^16
-        suffixes per call)."""
-        p = rc_default_params()
-        if args.rc_per_sample:
-            p.train_samples *= spf
-            p.train_steps *= spf
-        return p
+    rcp = rc_params_for(args, spf)
 
     def experiment(stratified, nee=False, reach=None):
-        """reach (with nee): the reference estimator's RMSE; also measures how long the
-        next-event plain tracer takes to get there, in frames of 1 sample."""
-        t0 = time.perf_counter()
-        refp = make_params(rw, rh, w["ref_spp"], 0, w["bounces"], 3.0, stratified, w["seed"] + 99991, cpt.ACCUM_F64,
-                           nee=nee)
-        ref = BatchRenderer([(lb, scene, cam, rw, rh)], refp, dev)
-        ref.render()
-        torch.cuda.synchronize()
-        ref.check_status()
-        ri = ref.accums[0].view(torch.float64).view(rh, rw, 4)
-        ref_img = ri[..., :3] / ri[..., 3:4].clamp(min=1)
-        ref_s = time.perf_counter() - t0
-        del ref
-
-        def rmse(acc):
-            a = acc.view(torch.float32).view(2, H_, W_, 4)[0]
-            img = (a[..., :3] / a[..., 3:4].clamp(min=1)).double()[::rdiv, ::rdiv][:rh, :rw]
-            return float(torch.sqrt(((img - ref_img) ** 2).mean()))
-
-        pp = make_params(W_, H_, 16, 0, w["bounces"], 3.0, stratified, w["seed"], cpt.ACCUM_KAHAN, nee=nee)
-        plain = BatchRenderer([(lb, scene, cam, W_, H_)], pp, dev)
-        for i in range(max(1, args.warmup)):
-            plain.render(frame0=100000 + 16 * i)
-        torch.cuda.synchronize()
-        plain.accums[0].zero_()
-        plain.counts.zero_()
-        t_plain = 0.0
-        for f in range(w["plain_spp"] // 16):
-            t_plain += timed(lambda: plain.render(frame0=16 * f))
-        plain.check_status()
-        rmse_plain = rmse(plain.accums[0])
-        plain_rays = int(plain.counts[:3].sum())
-        reach_out = None
-        if reach is not None:
-            plain.accums[0].zero_()
-            t_r, k, got = 0.0, 0, None
-            while k < w["plain_spp"]:
-                t_r += timed(lambda: plain.render(frame0=k, spp=1))
-                k += 1
-                e = rmse(plain.accums[0])
-                if e <= reach:
-                    got = e
-                    break
-            reach_out = {"target_rmse": round(reach, 6), "spp": k, "ms": round(t_r, 2),
-                         "rmse": None if got is None else round(got, 6)}
-        del plain
-
-        rc = RadianceCache(rc_params())
-        cp = make_params(W_, H_, spf, 0, w["bounces"], 3.0, stratified, w["seed"], cpt.ACCUM_KAHAN, nee=nee)
-        cr = CachedRenderer(rc, [(lb, scene, cam, W_, H_)], cp, dev)
-        cr.render(frame0=200000)  # warm the kernels on a throwaway network
-        torch.cuda.synchronize()
-        rc.reset(1337)
-        cr.accums[0].zero_()
-        cr.counts.zero_()
-        cpt.profile_begin()
-        launches0 = cpt.launch_count()
-        t_cache = 0.0
-        for u in range(w["warm_updates"]):
-            t_cache += timed(lambda: cr.update(frame0=300000 + u))
-        t_warm = t_cache
-        spp, curve, reached = 0, [], False
-        while spp < w["max_spp"]:
-            t_cache += timed(lambda: cr.render(frame0=spp))
-            spp += spf
-            e = rmse(cr.accums[0])
-            curve.append((spp, round(t_cache, 1), round(e, 6)))
-            if e <= rmse_plain:
-                reached = True
-                break
-        prof = cpt.profile_end()
-        launches = cpt.launch_count() - launches0
-        cr.check_status()
-        cache_rays = int(cr.counts[:3].sum())
-        rc.close()
-        return {"stratified": stratified, "nee": nee, "ratio": round(t_cache / t_plain, 4) if reached else None,
-                "t_cache_ms": round(t_cache, 2), "cache_curve": curve, "plain_to_reference_rmse": reach_out,
-                "plain": {"spp": w["plain_spp"], "ms": round(t_plain, 2), "rmse": round(rmse_plain, 6),
-                          "mrays_s": round(plain_rays / t_plain / 1e3, 3)},
-                "cache": {"spp": spp, "spp_per_frame": spf, "warm_updates": w["warm_updates"],
-                          "warm_ms": round(t_warm, 2), "ms": round(t_cache, 2), "reached": reached,
-                          "rmse_curve": curve, "mrays_s": round(cache_rays / t_cache / 1e3, 3),
-                          "kernel_ms": {k: round(v[0], 3) for k, v in sorted(prof.items())}},
-                "reference": {"resolution": f"{rw}x{rh} (every {rdiv}th pixel of {W_}x{H_})",
-                              "spp": w["ref_spp"], "accum": "f64", "s": round(ref_s, 2)},
-                "launches": int(launches)}
+        return cache_experiment(w, lb, scene, cam, dev, stratified, args.warmup, spf, rcp, nee=nee, reach=reach)
 
     main_run = experiment(True)
     alt = experiment(False)
@@ -1001,7 +1083,6 @@ def run_cache(args, w, world, rank, local):
                 "cache_nee": {"spp": first[0], "ms": first[1], "rmse": first[2]} if first else None,
                 "cache_vs_plain_both_nee": nee_run["ratio"]}
     if rank == 0:
-        rc_p = rc_params()
         line = {"metric": "time-to-equal-RMSE (cache / plain, vs FP64 image)", "value": main_run["ratio"],
                 "unit": "x", "n_gpus": world, "steps": main_run["cache"]["spp"] // spf, "warmup": args.warmup,
                 "ms_per_step": round(main_run["cache"]["ms"] / max(1, main_run["cache"]["spp"] // spf), 3),
@@ -1014,8 +1095,8 @@ def run_cache(args, w, world, rank, local):
                                 "unstratified": nee_summary(alt, nee_runs[1]),
                                 "runs": {"stratified": nee_runs[0], "unstratified": nee_runs[1]}}
                                if nee_runs else None),
-                "rc_params": {"train_samples": rc_p.train_samples, "train_steps": rc_p.train_steps,
-                              "learning_rate": rc_p.learning_rate, "beta2": rc_p.beta2},
+                "rc_params": {"train_samples": rcp.train_samples, "train_steps": rcp.train_steps,
+                              "learning_rate": rcp.learning_rate, "beta2": rcp.beta2},
                 "gpu_launches": main_run["launches"]}
         print(json.dumps(line), flush=True)
     return 0
@@ -1038,6 +1119,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cache-ratio", action="store_true",
+                    help="c2: skip the radiance cache's time-to-equal-RMSE measurement (the C4 configuration)")
     ap.add_argument("--res", default=None, help="override resolution WxH (profiling runs)")
     ap.add_argument("--spp", type=int, default=None, help="override samples per frame (profiling runs)")
     ap.add_argument("--sphere", default=None, help="override the sphere's grid NUxNV (profiling runs)")

@@ -359,12 +359,13 @@ __global__ void k_rc_to_bf16(const float* __restrict__ master, bf16* __restrict_
 
 // Training targets from the records of a finished wave: T = (R - R1) / W1 per
 // channel (0 where W1 is 0: such a channel never uses the cache), clamped at 0.
+// record_cap: records the buffer holds (appends past it were dropped).
 __global__ void __launch_bounds__(256) k_rc_collect(const float4* __restrict__ records,
-                                                    const uint32_t* __restrict__ record_count,
+                                                    const uint32_t* __restrict__ record_count, uint32_t record_cap,
                                                     const float4* __restrict__ state, float4* __restrict__ samples,
                                                     uint32_t* __restrict__ sample_count, uint32_t capacity)
 {
-    const uint32_t n = *record_count;
+    const uint32_t n = min(*record_count, record_cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 r0 = records[5 * (size_t)i], r1 = records[5 * (size_t)i + 1];
         const float4 r2 = records[5 * (size_t)i + 2], r3 = records[5 * (size_t)i + 3];
@@ -418,6 +419,9 @@ struct cpt_rc {
     float4* samples = nullptr;  // training samples of the current frame
     uint32_t* sample_count = nullptr;
     uint32_t sample_cap = 0;
+    float4* train_records = nullptr;  // vertex-1 records of the image's training paths (one wave)
+    uint32_t* train_count = nullptr;
+    uint32_t train_cap = 0;
     uint32_t t = 0;  // Adam steps taken
     void* block = nullptr;
 };
@@ -493,7 +497,8 @@ int train_batch(cpt_rc* rc, const float4* samples, const uint32_t* count_dev, ui
 struct Ctx {
     cpt_rc* rc;
     const float* box;
-    bool training;
+    bool training;    // a training-only pass: every record is a training record
+    bool own_paths;   // an image pass with training paths among its own paths
 };
 
 int after_wave(void* ctx, const float4* records, const uint32_t* record_count, uint32_t capacity, float4* state,
@@ -502,12 +507,21 @@ int after_wave(void* ctx, const float4* records, const uint32_t* record_count, u
     Ctx* c = static_cast<Ctx*>(ctx);
     if (c->training) {
         CPT_PROF(K_RC_COLLECT, stream);
-        k_rc_collect<<<sm_count() * 4, 256, 0, stream>>>(records, record_count, state, c->rc->samples,
+        k_rc_collect<<<sm_count() * 4, 256, 0, stream>>>(records, record_count, capacity, state, c->rc->samples,
                                                          c->rc->sample_count, c->rc->sample_cap);
         CPT_LAUNCH_CHECK();
         return CPT_OK;
     }
-    (void)capacity;
+    if (c->own_paths) {  // targets of this wave's training paths (their radiance is final now)
+        {
+            CPT_PROF(K_RC_COLLECT, stream);
+            k_rc_collect<<<sm_count() * 4, 256, 0, stream>>>(c->rc->train_records, c->rc->train_count,
+                                                             c->rc->train_cap, state, c->rc->samples,
+                                                             c->rc->sample_count, c->rc->sample_cap);
+        }
+        CPT_LAUNCH_CHECK();
+        CPT_CUDA_TRY(cudaMemsetAsync(c->rc->train_count, 0, sizeof(uint32_t), stream));  // the next wave's list
+    }
     {
         CPT_PROF(K_RC_INFER, stream);
         k_rc_infer<true><<<infer_grid(), kInferBlock, kInferSmem, stream>>>(c->rc->w_infer, records, record_count, 0,
@@ -573,6 +587,9 @@ extern "C" int cpt_rc_create(cpt_rc** out, const cpt_rc_params* params, cudaStre
     c.take<float>(6);
     c.take<float4>(4ull * rc->sample_cap);
     c.take<uint32_t>(1);
+    rc->train_cap = p.train_samples;
+    c.take<float4>(5ull * rc->train_cap);
+    c.take<uint32_t>(1);
     if (cudaMalloc(&rc->block, c.used()) != cudaSuccess) {
         delete rc;
         return CPT_ERR_CUDA;
@@ -589,6 +606,8 @@ extern "C" int cpt_rc_create(cpt_rc** out, const cpt_rc_params* params, cudaStre
     rc->box = d.take<float>(6);
     rc->samples = d.take<float4>(4ull * rc->sample_cap);
     rc->sample_count = d.take<uint32_t>(1);
+    rc->train_records = d.take<float4>(5ull * rc->train_cap);
+    rc->train_count = d.take<uint32_t>(1);
     const int r = cpt_rc_reset(rc, p.seed, stream);
     if (r) {
         cpt_rc_destroy(rc);
@@ -683,7 +702,6 @@ extern "C" size_t cpt_rc_render_scratch_bytes(const cpt_rc* rc, const cpt_view* 
     for (auto& v : tv) train_size(v, per_view, v.width, v.height);
     cpt_render_params pt = *params, pr = *params;
     pt.spp = 1;
-    pr.bounces = std::min(pr.bounces, 1u);
     const size_t a = cpt_render_views_scratch_bytes(tv.data(), n_views, &pt);
     const size_t b = cpt_render_views_scratch_bytes(views, n_views, &pr);
     if (!a || !b) return 0;
@@ -706,22 +724,24 @@ int rc_frame(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_rend
     std::vector<cpt_view> tv(views, views + n_views);
     const uint32_t per_view = std::max(1u, rc->params.train_samples / n_views);
     for (auto& v : tv) train_size(v, per_view, v.width, v.height);
-    cpt_render_params pt = *params, pr = *params;
+    cpt_render_params pt = *params;
     pt.spp = 1;
-    pt.seed_hi ^= 0xA511E9B3u;  // the training paths' own random stream
+    pt.seed_hi ^= 0xA511E9B3u;  // the training-only paths' own random stream
     pt.ray_sort = 0;
     pt.trace_stats = 0;
-    pr.bounces = std::min(pr.bounces, 1u);
     uint32_t cap_t = 0, cap_r = 0;
     const size_t rec_t = render_hook_layout(tv.data(), n_views, &pt, nullptr, &cap_t);
-    const size_t rec_r = render_hook_layout(views, n_views, &pr, nullptr, &cap_r);
+    const size_t rec_r = render_hook_layout(views, n_views, params, nullptr, &cap_r);
     const size_t render_part = need - std::max(rec_t, rec_r);
     float4* records = reinterpret_cast<float4*>(static_cast<char*>(scratch) + render_part);
     const float* box = reinterpret_cast<const float*>(views[0].bvh->node_boxes);
-    // 1. training paths: full depth, records at vertex 1, targets
-    if (params->bounces >= 2) {
+    const uint32_t steps = rc->params.train_steps;
+    if (!image) {
+        // training only (cpt_rc_update): full-depth paths over reduced copies of the views,
+        // records at vertex 1, targets, optimiser steps
+        if (params->bounces < 2) return CPT_OK;
         CPT_CUDA_TRY(cudaMemsetAsync(rc->sample_count, 0, sizeof(uint32_t), stream));
-        Ctx ct{rc, box, true};
+        Ctx ct{rc, box, true, false};
         RenderHook h{};
         h.records = records;
         h.capacity = cap_t;
@@ -731,24 +751,45 @@ int rc_frame(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_rend
         h.ctx = &ct;
         int r = cpt_render_views_hooked(tv.data(), n_views, &pt, scratch, render_part, ray_counts, status, &h, stream);
         if (r) return r;
-        // 2. optimiser steps over this frame's samples
-        const uint32_t steps = rc->params.train_steps;
         for (uint32_t s = 0; s < steps; ++s) {
             r = train_batch(rc, rc->samples, rc->sample_count, 0, s, steps, box, nullptr, stream);
             if (r) return r;
         }
+        return CPT_OK;
     }
-    if (!image) return CPT_OK;
-    // 3. the image: vertices 0 and 1 traced, the cache for the rest
-    Ctx cr{rc, box, false};
+    if (params->bounces < 2)  // nothing after vertex 1 to cache: plain paths
+        return cpt_render_views_hooked(views, n_views, params, scratch, render_part, ray_counts, status, nullptr,
+                                       stream);
+    // The image, training on its own paths: about train_samples of the frame's paths
+    // (chosen by a hash of pixel and sample) are traced to full depth — their vertex-1
+    // records give the training targets, their full estimate goes into the image — and
+    // every other path stops at vertex 1 and takes the cache's prediction for the rest.
+    CPT_CUDA_TRY(cudaMemsetAsync(rc->sample_count, 0, sizeof(uint32_t), stream));
+    CPT_CUDA_TRY(cudaMemsetAsync(rc->train_count, 0, sizeof(uint32_t), stream));
+    uint64_t pixels = 0;
+    for (uint32_t i = 0; i < n_views; ++i) pixels += (uint64_t)views[i].width * views[i].height;
+    const uint64_t paths = pixels * params->spp;
+    Ctx cr{rc, box, false, true};
     RenderHook h{};
-    h.records = params->bounces >= 2 ? records : nullptr;
+    h.records = records;
     h.capacity = cap_r;
     h.record_depth = 1;
     h.image_pass = true;
-    h.after_wave = params->bounces >= 2 ? after_wave : nullptr;
+    h.after_wave = after_wave;
     h.ctx = &cr;
-    return cpt_render_views_hooked(views, n_views, &pr, scratch, render_part, ray_counts, status, &h, stream);
+    h.train_records = rc->train_records;
+    h.train_count = rc->train_count;
+    h.train_capacity = rc->train_cap;
+    h.train_stride = (uint32_t)std::max<uint64_t>(1, paths / std::max(1u, rc->params.train_samples));
+    h.cut_at_record = true;
+    int r = cpt_render_views_hooked(views, n_views, params, scratch, render_part, ray_counts, status, &h, stream);
+    if (r) return r;
+    // optimiser steps over this frame's targets (the next frame's predictions use them)
+    for (uint32_t s = 0; s < steps; ++s) {
+        r = train_batch(rc, rc->samples, rc->sample_count, 0, s, steps, box, nullptr, stream);
+        if (r) return r;
+    }
+    return CPT_OK;
 }
 
 }  // namespace

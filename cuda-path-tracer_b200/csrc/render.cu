@@ -94,7 +94,25 @@ struct Wave {
     float4* records;          // nullable: vertex records (RenderHook)
     uint32_t* record_count;
     uint32_t record_depth;
+    float4* train_records;    // training paths' records (RenderHook::train_stride > 0)
+    uint32_t* train_count;
+    uint32_t train_capacity;
+    uint32_t train_stride;
+    uint32_t cut_at_record;   // paths other than training paths end at record_depth
 };
+
+// Training-path selection of a (pixel, global sample) pair: a fixed integer hash
+// (multiply / xor-shift rounds), so the choice does not depend on the wave layout.
+__device__ __forceinline__ bool training_path(uint32_t pixel, uint32_t frame, uint32_t stride)
+{
+    uint32_t h = pixel * 0x9E3779B1u ^ (frame + 0x7F4A7C15u) * 0x85EBCA77u;
+    h ^= h >> 16;
+    h *= 0x7FEB352Du;
+    h ^= h >> 15;
+    h *= 0x846CA68Bu;
+    h ^= h >> 16;
+    return h % stride == 0u;
+}
 
 // Slot -> pixel: 8-row bands, column-major inside a band.
 __device__ __forceinline__ void slot_to_pixel(uint32_t slot, uint32_t w, uint32_t h, uint32_t& x, uint32_t& y)
@@ -474,7 +492,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
         float4 nro = make_float4(0.f, 0.f, 0.f, 0.f), nrd = nro;
         uint32_t shadow = 0;
         bool bad_info = false;
-        bool rec = false;
+        bool rec = false, train = false;
         float4 rec0, rec1, rec2, rec3, rec4;
         bool nee = false;
         float4 sro, srd;
@@ -541,6 +559,12 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
                 }
                 state[2 * (size_t)pid] = make_float4(acc.x, acc.y, acc.z, 0.f);
                 state[2 * (size_t)pid + 1] = make_float4(absorbed.x, absorbed.y, absorbed.z, 0.f);
+                const uint32_t local = pid - v.pixel_base * wv.spw;
+                const uint32_t sl = local / v.pixels, slot = local - sl * v.pixels;
+                uint32_t x, y;
+                slot_to_pixel(slot, v.width, v.height, x, y);
+                const uint32_t frame = wave_frame0(wv) + wv.s0 + sl;
+                bool go_on = depth < wv.bounces;
                 if (kRecord && depth == wv.record_depth) {
                     rec = true;
                     rec0 = make_float4(hp.x, hp.y, hp.z, __uint_as_float(pid));
@@ -548,14 +572,12 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
                     rec2 = make_float4(normal.x, normal.y, normal.z, __fmul_rn(absorbed.y, wv.intensity));
                     rec3 = make_float4(albedo.x, albedo.y, albedo.z, __fmul_rn(absorbed.z, wv.intensity));
                     rec4 = make_float4(acc.x, acc.y, acc.z, 0.f);
+                    train = wv.train_stride && training_path(v.pixel_base + y * v.width + x, frame, wv.train_stride);
+                    if (train) rec = false;           // its record goes to the training list
+                    else if (wv.cut_at_record) go_on = false;  // the cache supplies the rest
                 }
-                if (depth < wv.bounces) {
+                if (go_on) {
                     // next direction (cuda_path_tracer.cu:269-284)
-                    const uint32_t local = pid - v.pixel_base * wv.spw;
-                    const uint32_t sl = local / v.pixels, slot = local - sl * v.pixels;
-                    uint32_t x, y;
-                    slot_to_pixel(slot, v.width, v.height, x, y);
-                    const uint32_t frame = wave_frame0(wv) + wv.s0 + sl;
                     const f3 no = add(hp, muls(normal, 1e-5f));
                     const uint4 r = philox4x32_10(make_uint4(y * v.width + x, frame, depth, vi), wv.k0, wv.k1);
                     float rx = u01(r.x), ry = u01(r.y);
@@ -592,6 +614,17 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(Views vs, Wave wv, uint32
                 r[2] = rec2;
                 r[3] = rec3;
                 r[4] = rec4;
+            }
+            if (wv.train_stride) {
+                const uint32_t tq = warp_append(wv.train_count, train);
+                if (train && tq < wv.train_capacity) {
+                    float4* r = wv.train_records + 5 * (size_t)tq;
+                    r[0] = rec0;
+                    r[1] = rec1;
+                    r[2] = rec2;
+                    r[3] = rec3;
+                    r[4] = rec4;
+                }
             }
         }
         if (kNee) {
@@ -943,6 +976,12 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
     wv.records = record ? hook->records : nullptr;
     wv.record_count = rs.counts + kRecordCountWord;
     wv.record_depth = hook ? hook->record_depth : 0u;
+    const bool train = record && hook->train_stride && hook->train_records && hook->train_count;
+    wv.train_records = train ? hook->train_records : nullptr;
+    wv.train_count = train ? hook->train_count : nullptr;
+    wv.train_capacity = train ? hook->train_capacity : 0u;
+    wv.train_stride = train ? hook->train_stride : 0u;
+    wv.cut_at_record = record && hook->cut_at_record ? 1u : 0u;
     const bool image = !hook || hook->image_pass;
 
     bool one_bvh = true, wide = true;

@@ -15,11 +15,23 @@ namespace cpt {
 // before the wave's samples are accumulated; it may add to the paths' radiance
 // (`state`: 2 float4 per path, radiance in the first). image_pass = false renders
 // no image: no accumulation and no frame-counter advance.
+//
+// Training on the image's own paths (train_stride > 0): a path whose (pixel, sample)
+// hash is 0 modulo train_stride is a training path — at vertex record_depth it
+// appends its record to train_records (at most train_capacity per wave, counted in
+// *train_count; later ones are dropped) instead of `records`, and goes on to full
+// depth. With cut_at_record, every other path ends at vertex record_depth (no bounce
+// ray, no shadow ray from it): its remainder is what after_wave adds.
 struct RenderHook {
     float4* records;
     uint32_t capacity;  // records the buffer holds; must cover a wave
     uint32_t record_depth;
     bool image_pass;
+    float4* train_records;
+    uint32_t* train_count;  // device word, zeroed by the hook's owner
+    uint32_t train_capacity;
+    uint32_t train_stride;  // 0: no training paths
+    bool cut_at_record;
     int (*after_wave)(void* ctx, const float4* records, const uint32_t* record_count, uint32_t capacity,
                       float4* state, cudaStream_t stream);
     void* ctx;

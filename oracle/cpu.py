@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref.so")      # reference, 30-bit keys (as shipped)
 REF64_LIB = os.path.join(HERE, "_ref", "libref64.so")  # reference, 63-bit key configuration
+REFGPU_LIB = os.path.join(HERE, "_ref", "librefgpu.so")  # reference's GPU LBVH build (sm_100a), 30-bit as shipped
 
 TRIANGLE_DTYPE = np.dtype([("v0", "<f4", 3), ("v1", "<f4", 3), ("v2", "<f4", 3), ("info_idx", "<u4")])
 BBOX_DTYPE = np.dtype([("min", "<f4", 3), ("max", "<f4", 3)])
@@ -85,6 +86,45 @@ def ref_lib(bits: int = 30) -> ctypes.CDLL:
         L.ref_render_rows.restype = I
         _ref[bits] = L
     return _ref[bits]
+
+
+_refgpu = None
+
+
+def refgpu_available() -> bool:
+    return os.path.exists(REFGPU_LIB)
+
+
+def refgpu_lib() -> ctypes.CDLL:
+    global _refgpu
+    if _refgpu is None:
+        if not os.path.exists(REFGPU_LIB):
+            raise ImportError(f"{REFGPU_LIB} missing: run `make -C oracle ref` where the reference tree exists")
+        L = ctypes.CDLL(REFGPU_LIB)
+        P, U, I = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int
+        L.refgpu_build.argtypes = [P, U, P, I, P, P, P, P, P, P, P, P]
+        L.refgpu_build.restype = I
+        L.refgpu_key_bits.restype = I
+        _refgpu = L
+    return _refgpu
+
+
+def refgpu_build(tris: np.ndarray, box=None, reps: int = 5, outputs: bool = False):
+    """The reference's own GPU build (CUDA::BVHBuilder::build compiled for sm_100a) on
+    the current device: ({"ms_mean", "ms_min", "wall_ms_mean"}, BuildResult or None).
+    The BuildResult holds the last build's reference-format arrays (keys left zero)."""
+    tris = np.ascontiguousarray(tris)
+    n = len(tris)
+    box = enclosing_box(tris) if box is None else np.ascontiguousarray(box, np.float32)
+    L = refgpu_lib()
+    ms, lo, wall = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+    r = BuildResult(n, int(L.refgpu_key_bits())) if outputs else None
+    arrs = [r.tris, r.children, r.parents_leaf, r.parents_internal, r.node_boxes] if outputs else [None] * 5
+    rc = L.refgpu_build(_p(tris), n, _p(box), int(reps), ctypes.byref(ms), ctypes.byref(lo), ctypes.byref(wall),
+                        *[_p(a) for a in arrs])
+    if rc != 0:
+        raise RuntimeError(f"refgpu_build failed (rc {rc})")
+    return {"ms_mean": ms.value, "ms_min": lo.value, "wall_ms_mean": wall.value}, r
 
 
 class BuildResult:

@@ -110,21 +110,47 @@ def views_of(tris, infos, cam, w=96, h=64):
     return [(lb, sc, cam, w, h)], (lb, sc)
 
 
-def test_zero_network_equals_plain_depth_two(cuda):
+def training_path(pixel, frame, stride):
+    """Host restatement of the renderer's training-path choice (render.cu training_path)."""
+    m = 0xFFFFFFFF
+    h = ((pixel * 0x9E3779B1) & m) ^ (((frame + 0x7F4A7C15) & m) * 0x85EBCA77 & m)
+    h ^= h >> 16
+    h = (h * 0x7FEB352D) & m
+    h ^= h >> 15
+    h = (h * 0x846CA68B) & m
+    h ^= h >> 16
+    return h % stride == 0
+
+
+def test_zero_network_image_is_cut_paths_plus_training_paths(cuda):
+    """With a zero network, a cached 1-sample frame is, pixel by pixel, the plain
+    depth-2 estimate (paths cut at vertex 1, remainder 0) or — for the training paths
+    picked by the (pixel, sample) hash — the plain full-depth estimate."""
     tris, infos, cam = cornell_like()
     views, keep = views_of(tris, infos, cam)
-    rc = RadianceCache(rc_default_params(learning_rate=0.0))
+    rc = RadianceCache(rc_default_params(learning_rate=0.0, train_samples=512))
     rc.set_weights([np.zeros((fi, fo), np.float32) for fi, fo in ref.LAYERS])
-    p = make_params(96, 64, 4, 7, 5, 3.0, True, 11, cpt.ACCUM_KAHAN)
-    cr = CachedRenderer(rc, views, p)
+    frame, bounces = 7, 5
+    cr = CachedRenderer(rc, views, make_params(96, 64, 1, frame, bounces, 3.0, True, 11, cpt.ACCUM_KAHAN))
     cr.render()
     torch.cuda.synchronize()
     cr.check_status()
-    assert rc.sample_count() > 1000
-    plain = BatchRenderer(views, make_params(96, 64, 4, 7, 1, 3.0, True, 11, cpt.ACCUM_KAHAN))
-    plain.render()
-    torch.cuda.synchronize()
-    assert cr.accums[0].cpu().numpy().tobytes() == plain.accums[0].cpu().numpy().tobytes()
+
+    def plain(b):
+        r = BatchRenderer(views, make_params(96, 64, 1, frame, b, 3.0, True, 11, cpt.ACCUM_KAHAN))
+        r.render()
+        torch.cuda.synchronize()
+        return r.accums[0].cpu().numpy().view(np.float32).reshape(2, 64, 96, 4)[0]
+
+    cut, full = plain(1), plain(bounces)
+    stride = (96 * 64) // 512
+    sel = np.array([[training_path(y * 96 + x, frame, stride) for x in range(96)] for y in range(64)])
+    assert 300 < sel.sum() < 800
+    want = np.where(sel[..., None], full, cut)
+    got = cr.accums[0].cpu().numpy().view(np.float32).reshape(2, 64, 96, 4)[0]
+    assert got.tobytes() == want.tobytes()
+    # the training paths that reached vertex 1 gave this frame's training samples
+    assert 0 < rc.sample_count() <= sel.sum()
 
 
 def test_training_targets_are_path_suffixes(cuda):
@@ -163,14 +189,15 @@ def test_bounces_below_two_render_plain(cuda):
 def test_trained_cache_agrees_with_plain_in_the_mean(cuda):
     tris, infos, cam = cornell_like()
     views, keep = views_of(tris, infos, cam)
-    rc = RadianceCache(rc_default_params(train_samples=1 << 14))
+    # 4 samples per frame, one path in six a training path
+    rc = RadianceCache(rc_default_params(train_samples=4096))
     bounces = 4
-    cr = CachedRenderer(rc, views, make_params(96, 64, 1, 0, bounces, 3.0, True, 21, cpt.ACCUM_KAHAN))
+    cr = CachedRenderer(rc, views, make_params(96, 64, 4, 0, bounces, 3.0, True, 21, cpt.ACCUM_KAHAN))
     for f in range(60):          # train on 60 frames, then start a fresh image
-        cr.render(frame0=f)
+        cr.render(frame0=4 * f)
     cr.accums[0].zero_()
     for f in range(60, 124):
-        cr.render(frame0=f)
+        cr.render(frame0=4 * f)
     plain = BatchRenderer(views, make_params(96, 64, 256, 0, bounces, 3.0, True, 33, cpt.ACCUM_KAHAN))
     plain.render()
     torch.cuda.synchronize()
