@@ -253,11 +253,14 @@ def cpu_reference_run(w, tris, infos, cam, bits, target_s=12.0, stride=None):
                       f"rows' rate; build of all {len(tris)} triangles"}
 
 
-def reference_gpu_build(tris, dev, reps=5):
-    """The reference's own GPU LBVH build (oracle/_ref/librefgpu.so: BVHBuilder::build
-    compiled from its sources for sm_100a, 30-bit keys as shipped) on this GPU, beside
-    this library's build of the same triangles at the same key width; None when that
-    library was not built."""
+def reference_gpu(w, tris, infos, cam, dev, ours_ms_per_spp, rays_per_spp, reps=5, frames=8):
+    """The reference's own GPU code on this GPU (oracle/_ref/librefgpu.so: its sources
+    compiled for sm_100a, 30-bit keys as shipped), beside this library on the same
+    triangles: BVHBuilder::build against cpt_lbvh_build at the same key width, and
+    raytrace_kernel (one sample per pixel per launch, its own curand stream) against this
+    library's time per sample of the timed frames. The reference counts no rays: its
+    Mrays/s uses this library's rays per sample of the same scene and estimator (the
+    expected count is the estimator's). None when that library was not built."""
     import torch
 
     from oracle import cpu
@@ -280,13 +283,27 @@ def reference_gpu_build(tris, dev, reps=5):
     lb.status()
     ours = e0.elapsed_time(e1) / reps
     del lb, d
-    return {"what": "the reference's CUDA::BVHBuilder::build (thrust + its kernels, BVHBuilder.cu:207-269) compiled "
-                    "from source for sm_100a, on this GPU; ours = cpt_lbvh_build at the same 30-bit key width on the "
-                    "same triangles", "triangles": n, "morton_bits": 30, "builds": reps,
-            "reference_ms": round(ref["ms_mean"], 3), "reference_ms_min": round(ref["ms_min"], 3),
-            "reference_wall_ms": round(ref["wall_ms_mean"], 3),
-            "reference_mtris_s": round(n / ref["ms_mean"] / 1e3, 2), "ours_ms": round(ours, 4),
-            "ours_mtris_s": round(n / ours / 1e3, 2), "speedup": round(ref["ms_mean"] / ours, 2)}
+    out = {"what": "the reference's own CUDA code compiled from its sources for sm_100a, on this GPU",
+           "lbvh": {"reference": "BVHBuilder::build (thrust sort + its kernels, BVHBuilder.cu:207-269)",
+                    "ours": "cpt_lbvh_build at the same 30-bit key width", "triangles": n, "morton_bits": 30,
+                    "builds": reps, "reference_ms": round(ref["ms_mean"], 3),
+                    "reference_ms_min": round(ref["ms_min"], 3), "reference_wall_ms": round(ref["wall_ms_mean"], 3),
+                    "reference_mtris_s": round(n / ref["ms_mean"] / 1e3, 2), "ours_ms": round(ours, 4),
+                    "ours_mtris_s": round(n / ours / 1e3, 2), "speedup": round(ref["ms_mean"] / ours, 2)}}
+    if w["width"] % 8 == 0 and w["height"] % 8 == 0:
+        r, img = cpu.refgpu_render(tris, infos, w["width"], w["height"], cam.as_array(), w["bounces"], 3.0, True,
+                                   warmup=2, frames=frames, seed=w["seed"] + 1, image=True)
+        ref_mrays = rays_per_spp / r["ms_per_frame"] / 1e3
+        out["render"] = {"reference": "raytrace_kernel (cuda_path_tracer.cu:385-421), 8x8 blocks, one sample per "
+                                      "pixel per launch, over its own 30-bit LBVH",
+                         "ours": "the timed frames (the benchmark's traversal tree), per sample",
+                         "frames": frames, "reference_ms_per_spp": round(r["ms_per_frame"], 3),
+                         "ours_ms_per_spp": round(ours_ms_per_spp, 4),
+                         "speedup": round(r["ms_per_frame"] / ours_ms_per_spp, 2),
+                         "reference_mrays_s_est": round(ref_mrays, 3),
+                         "rays_per_spp_used": int(rays_per_spp),
+                         "reference_image_mean": round(float(img[..., :3].mean()), 6)}
+    return out
 
 
 def frame_parity(gpu_sums, cpu_sums, spp):
@@ -336,11 +353,12 @@ def run_batch(args, w, world, rank, local):
     if not mine:
         raise SystemExit("more ranks than scenes")
     split = w.get("split", 0.0) if args.split is None else args.split
-    views, keep, n_tris, pixels = [], [], 0, 0
+    views, keep, n_tris, pixels, boxes = [], [], 0, 0, []
     for i, (kind, ntri, side) in enumerate(specs):
         if i not in mine:
             continue
         tris, infos = batch_scene(kind, ntri, w["seed"] + i)
+        boxes.append(cpt.scene_bounds(tris))
         lb = DeviceLbvh(len(tris), w["bits"], dev)
         d = to_device(tris, dev)
         lb.build(d, check_root=True)
@@ -359,13 +377,15 @@ def run_batch(args, w, world, rank, local):
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
 
-    def params(wave, sort, stats=False):
+    def params(wave, sort, stats=False, refill=0, blocks=0):
         return make_params(0, 0, w["spp"], 0, w["bounces"], 3.0, True, w["seed"],
-                           cpt.ACCUM_KAHAN, wave_paths=wave, ray_sort=sort, trace_stats=stats)
+                           cpt.ACCUM_KAHAN, wave_paths=wave, ray_sort=sort, trace_stats=stats, refill_lanes=refill,
+                           traverse_blocks_per_sm=blocks)
 
-    # --- autotuner (cpt/autotune.py): one warm + one timed frame per candidate, keep the fastest
-    def time_frame(wave, sort):
-        br = BatchRenderer(views, params(wave, sort), dev)
+    # --- autotuner (cpt/autotune.py): one warm + one timed frame per candidate, keep the
+    # fastest; first the wave size and ray sorting, then the traversal's launch shape
+    def time_frame(wave, sort, refill=0, blocks=0):
+        br = BatchRenderer(views, params(wave, sort, refill=refill, blocks=blocks), dev)
         br.render()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -377,11 +397,14 @@ def run_batch(args, w, world, rank, local):
         return e0.elapsed_time(e1)
 
     tuned = autotune.tune(time_frame, ((1 << 24, 0), (1 << 25, 0), (1 << 26, 0), (1 << 25, 1)))
-    tune = tuned.table
-    best = {"wave_paths": tuned.wave_paths, "ray_sort": tuned.ray_sort, "ms": tuned.ms}
+    shaped = autotune.tune(time_frame, autotune.launch_candidates(tuned))
+    tune = tuned.table + shaped.table
+    best = {"wave_paths": shaped.wave_paths, "ray_sort": shaped.ray_sort, "refill_lanes": shaped.refill_lanes,
+            "blocks_per_sm": shaped.blocks_per_sm, "ms": shaped.ms}
+    shape = {"refill": best["refill_lanes"], "blocks": best["blocks_per_sm"]}
 
     # --- instrumented frame: node visits per closest-hit ray
-    br = BatchRenderer(views, params(best["wave_paths"], best["ray_sort"], stats=True), dev)
+    br = BatchRenderer(views, params(best["wave_paths"], best["ray_sort"], stats=True, **shape), dev)
     br.render()
     torch.cuda.synchronize()
     c = br.counts.cpu().numpy()
@@ -391,7 +414,7 @@ def run_batch(args, w, world, rank, local):
 
     # --- one frame captured in a CUDA graph; the device frame counter advances per replay
     counter = torch.zeros(1, dtype=torch.int32, device=dev)
-    p = params(best["wave_paths"], best["ray_sort"])
+    p = params(best["wave_paths"], best["ray_sort"], **shape)
     p.frame_counter = counter.data_ptr()
     br = BatchRenderer(views, p, dev)
     side_stream = torch.cuda.Stream(device=dev)
@@ -450,16 +473,21 @@ def run_batch(args, w, world, rank, local):
             lb.wide(keep_scratch=True)
     torch.cuda.synchronize()
 
+    from cpt.device import LbvhBatch
+
+    batch = LbvhBatch([v[0] for v in views], dev)  # every scene's LBVH in one launch sequence
+    batch.build(keep, boxes, check_root=True)
+
     def rebuild_all():
+        batch.build(keep, boxes)
         for (lb, _, _, _, _), d, h in zip(views, keep, hair):
-            lb.build(d)
             if h:
                 lb.split(split, keep_scratch=True, flags=split_flags(args))
             if args.wide:
                 lb.wide(keep_scratch=True)
 
     counter2 = torch.zeros(1, dtype=torch.int32, device=dev)
-    p2 = params(best["wave_paths"], best["ray_sort"])
+    p2 = params(best["wave_paths"], best["ray_sort"], **shape)
     p2.frame_counter = counter2.data_ptr()
     br2 = BatchRenderer(views, p2, dev)
     with torch.cuda.stream(side_stream):
@@ -487,18 +515,28 @@ def run_batch(args, w, world, rank, local):
     c2n = br2.counts.cpu().numpy()
     rays2 = sum_over_ranks(float(c2n[0] + c2n[1] + c2n[2]), world)
     built_and_rendered = {"mrays_s": round(rays2 / (ms2 / 1e3) / 1e6, 3), "ms_per_step": round(ms2 / args.steps, 3),
-                          "note": "one CUDA graph replay per frame: every scene's LBVH build (and the split trees "
-                                  "of the hairball scenes) followed by the render of all scenes"}
+                          "note": "one CUDA graph replay per frame: every scene's LBVH (one batched build, "
+                                  "cpt_lbvh_build_batch), the split trees of the hairball scenes, then the render "
+                                  "of all scenes"}
     del graph2, br2
 
-    # --- rebuild of the rank's scenes (device-resident soups)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for (lb, _, _, _, _), d in zip(views, keep):
-        lb.build(d)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    build_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    # --- rebuild of the rank's scenes (device-resident soups): the batched build, and
+    # the same scenes built one call each for comparison
+    def time_builds(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    build_ms = max_over_ranks(time_builds(lambda: batch.build(keep, boxes)), world)
+    per_scene_ms = max_over_ranks(time_builds(lambda: [v[0].build(d) for v, d in zip(views, keep)]), world)
+    for v in views:
+        v[0].status()
     n_tris = int(sum_over_ranks(float(n_tris), world))
     pixels = int(sum_over_ranks(float(pixels), world))
     if rank == 0:
@@ -520,7 +558,10 @@ def run_batch(args, w, world, rank, local):
                              "bytes_per_ray": f"48 + {node_b:.0f} x {mean_nodes:.2f} nodes + 48 x {mean_tris:.2f} triangles",
                              "kernel_share": {k: round(v[0] / frame_ms, 4) for k, v in sorted(prof.items())}},
                 "lbvh": {"mtris_s": round(n_tris / build_ms / 1e3, 2), "ms": round(build_ms, 3),
-                         "note": "each rank's scenes built back to back (max over ranks)"},
+                         "per_scene_calls_ms": round(per_scene_ms, 3),
+                         "per_scene_calls_mtris_s": round(n_tris / per_scene_ms / 1e3, 2),
+                         "note": "each rank's scenes in one batched build (cpt_lbvh_build_batch; max over ranks); "
+                                 "per_scene_calls = the same scenes built by one cpt_lbvh_build call each"},
                 # kernels of one frame (graph nodes) x timed replays; the replays themselves make no
                 # library calls (graph_launches counts those: 0)
                 "gpu_launches": int(sum(v[1] for v in prof.values()) * args.steps),
@@ -880,7 +921,7 @@ def run_ours(args, w, world, rank, local):
             cpu_base["sample_rays_share"] = round(r["rays"] / max(frame_rays, 1.0), 5)
             cpu_base["sample_rows_share"] = round(len(r["rows"]) / H_, 5)
             del pr
-        ref_gpu = reference_gpu_build(tris, dev)
+        ref_gpu = reference_gpu(w, tris, infos, cams[0], dev, ms_max / args.steps / spp, rays_all / args.steps / spp)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -893,7 +934,7 @@ def run_ours(args, w, world, rank, local):
                                   + (f"split BVH (cpt_lbvh_split, extra pieces {split} x n"
                                      + (", treelet-restructured" if args.treelet else "") + ")" if split > 0
                                      else "LBVH (reference topology)")), "lbvh_topology": lbvh_topology,
-                "cpu_baseline": cpu_base, "parity": parity, "reference_gpu_lbvh": ref_gpu,
+                "cpu_baseline": cpu_base, "parity": parity, "reference_gpu": ref_gpu,
                 "radiance_cache_c4": cache_c4, "e2e": e2e,
                 "gpu_launches": int(launches),
                 "clocks": clocks,

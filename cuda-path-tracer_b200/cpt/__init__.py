@@ -37,6 +37,7 @@ ERRORS = {
 ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_SCRATCH_TOO_SMALL, ERR_NONFINITE_INPUT = 1, 2, 3, 4
 ERR_DEVICE_TIMEOUT, ERR_STACK_OVERFLOW, ERR_CHECK_FAILED, ERR_NO_DEVICE, ERR_BAD_INDEX = 5, 6, 7, 8, 9
 BUILD_CHECK = 1
+MAX_BATCH_SCENES = 64
 BUILD_TEST_WITHHOLD = 2  # test of the bounded sort wait: tile 0 of the first pass never publishes
 
 
@@ -105,7 +106,8 @@ class RenderParams(ctypes.Structure):
                 ("stratified", ctypes.c_uint32), ("seed_lo", ctypes.c_uint32), ("seed_hi", ctypes.c_uint32),
                 ("accum_mode", ctypes.c_uint32), ("ref_grid", ctypes.c_uint32), ("wave_paths", ctypes.c_uint32),
                 ("trace_stats", ctypes.c_uint32), ("ray_sort", ctypes.c_uint32), ("cameras", ctypes.c_uint32),
-                ("frame_counter", ctypes.c_void_p), ("nee", ctypes.c_uint32)]
+                ("frame_counter", ctypes.c_void_p), ("nee", ctypes.c_uint32), ("refill_lanes", ctypes.c_uint32),
+                ("traverse_blocks_per_sm", ctypes.c_uint32)]
 
 
 def _load() -> ctypes.CDLL:
@@ -130,6 +132,8 @@ _PROTOS = {
     "cpt_lbvh_scratch_bytes": (_SZ, [_U32, _I32]),
     "cpt_lbvh_build": (_I32, [_P, _U32, _P, _I32, ctypes.POINTER(Bvh), _P, _SZ, _U32, _P]),
     "cpt_lbvh_build_static": (_I32, [_P, _U32, _P, _I32, ctypes.POINTER(Bvh), _U32, _P]),
+    "cpt_lbvh_batch_scratch_bytes": (_SZ, [_P, _U32, _I32]),
+    "cpt_lbvh_build_batch": (_I32, [_P, _P, _U32, _P, _I32, _P, _P, _SZ, _U32, _P]),
     "cpt_status_check": (_I32, [_P, _P]),
     "cpt_trace": (_I32, [ctypes.POINTER(Bvh), _P, _U32, _I32, _P, _P, _P]),
     "cpt_accum_bytes": (_SZ, [_U32, _U32, _U32]),

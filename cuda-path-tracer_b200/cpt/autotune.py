@@ -1,4 +1,4 @@
-"""Wave-size and ray-sort autotuning for the wavefront renderer.
+"""Wave-size, ray-sort and traversal launch-shape autotuning for the wavefront renderer.
 
 A render call traces its samples in waves, and a wave holds whole samples of every
 view: clamp(wave_paths // pixels, 1, spp) samples per pixel are in flight at once
@@ -11,7 +11,15 @@ batched workload (64 scenes, one CUDA graph per frame) picks its wave this way.
 
     cands = candidates(pixels, spp, scratch_bytes, budget_bytes=8 << 30)
     result = tune(time_frame, cands)          # time_frame(wave_paths, ray_sort) -> ms
-    cache = TuneCache(path); cache.put(key, result)
+    shape = tune(time_frame4, launch_candidates(result))  # time_frame4(wave, sort, refill, blocks)
+    cache = TuneCache(path); cache.put(key, shape)
+
+The second stage tunes the persistent traversal's launch shape at the chosen wave:
+the refill threshold (a warp takes new rays once fewer than `refill_lanes` of its
+lanes still trace: fewer idle lanes against more refill bookkeeping) and the resident
+traversal blocks per SM (`traverse_blocks_per_sm`: fewer resident warps keep more of
+each warp's nodes in L1 and L2, more hide more latency). Both are
+cpt_render_params fields and leave the image unchanged.
 
 `time_frame` belongs to the caller (it renders on the GPU: one warm frame, one timed
 frame, CUDA events on the launching stream); everything here is host logic.
@@ -31,7 +39,9 @@ class TuneResult:
     wave_paths: int
     ray_sort: int
     ms: float
-    table: list = field(default_factory=list)  # every candidate: {"wave_paths", "ray_sort", "ms"}
+    table: list = field(default_factory=list)  # every candidate: {"wave_paths", "ray_sort", ..., "ms"}
+    refill_lanes: int = 0  # 0: the renderer's default
+    blocks_per_sm: int = 0  # 0: the traversal's occupancy
 
 
 def samples_per_wave(wave_paths: int, pixels: int, spp: int) -> int:
@@ -68,20 +78,49 @@ def candidates(pixels: int, spp: int, scratch_bytes: Callable[[int, int], int] |
     return out
 
 
-def tune(time_frame: Callable[[int, int], float], cands: Iterable[tuple[int, int]]) -> TuneResult:
-    """Times every candidate once with `time_frame(wave_paths, ray_sort) -> ms` and returns
-    the fastest (the first of equal times), with the whole table."""
+_FIELDS = ("wave_paths", "ray_sort", "refill_lanes", "blocks_per_sm")
+
+
+def launch_candidates(base: TuneResult, refills: Iterable[int] = (0, 28, 24, 16),
+                      blocks: Iterable[int] = (0, 6, 4)) -> list[tuple[int, int, int, int]]:
+    """(wave_paths, ray_sort, refill_lanes, blocks_per_sm) candidates at the wave and sort
+    of `base`: every refill threshold at full occupancy, then every smaller block count at
+    the default threshold (0 = the renderer's default in both)."""
+    out = [(base.wave_paths, base.ray_sort, int(r), 0) for r in refills]
+    out += [(base.wave_paths, base.ray_sort, 0, int(b)) for b in blocks if int(b)]
+    for r, b in ((c[2], c[3]) for c in out):
+        if not (0 <= r <= 32 and 0 <= b):
+            raise ValueError(f"bad launch candidate: refill {r}, blocks {b}")
+    seen, uniq = set(), []
+    for c in out:
+        if c not in seen:
+            seen.add(c)
+            uniq.append(c)
+    return uniq
+
+
+def tune(time_frame: Callable[..., float], cands: Iterable[tuple]) -> TuneResult:
+    """Times every candidate once and returns the fastest (the first of equal times),
+    with the whole table. A candidate is (wave_paths, ray_sort) or (wave_paths,
+    ray_sort, refill_lanes, blocks_per_sm); `time_frame` is called with the candidate's
+    values (two or four arguments) and returns milliseconds."""
     table = []
-    for wave, sort in cands:
-        ms = float(time_frame(int(wave), int(sort)))
+    for cand in cands:
+        cand = tuple(int(x) for x in cand)
+        if len(cand) not in (2, 4):
+            raise ValueError(f"a candidate has 2 or 4 values, not {cand}")
+        ms = float(time_frame(*cand))
         if not ms >= 0.0:
-            raise ValueError(f"time_frame returned {ms} ms for wave {wave}, sort {sort}")
-        table.append({"wave_paths": int(wave), "ray_sort": int(sort), "ms": round(ms, 3)})
+            raise ValueError(f"time_frame returned {ms} ms for candidate {cand}")
+        row = dict(zip(_FIELDS, cand))
+        row["ms"] = round(ms, 3)
+        table.append(row)
     if not table:
         raise ValueError("no candidates to time")
     best = min(range(len(table)), key=lambda i: (table[i]["ms"], i))
     b = table[best]
-    return TuneResult(b["wave_paths"], b["ray_sort"], b["ms"], table)
+    return TuneResult(b["wave_paths"], b["ray_sort"], b["ms"], table, b.get("refill_lanes", 0),
+                      b.get("blocks_per_sm", 0))
 
 
 def workload_key(device: str, pixels: int, spp: int, bounces: int, triangles: int, nee: bool = False) -> str:

@@ -183,12 +183,43 @@ class DeviceScene:
         return self.emitter_count
 
 
+class LbvhBatch:
+    """cpt_lbvh_build_batch over a list of DeviceLbvh (one key width): their LBVHs
+    built by one launch sequence; each output is the single build's."""
+
+    def __init__(self, lbvhs, device=None):
+        if not lbvhs:
+            raise ValueError("empty batch")
+        bits = {lb.bits for lb in lbvhs}
+        if len(bits) != 1:
+            raise ValueError("one key width per batch")
+        self.lbvhs = list(lbvhs)
+        self.bits = bits.pop()
+        k = len(self.lbvhs)
+        self.n = (ctypes.c_uint32 * k)(*[lb.n for lb in self.lbvhs])
+        self.bvh_ptrs = (ctypes.c_void_p * k)(*[ctypes.addressof(lb.bvh) for lb in self.lbvhs])
+        self.scratch_bytes = int(lib.cpt_lbvh_batch_scratch_bytes(self.n, k, self.bits))
+        if not self.scratch_bytes:
+            raise ValueError("batch rejected (scene count, sizes or key width)")
+        self.scratch = dev_bytes(self.scratch_bytes, device)
+
+    def build(self, tris, boxes, check_root: bool = False, stream: int | None = None) -> None:
+        """tris: one device tensor (or pointer) per scene; boxes: (scenes, 6) host boxes."""
+        k = len(self.lbvhs)
+        ptrs = (ctypes.c_void_p * k)(*[t if isinstance(t, int) else t.data_ptr() for t in tris])
+        bx = np.ascontiguousarray(boxes, np.float32).reshape(k, 6)
+        rc = lib.cpt_lbvh_build_batch(ptrs, self.n, k, bx.ctypes.data, self.bits, self.bvh_ptrs,
+                                      self.scratch.data_ptr(), self.scratch_bytes, BUILD_CHECK if check_root else 0,
+                                      stream_handle() if stream is None else stream)
+        check(rc, "cpt_lbvh_build_batch")
+
+
 def make_params(width, height, spp, frame0=0, bounces=3, intensity=3.0, stratified=True, seed=0,
                 accum_mode=ACCUM_KAHAN, ref_grid=False, wave_paths=0, trace_stats=False,
-                ray_sort=False, cameras=1, nee=False) -> RenderParams:
+                ray_sort=False, cameras=1, nee=False, refill_lanes=0, traverse_blocks_per_sm=0) -> RenderParams:
     return RenderParams(width, height, spp, frame0, bounces, intensity, int(stratified), seed & 0xFFFFFFFF,
                         (seed >> 32) & 0xFFFFFFFF, accum_mode, int(ref_grid), wave_paths, int(trace_stats),
-                        int(ray_sort), cameras, None, int(nee))
+                        int(ray_sort), cameras, None, int(nee), int(refill_lanes), int(traverse_blocks_per_sm))
 
 
 class DeviceRenderer:

@@ -191,88 +191,9 @@ __global__ void __launch_bounds__(kRefitBlock) k_gather_refit(const float* __res
     const uint32_t i = base + threadIdx.x;
     if (i >= n) return;
     if (sort_timed_out(status)) return;  // the order is not a sort: nothing to gather or refit
-    const uint32_t block_end = min(n, base + (uint32_t)kRefitBlock);  // leaves [base, block_end)
-    uint32_t src = order[i];
-    if (src >= n) {  // only after a failed sort pass (its status is already set): stay in bounds
-        atomicOr(status, CPT_STATUS_BAD_INDEX);
-        src = n - 1;
-    }
-    const float2* s2 = reinterpret_cast<const float2*>(tris_in + 10ull * src);
-    const float2 a = __ldg(s2), b = __ldg(s2 + 1), c = __ldg(s2 + 2), d = __ldg(s2 + 3), e = __ldg(s2 + 4);
-    float2* o2 = reinterpret_cast<float2*>(tris_out + 10ull * i);
-    o2[0] = a; o2[1] = b; o2[2] = c; o2[3] = d; o2[4] = e;
-    const float v[9] = {a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x};
-    // leaf slot: v0, the leaf's index (the triangle a hit reports), v1 - v0, v2 - v0
-    float slot[10] = {v[0], v[1], v[2], __uint_as_float(i),
-                      __fsub_rn(v[3], v[0]), __fsub_rn(v[4], v[1]), __fsub_rn(v[5], v[2]),
-                      __fsub_rn(v[6], v[0]), __fsub_rn(v[7], v[1]), __fsub_rn(v[8], v[2])};
-    Box box = leaf_box(v);  // BVHBuilder.cu:73-74, BBox.cpp:26-30
-    uint32_t child = i;
-    uint32_t p = parents_leaf[i];
-    // A node lets at most one arriver continue (the second; a third is refused), so
-    // a walk passes at most n - 1 nodes even on a corrupt topology; the step count
-    // makes that bound explicit.
-    for (uint32_t steps = 0; p != CPT_INVALID_INDEX; ++steps) {
-        if (p >= n - 1 || steps >= n - 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
-        float* node = nodes + 24 * (size_t)p;
-        const float4 meta = *reinterpret_cast<const float4*>(node + 20);  // Node word, right child, range end
-        const uint32_t word = __float_as_uint(meta.x);
-        const uint32_t left = word >> 2;
-        const int side = left == child ? 0 : 1;
-        const uint32_t j = __float_as_uint(meta.z);
-        const bool local = min(p, j) >= base && max(p, j) < block_end;
-        store_slot(node, side, slot);
-        const uint32_t sib = left + (uint32_t)(1 - side);
-        Box sb;
-        if (local) {
-            const uint32_t k = p - base;
-            float* mine = s_box[2 * k + side];
-#pragma unroll
-            for (int ax = 0; ax < 3; ++ax) { mine[ax] = box.mn[ax]; mine[3 + ax] = box.mx[ax]; }
-            __threadfence_block();
-            const int arrived = atomicAdd(&s_count[k], 1);
-            if (arrived == 0) return;
-            if (arrived != 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }  // a third visit: not a tree
-            __threadfence_block();
-            const volatile float* other = s_box[2 * k + (1 - side)];
-#pragma unroll
-            for (int ax = 0; ax < 3; ++ax) { sb.mn[ax] = other[ax]; sb.mx[ax] = other[3 + ax]; }
-        } else {
-            const int arrived = arrive_acq_rel(&counters[p]);
-            if (arrived == 0) return;
-            if (arrived != 1) { atomicOr(status, CPT_STATUS_BAD_INDEX); return; }
-            const bool sib_internal = (word >> (1 - side)) & 1u;
-            if (sib_internal) {
-                const float2* q = reinterpret_cast<const float2*>(node_boxes + sib);
-                const float2 x0 = __ldcg(q), x1 = __ldcg(q + 1), x2 = __ldcg(q + 2);
-                sb.mn[0] = x0.x; sb.mn[1] = x0.y; sb.mn[2] = x1.x; sb.mx[0] = x1.y; sb.mx[1] = x2.x; sb.mx[2] = x2.y;
-            } else {
-                const float2* q = reinterpret_cast<const float2*>(tris_out + 10ull * sib);
-                const float2 x0 = __ldcg(q), x1 = __ldcg(q + 1), x2 = __ldcg(q + 2), x3 = __ldcg(q + 3), x4 = __ldcg(q + 4);
-                const float sv[9] = {x0.x, x0.y, x1.x, x1.y, x2.x, x2.y, x3.x, x3.y, x4.x};
-                sb = leaf_box(sv);
-            }
-        }
-        Box u;
-#pragma unroll
-        for (int ax = 0; ax < 3; ++ax) {
-            const float lmn = side == 0 ? box.mn[ax] : sb.mn[ax], rmn = side == 0 ? sb.mn[ax] : box.mn[ax];
-            const float lmx = side == 0 ? box.mx[ax] : sb.mx[ax], rmx = side == 0 ? sb.mx[ax] : box.mx[ax];
-            u.mn[ax] = gmin(lmn, rmn);
-            u.mx[ax] = gmax(lmx, rmx);
-        }
-        box = u;
-        float2* ob = reinterpret_cast<float2*>(node_boxes + p);
-        ob[0] = make_float2(box.mn[0], box.mn[1]);
-        ob[1] = make_float2(box.mn[2], box.mx[0]);
-        ob[2] = make_float2(box.mx[1], box.mx[2]);
-        // internal slot for the next level: the box, padded
-#pragma unroll
-        for (int k = 0; k < 3; ++k) { slot[k] = box.mn[k]; slot[3 + k] = box.mx[k]; }
-        slot[6] = slot[7] = slot[8] = slot[9] = 0.0f;
-        child = p;
-        p = parents_internal[p];
-    }
+    (void)children;
+    gather_refit_leaf(tris_in, order[i], i, n, base, min(n, base + (uint32_t)kRefitBlock), tris_out, parents_leaf,
+                      parents_internal, counters, nodes, node_boxes, status, s_count, s_box);
 }
 
 // ---------------------------------------------------------------------------

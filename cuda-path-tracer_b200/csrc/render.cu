@@ -282,7 +282,8 @@ __global__ void __launch_bounds__(kExtendBlock, CPT_EXTEND_MIN_BLOCKS) k_extend(
                                                          const uint32_t* __restrict__ count, float4* __restrict__ hits,
                                                          uint32_t* __restrict__ pool,
                                                          unsigned long long* __restrict__ ray_counts,
-                                                         uint32_t* __restrict__ status, const uint32_t* __restrict__ order)
+                                                         uint32_t* __restrict__ status, const uint32_t* __restrict__ order,
+                                                         uint32_t refill)
 {
     __shared__ __align__(16) uint32_t s_stack[kSmemStack * kExtendBlock];
     const uint32_t n = *count;
@@ -306,7 +307,8 @@ __global__ void __launch_bounds__(kExtendBlock, CPT_EXTEND_MIN_BLOCKS) k_extend(
             wide_of, queue, n, pool, reinterpret_cast<uint2*>(s_stack) + threadIdx.x, overflow, nn, nt, order,
             [&](uint32_t ray, const WideState& s) {
                 hits[ray] = make_float4(s.best.t, s.best.u, s.best.v, __uint_as_float(s.best.tri));
-            });
+            },
+            refill);
         if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
         if (kStats && ray_counts) {
             warp_count_u64(ray_counts + 3, nn);
@@ -326,7 +328,8 @@ __global__ void __launch_bounds__(kExtendBlock, CPT_EXTEND_MIN_BLOCKS) k_extend(
         return vs.v[vi].nodes;
     };
     persistent_trace_views<false, kExtendBlock, kStats, kExtendSteps>(view_nodes, queue, n, hits, pool,
-                                                                      s_stack + threadIdx.x, overflow, nn, nt, order);
+                                                                      s_stack + threadIdx.x, overflow, nn, nt, order,
+                                                                      nullptr, refill);
     if (overflow) atomicOr(status, CPT_STATUS_STACK_OVERFLOW);
     if (kStats && ray_counts) {
         warp_count_u64(ray_counts + 3, nn);
@@ -1006,7 +1009,12 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
                          stream>>>(wv, vs, rs.queue[0], rs.counts, rs.state);
         }
         CPT_LAUNCH_CHECK();
-        const int ext_blocks = std::min<int>((int)((paths + kExtendBlock - 1) / kExtendBlock), sms * ext_occ);
+        // launch shape of the persistent traversal: resident blocks per SM (occupancy, or the
+        // caller's smaller figure) and the refill threshold of its warps (0: the default)
+        const int per_sm = params->traverse_blocks_per_sm ? std::min<int>(ext_occ, (int)params->traverse_blocks_per_sm)
+                                                          : ext_occ;
+        const int ext_blocks = std::min<int>((int)((paths + kExtendBlock - 1) / kExtendBlock), sms * per_sm);
+        const uint32_t refill = std::min<uint32_t>(params->refill_lanes, 32u);
         const int shade_blocks = std::min<int>((int)((paths + kShadeBlock - 1) / kShadeBlock), sms * 16);
         for (uint32_t b = 0; b <= params->bounces; ++b) {
             const float4* qin = rs.queue[b & 1];
@@ -1021,7 +1029,8 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
                 CPT_PROF(K_EXTEND, stream);
                 uint32_t* pool = rs.counts + kMaxDepth + 2 + b;
 #define CPT_EXTEND(S, O, W) \
-    k_extend<S, O, W><<<ext_blocks, kExtendBlock, 0, stream>>>(vs, qin, rs.counts + b, rs.hits, pool, ray_counts, status, order)
+    k_extend<S, O, W><<<ext_blocks, kExtendBlock, 0, stream>>>(vs, qin, rs.counts + b, rs.hits, pool, ray_counts, status, \
+                                                               order, refill)
                 if (wide) {
                     if (params->trace_stats) {
                         if (one_bvh) CPT_EXTEND(true, true, true); else CPT_EXTEND(true, false, true);

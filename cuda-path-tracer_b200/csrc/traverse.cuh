@@ -81,11 +81,66 @@ __device__ __forceinline__ float slab_test_fma(f3 odinv, f3 dinv, float ax, floa
     return (n <= f && f > 0.0f) ? n : FLT_MAX;
 }
 
+// Packed FP32 pairs (sm_100: add / sub / mul / fma .rn.f32x2). Each lane of the pair
+// is rounded exactly as the scalar round-to-nearest operation on it, so a packed
+// sequence gives the bits of the scalar one; it issues one instruction per pair.
+// Off by default: on C2 the packed forms ran 1.5 % faster (483.8 vs 476.8 Mrays/s), but
+// the packed triangle test did not reproduce the scalar sequence's bits on the device
+// (the render parity tests failed with it), and exact hits are required here.
+#ifndef CPT_PACKED_F32
+#define CPT_PACKED_F32 0
+#endif
+struct f2 { float x, y; };
+__device__ __forceinline__ f2 mk2(float x, float y) { f2 r; r.x = x; r.y = y; return r; }
+#define CPT_F2_OP(name, op)                                                                                    \
+    __device__ __forceinline__ f2 name(f2 a, f2 b)                                                              \
+    {                                                                                                         \
+        f2 d;                                                                                                 \
+        asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t" op            \
+            " rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"                                                         \
+            : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                  \
+        return d;                                                                                             \
+    }
+CPT_F2_OP(add2, "add.rn.f32x2")
+CPT_F2_OP(sub2, "sub.rn.f32x2")
+CPT_F2_OP(mul2, "mul.rn.f32x2")
+#undef CPT_F2_OP
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
+{
+    f2 d;
+    asm("{.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
 // Möller-Trumbore on a slot (v0 = s[0..2], e1 = s[4..6], e2 = s[7..9]), without
 // early exits: every lane of a warp runs the same instructions, and u, v, t are the
 // values the reference computes; only the final predicate decides the hit.
+// The packed form pairs the two cross products (q = d x e2, r = (o - v0) x e1) and
+// the dot products that share a factor ((e1, o - v0) . q and (d, e2) . r), with each
+// lane's operations in the scalar order: the same bits.
 __device__ __forceinline__ float tri_test(f3 o, f3 d, const float* s, float& u, float& v)
 {
+#if CPT_PACKED_F32
+    const f3 p0 = mk3(s[0], s[1], s[2]), e1 = mk3(s[4], s[5], s[6]), e2 = mk3(s[7], s[8], s[9]);
+    const f3 sv = sub(o, p0);
+    // (q, r) component-wise: q = cross(d, e2), r = cross(sv, e1) (cross(a, b).x = a.y b.z - b.y a.z, ...)
+    const f2 qrx = sub2(mul2(mk2(d.y, sv.y), mk2(e2.z, e1.z)), mul2(mk2(e2.y, e1.y), mk2(d.z, sv.z)));
+    const f2 qry = sub2(mul2(mk2(d.z, sv.z), mk2(e2.x, e1.x)), mul2(mk2(e2.z, e1.z), mk2(d.x, sv.x)));
+    const f2 qrz = sub2(mul2(mk2(d.x, sv.x), mk2(e2.y, e1.y)), mul2(mk2(e2.x, e1.x), mk2(d.y, sv.y)));
+    // (det, u') = (e1 . q, sv . q) and (v', t') = (d . r, e2 . r): (a.x b.x + a.y b.y) + a.z b.z
+    const f2 du = add2(add2(mul2(mk2(e1.x, sv.x), mk2(qrx.x, qrx.x)), mul2(mk2(e1.y, sv.y), mk2(qry.x, qry.x))),
+                       mul2(mk2(e1.z, sv.z), mk2(qrz.x, qrz.x)));
+    const f2 vt = add2(add2(mul2(mk2(d.x, e2.x), mk2(qrx.y, qrx.y)), mul2(mk2(d.y, e2.y), mk2(qry.y, qry.y))),
+                       mul2(mk2(d.z, e2.z), mk2(qrz.y, qrz.y)));
+    const float det = du.x;
+    const float inv = __frcp_rn(det);
+    u = __fmul_rn(inv, du.y);
+    const f2 vt2 = mul2(mk2(inv, inv), vt);
+    v = vt2.x;
+    const float t = vt2.y;
+#else
     const f3 p0 = mk3(s[0], s[1], s[2]), e1 = mk3(s[4], s[5], s[6]), e2 = mk3(s[7], s[8], s[9]);
     const f3 q = cross(d, e2);
     const float det = dot(e1, q);
@@ -95,6 +150,7 @@ __device__ __forceinline__ float tri_test(f3 o, f3 d, const float* s, float& u, 
     const f3 r = cross(sv, e1);
     v = __fmul_rn(inv, dot(d, r));
     const float t = __fmul_rn(inv, dot(e2, r));
+#endif
     const bool hit = !(det > -FLT_EPSILON && det < FLT_EPSILON) && !(u < 0.f) && !(v < 0.f) &&
                      !(__fadd_rn(u, v) > 1.f) && t >= 0.0f;
     return hit ? t : FLT_MAX;
@@ -405,6 +461,31 @@ __device__ __forceinline__ uint32_t wide_child_hits(const WideState& s, float4 n
     const uint32_t nz0 = fz ? hz0 : lz0, nz1 = fz ? hz1 : lz1, fz0 = fz ? lz0 : hz0, fz1 = fz ? lz1 : hz1;
     uint32_t hm = 0;
     const float tlim = s.best.t;
+#if CPT_PACKED_F32
+    // the near and far plane of an axis share the multiplier and the offset: one packed
+    // fused multiply-add per axis and child gives (t_near, t_far), each lane rounded as
+    // the scalar fmaf
+    const f2 ax2 = mk2(adx, adx), ay2 = mk2(ady, ady), az2 = mk2(adz, adz);
+    const f2 bx2 = mk2(bdx, bdx), by2 = mk2(bdy, bdy), bz2 = mk2(bdz, bdz);
+#pragma unroll
+    for (int i = 0; i < 8; i += 2) {  // two children at a time
+        float tn[2], tf[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t sel = 0x7440u | (uint32_t)((i + k) & 3);
+            const f2 tx = fma2(mk2(qbyte(i < 4 ? nx0 : nx1, sel), qbyte(i < 4 ? fx0 : fx1, sel)), ax2, bx2);
+            const f2 ty = fma2(mk2(qbyte(i < 4 ? ny0 : ny1, sel), qbyte(i < 4 ? fy0 : fy1, sel)), ay2, by2);
+            const f2 tz = fma2(mk2(qbyte(i < 4 ? nz0 : nz1, sel), qbyte(i < 4 ? fz0 : fz1, sel)), az2, bz2);
+            tn[k] = fmaxf(fmax3(tx.x, ty.x, tz.x), 0.0f);
+            tf[k] = fminf(fmin3(tx.y, ty.y, tz.y), tlim);
+        }
+        // the far ends grow by a relative 2^-18, both children in one packed multiply
+        const f2 g = mul2(mk2(tf[0], tf[1]), mk2(kWideGrow, kWideGrow));
+        hm |= (tn[0] <= g.x ? 1u : 0u) << i;
+        hm |= (tn[1] <= g.y ? 1u : 0u) << (i + 1);
+    }
+    return hm;
+#else
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const uint32_t sel = 0x7440u | (uint32_t)(i & 3);
@@ -420,6 +501,7 @@ __device__ __forceinline__ uint32_t wide_child_hits(const WideState& s, float4 n
         hm |= (tn <= tf ? 1u : 0u) << i;
     }
     return hm;
+#endif
 }
 
 // One step; returns true when the ray is finished.
@@ -522,8 +604,9 @@ template <bool kAny, int kBlock, bool kStats, int kSteps, bool kTmax, typename N
 __device__ __forceinline__ void persistent_trace(NodesOf nodes_of, const float4* __restrict__ rays, uint32_t n,
                                                  uint32_t* __restrict__ pool, uint32_t* smem_col, bool& overflow,
                                                  uint32_t& n_nodes, uint32_t& n_tris, const uint32_t* __restrict__ order,
-                                                 Done done)
+                                                 Done done, uint32_t refill = 0)
 {
+    const uint32_t refill_below = refill ? refill : (uint32_t)kRefillLanes;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t spill[CPT_TRAVERSAL_STACK - kSmemStack];
@@ -565,7 +648,7 @@ __device__ __forceinline__ void persistent_trace(NodesOf nodes_of, const float4*
             }
             const unsigned live = __ballot_sync(0xFFFFFFFFu, ray != CPT_INVALID_INDEX);
             if (live == 0) break;
-            if (!drained && (__popc(live) < kRefillLanes || k >= kSteps)) break;
+            if (!drained && ((uint32_t)__popc(live) < refill_below || k >= kSteps)) break;
         }
     }
 }
@@ -577,8 +660,10 @@ template <bool kAny, int kBlock, bool kStats, int kSteps, bool kTmax, typename W
 __device__ __forceinline__ void persistent_trace_wide(WideOf wide_of, const float4* __restrict__ rays, uint32_t n,
                                                       uint32_t* __restrict__ pool, uint2* smem_col, bool& overflow,
                                                       uint32_t& n_nodes, uint32_t& n_tris,
-                                                      const uint32_t* __restrict__ order, Done done)
+                                                      const uint32_t* __restrict__ order, Done done,
+                                                      uint32_t refill = 0)
 {
+    const uint32_t refill_below = refill ? refill : (uint32_t)kWideRefillLanes;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint2 spill[CPT_TRAVERSAL_STACK - kWideSmemStack];
@@ -618,7 +703,7 @@ __device__ __forceinline__ void persistent_trace_wide(WideOf wide_of, const floa
             }
             const unsigned live = __ballot_sync(0xFFFFFFFFu, ray != CPT_INVALID_INDEX);
             if (live == 0) break;
-            if (!drained && (__popc(live) < kWideRefillLanes || k >= kSteps)) break;
+            if (!drained && ((uint32_t)__popc(live) < refill_below || k >= kSteps)) break;
         }
     }
 }
@@ -630,14 +715,15 @@ __device__ __forceinline__ void persistent_trace_views(NodesOf nodes_of, const f
                                                        float4* __restrict__ hits, uint32_t* __restrict__ pool,
                                                        uint32_t* smem_col, bool& overflow, uint32_t& n_nodes,
                                                        uint32_t& n_tris, const uint32_t* __restrict__ order,
-                                                       uint2* __restrict__ ray_stats = nullptr)
+                                                       uint2* __restrict__ ray_stats = nullptr, uint32_t refill = 0)
 {
     persistent_trace<kAny, kBlock, kStats, kSteps, false>(
         nodes_of, rays, n, pool, smem_col, overflow, n_nodes, n_tris, order,
         [&](uint32_t ray, const TraceState& s) {
             hits[ray] = make_float4(s.best.t, s.best.u, s.best.v, __uint_as_float(s.best.tri));
             if (kStats && ray_stats) ray_stats[ray] = make_uint2(s.visits, s.tests);
-        });
+        },
+        refill);
 }
 
 }  // namespace cpt

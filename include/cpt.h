@@ -116,6 +116,25 @@ size_t cpt_lbvh_scratch_bytes(uint32_t n, int morton_bits);
 int cpt_lbvh_build(const cpt_triangle* tris_in, uint32_t n, const float* enclosing_box, int morton_bits,
                    cpt_bvh* bvh, void* scratch, size_t scratch_bytes, uint32_t flags, cudaStream_t stream);
 
+/* Batched LBVH build: the LBVHs of `scenes` triangle soups in one fixed sequence of
+ * launches, each launch covering every scene (one Morton launch, one stable radix
+ * sort over all scenes — the key digits, then a scene-id digit —, one topology launch,
+ * one refit launch). Replaces `scenes` calls of CUDA::BVHBuilder::build
+ * (source/application/cuda/BVHBuilder.cu:207-269), one per scene; every scene's
+ * outputs are bit-identical to cpt_lbvh_build's on the same triangles and box.
+ * Host arrays of `scenes` entries: tris_in[s] (device triangles; may equal
+ * bvhs[s]->tris for an in-place build), n[s] >= 2, bvhs[s] (bound for n[s] and
+ * morton_bits); boxes: host, 6 floats per scene (min xyz, max xyz), each scene's
+ * enclosingBBox as the reference's caller computes it (cpt_scene_bounds). The total
+ * triangle count must stay below 2^30. The kernels receive the scene table by value,
+ * so a call can be captured in a CUDA graph. flags: CPT_BUILD_CHECK (checks every
+ * scene's status and root volume; synchronizes) or 0. */
+#define CPT_MAX_BATCH_SCENES 64
+size_t cpt_lbvh_batch_scratch_bytes(const uint32_t* n, uint32_t scenes, int morton_bits);
+int cpt_lbvh_build_batch(const cpt_triangle* const* tris_in, const uint32_t* n, uint32_t scenes, const float* boxes,
+                         int morton_bits, cpt_bvh* const* bvhs, void* scratch, size_t scratch_bytes, uint32_t flags,
+                         cudaStream_t stream);
+
 /* LBVH build that allocates nothing: the same build and outputs as
  * cpt_lbvh_build, with its scratch in a fixed array inside the library's device
  * image instead of a caller buffer. It has no counterpart in the reference, whose
@@ -243,6 +262,12 @@ typedef struct cpt_render_params {
                                 * call captured once in a CUDA graph renders the next samples on each replay */
     uint32_t nee;              /* 1: next-event estimation (see cpt_emitters_build); every view's scene needs
                                 * an emitter table. 0: the reference's estimator */
+    /* launch shape of the persistent traversal kernels (results are unchanged; for tuning):
+     * refill_lanes: a warp takes new rays once fewer than this many of its lanes still trace
+     * (1..32; 0: 32 over wide trees, 16 over binary trees); traverse_blocks_per_sm: resident
+     * blocks per SM of the closest-hit traversal, at most its occupancy (0: occupancy) */
+    uint32_t refill_lanes;
+    uint32_t traverse_blocks_per_sm;
 } cpt_render_params;
 
 size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode); /* per camera / view */

@@ -105,6 +105,9 @@ def refgpu_lib() -> ctypes.CDLL:
         L.refgpu_build.argtypes = [P, U, P, I, P, P, P, P, P, P, P, P]
         L.refgpu_build.restype = I
         L.refgpu_key_bits.restype = I
+        F = ctypes.c_float
+        L.refgpu_render.argtypes = [P, U, P, P, U, U, U, P, U, F, I, U, U, U, P, P, P]
+        L.refgpu_render.restype = I
         _refgpu = L
     return _refgpu
 
@@ -125,6 +128,27 @@ def refgpu_build(tris: np.ndarray, box=None, reps: int = 5, outputs: bool = Fals
     if rc != 0:
         raise RuntimeError(f"refgpu_build failed (rc {rc})")
     return {"ms_mean": ms.value, "ms_min": lo.value, "wall_ms_mean": wall.value}, r
+
+
+def refgpu_render(tris: np.ndarray, infos: np.ndarray, width: int, height: int, cam15, bounces: int,
+                  intensity: float = 3.0, stratified: bool = True, warmup: int = 2, frames: int = 8, seed: int = 1,
+                  box=None, image: bool = False):
+    """The reference's own renderer on the current GPU (Scene::upload's LBVH build, then
+    raytrace_kernel launches of one sample per pixel): ({"ms_per_frame", "build_ms"},
+    running-mean image (height, width, 4) or None)."""
+    tris = np.ascontiguousarray(tris)
+    infos = np.ascontiguousarray(infos)
+    box = enclosing_box(tris) if box is None else np.ascontiguousarray(box, np.float32)
+    cam15 = np.ascontiguousarray(cam15, np.float32)
+    L = refgpu_lib()
+    ms, bms = ctypes.c_float(), ctypes.c_float()
+    img = np.zeros((height, width, 4), np.float32) if image else None
+    rc = L.refgpu_render(_p(tris), len(tris), _p(box), _p(infos), len(infos), width, height, _p(cam15), bounces,
+                         intensity, int(stratified), warmup, frames, seed, ctypes.byref(ms), ctypes.byref(bms),
+                         _p(img))
+    if rc != 0:
+        raise RuntimeError(f"refgpu_render failed (rc {rc})")
+    return {"ms_per_frame": ms.value, "build_ms": bms.value}, img
 
 
 class BuildResult:

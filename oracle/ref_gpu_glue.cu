@@ -13,9 +13,19 @@
 // the same translation unit, as the reference's build compiles them for the device.
 #include "engine/geometry/BBox.cpp"
 #include "application/cuda/BVHBuilder.cu"
+// The reference's path tracer (raytrace_kernel and the shading it calls,
+// cuda_path_tracer.cu:36-421) with the constant-memory scene descriptors it reads
+// (Globals.h; compiled as one translation unit without relocatable device code, the
+// extern declarations there are the variables themselves, which Scene.cu:8-11 defines in
+// the reference's separately compiled build). Its host-side helpers come along: the
+// mt19937 frame seeds (Random.cpp) and, as stand-ins without SDL / ImGui, the timer and
+// GUI settings types (oracle/ref_shim/engine/util/Timer.h, engine/gui/GUISettings.h).
+#include "engine/util/Random.cpp"
+#include "application/cuda/cuda_path_tracer.cu"
 
 #include <chrono>
 #include <cstdio>
+#include <exception>
 #include <unistd.h>
 
 namespace {
@@ -32,7 +42,9 @@ struct StdoutToStderr {
 
 extern "C" {
 
-int refgpu_key_bits(void) { return sizeof(MortonIntType) == 8 ? 63 : 30; }
+#define REFGPU_API __attribute__((visibility("default")))
+
+REFGPU_API int refgpu_key_bits(void) { return sizeof(MortonIntType) == 8 ? 63 : 30; }
 
 // Uploads n triangles (host, 40-B CUDA::Triangle records) and the enclosing box
 // (host, min xyz, max xyz), runs one untimed warm-up build, then `reps` builds, each
@@ -42,10 +54,33 @@ int refgpu_key_bits(void) { return sizeof(MortonIntType) == 8 ? 63 : 30; }
 // Outputs: mean and least event time (ms), mean wall time (ms); when the array
 // pointers are non-null, the last build's sorted triangles, Node words, both parent
 // arrays and the internal-node boxes (24 B each) are copied to host memory.
-// Returns 0, -1 for bad arguments, -2 for a CUDA error.
-int refgpu_build(const void* tris_host, uint32_t n, const float* box, int reps, float* ms_mean, float* ms_min,
-                 float* wall_ms_mean, void* tris_out, uint32_t* children_out, uint32_t* parents_leaf_out,
-                 uint32_t* parents_internal_out, float* boxes_out)
+// Returns 0, -1 for bad arguments, -2 for a CUDA error, -3 when thrust threw.
+static int refgpu_build_impl(const void* tris_host, uint32_t n, const float* box, int reps, float* ms_mean,
+                             float* ms_min, float* wall_ms_mean, void* tris_out, uint32_t* children_out,
+                             uint32_t* parents_leaf_out, uint32_t* parents_internal_out, float* boxes_out);
+
+// thrust reports CUDA failures by throwing; nothing may unwind through this C interface,
+// so an exception becomes -3 with its message on stderr
+REFGPU_API int refgpu_build(const void* tris_host, uint32_t n, const float* box, int reps, float* ms_mean,
+                            float* ms_min, float* wall_ms_mean, void* tris_out, uint32_t* children_out,
+                            uint32_t* parents_leaf_out, uint32_t* parents_internal_out, float* boxes_out)
+{
+    try {
+        return refgpu_build_impl(tris_host, n, box, reps, ms_mean, ms_min, wall_ms_mean, tris_out, children_out,
+                                 parents_leaf_out, parents_internal_out, boxes_out);
+    } catch (const std::exception& e) {
+        fprintf(stderr, "refgpu_build: %s\n", e.what());
+    } catch (...) {
+        fprintf(stderr, "refgpu_build: unknown exception\n");
+    }
+    return -3;
+}
+
+}  // extern "C"
+
+static int refgpu_build_impl(const void* tris_host, uint32_t n, const float* box, int reps, float* ms_mean,
+                             float* ms_min, float* wall_ms_mean, void* tris_out, uint32_t* children_out,
+                             uint32_t* parents_leaf_out, uint32_t* parents_internal_out, float* boxes_out)
 {
     if (!tris_host || !box || n < 2 || reps < 1) return -1;
     StdoutToStderr quiet;
@@ -88,6 +123,129 @@ int refgpu_build(const void* tris_host, uint32_t n, const float* box, int reps, 
     if (boxes_out)
         thrust::copy(desc.internalNodeBBoxes.begin(), desc.internalNodeBBoxes.end(), reinterpret_cast<BBox*>(boxes_out));
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// CUDAPathTracer's own methods (compiled with the kernel) refer to CUDA::Scene, whose
+// upload path (Scene.cu) logs through the engine's SDL/OpenGL logger; the render entry
+// below fills the same descriptors itself, so the class only needs to link.
+CUDA::Scene* CUDA::Scene::m_activeScene{nullptr};
+CUDA::Scene::Scene() {}
+CUDA::Scene::~Scene() {}
+void CUDA::Scene::upload(const CUDA::HostSceneDescription&) {}
+PathTracerSettings::Demo PathTracerSettings::DEMO;
+PathTracerSettings::GISettings PathTracerSettings::GI;
+
+static int refgpu_render_impl(const void* tris_host, uint32_t n, const float* box, const void* infos_host,
+                              uint32_t info_count, uint32_t width, uint32_t height, const float* cam15,
+                              uint32_t bounces, float intensity, int stratified, uint32_t warmup, uint32_t frames,
+                              uint32_t seed, float* ms_per_frame, float* build_ms, float* image_out)
+{
+    if (!tris_host || !box || !infos_host || !cam15 || n < 2 || width < 8 || height < 8 || frames < 1 ||
+        bounces > 255)
+        return -1;
+    StdoutToStderr quiet;
+    const CUDA::Triangle* in = static_cast<const CUDA::Triangle*>(tris_host);
+    const CUDA::TriangleInfo* inf = static_cast<const CUDA::TriangleInfo*>(infos_host);
+    // Scene::upload (Scene.cu:28-55): triangles and shading records to the device, the
+    // LBVH build, the four descriptors
+    CUDA::DeviceSceneDescription desc;
+    desc.triangles.assign(in, in + n);
+    desc.triangleInfo.assign(inf, inf + info_count);
+    desc.enclosingBBox = BBox(glm::vec3(box[0], box[1], box[2]), glm::vec3(box[3], box[4], box[5]));
+    CUDA::BVHBuilder builder;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return -2;
+    cudaEventRecord(e0, 0);
+    builder.build(desc, n);
+    cudaEventRecord(e1, 0);
+    if (cudaEventSynchronize(e1) != cudaSuccess) return -2;
+    if (build_ms) cudaEventElapsedTime(build_ms, e0, e1);
+    GeometryData geometry(thrust::raw_pointer_cast(desc.internalNodeBBoxes.data()),
+                          thrust::raw_pointer_cast(desc.children.data()),
+                          thrust::raw_pointer_cast(desc.triangles.data()), n);
+    ShadingData shading(thrust::raw_pointer_cast(desc.triangleInfo.data()));
+    shading.textures = nullptr;  // untextured materials (albedo / normal-map indices are invalid)
+    LightingData lighting;
+    lighting.dirLightCount = 0;  // the benchmark's light is an emissive quad
+    lighting.dirLights = nullptr;
+    lighting.indirectIntensity = intensity;
+    lighting.indirectBounceCount = static_cast<uint8_t>(bounces);
+    MiscData misc;
+    misc.useStratifiedSampling = stratified != 0;
+    if (cudaMemcpyToSymbol(g_geometryData, &geometry, sizeof(geometry)) != cudaSuccess ||
+        cudaMemcpyToSymbol(g_shadingData, &shading, sizeof(shading)) != cudaSuccess ||
+        cudaMemcpyToSymbol(g_lightingData, &lighting, sizeof(lighting)) != cudaSuccess ||
+        cudaMemcpyToSymbol(g_miscData, &misc, sizeof(misc)) != cudaSuccess)
+        return -2;
+    // the screen texture: a float4 array with surface load/store, cleared (frame 0's
+    // running mean reads it: lerp(hit, old, 0))
+    cudaChannelFormatDesc ch = cudaCreateChannelDesc<float4>();
+    cudaArray_t screen = nullptr;
+    if (cudaMallocArray(&screen, &ch, width, height, cudaArraySurfaceLoadStore) != cudaSuccess) return -2;
+    std::vector<float> zeros((size_t)width * height * 4, 0.0f);
+    cudaMemcpy2DToArray(screen, 0, 0, zeros.data(), width * sizeof(float4), width * sizeof(float4), height,
+                        cudaMemcpyHostToDevice);
+    cudaResourceDesc res;
+    memset(&res, 0, sizeof(res));
+    res.resType = cudaResourceTypeArray;
+    res.res.array.array = screen;
+    cudaSurfaceObject_t surf = 0;
+    if (cudaCreateSurfaceObject(&surf, &res) != cudaSuccess) { cudaFreeArray(screen); return -2; }
+    const glm::vec3 eye(cam15[0], cam15[1], cam15[2]);
+    const glm::vec3 d00(cam15[3], cam15[4], cam15[5]), d10(cam15[6], cam15[7], cam15[8]);
+    const glm::vec3 d11(cam15[9], cam15[10], cam15[11]), d01(cam15[12], cam15[13], cam15[14]);
+    // CUDAPathTracer::raytrace (cuda_path_tracer.cu:444-459): 8x8 blocks over the
+    // truncated grid, one sample per launch, a new random seed per frame
+    const dim3 threads(8, 8), blocks(width / 8, height / 8);
+    Random::seed(seed);
+    uint32_t frame = 0;
+    for (uint32_t f = 0; f < warmup; ++f, ++frame)
+        raytrace_kernel<<<blocks, threads>>>(surf, eye, d00, d10, d11, d01, glm::ivec2(width, height), frame,
+                                             Random::getUInt(0, std::numeric_limits<uint32_t>().max()));
+    if (cudaDeviceSynchronize() != cudaSuccess) { cudaDestroySurfaceObject(surf); cudaFreeArray(screen); return -2; }
+    cudaEventRecord(e0, 0);
+    for (uint32_t f = 0; f < frames; ++f, ++frame)
+        raytrace_kernel<<<blocks, threads>>>(surf, eye, d00, d10, d11, d01, glm::ivec2(width, height), frame,
+                                             Random::getUInt(0, std::numeric_limits<uint32_t>().max()));
+    cudaEventRecord(e1, 0);
+    const cudaError_t err = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms_per_frame) *ms_per_frame = ms / frames;
+    if (err == cudaSuccess && image_out)
+        cudaMemcpy2DFromArray(image_out, width * sizeof(float4), screen, 0, 0, width * sizeof(float4), height,
+                              cudaMemcpyDeviceToHost);
+    cudaDestroySurfaceObject(surf);
+    cudaFreeArray(screen);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return err == cudaSuccess && cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+extern "C" {
+
+// The reference's renderer on this GPU: Scene::upload's work (its LBVH build, timed
+// into *build_ms) for n triangles with info_count shading records, then `warmup`
+// untimed and `frames` timed launches of raytrace_kernel at width x height (one sample
+// per pixel per launch, the running mean in a float4 surface), the camera as eye and
+// four corner directions (00, 10, 11, 01), `bounces` indirect bounces, no directional
+// lights. *ms_per_frame: mean device time of a timed launch. image_out (nullable,
+// width x height x 4 floats): the running-mean image after the last frame. Returns 0,
+// -1 for bad arguments, -2 for a CUDA error, -3 when thrust threw.
+REFGPU_API int refgpu_render(const void* tris_host, uint32_t n, const float* box, const void* infos_host,
+                             uint32_t info_count, uint32_t width, uint32_t height, const float* cam15, uint32_t bounces,
+                             float intensity, int stratified, uint32_t warmup, uint32_t frames, uint32_t seed,
+                             float* ms_per_frame, float* build_ms, float* image_out)
+{
+    try {
+        return refgpu_render_impl(tris_host, n, box, infos_host, info_count, width, height, cam15, bounces, intensity,
+                                  stratified, warmup, frames, seed, ms_per_frame, build_ms, image_out);
+    } catch (const std::exception& e) {
+        fprintf(stderr, "refgpu_render: %s\n", e.what());
+    } catch (...) {
+        fprintf(stderr, "refgpu_render: unknown exception\n");
+    }
+    return -3;
 }
 
 }  // extern "C"

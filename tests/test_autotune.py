@@ -76,3 +76,21 @@ def test_cache_round_trip(tmp_path):
     again = autotune.TuneCache(path).get(key)
     assert again == r and again.wave_paths == PIXELS and again.ray_sort == 0
     assert sorted(p.name for p in tmp_path.iterdir()) == ["tune.json"]
+
+
+def test_launch_shape_stage():
+    base = autotune.TuneResult(4 * PIXELS, 0, 10.0)
+    c = autotune.launch_candidates(base, refills=(0, 24, 24, 16), blocks=(0, 6))
+    assert c == [(4 * PIXELS, 0, 0, 0), (4 * PIXELS, 0, 24, 0), (4 * PIXELS, 0, 16, 0), (4 * PIXELS, 0, 0, 6)]
+    times = {(24, 0): 7.0, (16, 0): 8.0, (0, 6): 7.0}
+    r = autotune.tune(lambda w, s, rl, b: times.get((rl, b), 9.0), c)
+    assert (r.refill_lanes, r.blocks_per_sm, r.ms) == (24, 0, 7.0)
+    assert r.table[0] == {"wave_paths": 4 * PIXELS, "ray_sort": 0, "refill_lanes": 0, "blocks_per_sm": 0, "ms": 9.0}
+    with pytest.raises(ValueError):
+        autotune.launch_candidates(base, refills=(40,))
+    with pytest.raises(ValueError):
+        autotune.tune(lambda *a: 1.0, [(1, 0, 0)])
+    # the renderer accepts every candidate's fields (scratch sizes do not depend on them)
+    p = make_params(W, H, SPP, 0, 3, 3.0, True, 0, cpt.ACCUM_KAHAN, wave_paths=4 * PIXELS, refill_lanes=24,
+                    traverse_blocks_per_sm=6)
+    assert cpt.render_scratch_bytes(p) == scratch(4 * PIXELS, 0)

@@ -10,7 +10,9 @@
   extra pieces per triangle under the compressed 8-wide tree) over a 1.31 M-triangle
   sphere + hairball: the closest-hit triangle equals the oracle's reference
   traversal except for rays whose two nearest hits lie within 1 ulp of each other
-  (counted, required rare, and each alternative checked to be a real hit there).
+  (counted, required rare, and each alternative checked to be a real hit there) and
+  for rays the reference traversal's rounded slab test loses (each checked against
+  an exhaustive scan of all triangles: the GPU's hit is the nearest).
 * The deforming-mesh step (cpt_scene_deform) against a float64 host restatement,
   and the rebuild of the deformed mesh bit-exact against the oracle.
 """
@@ -115,13 +117,34 @@ def test_benchmark_traversal_matches_reference_hits_at_scale(cuda):
     t, idx, uv = cpu.trace(ob, rays[:, [0, 1, 2, 4, 5, 6]])
     ho = np.stack([t, uv[:, 0], uv[:, 1], idx.view(np.float32)], 1)
     ok, exact = tie_or_equal(hg, ho, ulps=1)
-    assert ok.all(), f"{int((~ok).sum())} rays differ beyond a 1-ulp tie"
     hit = idx != cpu.INVALID
     assert hit.mean() > 0.25
+    # Rays that differ beyond a 1-ulp tie: each is scanned against every triangle with
+    # the same float32 arithmetic. The reference's traversal rounds its slab test, so a
+    # ray grazing a box face can miss the box while the triangle inside is hit
+    # (test_oracle_bruteforce.py); the split and wide trees' boxes are widened, so they
+    # find it. Such a ray passes when the GPU's hit is the scan's nearest (up to a 1-ulp
+    # tie) and the reference's is farther or missing; any other difference fails.
+    bad = np.nonzero(~ok)[0]
+    assert len(bad) <= 1e-4 * len(rays), f"{len(bad)} rays differ beyond a 1-ulp tie"
+    if len(bad):
+        from test_oracle_bruteforce import mt_all
+
+        r6 = rays[bad][:, [0, 1, 2, 4, 5, 6]]
+        tb = mt_all(ob.tris, r6, block=1).min(axis=1)
+        tg = np.where(hg[bad, 0] < 3e38, hg[bad, 0], np.inf).astype(np.float64)
+        with np.errstate(over="ignore"):
+            ulp = np.spacing(np.abs(tb.astype(np.float32))).astype(np.float64)
+        gpu_nearest = np.isfinite(tb) & (np.abs(tg - tb.astype(np.float64)) <= ulp)
+        ref_farther = t[bad].astype(np.float64) > tb.astype(np.float64) + ulp
+        detail = [(int(i), float(hg[i, 0]), int(hg[i, 3].view(np.uint32)), float(t[i]), int(idx[i]), float(b))
+                  for i, b in zip(bad, tb)]
+        assert (gpu_nearest & ref_farther).all(), detail
     ties = ~exact
     assert ties.mean() < 1e-3, ties.sum()
     same_tri = hg[:, 3].view(np.uint32) == idx
     assert same_tri[~ties].all()
+    ties &= ok
     if ties.any():  # each alternative triangle is really hit at that distance
         alt = ob.tris[hg[ties, 3].view(np.uint32)]
         o = rays[ties, 0:3].astype(np.float64)

@@ -36,3 +36,36 @@ def test_reference_gpu_build_equals_ours(cuda, case):
     # counter (BVHBuilder.cu:63-86); a stale read would show here as a differing box
     differ = (out["node_boxes"].view(np.uint32).reshape(-1, 6) != ref.node_boxes.view(np.uint32).reshape(-1, 6))
     assert not differ.any(), f"{int(differ.any(1).sum())} internal boxes differ"
+
+
+def test_reference_gpu_render_estimates_the_same_image(cuda):
+    """The reference's raytrace_kernel (cuda_path_tracer.cu:385-421, its own curand
+    stream) and this library's renderer (the Philox stream) estimate the same image: over
+    512 one-sample frames each, the image means agree within 2 % and coarse 8x8-pixel
+    block means within 8 % (noise, not bias, at these sample counts)."""
+    if not cpu.refgpu_available():
+        pytest.fail("oracle/_ref/librefgpu.so was not built (make -C oracle ref)")
+    import torch
+
+    from cpt.device import DeviceRenderer, DeviceScene, make_params
+
+    tris, infos = cpt.scene_random(20_000, seed=5)
+    w, h, bounces, spp = 64, 48, 3, 512
+    cam = cpt.camera_look_at((0.5, 0.5, -1.2), (0.5, 0.5, 0.0), aspect=w / h)
+    stats, ref_img = cpu.refgpu_render(tris, infos, w, h, cam.as_array(), bounces, 3.0, True, warmup=0, frames=spp,
+                                       seed=3, image=True)
+    assert stats["ms_per_frame"] > 0 and np.isfinite(ref_img).all()
+    lb = DeviceLbvh(len(tris), 30)
+    lb.build(to_device(tris), check_root=True)
+    r = DeviceRenderer(make_params(w, h, spp, 0, bounces, 3.0, True, 9, cpt.ACCUM_KAHAN))
+    r.render(lb, DeviceScene(infos), cam)
+    torch.cuda.synchronize()
+    r.check_status()
+    ours = r.resolve().cpu().numpy()[..., :3].astype(np.float64)
+    theirs = ref_img[..., :3].astype(np.float64)
+    assert ours.mean() > 0.01
+    assert abs(theirs.mean() - ours.mean()) <= 0.02 * ours.mean(), (theirs.mean(), ours.mean())
+    bo = ours.reshape(h // 8, 8, w // 8, 8, 3).mean(axis=(1, 3))
+    bt = theirs.reshape(h // 8, 8, w // 8, 8, 3).mean(axis=(1, 3))
+    lit = bo > 0.05 * bo.max()
+    assert np.all(np.abs(bt[lit] - bo[lit]) <= 0.08 * bo[lit] + 1e-3)
