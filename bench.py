@@ -263,13 +263,19 @@ def reference_gpu(w, tris, infos, cam, dev, ours_ms_per_spp, rays_per_spp, reps=
     expected count is the estimator's). None when that library was not built."""
     import torch
 
-    from oracle import cpu
+    import cpt
+    from oracle import cpu, refgpu_child
     from cpt.device import DeviceLbvh, to_device
 
     if not cpu.refgpu_available():
         return None
     n = len(tris)
-    ref, _ = cpu.refgpu_build(tris, reps=reps)
+    box = cpt.scene_bounds(tris)
+    try:  # in a child process: the reference's thrust and CUDA runtime stay out of this one
+        r = refgpu_child.run("build", tris, box, reps=reps, outputs=False)
+    except Exception as e:
+        return {"unavailable": str(e)[-300:]}
+    ref = {k: float(r[k]) for k in ("ms_mean", "ms_min", "wall_ms_mean")}
     lb = DeviceLbvh(n, 30, dev)
     d = to_device(tris, dev)
     lb.build(d, check_root=True)
@@ -291,8 +297,15 @@ def reference_gpu(w, tris, infos, cam, dev, ours_ms_per_spp, rays_per_spp, reps=
                     "reference_mtris_s": round(n / ref["ms_mean"] / 1e3, 2), "ours_ms": round(ours, 4),
                     "ours_mtris_s": round(n / ours / 1e3, 2), "speedup": round(ref["ms_mean"] / ours, 2)}}
     if w["width"] % 8 == 0 and w["height"] % 8 == 0:
-        r, img = cpu.refgpu_render(tris, infos, w["width"], w["height"], cam.as_array(), w["bounces"], 3.0, True,
-                                   warmup=2, frames=frames, seed=w["seed"] + 1, image=True)
+        try:
+            rr = refgpu_child.run("render", tris, box, infos=infos, width=w["width"], height=w["height"],
+                                  cam15=cam.as_array(), bounces=w["bounces"], intensity=3.0, stratified=1, warmup=2,
+                                  frames=frames, seed=w["seed"] + 1)
+        except Exception as e:
+            out["render"] = {"unavailable": str(e)[-300:]}
+            return out
+        r = {"ms_per_frame": float(rr["ms_per_frame"]), "build_ms": float(rr["build_ms"])}
+        img = rr["image"]
         ref_mrays = rays_per_spp / r["ms_per_frame"] / 1e3
         out["render"] = {"reference": "raytrace_kernel (cuda_path_tracer.cu:385-421), 8x8 blocks, one sample per "
                                       "pixel per launch, over its own 30-bit LBVH",
@@ -638,7 +651,8 @@ def run_ours(args, w, world, rank, local):
     if args.wide:
         lb.wide(keep_scratch=True)
     params = make_params(W_, H_, spp, 0, w["bounces"], 3.0, True, w["seed"], cpt.ACCUM_KAHAN,
-                         wave_paths=args.wave_paths, ray_sort=bool(args.ray_sort), cameras=len(cams))
+                         wave_paths=args.wave_paths, ray_sort=bool(args.ray_sort), cameras=len(cams),
+                         refill_lanes=args.refill_lanes, traverse_blocks_per_sm=args.blocks_per_sm)
 
     def deform_and_rebuild(frame_index):
         # the deforming-mesh step: move the vertices, then a full LBVH rebuild
@@ -889,9 +903,7 @@ def run_ours(args, w, world, rank, local):
     if rank == 0 and world == 1 and args.workload == "c2" and not args.no_cache_ratio:
         wc = dict(WORKLOADS["c4"])
         wc.update(width=W_, height=H_)
-        from cpt.device import rc_default_params
-
-        r4 = cache_experiment(wc, lb, scene, cams[0], dev, True, args.warmup, wc["spp"], rc_default_params())
+        r4 = cache_experiment(wc, lb, scene, cams[0], dev, True, args.warmup, wc["spp"], rc_params_for(args, wc["spp"]))
         cache_c4 = {"metric": "time-to-equal-RMSE (cache / plain, vs FP64 image), stratified first bounce",
                     "value": r4["ratio"], "unit": "x", "higher_is_better": False,
                     "plain": r4["plain"], "cache": {k: r4["cache"][k] for k in
@@ -1060,7 +1072,8 @@ def cache_experiment(w, lb, scene, cam, dev, stratified, warmup, spf, rc_params,
             "cache": {"spp": spp, "spp_per_frame": spf, "warm_updates": w["warm_updates"],
                       "warm_ms": round(t_warm, 2), "ms": round(t_cache, 2), "reached": reached,
                       "mrays_s": round(cache_rays / t_cache / 1e3, 3), "training_samples_last_frame": samples_last,
-                      "training": "about train_samples of each frame's own paths, traced to full depth",
+                      "training": f"about {rc_params.train_samples} of a frame's own paths traced to full depth, "
+                                  f"every {max(1, rc_params.train_interval)} frame(s)",
                       "kernel_ms": {k: round(v[0], 3) for k, v in sorted(prof.items())}},
             "reference": {"resolution": f"{rw}x{rh} (every {rdiv}th pixel of {W_}x{H_})",
                           "spp": w["ref_spp"], "accum": "f64", "s": round(ref_s, 2)},
@@ -1068,11 +1081,14 @@ def cache_experiment(w, lb, scene, cam, dev, stratified, warmup, spf, rc_params,
 
 
 def rc_params_for(args, spf):
-    """2^16 training paths and 4 optimiser steps per frame (one render call of `spf`
-    samples), or — with --rc-per-sample — per image sample."""
+    """2^16 training paths and 4 optimiser steps per training frame (one render call of
+    `spf` samples; every --rc-interval-th frame trains), or — with --rc-per-sample — per
+    image sample."""
     from cpt.device import rc_default_params
 
-    p = rc_default_params()
+    p = rc_default_params(train_interval=args.rc_interval)
+    if args.rc_train_paths:
+        p.train_samples = args.rc_train_paths
     if args.rc_per_sample:
         p.train_samples *= spf
         p.train_steps *= spf
@@ -1168,11 +1184,19 @@ def main():
     ap.add_argument("--hair", type=int, default=None, help="override the hairball's triangle count (profiling runs)")
     ap.add_argument("--wave-paths", type=int, default=0, help="paths per wave (0: library default)")
     ap.add_argument("--ray-sort", type=int, default=0, help="1: coherence-sort bounce queues")
+    ap.add_argument("--refill-lanes", type=int, default=0,
+                    help="traversal warps take new rays below this many busy lanes (0: library default)")
+    ap.add_argument("--blocks-per-sm", type=int, default=0,
+                    help="resident traversal blocks per SM (0: occupancy)")
     ap.add_argument("--wide", type=int, default=None,
                     help="1: traverse the compressed 8-wide tree built from the (split) binary tree, 0: the binary "
                          "tree (default per workload)")
     ap.add_argument("--rc-per-sample", action="store_true",
                     help="c4: 2^16 training suffixes per image sample instead of per render call (frame)")
+    ap.add_argument("--rc-interval", type=int, default=8,
+                    help="radiance cache: train on every n-th frame's own paths (the others only read the cache)")
+    ap.add_argument("--rc-train-paths", type=int, default=0,
+                    help="radiance cache: training paths per training frame (0: the library default, 2^16)")
     ap.add_argument("--nee", type=int, default=1,
                     help="c4: also compare with next-event estimation in both tracers (1) or not (0)")
     ap.add_argument("--split", type=float, default=None,

@@ -125,7 +125,7 @@ _P, _U32, _I32, _SZ, _F = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes
 class RcParams(ctypes.Structure):
     _fields_ = [("learning_rate", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
                 ("epsilon", ctypes.c_float), ("ema_decay", ctypes.c_float), ("train_samples", ctypes.c_uint32),
-                ("train_steps", ctypes.c_uint32), ("seed", ctypes.c_uint32)]
+                ("train_steps", ctypes.c_uint32), ("seed", ctypes.c_uint32), ("train_interval", ctypes.c_uint32)]
 _PROTOS = {
     "cpt_bvh_bytes": (_SZ, [_U32, _I32]),
     "cpt_bvh_bind": (_I32, [_P, _SZ, _U32, _I32, ctypes.POINTER(Bvh)]),

@@ -554,6 +554,7 @@ extern "C" void cpt_rc_default_params(cpt_rc_params* p)
     p->train_samples = 1u << 16;
     p->train_steps = 4;
     p->seed = 1337u;
+    p->train_interval = 1;
 }
 
 extern "C" size_t cpt_rc_param_count(void) { return (size_t)kParams; }
@@ -764,12 +765,14 @@ int rc_frame(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_rend
     // (chosen by a hash of pixel and sample) are traced to full depth — their vertex-1
     // records give the training targets, their full estimate goes into the image — and
     // every other path stops at vertex 1 and takes the cache's prediction for the rest.
+    const uint32_t interval = std::max(1u, rc->params.train_interval);
+    const bool train = (params->frame0 / std::max(1u, params->spp)) % interval == 0;
     CPT_CUDA_TRY(cudaMemsetAsync(rc->sample_count, 0, sizeof(uint32_t), stream));
     CPT_CUDA_TRY(cudaMemsetAsync(rc->train_count, 0, sizeof(uint32_t), stream));
     uint64_t pixels = 0;
     for (uint32_t i = 0; i < n_views; ++i) pixels += (uint64_t)views[i].width * views[i].height;
     const uint64_t paths = pixels * params->spp;
-    Ctx cr{rc, box, false, true};
+    Ctx cr{rc, box, false, train};
     RenderHook h{};
     h.records = records;
     h.capacity = cap_r;
@@ -780,10 +783,10 @@ int rc_frame(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_rend
     h.train_records = rc->train_records;
     h.train_count = rc->train_count;
     h.train_capacity = rc->train_cap;
-    h.train_stride = (uint32_t)std::max<uint64_t>(1, paths / std::max(1u, rc->params.train_samples));
+    h.train_stride = train ? (uint32_t)std::max<uint64_t>(1, paths / std::max(1u, rc->params.train_samples)) : 0u;
     h.cut_at_record = true;
     int r = cpt_render_views_hooked(views, n_views, params, scratch, render_part, ray_counts, status, &h, stream);
-    if (r) return r;
+    if (r || !train) return r;
     // optimiser steps over this frame's targets (the next frame's predictions use them)
     for (uint32_t s = 0; s < steps; ++s) {
         r = train_batch(rc, rc->samples, rc->sample_count, 0, s, steps, box, nullptr, stream);

@@ -84,11 +84,16 @@ __device__ __forceinline__ float slab_test_fma(f3 odinv, f3 dinv, float ax, floa
 // Packed FP32 pairs (sm_100: add / sub / mul / fma .rn.f32x2). Each lane of the pair
 // is rounded exactly as the scalar round-to-nearest operation on it, so a packed
 // sequence gives the bits of the scalar one; it issues one instruction per pair.
-// Off by default: on C2 the packed forms ran 1.5 % faster (483.8 vs 476.8 Mrays/s), but
-// the packed triangle test did not reproduce the scalar sequence's bits on the device
-// (the render parity tests failed with it), and exact hits are required here.
-#ifndef CPT_PACKED_F32
-#define CPT_PACKED_F32 0
+// CPT_PACKED_TRI: the packed Moller-Trumbore. Off: on the device it did not reproduce the
+// scalar sequence's bits (the render parity tests failed with it), and exact hits are
+// required here. CPT_PACKED_BOX: the packed plane evaluation of the wide tree's box test,
+// which only steers pruning (its slack absorbs rounding); both together ran C2 1.5 %
+// faster (483.8 vs 476.8 Mrays/s).
+#ifndef CPT_PACKED_TRI
+#define CPT_PACKED_TRI 0
+#endif
+#ifndef CPT_PACKED_BOX
+#define CPT_PACKED_BOX 0
 #endif
 struct f2 { float x, y; };
 __device__ __forceinline__ f2 mk2(float x, float y) { f2 r; r.x = x; r.y = y; return r; }
@@ -122,7 +127,7 @@ __device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
 // lane's operations in the scalar order: the same bits.
 __device__ __forceinline__ float tri_test(f3 o, f3 d, const float* s, float& u, float& v)
 {
-#if CPT_PACKED_F32
+#if CPT_PACKED_TRI
     const f3 p0 = mk3(s[0], s[1], s[2]), e1 = mk3(s[4], s[5], s[6]), e2 = mk3(s[7], s[8], s[9]);
     const f3 sv = sub(o, p0);
     // (q, r) component-wise: q = cross(d, e2), r = cross(sv, e1) (cross(a, b).x = a.y b.z - b.y a.z, ...)
@@ -461,7 +466,7 @@ __device__ __forceinline__ uint32_t wide_child_hits(const WideState& s, float4 n
     const uint32_t nz0 = fz ? hz0 : lz0, nz1 = fz ? hz1 : lz1, fz0 = fz ? lz0 : hz0, fz1 = fz ? lz1 : hz1;
     uint32_t hm = 0;
     const float tlim = s.best.t;
-#if CPT_PACKED_F32
+#if CPT_PACKED_BOX
     // the near and far plane of an axis share the multiplier and the offset: one packed
     // fused multiply-add per axis and child gives (t_near, t_far), each lane rounded as
     // the scalar fmaf

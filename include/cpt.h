@@ -477,9 +477,12 @@ typedef struct cpt_rc_params {
     float beta1, beta2;      /* 0.9, 0.99 */
     float epsilon;           /* 1e-15 */
     float ema_decay;         /* inference weights: 0 = the trained weights, else their moving average */
-    uint32_t train_samples;  /* training paths per frame, 65536 */
-    uint32_t train_steps;    /* optimizer steps per frame; the samples are split between them */
+    uint32_t train_samples;  /* training paths per training frame, 65536 */
+    uint32_t train_steps;    /* optimizer steps per training frame; the samples are split between them */
     uint32_t seed;           /* weight initialisation */
+    uint32_t train_interval; /* cpt_rc_render trains on the frames whose first sample index / spp is a
+                              * multiple of this (0 or 1: every frame); the other frames stop every path
+                              * at vertex 1 and only read the cache */
 } cpt_rc_params;
 void cpt_rc_default_params(cpt_rc_params* p);
 size_t cpt_rc_param_count(void);
@@ -496,11 +499,14 @@ int cpt_rc_infer(cpt_rc* rc, const float* samples, uint32_t n, const float box[6
  * (nullable) = mean relative L2 over the samples before their step. Synchronizes. */
 int cpt_rc_train(cpt_rc* rc, const float* samples, uint32_t n, const float box[6], uint32_t steps, float* loss_out,
                  cudaStream_t stream);
-/* One cached frame of the views (as cpt_render_views): trains on this frame's
- * training paths (train_samples full-depth paths over reduced copies of the views,
- * an independent random stream), then renders vertices 0 and 1 exactly and the
- * rest of each path from the cache. bounces < 2 renders plain paths. The position
- * box is views[0].bvh's root box. */
+/* One cached frame of the views (as cpt_render_views), training on its own paths:
+ * about train_samples of the frame's paths, chosen by a hash of pixel and sample, are
+ * traced to full depth — their estimate goes into the image and their radiance after
+ * vertex 1 becomes a training target — and every other path is traced through vertex 1
+ * and takes the cache's prediction for the rest; then train_steps optimizer steps over
+ * the targets (used by the next frame). On frames that the train_interval skips, every
+ * path takes the prediction and nothing is trained. bounces < 2 renders plain paths.
+ * The position box is views[0].bvh's root box. */
 size_t cpt_rc_render_scratch_bytes(const cpt_rc* rc, const cpt_view* views, uint32_t n_views,
                                    const cpt_render_params* params);
 int cpt_rc_render(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_render_params* params, void* scratch,

@@ -143,7 +143,8 @@ def refgpu_render(tris: np.ndarray, infos: np.ndarray, width: int, height: int, 
     L = refgpu_lib()
     ms, bms = ctypes.c_float(), ctypes.c_float()
     img = np.zeros((height, width, 4), np.float32) if image else None
-    rc = L.refgpu_render(_p(tris), len(tris), _p(box), _p(infos), len(infos), width, height, _p(cam15), bounces,
+    info_count = infos.nbytes // 192  # CUDA::TriangleInfo records (TriangleInfo.h:31-75), 192 B each
+    rc = L.refgpu_render(_p(tris), len(tris), _p(box), _p(infos), info_count, width, height, _p(cam15), bounces,
                          intensity, int(stratified), warmup, frames, seed, ctypes.byref(ms), ctypes.byref(bms),
                          _p(img))
     if rc != 0:

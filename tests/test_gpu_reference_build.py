@@ -9,7 +9,7 @@ import pytest
 import cpt
 from conftest import quantized
 from cpt.device import DeviceLbvh, to_device
-from oracle import cpu
+from oracle import cpu, refgpu_child
 
 pytestmark = pytest.mark.gpu
 
@@ -25,8 +25,12 @@ def test_reference_gpu_build_equals_ours(cuda, case):
     else:
         tris = cpt.scene_sphere_hairball(256, 128, 30_000, seed=5)[0]
     box = cpu.enclosing_box(tris)
-    stats, ref = cpu.refgpu_build(tris, box=box, reps=1, outputs=True)
-    assert stats["ms_mean"] > 0
+    r = refgpu_child.run("build", tris, box, reps=1, outputs=True)  # in a process of its own
+    assert float(r["ms_mean"]) > 0
+    ref = cpu.BuildResult(len(tris), 30)
+    ref.tris = r["tris_out"].view(cpu.TRIANGLE_DTYPE)
+    ref.children, ref.parents_leaf, ref.parents_internal = r["children"], r["parents_leaf"], r["parents_internal"]
+    ref.node_boxes = r["node_boxes"].view(cpu.BBOX_DTYPE)
     lb = DeviceLbvh(len(tris), 30)
     lb.build(to_device(tris), box=box, check_root=True)
     out = lb.download()
@@ -52,9 +56,11 @@ def test_reference_gpu_render_estimates_the_same_image(cuda):
     tris, infos = cpt.scene_random(20_000, seed=5)
     w, h, bounces, spp = 64, 48, 3, 512
     cam = cpt.camera_look_at((0.5, 0.5, -1.2), (0.5, 0.5, 0.0), aspect=w / h)
-    stats, ref_img = cpu.refgpu_render(tris, infos, w, h, cam.as_array(), bounces, 3.0, True, warmup=0, frames=spp,
-                                       seed=3, image=True)
-    assert stats["ms_per_frame"] > 0 and np.isfinite(ref_img).all()
+    rr = refgpu_child.run("render", tris, cpu.enclosing_box(tris), infos=infos, width=w, height=h,
+                          cam15=cam.as_array(), bounces=bounces, intensity=3.0, stratified=1, warmup=0, frames=spp,
+                          seed=3)
+    ref_img = rr["image"]
+    assert float(rr["ms_per_frame"]) > 0 and np.isfinite(ref_img).all()
     lb = DeviceLbvh(len(tris), 30)
     lb.build(to_device(tris), check_root=True)
     r = DeviceRenderer(make_params(w, h, spp, 0, bounces, 3.0, True, 9, cpt.ACCUM_KAHAN))
