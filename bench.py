@@ -319,6 +319,66 @@ def reference_gpu(w, tris, infos, cam, dev, ours_ms_per_spp, rays_per_spp, reps=
     return out
 
 
+def extra_builds(dev, reps=5):
+    """Two build measurements the driver's default run carries beside C2: a full rebuild
+    of the 16.8 M-triangle displaced sphere of C5 after a deformation step (63-bit keys),
+    and C3's 64 scenes as one batched build against 64 single builds. Scenes generated on
+    the host (seeded), resident on the device; CUDA events."""
+    import torch
+
+    import cpt
+    from cpt.device import DeviceLbvh, LbvhBatch, stream_handle, to_device
+
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {}
+    w5 = WORKLOADS["c5"]
+    rest, _ = cpt.scene_sphere_hairball(w5["nu"], w5["nv"], 0, seed=w5["seed"])
+    n5 = len(rest)
+    d_rest, d_tris = to_device(rest, dev), to_device(rest, dev)
+    cpt.check(cpt.lib.cpt_scene_deform(d_rest.data_ptr(), d_tris.data_ptr(), n5, w5["amp"], w5["omega"], 0.1,
+                                       stream_handle()), "cpt_scene_deform")
+    lb = DeviceLbvh(n5, 63, dev)
+    lb.build(d_tris, check_root=True)
+    ms = timed(lambda: lb.build(d_tris))
+    lb.status()
+    out["c5_rebuild"] = {"triangles": n5, "morton_bits": 63, "ms": round(ms, 3), "mtris_s": round(n5 / ms / 1e3, 2),
+                         "what": "cpt_lbvh_build of the deformed 4096x2048x2 displaced sphere, box computed on the "
+                                 "device"}
+    del lb, d_rest, d_tris
+    torch.cuda.empty_cache()
+    w3 = WORKLOADS["c3"]
+    lbs, srcs, boxes = [], [], []
+    for i, (kind, ntri, _side) in enumerate(batch_specs(w3)):
+        tris, _ = batch_scene(kind, ntri, w3["seed"] + i)
+        lbs.append(DeviceLbvh(len(tris), w3["bits"], dev))
+        srcs.append(to_device(tris, dev))
+        boxes.append(cpt.scene_bounds(tris))
+    batch = LbvhBatch(lbs, dev)
+    batch.build(srcs, boxes, check_root=True)
+    n3 = sum(lb.n for lb in lbs)
+    t_batch = timed(lambda: batch.build(srcs, boxes))
+    t_single = timed(lambda: [lb.build(d) for lb, d in zip(lbs, srcs)])
+    for lb in lbs:
+        lb.status()
+    out["c3_batch_build"] = {"scenes": len(lbs), "triangles": n3, "morton_bits": w3["bits"],
+                             "batched_ms": round(t_batch, 3), "batched_mtris_s": round(n3 / t_batch / 1e3, 2),
+                             "single_calls_ms": round(t_single, 3),
+                             "single_calls_mtris_s": round(n3 / t_single / 1e3, 2)}
+    return out
+
+
 def frame_parity(gpu_sums, cpu_sums, spp):
     """GPU frame-0 rows (FP64 accumulator) against the reference's rows (float64 sums
     of the same float samples in the same order): pixels whose three sums differ in
@@ -899,17 +959,36 @@ def run_ours(args, w, world, rank, local):
 
     # --- radiance cache (the C4 configuration on this scene and tree): time to reach the
     # plain tracer's 64-sample error against an FP64 image, 1-sample cached frames
-    cache_c4 = None
+    cache_c4, r4 = None, None
     if rank == 0 and world == 1 and args.workload == "c2" and not args.no_cache_ratio:
         wc = dict(WORKLOADS["c4"])
         wc.update(width=W_, height=H_)
-        r4 = cache_experiment(wc, lb, scene, cams[0], dev, True, args.warmup, wc["spp"], rc_params_for(args, wc["spp"]))
+        try:
+            r4 = cache_experiment(wc, lb, scene, cams[0], dev, True, args.warmup, wc["spp"],
+                                  rc_params_for(args, wc["spp"]))
+        except Exception as e:  # an extra measurement never takes the main line down
+            r4 = None
+            cache_c4 = {"error": f"{type(e).__name__}: {e}"[:300]}
+    if r4 is not None:
         cache_c4 = {"metric": "time-to-equal-RMSE (cache / plain, vs FP64 image), stratified first bounce",
                     "value": r4["ratio"], "unit": "x", "higher_is_better": False,
+                    "value_same_frames": r4["ratio_same_frames"],
+                    "note": "value: plain tracer in 16-sample frames (its fastest); value_same_frames: plain "
+                            "tracer in frames of the cached tracer's size (1 sample, the C4 configuration)",
+                    "plain_same_frames_ms": r4["plain_same_frames_ms"],
                     "plain": r4["plain"], "cache": {k: r4["cache"][k] for k in
                                                     ("spp", "spp_per_frame", "ms", "warm_ms", "reached", "mrays_s",
                                                      "training_samples_last_frame", "training")},
                     "reference": r4["reference"], "curve_tail": r4["cache_curve"][-4:]}
+
+    # --- build measurements at the C5 and C3 scales (default C2 run, rank 0)
+    builds = None
+    if rank == 0 and world == 1 and args.workload == "c2" and not args.no_extra_builds:
+        try:
+            builds = extra_builds(dev)
+        except Exception as e:  # an extra measurement never takes the main line down
+            builds = {"error": f"{type(e).__name__}: {e}"[:300]}
+        torch.cuda.empty_cache()
 
     # --- CPU baseline (rank 0, N = 1): the reference's code on every k-th row of frame 0,
     # and the parity of the GPU's frame 0 (FP64 accumulator, same traversal tree as the
@@ -947,7 +1026,7 @@ def run_ours(args, w, world, rank, local):
                                      + (", treelet-restructured" if args.treelet else "") + ")" if split > 0
                                      else "LBVH (reference topology)")), "lbvh_topology": lbvh_topology,
                 "cpu_baseline": cpu_base, "parity": parity, "reference_gpu": ref_gpu,
-                "radiance_cache_c4": cache_c4, "e2e": e2e,
+                "radiance_cache_c4": cache_c4, "builds_c5_c3": builds, "e2e": e2e,
                 "gpu_launches": int(launches),
                 "clocks": clocks,
                 "parallelism": f"replicas x{world}: own BVH per GPU, disjoint sample streams, "
@@ -1011,11 +1090,19 @@ def cache_experiment(w, lb, scene, cam, dev, stratified, warmup, spf, rc_params,
     for i in range(max(1, warmup)):
         plain.render(frame0=100000 + 16 * i)
     torch.cuda.synchronize()
-    plain.accums[0].zero_()
-    plain.counts.zero_()
-    t_plain = 0.0
-    for f in range(w["plain_spp"] // 16):
-        t_plain += timed(lambda: plain.render(frame0=16 * f))
+
+    def plain_run(frame_spp):
+        """The plain tracer's first plain_spp samples in frames of frame_spp samples: time,
+        and the accumulator (the same samples in the same order whatever the frame size)."""
+        plain.accums[0].zero_()
+        plain.counts.zero_()
+        t = 0.0
+        for f in range(w["plain_spp"] // frame_spp):
+            t += timed(lambda: plain.render(frame0=frame_spp * f, spp=frame_spp))
+        return t
+
+    t_plain_same = plain_run(spf) if spf != 16 else None  # frames of the cached tracer's size
+    t_plain = plain_run(16)
     plain.check_status()
     rmse_plain = rmse(plain.accums[0])
     plain_rays = int(plain.counts[:3].sum())
@@ -1065,6 +1152,8 @@ def cache_experiment(w, lb, scene, cam, dev, stratified, warmup, spf, rc_params,
     rc.close()
     # the curve at the plain tracer's sample count, for the record
     return {"stratified": stratified, "nee": nee, "ratio": round(t_cache / t_plain, 4) if reached else None,
+            "ratio_same_frames": (round(t_cache / t_plain_same, 4) if reached and t_plain_same else None),
+            "plain_same_frames_ms": None if t_plain_same is None else round(t_plain_same, 2),
             "t_cache_ms": round(t_cache, 2), "cache_curve": curve if len(curve) <= 80 else curve[::4] + curve[-1:],
             "plain_to_reference_rmse": reach_out,
             "plain": {"spp": w["plain_spp"], "frames_spp": 16, "ms": round(t_plain, 2), "rmse": round(rmse_plain, 6),
@@ -1141,6 +1230,9 @@ def run_cache(args, w, world, rank, local):
                 "cache_vs_plain_both_nee": nee_run["ratio"]}
     if rank == 0:
         line = {"metric": "time-to-equal-RMSE (cache / plain, vs FP64 image)", "value": main_run["ratio"],
+                "value_same_frames": main_run["ratio_same_frames"],
+                "note": "value: plain tracer in 16-sample frames (its fastest); value_same_frames: plain tracer in "
+                        "frames of the cached tracer's size",
                 "unit": "x", "n_gpus": world, "steps": main_run["cache"]["spp"] // spf, "warmup": args.warmup,
                 "ms_per_step": round(main_run["cache"]["ms"] / max(1, main_run["cache"]["spp"] // spf), 3),
                 "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -1176,12 +1268,15 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extra-builds", action="store_true",
+                    help="c2: skip the C5-scale rebuild and the C3 batched build measurements")
     ap.add_argument("--no-cache-ratio", action="store_true",
                     help="c2: skip the radiance cache's time-to-equal-RMSE measurement (the C4 configuration)")
     ap.add_argument("--res", default=None, help="override resolution WxH (profiling runs)")
     ap.add_argument("--spp", type=int, default=None, help="override samples per frame (profiling runs)")
     ap.add_argument("--sphere", default=None, help="override the sphere's grid NUxNV (profiling runs)")
     ap.add_argument("--hair", type=int, default=None, help="override the hairball's triangle count (profiling runs)")
+    ap.add_argument("--scenes", type=int, default=None, help="c3: override the scene count (profiling runs)")
     ap.add_argument("--wave-paths", type=int, default=0, help="paths per wave (0: library default)")
     ap.add_argument("--ray-sort", type=int, default=0, help="1: coherence-sort bounce queues")
     ap.add_argument("--refill-lanes", type=int, default=0,
@@ -1219,6 +1314,8 @@ def main():
         w["nu"], w["nv"] = (int(x) for x in args.sphere.lower().split("x"))
     if args.hair is not None:
         w["n_hair"] = args.hair
+    if args.scenes is not None:
+        w["scenes"] = args.scenes
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))

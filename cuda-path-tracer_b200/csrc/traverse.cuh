@@ -84,16 +84,17 @@ __device__ __forceinline__ float slab_test_fma(f3 odinv, f3 dinv, float ax, floa
 // Packed FP32 pairs (sm_100: add / sub / mul / fma .rn.f32x2). Each lane of the pair
 // is rounded exactly as the scalar round-to-nearest operation on it, so a packed
 // sequence gives the bits of the scalar one; it issues one instruction per pair.
-// CPT_PACKED_TRI: the packed Moller-Trumbore. Off: on the device it did not reproduce the
-// scalar sequence's bits (the render parity tests failed with it), and exact hits are
-// required here. CPT_PACKED_BOX: the packed plane evaluation of the wide tree's box test,
-// which only steers pruning (its slack absorbs rounding); both together ran C2 1.5 %
-// faster (483.8 vs 476.8 Mrays/s).
+// CPT_PACKED_BOX (on): the packed plane evaluation of the wide tree's box test — one
+// packed fused multiply-add gives an axis's near and far plane — which only steers
+// pruning: C2 495.2 against 474.0 Mrays/s. CPT_PACKED_TRI (off): the packed
+// Moller-Trumbore; on the device a quarter of its cross-product lanes came out 1 ulp from
+// the scalar sequence (a packed multiply and subtract contracted into one fused
+// operation), and exact hits are required here.
 #ifndef CPT_PACKED_TRI
 #define CPT_PACKED_TRI 0
 #endif
 #ifndef CPT_PACKED_BOX
-#define CPT_PACKED_BOX 0
+#define CPT_PACKED_BOX 1
 #endif
 struct f2 { float x, y; };
 __device__ __forceinline__ f2 mk2(float x, float y) { f2 r; r.x = x; r.y = y; return r; }

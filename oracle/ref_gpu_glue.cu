@@ -11,6 +11,32 @@
 // (:238-242) and the root-box read-back (:258-265). Only the QueryManager timer is a
 // no-op stand-in (oracle/ref_shim). BBox.cpp's host/device methods are compiled in
 // the same translation unit, as the reference's build compiles them for the device.
+// The reference declares CUDA::swap(T&, T&) as a __device__-only template
+// (application/cuda/util.h:14-20). This toolkit's thrust swaps a vector's storage with an
+// unqualified swap, so for vectors of CUDA:: types (CUDA::Triangle, CUDA::TriangleInfo)
+// argument-dependent lookup selects that device-only function in host code, whose host
+// copy ends the process (the reference's own Scene::upload assignment takes this path).
+// These overloads for thrust's vector iterators and allocators are more specialized, so
+// overload resolution prefers them, and they run on the host.
+#include <thrust/device_vector.h>
+namespace CUDA
+{
+template <typename Ptr>
+__host__ __device__ inline void swap(thrust::detail::normal_iterator<Ptr>& a, thrust::detail::normal_iterator<Ptr>& b)
+{
+    thrust::detail::normal_iterator<Ptr> t = a;
+    a = b;
+    b = t;
+}
+template <typename T>
+__host__ __device__ inline void swap(thrust::device_allocator<T>& a, thrust::device_allocator<T>& b)
+{
+    thrust::device_allocator<T> t = a;
+    a = b;
+    b = t;
+}
+}  // namespace CUDA
+
 #include "engine/geometry/BBox.cpp"
 #include "application/cuda/BVHBuilder.cu"
 // The reference's path tracer (raytrace_kernel and the shading it calls,
@@ -25,7 +51,9 @@
 
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <exception>
+#include <execinfo.h>
 #include <unistd.h>
 
 namespace {
@@ -37,6 +65,37 @@ struct StdoutToStderr {
     StdoutToStderr() { std::cout.flush(); fflush(stdout); saved = dup(1); dup2(2, 1); }
     ~StdoutToStderr() { std::cout.flush(); fflush(stdout); dup2(saved, 1); close(saved); }
 };
+
+// With CPT_REFGPU_TRACE set, each step of a call is reported on stderr, and a process
+// exit that passes through exit() prints where it came from (diagnostics of the child
+// process that runs this library).
+bool trace_on()
+{
+    static const bool on = getenv("CPT_REFGPU_TRACE") != nullptr;
+    return on;
+}
+
+void trace(const char* what)
+{
+    if (!trace_on()) return;
+    fprintf(stderr, "refgpu: %s\n", what);
+    fflush(stderr);
+}
+
+void exit_backtrace()
+{
+    void* frames[32];
+    const int k = backtrace(frames, 32);
+    fprintf(stderr, "refgpu: process exit via exit(); backtrace:\n");
+    backtrace_symbols_fd(frames, k, 2);
+}
+
+struct ExitTrace {
+    ExitTrace()
+    {
+        if (trace_on()) atexit(exit_backtrace);
+    }
+} g_exit_trace;
 
 }  // namespace
 
@@ -83,14 +142,17 @@ static int refgpu_build_impl(const void* tris_host, uint32_t n, const float* box
                              uint32_t* parents_leaf_out, uint32_t* parents_internal_out, float* boxes_out)
 {
     if (!tris_host || !box || n < 2 || reps < 1) return -1;
+    trace("build: start");
     StdoutToStderr quiet;
     const CUDA::Triangle* in = static_cast<const CUDA::Triangle*>(tris_host);
     thrust::device_vector<CUDA::Triangle> source(in, in + n);
+    trace("build: triangles uploaded");
     CUDA::DeviceSceneDescription desc;
     desc.triangles = source;
     desc.enclosingBBox = BBox(glm::vec3(box[0], box[1], box[2]), glm::vec3(box[3], box[4], box[5]));
     CUDA::BVHBuilder builder;
     builder.build(desc, n);  // warm-up: first allocations, thrust's temporary storage
+    trace("build: warm-up build done");
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return -2;
     double sum = 0.0, wall = 0.0;
@@ -122,6 +184,7 @@ static int refgpu_build_impl(const void* tris_host, uint32_t n, const float* box
     if (parents_internal_out) thrust::copy(desc.parents[1].begin(), desc.parents[1].end(), parents_internal_out);
     if (boxes_out)
         thrust::copy(desc.internalNodeBBoxes.begin(), desc.internalNodeBBoxes.end(), reinterpret_cast<BBox*>(boxes_out));
+    trace("build: done");
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

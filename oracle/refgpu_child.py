@@ -46,9 +46,19 @@ def run(op: str, tris: np.ndarray, box, infos=None, timeout: float = 600.0, **kw
             return {k: z[k] for k in z.files}
 
 
+def _trace(what: str) -> None:
+    if os.environ.get("CPT_REFGPU_TRACE"):
+        print(f"refgpu_child: {what}", file=sys.stderr, flush=True)
+
+
 def _main(src: str, dst: str) -> int:
     sys.path.insert(0, os.path.dirname(HERE))
+    _trace("start")
     from oracle import cpu
+
+    _trace("oracle imported")
+    cpu.refgpu_lib()
+    _trace("library loaded")
 
     z = np.load(src)
     op = str(z["op"])
@@ -71,7 +81,9 @@ def _main(src: str, dst: str) -> int:
     else:
         print(json.dumps({"error": f"unknown op {op}"}), file=sys.stderr)
         return 2
+    _trace(f"{op} returned")
     np.savez(dst, **out)
+    _trace("results written")
     return 0
 
 

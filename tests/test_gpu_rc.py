@@ -163,7 +163,7 @@ def test_training_targets_are_path_suffixes(cuda):
     cr.render()
     torch.cuda.synchronize()
     s = rc.samples()
-    assert len(s) > 1000
+    assert len(s) > 500  # every path of this small frame is a training path; those reaching vertex 1
     t = s[:, [3, 7, 11]]
     assert np.all(t >= 0) and np.isfinite(t).all()
     assert (t > 0).any()
