@@ -36,8 +36,8 @@
 namespace cpt {
 
 constexpr int kMortonBlock = 256;
-constexpr int kBoundsBlock = 256;
-constexpr int kBoundsBlocks = 1024;
+constexpr int kBoundsBlock = 320;   // 10 warps; a multiple of 5 (one word phase per thread)
+constexpr int kBoundsBlocks = 888;  // 148 SMs x 6 blocks
 
 struct BoxArg {
     float mn[3];
@@ -52,62 +52,92 @@ struct BoxArg {
 // The soup is read as one flat array of 16-B words (n x 10 floats, 16-B aligned): a
 // float at flat position f belongs to field f % 10 of its triangle, a coordinate of
 // axis (f % 10) % 3 when f % 10 < 9 (the tenth is info_idx). Coalesced 16-B loads
-// instead of nine 4-B loads 40 B apart per triangle.
-__device__ __forceinline__ void bounds_take(float v, uint32_t field, float mn[3], float mx[3])
+// instead of nine 4-B loads 40 B apart per triangle. Word q starts at field
+// (4 q) % 10, which depends on q % 5 only; with a block of 320 threads (a multiple of
+// 5) and a grid-stride loop every word a thread reads has the same phase
+// threadIdx.x % 5, so each of the four lanes of the word keeps its own running
+// min / max in registers and is mapped to its axis once, after the loop.
+__device__ __forceinline__ void bounds_fold(float lo, float hi, uint32_t field, float mn[3], float mx[3])
 {
-    if (field < 9u) {
-        const uint32_t a = field - 3u * (field / 3u);
-        mn[a] = gmin(mn[a], v);
-        mx[a] = gmax(mx[a], v);
+#pragma unroll
+    for (uint32_t a = 0; a < 3; ++a) {
+        const bool take = field < 9u && field % 3u == a;
+        mn[a] = take ? gmin(mn[a], lo) : mn[a];
+        mx[a] = take ? gmax(mx[a], hi) : mx[a];
     }
 }
 
 __global__ void __launch_bounds__(kBoundsBlock) k_bounds_partial(const float* __restrict__ tris, uint32_t n,
                                                                  float* __restrict__ partial)
 {
-    float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    static_assert(kBoundsBlock % 5 == 0 && kBoundsBlock % 32 == 0, "one phase per thread, whole warps");
+    float lo[4] = {FLT_MAX, FLT_MAX, FLT_MAX, FLT_MAX}, hi[4] = {-FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
     const uint64_t floats = 10ull * n, quads = floats / 4;
     const float4* q4 = reinterpret_cast<const float4*>(tris);
-    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < quads; q += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t q = (uint64_t)blockIdx.x * kBoundsBlock + threadIdx.x; q < quads;
+         q += (uint64_t)gridDim.x * kBoundsBlock) {
         const float4 v = __ldg(q4 + q);
-        uint32_t f = (uint32_t)((4 * q) % 10);
-        bounds_take(v.x, f, mn, mx);
-        f = f == 9u ? 0u : f + 1u;
-        bounds_take(v.y, f, mn, mx);
-        f = f == 9u ? 0u : f + 1u;
-        bounds_take(v.z, f, mn, mx);
-        f = f == 9u ? 0u : f + 1u;
-        bounds_take(v.w, f, mn, mx);
+        lo[0] = gmin(lo[0], v.x); hi[0] = gmax(hi[0], v.x);
+        lo[1] = gmin(lo[1], v.y); hi[1] = gmax(hi[1], v.y);
+        lo[2] = gmin(lo[2], v.z); hi[2] = gmax(hi[2], v.z);
+        lo[3] = gmin(lo[3], v.w); hi[3] = gmax(hi[3], v.w);
     }
-    if (blockIdx.x == 0 && threadIdx.x < floats - 4 * quads) {  // the last 2 floats of an odd count
-        const uint64_t f = 4 * quads + threadIdx.x;
-        bounds_take(tris[f], (uint32_t)(f % 10), mn, mx);
+    float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    const uint32_t f0 = (4u * (threadIdx.x % 5u)) % 10u;
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) bounds_fold(lo[j], hi[j], (f0 + j) % 10u, mn, mx);
+    if (blockIdx.x == 0 && threadIdx.x < floats - 4 * quads) {  // an odd count leaves fields 8 and 9 of the last
+        const float v = tris[4 * quads + threadIdx.x];
+        bounds_fold(v, v, 8u + threadIdx.x, mn, mx);
     }
-    __shared__ float s[6][kBoundsBlock];
-    for (int a = 0; a < 3; ++a) { s[a][threadIdx.x] = mn[a]; s[3 + a][threadIdx.x] = mx[a]; }
-    __syncthreads();
-    for (int w = kBoundsBlock / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) {
-            for (int a = 0; a < 3; ++a) {
-                s[a][threadIdx.x] = gmin(s[a][threadIdx.x], s[a][threadIdx.x + w]);
-                s[3 + a][threadIdx.x] = gmax(s[3 + a][threadIdx.x], s[3 + a][threadIdx.x + w]);
-            }
+    // Block fold: warp shuffles, then one value per warp through shared memory.
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = gmin(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+            mx[a] = gmax(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
         }
-        __syncthreads();
+    constexpr int kWarps = kBoundsBlock / 32;
+    __shared__ float s[6][kWarps];
+    if ((threadIdx.x & 31) == 0)
+        for (int a = 0; a < 3; ++a) { s[a][threadIdx.x >> 5] = mn[a]; s[3 + a][threadIdx.x >> 5] = mx[a]; }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        float b = s[threadIdx.x][0];
+        for (int w = 1; w < kWarps; ++w) b = threadIdx.x < 3 ? gmin(b, s[threadIdx.x][w]) : gmax(b, s[threadIdx.x][w]);
+        partial[6 * blockIdx.x + threadIdx.x] = b;
     }
-    if (threadIdx.x < 6) partial[6 * blockIdx.x + threadIdx.x] = s[threadIdx.x][0];
 }
 
-__global__ void k_bounds_final(const float* __restrict__ partial, int blocks, float* __restrict__ box)
+// One block folds the per-block boxes: each thread a strided subset, then shuffles.
+__global__ void __launch_bounds__(256) k_bounds_final(const float* __restrict__ partial, int blocks,
+                                                      float* __restrict__ box)
 {
-    if (threadIdx.x != 0) return;
     float b[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
-    for (int i = 0; i < blocks; ++i)
+    for (int i = threadIdx.x; i < blocks; i += blockDim.x)
+#pragma unroll
         for (int a = 0; a < 3; ++a) {
             b[a] = gmin(b[a], partial[6 * i + a]);
             b[3 + a] = gmax(b[3 + a], partial[6 * i + 3 + a]);
         }
-    for (int a = 0; a < 6; ++a) box[a] = b[a];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            b[a] = gmin(b[a], __shfl_xor_sync(0xffffffffu, b[a], o));
+            b[3 + a] = gmax(b[3 + a], __shfl_xor_sync(0xffffffffu, b[3 + a], o));
+        }
+    __shared__ float s[6][8];
+    if ((threadIdx.x & 31) == 0)
+        for (int a = 0; a < 6; ++a) s[a][threadIdx.x >> 5] = b[a];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int warps = (int)(blockDim.x + 31) / 32;
+        float r = s[threadIdx.x][0];
+        for (int w = 1; w < warps; ++w) r = threadIdx.x < 3 ? gmin(r, s[threadIdx.x][w]) : gmax(r, s[threadIdx.x][w]);
+        box[threadIdx.x] = r;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -259,6 +289,50 @@ size_t scratch_layout(uint32_t n, void* base, SortScratch<K>* s)
     return c.used();
 }
 
+// The stable key sort: P passes of 8-bit digits. 32-bit keys: key and value passes
+// ping-pong between keys and keys_alt. 64-bit keys (in keys_alt, input order): four
+// passes over the low halves and three over the high halves, ping-ponging 32-bit
+// halves in the two halves of `keys` (free until the last pass), then the last pass
+// gathers whole keys by value and writes them, sorted, to `keys`. Values end in
+// vals[(P - 1) & 1] either way.
+template <typename K>
+int sort_keys(const SortScratch<K>& s, uint32_t n, K* keys, uint32_t* status, SortWait wait, cudaStream_t stream)
+{
+    if constexpr (sizeof(K) == 8) {
+        return onesweep_sort64_halves(reinterpret_cast<const uint64_t*>(s.keys_alt), reinterpret_cast<uint64_t*>(keys),
+                                      n, n, nullptr, s.vals, s.offsets, s.lookback, s.tile_counters, status, wait, true,
+                                      true, stream);
+    } else {
+        constexpr int P = KeyTraits<K>::passes;
+        const uint32_t tiles = num_tiles(n);
+        const size_t smem = onesweep_smem<K>();
+        CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        K* kbuf[2] = {keys, s.keys_alt};
+        for (int p = 0; p < P; ++p) {
+            const K* kin = kbuf[p & 1];
+            K* kout = kbuf[(p + 1) & 1];
+            const uint32_t* vin = p == 0 ? nullptr : s.vals[(p + 1) & 1];
+            uint32_t* vout = s.vals[p & 1];
+            uint32_t* lb = s.lookback + (size_t)p * tiles * kRadix;
+            CPT_PROF(K_ONESWEEP, stream);
+            if (p == 0)
+                k_onesweep<K, true><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, n, nullptr, 8 * p,
+                                                                         s.offsets + p * kRadix,
+                                                                         lb, s.tile_counters + p, status, wait);
+            else {
+                SortWait later = wait;
+                later.withhold_tile0 = 0;  // (the test hook stalls the first pass only)
+                k_onesweep<K, false><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, n, nullptr, 8 * p,
+                                                                          s.offsets + p * kRadix,
+                                                                          lb, s.tile_counters + p, status, later);
+            }
+            CPT_LAUNCH_CHECK();
+        }
+        return CPT_OK;
+    }
+}
+
 template <typename K>
 int build_impl(const cpt_triangle* tris_in, uint32_t n, const float* host_box, cpt_bvh* bvh, void* scratch,
                SortWait wait, cudaStream_t stream)
@@ -291,7 +365,7 @@ int build_impl(const cpt_triangle* tris_in, uint32_t n, const float* host_box, c
         CPT_LAUNCH_CHECK();
         {
             CPT_PROF(K_BOUNDS, stream);
-            k_bounds_final<<<1, 32, 0, stream>>>(s.bounds_partial, kBoundsBlocks, s.dev_box);
+            k_bounds_final<<<1, 256, 0, stream>>>(s.bounds_partial, kBoundsBlocks, s.dev_box);
         }
         CPT_LAUNCH_CHECK();
         box.dev = s.dev_box;
@@ -302,8 +376,9 @@ int build_impl(const cpt_triangle* tris_in, uint32_t n, const float* host_box, c
     const int morton_blocks = (int)std::min<size_t>((n + kMortonBlock - 1) / kMortonBlock, (size_t)sms * 8);
     {
         CPT_PROF(K_MORTON, stream);
-        k_morton<K><<<morton_blocks, kMortonBlock, 0, stream>>>(tri_src, n, box, keys, s.hist, s.zero_region,
-                                                                s.zero_words, bvh->status);
+        // 64-bit keys go to keys_alt: the sort reads them from there (sort_keys)
+        k_morton<K><<<morton_blocks, kMortonBlock, 0, stream>>>(tri_src, n, box, sizeof(K) == 8 ? s.keys_alt : keys,
+                                                                s.hist, s.zero_region, s.zero_words, bvh->status);
     }
     CPT_LAUNCH_CHECK();
     {
@@ -312,31 +387,7 @@ int build_impl(const cpt_triangle* tris_in, uint32_t n, const float* host_box, c
     }
     CPT_LAUNCH_CHECK();
 
-    const size_t smem = onesweep_smem<K>();
-    CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const uint32_t tiles = num_tiles(n);
-    K* kbuf[2] = {keys, s.keys_alt};
-    for (int p = 0; p < P; ++p) {
-        const K* kin = kbuf[p & 1];
-        K* kout = kbuf[(p + 1) & 1];
-        const uint32_t* vin = p == 0 ? nullptr : s.vals[(p + 1) & 1];
-        uint32_t* vout = s.vals[p & 1];
-        uint32_t* lb = s.lookback + (size_t)p * tiles * kRadix;
-        CPT_PROF(K_ONESWEEP, stream);
-        if (p == 0)
-            k_onesweep<K, true><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, n, nullptr, 8 * p,
-                                                                     s.offsets + p * kRadix,
-                                                                     lb, s.tile_counters + p, bvh->status, wait);
-        else {
-            SortWait later = wait;
-            later.withhold_tile0 = 0;  // (the test hook stalls the first pass only)
-            k_onesweep<K, false><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, n, nullptr, 8 * p,
-                                                                      s.offsets + p * kRadix,
-                                                                      lb, s.tile_counters + p, bvh->status, later);
-        }
-        CPT_LAUNCH_CHECK();
-    }
+    if (const int rc = sort_keys<K>(s, n, keys, bvh->status, wait, stream)) return rc;
     // P is even: keys end in bvh->keys, values in vals[(P - 1) & 1].
     const uint32_t* order = s.vals[(P - 1) & 1];
 

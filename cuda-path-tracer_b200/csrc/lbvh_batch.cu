@@ -252,26 +252,38 @@ int batch_impl(BatchTable& bt, const cpt_triangle* const* tris_in, cpt_bvh* cons
         k_scan_offsets<<<P + 1, kRadix, 0, stream>>>(s.hist, s.offsets);
     }
     CPT_LAUNCH_CHECK();
-    const size_t smem = onesweep_smem<K>();
-    CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const uint32_t tiles = (bt.total + kSortTile - 1) / kSortTile;
     uint32_t* lookback = s.zero + 32;
-    // key passes: keys[0] -> keys[1] -> keys[2] -> keys[1] ...; values 0 -> 1 -> 0 ...
-    for (int p = 0; p < P; ++p) {
-        const K* kin = p == 0 ? s.keys[0] : s.keys[1 + ((p + 1) & 1)];
-        K* kout = s.keys[1 + (p & 1)];
-        const uint32_t* vin = p == 0 ? nullptr : s.vals[(p + 1) & 1];
-        uint32_t* vout = s.vals[p & 1];
-        uint32_t* lb = lookback + (size_t)p * tiles * kRadix;
-        CPT_PROF(K_ONESWEEP, stream);
-        if (p == 0)
-            k_onesweep<K, true><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, bt.total, nullptr, 8 * p,
-                                                                     s.offsets + p * kRadix, lb, s.zero + p, s.status);
-        else
-            k_onesweep<K, false><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, bt.total, nullptr, 8 * p,
-                                                                      s.offsets + p * kRadix, lb, s.zero + p, s.status);
-        CPT_LAUNCH_CHECK();
+    if constexpr (sizeof(K) == 8) {
+        // as 32-bit halves (in keys[1]); only the order is needed, k_batch_keys gathers
+        // each scene's sorted keys from keys[0] afterwards
+        if (const int rc = onesweep_sort64_halves(reinterpret_cast<const uint64_t*>(s.keys[0]),
+                                                  reinterpret_cast<uint64_t*>(s.keys[1]), bt.total, bt.total, nullptr,
+                                                  s.vals, s.offsets, lookback, s.zero, s.status, SortWait(), false,
+                                                  true, stream))
+            return rc;
+    } else {
+        const size_t smem = onesweep_smem<K>();
+        CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // key passes: keys[0] -> keys[1] -> keys[2] -> keys[1] ...; values 0 -> 1 -> 0 ...
+        for (int p = 0; p < P; ++p) {
+            const K* kin = p == 0 ? s.keys[0] : s.keys[1 + ((p + 1) & 1)];
+            K* kout = s.keys[1 + (p & 1)];
+            const uint32_t* vin = p == 0 ? nullptr : s.vals[(p + 1) & 1];
+            uint32_t* vout = s.vals[p & 1];
+            uint32_t* lb = lookback + (size_t)p * tiles * kRadix;
+            CPT_PROF(K_ONESWEEP, stream);
+            if (p == 0)
+                k_onesweep<K, true><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, bt.total, nullptr, 8 * p,
+                                                                         s.offsets + p * kRadix, lb, s.zero + p,
+                                                                         s.status);
+            else
+                k_onesweep<K, false><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, bt.total, nullptr,
+                                                                          8 * p, s.offsets + p * kRadix, lb,
+                                                                          s.zero + p, s.status);
+            CPT_LAUNCH_CHECK();
+        }
     }
     const uint32_t* order = s.vals[(P - 1) & 1];
     if (bt.scenes > 1) {  // the scene digit: one more stable pass

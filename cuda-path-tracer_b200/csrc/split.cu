@@ -980,29 +980,39 @@ int split_impl(cpt_bvh* bvh, uint32_t cap, bool treelet, void* nodes, void* scra
     CPT_LAUNCH_CHECK();
     k_scan_offsets<<<P, kRadix, 0, stream>>>(s.hist, s.offsets);
     CPT_LAUNCH_CHECK();
-    const size_t smem = onesweep_smem<K>();
-    CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const uint32_t tiles = (cap + kSortTile - 1) / kSortTile;
     uint32_t* lookback = s.zero + 32;
-    for (int p = 0; p < P; ++p) {
-        const K* kin = s.keys[p & 1];
-        K* kout = s.keys[(p + 1) & 1];
-        const uint32_t* vin = p == 0 ? nullptr : s.vals[(p + 1) & 1];
-        uint32_t* vout = s.vals[p & 1];
-        uint32_t* lb = lookback + (size_t)p * tiles * kRadix;
-        if (p == 0)
-            k_onesweep<K, true><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, 0, s.n_pieces, 8 * p,
-                                                                     s.offsets + p * kRadix, lb, s.zero + p,
-                                                                     bvh->status);
-        else
-            k_onesweep<K, false><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, 0, s.n_pieces, 8 * p,
-                                                                      s.offsets + p * kRadix, lb, s.zero + p,
-                                                                      bvh->status);
-        CPT_LAUNCH_CHECK();
+    const K* keys;
+    if constexpr (sizeof(K) == 8) {  // as 32-bit halves: the sorted keys end in keys[1]
+        if (const int rc = onesweep_sort64_halves(reinterpret_cast<const uint64_t*>(s.keys[0]),
+                                                  reinterpret_cast<uint64_t*>(s.keys[1]), cap, 0, s.n_pieces, s.vals,
+                                                  s.offsets, lookback, s.zero, bvh->status, SortWait(), true, false,
+                                                  stream))
+            return rc;
+        keys = s.keys[1];
+    } else {
+        const size_t smem = onesweep_smem<K>();
+        CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CPT_CUDA_TRY(cudaFuncSetAttribute(k_onesweep<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        for (int p = 0; p < P; ++p) {
+            const K* kin = s.keys[p & 1];
+            K* kout = s.keys[(p + 1) & 1];
+            const uint32_t* vin = p == 0 ? nullptr : s.vals[(p + 1) & 1];
+            uint32_t* vout = s.vals[p & 1];
+            uint32_t* lb = lookback + (size_t)p * tiles * kRadix;
+            if (p == 0)
+                k_onesweep<K, true><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, 0, s.n_pieces, 8 * p,
+                                                                         s.offsets + p * kRadix, lb, s.zero + p,
+                                                                         bvh->status);
+            else
+                k_onesweep<K, false><<<tiles, kSortBlock, smem, stream>>>(kin, vin, kout, vout, 0, s.n_pieces, 8 * p,
+                                                                          s.offsets + p * kRadix, lb, s.zero + p,
+                                                                          bvh->status);
+            CPT_LAUNCH_CHECK();
+        }
+        keys = s.keys[P & 1];
     }
     const uint32_t* order = s.vals[(P - 1) & 1];
-    const K* keys = s.keys[P & 1];
     k_topology<K><<<(cap + 255) / 256, 256, 0, stream>>>(keys, 0, s.n_pieces, s.children, s.parents_leaf,
                                                           s.parents_internal, s.counters, static_cast<float4*>(nodes),
                                                           bvh->status);

@@ -633,11 +633,16 @@ __device__ __forceinline__ void persistent_trace(NodesOf nodes_of, const float4*
                     const uint32_t r = base + (uint32_t)__popc(m & lt_mask);
                     if (r < n) {
                         ray = order ? order[r] : r;
-                        const float4 ro = rays[2 * (size_t)ray], rd = rays[2 * (size_t)ray + 1];
-                        uint32_t mv;
-                        const float4* nodes = nodes_of(__float_as_uint(rd.w), mv);
-                        trace_init(s, nodes, mv, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z));
-                        if (kTmax) s.best.t = ro.w;
+                        if (ray < n) {
+                            const float4 ro = rays[2 * (size_t)ray], rd = rays[2 * (size_t)ray + 1];
+                            uint32_t mv;
+                            const float4* nodes = nodes_of(__float_as_uint(rd.w), mv);
+                            trace_init(s, nodes, mv, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z));
+                            if (kTmax) s.best.t = ro.w;
+                        } else {  // a ray order left void by a failed sort
+                            overflow = true;
+                            ray = CPT_INVALID_INDEX;
+                        }
                     }
                 }
             }
@@ -690,12 +695,17 @@ __device__ __forceinline__ void persistent_trace_wide(WideOf wide_of, const floa
                     const uint32_t r = base + (uint32_t)__popc(m & lt_mask);
                     if (r < n) {
                         ray = order ? order[r] : r;
-                        const float4 ro = rays[2 * (size_t)ray], rd = rays[2 * (size_t)ray + 1];
-                        uint32_t mv;
-                        const float4* tris;
-                        const float4* nodes = wide_of(__float_as_uint(rd.w), mv, tris);
-                        wide_init(s, nodes, tris, mv, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z));
-                        if (kTmax) s.best.t = ro.w;
+                        if (ray < n) {
+                            const float4 ro = rays[2 * (size_t)ray], rd = rays[2 * (size_t)ray + 1];
+                            uint32_t mv;
+                            const float4* tris;
+                            const float4* nodes = wide_of(__float_as_uint(rd.w), mv, tris);
+                            wide_init(s, nodes, tris, mv, mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z));
+                            if (kTmax) s.best.t = ro.w;
+                        } else {  // a ray order left void by a failed sort
+                            overflow = true;
+                            ray = CPT_INVALID_INDEX;
+                        }
                     }
                 }
             }

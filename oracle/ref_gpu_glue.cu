@@ -41,13 +41,18 @@ __host__ __device__ inline void swap(thrust::device_allocator<T>& a, thrust::dev
 #include "application/cuda/BVHBuilder.cu"
 // The reference's path tracer (raytrace_kernel and the shading it calls,
 // cuda_path_tracer.cu:36-421) with the constant-memory scene descriptors it reads
-// (Globals.h; compiled as one translation unit without relocatable device code, the
-// extern declarations there are the variables themselves, which Scene.cu:8-11 defines in
-// the reference's separately compiled build). Its host-side helpers come along: the
-// mt19937 frame seeds (Random.cpp) and, as stand-ins without SDL / ImGui, the timer and
-// GUI settings types (oracle/ref_shim/engine/util/Timer.h, engine/gui/GUISettings.h).
+// (declared extern in Globals.h). As in the reference's build, the library is compiled
+// with relocatable device code and the descriptors are defined once, here, as
+// Scene.cu:8-11 defines them. Its host-side helpers come along: the mt19937 frame seeds
+// (Random.cpp) and, as stand-ins without SDL / ImGui, the timer and GUI settings types
+// (oracle/ref_shim/engine/util/Timer.h, engine/gui/GUISettings.h).
 #include "engine/util/Random.cpp"
 #include "application/cuda/cuda_path_tracer.cu"
+
+__constant__ GeometryData g_geometryData;
+__constant__ ShadingData g_shadingData;
+__constant__ LightingData g_lightingData;
+__constant__ MiscData g_miscData;
 
 #include <chrono>
 #include <cstdio>
@@ -88,6 +93,31 @@ void exit_backtrace()
     const int k = backtrace(frames, 32);
     fprintf(stderr, "refgpu: process exit via exit(); backtrace:\n");
     backtrace_symbols_fd(frames, k, 2);
+}
+
+// trace() with the device's last error
+void trace_error(const char* what)
+{
+    if (!trace_on()) return;
+    const cudaError_t e = cudaGetLastError();
+    fprintf(stderr, "refgpu: %s (%s)\n", what, cudaGetErrorString(e));
+    fflush(stderr);
+}
+
+template <typename V>
+void release(V& v)
+{
+    v.clear();
+    v.shrink_to_fit();
+}
+
+// A failed CUDA call: reported, and the runtime's last error cleared so that the
+// thrust vectors' destructors on the way out do not see it and throw.
+int fail(cudaError_t e, const char* what)
+{
+    fprintf(stderr, "refgpu: %s: %s\n", what, cudaGetErrorName(e));
+    cudaGetLastError();
+    return -2;
 }
 
 struct ExitTrace {
@@ -206,6 +236,7 @@ static int refgpu_render_impl(const void* tris_host, uint32_t n, const float* bo
     if (!tris_host || !box || !infos_host || !cam15 || n < 2 || width < 8 || height < 8 || frames < 1 ||
         bounces > 255)
         return -1;
+    trace("render: start");
     StdoutToStderr quiet;
     const CUDA::Triangle* in = static_cast<const CUDA::Triangle*>(tris_host);
     const CUDA::TriangleInfo* inf = static_cast<const CUDA::TriangleInfo*>(infos_host);
@@ -215,14 +246,16 @@ static int refgpu_render_impl(const void* tris_host, uint32_t n, const float* bo
     desc.triangles.assign(in, in + n);
     desc.triangleInfo.assign(inf, inf + info_count);
     desc.enclosingBBox = BBox(glm::vec3(box[0], box[1], box[2]), glm::vec3(box[3], box[4], box[5]));
+    trace_error("render: scene uploaded");
     CUDA::BVHBuilder builder;
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return -2;
     cudaEventRecord(e0, 0);
     builder.build(desc, n);
     cudaEventRecord(e1, 0);
-    if (cudaEventSynchronize(e1) != cudaSuccess) return -2;
+    if (const cudaError_t e = cudaEventSynchronize(e1)) return fail(e, "render: build");
     if (build_ms) cudaEventElapsedTime(build_ms, e0, e1);
+    trace_error("render: built");
     GeometryData geometry(thrust::raw_pointer_cast(desc.internalNodeBBoxes.data()),
                           thrust::raw_pointer_cast(desc.children.data()),
                           thrust::raw_pointer_cast(desc.triangles.data()), n);
@@ -235,16 +268,19 @@ static int refgpu_render_impl(const void* tris_host, uint32_t n, const float* bo
     lighting.indirectBounceCount = static_cast<uint8_t>(bounces);
     MiscData misc;
     misc.useStratifiedSampling = stratified != 0;
-    if (cudaMemcpyToSymbol(g_geometryData, &geometry, sizeof(geometry)) != cudaSuccess ||
-        cudaMemcpyToSymbol(g_shadingData, &shading, sizeof(shading)) != cudaSuccess ||
-        cudaMemcpyToSymbol(g_lightingData, &lighting, sizeof(lighting)) != cudaSuccess ||
-        cudaMemcpyToSymbol(g_miscData, &misc, sizeof(misc)) != cudaSuccess)
-        return -2;
+    const cudaError_t copied[4] = {cudaMemcpyToSymbol(g_geometryData, &geometry, sizeof(geometry)),
+                                   cudaMemcpyToSymbol(g_shadingData, &shading, sizeof(shading)),
+                                   cudaMemcpyToSymbol(g_lightingData, &lighting, sizeof(lighting)),
+                                   cudaMemcpyToSymbol(g_miscData, &misc, sizeof(misc))};
+    for (int k = 0; k < 4; ++k)
+        if (copied[k] != cudaSuccess) return fail(copied[k], "render: scene descriptor copy");
+    trace_error("render: descriptors set");
     // the screen texture: a float4 array with surface load/store, cleared (frame 0's
     // running mean reads it: lerp(hit, old, 0))
     cudaChannelFormatDesc ch = cudaCreateChannelDesc<float4>();
     cudaArray_t screen = nullptr;
-    if (cudaMallocArray(&screen, &ch, width, height, cudaArraySurfaceLoadStore) != cudaSuccess) return -2;
+    if (const cudaError_t e = cudaMallocArray(&screen, &ch, width, height, cudaArraySurfaceLoadStore))
+        return fail(e, "render: screen array");
     std::vector<float> zeros((size_t)width * height * 4, 0.0f);
     cudaMemcpy2DToArray(screen, 0, 0, zeros.data(), width * sizeof(float4), width * sizeof(float4), height,
                         cudaMemcpyHostToDevice);
@@ -253,7 +289,11 @@ static int refgpu_render_impl(const void* tris_host, uint32_t n, const float* bo
     res.resType = cudaResourceTypeArray;
     res.res.array.array = screen;
     cudaSurfaceObject_t surf = 0;
-    if (cudaCreateSurfaceObject(&surf, &res) != cudaSuccess) { cudaFreeArray(screen); return -2; }
+    if (const cudaError_t e = cudaCreateSurfaceObject(&surf, &res)) {
+        cudaFreeArray(screen);
+        return fail(e, "render: surface object");
+    }
+    trace_error("render: surface created");
     const glm::vec3 eye(cam15[0], cam15[1], cam15[2]);
     const glm::vec3 d00(cam15[3], cam15[4], cam15[5]), d10(cam15[6], cam15[7], cam15[8]);
     const glm::vec3 d11(cam15[9], cam15[10], cam15[11]), d01(cam15[12], cam15[13], cam15[14]);
@@ -265,13 +305,21 @@ static int refgpu_render_impl(const void* tris_host, uint32_t n, const float* bo
     for (uint32_t f = 0; f < warmup; ++f, ++frame)
         raytrace_kernel<<<blocks, threads>>>(surf, eye, d00, d10, d11, d01, glm::ivec2(width, height), frame,
                                              Random::getUInt(0, std::numeric_limits<uint32_t>().max()));
-    if (cudaDeviceSynchronize() != cudaSuccess) { cudaDestroySurfaceObject(surf); cudaFreeArray(screen); return -2; }
+    trace_error("render: warm-up launched");
+    if (const cudaError_t e = cudaDeviceSynchronize()) {
+        cudaDestroySurfaceObject(surf);
+        cudaFreeArray(screen);
+        return fail(e, "render: warm-up frames");
+    }
+    trace_error("render: warm-up done");
     cudaEventRecord(e0, 0);
     for (uint32_t f = 0; f < frames; ++f, ++frame)
         raytrace_kernel<<<blocks, threads>>>(surf, eye, d00, d10, d11, d01, glm::ivec2(width, height), frame,
                                              Random::getUInt(0, std::numeric_limits<uint32_t>().max()));
     cudaEventRecord(e1, 0);
+    trace_error("render: frames launched");
     const cudaError_t err = cudaEventSynchronize(e1);
+    trace_error("render: frames done");
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e0, e1);
     if (ms_per_frame) *ms_per_frame = ms / frames;
@@ -282,6 +330,15 @@ static int refgpu_render_impl(const void* tris_host, uint32_t n, const float* bo
     cudaFreeArray(screen);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    // release the vectors here, where a failure is still caught by the caller's handler
+    // (their destructors would run destroy kernels where an exception cannot propagate)
+    release(desc.triangles);
+    release(desc.triangleInfo);
+    release(desc.children);
+    release(desc.parents[0]);
+    release(desc.parents[1]);
+    release(desc.internalNodeBBoxes);
+    trace_error("render: released");
     return err == cudaSuccess && cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

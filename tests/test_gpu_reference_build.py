@@ -44,9 +44,13 @@ def test_reference_gpu_build_equals_ours(cuda, case):
 
 def test_reference_gpu_render_estimates_the_same_image(cuda):
     """The reference's raytrace_kernel (cuda_path_tracer.cu:385-421, its own curand
-    stream) and this library's renderer (the Philox stream) estimate the same image: over
-    512 one-sample frames each, the image means agree within 2 % and coarse 8x8-pixel
-    block means within 8 % (noise, not bias, at these sample counts)."""
+    stream) and this library's renderer (the Philox stream) estimate the same image,
+    512 one-sample frames each. The image means agree within 2 %. Block by block
+    (8x8 pixels, 3 channels), the squared differences to the reference's image sum to
+    about what two independent renders of this library (seeds 9 and 10) differ by —
+    noise of equal size on both sides gives a ratio near 1, a bias of a few percent
+    in lit blocks would push it far above; it must stay below 2 (with 144 block values
+    per side the ratio's spread is about 0.2)."""
     if not cpu.refgpu_available():
         pytest.fail("oracle/_ref/librefgpu.so was not built (make -C oracle ref)")
     import torch
@@ -63,15 +67,23 @@ def test_reference_gpu_render_estimates_the_same_image(cuda):
     assert float(rr["ms_per_frame"]) > 0 and np.isfinite(ref_img).all()
     lb = DeviceLbvh(len(tris), 30)
     lb.build(to_device(tris), check_root=True)
-    r = DeviceRenderer(make_params(w, h, spp, 0, bounces, 3.0, True, 9, cpt.ACCUM_KAHAN))
-    r.render(lb, DeviceScene(infos), cam)
-    torch.cuda.synchronize()
-    r.check_status()
-    ours = r.resolve().cpu().numpy()[..., :3].astype(np.float64)
+    scene = DeviceScene(infos)
+    ours = []
+    for seed in (9, 10):
+        r = DeviceRenderer(make_params(w, h, spp, 0, bounces, 3.0, True, seed, cpt.ACCUM_KAHAN))
+        r.render(lb, scene, cam)
+        torch.cuda.synchronize()
+        r.check_status()
+        ours.append(r.resolve().cpu().numpy()[..., :3].astype(np.float64))
     theirs = ref_img[..., :3].astype(np.float64)
-    assert ours.mean() > 0.01
-    assert abs(theirs.mean() - ours.mean()) <= 0.02 * ours.mean(), (theirs.mean(), ours.mean())
-    bo = ours.reshape(h // 8, 8, w // 8, 8, 3).mean(axis=(1, 3))
-    bt = theirs.reshape(h // 8, 8, w // 8, 8, 3).mean(axis=(1, 3))
-    lit = bo > 0.05 * bo.max()
-    assert np.all(np.abs(bt[lit] - bo[lit]) <= 0.08 * bo[lit] + 1e-3)
+    assert ours[0].mean() > 0.01
+    assert abs(theirs.mean() - ours[0].mean()) <= 0.02 * ours[0].mean(), (theirs.mean(), ours[0].mean())
+
+    def blocks(img):
+        return img.reshape(h // 8, 8, w // 8, 8, 3).mean(axis=(1, 3))
+
+    b1, b2, bt = blocks(ours[0]), blocks(ours[1]), blocks(theirs)
+    lit = b1 > 0.05 * b1.max()
+    assert lit.sum() >= 40
+    ratio = ((bt - b1)[lit] ** 2).sum() / ((b2 - b1)[lit] ** 2).sum()
+    assert ratio < 2.0, ratio
