@@ -990,6 +990,12 @@ def run_ours(args, w, world, rank, local):
             builds = {"error": f"{type(e).__name__}: {e}"[:300]}
         torch.cuda.empty_cache()
 
+    # --- the other workloads (default C2 run, rank 0): short child runs of C1, C3 and C5
+    workloads = None
+    if rank == 0 and world == 1 and args.workload == "c2" and not args.no_other_workloads:
+        torch.cuda.empty_cache()
+        workloads = other_workloads()
+
     # --- CPU baseline (rank 0, N = 1): the reference's code on every k-th row of frame 0,
     # and the parity of the GPU's frame 0 (FP64 accumulator, same traversal tree as the
     # timed frames) on those rows
@@ -1026,7 +1032,7 @@ def run_ours(args, w, world, rank, local):
                                      + (", treelet-restructured" if args.treelet else "") + ")" if split > 0
                                      else "LBVH (reference topology)")), "lbvh_topology": lbvh_topology,
                 "cpu_baseline": cpu_base, "parity": parity, "reference_gpu": ref_gpu,
-                "radiance_cache_c4": cache_c4, "builds_c5_c3": builds, "e2e": e2e,
+                "radiance_cache_c4": cache_c4, "builds_c5_c3": builds, "workloads": workloads, "e2e": e2e,
                 "gpu_launches": int(launches),
                 "clocks": clocks,
                 "parallelism": f"replicas x{world}: own BVH per GPU, disjoint sample streams, "
@@ -1034,6 +1040,41 @@ def run_ours(args, w, world, rank, local):
                 "scene_gen_s": round(gen_s, 2)}
         print(json.dumps(line), flush=True)
     return 0
+
+
+def other_workloads(timeout_s=240.0):
+    """C1, C3 and C5 as short runs of this script in child processes (the default C2
+    line carries their headline figures). Each child is a full run of its workload
+    (its own scene, build, warm-up and timed frames, CUDA events, clocks), without the
+    CPU baseline and the end-to-end leg; what comes back is the child's JSON line,
+    reduced to its measurements."""
+    runs = {"c1": ["--steps", "10", "--warmup", "3"], "c3": ["--steps", "3", "--warmup", "3"],
+            "c5": ["--steps", "5", "--warmup", "3"]}
+    out = {}
+    for wl, extra in runs.items():
+        cmd = [sys.executable, os.path.abspath(__file__), "--workload", wl, "--no-cpu-baseline", "--no-e2e"] + extra
+        t0 = time.perf_counter()
+        try:
+            p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s, cwd=os.path.dirname(
+                os.path.abspath(__file__)))
+            lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+            if p.returncode != 0 or not lines:
+                out[wl] = {"error": f"exit {p.returncode}: {p.stderr.strip()[-300:]}"}
+                continue
+            d = json.loads(lines[-1])
+        except Exception as e:  # an extra measurement never takes the main line down
+            out[wl] = {"error": f"{type(e).__name__}: {e}"[:300]}
+            continue
+        keep = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "rays_per_step", "clocks",
+                "gpu_launches", "built_and_rendered_per_frame", "lbvh", "parallelism")
+        r = {k: d[k] for k in keep if k in d}
+        r["workload"] = d.get("config", {}).get("workload")
+        if isinstance(d.get("roofline"), dict):
+            r["roofline_frac"] = d["roofline"].get("frac")
+        r["command"] = "python bench.py " + " ".join(cmd[2:])
+        r["child_s"] = round(time.perf_counter() - t0, 1)
+        out[wl] = r
+    return out
 
 
 def cache_experiment(w, lb, scene, cam, dev, stratified, warmup, spf, rc_params, nee=False, reach=None):
@@ -1270,6 +1311,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra-builds", action="store_true",
                     help="c2: skip the C5-scale rebuild and the C3 batched build measurements")
+    ap.add_argument("--no-other-workloads", action="store_true",
+                    help="c2: skip the C1, C3 and C5 runs (short child runs reported under 'workloads')")
     ap.add_argument("--no-cache-ratio", action="store_true",
                     help="c2: skip the radiance cache's time-to-equal-RMSE measurement (the C4 configuration)")
     ap.add_argument("--res", default=None, help="override resolution WxH (profiling runs)")
