@@ -86,13 +86,11 @@ __device__ __forceinline__ float slab_test_fma(f3 odinv, f3 dinv, float ax, floa
 // sequence gives the bits of the scalar one; it issues one instruction per pair.
 // CPT_PACKED_BOX (on): the packed plane evaluation of the wide tree's box test — one
 // packed fused multiply-add gives an axis's near and far plane — which only steers
-// pruning: C2 495.2 against 474.0 Mrays/s. CPT_PACKED_TRI (off): the packed
-// Moller-Trumbore; on the device a quarter of its cross-product lanes came out 1 ulp from
-// the scalar sequence (a packed multiply and subtract contracted into one fused
-// operation), and exact hits are required here.
-#ifndef CPT_PACKED_TRI
-#define CPT_PACKED_TRI 0
-#endif
+// pruning: C2 495.2 against 474.0 Mrays/s. The triangle test stays scalar: a packed
+// Moller-Trumbore (the two cross products and the dot products that share a factor in
+// pairs) gave a quarter of its cross-product lanes 1 ulp off the scalar sequence on the
+// device (a packed multiply and subtract contracted into one fused operation), and
+// exact hits are required here.
 #ifndef CPT_PACKED_BOX
 #define CPT_PACKED_BOX 1
 #endif
@@ -123,30 +121,8 @@ __device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
 // Möller-Trumbore on a slot (v0 = s[0..2], e1 = s[4..6], e2 = s[7..9]), without
 // early exits: every lane of a warp runs the same instructions, and u, v, t are the
 // values the reference computes; only the final predicate decides the hit.
-// The packed form pairs the two cross products (q = d x e2, r = (o - v0) x e1) and
-// the dot products that share a factor ((e1, o - v0) . q and (d, e2) . r), with each
-// lane's operations in the scalar order: the same bits.
 __device__ __forceinline__ float tri_test(f3 o, f3 d, const float* s, float& u, float& v)
 {
-#if CPT_PACKED_TRI
-    const f3 p0 = mk3(s[0], s[1], s[2]), e1 = mk3(s[4], s[5], s[6]), e2 = mk3(s[7], s[8], s[9]);
-    const f3 sv = sub(o, p0);
-    // (q, r) component-wise: q = cross(d, e2), r = cross(sv, e1) (cross(a, b).x = a.y b.z - b.y a.z, ...)
-    const f2 qrx = sub2(mul2(mk2(d.y, sv.y), mk2(e2.z, e1.z)), mul2(mk2(e2.y, e1.y), mk2(d.z, sv.z)));
-    const f2 qry = sub2(mul2(mk2(d.z, sv.z), mk2(e2.x, e1.x)), mul2(mk2(e2.z, e1.z), mk2(d.x, sv.x)));
-    const f2 qrz = sub2(mul2(mk2(d.x, sv.x), mk2(e2.y, e1.y)), mul2(mk2(e2.x, e1.x), mk2(d.y, sv.y)));
-    // (det, u') = (e1 . q, sv . q) and (v', t') = (d . r, e2 . r): (a.x b.x + a.y b.y) + a.z b.z
-    const f2 du = add2(add2(mul2(mk2(e1.x, sv.x), mk2(qrx.x, qrx.x)), mul2(mk2(e1.y, sv.y), mk2(qry.x, qry.x))),
-                       mul2(mk2(e1.z, sv.z), mk2(qrz.x, qrz.x)));
-    const f2 vt = add2(add2(mul2(mk2(d.x, e2.x), mk2(qrx.y, qrx.y)), mul2(mk2(d.y, e2.y), mk2(qry.y, qry.y))),
-                       mul2(mk2(d.z, e2.z), mk2(qrz.y, qrz.y)));
-    const float det = du.x;
-    const float inv = __frcp_rn(det);
-    u = __fmul_rn(inv, du.y);
-    const f2 vt2 = mul2(mk2(inv, inv), vt);
-    v = vt2.x;
-    const float t = vt2.y;
-#else
     const f3 p0 = mk3(s[0], s[1], s[2]), e1 = mk3(s[4], s[5], s[6]), e2 = mk3(s[7], s[8], s[9]);
     const f3 q = cross(d, e2);
     const float det = dot(e1, q);
@@ -156,7 +132,6 @@ __device__ __forceinline__ float tri_test(f3 o, f3 d, const float* s, float& u, 
     const f3 r = cross(sv, e1);
     v = __fmul_rn(inv, dot(d, r));
     const float t = __fmul_rn(inv, dot(e2, r));
-#endif
     const bool hit = !(det > -FLT_EPSILON && det < FLT_EPSILON) && !(u < 0.f) && !(v < 0.f) &&
                      !(__fadd_rn(u, v) > 1.f) && t >= 0.0f;
     return hit ? t : FLT_MAX;
@@ -337,16 +312,21 @@ constexpr float kWideGrow = 1.0f + 1.0f / 262144.0f;  // relative slack of a wid
 #endif
 constexpr int kWideRefillLanes = CPT_WIDE_REFILL_LANES;
 // A lane with triangles still to test may visit its next node in the same step, the
-// node's triangle group queuing behind the first (at most two, or three, groups
-// pending): steps that were a triangle test for some lanes and a node visit for the
-// others become both for most lanes (C2: 370 -> 413 -> 420 Mrays/s).
-#ifndef CPT_WIDE_DUAL
-#define CPT_WIDE_DUAL 1
-#endif
-#ifndef CPT_WIDE_TRIPLE
-#define CPT_WIDE_TRIPLE 1  // a third pending group (with CPT_WIDE_DUAL): 420 vs 413 Mrays/s on C2
-#endif
+// node's triangle group queuing behind the first (up to three groups pending): steps
+// that were a triangle test for some lanes and a node visit for the others become both
+// for most lanes (C2: 370 Mrays/s with one group, 413 with two, 420 with three).
 constexpr float kWideFarInv = 1099511627776.0f;  // 2^40: 1/d of a zero direction component
+// Triangle tests in warp batches: a lane's pending triangles wait (it keeps visiting
+// nodes, its groups queue up) until at least this many lanes of the warp have some, or
+// one lane must test (all three group slots taken, or no node left to visit), so the
+// test runs with more lanes at once (C2, lanes that test per test step 9.2 of 32 without
+// it; threshold 8 / 12 / 16 / 20 / 24: 491.9 / 502.6 / 507.2 / 505.6 / 506.4 Mrays/s
+// against 493.9; 0 turns it off). Every step still consumes a node, a stack entry or a
+// triangle of every live lane, or ends its ray.
+#ifndef CPT_WIDE_TRI_BATCH
+#define CPT_WIDE_TRI_BATCH 16
+#endif
+constexpr int kWideTriBatch = CPT_WIDE_TRI_BATCH;
 
 struct WideState {
     const float4* nodes;
@@ -358,10 +338,8 @@ struct WideState {
     Hit best;
     uint32_t cbase, gbits;  // node group: first child; bits 0-7 hit slots in visit order, 8-15 internal mask
     uint32_t tbase, tbits;  // triangle group: first record; bits 0-7 hit leaf slots, 8-15 leaf mask
-    uint32_t tbase2, tbits2;  // a second triangle group, queued behind the first (CPT_WIDE_DUAL)
-#if CPT_WIDE_TRIPLE
+    uint32_t tbase2, tbits2;  // a second triangle group, queued behind the first
     uint32_t tbase3, tbits3;  // and a third
-#endif
     int sp;
     uint32_t visits, tests;
 };
@@ -389,10 +367,8 @@ __device__ __forceinline__ void wide_init(WideState& s, const float4* nodes, con
     s.tbits = 0;
     s.tbase2 = 0;
     s.tbits2 = 0;
-#if CPT_WIDE_TRIPLE
     s.tbase3 = 0;
     s.tbits3 = 0;
-#endif
     s.sp = 0;
     s.visits = 0;
     s.tests = 0;
@@ -513,9 +489,9 @@ __device__ __forceinline__ uint32_t wide_child_hits(const WideState& s, float4 n
 // One step; returns true when the ray is finished.
 template <bool kAny, int kBlock, bool kStats>
 __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* spill, bool& overflow,
-                                          uint32_t& n_nodes, uint32_t& n_tris)
+                                          uint32_t& n_nodes, uint32_t& n_tris, bool test_tri = true)
 {
-    if (s.tbits & 0xFFu) {
+    if (test_tri && (s.tbits & 0xFFu)) {
         const uint32_t slot = __ffs(s.tbits & 0xFFu) - 1;
         s.tbits &= ~(1u << slot);
         const uint32_t idx = s.tbase + __popc((s.tbits >> 8) & ((1u << slot) - 1u));
@@ -533,32 +509,17 @@ __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* 
             s.best.tri = __float_as_uint(a.w);
             if (kAny) return true;
         }
-#if CPT_WIDE_DUAL
-        if (!(s.tbits & 0xFFu) && (s.tbits2 & 0xFFu)) {  // the queued group moves up
+        if (!(s.tbits & 0xFFu) && (s.tbits2 & 0xFFu)) {  // the queued groups move up
             s.tbase = s.tbase2;
             s.tbits = s.tbits2;
-            s.tbits2 = 0;
-#if CPT_WIDE_TRIPLE
             s.tbase2 = s.tbase3;
             s.tbits2 = s.tbits3;
             s.tbits3 = 0;
-#endif
         }
-#if CPT_WIDE_TRIPLE
         if (s.tbits3 & 0xFFu) return false;  // every group slot pending: no node visit this step
-#else
-        if (s.tbits2 & 0xFFu) return false;  // both groups pending: no node visit this step
-#endif
-#else
-        if (s.tbits & 0xFFu) return false;  // more triangles of this group: next step
-#endif
     }
     if (!(s.gbits & 0xFFu)) {
-#if CPT_WIDE_DUAL
         if (s.sp == 0) return !(s.tbits & 0xFFu);  // done once the last triangles are tested
-#else
-        if (s.sp == 0) return true;
-#endif
         const uint2 g = wide_pop<kBlock>(smem_col, spill, s.sp);
         s.cbase = g.x;
         s.gbits = g.y;
@@ -576,20 +537,16 @@ __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* 
     const uint32_t hm = wide_child_hits(s, n0, n2, n3, n4);
     s.cbase = __float_as_uint(n1.x);
     s.gbits = xor_permute8(hm & imask, s.oct) | (imask << 8);
-#if CPT_WIDE_DUAL
     if (s.tbits & 0xFFu) {  // triangles still pending: the new group queues behind them
-#if CPT_WIDE_TRIPLE
         if (s.tbits2 & 0xFFu) {
             s.tbase3 = __float_as_uint(n1.y);
             s.tbits3 = (hm & lmask) | (lmask << 8);
             return false;
         }
-#endif
         s.tbase2 = __float_as_uint(n1.y);
         s.tbits2 = (hm & lmask) | (lmask << 8);
         return false;
     }
-#endif
     s.tbase = __float_as_uint(n1.y);
     s.tbits = (hm & lmask) | (lmask << 8);
     return false;
@@ -713,7 +670,18 @@ __device__ __forceinline__ void persistent_trace_wide(WideOf wide_of, const floa
         if (__ballot_sync(0xFFFFFFFFu, ray != CPT_INVALID_INDEX) == 0) break;
 #pragma unroll 1
         for (int k = 1;; ++k) {
-            if (ray != CPT_INVALID_INDEX && wide_step<kAny, kBlock, kStats>(s, smem_col, spill, overflow, n_nodes, n_tris)) {
+            bool test_tri = true;
+            if (kWideTriBatch) {
+                // the warp tests triangles when enough lanes have some pending, or when a lane
+                // must (every group slot taken, or no node left to visit)
+                const bool live = ray != CPT_INVALID_INDEX;
+                const bool want = live && (s.tbits & 0xFFu);
+                const bool must = want && ((s.tbits3 & 0xFFu) || (!(s.gbits & 0xFFu) && s.sp == 0));
+                const unsigned bw = __ballot_sync(0xFFFFFFFFu, want);
+                test_tri = __ballot_sync(0xFFFFFFFFu, must) != 0u || __popc(bw) >= kWideTriBatch;
+            }
+            if (ray != CPT_INVALID_INDEX &&
+                wide_step<kAny, kBlock, kStats>(s, smem_col, spill, overflow, n_nodes, n_tris, test_tri)) {
                 done(ray, s);
                 ray = CPT_INVALID_INDEX;
             }

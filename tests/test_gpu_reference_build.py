@@ -36,10 +36,15 @@ def test_reference_gpu_build_equals_ours(cuda, case):
     out = lb.download()
     for k in ("tris", "children", "parents_leaf", "parents_internal"):
         assert np.ascontiguousarray(out[k]).tobytes() == np.ascontiguousarray(getattr(ref, k)).tobytes(), k
-    # boxes: the reference's refit reads its sibling's box with no fence after the
-    # counter (BVHBuilder.cu:63-86); a stale read would show here as a differing box
-    differ = (out["node_boxes"].view(np.uint32).reshape(-1, 6) != ref.node_boxes.view(np.uint32).reshape(-1, 6))
-    assert not differ.any(), f"{int(differ.any(1).sum())} internal boxes differ"
+    # boxes: this library's equal the oracle's bit for bit. The reference's refit reads a
+    # sibling's box with no fence after the counter (BVHBuilder.cu:63-86), so on the GPU
+    # an occasional stale read leaves a box off (3 of 200,001 in one run, none in the
+    # others); its boxes may differ from the fenced result at a few nodes, never more.
+    mine = out["node_boxes"].view(np.uint32).reshape(-1, 6)
+    ob = cpu.build(tris, 30, box=box)
+    assert mine.tobytes() == ob.node_boxes.view(np.uint32).reshape(-1, 6).tobytes()
+    differ = (mine != ref.node_boxes.view(np.uint32).reshape(-1, 6)).any(1)
+    assert differ.sum() <= max(16, len(tris) // 10_000), f"{int(differ.sum())} of the reference's boxes differ"
 
 
 def test_reference_gpu_render_estimates_the_same_image(cuda):
