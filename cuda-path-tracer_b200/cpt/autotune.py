@@ -81,7 +81,7 @@ def candidates(pixels: int, spp: int, scratch_bytes: Callable[[int, int], int] |
 _FIELDS = ("wave_paths", "ray_sort", "refill_lanes", "blocks_per_sm")
 
 
-def launch_candidates(base: TuneResult, refills: Iterable[int] = (0, 28, 24, 16),
+def launch_candidates(base: TuneResult, refills: Iterable[int] = (0, 32, 28, 24, 16),
                       blocks: Iterable[int] = (0, 6, 4)) -> list[tuple[int, int, int, int]]:
     """(wave_paths, ray_sort, refill_lanes, blocks_per_sm) candidates at the wave and sort
     of `base`: every refill threshold at full occupancy, then every smaller block count at

@@ -304,11 +304,13 @@ __device__ __forceinline__ Hit traverse(const float4* __restrict__ nodes, f3 o, 
 // is tri_test on the binary leaf slot's words, so a hit's t, u, v are unchanged.
 constexpr int kWideSmemStack = 16;  // stack entries (2 words) per thread in shared memory
 constexpr float kWideGrow = 1.0f + 1.0f / 262144.0f;  // relative slack of a wide child's box test
-// The wide traversal refills as soon as one lane of the warp is idle: its steps are
-// long (8 child boxes), so an idle lane costs more than the refill's ballot and
-// atomic (C2: 313 Mrays/s at 32, 302 at 28, 283 at 24, 242 at 16, 196 at 8).
+// The wide traversal refills once two lanes of the warp are idle (fewer than 31 busy):
+// its steps are long (8 child boxes), so idle lanes cost more than the refill's ballot
+// and atomic (C2 with one triangle test per step: 313 Mrays/s at 32, 302 at 28, 283 at
+// 24, 242 at 16, 196 at 8; with the tests batched per warp: 505.5 / 506.0 at 32,
+// 514.7 / 514.3 at 31, 513.6 / 513.6 at 30, 509.0 at 29, 506.2 at 28).
 #ifndef CPT_WIDE_REFILL_LANES
-#define CPT_WIDE_REFILL_LANES 32
+#define CPT_WIDE_REFILL_LANES 31
 #endif
 constexpr int kWideRefillLanes = CPT_WIDE_REFILL_LANES;
 // A lane with triangles still to test may visit its next node in the same step, the

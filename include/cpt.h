@@ -264,7 +264,7 @@ typedef struct cpt_render_params {
                                 * an emitter table. 0: the reference's estimator */
     /* launch shape of the persistent traversal kernels (results are unchanged; for tuning):
      * refill_lanes: a warp takes new rays once fewer than this many of its lanes still trace
-     * (1..32; 0: 32 over wide trees, 16 over binary trees); traverse_blocks_per_sm: resident
+     * (1..32; 0: 31 over wide trees, 16 over binary trees); traverse_blocks_per_sm: resident
      * blocks per SM of the closest-hit traversal, at most its occupancy (0: occupancy) */
     uint32_t refill_lanes;
     uint32_t traverse_blocks_per_sm;
