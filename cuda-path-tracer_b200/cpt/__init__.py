@@ -107,7 +107,7 @@ class RenderParams(ctypes.Structure):
                 ("accum_mode", ctypes.c_uint32), ("ref_grid", ctypes.c_uint32), ("wave_paths", ctypes.c_uint32),
                 ("trace_stats", ctypes.c_uint32), ("ray_sort", ctypes.c_uint32), ("cameras", ctypes.c_uint32),
                 ("frame_counter", ctypes.c_void_p), ("nee", ctypes.c_uint32), ("refill_lanes", ctypes.c_uint32),
-                ("traverse_blocks_per_sm", ctypes.c_uint32)]
+                ("traverse_blocks_per_sm", ctypes.c_uint32), ("wave_lanes", ctypes.c_uint32)]
 
 
 def _load() -> ctypes.CDLL:
@@ -198,6 +198,7 @@ _PROTOS = {
     "cpt_profile_begin": (_I32, []),
     "cpt_profile_end": (_I32, []),
     "cpt_profile_get": (_I32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_ulonglong)]),
+    "cpt_profile_get_busy": (_I32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]),
     "cpt_version": (ctypes.c_char_p, []),
     "cpt_launch_count": (ctypes.c_ulonglong, []),
 }
@@ -368,6 +369,17 @@ def profile_end() -> dict:
         check(lib.cpt_profile_get(k.encode(), ctypes.byref(ms), ctypes.byref(n)), "cpt_profile_get")
         if n.value:
             out[k] = (ms.value, int(n.value))
+    return out
+
+
+def profile_busy() -> dict:
+    """After profile_end: {kernel: milliseconds during which at least one of its launches ran}."""
+    out = {}
+    for k in KERNELS:
+        ms = ctypes.c_double()
+        check(lib.cpt_profile_get_busy(k.encode(), ctypes.byref(ms)), "cpt_profile_get_busy")
+        if ms.value:
+            out[k] = ms.value
     return out
 
 

@@ -42,6 +42,7 @@ class TuneResult:
     table: list = field(default_factory=list)  # every candidate: {"wave_paths", "ray_sort", ..., "ms"}
     refill_lanes: int = 0  # 0: the renderer's default
     blocks_per_sm: int = 0  # 0: the traversal's occupancy
+    wave_lanes: int = 0  # 0: the renderer's default (one lane)
 
 
 def samples_per_wave(wave_paths: int, pixels: int, spp: int) -> int:
@@ -78,19 +79,22 @@ def candidates(pixels: int, spp: int, scratch_bytes: Callable[[int, int], int] |
     return out
 
 
-_FIELDS = ("wave_paths", "ray_sort", "refill_lanes", "blocks_per_sm")
+_FIELDS = ("wave_paths", "ray_sort", "refill_lanes", "blocks_per_sm", "wave_lanes")
 
 
 def launch_candidates(base: TuneResult, refills: Iterable[int] = (0, 32, 28, 24, 16),
-                      blocks: Iterable[int] = (0, 6, 4)) -> list[tuple[int, int, int, int]]:
-    """(wave_paths, ray_sort, refill_lanes, blocks_per_sm) candidates at the wave and sort
-    of `base`: every refill threshold at full occupancy, then every smaller block count at
-    the default threshold (0 = the renderer's default in both)."""
-    out = [(base.wave_paths, base.ray_sort, int(r), 0) for r in refills]
-    out += [(base.wave_paths, base.ray_sort, 0, int(b)) for b in blocks if int(b)]
-    for r, b in ((c[2], c[3]) for c in out):
-        if not (0 <= r <= 32 and 0 <= b):
-            raise ValueError(f"bad launch candidate: refill {r}, blocks {b}")
+                      blocks: Iterable[int] = (0, 6, 4),
+                      lanes: Iterable[int] = (2,)) -> list[tuple[int, int, int, int, int]]:
+    """(wave_paths, ray_sort, refill_lanes, blocks_per_sm, wave_lanes) candidates at the
+    wave and sort of `base`: every refill threshold at full occupancy, every smaller block
+    count at the default threshold, then every other lane count at the default shape
+    (0 = the renderer's default in each)."""
+    out = [(base.wave_paths, base.ray_sort, int(r), 0, 0) for r in refills]
+    out += [(base.wave_paths, base.ray_sort, 0, int(b), 0) for b in blocks if int(b)]
+    out += [(base.wave_paths, base.ray_sort, 0, 0, int(n)) for n in lanes if int(n)]
+    for r, b, n in ((c[2], c[3], c[4]) for c in out):
+        if not (0 <= r <= 32 and 0 <= b and 0 <= n <= 2):
+            raise ValueError(f"bad launch candidate: refill {r}, blocks {b}, lanes {n}")
     seen, uniq = set(), []
     for c in out:
         if c not in seen:
@@ -101,14 +105,14 @@ def launch_candidates(base: TuneResult, refills: Iterable[int] = (0, 32, 28, 24,
 
 def tune(time_frame: Callable[..., float], cands: Iterable[tuple]) -> TuneResult:
     """Times every candidate once and returns the fastest (the first of equal times),
-    with the whole table. A candidate is (wave_paths, ray_sort) or (wave_paths,
-    ray_sort, refill_lanes, blocks_per_sm); `time_frame` is called with the candidate's
-    values (two or four arguments) and returns milliseconds."""
+    with the whole table. A candidate is (wave_paths, ray_sort), (wave_paths, ray_sort,
+    refill_lanes, blocks_per_sm) or that and wave_lanes; `time_frame` is called with the
+    candidate's values (two, four or five arguments) and returns milliseconds."""
     table = []
     for cand in cands:
         cand = tuple(int(x) for x in cand)
-        if len(cand) not in (2, 4):
-            raise ValueError(f"a candidate has 2 or 4 values, not {cand}")
+        if len(cand) not in (2, 4, 5):
+            raise ValueError(f"a candidate has 2, 4 or 5 values, not {cand}")
         ms = float(time_frame(*cand))
         if not ms >= 0.0:
             raise ValueError(f"time_frame returned {ms} ms for candidate {cand}")
@@ -120,7 +124,7 @@ def tune(time_frame: Callable[..., float], cands: Iterable[tuple]) -> TuneResult
     best = min(range(len(table)), key=lambda i: (table[i]["ms"], i))
     b = table[best]
     return TuneResult(b["wave_paths"], b["ray_sort"], b["ms"], table, b.get("refill_lanes", 0),
-                      b.get("blocks_per_sm", 0))
+                      b.get("blocks_per_sm", 0), b.get("wave_lanes", 0))
 
 
 def workload_key(device: str, pixels: int, spp: int, bounces: int, triangles: int, nee: bool = False) -> str:

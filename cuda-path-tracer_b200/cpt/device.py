@@ -216,10 +216,12 @@ class LbvhBatch:
 
 def make_params(width, height, spp, frame0=0, bounces=3, intensity=3.0, stratified=True, seed=0,
                 accum_mode=ACCUM_KAHAN, ref_grid=False, wave_paths=0, trace_stats=False,
-                ray_sort=False, cameras=1, nee=False, refill_lanes=0, traverse_blocks_per_sm=0) -> RenderParams:
+                ray_sort=False, cameras=1, nee=False, refill_lanes=0, traverse_blocks_per_sm=0,
+                wave_lanes=0) -> RenderParams:
     return RenderParams(width, height, spp, frame0, bounces, intensity, int(stratified), seed & 0xFFFFFFFF,
                         (seed >> 32) & 0xFFFFFFFF, accum_mode, int(ref_grid), wave_paths, int(trace_stats),
-                        int(ray_sort), cameras, None, int(nee), int(refill_lanes), int(traverse_blocks_per_sm))
+                        int(ray_sort), cameras, None, int(nee), int(refill_lanes), int(traverse_blocks_per_sm),
+                        int(wave_lanes))
 
 
 class DeviceRenderer:

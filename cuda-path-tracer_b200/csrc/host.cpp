@@ -30,6 +30,7 @@ std::mutex g_prof_mu;
 std::vector<ProfRecord> g_prof_records;
 std::vector<cudaEvent_t> g_event_pool;
 double g_prof_ms[K_KERNEL_COUNT];
+double g_prof_busy_ms[K_KERNEL_COUNT];  // union of the launches' intervals (launches on several streams overlap)
 unsigned long long g_prof_launches[K_KERNEL_COUNT];
 
 cudaEvent_t take_event()
@@ -200,7 +201,7 @@ extern "C" const char* cpt_version(void) { return "cpt-b200 0.1 (sm_100a)"; }
 extern "C" int cpt_profile_begin(void)
 {
     std::lock_guard<std::mutex> lk(g_prof_mu);
-    for (int k = 0; k < K_KERNEL_COUNT; ++k) { g_prof_ms[k] = 0.0; g_prof_launches[k] = 0; }
+    for (int k = 0; k < K_KERNEL_COUNT; ++k) { g_prof_ms[k] = 0.0; g_prof_busy_ms[k] = 0.0; g_prof_launches[k] = 0; }
     g_profiling.store(true);
     return CPT_OK;
 }
@@ -210,11 +211,35 @@ extern "C" int cpt_profile_end(void)
     g_profiling.store(false);
     std::lock_guard<std::mutex> lk(g_prof_mu);
     int rc = CPT_OK;
+    // each launch as an interval on a common time axis (offsets from the first record's
+    // start event), then per kernel the length of the union of its intervals
+    std::vector<std::pair<double, double>> spans[K_KERNEL_COUNT];
+    const cudaEvent_t origin = g_prof_records.empty() ? nullptr : g_prof_records.front().a;
     for (const ProfRecord& r : g_prof_records) {
-        float ms = 0.f;
-        if (cudaEventSynchronize(r.b) != cudaSuccess || cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) rc = CPT_ERR_CUDA;
+        float ms = 0.f, t0 = 0.f;
+        if (cudaEventSynchronize(r.b) != cudaSuccess || cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess ||
+            cudaEventElapsedTime(&t0, origin, r.a) != cudaSuccess)
+            rc = CPT_ERR_CUDA;
         g_prof_ms[r.id] += ms;
         g_prof_launches[r.id] += 1;
+        spans[r.id].push_back({(double)t0, (double)t0 + ms});
+    }
+    for (int k = 0; k < K_KERNEL_COUNT; ++k) {
+        std::sort(spans[k].begin(), spans[k].end());
+        double busy = 0.0, a = 0.0, b = -1.0;
+        for (const auto& iv : spans[k]) {
+            if (iv.first > b) {
+                if (b > a) busy += b - a;
+                a = iv.first;
+                b = iv.second;
+            } else if (iv.second > b) {
+                b = iv.second;
+            }
+        }
+        if (b > a) busy += b - a;
+        g_prof_busy_ms[k] += busy;
+    }
+    for (const ProfRecord& r : g_prof_records) {
         g_event_pool.push_back(r.a);
         g_event_pool.push_back(r.b);
     }
@@ -234,6 +259,18 @@ extern "C" int cpt_profile_get(const char* kernel, double* total_ms, unsigned lo
         }
     return CPT_ERR_INVALID_ARGUMENT;
 }
+extern "C" int cpt_profile_get_busy(const char* kernel, double* busy_ms)
+{
+    if (!kernel || !busy_ms) return CPT_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    for (int k = 0; k < K_KERNEL_COUNT; ++k)
+        if (strcmp(kernel, kKernelNames[k]) == 0) {
+            *busy_ms = g_prof_busy_ms[k];
+            return CPT_OK;
+        }
+    return CPT_ERR_INVALID_ARGUMENT;
+}
+
 extern "C" unsigned long long cpt_launch_count(void) { return g_launches.load(); }
 
 extern "C" uint32_t cpt_scene_random(uint32_t n_random, uint32_t seed, float edge_min, float edge_max, float albedo,

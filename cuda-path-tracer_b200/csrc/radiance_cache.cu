@@ -698,6 +698,9 @@ extern "C" size_t cpt_rc_render_scratch_bytes(const cpt_rc* rc, const cpt_view* 
                                               const cpt_render_params* params)
 {
     if (!rc || !views || n_views == 0 || n_views > CPT_MAX_VIEWS || !params) return 0;
+    cpt_render_params one = *params;
+    one.wave_lanes = 1;  // cached renders run as one lane (their records are per wave)
+    params = &one;
     std::vector<cpt_view> tv(views, views + n_views);
     const uint32_t per_view = std::max(1u, rc->params.train_samples / n_views);
     for (auto& v : tv) train_size(v, per_view, v.width, v.height);
@@ -722,6 +725,9 @@ int rc_frame(cpt_rc* rc, const cpt_view* views, uint32_t n_views, const cpt_rend
     const size_t need = cpt_rc_render_scratch_bytes(rc, views, n_views, params);
     if (!need) return CPT_ERR_INVALID_ARGUMENT;
     if (scratch_bytes < need) return CPT_ERR_SCRATCH_TOO_SMALL;
+    cpt_render_params one = *params;
+    one.wave_lanes = 1;  // as sized above
+    params = &one;
     std::vector<cpt_view> tv(views, views + n_views);
     const uint32_t per_view = std::max(1u, rc->params.train_samples / n_views);
     for (auto& v : tv) train_size(v, per_view, v.width, v.height);

@@ -85,6 +85,7 @@ struct Views {
 // [pixel_base(v) * spw, (pixel_base(v) + pixels(v)) * spw), sample-major inside.
 struct Wave {
     uint32_t s0, spw;
+    uint32_t p0, p1;  // the paths of the wave this launch sequence generates (a lane's half, or all)
     uint32_t frame0;
     const uint32_t* frame_dev;  // nullable: added to frame0 on the device (CUDA-graph replays)
     uint32_t bounces;
@@ -246,9 +247,8 @@ __device__ __forceinline__ uint32_t wave_frame0(const Wave& wv) { return wv.fram
 __global__ void __launch_bounds__(kGenBlock) k_generate(Wave wv, Views vs, float4* __restrict__ queue,
                                                         uint32_t* __restrict__ counts, float4* __restrict__ state)
 {
-    const uint32_t total = wv.spw * vs.total_pixels;
     const uint32_t frame0 = wave_frame0(wv);
-    for (uint32_t pid = blockIdx.x * kGenBlock + threadIdx.x; pid < total; pid += gridDim.x * kGenBlock) {
+    for (uint32_t pid = wv.p0 + blockIdx.x * kGenBlock + threadIdx.x; pid < wv.p1; pid += gridDim.x * kGenBlock) {
         const uint32_t vi = view_of_path(vs, pid, wv.spw);
         const View& v = vs.v[vi];
         const uint32_t local = pid - v.pixel_base * wv.spw;
@@ -786,6 +786,16 @@ constexpr int kShadowCountWord = 2 * (kMaxDepth + 2);
 constexpr int kShadowPoolWord = 3 * (kMaxDepth + 2);
 constexpr int kRecordCountWord = 4 * (kMaxDepth + 2);
 
+// What one lane of a wave owns: its ray queues, hits, counters and shadow-ray queue
+// (paths and their state belong to the wave).
+struct Lane {
+    float4* queue[2];
+    float4* hits;
+    uint32_t* counts;
+    float4* shadow_rays;      // next-event estimation: 2 float4 per shadow ray
+    float4* shadow_emission;  // and its emission | path id
+};
+
 struct RenderScratch {
     float4* queue[2];
     float4* hits;
@@ -794,6 +804,8 @@ struct RenderScratch {
     uint32_t capacity;  // paths per wave
     float4* shadow_rays;      // next-event estimation: 2 float4 per shadow ray
     float4* shadow_emission;  // and its emission | path id
+    Lane second;              // the second lane (wave_lanes 2): queues for half the capacity
+    bool two_lanes;
     // coherence sort of bounce queues
     uint32_t* sort_keys[2];
     uint32_t* sort_vals[2];
@@ -802,6 +814,16 @@ struct RenderScratch {
     uint32_t* sort_zero;  // tile counters (32 words) + look-back
     size_t sort_zero_words;
 };
+
+// Lanes per wave the scratch is laid out for: 2 on request (not with ray sorting, whose
+// buffers are the wave's), else 1. A call with a render hook uses one lane whatever the
+// scratch holds. Measured (events per frame): C3's 64 views 1067 -> 1099 Mrays/s with
+// two lanes; C2 516 -> 514 and C1 400 -> 369 (small waves pay for the second sequence
+// of launches), so one lane is the default and the autotuner tries two.
+inline uint32_t wave_lanes(const cpt_render_params* p)
+{
+    return (p->wave_lanes == 2 && !p->ray_sort) ? 2u : 1u;
+}
 
 // Image-samples per wave for `pixels` pixels over all views.
 inline uint32_t wave_samples(const cpt_render_params* p, uint64_t pixels)
@@ -828,6 +850,22 @@ size_t render_layout(const cpt_render_params* p, uint64_t pixels, void* base, Re
         s.shadow_emission = c.take<float4>(s.capacity);
     } else {
         s.shadow_rays = s.shadow_emission = nullptr;
+    }
+    s.two_lanes = wave_lanes(p) == 2;
+    if (s.two_lanes) {
+        const uint64_t half = s.capacity / 2 + 1;
+        s.second.queue[0] = c.take<float4>(2ull * half);
+        s.second.queue[1] = c.take<float4>(2ull * half);
+        s.second.hits = c.take<float4>(half);
+        s.second.counts = c.take<uint32_t>(kCountWords);
+        if (p->nee) {
+            s.second.shadow_rays = c.take<float4>(2ull * half);
+            s.second.shadow_emission = c.take<float4>(half);
+        } else {
+            s.second.shadow_rays = s.second.shadow_emission = nullptr;
+        }
+    } else {
+        s.second = Lane{};
     }
     if (p->ray_sort) {
         const size_t tiles = (s.capacity + kSortTile - 1) / kSortTile;
@@ -897,7 +935,7 @@ bool params_ok(const cpt_render_params* p, uint64_t pixels)
 {
     if (!p || p->spp == 0 || pixels == 0 || pixels > (1ull << 31)) return false;
     if (p->bounces + 1 > (uint32_t)kMaxDepth) return false;
-    if (p->accum_mode > CPT_ACCUM_F64 || p->nee > 1) return false;
+    if (p->accum_mode > CPT_ACCUM_F64 || p->nee > 1 || p->wave_lanes > 2) return false;
     return pixels * wave_samples(p, pixels) < (1ull << 31);
 }
 
@@ -955,6 +993,43 @@ uint64_t make_views(const cpt_view* views, uint32_t n, uint32_t ref_grid, bool n
     return total;
 }
 
+// The second lane's stream and the three events that order it against the caller's
+// stream (fork at the wave's start, the one-launch stagger, the join before the
+// accumulation), one set per device, created on first use and kept for the process.
+struct LaneStreams {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, stagger = nullptr, join = nullptr;
+};
+constexpr uint32_t kMinLanePaths = 1u << 12;  // waves below twice this run as one lane
+
+LaneStreams* lane_streams()
+{
+    constexpr int kMaxDevices = 64;
+    static LaneStreams table[kMaxDevices];
+    static std::mutex mu;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    LaneStreams& l = table[dev];
+    if (!l.stream) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+        bool ok = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
+        for (int k = 0; k < 3 && ok; ++k) ok = cudaEventCreateWithFlags(&e[k], cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) {
+            for (int k = 0; k < 3; ++k)
+                if (e[k]) cudaEventDestroy(e[k]);
+            if (st) cudaStreamDestroy(st);
+            return nullptr;
+        }
+        l.fork = e[0];
+        l.stagger = e[1];
+        l.join = e[2];
+        l.stream = st;
+    }
+    return &l;
+}
+
 int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, const cpt_render_params* params,
                  void* scratch, size_t scratch_bytes, unsigned long long* ray_counts, uint32_t* status,
                  const RenderHook* hook, cudaStream_t stream)
@@ -997,40 +1072,55 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
             ext_occ < 1)
             ext_occ = 1;
     }
-    const uint32_t spw_max = wave_samples(params, pixels);
-    for (uint32_t s0 = 0; s0 < params->spp; s0 += spw_max) {
-        wv.s0 = s0;
-        wv.spw = std::min(spw_max, params->spp - s0);
-        const uint32_t paths = wv.spw * vs.total_pixels;
-        CPT_CUDA_TRY(cudaMemsetAsync(rs.counts, 0, sizeof(uint32_t) * kCountWords, stream));
+    // Two lanes: the wave's paths split in halves, the second half on the library's own
+    // stream, its first traversal launch one launch behind the first half's, the halves
+    // joined before the wave's accumulation (paths and their state are the wave's, so
+    // the image is the one-lane image).
+    const bool two = rs.two_lanes && !hook;
+    LaneStreams* ls = nullptr;
+    if (two) {
+        ls = lane_streams();
+        if (!ls) return CPT_ERR_CUDA;
+    }
+    const Lane first{{rs.queue[0], rs.queue[1]}, rs.hits, rs.counts, rs.shadow_rays, rs.shadow_emission};
+    // launch shape of the persistent traversal: resident blocks per SM (occupancy, or the
+    // caller's smaller figure) and the refill threshold of its warps (0: the default)
+    const int per_sm = params->traverse_blocks_per_sm ? std::min<int>(ext_occ, (int)params->traverse_blocks_per_sm)
+                                                      : ext_occ;
+    const uint32_t refill = std::min<uint32_t>(params->refill_lanes, 32u);
+
+    // Generation, every vertex's extension + shading (+ shadow rays), and the lane's ray
+    // counts, for the wave's paths [wl.p0, wl.p1) on stream st. after_first (nullable):
+    // recorded after the lane's first traversal launch; before_first (nullable): waited
+    // on before it.
+    auto run_lane = [&](const Lane& L, const Wave& wl, cudaStream_t st, cudaEvent_t after_first,
+                        cudaEvent_t before_first) -> int {
+        const uint32_t paths = wl.p1 - wl.p0;
+        CPT_CUDA_TRY(cudaMemsetAsync(L.counts, 0, sizeof(uint32_t) * kCountWords, st));
         {
-            CPT_PROF(K_GENERATE, stream);
+            CPT_PROF(K_GENERATE, st);
             k_generate<<<(int)std::min<uint32_t>((paths + kGenBlock - 1) / kGenBlock, (uint32_t)sms * 16), kGenBlock, 0,
-                         stream>>>(wv, vs, rs.queue[0], rs.counts, rs.state);
+                         st>>>(wl, vs, L.queue[0], L.counts, rs.state);
         }
         CPT_LAUNCH_CHECK();
-        // launch shape of the persistent traversal: resident blocks per SM (occupancy, or the
-        // caller's smaller figure) and the refill threshold of its warps (0: the default)
-        const int per_sm = params->traverse_blocks_per_sm ? std::min<int>(ext_occ, (int)params->traverse_blocks_per_sm)
-                                                          : ext_occ;
         const int ext_blocks = std::min<int>((int)((paths + kExtendBlock - 1) / kExtendBlock), sms * per_sm);
-        const uint32_t refill = std::min<uint32_t>(params->refill_lanes, 32u);
         const int shade_blocks = std::min<int>((int)((paths + kShadeBlock - 1) / kShadeBlock), sms * 16);
         for (uint32_t b = 0; b <= params->bounces; ++b) {
-            const float4* qin = rs.queue[b & 1];
-            float4* qout = rs.queue[(b + 1) & 1];
+            const float4* qin = L.queue[b & 1];
+            float4* qout = L.queue[(b + 1) & 1];
             const uint32_t* order = nullptr;
             if (params->ray_sort && b > 0) {
-                const int rc = sort_queue(rs, qin, rs.counts + b, sort_root, status, stream);
+                const int rc = sort_queue(rs, qin, L.counts + b, sort_root, status, st);
                 if (rc != CPT_OK) return rc;
                 order = rs.sort_vals[(kRayKeyPasses - 1) & 1];
             }
+            if (b == 0 && before_first) CPT_CUDA_TRY(cudaStreamWaitEvent(st, before_first, 0));
             {
-                CPT_PROF(K_EXTEND, stream);
-                uint32_t* pool = rs.counts + kMaxDepth + 2 + b;
+                CPT_PROF(K_EXTEND, st);
+                uint32_t* pool = L.counts + kMaxDepth + 2 + b;
 #define CPT_EXTEND(S, O, W) \
-    k_extend<S, O, W><<<ext_blocks, kExtendBlock, 0, stream>>>(vs, qin, rs.counts + b, rs.hits, pool, ray_counts, status, \
-                                                               order, refill)
+    k_extend<S, O, W><<<ext_blocks, kExtendBlock, 0, st>>>(vs, qin, L.counts + b, L.hits, pool, ray_counts, status, \
+                                                           order, refill)
                 if (wide) {
                     if (params->trace_stats) {
                         if (one_bvh) CPT_EXTEND(true, true, true); else CPT_EXTEND(true, false, true);
@@ -1045,17 +1135,18 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
 #undef CPT_EXTEND
             }
             CPT_LAUNCH_CHECK();
+            if (b == 0 && after_first) CPT_CUDA_TRY(cudaEventRecord(after_first, st));
             const bool nee_here = params->nee && b < params->bounces;
-            if (hook && hook->shade_after && s0 == 0 && b == 0)
-                CPT_CUDA_TRY(cudaStreamWaitEvent(stream, hook->shade_after, 0));
+            if (hook && hook->shade_after && wl.s0 == 0 && b == 0)
+                CPT_CUDA_TRY(cudaStreamWaitEvent(st, hook->shade_after, 0));
             {
-                CPT_PROF(K_SHADE, stream);
-#define CPT_SHADE(L, R, N)                                                                                          \
-    k_shade<L, R, N><<<shade_blocks, kShadeBlock, 0, stream>>>(vs, wv, b, qin, rs.hits, rs.counts + b, qout,        \
-                                                               rs.counts + b + 1, rs.state, ray_counts, status,    \
-                                                               rs.shadow_rays, rs.shadow_emission,                 \
-                                                               rs.counts + kShadowCountWord + b)
-                const bool rec_here = record && b == wv.record_depth;
+                CPT_PROF(K_SHADE, st);
+#define CPT_SHADE(LI, R, N)                                                                                         \
+    k_shade<LI, R, N><<<shade_blocks, kShadeBlock, 0, st>>>(vs, wl, b, qin, L.hits, L.counts + b, qout,            \
+                                                            L.counts + b + 1, rs.state, ray_counts, status,        \
+                                                            L.shadow_rays, L.shadow_emission,                      \
+                                                            L.counts + kShadowCountWord + b)
+                const bool rec_here = record && b == wl.record_depth;
                 if (params->nee) {  // (the last vertex queues no shadow ray: it does not bounce)
                     if (any_lights) {
                         if (rec_here) CPT_SHADE(true, true, true); else CPT_SHADE(true, false, true);
@@ -1073,12 +1164,12 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
             }
             CPT_LAUNCH_CHECK();
             if (nee_here) {
-                CPT_PROF(K_OCCLUDE, stream);
-                uint32_t* spool = rs.counts + kShadowPoolWord + b;
-                const uint32_t* scount = rs.counts + kShadowCountWord + b;
+                CPT_PROF(K_OCCLUDE, st);
+                uint32_t* spool = L.counts + kShadowPoolWord + b;
+                const uint32_t* scount = L.counts + kShadowCountWord + b;
 #define CPT_OCCLUDE(O, W)                                                                                   \
-    k_occlude<O, W><<<ext_blocks, kExtendBlock, 0, stream>>>(vs, rs.shadow_rays, rs.shadow_emission, scount, spool, \
-                                                             rs.state, status)
+    k_occlude<O, W><<<ext_blocks, kExtendBlock, 0, st>>>(vs, L.shadow_rays, L.shadow_emission, scount, spool, \
+                                                         rs.state, status)
                 if (wide) {
                     if (one_bvh) CPT_OCCLUDE(true, true); else CPT_OCCLUDE(false, true);
                 } else {
@@ -1090,10 +1181,35 @@ int render_views(const Views& vs, bool any_lights, const cpt_bbox* sort_root, co
         }
         if (ray_counts) {
             {
-                CPT_PROF(K_WAVE_COUNTS, stream);
-                k_wave_counts<<<1, 32, 0, stream>>>(rs.counts, params->bounces + 1, ray_counts);
+                CPT_PROF(K_WAVE_COUNTS, st);
+                k_wave_counts<<<1, 32, 0, st>>>(L.counts, params->bounces + 1, ray_counts);
             }
             CPT_LAUNCH_CHECK();
+        }
+        return CPT_OK;
+    };
+
+    const uint32_t spw_max = wave_samples(params, pixels);
+    for (uint32_t s0 = 0; s0 < params->spp; s0 += spw_max) {
+        wv.s0 = s0;
+        wv.spw = std::min(spw_max, params->spp - s0);
+        const uint32_t paths = wv.spw * vs.total_pixels;
+        if (two && paths >= 2 * kMinLanePaths) {
+            Wave wa = wv, wb = wv;
+            wa.p0 = 0;
+            wa.p1 = paths / 2;
+            wb.p0 = paths / 2;
+            wb.p1 = paths;
+            CPT_CUDA_TRY(cudaEventRecord(ls->fork, stream));
+            CPT_CUDA_TRY(cudaStreamWaitEvent(ls->stream, ls->fork, 0));
+            if (const int rc = run_lane(first, wa, stream, ls->stagger, nullptr)) return rc;
+            if (const int rc = run_lane(rs.second, wb, ls->stream, nullptr, ls->stagger)) return rc;
+            CPT_CUDA_TRY(cudaEventRecord(ls->join, ls->stream));
+            CPT_CUDA_TRY(cudaStreamWaitEvent(stream, ls->join, 0));
+        } else {
+            wv.p0 = 0;
+            wv.p1 = paths;
+            if (const int rc = run_lane(first, wv, stream, nullptr, nullptr)) return rc;
         }
         if (hook && hook->after_wave) {
             const int rc = hook->after_wave(hook->ctx, hook->records, wv.record_count, hook->capacity, rs.state, stream);

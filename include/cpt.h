@@ -268,6 +268,12 @@ typedef struct cpt_render_params {
      * blocks per SM of the closest-hit traversal, at most its occupancy (0: occupancy) */
     uint32_t refill_lanes;
     uint32_t traverse_blocks_per_sm;
+    /* wave_lanes: 2 splits each wave's paths into two halves traced and shaded at once on
+     * the caller's stream and a second stream the library owns, the second half one
+     * launch behind, so that each launch's slowest rays overlap the other half's work
+     * (images unchanged); 1: one sequence on the caller's stream; 0: the library's
+     * default (1). Calls with a radiance cache or ray sorting use one lane. */
+    uint32_t wave_lanes;
 } cpt_render_params;
 
 size_t cpt_accum_bytes(uint32_t width, uint32_t height, uint32_t accum_mode); /* per camera / view */
@@ -526,6 +532,10 @@ int cpt_rc_samples(cpt_rc* rc, const float** samples_dev);
 int cpt_profile_begin(void);
 int cpt_profile_end(void);
 int cpt_profile_get(const char* kernel, double* total_ms, unsigned long long* launches);
+/* Milliseconds during which at least one launch of the kernel ran, between the last
+ * begin and end (the union of the launches' event intervals; below the total when
+ * launches on two streams overlap, e.g. two wave lanes). */
+int cpt_profile_get_busy(const char* kernel, double* busy_ms);
 
 /* ---- library info ---- */
 const char* cpt_version(void);

@@ -81,13 +81,19 @@ def test_cache_round_trip(tmp_path):
 def test_launch_shape_stage():
     base = autotune.TuneResult(4 * PIXELS, 0, 10.0)
     c = autotune.launch_candidates(base, refills=(0, 24, 24, 16), blocks=(0, 6))
-    assert c == [(4 * PIXELS, 0, 0, 0), (4 * PIXELS, 0, 24, 0), (4 * PIXELS, 0, 16, 0), (4 * PIXELS, 0, 0, 6)]
-    times = {(24, 0): 7.0, (16, 0): 8.0, (0, 6): 7.0}
-    r = autotune.tune(lambda w, s, rl, b: times.get((rl, b), 9.0), c)
-    assert (r.refill_lanes, r.blocks_per_sm, r.ms) == (24, 0, 7.0)
-    assert r.table[0] == {"wave_paths": 4 * PIXELS, "ray_sort": 0, "refill_lanes": 0, "blocks_per_sm": 0, "ms": 9.0}
+    assert c == [(4 * PIXELS, 0, 0, 0, 0), (4 * PIXELS, 0, 24, 0, 0), (4 * PIXELS, 0, 16, 0, 0),
+                 (4 * PIXELS, 0, 0, 6, 0), (4 * PIXELS, 0, 0, 0, 2)]
+    times = {(24, 0, 0): 7.0, (16, 0, 0): 8.0, (0, 6, 0): 7.0, (0, 0, 2): 7.5}
+    r = autotune.tune(lambda w, s, rl, b, n: times.get((rl, b, n), 9.0), c)
+    assert (r.refill_lanes, r.blocks_per_sm, r.wave_lanes, r.ms) == (24, 0, 0, 7.0)
+    assert r.table[0] == {"wave_paths": 4 * PIXELS, "ray_sort": 0, "refill_lanes": 0, "blocks_per_sm": 0,
+                          "wave_lanes": 0, "ms": 9.0}
+    r2 = autotune.tune(lambda w, s, rl, b, n: 5.0 if n == 2 else 9.0, c)
+    assert r2.wave_lanes == 2
     with pytest.raises(ValueError):
         autotune.launch_candidates(base, refills=(40,))
+    with pytest.raises(ValueError):
+        autotune.launch_candidates(base, lanes=(3,))
     with pytest.raises(ValueError):
         autotune.tune(lambda *a: 1.0, [(1, 0, 0)])
     # the renderer accepts every candidate's fields (scratch sizes do not depend on them)

@@ -51,11 +51,12 @@ def test_reference_gpu_render_estimates_the_same_image(cuda):
     """The reference's raytrace_kernel (cuda_path_tracer.cu:385-421, its own curand
     stream) and this library's renderer (the Philox stream) estimate the same image,
     512 one-sample frames each. The image means agree within 2 %. Block by block
-    (8x8 pixels, 3 channels), the squared differences to the reference's image sum to
-    about what two independent renders of this library (seeds 9 and 10) differ by —
-    noise of equal size on both sides gives a ratio near 1, a bias of a few percent
-    in lit blocks would push it far above; it must stay below 2 (with 144 block values
-    per side the ratio's spread is about 0.2)."""
+    (8x8 pixels, 3 channels), the squared differences between a reference image and one
+    of this library's sum to about the two renderers' own noise, measured by two
+    independent renders of each (seeds 3, 4 and 9, 10): without a bias the ratio is near
+    1 whatever each renderer's variance; a bias of a few percent in the lit blocks would
+    push it far above. It must stay below 2 (with about 50-150 lit block values the
+    ratio's spread is a few tenths)."""
     if not cpu.refgpu_available():
         pytest.fail("oracle/_ref/librefgpu.so was not built (make -C oracle ref)")
     import torch
@@ -65,11 +66,13 @@ def test_reference_gpu_render_estimates_the_same_image(cuda):
     tris, infos = cpt.scene_random(20_000, seed=5)
     w, h, bounces, spp = 64, 48, 3, 512
     cam = cpt.camera_look_at((0.5, 0.5, -1.2), (0.5, 0.5, 0.0), aspect=w / h)
-    rr = refgpu_child.run("render", tris, cpu.enclosing_box(tris), infos=infos, width=w, height=h,
-                          cam15=cam.as_array(), bounces=bounces, intensity=3.0, stratified=1, warmup=0, frames=spp,
-                          seed=3)
-    ref_img = rr["image"]
-    assert float(rr["ms_per_frame"]) > 0 and np.isfinite(ref_img).all()
+    theirs = []
+    for seed in (3, 4):
+        rr = refgpu_child.run("render", tris, cpu.enclosing_box(tris), infos=infos, width=w, height=h,
+                              cam15=cam.as_array(), bounces=bounces, intensity=3.0, stratified=1, warmup=0,
+                              frames=spp, seed=seed)
+        assert float(rr["ms_per_frame"]) > 0 and np.isfinite(rr["image"]).all()
+        theirs.append(rr["image"][..., :3].astype(np.float64))
     lb = DeviceLbvh(len(tris), 30)
     lb.build(to_device(tris), check_root=True)
     scene = DeviceScene(infos)
@@ -80,15 +83,15 @@ def test_reference_gpu_render_estimates_the_same_image(cuda):
         torch.cuda.synchronize()
         r.check_status()
         ours.append(r.resolve().cpu().numpy()[..., :3].astype(np.float64))
-    theirs = ref_img[..., :3].astype(np.float64)
     assert ours[0].mean() > 0.01
-    assert abs(theirs.mean() - ours[0].mean()) <= 0.02 * ours[0].mean(), (theirs.mean(), ours[0].mean())
+    assert abs(theirs[0].mean() - ours[0].mean()) <= 0.02 * ours[0].mean(), (theirs[0].mean(), ours[0].mean())
 
     def blocks(img):
         return img.reshape(h // 8, 8, w // 8, 8, 3).mean(axis=(1, 3))
 
-    b1, b2, bt = blocks(ours[0]), blocks(ours[1]), blocks(theirs)
-    lit = b1 > 0.05 * b1.max()
+    o1, o2, t1, t2 = (blocks(x) for x in (ours[0], ours[1], theirs[0], theirs[1]))
+    lit = o1 > 0.05 * o1.max()
     assert lit.sum() >= 40
-    ratio = ((bt - b1)[lit] ** 2).sum() / ((b2 - b1)[lit] ** 2).sum()
+    own_noise = 0.5 * (((o2 - o1)[lit] ** 2).sum() + ((t2 - t1)[lit] ** 2).sum())
+    ratio = ((t1 - o1)[lit] ** 2).sum() / own_noise
     assert ratio < 2.0, ratio

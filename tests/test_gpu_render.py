@@ -36,14 +36,14 @@ def ocam(cam, jitter=False):
 
 
 def gpu_render(tris, infos, lights, cam, mode, spp=4, frame0=5, bounces=3, seed=77, bits=30, jitter=False,
-               wave_paths=0, ref_grid=False, w=W, h=H, stratified=True, ray_sort=False):
+               wave_paths=0, ref_grid=False, w=W, h=H, stratified=True, ray_sort=False, wave_lanes=0):
     lb = DeviceLbvh(len(tris), bits)
     lb.build(to_device(tris), check_root=True)
     sc = DeviceScene(infos, lights)
     c = cpt.Camera.from_buffer_copy(cam)
     c.jitter, c.jitter_x, c.jitter_y = int(jitter), 2.0 / w, 2.0 / h
     r = DeviceRenderer(make_params(w, h, spp, frame0, bounces, 3.0, stratified, seed, mode, ref_grid, wave_paths,
-                                   ray_sort=ray_sort))
+                                   ray_sort=ray_sort, wave_lanes=wave_lanes))
     r.render(lb, sc, c)
     torch.cuda.synchronize()
     r.check_status()
@@ -119,6 +119,20 @@ def test_wave_size_does_not_change_the_image(cuda):
     assert a.accum.cpu().numpy().tobytes() == b.accum.cpu().numpy().tobytes() == c.accum.cpu().numpy().tobytes()
 
 
+@pytest.mark.parametrize("mode", [cpt.ACCUM_KAHAN, cpt.ACCUM_LERP])
+def test_wave_lanes_do_not_change_the_image(cuda, mode):
+    """Two lanes (each wave's paths in halves on two streams) against one: the same
+    accumulator bytes and ray counts, with one wave and with several."""
+    tris, infos, _, cam = scene()
+    lights = dir_lights()
+    for wave_paths in (0, 2 * W * H):
+        one, _ = gpu_render(tris, infos, lights, cam, mode, spp=6, bounces=4, wave_paths=wave_paths, wave_lanes=1)
+        two, _ = gpu_render(tris, infos, lights, cam, mode, spp=6, bounces=4, wave_paths=wave_paths, wave_lanes=2)
+        assert one.accum.cpu().numpy().tobytes() == two.accum.cpu().numpy().tobytes()
+        assert np.array_equal(one.counts.cpu().numpy()[:16], two.counts.cpu().numpy()[:16])
+        assert int(two.counts[0]) > 0
+
+
 def test_coherence_sort_does_not_change_the_image(cuda):
     tris, infos, _, cam = scene()
     lights = dir_lights()
@@ -180,6 +194,28 @@ def test_batched_scenes_in_one_call(cuda):
         s, _, n = cpu.accumulate_kahan(rad)
         assert acc[..., :3].tobytes() == s.tobytes(), i
         assert np.all(acc[..., 3] == n)
+
+
+def test_batched_scenes_with_two_lanes(cuda):
+    """Views of different scenes split between two wave lanes (the halves of the path
+    range cut through a view): every accumulator equals the one-lane call's."""
+    from cpt.device import BatchRenderer
+
+    views = []
+    for k, (n, (w, h)) in enumerate([(9000, (40, 24)), (15000, (64, 48)), (6000, (48, 40))]):
+        tris, infos = cpt.scene_random(n, seed=20 + k)
+        lb = DeviceLbvh(len(tris), 30)
+        lb.build(to_device(tris), check_root=True)
+        views.append((lb, DeviceScene(infos), cpt.camera_look_at((0.5, 0.5, -1.2), (0.5, 0.5, 0.0), aspect=w / h), w, h))
+    out = []
+    for lanes in (1, 2):
+        br = BatchRenderer(views, make_params(0, 0, 3, 1, 4, 3.0, True, 13, cpt.ACCUM_KAHAN, wave_lanes=lanes))
+        br.render()
+        torch.cuda.synchronize()
+        br.check_status()
+        out.append(([a.cpu().numpy().tobytes() for a in br.accums], br.counts.cpu().numpy()[:16].copy()))
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
 
 
 def test_directional_lights_shadow_rays(cuda):
