@@ -45,7 +45,7 @@ WORKLOADS = {
     # radiance cache on the C2 scene: 1 spp frames through the cache vs plain 16 spp, RMSE vs an FP64 image
     "c4": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=1,
                bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, plain_spp=64, ref_spp=4096,
-               ref_div=4, warm_updates=4, max_spp=256, split=8.0, wide=1, treelet=1),
+               ref_div=4, warm_updates=2, max_spp=256, split=8.0, wide=1, treelet=1),
     # deforming 16.8 M-triangle displaced sphere, full rebuild every frame, 8 cameras
     "c5": dict(kind="deform", nu=4096, nv=2048, n_hair=0, bits=63, width=1280, height=720, spp=1, bounces=7,
                eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, cameras=8, amp=0.01, omega=40.0, cache=True),
@@ -971,6 +971,8 @@ def run_ours(args, w, world, rank, local):
     if rank == 0 and world == 1 and args.workload == "c2" and not args.no_cache_ratio:
         wc = dict(WORKLOADS["c4"])
         wc.update(width=W_, height=H_)
+        if args.rc_warm is not None:
+            wc["warm_updates"] = args.rc_warm
         try:
             r4 = cache_experiment(wc, lb, scene, cams[0], dev, True, args.warmup, wc["spp"],
                                   rc_params_for(args, wc["spp"]))
@@ -1341,8 +1343,10 @@ def main():
                          "tree (default per workload)")
     ap.add_argument("--rc-per-sample", action="store_true",
                     help="c4: 2^16 training suffixes per image sample instead of per render call (frame)")
-    ap.add_argument("--rc-interval", type=int, default=8,
+    ap.add_argument("--rc-interval", type=int, default=12,
                     help="radiance cache: train on every n-th frame's own paths (the others only read the cache)")
+    ap.add_argument("--rc-warm", type=int, default=None,
+                    help="radiance cache: training-only updates before the first cached frame (default per workload)")
     ap.add_argument("--rc-train-paths", type=int, default=0,
                     help="radiance cache: training paths per training frame (0: the library default, 2^16)")
     ap.add_argument("--nee", type=int, default=1,
@@ -1363,6 +1367,8 @@ def main():
         w["width"], w["height"] = (int(x) for x in args.res.lower().split("x"))
     if args.spp:
         w["spp"] = args.spp
+    if args.rc_warm is not None and "warm_updates" in w:
+        w["warm_updates"] = args.rc_warm
     if args.sphere:
         w["nu"], w["nv"] = (int(x) for x in args.sphere.lower().split("x"))
     if args.hair is not None:
