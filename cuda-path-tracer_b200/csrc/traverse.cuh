@@ -29,7 +29,8 @@
 //
 // The second half of the file traverses the compressed 8-wide tree (cpt_lbvh_wide)
 // built over a binary tree: 80-B nodes with 8-bit child planes, the same triangle
-// test on the binary leaf slot's words, and a refill as soon as one lane is idle.
+// test on the binary leaf slot's words, triangle tests in warp batches and a refill
+// once two lanes are idle.
 #pragma once
 #include "cpt_device.cuh"
 #include "cpt.h"
