@@ -528,13 +528,15 @@ def run_batch(args, w, world, rank, local):
     br.render()
     torch.cuda.synchronize()
     prof = cpt.profile_end()
+    busy = cpt.profile_busy()
     ext_ms, ext_n = prof.get("k_extend", (0.0, 0))
+    ext_ms = busy.get("k_extend", ext_ms)  # two wave lanes overlap their launches: the time any one ran
     closest_frame = float(counts[0] + counts[1]) / args.steps
     node_b = 80.0 if args.wide else 64.0  # a wide node record, or the compact two-child node
     alg = closest_frame * (48 + node_b * mean_nodes + 48.0 * mean_tris)
     peak, peak_kind = measured_peaks()
     ach = alg / (ext_ms / 1e3) / 1e9 if ext_ms else 0.0
-    frame_ms = sum(v[0] for v in prof.values())
+    frame_ms = sum(busy.get(k, v[0]) for k, v in prof.items())
 
     # --- one CUDA graph for a whole frame: every scene's LBVH rebuilt (and the split
     # trees of the hairball scenes), then all scenes rendered; one replay per frame
@@ -608,6 +610,12 @@ def run_batch(args, w, world, rank, local):
 
     build_ms = max_over_ranks(time_builds(lambda: batch.build(keep, boxes)), world)
     per_scene_ms = max_over_ranks(time_builds(lambda: [v[0].build(d) for v, d in zip(views, keep)]), world)
+    # the frame's rebuild part by part (outside the graph): the batched LBVH build, the
+    # split trees of the hairball scenes, the wide trees
+    split_ms = max_over_ranks(time_builds(lambda: [v[0].split(split, keep_scratch=True, flags=split_flags(args))
+                                                   for v, h in zip(views, hair) if h]), world)
+    wide_ms = max_over_ranks(time_builds(lambda: [v[0].wide(keep_scratch=True) for v in views]), world) \
+        if args.wide else 0.0
     for v in views:
         v[0].status()
     n_tris = int(sum_over_ranks(float(n_tris), world))
@@ -629,9 +637,13 @@ def run_batch(args, w, world, rank, local):
                 "roofline": {"bound": "hbm", "kernel": "k_extend", "achieved": round(ach, 1), "peak": peak,
                              "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
                              "bytes_per_ray": f"48 + {node_b:.0f} x {mean_nodes:.2f} nodes + 48 x {mean_tris:.2f} triangles",
-                             "kernel_share": {k: round(v[0] / frame_ms, 4) for k, v in sorted(prof.items())}},
+                             "busy_ms": round(ext_ms, 3),
+                             "kernel_share": {k: round(busy.get(k, v[0]) / frame_ms, 4)
+                                              for k, v in sorted(prof.items())}},
                 "lbvh": {"mtris_s": round(n_tris / build_ms / 1e3, 2), "ms": round(build_ms, 3),
                          "per_scene_calls_ms": round(per_scene_ms, 3),
+                         "frame_rebuild_parts_ms": {"lbvh_batch": round(build_ms, 3), "split_trees": round(split_ms, 3),
+                                                    "wide_trees": round(wide_ms, 3)},
                          "per_scene_calls_mtris_s": round(n_tris / per_scene_ms / 1e3, 2),
                          "note": "each rank's scenes in one batched build (cpt_lbvh_build_batch; max over ranks); "
                                  "per_scene_calls = the same scenes built by one cpt_lbvh_build call each"},

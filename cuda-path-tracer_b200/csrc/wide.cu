@@ -36,6 +36,7 @@
 #include "cpt_internal.h"
 #include "lbvh_common.cuh"
 #include "traverse.cuh"
+#include <cooperative_groups.h>
 
 namespace cpt {
 namespace {
@@ -144,21 +145,21 @@ __device__ __forceinline__ int scale_exp(double ext)
     return max(-126, min(127, e));
 }
 
-__global__ void __launch_bounds__(kWideBlock) k_wide_level(const float4* __restrict__ bin, float4* __restrict__ wide,
-                                                           float4* __restrict__ tris, float4* __restrict__ queue,
-                                                           uint32_t* __restrict__ ctr, int level, uint32_t node_cap,
-                                                           uint32_t tri_cap, uint32_t bin_internal,
-                                                           uint32_t* __restrict__ status)
+// The wide nodes [start, end) of one level: each collapses its binary subtree into up
+// to 8 children, allocates its internal children (queued as the next level) and its
+// leaf records.
+__device__ __forceinline__ void wide_level_nodes(const float4* __restrict__ bin, float4* __restrict__ wide,
+                                                 float4* __restrict__ tris, float4* __restrict__ queue,
+                                                 uint32_t* __restrict__ ctr, uint32_t start, uint32_t end, float m,
+                                                 uint32_t node_cap, uint32_t tri_cap, uint32_t bin_internal,
+                                                 uint32_t* __restrict__ status, float (*s_box)[kWideBlock],
+                                                 uint32_t (*s_ref)[kWideBlock])
 {
-    __shared__ float s_box[8 * 6][kWideBlock];
-    __shared__ uint32_t s_ref[8][kWideBlock];
-    // A sort of the build (or of the split tree) gave up a look-back wait: the binary
-    // tree is not one. Every block leaves (the word was set before this launch), so
-    // the level counters keep their initial values and no node is written.
-    if (__ldcg(status) & CPT_STATUS_TIMEOUT) return;
-    const uint32_t start = ctr[4 + level], end = ctr[4 + level + 1];
-    const float m = __uint_as_float(ctr[3]);
     const int t = threadIdx.x;
+    if (end > node_cap) {  // (only when the binary tree was not one: allocations past the cap were refused)
+        if (blockIdx.x == 0 && t == 0) atomicOr(status, CPT_STATUS_BAD_INDEX);
+        end = node_cap;
+    }
     for (uint32_t wi = start + blockIdx.x * kWideBlock + t; wi < end; wi += gridDim.x * kWideBlock) {
         const float4 q0 = queue[2 * (size_t)wi], q1 = queue[2 * (size_t)wi + 1];
         const uint32_t b = __float_as_uint(q0.w);
@@ -297,16 +298,44 @@ __global__ void __launch_bounds__(kWideBlock) k_wide_level(const float4* __restr
         o[4] = make_float4(__uint_as_float(qhi[1][0]), __uint_as_float(qhi[1][1]), __uint_as_float(qhi[2][0]),
                            __uint_as_float(qhi[2][1]));
     }
-    // the last block of the level closes it: the next level is what this one allocated
-    __syncthreads();
-    if (t == 0) {
-        __threadfence();
-        const uint32_t done = atomicAdd(&ctr[2], 1u);
-        if (done == gridDim.x - 1) {
-            __threadfence();
-            ctr[4 + level + 2] = atomicAdd(&ctr[0], 0u);
-            ctr[2] = 0;
-        }
+}
+
+// Every level in one cooperative launch: the blocks process a level's nodes and meet
+// at a grid barrier (cooperative launch: all blocks are resident); the next level is
+// what this one allocated, read by every thread between that barrier and a second one
+// (so that no block allocates for the next level before every thread has read the
+// same bound, and every block takes the same number of barriers). The walk stops at
+// the first empty level, so a small tree costs its height in barriers, not kWideLevels
+// launches. The last level bounds are left in ctr for k_wide_check (nodes still
+// queued after kWideLevels levels: the tree was too tall).
+__global__ void __launch_bounds__(kWideBlock) k_wide_levels(const float4* __restrict__ bin, float4* __restrict__ wide,
+                                                            float4* __restrict__ tris, float4* __restrict__ queue,
+                                                            uint32_t* __restrict__ ctr, uint32_t node_cap,
+                                                            uint32_t tri_cap, uint32_t bin_internal,
+                                                            uint32_t* __restrict__ status)
+{
+    __shared__ float s_box[8 * 6][kWideBlock];
+    __shared__ uint32_t s_ref[8][kWideBlock];
+    // A sort of the build (or of the split tree) gave up a look-back wait: the binary
+    // tree is not one. Every block leaves at once (the word was set before this launch,
+    // so all see it and none waits at the barrier), and no node is written.
+    if (__ldcg(status) & CPT_STATUS_TIMEOUT) return;
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    const float m = __uint_as_float(__ldcg(&ctr[3]));
+    uint32_t start = 0, end = 1;  // level 0: the root, queued by k_wide_init
+    int level = 0;
+    for (; level < kWideLevels && start < end; ++level) {
+        wide_level_nodes(bin, wide, tris, queue, ctr, start, end, m, node_cap, tri_cap, bin_internal, status, s_box,
+                         s_ref);
+        grid.sync();
+        const uint32_t next = __ldcg(&ctr[0]);  // every node allocated so far: final after the barrier
+        grid.sync();
+        start = end;
+        end = next;
+    }
+    if (grid.thread_rank() == 0) {
+        ctr[4 + kWideLevels] = start;
+        ctr[4 + kWideLevels + 1] = end;
     }
 }
 
@@ -354,13 +383,32 @@ extern "C" int cpt_lbvh_wide(cpt_bvh* bvh, void* nodes, size_t node_bytes, void*
     const float4* bin = static_cast<const float4*>(split ? bvh->split_nodes : bvh->nodes);
     k_wide_init<<<1, 32, 0, stream>>>(bin, ws.queue, ws.ctr);
     CPT_LAUNCH_CHECK();
-    const int blocks = sm_count() * 8;
-    for (int l = 0; l < kWideLevels; ++l) {
-        k_wide_level<<<blocks, kWideBlock, 0, stream>>>(bin, static_cast<float4*>(nodes), static_cast<float4*>(tris),
-                                                        ws.queue, ws.ctr, l, leaves - 1, leaves, leaves - 1,
-                                                        bvh->status);
-        CPT_LAUNCH_CHECK();
+    // one cooperative launch over every level: as many blocks as the largest level can
+    // use, no more than can be resident at once
+    static int occ[64] = {0};
+    int dev = 0;
+    CPT_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return CPT_ERR_INVALID_ARGUMENT;
+    if (!occ[dev]) {
+        int o = 0;
+        CPT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_wide_levels, kWideBlock, 0));
+        occ[dev] = std::max(1, o);
     }
+    const uint64_t widest = std::min<uint64_t>((uint64_t)leaves - 1, (uint64_t)sm_count() * occ[dev] * kWideBlock);
+    const int blocks = (int)std::max<uint64_t>(1, (widest + kWideBlock - 1) / kWideBlock);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(kWideBlock);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;  // (also as a node of a captured graph)
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CPT_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_wide_levels, bin, static_cast<float4*>(nodes), static_cast<float4*>(tris),
+                                    ws.queue, ws.ctr, leaves - 1, leaves, leaves - 1, bvh->status));
+    note_launch();
     k_wide_check<<<1, 32, 0, stream>>>(ws.ctr, bvh->status, bvh->status + 2);
     CPT_LAUNCH_CHECK();
     bvh->wide_nodes = nodes;
