@@ -4,7 +4,8 @@
 // in which exactly equal distances are found: every triangle keeps its arithmetic
 // (the leaf record holds the binary leaf slot's words), only the culling boxes change.
 //
-// Collapse: top-down, one launch per level of the wide tree. A wide node starts from
+// Collapse: top-down, level by level of the wide tree inside one cooperative launch
+// (k_wide_levels). A wide node starts from
 // its binary node's two children and repeatedly opens the internal child of largest
 // surface area until it has 8 children or only leaves. Its children go to slots by
 // direction (Ylitie, Karras, Laine, "Efficient Incoherent Ray Traversal on GPUs
