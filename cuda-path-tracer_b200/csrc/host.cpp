@@ -460,13 +460,11 @@ extern "C" void cpt_camera_look_at(const float eye[3], const float target[3], co
 // ---------------------------------------------------------------------------
 // cpt_tracer: CUDAPathTracer + Scene with caller-free memory management.
 // ---------------------------------------------------------------------------
-struct cpt_tracer {
-    int bits = 63;
-    cudaStream_t stream = nullptr;
-    cudaStream_t copy_stream = nullptr;  // shading-record uploads, overlapped with the builds
-    cudaEvent_t ev_upload = nullptr, ev_copied = nullptr;
-    int device = 0;
-    // scene
+// One uploaded scene with its trees: the triangles, shading records and lights, the
+// LBVH and its build scratch, the optional split and wide trees, the emitter table.
+// The tracer keeps two: an upload fills the one the current frames do not read, so
+// its copies and builds overlap the frames still rendering the other.
+struct TracerScene {
     uint32_t n = 0, info_count = 0, light_count = 0;
     void* d_tris = nullptr;
     size_t tris_cap = 0;
@@ -482,23 +480,39 @@ struct cpt_tracer {
     size_t split_nodes_cap = 0;
     void* d_split_scratch = nullptr;
     size_t split_scratch_cap = 0;
-    float split_ratio = 0.f;  // 0: traverse the LBVH itself
-    uint32_t split_flags = 0;
-    void* d_textures = nullptr;  // cudaTextureObject_t handles (the caller owns the textures)
-    size_t textures_cap = 0;
-    uint32_t texture_count = 0;
     void* d_wide_nodes = nullptr;  // compressed wide tree (cpt_tracer_set_wide)
     size_t wide_nodes_cap = 0;
     void* d_wide_tris = nullptr;
     size_t wide_tris_cap = 0;
     void* d_wide_scratch = nullptr;
     size_t wide_scratch_cap = 0;
-    bool wide = false;
     void* d_emitters = nullptr;  // emitter table (cpt_tracer_set_nee)
     size_t emitters_cap = 0;
-    bool nee = false, emitters_ready = false;
+    bool emitters_ready = false;
     cpt_bvh bvh{};
     bool ready = false;
+    // built: the trees are complete (build stream); copied: the shading records and
+    // lights have landed (copy stream); released: the last frame that read this scene
+    // has finished (render stream), so an upload may overwrite it
+    cudaEvent_t ev_built = nullptr, ev_copied = nullptr, ev_released = nullptr;
+};
+
+struct cpt_tracer {
+    int bits = 63;
+    cudaStream_t stream = nullptr;        // frames (render, resolve, read-back)
+    cudaStream_t build_stream = nullptr;  // triangle uploads and tree builds
+    cudaStream_t copy_stream = nullptr;   // shading-record uploads, overlapped with the builds
+    int device = 0;
+    TracerScene scene[2];
+    int front = -1;     // the scene frames render (-1: none uploaded)
+    int rendered = -1;  // the scene of the last frame (its status word is the frame's)
+    float split_ratio = 0.f;  // 0: traverse the LBVH itself
+    uint32_t split_flags = 0;
+    bool wide = false;
+    bool nee = false;
+    void* d_textures = nullptr;  // cudaTextureObject_t handles (the caller owns the textures)
+    size_t textures_cap = 0;
+    uint32_t texture_count = 0;
     // frame
     uint32_t width = 0, height = 0;
     void* d_accum = nullptr;
@@ -534,11 +548,20 @@ extern "C" int cpt_tracer_create(cpt_tracer** out, int morton_bits)
     if (!t) return CPT_ERR_CUDA;
     t->bits = morton_bits;
     cudaGetDevice(&t->device);
-    if (cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&t->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&t->ev_upload, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&t->ev_copied, cudaEventDisableTiming) != cudaSuccess ||
-        cudaMalloc(reinterpret_cast<void**>(&t->d_counts), CPT_RAY_COUNTS * sizeof(unsigned long long)) != cudaSuccess) {
+    // the build stream at the highest priority: its blocks take the SMs that a frame's
+    // launches leave idle (each traversal launch ends on a few long rays) first
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    bool ok = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithPriority(&t->build_stream, cudaStreamNonBlocking, greatest) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&t->copy_stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaMalloc(reinterpret_cast<void**>(&t->d_counts), CPT_RAY_COUNTS * sizeof(unsigned long long)) ==
+                  cudaSuccess;
+    for (TracerScene& sc : t->scene)
+        ok = ok && cudaEventCreateWithFlags(&sc.ev_built, cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&sc.ev_copied, cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&sc.ev_released, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
         cpt_tracer_destroy(t);
         return CPT_ERR_CUDA;
     }
@@ -550,18 +573,22 @@ extern "C" int cpt_tracer_create(cpt_tracer** out, int morton_bits)
 extern "C" void cpt_tracer_destroy(cpt_tracer* t)
 {
     if (!t) return;
-    // both streams may still use the buffers (the copy stream uploads shading records)
-    if (t->stream) cudaStreamSynchronize(t->stream);
-    if (t->copy_stream) cudaStreamSynchronize(t->copy_stream);
-    void* bufs[] = {t->d_tris, t->d_bvh, t->d_build_scratch, t->d_infos, t->d_lights, t->d_textures, t->d_accum,
-                    t->d_render_scratch, t->d_image, t->d_counts, t->d_split_nodes, t->d_split_scratch,
-                    t->d_emitters, t->d_wide_nodes, t->d_wide_tris, t->d_wide_scratch};
+    // every stream may still use the buffers (uploads, builds, frames)
+    for (cudaStream_t st : {t->stream, t->build_stream, t->copy_stream})
+        if (st) cudaStreamSynchronize(st);
+    for (TracerScene& sc : t->scene) {
+        void* bufs[] = {sc.d_tris, sc.d_bvh, sc.d_build_scratch, sc.d_infos, sc.d_lights, sc.d_split_nodes,
+                        sc.d_split_scratch, sc.d_emitters, sc.d_wide_nodes, sc.d_wide_tris, sc.d_wide_scratch};
+        for (void* b : bufs)
+            if (b) cudaFree(b);
+        for (cudaEvent_t e : {sc.ev_built, sc.ev_copied, sc.ev_released})
+            if (e) cudaEventDestroy(e);
+    }
+    void* bufs[] = {t->d_textures, t->d_accum, t->d_render_scratch, t->d_image, t->d_counts};
     for (void* b : bufs)
         if (b) cudaFree(b);
-    if (t->ev_upload) cudaEventDestroy(t->ev_upload);
-    if (t->ev_copied) cudaEventDestroy(t->ev_copied);
-    if (t->copy_stream) cudaStreamDestroy(t->copy_stream);
-    if (t->stream) cudaStreamDestroy(t->stream);
+    for (cudaStream_t st : {t->copy_stream, t->build_stream, t->stream})
+        if (st) cudaStreamDestroy(st);
     delete t;
 }
 
@@ -572,60 +599,66 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
     CPT_RANGE("cpt_tracer_upload");
     if (!t || !tris || !infos || n < 2 || n > kMaxTriangles || info_count == 0 || (light_count && !lights))
         return CPT_ERR_INVALID_ARGUMENT;
+    // The scene the frames do not read; its buffers are reused once the last frame that
+    // read it has finished (the build and copy streams wait for that, the host does not).
+    const int b = t->front < 0 ? 0 : 1 - t->front;
+    TracerScene& S = t->scene[b];
+    S.ready = false;  // until this upload has queued its builds
+    t->front = -1;    // the upload replaces the scene: until it succeeds there is none to render
     int rc;
-    t->ready = false;  // until this upload has completed its builds
-    if ((rc = ensure(&t->d_tris, &t->tris_cap, sizeof(cpt_triangle) * (size_t)n))) return rc;
+    if ((rc = ensure(&S.d_tris, &S.tris_cap, sizeof(cpt_triangle) * (size_t)n))) return rc;
     const size_t bvh_bytes = cpt_bvh_bytes(n, t->bits), scr = cpt_lbvh_scratch_bytes(n, t->bits);
-    if ((rc = ensure(&t->d_bvh, &t->bvh_cap, bvh_bytes))) return rc;
-    if ((rc = ensure(&t->d_build_scratch, &t->build_cap, scr))) return rc;
-    if ((rc = ensure(&t->d_infos, &t->infos_cap, sizeof(cpt_triangle_info) * (size_t)info_count))) return rc;
-    if (light_count && (rc = ensure(&t->d_lights, &t->lights_cap, sizeof(cpt_dir_light) * (size_t)light_count))) return rc;
-    if ((rc = cpt_bvh_bind(t->d_bvh, t->bvh_cap, n, t->bits, &t->bvh))) return rc;
-    // The triangles go first on the tracer's stream (the builds read them); the shading
-    // records and lights, which only the renderer reads, go on a second stream that
-    // starts after everything already queued on the tracer's stream (an earlier frame
-    // may still read them) and overlaps the builds; the next render waits for them.
-    CPT_CUDA_TRY(cudaEventRecord(t->ev_upload, t->stream));
-    CPT_CUDA_TRY(cudaStreamWaitEvent(t->copy_stream, t->ev_upload, 0));
-    CPT_CUDA_TRY(cudaMemcpyAsync(t->d_tris, tris, sizeof(cpt_triangle) * (size_t)n, cudaMemcpyHostToDevice, t->stream));
-    CPT_CUDA_TRY(cudaMemcpyAsync(t->d_infos, infos, sizeof(cpt_triangle_info) * (size_t)info_count, cudaMemcpyHostToDevice,
-                                 t->copy_stream));
+    if ((rc = ensure(&S.d_bvh, &S.bvh_cap, bvh_bytes))) return rc;
+    if ((rc = ensure(&S.d_build_scratch, &S.build_cap, scr))) return rc;
+    if ((rc = ensure(&S.d_infos, &S.infos_cap, sizeof(cpt_triangle_info) * (size_t)info_count))) return rc;
+    if (light_count && (rc = ensure(&S.d_lights, &S.lights_cap, sizeof(cpt_dir_light) * (size_t)light_count))) return rc;
+    CPT_CUDA_TRY(cudaStreamWaitEvent(t->build_stream, S.ev_released, 0));
+    CPT_CUDA_TRY(cudaStreamWaitEvent(t->copy_stream, S.ev_released, 0));
+    if ((rc = cpt_bvh_bind(S.d_bvh, S.bvh_cap, n, t->bits, &S.bvh))) return rc;
+    // The triangles go first on the build stream (the builds read them); the shading
+    // records and lights, which only the renderer reads, go on the copy stream and
+    // overlap the builds; the next frame's first shading launch waits for them.
+    CPT_CUDA_TRY(cudaMemcpyAsync(S.d_tris, tris, sizeof(cpt_triangle) * (size_t)n, cudaMemcpyHostToDevice,
+                                 t->build_stream));
+    CPT_CUDA_TRY(cudaMemcpyAsync(S.d_infos, infos, sizeof(cpt_triangle_info) * (size_t)info_count,
+                                 cudaMemcpyHostToDevice, t->copy_stream));
     if (light_count)
-        CPT_CUDA_TRY(cudaMemcpyAsync(t->d_lights, lights, sizeof(cpt_dir_light) * (size_t)light_count,
+        CPT_CUDA_TRY(cudaMemcpyAsync(S.d_lights, lights, sizeof(cpt_dir_light) * (size_t)light_count,
                                      cudaMemcpyHostToDevice, t->copy_stream));
-    CPT_CUDA_TRY(cudaEventRecord(t->ev_copied, t->copy_stream));
-    rc = cpt_lbvh_build(static_cast<const cpt_triangle*>(t->d_tris), n, enclosing_box, t->bits, &t->bvh,
-                        t->d_build_scratch, t->build_cap, 0, t->stream);
+    CPT_CUDA_TRY(cudaEventRecord(S.ev_copied, t->copy_stream));
+    rc = cpt_lbvh_build(static_cast<const cpt_triangle*>(S.d_tris), n, enclosing_box, t->bits, &S.bvh,
+                        S.d_build_scratch, S.build_cap, 0, t->build_stream);
     if (rc) return rc;
     if (t->split_ratio > 0.f) {
         size_t nb = 0;
         const size_t sb = cpt_lbvh_split_bytes(n, t->bits, t->split_ratio, t->split_flags, &nb);
         if (!sb) return CPT_ERR_INVALID_ARGUMENT;
-        if ((rc = ensure(&t->d_split_nodes, &t->split_nodes_cap, nb))) return rc;
-        if ((rc = ensure(&t->d_split_scratch, &t->split_scratch_cap, sb))) return rc;
-        rc = cpt_lbvh_split(&t->bvh, t->split_ratio, t->split_flags, t->d_split_nodes, t->split_nodes_cap,
-                            t->d_split_scratch,
-                            t->split_scratch_cap, t->stream);
+        if ((rc = ensure(&S.d_split_nodes, &S.split_nodes_cap, nb))) return rc;
+        if ((rc = ensure(&S.d_split_scratch, &S.split_scratch_cap, sb))) return rc;
+        rc = cpt_lbvh_split(&S.bvh, t->split_ratio, t->split_flags, S.d_split_nodes, S.split_nodes_cap,
+                            S.d_split_scratch, S.split_scratch_cap, t->build_stream);
         if (rc) return rc;
     }
     if (t->wide) {
-        const uint32_t leaves = t->bvh.split_nodes ? t->bvh.split_capacity : n;
+        const uint32_t leaves = S.bvh.split_nodes ? S.bvh.split_capacity : n;
         size_t nb = 0, tb = 0;
         const size_t sb = cpt_lbvh_wide_bytes(leaves, &nb, &tb);
         if (!sb) return CPT_ERR_INVALID_ARGUMENT;
-        if ((rc = ensure(&t->d_wide_nodes, &t->wide_nodes_cap, nb))) return rc;
-        if ((rc = ensure(&t->d_wide_tris, &t->wide_tris_cap, tb))) return rc;
-        if ((rc = ensure(&t->d_wide_scratch, &t->wide_scratch_cap, sb))) return rc;
-        rc = cpt_lbvh_wide(&t->bvh, t->d_wide_nodes, t->wide_nodes_cap, t->d_wide_tris, t->wide_tris_cap,
-                           t->d_wide_scratch, t->wide_scratch_cap, t->stream);
+        if ((rc = ensure(&S.d_wide_nodes, &S.wide_nodes_cap, nb))) return rc;
+        if ((rc = ensure(&S.d_wide_tris, &S.wide_tris_cap, tb))) return rc;
+        if ((rc = ensure(&S.d_wide_scratch, &S.wide_scratch_cap, sb))) return rc;
+        rc = cpt_lbvh_wide(&S.bvh, S.d_wide_nodes, S.wide_nodes_cap, S.d_wide_tris, S.wide_tris_cap, S.d_wide_scratch,
+                           S.wide_scratch_cap, t->build_stream);
         if (rc) return rc;
     }
-    t->n = n;
-    t->info_count = info_count;
-    t->light_count = light_count;
+    CPT_CUDA_TRY(cudaEventRecord(S.ev_built, t->build_stream));
+    S.n = n;
+    S.info_count = info_count;
+    S.light_count = light_count;
+    S.ready = true;
+    S.emitters_ready = false;
+    t->front = b;
     t->frame = 0;  // CUDAPathTracer::upload resets the frame counter (cuda_path_tracer.cu:469)
-    t->ready = true;
-    t->emitters_ready = false;
     CPT_CUDA_TRY(cudaMemsetAsync(t->d_counts, 0, CPT_RAY_COUNTS * sizeof(unsigned long long), t->stream));
     return CPT_OK;
 }
@@ -655,16 +688,16 @@ extern "C" int cpt_tracer_set_nee(cpt_tracer* t, uint32_t on)
 }
 
 // The emitter table of the uploaded scene, sized by a first count (synchronizes once per upload).
-static int tracer_emitters(cpt_tracer* t, const cpt_scene& sc)
+static int tracer_emitters(cpt_tracer* t, TracerScene& S, const cpt_scene& sc)
 {
-    if (t->emitters_ready) return CPT_OK;
+    if (S.emitters_ready) return CPT_OK;
     uint32_t cap = 1024, found = 0;
     for (int pass = 0; pass < 2; ++pass) {
-        int rc = ensure(&t->d_emitters, &t->emitters_cap, cpt_emitters_bytes(t->n, cap));
+        int rc = ensure(&S.d_emitters, &S.emitters_cap, cpt_emitters_bytes(S.n, cap));
         if (rc) return rc;
-        rc = cpt_emitters_build(&t->bvh, &sc, cap, t->d_emitters, t->emitters_cap, &found, t->stream);
+        rc = cpt_emitters_build(&S.bvh, &sc, cap, S.d_emitters, S.emitters_cap, &found, t->stream);
         if (rc == CPT_OK) {
-            t->emitters_ready = true;
+            S.emitters_ready = true;
             return CPT_OK;
         }
         if (rc != CPT_ERR_SCRATCH_TOO_SMALL) return rc;
@@ -727,7 +760,9 @@ extern "C" int cpt_tracer_set_settings(cpt_tracer* t, uint32_t bounces, float in
 extern "C" int cpt_tracer_raytrace(cpt_tracer* t, uint32_t width, uint32_t height, uint32_t spp)
 {
     CPT_RANGE("cpt_tracer_raytrace");
-    if (!t || !t->ready || width == 0 || height == 0 || spp == 0) return CPT_ERR_INVALID_ARGUMENT;
+    if (!t || t->front < 0 || !t->scene[t->front].ready || width == 0 || height == 0 || spp == 0)
+        return CPT_ERR_INVALID_ARGUMENT;
+    TracerScene& S = t->scene[t->front];
     cpt_render_params p{};
     p.width = width;
     p.height = height;
@@ -754,19 +789,20 @@ extern "C" int cpt_tracer_raytrace(cpt_tracer* t, uint32_t width, uint32_t heigh
     t->width = width;
     t->height = height;
     if (t->frame == 0) CPT_CUDA_TRY(cudaMemsetAsync(t->d_accum, 0, ab, t->stream));
-    cpt_scene sc{static_cast<const cpt_triangle_info*>(t->d_infos), t->info_count,
-                 static_cast<const cpt_dir_light*>(t->d_lights), t->light_count,
+    CPT_CUDA_TRY(cudaStreamWaitEvent(t->stream, S.ev_built, 0));  // the scene's trees
+    cpt_scene sc{static_cast<const cpt_triangle_info*>(S.d_infos), S.info_count,
+                 static_cast<const cpt_dir_light*>(S.d_lights), S.light_count,
                  t->texture_count ? static_cast<const cudaTextureObject_t*>(t->d_textures) : nullptr, t->texture_count,
                  nullptr};
     if (t->nee) {
-        CPT_CUDA_TRY(cudaStreamWaitEvent(t->stream, t->ev_copied, 0));  // the table reads the shading records
-        if ((rc = tracer_emitters(t, sc))) return rc;
-        sc.emitters = t->d_emitters;
+        CPT_CUDA_TRY(cudaStreamWaitEvent(t->stream, S.ev_copied, 0));  // the table reads the shading records
+        if ((rc = tracer_emitters(t, S, sc))) return rc;
+        sc.emitters = S.d_emitters;
     }
     // the shading records of the last upload may still be copying: the frame's first
     // shading launch waits for them, the primary traversal does not
     cpt_view view{};
-    view.bvh = &t->bvh;
+    view.bvh = &S.bvh;
     view.scene = &sc;
     view.camera = t->cam;
     view.width = width;
@@ -774,10 +810,12 @@ extern "C" int cpt_tracer_raytrace(cpt_tracer* t, uint32_t width, uint32_t heigh
     view.accum = t->d_accum;
     RenderHook hook{};
     hook.image_pass = true;
-    hook.shade_after = t->ev_copied;
-    rc = cpt_render_views_hooked(&view, 1, &p, t->d_render_scratch, t->render_cap, t->d_counts, t->bvh.status, &hook,
+    hook.shade_after = S.ev_copied;
+    rc = cpt_render_views_hooked(&view, 1, &p, t->d_render_scratch, t->render_cap, t->d_counts, S.bvh.status, &hook,
                                  t->stream);
     if (rc) return rc;
+    CPT_CUDA_TRY(cudaEventRecord(S.ev_released, t->stream));  // the next upload into this scene waits for it
+    t->rendered = t->front;
     t->frame += spp;
     return CPT_OK;
 }
@@ -799,7 +837,8 @@ extern "C" int cpt_tracer_read_image(cpt_tracer* t, float* rgba_host)
     if ((rc = cpt_resolve(t->d_accum, t->width, t->height, t->accum_mode, t->d_image, t->stream))) return rc;
     CPT_CUDA_TRY(cudaMemcpyAsync(rgba_host, t->d_image, bytes, cudaMemcpyDeviceToHost, t->stream));
     CPT_CUDA_TRY(cudaStreamSynchronize(t->stream));
-    return cpt_status_check(t->bvh.status, t->stream);
+    // the status word of the scene the image was rendered from
+    return t->rendered < 0 ? CPT_OK : cpt_status_check(t->scene[t->rendered].bvh.status, t->stream);
 }
 
 extern "C" int cpt_tracer_resolve(cpt_tracer* t, float* rgba_dev)
@@ -853,4 +892,7 @@ extern "C" int cpt_tracer_ray_counts(cpt_tracer* t, unsigned long long out[3])
 }
 
 extern "C" cudaStream_t cpt_tracer_stream(cpt_tracer* t) { return t ? t->stream : nullptr; }
-extern "C" const cpt_bvh* cpt_tracer_bvh(const cpt_tracer* t) { return t ? &t->bvh : nullptr; }
+extern "C" const cpt_bvh* cpt_tracer_bvh(const cpt_tracer* t)
+{
+    return t && t->front >= 0 ? &t->scene[t->front].bvh : nullptr;
+}

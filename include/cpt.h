@@ -369,13 +369,20 @@ int cpt_bvh_heatmap(const cpt_bvh* bvh, const cpt_camera* camera, uint32_t width
  * per GPU, as the reference's single-device application has one).
  * Host buffers: cpt_tracer_upload copies asynchronously. Pageable host memory may be
  * reused when the call returns. Page-locked (pinned) memory — which lets the copies
- * overlap the builds — must stay unchanged until the copies have run: until the next
- * cpt_tracer_read_image or cpt_tracer_ray_counts returns after a cpt_tracer_raytrace. */
+ * overlap the builds and earlier frames — must stay unchanged until the copies have run:
+ * until cpt_tracer_read_image or cpt_tracer_ray_counts returns after a
+ * cpt_tracer_raytrace of that scene. */
 typedef struct cpt_tracer cpt_tracer;
 int cpt_tracer_create(cpt_tracer** out, int morton_bits);
 void cpt_tracer_destroy(cpt_tracer* t);
 /* CUDAPathTracer::upload + Scene::upload (cuda_path_tracer.cu:466-470, Scene.cu:28-55):
- * host triangles / infos / lights, host enclosing box (NULL: computed). */
+ * host triangles / infos / lights, host enclosing box (NULL: computed).
+ * The tracer keeps two scenes: an upload fills the one the queued frames do not read
+ * (waiting on the device, not the host, for the last frame that read it), on streams of
+ * its own, and the next raytrace renders it; so an upload issued while a frame is still
+ * in flight (before its read-back) copies and builds beside that frame. The second
+ * scene's memory is allocated at the second upload. A failed upload leaves no scene to
+ * render. */
 int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32_t n, const cpt_triangle_info* infos,
                       uint32_t info_count, const cpt_dir_light* lights, uint32_t light_count,
                       const float* enclosing_box);

@@ -286,6 +286,40 @@ def test_tracer_object_host_buffers(cuda):
     t.close()
 
 
+def test_tracer_uploads_overlap_frames(cuda):
+    """The tracer keeps two scenes: an upload issued while the previous scene's frame is
+    still in flight (before its read-back) builds into the other scene, and every image
+    equals the image of a tracer given that scene alone."""
+    (ta, ia, _, cam), (tb, ib) = scene(n=8000), cpt.scene_random(6000, seed=17)
+
+    def alone(tris, infos):
+        t = cpt.Tracer(63)
+        t.set_camera(cam)
+        t.set_settings(bounces=2, intensity=3.0, stratified=True, seed=5)
+        t.upload(tris, infos)
+        t.raytrace(W, H, 2)
+        img = t.read_image(W, H)
+        t.close()
+        return img
+
+    want = [alone(ta, ia), alone(tb, ib)]
+    t = cpt.Tracer(63)
+    t.set_camera(cam)
+    t.set_settings(bounces=2, intensity=3.0, stratified=True, seed=5)
+    order = [0, 1, 0, 1, 1]
+    t.upload(*((ta, ia), (tb, ib))[order[0]])
+    t.raytrace(W, H, 2)
+    for i, k in enumerate(order):
+        if i + 1 < len(order):
+            t.upload(*((ta, ia), (tb, ib))[order[i + 1]])  # before this frame's read-back
+        img = t.read_image(W, H)
+        assert img.tobytes() == want[k].tobytes(), (i, k)
+        if i + 1 < len(order):
+            t.raytrace(W, H, 2)
+    assert t.bvh().n == len(tb)
+    t.close()
+
+
 def test_graph_replay_advances_the_sample_stream(cuda):
     """One render call captured in a CUDA graph, replayed twice, equals two direct
     calls with frame0 = 0 and spp (the device frame counter advances per replay)."""
