@@ -32,6 +32,7 @@
 // test on the binary leaf slot's words, triangle tests in warp batches and a refill
 // once two lanes are idle.
 #pragma once
+#include <cuda_fp16.h>
 #include "cpt_device.cuh"
 #include "cpt.h"
 
@@ -85,16 +86,12 @@ __device__ __forceinline__ float slab_test_fma(f3 odinv, f3 dinv, float ax, floa
 // Packed FP32 pairs (sm_100: add / sub / mul / fma .rn.f32x2). Each lane of the pair
 // is rounded exactly as the scalar round-to-nearest operation on it, so a packed
 // sequence gives the bits of the scalar one; it issues one instruction per pair.
-// CPT_PACKED_BOX (on): the packed plane evaluation of the wide tree's box test — one
-// packed fused multiply-add gives an axis's near and far plane — which only steers
-// pruning: C2 495.2 against 474.0 Mrays/s. The triangle test stays scalar: a packed
-// Moller-Trumbore (the two cross products and the dot products that share a factor in
-// pairs) gave a quarter of its cross-product lanes 1 ulp off the scalar sequence on the
-// device (a packed multiply and subtract contracted into one fused operation), and
-// exact hits are required here.
-#ifndef CPT_PACKED_BOX
-#define CPT_PACKED_BOX 1
-#endif
+// The wide tree's box test evaluates an axis's near and far plane with one packed
+// fused multiply-add. The triangle test stays scalar: a packed Moller-Trumbore (the two
+// cross products and the dot products that share a factor in pairs) gave a quarter of
+// its cross-product lanes 1 ulp off the scalar sequence on the device (a packed
+// multiply and subtract contracted into one fused operation), and exact hits are
+// required here.
 struct f2 { float x, y; };
 __device__ __forceinline__ f2 mk2(float x, float y) { f2 r; r.x = x; r.y = y; return r; }
 #define CPT_F2_OP(name, op)                                                                                    \
@@ -122,6 +119,15 @@ __device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
 // Möller-Trumbore on a slot (v0 = s[0..2], e1 = s[4..6], e2 = s[7..9]), without
 // early exits: every lane of a warp runs the same instructions, and u, v, t are the
 // values the reference computes; only the final predicate decides the hit.
+// the two halves of w as floats (exact)
+__device__ __forceinline__ f2 half_pair(uint32_t w)
+{
+    __half2 h;
+    memcpy(&h, &w, 4);
+    const float2 f = __half22float2(h);
+    return mk2(f.x, f.y);
+}
+
 __device__ __forceinline__ float tri_test(f3 o, f3 d, const float* s, float& u, float& v)
 {
     const f3 p0 = mk3(s[0], s[1], s[2]), e1 = mk3(s[4], s[5], s[6]), e2 = mk3(s[7], s[8], s[9]);
@@ -293,10 +299,13 @@ __device__ __forceinline__ Hit traverse(const float4* __restrict__ nodes, f3 o, 
 }
 
 // ---------------------------------------------------------------------------
-// Compressed 8-wide BVH (cpt_lbvh_wide). A wide node is five float4: origin p and
-// per-axis exponents e (child box planes p + q * 2^e, q one byte), the masks of its
-// internal and leaf slots, the index of its first internal child and of its first
-// triangle record, and the 48 quantized planes. The ray carries a node group — the
+// Compressed 8-wide BVH (cpt_lbvh_wide). A wide node is five float4 (child box planes
+// p + q * 2^e, q one byte):
+//   n0 = (p.x, p.y, p.z, bits of 2^e_z >> 16 | internal slot mask << 24)
+//   n1 = (first internal child, first triangle record, leaf slot mask,
+//         bits of 2^e_x >> 16 | bits of 2^e_y & 0xFFFF0000)
+//   n2, n3, n4 = the planes of x, y, z: word j holds slots 2j, 2j+1 as bytes (lo, hi, lo, hi)
+// The ray carries a node group — the
 // hit internal slots of one node still to visit, in the order k ^ octant(ray) — and up
 // to three triangle groups — the hit leaf slots of nodes visited, in visiting order. A
 // step tests one triangle of the first triangle group and, unless every group slot is
@@ -360,6 +369,7 @@ __device__ __forceinline__ void wide_init(WideState& s, const float4* nodes, con
     s.dinv = mk3(isfinite(ix) ? ix : copysignf(kWideFarInv, d.x), isfinite(iy) ? iy : copysignf(kWideFarInv, d.y),
                  isfinite(iz) ? iz : copysignf(kWideFarInv, d.z));
     s.oct = (s.dinv.x < 0.f ? 1u : 0u) | (s.dinv.y < 0.f ? 2u : 0u) | (s.dinv.z < 0.f ? 4u : 0u);
+
     s.best.t = FLT_MAX;
     s.best.u = 0.f;
     s.best.v = 0.f;
@@ -375,12 +385,6 @@ __device__ __forceinline__ void wide_init(WideState& s, const float4* nodes, con
     s.sp = 0;
     s.visits = 0;
     s.tests = 0;
-}
-
-// byte i of w plus 2^23, as a float: 0x4B0000qq is exactly 2^23 + q
-__device__ __forceinline__ float qbyte(uint32_t w, uint32_t sel)
-{
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, sel));
 }
 
 __device__ __forceinline__ float fmax3(float a, float b, float c)
@@ -424,69 +428,56 @@ __device__ __forceinline__ uint2 wide_pop(const uint2* smem_col, const uint2* sp
 
 // The children of a wide node (five float4 n0..n4) whose boxes the ray's interval
 // [0, best] meets: bit i for slot i.
-__device__ __forceinline__ uint32_t wide_child_hits(const WideState& s, float4 n0, float4 n2, float4 n3, float4 n4)
+__device__ __forceinline__ uint32_t wide_child_hits(const WideState& s, float4 n0, float4 n1, float4 n2, float4 n3,
+                                                    float4 n4)
 {
-    const uint32_t ew = __float_as_uint(n0.w);
-    // plane t = q * (2^e / d) + (p - o) / d, evaluated as (2^23 + q) * a + (b - 2^23 * a): the
-    // folded offset costs at most half a quantum, and the build leaves one quantum of slack
-    const float sx = __uint_as_float((ew & 0xFFu) << 23), sy = __uint_as_float(((ew >> 8) & 0xFFu) << 23),
-                sz = __uint_as_float(((ew >> 16) & 0xFFu) << 23);
+    // per-axis scales 2^e: the float bits e << 23 are stored as half-words (x, y in n1.w,
+    // z in the low half of n0.w), moved to the high half by one byte permute each
+    const uint32_t h01 = __float_as_uint(n1.w), h2 = __float_as_uint(n0.w);
+    const float sx = __uint_as_float(__byte_perm(h01, 0u, 0x1044u)), sy = __uint_as_float(h01 & 0xFFFF0000u),
+                sz = __uint_as_float(__byte_perm(h2, 0u, 0x1044u));
+    // plane t = q * (2^e / d) + (p - o) / d, evaluated as (1024 + q) * a + (b - 1024 * a):
+    // the folded offset rounds at the scale of b, well inside the build's spare quantum
     const float adx = sx * s.dinv.x, ady = sy * s.dinv.y, adz = sz * s.dinv.z;
-    const float bdx = fmaf(-8388608.0f, adx, (n0.x - s.o.x) * s.dinv.x);
-    const float bdy = fmaf(-8388608.0f, ady, (n0.y - s.o.y) * s.dinv.y);
-    const float bdz = fmaf(-8388608.0f, adz, (n0.z - s.o.z) * s.dinv.z);
-    // near / far planes per axis: lo and hi, swapped for a negative direction
-    const uint32_t lx0 = __float_as_uint(n2.x), lx1 = __float_as_uint(n2.y), ly0 = __float_as_uint(n2.z),
-                   ly1 = __float_as_uint(n2.w), lz0 = __float_as_uint(n3.x), lz1 = __float_as_uint(n3.y);
-    const uint32_t hx0 = __float_as_uint(n3.z), hx1 = __float_as_uint(n3.w), hy0 = __float_as_uint(n4.x),
-                   hy1 = __float_as_uint(n4.y), hz0 = __float_as_uint(n4.z), hz1 = __float_as_uint(n4.w);
-    const bool fx = s.oct & 1u, fy = s.oct & 2u, fz = s.oct & 4u;
-    const uint32_t nx0 = fx ? hx0 : lx0, nx1 = fx ? hx1 : lx1, fx0 = fx ? lx0 : hx0, fx1 = fx ? lx1 : hx1;
-    const uint32_t ny0 = fy ? hy0 : ly0, ny1 = fy ? hy1 : ly1, fy0 = fy ? ly0 : hy0, fy1 = fy ? ly1 : hy1;
-    const uint32_t nz0 = fz ? hz0 : lz0, nz1 = fz ? hz1 : lz1, fz0 = fz ? lz0 : hz0, fz1 = fz ? lz1 : hz1;
-    uint32_t hm = 0;
-    const float tlim = s.best.t;
-#if CPT_PACKED_BOX
-    // the near and far plane of an axis share the multiplier and the offset: one packed
-    // fused multiply-add per axis and child gives (t_near, t_far), each lane rounded as
-    // the scalar fmaf
     const f2 ax2 = mk2(adx, adx), ay2 = mk2(ady, ady), az2 = mk2(adz, adz);
+    const float bdx = fmaf(-1024.0f, adx, (n0.x - s.o.x) * s.dinv.x);
+    const float bdy = fmaf(-1024.0f, ady, (n0.y - s.o.y) * s.dinv.y);
+    const float bdz = fmaf(-1024.0f, adz, (n0.z - s.o.z) * s.dinv.z);
     const f2 bx2 = mk2(bdx, bdx), by2 = mk2(bdy, bdy), bz2 = mk2(bdz, bdz);
+    const uint32_t px[4] = {__float_as_uint(n2.x), __float_as_uint(n2.y), __float_as_uint(n2.z), __float_as_uint(n2.w)};
+    const uint32_t py[4] = {__float_as_uint(n3.x), __float_as_uint(n3.y), __float_as_uint(n3.z), __float_as_uint(n3.w)};
+    const uint32_t pz[4] = {__float_as_uint(n4.x), __float_as_uint(n4.y), __float_as_uint(n4.z), __float_as_uint(n4.w)};
+    // byte permute selectors: result bytes (near plane, 0x64, far plane, 0x64) of (word,
+    // 0x64646464) are the halves 1024 + q_near, 1024 + q_far; the near plane is hi for a
+    // negative direction; odd slots read bytes 2, 3
+    uint32_t oct = s.oct;
+    asm volatile("" : "+r"(oct));  // derived per node: loop-invariant copies would cost registers
+    const uint32_t px0 = (oct & 1u) ? 0x4041u : 0x4140u, py0 = (oct & 2u) ? 0x4041u : 0x4140u,
+                   pz0 = (oct & 4u) ? 0x4041u : 0x4140u;
+    const uint32_t sel[2][3] = {{px0, py0, pz0}, {px0 + 0x0202u, py0 + 0x0202u, pz0 + 0x0202u}};
+    const float tlim = s.best.t;
+    uint32_t hm = 0;
 #pragma unroll
     for (int i = 0; i < 8; i += 2) {  // two children at a time
         float tn[2], tf[2];
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-            const uint32_t sel = 0x7440u | (uint32_t)((i + k) & 3);
-            const f2 tx = fma2(mk2(qbyte(i < 4 ? nx0 : nx1, sel), qbyte(i < 4 ? fx0 : fx1, sel)), ax2, bx2);
-            const f2 ty = fma2(mk2(qbyte(i < 4 ? ny0 : ny1, sel), qbyte(i < 4 ? fy0 : fy1, sel)), ay2, by2);
-            const f2 tz = fma2(mk2(qbyte(i < 4 ? nz0 : nz1, sel), qbyte(i < 4 ? fz0 : fz1, sel)), az2, bz2);
+            // one packed fused multiply-add per axis gives (t_near, t_far), each lane
+            // rounded as the scalar fmaf
+            const f2 tx = fma2(half_pair(__byte_perm(px[i >> 1], 0x64646464u, sel[k][0])), ax2, bx2);
+            const f2 ty = fma2(half_pair(__byte_perm(py[i >> 1], 0x64646464u, sel[k][1])), ay2, by2);
+            const f2 tz = fma2(half_pair(__byte_perm(pz[i >> 1], 0x64646464u, sel[k][2])), az2, bz2);
             tn[k] = fmaxf(fmax3(tx.x, ty.x, tz.x), 0.0f);
             tf[k] = fminf(fmin3(tx.y, ty.y, tz.y), tlim);
         }
-        // the far ends grow by a relative 2^-18, both children in one packed multiply
+        // [max(tn, 0), min(tf, best) * (1 + 2^-18)] non-empty: the far end grows by a
+        // relative 2^-18, which covers the rounding of (p - o) / d for ray origins at any
+        // distance; both children in one packed multiply
         const f2 g = mul2(mk2(tf[0], tf[1]), mk2(kWideGrow, kWideGrow));
         hm |= (tn[0] <= g.x ? 1u : 0u) << i;
         hm |= (tn[1] <= g.y ? 1u : 0u) << (i + 1);
     }
     return hm;
-#else
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const uint32_t sel = 0x7440u | (uint32_t)(i & 3);
-        const float tnx = fmaf(qbyte(i < 4 ? nx0 : nx1, sel), adx, bdx);
-        const float tny = fmaf(qbyte(i < 4 ? ny0 : ny1, sel), ady, bdy);
-        const float tnz = fmaf(qbyte(i < 4 ? nz0 : nz1, sel), adz, bdz);
-        const float tfx = fmaf(qbyte(i < 4 ? fx0 : fx1, sel), adx, bdx);
-        const float tfy = fmaf(qbyte(i < 4 ? fy0 : fy1, sel), ady, bdy);
-        const float tfz = fmaf(qbyte(i < 4 ? fz0 : fz1, sel), adz, bdz);
-        // [max(tn, 0), min(tf, best) * (1 + 2^-18)] non-empty: the far end grows by a relative
-        // 2^-18, which covers the rounding of (p - o) / d for ray origins at any distance
-        const float tn = fmaxf(fmax3(tnx, tny, tnz), 0.0f), tf = fminf(fmin3(tfx, tfy, tfz), tlim) * kWideGrow;
-        hm |= (tn <= tf ? 1u : 0u) << i;
-    }
-    return hm;
-#endif
 }
 
 // One step; returns true when the ray is finished.
@@ -537,7 +528,7 @@ __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* 
     const float4* nd = s.nodes + 5 * (size_t)child;
     const float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3), n4 = __ldg(nd + 4);
     const uint32_t imask = __float_as_uint(n0.w) >> 24, lmask = __float_as_uint(n1.z);
-    const uint32_t hm = wide_child_hits(s, n0, n2, n3, n4);
+    const uint32_t hm = wide_child_hits(s, n0, n1, n2, n3, n4);
     s.cbase = __float_as_uint(n1.x);
     s.gbits = xor_permute8(hm & imask, s.oct) | (imask << 8);
     if (s.tbits & 0xFFu) {  // triangles still pending: the new group queues behind them

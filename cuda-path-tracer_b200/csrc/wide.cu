@@ -20,8 +20,9 @@
 // scale 2^e with (hi - lo + 2m) <= 253 * 2^e and the origin p = lo - m - 2^e (rounded
 // down); a child box, widened by the same m, is stored as qlo = floor((lo - m - p) /
 // 2^e) - 1, qhi = ceil((hi + m - p) / 2^e) + 1. The traversal evaluates a plane as
-// fma(2^23 + q, 2^e / d, (p - o) / d - 2^23 * 2^e / d), whose folded offset errs by at
-// most half a quantum (the spare quantum on each side covers it); m = 2^-20 x
+// fma(1024 + q, 2^e / d, (p - o) / d - 1024 * 2^e / d) (the byte read as the half
+// 1024 + q, a slot's lo and hi bytes side by side), whose folded offset errs by far less
+// than half a quantum (the spare quantum on each side covers it); m = 2^-20 x
 // (largest root-box coordinate magnitude + root-box diagonal) covers the rounding of
 // the quantized planes at the scene's scale, and the traversal's relative slack of
 // 2^-18 on the far end of each interval covers the rounding of (p - o) / d, which
@@ -255,8 +256,10 @@ __device__ __forceinline__ void wide_level_nodes(const float4* __restrict__ bin,
             atomicOr(status, CPT_STATUS_BAD_INDEX);
             continue;
         }
-        uint32_t qlo[3][2] = {{0xFFFFFFFFu, 0xFFFFFFFFu}, {0xFFFFFFFFu, 0xFFFFFFFFu}, {0xFFFFFFFFu, 0xFFFFFFFFu}};
-        uint32_t qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+        // per axis, word j: slots 2j, 2j+1 as bytes (lo, hi, lo, hi); an empty slot is (255, 0)
+        uint32_t qp[3][4];
+        for (int a = 0; a < 3; ++a)
+            for (int j = 0; j < 4; ++j) qp[a][j] = 0x00FF00FFu;
         for (int i = 0; i < count; ++i) {
             const int s = slot_of[i];
             const uint32_t ref = s_ref[i][t];
@@ -267,9 +270,8 @@ __device__ __forceinline__ void wide_level_nodes(const float4* __restrict__ bin,
                 const double lo = (double)bx[a] - (double)m, hi = (double)bx[3 + a] + (double)m;
                 const int ql = (int)fmin(fmax(floor((lo - (double)p[a]) / sc[a]) - 1.0, 0.0), 255.0);
                 const int qh = (int)fmin(fmax(ceil((hi - (double)p[a]) / sc[a]) + 1.0, 0.0), 255.0);
-                const int sh = 8 * (s & 3);
-                qlo[a][s >> 2] = (qlo[a][s >> 2] & ~(0xFFu << sh)) | ((uint32_t)ql << sh);
-                qhi[a][s >> 2] = (qhi[a][s >> 2] & ~(0xFFu << sh)) | ((uint32_t)qh << sh);
+                const int sh = 16 * (s & 1);
+                qp[a][s >> 1] = (qp[a][s >> 1] & ~(0xFFFFu << sh)) | (((uint32_t)ql | ((uint32_t)qh << 8)) << sh);
             }
             const uint32_t below = (1u << s) - 1u;
             if (ref & kLeafRef) {
@@ -287,17 +289,16 @@ __device__ __forceinline__ void wide_level_nodes(const float4* __restrict__ bin,
                 qd[1] = make_float4(bx[3], bx[4], bx[5], 0.f);
             }
         }
-        const uint32_t ew = (uint32_t)(e[0] + 127) | ((uint32_t)(e[1] + 127) << 8) | ((uint32_t)(e[2] + 127) << 16) |
-                            (imask << 24);
+        // the scale 2^e of an axis as the high half-word of its float bits: (e + 127) << 7
+        const uint32_t hx = (uint32_t)(e[0] + 127) << 7, hy = (uint32_t)(e[1] + 127) << 7,
+                       hz = (uint32_t)(e[2] + 127) << 7;
         float4* o = wide + 5 * (size_t)wi;
-        o[0] = make_float4(p[0], p[1], p[2], __uint_as_float(ew));
-        o[1] = make_float4(__uint_as_float(child_base), __uint_as_float(tri_base), __uint_as_float(lmask), 0.f);
-        o[2] = make_float4(__uint_as_float(qlo[0][0]), __uint_as_float(qlo[0][1]), __uint_as_float(qlo[1][0]),
-                           __uint_as_float(qlo[1][1]));
-        o[3] = make_float4(__uint_as_float(qlo[2][0]), __uint_as_float(qlo[2][1]), __uint_as_float(qhi[0][0]),
-                           __uint_as_float(qhi[0][1]));
-        o[4] = make_float4(__uint_as_float(qhi[1][0]), __uint_as_float(qhi[1][1]), __uint_as_float(qhi[2][0]),
-                           __uint_as_float(qhi[2][1]));
+        o[0] = make_float4(p[0], p[1], p[2], __uint_as_float(hz | (imask << 24)));
+        o[1] = make_float4(__uint_as_float(child_base), __uint_as_float(tri_base), __uint_as_float(lmask),
+                           __uint_as_float(hx | (hy << 16)));
+        for (int a = 0; a < 3; ++a)
+            o[2 + a] = make_float4(__uint_as_float(qp[a][0]), __uint_as_float(qp[a][1]), __uint_as_float(qp[a][2]),
+                                   __uint_as_float(qp[a][3]));
     }
 }
 
