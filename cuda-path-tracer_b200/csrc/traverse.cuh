@@ -410,6 +410,14 @@ __device__ __forceinline__ uint32_t xor_permute8(uint32_t x, uint32_t oct)
     return x;
 }
 
+// Fills the block's octant permutation table (byte oct * 256 + x = xor_permute8(x, oct));
+// every thread of the block calls it, before any traversal.
+__device__ __forceinline__ void wide_perm_table(uint8_t* perm)
+{
+    for (uint32_t i = threadIdx.x; i < 2048u; i += blockDim.x) perm[i] = (uint8_t)xor_permute8(i & 255u, i >> 8);
+    __syncthreads();
+}
+
 template <int kBlock>
 __device__ __forceinline__ void wide_push(uint2* smem_col, uint2* spill, int& sp, uint2 v, bool& overflow)
 {
@@ -481,9 +489,11 @@ __device__ __forceinline__ uint32_t wide_child_hits(const WideState& s, float4 n
 }
 
 // One step; returns true when the ray is finished.
+// perm: xor_permute8 as a table in shared memory, byte oct * 256 + x (wide_perm_table).
 template <bool kAny, int kBlock, bool kStats>
 __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* spill, bool& overflow,
-                                          uint32_t& n_nodes, uint32_t& n_tris, bool test_tri = true)
+                                          uint32_t& n_nodes, uint32_t& n_tris, const uint8_t* perm,
+                                          bool test_tri = true)
 {
     if (test_tri && (s.tbits & 0xFFu)) {
         const uint32_t slot = __ffs(s.tbits & 0xFFu) - 1;
@@ -530,7 +540,7 @@ __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* 
     const uint32_t imask = __float_as_uint(n0.w) >> 24, lmask = __float_as_uint(n1.z);
     const uint32_t hm = wide_child_hits(s, n0, n1, n2, n3, n4);
     s.cbase = __float_as_uint(n1.x);
-    s.gbits = xor_permute8(hm & imask, s.oct) | (imask << 8);
+    s.gbits = (uint32_t)perm[(s.oct << 8) | (hm & imask)] | (imask << 8);
     if (s.tbits & 0xFFu) {  // triangles still pending: the new group queues behind them
         if (s.tbits2 & 0xFFu) {
             s.tbase3 = __float_as_uint(n1.y);
@@ -628,6 +638,8 @@ __device__ __forceinline__ void persistent_trace_wide(WideOf wide_of, const floa
     const uint32_t refill_below = refill ? refill : (uint32_t)kWideRefillLanes;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
+    __shared__ uint8_t s_perm[2048];
+    wide_perm_table(s_perm);
     uint2 spill[CPT_TRAVERSAL_STACK - kWideSmemStack];
     WideState s;
     uint32_t ray = CPT_INVALID_INDEX;
@@ -675,7 +687,7 @@ __device__ __forceinline__ void persistent_trace_wide(WideOf wide_of, const floa
                 test_tri = __ballot_sync(0xFFFFFFFFu, must) != 0u || __popc(bw) >= kWideTriBatch;
             }
             if (ray != CPT_INVALID_INDEX &&
-                wide_step<kAny, kBlock, kStats>(s, smem_col, spill, overflow, n_nodes, n_tris, test_tri)) {
+                wide_step<kAny, kBlock, kStats>(s, smem_col, spill, overflow, n_nodes, n_tris, s_perm, test_tri)) {
                 done(ray, s);
                 ray = CPT_INVALID_INDEX;
             }
