@@ -302,18 +302,34 @@ __device__ __forceinline__ Hit traverse(const float4* __restrict__ nodes, f3 o, 
 // Compressed 8-wide BVH (cpt_lbvh_wide). A wide node is five float4 (child box planes
 // p + q * 2^e, q one byte):
 //   n0 = (p.x, p.y, p.z, bits of 2^e_z >> 16 | internal slot mask << 24)
-//   n1 = (first internal child, first triangle record, leaf slot mask,
+//   n1 = (first internal child, first triangle record,
+//         leaf slot mask | slots with 2+ records << 8 | slots with 3 records << 16,
 //         bits of 2^e_x >> 16 | bits of 2^e_y & 0xFFFF0000)
 //   n2, n3, n4 = the planes of x, y, z: word j holds slots 2j, 2j+1 as bytes (lo, hi, lo, hi)
-// The ray carries a node group — the
-// hit internal slots of one node still to visit, in the order k ^ octant(ray) — and up
-// to three triangle groups — the hit leaf slots of nodes visited, in visiting order. A
+// A leaf slot holds 1 to 3 triangle records (a binary subtree of up to three leaves under
+// one box). Record j of the leaf slot of rank r among the node's L leaf slots is the
+// node's record j * L + r (layers of L records; a slot with fewer records leaves holes).
+// The ray carries a node group — the hit internal slots of one node still to visit, in
+// the order k ^ octant(ray) — and up to three triangle groups — the records of the hit
+// leaf slots of nodes visited, in visiting order: bits 8j + s for record j of slot s, the
+// node's leaf slot mask in bits 24-31. A
 // step tests one triangle of the first triangle group and, unless every group slot is
 // taken, visits the next node of the node group (the rest of the group goes on the
 // stack; the node's triangle group queues behind), or pops a group. The triangle test
 // is tri_test on the binary leaf slot's words, so a hit's t, u, v are unchanged.
 constexpr int kWideSmemStack = 16;  // stack entries (2 words) per thread in shared memory
 constexpr float kWideGrow = 1.0f + 1.0f / 262144.0f;  // relative slack of a wide child's box test
+// Records a leaf slot holds at most: binary subtrees of up to this many leaves become one
+// leaf slot of their parent wide node instead of a wide node of their own; a wide tree
+// over L binary leaves has kWideRecordLayers * L record positions. C2: 544.5 Mrays/s
+// with 1 (65.9 node visits and 20.1 triangle tests per ray), 559.8 with 2 (63.7, 20.9),
+// 559.6 with 3 (61.7, 23.7).
+#ifndef CPT_WIDE_LEAF_MAX
+#define CPT_WIDE_LEAF_MAX 2
+#endif
+constexpr uint32_t kWideRecordLayers = CPT_WIDE_LEAF_MAX;
+static_assert(kWideRecordLayers >= 1 && kWideRecordLayers <= 3, "a leaf slot holds 1 to 3 records");
+constexpr uint32_t kWideRecBits = 0x00FFFFFFu;  // a triangle group's record bits
 // The wide traversal refills once two lanes of the warp are idle (fewer than 31 busy):
 // its steps are long (8 child boxes), so idle lanes cost more than the refill's ballot
 // and atomic (C2 with one triangle test per step: 313 Mrays/s at 32, 302 at 28, 283 at
@@ -349,7 +365,7 @@ struct WideState {
     uint32_t oct;         // direction sign bits (x: 1, y: 2, z: 4)
     Hit best;
     uint32_t cbase, gbits;  // node group: first child; bits 0-7 hit slots in visit order, 8-15 internal mask
-    uint32_t tbase, tbits;  // triangle group: first record; bits 0-7 hit leaf slots, 8-15 leaf mask
+    uint32_t tbase, tbits;  // triangle group: first record; records to test (kWideRecBits), leaf mask << 24
     uint32_t tbase2, tbits2;  // a second triangle group, queued behind the first
     uint32_t tbase3, tbits3;  // and a third
     int sp;
@@ -362,7 +378,7 @@ __device__ __forceinline__ void wide_init(WideState& s, const float4* nodes, con
     s.nodes = nodes;
     s.tris = tris;
     s.max_visits = max_visits;
-    s.tri_cap = max_visits + 1;
+    s.tri_cap = kWideRecordLayers * (max_visits + 1);
     s.o = o;
     s.d = d;
     const float ix = __frcp_rn(d.x), iy = __frcp_rn(d.y), iz = __frcp_rn(d.z);
@@ -495,10 +511,11 @@ __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* 
                                           uint32_t& n_nodes, uint32_t& n_tris, const uint8_t* perm,
                                           bool test_tri = true)
 {
-    if (test_tri && (s.tbits & 0xFFu)) {
-        const uint32_t slot = __ffs(s.tbits & 0xFFu) - 1;
-        s.tbits &= ~(1u << slot);
-        const uint32_t idx = s.tbase + __popc((s.tbits >> 8) & ((1u << slot) - 1u));
+    if (test_tri && (s.tbits & kWideRecBits)) {
+        const uint32_t rb = __ffs(s.tbits) - 1;  // bit 8j + slot (the leaf mask lies above)
+        s.tbits &= ~(1u << rb);
+        const uint32_t lm = s.tbits >> 24;
+        const uint32_t idx = s.tbase + (rb >> 3) * __popc(lm) + __popc(lm & ((1u << (rb & 7u)) - 1u));
         if (idx >= s.tri_cap) { overflow = true; return true; }
         const float4 a = __ldg(s.tris + 3 * (size_t)idx), b = __ldg(s.tris + 3 * (size_t)idx + 1),
                      c = __ldg(s.tris + 3 * (size_t)idx + 2);
@@ -513,17 +530,17 @@ __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* 
             s.best.tri = __float_as_uint(a.w);
             if (kAny) return true;
         }
-        if (!(s.tbits & 0xFFu) && (s.tbits2 & 0xFFu)) {  // the queued groups move up
+        if (!(s.tbits & kWideRecBits) && (s.tbits2 & kWideRecBits)) {  // the queued groups move up
             s.tbase = s.tbase2;
             s.tbits = s.tbits2;
             s.tbase2 = s.tbase3;
             s.tbits2 = s.tbits3;
             s.tbits3 = 0;
         }
-        if (s.tbits3 & 0xFFu) return false;  // every group slot pending: no node visit this step
+        if (s.tbits3 & kWideRecBits) return false;  // every group slot pending: no node visit this step
     }
     if (!(s.gbits & 0xFFu)) {
-        if (s.sp == 0) return !(s.tbits & 0xFFu);  // done once the last triangles are tested
+        if (s.sp == 0) return !(s.tbits & kWideRecBits);  // done once the last triangles are tested
         const uint2 g = wide_pop<kBlock>(smem_col, spill, s.sp);
         s.cbase = g.x;
         s.gbits = g.y;
@@ -537,22 +554,25 @@ __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* 
     if (kStats) ++n_nodes;
     const float4* nd = s.nodes + 5 * (size_t)child;
     const float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3), n4 = __ldg(nd + 4);
-    const uint32_t imask = __float_as_uint(n0.w) >> 24, lmask = __float_as_uint(n1.z);
+    const uint32_t imask = __float_as_uint(n0.w) >> 24, lw = __float_as_uint(n1.z);
     const uint32_t hm = wide_child_hits(s, n0, n1, n2, n3, n4);
     s.cbase = __float_as_uint(n1.x);
     s.gbits = (uint32_t)perm[(s.oct << 8) | (hm & imask)] | (imask << 8);
-    if (s.tbits & 0xFFu) {  // triangles still pending: the new group queues behind them
-        if (s.tbits2 & 0xFFu) {
+    // the hit slots' records: the hit mask copied into bytes 0-2, masked by the slots
+    // holding a first / second / third record; the leaf mask above
+    const uint32_t recs = ((hm * 0x010101u) & lw) | (lw << 24);
+    if (s.tbits & kWideRecBits) {  // triangles still pending: the new group queues behind them
+        if (s.tbits2 & kWideRecBits) {
             s.tbase3 = __float_as_uint(n1.y);
-            s.tbits3 = (hm & lmask) | (lmask << 8);
+            s.tbits3 = recs;
             return false;
         }
         s.tbase2 = __float_as_uint(n1.y);
-        s.tbits2 = (hm & lmask) | (lmask << 8);
+        s.tbits2 = recs;
         return false;
     }
     s.tbase = __float_as_uint(n1.y);
-    s.tbits = (hm & lmask) | (lmask << 8);
+    s.tbits = recs;
     return false;
 }
 
@@ -681,8 +701,8 @@ __device__ __forceinline__ void persistent_trace_wide(WideOf wide_of, const floa
                 // the warp tests triangles when enough lanes have some pending, or when a lane
                 // must (every group slot taken, or no node left to visit)
                 const bool live = ray != CPT_INVALID_INDEX;
-                const bool want = live && (s.tbits & 0xFFu);
-                const bool must = want && ((s.tbits3 & 0xFFu) || (!(s.gbits & 0xFFu) && s.sp == 0));
+                const bool want = live && (s.tbits & kWideRecBits);
+                const bool must = want && ((s.tbits3 & kWideRecBits) || (!(s.gbits & 0xFFu) && s.sp == 0));
                 const unsigned bw = __ballot_sync(0xFFFFFFFFu, want);
                 test_tri = __ballot_sync(0xFFFFFFFFu, must) != 0u || __popc(bw) >= kWideTriBatch;
             }

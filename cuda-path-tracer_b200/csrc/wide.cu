@@ -12,9 +12,13 @@
 // Through Compressed Wide BVHs", HPG 2017): slot s is meant to be met first by rays
 // whose direction has sign pattern s, so that visiting the slots in the order
 // k ^ octant(ray), k = 0..7, is near-to-far; children are assigned greedily by the
-// smallest projection of their centre on the octant's diagonal. Internal children are
-// allocated consecutively (one atomic per node) and queued for the next level;
-// leaf children's triangle records likewise.
+// smallest projection of their centre on the octant's diagonal. After the collapse, an
+// internal child whose binary subtree has up to kWideRecordLayers (2) leaves becomes a
+// leaf slot holding those triangles (one box for them, no wide node of its own: C2's
+// 8-wide tree had 5.2 M two-leaf and 2.0 M three-leaf nodes among 14.0 M). Internal children are allocated
+// consecutively (one atomic per node) and queued for the next level; the leaf slots'
+// triangle records likewise, in layers (record j of the leaf slot of rank r among L at
+// j * L + r).
 //
 // Quantization: the node box, widened by a margin m, gives a per-axis power-of-two
 // scale 2^e with (hi - lo + 2m) <= 253 * 2^e and the origin p = lo - m - 2^e (rounded
@@ -135,6 +139,63 @@ __global__ void k_wide_init(const float4* __restrict__ bin, float4* __restrict__
     for (int l = 0; l < kWideLevels + 2; ++l) ctr[4 + l] = l == 0 ? 0u : 1u;  // bounds[0] = 0, bounds[1] = 1
 }
 
+// Records a child of a wide node becomes: 1 for a binary leaf; for an internal binary
+// node whose subtree has 2 or 3 leaves (up to kWideRecordLayers), that many — the child
+// is then a leaf slot whose box holds those triangles; 0 for an internal child (a wide node).
+__device__ __forceinline__ uint32_t leaf_records(const float4* __restrict__ bin, uint32_t ref, uint32_t bin_internal)
+{
+    if (ref & kLeafRef) return 1;
+    if (kWideRecordLayers < 2 || ref >= bin_internal) return 0;
+    const float4 f = bin[6 * (size_t)ref + 5];
+    const uint32_t word = __float_as_uint(f.x);
+    if (!(word & 3u)) return 2;  // both children leaves
+    if ((word & 3u) == 3u || kWideRecordLayers < 3) return 0;
+    const uint32_t d = (word & 1u) ? (word >> 2) : __float_as_uint(f.y);  // the internal child
+    if (d >= bin_internal) return 0;
+    return (__float_as_uint(bin[6 * (size_t)d + 5].x) & 3u) ? 0u : 3u;
+}
+
+// The triangle record of leaf `side` of binary node `parent`: the binary leaf slot's
+// words (v0, index) (v1 - v0, 0) (v2 - v0, 0).
+__device__ __forceinline__ void emit_leaf(const float4* __restrict__ bin, uint32_t parent, uint32_t side,
+                                          float4* __restrict__ tr)
+{
+    const float2* sl = reinterpret_cast<const float2*>(bin + 6 * (size_t)parent) + 5 * side;
+    const float2 a0 = sl[0], a1 = sl[1], a2 = sl[2], a3 = sl[3], a4 = sl[4];
+    tr[0] = make_float4(a0.x, a0.y, a1.x, a1.y);  // v0, triangle index
+    tr[1] = make_float4(a2.x, a2.y, a3.x, 0.f);   // v1 - v0
+    tr[2] = make_float4(a3.y, a4.x, a4.y, 0.f);   // v2 - v0
+}
+
+// The cnt records (leaf_records) of child ref, in binary order: record j at rec + j * stride.
+__device__ __forceinline__ void emit_records(const float4* __restrict__ bin, uint32_t ref, uint32_t cnt,
+                                             float4* __restrict__ rec, size_t stride)
+{
+    const size_t st = 3 * stride;
+    if (ref & kLeafRef) {
+        emit_leaf(bin, (ref & ~kLeafRef) >> 1, ref & 1u, rec);
+        return;
+    }
+    if (cnt == 2) {
+        emit_leaf(bin, ref, 0, rec);
+        emit_leaf(bin, ref, 1, rec + st);
+        return;
+    }
+    const float4 f = bin[6 * (size_t)ref + 5];
+    const uint32_t word = __float_as_uint(f.x);
+    if (word & 1u) {  // side 0 is the two-leaf subtree
+        const uint32_t d = word >> 2;
+        emit_leaf(bin, d, 0, rec);
+        emit_leaf(bin, d, 1, rec + st);
+        emit_leaf(bin, ref, 1, rec + 2 * st);
+    } else {
+        const uint32_t d = __float_as_uint(f.y);
+        emit_leaf(bin, ref, 0, rec);
+        emit_leaf(bin, d, 0, rec + st);
+        emit_leaf(bin, d, 1, rec + 2 * st);
+    }
+}
+
 // Smallest e with ext <= 253 * 2^e (e in [-126, 127]): the 255 quanta of a byte less
 // one quantum of slack on each side.
 __device__ __forceinline__ int scale_exp(double ext)
@@ -244,15 +305,23 @@ __device__ __forceinline__ void wide_level_nodes(const float4* __restrict__ bin,
             placed |= 1u << bi;
             used |= 1u << bs;
         }
-        uint32_t imask = 0, lmask = 0;
+        // leaf slots (m1) and those holding a second (m2) and third (m3) record; the
+        // node's records are layers of n_leaf records, one per leaf slot in slot order
+        uint32_t cnt_of[8];
+        uint32_t imask = 0, m1 = 0, m2 = 0, m3 = 0;
         for (int i = 0; i < count; ++i) {
-            if (s_ref[i][t] & kLeafRef) lmask |= 1u << slot_of[i];
-            else imask |= 1u << slot_of[i];
+            cnt_of[i] = leaf_records(bin, s_ref[i][t], bin_internal);
+            const uint32_t bit = 1u << slot_of[i];
+            if (!cnt_of[i]) imask |= bit;
+            if (cnt_of[i] >= 1) m1 |= bit;
+            if (cnt_of[i] >= 2) m2 |= bit;
+            if (cnt_of[i] >= 3) m3 |= bit;
         }
-        const uint32_t n_int = __popc(imask), n_leaf = __popc(lmask);
+        const uint32_t n_int = __popc(imask), n_leaf = __popc(m1);
+        const uint32_t n_rec = n_leaf * (m3 ? 3u : m2 ? 2u : 1u);
         const uint32_t child_base = n_int ? atomicAdd(&ctr[0], n_int) : 0u;
-        const uint32_t tri_base = n_leaf ? atomicAdd(&ctr[1], n_leaf) : 0u;
-        if (child_base + n_int > node_cap || tri_base + n_leaf > tri_cap) {
+        const uint32_t tri_base = n_rec ? atomicAdd(&ctr[1], n_rec) : 0u;
+        if (child_base + n_int > node_cap || tri_base + n_rec > tri_cap) {
             atomicOr(status, CPT_STATUS_BAD_INDEX);
             continue;
         }
@@ -274,15 +343,8 @@ __device__ __forceinline__ void wide_level_nodes(const float4* __restrict__ bin,
                 qp[a][s >> 1] = (qp[a][s >> 1] & ~(0xFFFFu << sh)) | (((uint32_t)ql | ((uint32_t)qh << 8)) << sh);
             }
             const uint32_t below = (1u << s) - 1u;
-            if (ref & kLeafRef) {
-                const uint32_t parent = (ref & ~kLeafRef) >> 1, side = ref & 1u;
-                const float4* pr = bin + 6 * (size_t)parent;
-                const float2* sl = reinterpret_cast<const float2*>(pr) + 5 * side;
-                const float2 a0 = sl[0], a1 = sl[1], a2 = sl[2], a3 = sl[3], a4 = sl[4];
-                float4* tr = tris + 3 * (size_t)(tri_base + __popc(lmask & below));
-                tr[0] = make_float4(a0.x, a0.y, a1.x, a1.y);  // v0, triangle index
-                tr[1] = make_float4(a2.x, a2.y, a3.x, 0.f);   // v1 - v0
-                tr[2] = make_float4(a3.y, a4.x, a4.y, 0.f);   // v2 - v0
+            if (cnt_of[i]) {
+                emit_records(bin, ref, cnt_of[i], tris + 3 * (size_t)(tri_base + __popc(m1 & below)), n_leaf);
             } else {
                 float4* qd = queue + 2 * (size_t)(child_base + __popc(imask & below));
                 qd[0] = make_float4(bx[0], bx[1], bx[2], __uint_as_float(ref));
@@ -294,8 +356,8 @@ __device__ __forceinline__ void wide_level_nodes(const float4* __restrict__ bin,
                        hz = (uint32_t)(e[2] + 127) << 7;
         float4* o = wide + 5 * (size_t)wi;
         o[0] = make_float4(p[0], p[1], p[2], __uint_as_float(hz | (imask << 24)));
-        o[1] = make_float4(__uint_as_float(child_base), __uint_as_float(tri_base), __uint_as_float(lmask),
-                           __uint_as_float(hx | (hy << 16)));
+        o[1] = make_float4(__uint_as_float(child_base), __uint_as_float(tri_base),
+                           __uint_as_float(m1 | (m2 << 8) | (m3 << 16)), __uint_as_float(hx | (hy << 16)));
         for (int a = 0; a < 3; ++a)
             o[2 + a] = make_float4(__uint_as_float(qp[a][0]), __uint_as_float(qp[a][1]), __uint_as_float(qp[a][2]),
                                    __uint_as_float(qp[a][3]));
@@ -357,9 +419,9 @@ using namespace cpt;
 
 extern "C" size_t cpt_lbvh_wide_bytes(uint32_t leaves, size_t* node_bytes, size_t* tri_bytes)
 {
-    if (leaves < 2 || leaves >= (1u << 31)) return 0;
+    if (leaves < 2 || leaves > 0xFFFFFFFFu / kWideRecordLayers) return 0;
     if (node_bytes) *node_bytes = align_up((size_t)(leaves - 1) * 80, 256);
-    if (tri_bytes) *tri_bytes = align_up((size_t)leaves * 48, 256);
+    if (tri_bytes) *tri_bytes = align_up((size_t)leaves * kWideRecordLayers * 48, 256);
     return wide_scratch_layout(leaves, nullptr, nullptr);
 }
 
@@ -409,7 +471,7 @@ extern "C" int cpt_lbvh_wide(cpt_bvh* bvh, void* nodes, size_t node_bytes, void*
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     CPT_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_wide_levels, bin, static_cast<float4*>(nodes), static_cast<float4*>(tris),
-                                    ws.queue, ws.ctr, leaves - 1, leaves, leaves - 1, bvh->status));
+                                    ws.queue, ws.ctr, leaves - 1, leaves * kWideRecordLayers, leaves - 1, bvh->status));
     note_launch();
     k_wide_check<<<1, 32, 0, stream>>>(ws.ctr, bvh->status, bvh->status + 2);
     CPT_LAUNCH_CHECK();

@@ -313,12 +313,13 @@ int cpt_render_views(const cpt_view* views, uint32_t n_views, const cpt_render_p
 /* ---- compressed 8-wide traversal BVH (an extension; no reference counterpart) ----
  * Collapses the binary traversal tree in use (the split tree when one was built,
  * else the LBVH's nodes) into 8-wide nodes of 80 B with 8-bit child boxes and
- * direction-ordered slots, and copies the leaf triangles into 48-B records in
- * visiting order. Tracing and rendering then traverse it. Hits are those of the
- * binary tree (same triangle arithmetic) up to which of several exactly equal
- * distances is reported. `leaves` for the sizes: bvh->n, or bvh->split_capacity
- * after cpt_lbvh_split. status[2] / status[3] receive the wide node and triangle
- * record counts. */
+ * direction-ordered slots (a binary subtree of two leaves becomes one slot), and
+ * copies the leaf triangles into 48-B records in visiting order (two record positions
+ * per binary leaf are reserved). Tracing and rendering then traverse it.
+ * Hits are those of the binary tree (same triangle arithmetic) up to which of several
+ * exactly equal distances is reported. `leaves` for the sizes: bvh->n, or
+ * bvh->split_capacity after cpt_lbvh_split. status[2] / status[3] receive the wide
+ * node count and the record positions used. */
 size_t cpt_lbvh_wide_bytes(uint32_t leaves, size_t* node_bytes, size_t* tri_bytes); /* returns scratch bytes */
 int cpt_lbvh_wide(cpt_bvh* bvh, void* nodes, size_t node_bytes, void* tris, size_t tri_bytes, void* scratch,
                   size_t scratch_bytes, cudaStream_t stream);
