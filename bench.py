@@ -35,17 +35,18 @@ sys.path.insert(0, os.path.join(ROOT, "cuda-path-tracer_b200"))
 WORKLOADS = {
     "c2": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=16,
                bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, split=8.0, wide=1, treelet=1,
+               wide_sah=1,
                # every e2e step rebuilds the trees inside its timed region: there the cheaper build wins
                e2e_split=4.0, e2e_treelet=0),
     "c1": dict(kind="random", n=65536, bits=30, width=512, height=512, spp=1, bounces=3, eye=(0.5, 0.5, -1.2),
                target=(0.5, 0.5, 0.0), seed=0),
     # 64 scenes, 10k-2M triangles (log-uniform, alternating generators), 256^2-1024^2, one graph launch per frame
     "c3": dict(kind="batch", scenes=64, tri_min=10_000, tri_max=2_000_000, res_min=256, res_max=1024, spp=4,
-               bounces=5, bits=63, seed=0, width=0, height=0, split=1.25, wide=1),
+               bounces=5, bits=63, seed=0, width=0, height=0, split=1.25, wide=1, wide_sah=1),
     # radiance cache on the C2 scene: 1 spp frames through the cache vs plain 16 spp, RMSE vs an FP64 image
     "c4": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=1,
                bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, plain_spp=64, ref_spp=4096,
-               ref_div=4, warm_updates=2, max_spp=256, split=8.0, wide=1, treelet=1),
+               ref_div=4, warm_updates=2, max_spp=256, split=8.0, wide=1, treelet=1, wide_sah=1),
     # deforming 16.8 M-triangle displaced sphere, full rebuild every frame, 8 cameras
     "c5": dict(kind="deform", nu=4096, nv=2048, n_hair=0, bits=63, width=1280, height=720, spp=1, bounces=7,
                eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, cameras=8, amp=0.01, omega=40.0, cache=True),
@@ -438,7 +439,7 @@ def run_batch(args, w, world, rank, local):
         if kind != "random" and split > 0:  # the hairball scenes traverse a split BVH
             lb.split(split, flags=split_flags(args))
         if args.wide:
-            lb.wide(keep_scratch=True)
+            lb.wide(keep_scratch=True, sah=bool(args.wide_sah))
         sc = DeviceScene(infos, None, dev)
         eye, tgt = ((0.5, 0.5, -1.2), (0.5, 0.5, 0.0)) if kind == "random" else ((0.0, 0.35, -3.6), (0.0, 0.0, 0.0))
         cam = cpt.camera_look_at(eye, tgt, fov_deg=45.0, aspect=1.0)
@@ -721,7 +722,7 @@ def run_ours(args, w, world, rank, local):
     if split > 0:
         lb.split(split, keep_scratch=True, flags=split_flags(args))
     if args.wide:
-        lb.wide(keep_scratch=True)
+        lb.wide(keep_scratch=True, sah=bool(args.wide_sah))
     params = make_params(W_, H_, spp, 0, w["bounces"], 3.0, True, w["seed"], cpt.ACCUM_KAHAN,
                          wave_paths=args.wave_paths, ray_sort=bool(args.ray_sort), cameras=len(cams),
                          refill_lanes=args.refill_lanes, traverse_blocks_per_sm=args.blocks_per_sm,
@@ -871,13 +872,16 @@ def run_ours(args, w, world, rank, local):
         torch.cuda.synchronize()
         lbvh_topology["split_build_ms"] = round(s0.elapsed_time(s1), 3)
         if args.wide:
-            lb.wide(keep_scratch=True)
-            torch.cuda.synchronize()
-            s0.record(stream)
-            lb.wide(keep_scratch=True)
-            s1.record(stream)
-            torch.cuda.synchronize()
-            lbvh_topology["wide_build_ms"] = round(s0.elapsed_time(s1), 3)
+            # both collapses timed; the tree left for what follows is the workload's
+            for key, sah in (("wide_build_ms", False), ("wide_sah_build_ms", True)):
+                lb.wide(keep_scratch=True, sah=sah)
+                torch.cuda.synchronize()
+                s0.record(stream)
+                lb.wide(keep_scratch=True, sah=sah)
+                s1.record(stream)
+                torch.cuda.synchronize()
+                lbvh_topology[key] = round(s0.elapsed_time(s1), 3)
+            lb.wide(keep_scratch=True, sah=bool(args.wide_sah))
 
     # --- LBVH build of the same scene (device-resident triangles); the deforming
     # workload already rebuilt inside every timed step: those builds are reported
@@ -989,7 +993,7 @@ def run_ours(args, w, world, rank, local):
         if split > 0:
             lb.split(split, keep_scratch=True, flags=split_flags(args))
         if args.wide:
-            lb.wide(keep_scratch=True)
+            lb.wide(keep_scratch=True, sah=bool(args.wide_sah))
         torch.cuda.synchronize()
 
     # --- radiance cache (the C4 configuration on this scene and tree): time to reach the
@@ -1280,7 +1284,7 @@ def run_cache(args, w, world, rank, local):
     if split > 0:
         lb.split(split, flags=split_flags(args))
     if args.wide:
-        lb.wide()
+        lb.wide(sah=bool(args.wide_sah))
     scene = DeviceScene(infos, None, dev)
     scene.build_emitters(lb)
     spf = w["spp"]
@@ -1368,6 +1372,10 @@ def main():
     ap.add_argument("--wide", type=int, default=None,
                     help="1: traverse the compressed 8-wide tree built from the (split) binary tree, 0: the binary "
                          "tree (default per workload)")
+    ap.add_argument("--wide-sah", type=int, default=None,
+                    help="1: the surface-area collapse (CPT_WIDE_SAH) for trees built once before the timed frames; "
+                         "trees rebuilt inside a timed step always use the faster largest-child collapse "
+                         "(default per workload)")
     ap.add_argument("--rc-per-sample", action="store_true",
                     help="c4: 2^16 training suffixes per image sample instead of per render call (frame)")
     ap.add_argument("--rc-interval", type=int, default=12,
@@ -1387,6 +1395,8 @@ def main():
     w = dict(WORKLOADS[args.workload])
     if args.wide is None:
         args.wide = int(w.get("wide", 0))
+    if args.wide_sah is None:
+        args.wide_sah = int(w.get("wide_sah", 0))
     args.treelet_given = args.treelet
     if args.treelet is None:
         args.treelet = int(w.get("treelet", 0))

@@ -49,6 +49,7 @@ def build_lookback_limit(log2_polls: int) -> int:
 ACCUM_KAHAN, ACCUM_LERP, ACCUM_F64 = 0, 1, 2
 INVALID_INDEX = 0xFFFFFFFF
 SPLIT_TREELET = 2
+WIDE_SAH = 1  # cpt_lbvh_wide flag: surface-area collapse
 TRAVERSAL_STACK = 64
 
 TRIANGLE_DTYPE = np.dtype([("v0", "<f4", 3), ("v1", "<f4", 3), ("v2", "<f4", 3), ("info_idx", "<u4")])
@@ -141,8 +142,8 @@ _PROTOS = {
     "cpt_render": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Scene), ctypes.c_void_p,
                           ctypes.POINTER(RenderParams), _P, _P, _SZ, _P, _P, _P]),
     "cpt_resolve": (_I32, [_P, _U32, _U32, _U32, _P, _P]),
-    "cpt_lbvh_wide_bytes": (_SZ, [_U32, ctypes.POINTER(_SZ), ctypes.POINTER(_SZ)]),
-    "cpt_lbvh_wide": (_I32, [ctypes.POINTER(Bvh), _P, _SZ, _P, _SZ, _P, _SZ, _P]),
+    "cpt_lbvh_wide_bytes": (_SZ, [_U32, _U32, ctypes.POINTER(_SZ), ctypes.POINTER(_SZ)]),
+    "cpt_lbvh_wide": (_I32, [ctypes.POINTER(Bvh), _U32, _P, _SZ, _P, _SZ, _P, _SZ, _P]),
     "cpt_emitters_bytes": (_SZ, [_U32, _U32]),
     "cpt_emitters_build": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Scene), _U32, _P, _SZ,
                                   ctypes.POINTER(_U32), _P]),

@@ -13,7 +13,7 @@ import ctypes
 
 from . import (ACCUM_KAHAN, BBOX_DTYPE, RcParams, BUILD_CHECK, TRIANGLE_DTYPE, Bvh, Camera, RenderParams, Scene, View, accum_bytes,
                bvh_bind, bvh_bytes, check, emitters_build, emitters_bytes, lbvh_build, lbvh_scratch_bytes, lib, render, render_scratch_bytes, resolve,
-               status_check, texture_handles, trace)
+               status_check, texture_handles, trace, WIDE_SAH)
 
 
 def stream_handle(stream: torch.cuda.Stream | None = None) -> int:
@@ -67,13 +67,15 @@ class DeviceLbvh:
         off = self.bvh.status - self.mem.data_ptr()
         return self.mem[off:off + 16].cpu().numpy().view(np.uint32).copy()
 
-    def wide(self, stream: int | None = None, keep_scratch: bool = False) -> None:
+    def wide(self, stream: int | None = None, keep_scratch: bool = False, sah: bool = False) -> None:
         """Builds the compressed 8-wide traversal tree (cpt_lbvh_wide) from the binary
         tree in use (the split tree when one was built); tracing and rendering then
-        traverse it. Call again after every build or split."""
+        traverse it. Call again after every build or split. sah: the surface-area
+        collapse (CPT_WIDE_SAH; a slower build, a faster traversal)."""
         leaves = self.bvh.split_capacity if self.bvh.split_nodes else self.n
+        flags = WIDE_SAH if sah else 0
         nb, tb = ctypes.c_size_t(), ctypes.c_size_t()
-        sb = int(lib.cpt_lbvh_wide_bytes(leaves, ctypes.byref(nb), ctypes.byref(tb)))
+        sb = int(lib.cpt_lbvh_wide_bytes(leaves, flags, ctypes.byref(nb), ctypes.byref(tb)))
         if not sb:
             raise ValueError("wide BVH parameters rejected")
         dev = self.mem.device
@@ -83,7 +85,7 @@ class DeviceLbvh:
             self.wide_tris = dev_bytes(tb.value, dev)
         if getattr(self, "wide_scratch", None) is None or self.wide_scratch.numel() < sb:
             self.wide_scratch = dev_bytes(sb, dev)
-        check(lib.cpt_lbvh_wide(ctypes.byref(self.bvh), self.wide_nodes.data_ptr(), self.wide_nodes.numel(),
+        check(lib.cpt_lbvh_wide(ctypes.byref(self.bvh), flags, self.wide_nodes.data_ptr(), self.wide_nodes.numel(),
                                 self.wide_tris.data_ptr(), self.wide_tris.numel(), self.wide_scratch.data_ptr(),
                                 self.wide_scratch.numel(), stream_handle() if stream is None else stream),
               "cpt_lbvh_wide")

@@ -642,13 +642,13 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
     if (t->wide) {
         const uint32_t leaves = S.bvh.split_nodes ? S.bvh.split_capacity : n;
         size_t nb = 0, tb = 0;
-        const size_t sb = cpt_lbvh_wide_bytes(leaves, &nb, &tb);
+        const size_t sb = cpt_lbvh_wide_bytes(leaves, 0, &nb, &tb);
         if (!sb) return CPT_ERR_INVALID_ARGUMENT;
         if ((rc = ensure(&S.d_wide_nodes, &S.wide_nodes_cap, nb))) return rc;
         if ((rc = ensure(&S.d_wide_tris, &S.wide_tris_cap, tb))) return rc;
         if ((rc = ensure(&S.d_wide_scratch, &S.wide_scratch_cap, sb))) return rc;
-        rc = cpt_lbvh_wide(&S.bvh, S.d_wide_nodes, S.wide_nodes_cap, S.d_wide_tris, S.wide_tris_cap, S.d_wide_scratch,
-                           S.wide_scratch_cap, t->build_stream);
+        rc = cpt_lbvh_wide(&S.bvh, 0, S.d_wide_nodes, S.wide_nodes_cap, S.d_wide_tris, S.wide_tris_cap,
+                           S.d_wide_scratch, S.wide_scratch_cap, t->build_stream);
         if (rc) return rc;
     }
     CPT_CUDA_TRY(cudaEventRecord(S.ev_built, t->build_stream));

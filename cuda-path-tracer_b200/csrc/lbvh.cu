@@ -396,7 +396,8 @@ int build_impl(const cpt_triangle* tris_in, uint32_t n, const float* host_box, c
         CPT_PROF(K_TOPOLOGY, stream);
         k_topology<K><<<(inner + 255) / 256, 256, 0, stream>>>(keys, n, nullptr, bvh->children, bvh->parents_leaf,
                                                                 bvh->parents_internal, s.counters,
-                                                                static_cast<float4*>(bvh->nodes), bvh->status);
+                                                                static_cast<float4*>(bvh->nodes), bvh->status,
+                                                                inner);
     }
     CPT_LAUNCH_CHECK();
     {

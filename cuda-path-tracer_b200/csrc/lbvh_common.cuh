@@ -106,16 +106,26 @@ __device__ __forceinline__ void topology_node(const K* __restrict__ keys, int nn
     if (i == 0) parents_internal[0] = CPT_INVALID_INDEX;
 }
 
+// Node word of a traversal record past the tree's last internal node (a tree over fewer
+// leaves than its arrays hold, the split tree): no valid node word has both type bits and
+// an all-ones left index.
+constexpr uint32_t kUnusedNode = 0xFFFFFFFFu;
+
+// node_cap: the internal-node records of `nodes`; those past the tree get kUnusedNode.
 template <typename K>
 __global__ void __launch_bounds__(256) k_topology(const K* __restrict__ keys, uint32_t n_arg,
                                                   const uint32_t* __restrict__ n_ptr, uint32_t* __restrict__ children,
                                                   uint32_t* __restrict__ parents_leaf,
                                                   uint32_t* __restrict__ parents_internal, int* __restrict__ counters,
-                                                  float4* __restrict__ nodes, const uint32_t* __restrict__ status)
+                                                  float4* __restrict__ nodes, const uint32_t* __restrict__ status,
+                                                  uint32_t node_cap)
 {
     const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int nn = (int)(n_ptr ? *n_ptr : n_arg);
-    if (i >= nn - 1) return;
+    if (i >= nn - 1) {
+        if ((uint32_t)i < node_cap) nodes[6 * (size_t)i + 5] = make_float4(__uint_as_float(kUnusedNode), 0.f, 0.f, 0.f);
+        return;
+    }
     if (sort_timed_out(status)) return;  // the keys are not sorted: build nothing from them
     topology_node(keys, nn, i, children, parents_leaf, parents_internal, counters, nodes);
 }

@@ -1015,7 +1015,7 @@ int split_impl(cpt_bvh* bvh, uint32_t cap, bool treelet, void* nodes, void* scra
     const uint32_t* order = s.vals[(P - 1) & 1];
     k_topology<K><<<(cap + 255) / 256, 256, 0, stream>>>(keys, 0, s.n_pieces, s.children, s.parents_leaf,
                                                           s.parents_internal, s.counters, static_cast<float4*>(nodes),
-                                                          bvh->status);
+                                                          bvh->status, cap - 1);
     CPT_LAUNCH_CHECK();
     k_split_refit<<<(cap + kSplitRefitBlock - 1) / kSplitRefitBlock, kSplitRefitBlock, 0, stream>>>(
         bvh->tris, s.pieces, order, s.n_pieces, s.children,

@@ -512,10 +512,12 @@ __device__ __forceinline__ bool wide_step(WideState& s, uint2* smem_col, uint2* 
                                           bool test_tri = true)
 {
     if (test_tri && (s.tbits & kWideRecBits)) {
-        const uint32_t rb = __ffs(s.tbits) - 1;  // bit 8j + slot (the leaf mask lies above)
-        s.tbits &= ~(1u << rb);
-        const uint32_t lm = s.tbits >> 24;
-        const uint32_t idx = s.tbase + (rb >> 3) * __popc(lm) + __popc(lm & ((1u << (rb & 7u)) - 1u));
+        // the lowest record bit, 8j + slot (the leaf mask lies above): record j * L + rank
+        // of the slot = the set bits below it in the leaf mask copied into bytes 0-2
+        const uint32_t t1 = s.tbits - 1u;
+        const uint32_t below = (s.tbits ^ t1) >> 1;
+        const uint32_t idx = s.tbase + __popc(((s.tbits >> 24) * 0x010101u) & below);
+        s.tbits &= t1;
         if (idx >= s.tri_cap) { overflow = true; return true; }
         const float4 a = __ldg(s.tris + 3 * (size_t)idx), b = __ldg(s.tris + 3 * (size_t)idx + 1),
                      c = __ldg(s.tris + 3 * (size_t)idx + 2);

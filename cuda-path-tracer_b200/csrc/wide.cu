@@ -52,17 +52,49 @@ constexpr int kWideLevels = 96;
 constexpr uint32_t kLeafRef = 0x80000000u;
 constexpr int kCtrWords = 4 + kWideLevels + 2;  // alloc nodes, alloc tris, done blocks, margin | level bounds
 
+// Surface-area collapse (flag CPT_WIDE_SAH): which binary nodes become a wide node's children is
+// chosen by the cost of each subtree as at most i children of a wide node, i = 1..8,
+// computed bottom-up over the binary tree (Ylitie, Karras and Laine, "Efficient
+// Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs", HPG 2017, section
+// 3.1, restated): for node n with children a, b and box area A,
+//   D(n, j) = min over k in 1..j-1 of C(a, k) + C(b, j - k)
+//   C(n, 1) = min(A * kSahNode + D(n, 8),                       n a wide node
+//                 A * kSahPrim * P(n) if P(n) <= kWideRecordLayers)  n one leaf slot
+//   C(n, j) = min(D(n, j), C(n, j - 1)) for j >= 2
+// with a binary leaf costing its (clipped) box area times kSahPrim for every j, and
+// P(n) the leaves under n. Without the flag the collapse opens the internal child of
+// largest area until the node has 8 children.
+#ifndef CPT_WIDE_SAH_PRIM
+#define CPT_WIDE_SAH_PRIM 0.3f
+#endif
+constexpr float kSahNode = 1.0f, kSahPrim = CPT_WIDE_SAH_PRIM;
+// choice word of a binary internal node: bit 0 one leaf slot; bit j - 1 (j = 2..8): C(n, j)
+// = C(n, j - 1); bits 8 + 3 (j - 2): the k of D(n, j); bits 29-30: P(n), at most 3
+__device__ __forceinline__ bool sah_leaf(uint32_t c) { return c & 1u; }
+__device__ __forceinline__ bool sah_reduce(uint32_t c, int j) { return (c >> (j - 1)) & 1u; }
+__device__ __forceinline__ int sah_split(uint32_t c, int j) { return (int)((c >> (8 + 3 * (j - 2))) & 7u); }
+__device__ __forceinline__ uint32_t sah_leaves(uint32_t c) { return (c >> 29) & 3u; }
+
 struct WideScratch {
     float4* queue;  // per wide node: (box lo, binary node) (box hi, 0)
     uint32_t* ctr;
+    uint32_t* parent;  // per binary internal node (CPT_WIDE_SAH only): its parent, arrivals, choice word
+    uint32_t* arrive;
+    uint32_t* choice;
+    float* cost;       // C(n, 1..8)
 };
 
-size_t wide_scratch_layout(uint32_t leaves, void* base, WideScratch* out)
+size_t wide_scratch_layout(uint32_t leaves, bool sah, void* base, WideScratch* out)
 {
     Carver c(base);
     WideScratch s;
-    s.queue = c.take<float4>(2ull * std::max<uint32_t>(leaves - 1, 1u));
+    const size_t internal = std::max<uint32_t>(leaves - 1, 1u);
+    s.queue = c.take<float4>(2 * internal);
     s.ctr = c.take<uint32_t>(kCtrWords);
+    s.parent = sah ? c.take<uint32_t>(internal) : nullptr;
+    s.arrive = sah ? c.take<uint32_t>(internal) : nullptr;
+    s.choice = sah ? c.take<uint32_t>(internal) : nullptr;
+    s.cost = sah ? c.take<float>(8 * internal) : nullptr;
     if (out) *out = s;
     return c.used();
 }
@@ -196,6 +228,115 @@ __device__ __forceinline__ void emit_records(const float4* __restrict__ bin, uin
     }
 }
 
+// Parents of the binary internal nodes and zeroed arrival counters (CPT_WIDE_SAH).
+__global__ void k_sah_init(const float4* __restrict__ bin, uint32_t bin_internal, uint32_t* __restrict__ parent,
+                           uint32_t* __restrict__ arrive)
+{
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= bin_internal) return;
+    const float4 f = bin[6 * (size_t)n + 5];
+    const uint32_t word = __float_as_uint(f.x), right = __float_as_uint(f.y);
+    arrive[n] = 0;
+    if (n == 0) parent[0] = CPT_INVALID_INDEX;  // the root (no node has it as a child)
+    if (word == kUnusedNode) return;            // a record past the tree (split tree below its capacity)
+    if ((word & 1u) && (word >> 2) < bin_internal) parent[word >> 2] = n;
+    if ((word & 2u) && right < bin_internal) parent[right] = n;
+}
+
+// C(n, 1..8) and the choice word of binary internal node n from its children's (see
+// CPT_WIDE_SAH); an internal child's table is final (its walk arrived before this one).
+__device__ void sah_node(const float4* __restrict__ bin, uint32_t bin_internal, const uint32_t* __restrict__ parent,
+                         uint32_t* __restrict__ choice, float* __restrict__ cost, uint32_t n)
+{
+    float w[24];
+    read_record(bin, n, w);
+    const uint32_t word = __float_as_uint(w[20]);
+    // n's box: its slot in the parent's record, or for the root the union of its children
+    float nb[6];
+    const uint32_t p = parent[n];
+    if (p < bin_internal) {
+        const float* pr = reinterpret_cast<const float*>(bin + 6 * (size_t)p);
+        const uint32_t pw = __float_as_uint(pr[20]);
+        const int side = ((pw & 1u) && (pw >> 2) == n) ? 0 : 1;
+        for (int k = 0; k < 6; ++k) nb[k] = pr[10 * side + k];
+    } else {
+        const float inf[6] = {-FLT_MAX, -FLT_MAX, -FLT_MAX, FLT_MAX, FLT_MAX, FLT_MAX};
+        for (int a = 0; a < 3; ++a) { nb[a] = FLT_MAX; nb[3 + a] = -FLT_MAX; }
+        for (int side = 0; side < 2; ++side) {
+            float bx[6];
+            uint32_t ref;
+            child_of(w, n, inf, side, bx, ref);
+            for (int a = 0; a < 3; ++a) { nb[a] = fminf(nb[a], bx[a]); nb[3 + a] = fmaxf(nb[3 + a], bx[3 + a]); }
+        }
+    }
+    float tc[2][8];
+    uint32_t pc[2];
+    for (int side = 0; side < 2; ++side) {
+        const bool internal = side ? (word & 2u) : (word & 1u);
+        const uint32_t c = side ? __float_as_uint(w[21]) : (word >> 2);
+        if (internal && c < bin_internal) {
+            for (int i = 0; i < 8; ++i) tc[side][i] = __ldcg(cost + 8 * (size_t)c + i);
+            pc[side] = sah_leaves(__ldcg(choice + c));
+        } else {
+            float bx[6];
+            uint32_t ref;
+            child_of(w, n, nb, side, bx, ref);
+            const float leaf = box_area(bx) * kSahPrim;
+            for (int i = 0; i < 8; ++i) tc[side][i] = leaf;
+            pc[side] = 1;
+        }
+    }
+    float d[9];
+    uint32_t ch = 0;
+    for (int j = 2; j <= 8; ++j) {
+        float best = FLT_MAX;
+        int bk = 1;
+        for (int k = 1; k < j; ++k) {
+            const float v = tc[0][k - 1] + tc[1][j - k - 1];
+            if (v < best) { best = v; bk = k; }
+        }
+        d[j] = best;
+        ch |= (uint32_t)bk << (8 + 3 * (j - 2));
+    }
+    const float area = box_area(nb);
+    const uint32_t leaves = min(3u, pc[0] + pc[1]);
+    const float c_node = area * kSahNode + d[8];
+    const float c_leaf = leaves <= kWideRecordLayers ? area * kSahPrim * (float)leaves : FLT_MAX;
+    ch |= leaves << 29;
+    float c = c_node;
+    if (c_leaf <= c_node) { c = c_leaf; ch |= 1u; }
+    cost[8 * (size_t)n] = c;
+    for (int j = 2; j <= 8; ++j) {
+        if (d[j] < c) c = d[j];
+        else ch |= 1u << (j - 1);
+        cost[8 * (size_t)n + j - 1] = c;
+    }
+    choice[n] = ch;
+}
+
+// The cost tables bottom-up: a walk starts at every node with two leaf children and goes
+// up while it is the last of a node's internal children to arrive (as the refit).
+__global__ void k_sah_up(const float4* __restrict__ bin, uint32_t bin_internal, const uint32_t* __restrict__ parent,
+                         uint32_t* __restrict__ arrive, uint32_t* __restrict__ choice, float* __restrict__ cost,
+                         uint32_t* __restrict__ status)
+{
+    uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= bin_internal) return;
+    if (__ldcg(status) & CPT_STATUS_TIMEOUT) return;  // no tree to walk (a sort gave up)
+    if (__float_as_uint(bin[6 * (size_t)n + 5].x) & 3u) return;  // (kUnusedNode has both type bits)
+    for (uint32_t steps = 0; steps < bin_internal; ++steps) {
+        sah_node(bin, bin_internal, parent, choice, cost, n);
+        const uint32_t p = parent[n];
+        if (p >= bin_internal) return;  // the root
+        __threadfence();
+        const uint32_t need = __popc(__float_as_uint(bin[6 * (size_t)p + 5].x) & 3u);
+        if (atomicAdd(&arrive[p], 1u) + 1u < need) return;
+        __threadfence();
+        n = p;
+    }
+    atomicOr(status, CPT_STATUS_BAD_INDEX);  // a cycle: not a tree
+}
+
 // Smallest e with ext <= 253 * 2^e (e in [-126, 127]): the 255 quanta of a byte less
 // one quantum of slack on each side.
 __device__ __forceinline__ int scale_exp(double ext)
@@ -216,7 +357,8 @@ __device__ __forceinline__ void wide_level_nodes(const float4* __restrict__ bin,
                                                  uint32_t* __restrict__ ctr, uint32_t start, uint32_t end, float m,
                                                  uint32_t node_cap, uint32_t tri_cap, uint32_t bin_internal,
                                                  uint32_t* __restrict__ status, float (*s_box)[kWideBlock],
-                                                 uint32_t (*s_ref)[kWideBlock])
+                                                 uint32_t (*s_ref)[kWideBlock],
+                                                 const uint32_t* __restrict__ choice)  // null: the greedy collapse
 {
     const int t = threadIdx.x;
     if (end > node_cap) {  // (only when the binary tree was not one: allocations past the cap were refused)
@@ -228,44 +370,87 @@ __device__ __forceinline__ void wide_level_nodes(const float4* __restrict__ bin,
         const uint32_t b = __float_as_uint(q0.w);
         const float nb[6] = {q0.x, q0.y, q0.z, q1.x, q1.y, q1.z};
         if (b >= bin_internal) { atomicOr(status, CPT_STATUS_BAD_INDEX); continue; }
-        // frontier: the binary node's children, then open the largest internal one
         int count = 0;
-        {
-            float w[24];
-            read_record(bin, b, w);
-            for (int side = 0; side < 2; ++side) {
-                float bx[6];
-                uint32_t ref;
-                child_of(w, b, nb, side, bx, ref);
-                for (int k = 0; k < 6; ++k) s_box[6 * count + k][t] = bx[k];
-                s_ref[count][t] = ref;
-                ++count;
+        if (choice) {
+            // frontier: the binary node's children with the budgets of D(b, 8), then every
+            // child whose budget (after the C(n, j) = C(n, j - 1) steps) is 2 or more is
+            // replaced by its own two children with the budgets of its D(n, j)
+            int budget[8];
+            {
+                float w[24];
+                read_record(bin, b, w);
+                const int k = sah_split(__ldcg(choice + b), 8);
+                for (int side = 0; side < 2; ++side) {
+                    float bx[6];
+                    uint32_t ref;
+                    child_of(w, b, nb, side, bx, ref);
+                    for (int q = 0; q < 6; ++q) s_box[6 * count + q][t] = bx[q];
+                    s_ref[count][t] = ref;
+                    budget[count] = side ? 8 - k : k;
+                    ++count;
+                }
             }
-        }
-        while (count < 8) {
-            int best = -1;
-            float best_area = -1.f;
-            for (int i = 0; i < count; ++i) {
-                if (s_ref[i][t] & kLeafRef) continue;
-                float bx[6];
-                for (int k = 0; k < 6; ++k) bx[k] = s_box[6 * i + k][t];
-                const float a = box_area(bx);
-                if (a > best_area) { best_area = a; best = i; }
+            for (int i = 0; i < count;) {
+                const uint32_t c = s_ref[i][t];
+                if ((c & kLeafRef) || c >= bin_internal) { ++i; continue; }
+                const uint32_t cc = __ldcg(choice + c);
+                int j = budget[i];
+                while (j >= 2 && sah_reduce(cc, j)) --j;
+                if (j < 2 || count >= 8) { ++i; continue; }  // one child: a wide node or a leaf slot
+                const int k = sah_split(cc, j);
+                float pb[6];
+                for (int q = 0; q < 6; ++q) pb[q] = s_box[6 * i + q][t];
+                float w[24];
+                read_record(bin, c, w);
+                for (int side = 0; side < 2; ++side) {
+                    float bx[6];
+                    uint32_t ref;
+                    child_of(w, c, pb, side, bx, ref);
+                    const int slot = side == 0 ? i : count++;
+                    for (int q = 0; q < 6; ++q) s_box[6 * slot + q][t] = bx[q];
+                    s_ref[slot][t] = ref;
+                    budget[slot] = side ? j - k : k;
+                }
             }
-            if (best < 0) break;
-            const uint32_t c = s_ref[best][t];
-            if (c >= bin_internal) { atomicOr(status, CPT_STATUS_BAD_INDEX); break; }
-            float pb[6];
-            for (int k = 0; k < 6; ++k) pb[k] = s_box[6 * best + k][t];
-            float w[24];
-            read_record(bin, c, w);
-            for (int side = 0; side < 2; ++side) {
-                float bx[6];
-                uint32_t ref;
-                child_of(w, c, pb, side, bx, ref);
-                const int slot = side == 0 ? best : count++;
-                for (int k = 0; k < 6; ++k) s_box[6 * slot + k][t] = bx[k];
-                s_ref[slot][t] = ref;
+        } else {
+            // frontier: the binary node's children, then open the largest internal one
+            {
+                float w[24];
+                read_record(bin, b, w);
+                for (int side = 0; side < 2; ++side) {
+                    float bx[6];
+                    uint32_t ref;
+                    child_of(w, b, nb, side, bx, ref);
+                    for (int k = 0; k < 6; ++k) s_box[6 * count + k][t] = bx[k];
+                    s_ref[count][t] = ref;
+                    ++count;
+                }
+            }
+            while (count < 8) {
+                int best = -1;
+                float best_area = -1.f;
+                for (int i = 0; i < count; ++i) {
+                    if (s_ref[i][t] & kLeafRef) continue;
+                    float bx[6];
+                    for (int k = 0; k < 6; ++k) bx[k] = s_box[6 * i + k][t];
+                    const float a = box_area(bx);
+                    if (a > best_area) { best_area = a; best = i; }
+                }
+                if (best < 0) break;
+                const uint32_t c = s_ref[best][t];
+                if (c >= bin_internal) { atomicOr(status, CPT_STATUS_BAD_INDEX); break; }
+                float pb[6];
+                for (int k = 0; k < 6; ++k) pb[k] = s_box[6 * best + k][t];
+                float w[24];
+                read_record(bin, c, w);
+                for (int side = 0; side < 2; ++side) {
+                    float bx[6];
+                    uint32_t ref;
+                    child_of(w, c, pb, side, bx, ref);
+                    const int slot = side == 0 ? best : count++;
+                    for (int k = 0; k < 6; ++k) s_box[6 * slot + k][t] = bx[k];
+                    s_ref[slot][t] = ref;
+                }
             }
         }
         // quantization frame
@@ -310,7 +495,10 @@ __device__ __forceinline__ void wide_level_nodes(const float4* __restrict__ bin,
         uint32_t cnt_of[8];
         uint32_t imask = 0, m1 = 0, m2 = 0, m3 = 0;
         for (int i = 0; i < count; ++i) {
-            cnt_of[i] = leaf_records(bin, s_ref[i][t], bin_internal);
+            const uint32_t ref = s_ref[i][t];
+            cnt_of[i] = (!choice || (ref & kLeafRef) || (ref < bin_internal && sah_leaf(__ldcg(choice + ref))))
+                            ? leaf_records(bin, ref, bin_internal)
+                            : 0u;
             const uint32_t bit = 1u << slot_of[i];
             if (!cnt_of[i]) imask |= bit;
             if (cnt_of[i] >= 1) m1 |= bit;
@@ -376,7 +564,8 @@ __global__ void __launch_bounds__(kWideBlock) k_wide_levels(const float4* __rest
                                                             float4* __restrict__ tris, float4* __restrict__ queue,
                                                             uint32_t* __restrict__ ctr, uint32_t node_cap,
                                                             uint32_t tri_cap, uint32_t bin_internal,
-                                                            uint32_t* __restrict__ status)
+                                                            uint32_t* __restrict__ status,
+                                                            const uint32_t* __restrict__ choice)
 {
     __shared__ float s_box[8 * 6][kWideBlock];
     __shared__ uint32_t s_ref[8][kWideBlock];
@@ -390,7 +579,7 @@ __global__ void __launch_bounds__(kWideBlock) k_wide_levels(const float4* __rest
     int level = 0;
     for (; level < kWideLevels && start < end; ++level) {
         wide_level_nodes(bin, wide, tris, queue, ctr, start, end, m, node_cap, tri_cap, bin_internal, status, s_box,
-                         s_ref);
+                         s_ref, choice);
         grid.sync();
         const uint32_t next = __ldcg(&ctr[0]);  // every node allocated so far: final after the barrier
         grid.sync();
@@ -417,23 +606,24 @@ __global__ void k_wide_check(const uint32_t* __restrict__ ctr, uint32_t* __restr
 
 using namespace cpt;
 
-extern "C" size_t cpt_lbvh_wide_bytes(uint32_t leaves, size_t* node_bytes, size_t* tri_bytes)
+extern "C" size_t cpt_lbvh_wide_bytes(uint32_t leaves, uint32_t flags, size_t* node_bytes, size_t* tri_bytes)
 {
+    if (flags & ~CPT_WIDE_SAH) return 0;
     if (leaves < 2 || leaves > 0xFFFFFFFFu / kWideRecordLayers) return 0;
     if (node_bytes) *node_bytes = align_up((size_t)(leaves - 1) * 80, 256);
     if (tri_bytes) *tri_bytes = align_up((size_t)leaves * kWideRecordLayers * 48, 256);
-    return wide_scratch_layout(leaves, nullptr, nullptr);
+    return wide_scratch_layout(leaves, flags & CPT_WIDE_SAH, nullptr, nullptr);
 }
 
-extern "C" int cpt_lbvh_wide(cpt_bvh* bvh, void* nodes, size_t node_bytes, void* tris, size_t tri_bytes, void* scratch,
-                             size_t scratch_bytes, cudaStream_t stream)
+extern "C" int cpt_lbvh_wide(cpt_bvh* bvh, uint32_t flags, void* nodes, size_t node_bytes, void* tris,
+                             size_t tri_bytes, void* scratch, size_t scratch_bytes, cudaStream_t stream)
 {
     CPT_RANGE("cpt_lbvh_wide");
     if (!bvh || !bvh->nodes || !bvh->status || !nodes || !tris || !scratch) return CPT_ERR_INVALID_ARGUMENT;
     const bool split = bvh->split_nodes != nullptr;
     const uint32_t leaves = split ? bvh->split_capacity : bvh->n;
     size_t nb = 0, tb = 0;
-    const size_t need = cpt_lbvh_wide_bytes(leaves, &nb, &tb);
+    const size_t need = cpt_lbvh_wide_bytes(leaves, flags, &nb, &tb);
     if (!need) return CPT_ERR_INVALID_ARGUMENT;
     if (scratch_bytes < need || node_bytes < nb || tri_bytes < tb) return CPT_ERR_SCRATCH_TOO_SMALL;
     if ((reinterpret_cast<uintptr_t>(nodes) & 15) || (reinterpret_cast<uintptr_t>(tris) & 15) ||
@@ -443,10 +633,19 @@ extern "C" int cpt_lbvh_wide(cpt_bvh* bvh, void* nodes, size_t node_bytes, void*
     bvh->wide_tris = nullptr;
     bvh->wide_capacity = 0;
     WideScratch ws;
-    wide_scratch_layout(leaves, scratch, &ws);
+    const bool sah = flags & CPT_WIDE_SAH;
+    wide_scratch_layout(leaves, sah, scratch, &ws);
     const float4* bin = static_cast<const float4*>(split ? bvh->split_nodes : bvh->nodes);
     k_wide_init<<<1, 32, 0, stream>>>(bin, ws.queue, ws.ctr);
     CPT_LAUNCH_CHECK();
+    if (sah) {
+        const uint32_t internal = leaves - 1;
+        const unsigned g = (internal + 255) / 256;
+        k_sah_init<<<g, 256, 0, stream>>>(bin, internal, ws.parent, ws.arrive);
+        CPT_LAUNCH_CHECK();
+        k_sah_up<<<g, 256, 0, stream>>>(bin, internal, ws.parent, ws.arrive, ws.choice, ws.cost, bvh->status);
+        CPT_LAUNCH_CHECK();
+    }
     // one cooperative launch over every level: as many blocks as the largest level can
     // use, no more than can be resident at once
     static int occ[64] = {0};
@@ -471,7 +670,8 @@ extern "C" int cpt_lbvh_wide(cpt_bvh* bvh, void* nodes, size_t node_bytes, void*
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     CPT_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_wide_levels, bin, static_cast<float4*>(nodes), static_cast<float4*>(tris),
-                                    ws.queue, ws.ctr, leaves - 1, leaves * kWideRecordLayers, leaves - 1, bvh->status));
+                                    ws.queue, ws.ctr, leaves - 1, leaves * kWideRecordLayers, leaves - 1, bvh->status,
+                                    static_cast<const uint32_t*>(ws.choice)));
     note_launch();
     k_wide_check<<<1, 32, 0, stream>>>(ws.ctr, bvh->status, bvh->status + 2);
     CPT_LAUNCH_CHECK();

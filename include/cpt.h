@@ -320,9 +320,13 @@ int cpt_render_views(const cpt_view* views, uint32_t n_views, const cpt_render_p
  * exactly equal distances is reported. `leaves` for the sizes: bvh->n, or
  * bvh->split_capacity after cpt_lbvh_split. status[2] / status[3] receive the wide
  * node count and the record positions used. */
-size_t cpt_lbvh_wide_bytes(uint32_t leaves, size_t* node_bytes, size_t* tri_bytes); /* returns scratch bytes */
-int cpt_lbvh_wide(cpt_bvh* bvh, void* nodes, size_t node_bytes, void* tris, size_t tri_bytes, void* scratch,
-                  size_t scratch_bytes, cudaStream_t stream);
+#define CPT_WIDE_SAH 1u /* choose each wide node's children by a surface-area cost computed bottom-up over
+                          the binary tree (a second pass before the collapse, more scratch) instead of
+                          opening the largest child: a slower build for a faster traversal */
+size_t cpt_lbvh_wide_bytes(uint32_t leaves, uint32_t flags, size_t* node_bytes,
+                           size_t* tri_bytes); /* returns scratch bytes */
+int cpt_lbvh_wide(cpt_bvh* bvh, uint32_t flags, void* nodes, size_t node_bytes, void* tris, size_t tri_bytes,
+                  void* scratch, size_t scratch_bytes, cudaStream_t stream);
 
 /* ---- next-event estimation (an extension; no reference counterpart) ----
  * The reference gathers emitted light only where a bounce ray happens to hit an

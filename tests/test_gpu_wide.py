@@ -24,9 +24,12 @@ def trace_pair(lb, d_rays):
     return h.cpu().numpy(), st.cpu().numpy(), a.cpu().numpy()
 
 
+@pytest.mark.parametrize("sah", [False, True])
 @pytest.mark.parametrize("bits", [30, 63])
 @pytest.mark.parametrize("split,flags", [(0.0, 0), (1.25, 0), (1.25, cpt.SPLIT_TREELET)])
-def test_wide_hits_match_binary(cuda, bits, split, flags):
+def test_wide_hits_match_binary(cuda, bits, split, flags, sah):
+    """Both collapses (largest child first; surface-area cost, CPT_WIDE_SAH) over the LBVH
+    and over split trees, whose node arrays hold more records than the tree uses."""
     tris, _ = hairball()
     lb = DeviceLbvh(len(tris), bits)
     lb.build(to_device(tris), check_root=True)
@@ -35,7 +38,7 @@ def test_wide_hits_match_binary(cuda, bits, split, flags):
     rays = np.concatenate([random_rays(20_000, 1), random_rays(10_000, 2, inside=True)])
     d_rays = torch.from_numpy(rays).cuda()
     hb, sb, ab = trace_pair(lb, d_rays)
-    lb.wide()
+    lb.wide(sah=sah)
     hw, sw, aw = trace_pair(lb, d_rays)
     ok, exact = tie_or_equal(hw, hb)
     assert ok.all()
@@ -77,8 +80,8 @@ def test_wide_far_limit_and_zero_direction(cuda):
     assert (hb[:, 0] < 3e38).mean() > 0.1
 
 
-@pytest.mark.parametrize("nee", [False, True])
-def test_wide_render_matches_binary(cuda, nee):
+@pytest.mark.parametrize("nee,sah", [(False, False), (True, False), (False, True)])
+def test_wide_render_matches_binary(cuda, nee, sah):
     tris, infos = hairball(n_hair=30_000)
     cam = cpt.camera_look_at((0.0, 0.35, -3.6), (0.0, 0.0, 0.0), aspect=64 / 48)
     lb = DeviceLbvh(len(tris), 63)
@@ -90,7 +93,7 @@ def test_wide_render_matches_binary(cuda, nee):
     p = make_params(64, 48, 8, 3, 5, 3.0, True, 17, cpt.ACCUM_KAHAN, nee=nee)
     r0 = BatchRenderer([(lb, sc, cam, 64, 48)], p)
     r0.render()
-    lb.wide()
+    lb.wide(sah=sah)
     r1 = BatchRenderer([(lb, sc, cam, 64, 48)], p)
     r1.render()
     torch.cuda.synchronize()
@@ -268,23 +271,28 @@ def test_wide_build_rejects_bad_arguments(cuda):
     lb = DeviceLbvh(len(tris), 30)
     lb.build(to_device(tris))
     nb, tb = ctypes.c_size_t(), ctypes.c_size_t()
-    sb = int(cpt.lib.cpt_lbvh_wide_bytes(lb.n, ctypes.byref(nb), ctypes.byref(tb)))
+    sb = int(cpt.lib.cpt_lbvh_wide_bytes(lb.n, 0, ctypes.byref(nb), ctypes.byref(tb)))
     assert sb > 0 and nb.value >= (lb.n - 1) * 80 and tb.value >= lb.n * 48
-    assert cpt.lib.cpt_lbvh_wide_bytes(1, None, None) == 0
+    assert cpt.lib.cpt_lbvh_wide_bytes(1, 0, None, None) == 0
+    assert cpt.lib.cpt_lbvh_wide_bytes(lb.n, 2, None, None) == 0  # an unknown flag
+    assert cpt.lib.cpt_lbvh_wide_bytes(lb.n, cpt.WIDE_SAH, None, None) > sb  # the cost tables
     nodes = torch.empty(nb.value, dtype=torch.uint8, device="cuda")
     trs = torch.empty(tb.value, dtype=torch.uint8, device="cuda")
     scr = torch.empty(sb, dtype=torch.uint8, device="cuda")
     b = ctypes.byref(lb.bvh)
-    assert cpt.lib.cpt_lbvh_wide(b, nodes.data_ptr(), nb.value - 16, trs.data_ptr(), tb.value, scr.data_ptr(), sb,
+    assert cpt.lib.cpt_lbvh_wide(b, 0, nodes.data_ptr(), nb.value - 16, trs.data_ptr(), tb.value, scr.data_ptr(), sb,
                                  0) == cpt.ERR_SCRATCH_TOO_SMALL
-    assert cpt.lib.cpt_lbvh_wide(b, nodes.data_ptr(), nb.value, trs.data_ptr(), tb.value, scr.data_ptr(), sb - 1,
+    assert cpt.lib.cpt_lbvh_wide(b, 0, nodes.data_ptr(), nb.value, trs.data_ptr(), tb.value, scr.data_ptr(), sb - 1,
                                  0) == cpt.ERR_SCRATCH_TOO_SMALL
-    assert cpt.lib.cpt_lbvh_wide(b, nodes.data_ptr() + 4, nb.value, trs.data_ptr(), tb.value, scr.data_ptr(), sb,
+    assert cpt.lib.cpt_lbvh_wide(b, 0, nodes.data_ptr() + 4, nb.value, trs.data_ptr(), tb.value, scr.data_ptr(), sb,
                                  0) == cpt.ERR_INVALID_ARGUMENT
-    assert cpt.lib.cpt_lbvh_wide(b, None, nb.value, trs.data_ptr(), tb.value, scr.data_ptr(), sb,
+    assert cpt.lib.cpt_lbvh_wide(b, 0, None, nb.value, trs.data_ptr(), tb.value, scr.data_ptr(), sb,
                                  0) == cpt.ERR_INVALID_ARGUMENT
+    assert cpt.lib.cpt_lbvh_wide(b, cpt.WIDE_SAH, nodes.data_ptr(), nb.value, trs.data_ptr(), tb.value, scr.data_ptr(),
+                                 sb, 0) == cpt.ERR_SCRATCH_TOO_SMALL  # the surface-area collapse needs more
     assert not lb.bvh.wide_nodes
-    assert cpt.lib.cpt_lbvh_wide(b, nodes.data_ptr(), nb.value, trs.data_ptr(), tb.value, scr.data_ptr(), sb, 0) == 0
+    assert cpt.lib.cpt_lbvh_wide(b, 0, nodes.data_ptr(), nb.value, trs.data_ptr(), tb.value, scr.data_ptr(), sb,
+                                 0) == 0
     torch.cuda.synchronize()
     lb.status()
     assert lb.bvh.wide_nodes == nodes.data_ptr() and lb.bvh.wide_capacity == lb.n
