@@ -549,9 +549,10 @@ def run_batch(args, w, world, rank, local):
             lb.wide(keep_scratch=True)
     torch.cuda.synchronize()
 
-    from cpt.device import LbvhBatch
+    from cpt.device import LbvhBatch, WideBatch
 
     batch = LbvhBatch([v[0] for v in views], dev)  # every scene's LBVH in one launch sequence
+    wbatch = WideBatch([v[0] for v in views], dev) if args.wide else None  # and every wide tree
     batch.build(keep, boxes, check_root=True)
 
     def rebuild_all():
@@ -559,8 +560,8 @@ def run_batch(args, w, world, rank, local):
         for (lb, _, _, _, _), d, h in zip(views, keep, hair):
             if h:
                 lb.split(split, keep_scratch=True, flags=split_flags(args))
-            if args.wide:
-                lb.wide(keep_scratch=True)
+        if wbatch is not None:
+            wbatch.build()
 
     counter2 = torch.zeros(1, dtype=torch.int32, device=dev)
     p2 = params(best["wave_paths"], best["ray_sort"], **shape)
@@ -592,7 +593,8 @@ def run_batch(args, w, world, rank, local):
     rays2 = sum_over_ranks(float(c2n[0] + c2n[1] + c2n[2]), world)
     built_and_rendered = {"mrays_s": round(rays2 / (ms2 / 1e3) / 1e6, 3), "ms_per_step": round(ms2 / args.steps, 3),
                           "note": "one CUDA graph replay per frame: every scene's LBVH (one batched build, "
-                                  "cpt_lbvh_build_batch), the split trees of the hairball scenes, then the render "
+                                  "cpt_lbvh_build_batch), the split trees of the hairball scenes, every wide tree "
+                                  "(one batched build, cpt_lbvh_wide_batch, largest-child collapse), then the render "
                                   "of all scenes"}
     del graph2, br2
 
@@ -615,7 +617,8 @@ def run_batch(args, w, world, rank, local):
     # split trees of the hairball scenes, the wide trees
     split_ms = max_over_ranks(time_builds(lambda: [v[0].split(split, keep_scratch=True, flags=split_flags(args))
                                                    for v, h in zip(views, hair) if h]), world)
-    wide_ms = max_over_ranks(time_builds(lambda: [v[0].wide(keep_scratch=True) for v in views]), world) \
+    wide_ms = max_over_ranks(time_builds(lambda: wbatch.build()), world) if args.wide else 0.0
+    wide_single_ms = max_over_ranks(time_builds(lambda: [v[0].wide(keep_scratch=True) for v in views]), world) \
         if args.wide else 0.0
     for v in views:
         v[0].status()
@@ -644,7 +647,8 @@ def run_batch(args, w, world, rank, local):
                 "lbvh": {"mtris_s": round(n_tris / build_ms / 1e3, 2), "ms": round(build_ms, 3),
                          "per_scene_calls_ms": round(per_scene_ms, 3),
                          "frame_rebuild_parts_ms": {"lbvh_batch": round(build_ms, 3), "split_trees": round(split_ms, 3),
-                                                    "wide_trees": round(wide_ms, 3)},
+                                                    "wide_trees": round(wide_ms, 3),
+                                                    "wide_trees_per_scene_calls": round(wide_single_ms, 3)},
                          "per_scene_calls_mtris_s": round(n_tris / per_scene_ms / 1e3, 2),
                          "note": "each rank's scenes in one batched build (cpt_lbvh_build_batch; max over ranks); "
                                  "per_scene_calls = the same scenes built by one cpt_lbvh_build call each"},

@@ -144,6 +144,8 @@ _PROTOS = {
     "cpt_resolve": (_I32, [_P, _U32, _U32, _U32, _P, _P]),
     "cpt_lbvh_wide_bytes": (_SZ, [_U32, _U32, ctypes.POINTER(_SZ), ctypes.POINTER(_SZ)]),
     "cpt_lbvh_wide": (_I32, [ctypes.POINTER(Bvh), _U32, _P, _SZ, _P, _SZ, _P, _SZ, _P]),
+    "cpt_lbvh_wide_batch_scratch_bytes": (_SZ, [_P, _U32]),
+    "cpt_lbvh_wide_batch": (_I32, [_P, _U32, _P, _P, _P, _P, _P, _SZ, _P]),
     "cpt_emitters_bytes": (_SZ, [_U32, _U32]),
     "cpt_emitters_build": (_I32, [ctypes.POINTER(Bvh), ctypes.POINTER(Scene), _U32, _P, _SZ,
                                   ctypes.POINTER(_U32), _P]),

@@ -185,6 +185,44 @@ class DeviceScene:
         return self.emitter_count
 
 
+class WideBatch:
+    """cpt_lbvh_wide_batch over a list of DeviceLbvh whose binary trees (LBVH or split
+    tree) are built: their wide trees (largest-child collapse) in one launch sequence.
+    Sized for the trees in use when created; build() again after every rebuild."""
+
+    def __init__(self, lbvhs, device=None):
+        if not lbvhs:
+            raise ValueError("empty batch")
+        self.lbvhs = list(lbvhs)
+        k = len(self.lbvhs)
+        leaves = [lb.bvh.split_capacity if lb.bvh.split_nodes else lb.n for lb in self.lbvhs]
+        self.leaves = (ctypes.c_uint32 * k)(*leaves)
+        for lb, nl in zip(self.lbvhs, leaves):
+            nb, tb = ctypes.c_size_t(), ctypes.c_size_t()
+            if not lib.cpt_lbvh_wide_bytes(nl, 0, ctypes.byref(nb), ctypes.byref(tb)):
+                raise ValueError("wide BVH parameters rejected")
+            dev = lb.mem.device
+            if getattr(lb, "wide_nodes", None) is None or lb.wide_nodes.numel() < nb.value:
+                lb.wide_nodes = dev_bytes(nb.value, dev)
+            if getattr(lb, "wide_tris", None) is None or lb.wide_tris.numel() < tb.value:
+                lb.wide_tris = dev_bytes(tb.value, dev)
+        self.bvh_ptrs = (ctypes.c_void_p * k)(*[ctypes.addressof(lb.bvh) for lb in self.lbvhs])
+        self.nodes = (ctypes.c_void_p * k)(*[lb.wide_nodes.data_ptr() for lb in self.lbvhs])
+        self.node_bytes = (ctypes.c_size_t * k)(*[lb.wide_nodes.numel() for lb in self.lbvhs])
+        self.tris = (ctypes.c_void_p * k)(*[lb.wide_tris.data_ptr() for lb in self.lbvhs])
+        self.tri_bytes = (ctypes.c_size_t * k)(*[lb.wide_tris.numel() for lb in self.lbvhs])
+        self.scratch_bytes = int(lib.cpt_lbvh_wide_batch_scratch_bytes(self.leaves, k))
+        if not self.scratch_bytes:
+            raise ValueError("wide batch rejected (tree count or sizes)")
+        self.scratch = dev_bytes(self.scratch_bytes, device)
+
+    def build(self, stream: int | None = None) -> None:
+        rc = lib.cpt_lbvh_wide_batch(self.bvh_ptrs, len(self.lbvhs), self.nodes, self.node_bytes, self.tris,
+                                     self.tri_bytes, self.scratch.data_ptr(), self.scratch_bytes,
+                                     stream_handle() if stream is None else stream)
+        check(rc, "cpt_lbvh_wide_batch")
+
+
 class LbvhBatch:
     """cpt_lbvh_build_batch over a list of DeviceLbvh (one key width): their LBVHs
     built by one launch sequence; each output is the single build's."""

@@ -140,9 +140,9 @@ __device__ __forceinline__ void child_of(const float w[24], uint32_t parent, con
     }
 }
 
-__global__ void k_wide_init(const float4* __restrict__ bin, float4* __restrict__ queue, uint32_t* __restrict__ ctr)
+// The root of the wide tree queued (level 0), the counters zeroed, the margin m.
+__device__ void wide_init_tree(const float4* __restrict__ bin, float4* __restrict__ queue, uint32_t* __restrict__ ctr)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
     float w[24];
     read_record(bin, 0, w);
     const uint32_t word = __float_as_uint(w[20]);
@@ -169,6 +169,12 @@ __global__ void k_wide_init(const float4* __restrict__ bin, float4* __restrict__
     ctr[2] = 0;  // blocks done in the current level
     ctr[3] = __float_as_uint(margin);
     for (int l = 0; l < kWideLevels + 2; ++l) ctr[4 + l] = l == 0 ? 0u : 1u;  // bounds[0] = 0, bounds[1] = 1
+}
+
+__global__ void k_wide_init(const float4* __restrict__ bin, float4* __restrict__ queue, uint32_t* __restrict__ ctr)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    wide_init_tree(bin, queue, ctr);
 }
 
 // Records a child of a wide node becomes: 1 for a binary leaf; for an internal binary
@@ -358,14 +364,17 @@ __device__ __forceinline__ void wide_level_nodes(const float4* __restrict__ bin,
                                                  uint32_t node_cap, uint32_t tri_cap, uint32_t bin_internal,
                                                  uint32_t* __restrict__ status, float (*s_box)[kWideBlock],
                                                  uint32_t (*s_ref)[kWideBlock],
-                                                 const uint32_t* __restrict__ choice)  // null: the greedy collapse
+                                                 const uint32_t* __restrict__ choice,  // null: the greedy collapse
+                                                 uint32_t rot = 0)  // node start + j goes to thread (j + rot) mod T
 {
     const int t = threadIdx.x;
     if (end > node_cap) {  // (only when the binary tree was not one: allocations past the cap were refused)
         if (blockIdx.x == 0 && t == 0) atomicOr(status, CPT_STATUS_BAD_INDEX);
         end = node_cap;
     }
-    for (uint32_t wi = start + blockIdx.x * kWideBlock + t; wi < end; wi += gridDim.x * kWideBlock) {
+    const uint32_t nt = gridDim.x * kWideBlock, tid = blockIdx.x * kWideBlock + t;
+    const uint32_t first = (tid + nt - rot % nt) % nt;
+    for (uint32_t wi = start + first; wi < end; wi += nt) {
         const float4 q0 = queue[2 * (size_t)wi], q1 = queue[2 * (size_t)wi + 1];
         const uint32_t b = __float_as_uint(q0.w);
         const float nb[6] = {q0.x, q0.y, q0.z, q1.x, q1.y, q1.z};
@@ -601,6 +610,94 @@ __global__ void k_wide_check(const uint32_t* __restrict__ ctr, uint32_t* __restr
     if (counts_out) { counts_out[0] = ctr[0]; counts_out[1] = ctr[1]; }
 }
 
+// ---- batched wide build: the wide trees of several binary trees in one cooperative
+// launch, every level of every tree between the same grid barriers ----
+constexpr uint32_t kWideBatchMax = CPT_MAX_BATCH_SCENES;
+struct WideBatchTree {
+    const float4* bin;
+    float4* wide;
+    float4* tris;
+    float4* queue;
+    uint32_t* ctr;
+    uint32_t* status;
+    uint32_t node_cap, tri_cap, bin_internal;
+};
+struct WideBatch {  // passed by value: a call can be captured in a CUDA graph
+    WideBatchTree t[kWideBatchMax];
+    uint32_t count;
+    uint32_t* bounds;  // per tree: the current level's [start, end)
+};
+
+__global__ void k_wide_init_batch(WideBatch wb)
+{
+    if (threadIdx.x != 0 || blockIdx.x >= wb.count) return;
+    const WideBatchTree& T = wb.t[blockIdx.x];
+    wide_init_tree(T.bin, T.queue, T.ctr);
+    wb.bounds[2 * blockIdx.x] = 0;  // level 0: the root
+    wb.bounds[2 * blockIdx.x + 1] = 1;
+}
+
+// As k_wide_levels, over every tree of the batch: a level's nodes of all trees are
+// numbered one after the other (tree by tree), and node g of that numbering goes to
+// thread g mod (threads of the grid), so the work is shared out whatever the trees'
+// sizes. Block 0 moves every tree to its next level between the two barriers.
+__global__ void __launch_bounds__(kWideBlock) k_wide_levels_batch(WideBatch wb)
+{
+    __shared__ float s_box[8 * 6][kWideBlock];
+    __shared__ uint32_t s_ref[8][kWideBlock];
+    __shared__ uint32_t s_start[kWideBatchMax], s_end[kWideBatchMax], s_rot[kWideBatchMax + 1];
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    const uint32_t n = min(wb.count, kWideBatchMax);
+    int level = 0;
+    for (; level < kWideLevels; ++level) {
+        if (threadIdx.x < n) {
+            const WideBatchTree& T = wb.t[threadIdx.x];
+            const bool skip = __ldcg(T.status) & CPT_STATUS_TIMEOUT;  // (set before the launch: every block agrees)
+            s_start[threadIdx.x] = __ldcg(wb.bounds + 2 * threadIdx.x);
+            s_end[threadIdx.x] = skip ? s_start[threadIdx.x] : __ldcg(wb.bounds + 2 * threadIdx.x + 1);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                s_rot[i] = acc;
+                acc += s_end[i] > s_start[i] ? s_end[i] - s_start[i] : 0u;
+            }
+            s_rot[n] = acc;
+        }
+        __syncthreads();
+        if (s_rot[n] == 0) break;  // every tree done (the same bounds in every block)
+        for (uint32_t i = 0; i < n; ++i) {
+            if (s_end[i] <= s_start[i]) continue;
+            const WideBatchTree& T = wb.t[i];
+            wide_level_nodes(T.bin, T.wide, T.tris, T.queue, T.ctr, s_start[i], s_end[i],
+                             __uint_as_float(__ldcg(&T.ctr[3])), T.node_cap, T.tri_cap, T.bin_internal, T.status,
+                             s_box, s_ref, nullptr, s_rot[i]);
+        }
+        grid.sync();
+        if (blockIdx.x == 0 && threadIdx.x < n) {  // every node allocated so far: final after the barrier
+            wb.bounds[2 * threadIdx.x] = s_end[threadIdx.x];
+            wb.bounds[2 * threadIdx.x + 1] = __ldcg(&wb.t[threadIdx.x].ctr[0]);
+        }
+        grid.sync();
+    }
+    if (blockIdx.x == 0 && threadIdx.x < n && !(__ldcg(wb.t[threadIdx.x].status) & CPT_STATUS_TIMEOUT)) {
+        const WideBatchTree& T = wb.t[threadIdx.x];  // the last bounds, for k_wide_check_batch
+        T.ctr[4 + kWideLevels] = __ldcg(wb.bounds + 2 * threadIdx.x);
+        T.ctr[4 + kWideLevels + 1] = __ldcg(wb.bounds + 2 * threadIdx.x + 1);
+    }
+}
+
+__global__ void k_wide_check_batch(WideBatch wb)
+{
+    const uint32_t i = threadIdx.x;
+    if (i >= wb.count) return;
+    const WideBatchTree& T = wb.t[i];
+    if (T.ctr[4 + kWideLevels + 1] != T.ctr[4 + kWideLevels]) atomicOr(T.status, CPT_STATUS_STACK_OVERFLOW);
+    T.status[2] = T.ctr[0];
+    T.status[3] = T.ctr[1];
+}
+
 }  // namespace
 }  // namespace cpt
 
@@ -678,5 +775,98 @@ extern "C" int cpt_lbvh_wide(cpt_bvh* bvh, uint32_t flags, void* nodes, size_t n
     bvh->wide_nodes = nodes;
     bvh->wide_tris = tris;
     bvh->wide_capacity = leaves;
+    return CPT_OK;
+}
+
+extern "C" size_t cpt_lbvh_wide_batch_scratch_bytes(const uint32_t* leaves, uint32_t trees)
+{
+    if (!leaves || trees < 1 || trees > kWideBatchMax) return 0;
+    size_t total = align_up(2 * sizeof(uint32_t) * kWideBatchMax, 256);  // the level bounds
+    for (uint32_t i = 0; i < trees; ++i) {
+        const size_t one = cpt_lbvh_wide_bytes(leaves[i], 0, nullptr, nullptr);
+        if (!one) return 0;
+        total += one;
+    }
+    return total;
+}
+
+extern "C" int cpt_lbvh_wide_batch(cpt_bvh* const* bvhs, uint32_t trees, void* const* nodes, const size_t* node_bytes,
+                                   void* const* tris, const size_t* tri_bytes, void* scratch, size_t scratch_bytes,
+                                   cudaStream_t stream)
+{
+    CPT_RANGE("cpt_lbvh_wide_batch");
+    if (!bvhs || !nodes || !node_bytes || !tris || !tri_bytes || !scratch || trees < 1 || trees > kWideBatchMax)
+        return CPT_ERR_INVALID_ARGUMENT;
+    if (reinterpret_cast<uintptr_t>(scratch) & 255) return CPT_ERR_INVALID_ARGUMENT;
+    WideBatch wb = {};
+    wb.count = trees;
+    char* base = static_cast<char*>(scratch);
+    size_t off = align_up(2 * sizeof(uint32_t) * kWideBatchMax, 256);
+    wb.bounds = reinterpret_cast<uint32_t*>(base);
+    uint64_t total_internal = 0;
+    for (uint32_t i = 0; i < trees; ++i) {
+        cpt_bvh* bvh = bvhs[i];
+        if (!bvh || !bvh->nodes || !bvh->status || !nodes[i] || !tris[i]) return CPT_ERR_INVALID_ARGUMENT;
+        if ((reinterpret_cast<uintptr_t>(nodes[i]) & 15) || (reinterpret_cast<uintptr_t>(tris[i]) & 15))
+            return CPT_ERR_INVALID_ARGUMENT;
+        const bool split = bvh->split_nodes != nullptr;
+        const uint32_t leaves = split ? bvh->split_capacity : bvh->n;
+        size_t nb = 0, tb = 0;
+        const size_t one = cpt_lbvh_wide_bytes(leaves, 0, &nb, &tb);
+        if (!one) return CPT_ERR_INVALID_ARGUMENT;
+        if (node_bytes[i] < nb || tri_bytes[i] < tb || off + one > scratch_bytes) return CPT_ERR_SCRATCH_TOO_SMALL;
+        WideScratch ws;
+        wide_scratch_layout(leaves, false, base + off, &ws);
+        off += one;
+        WideBatchTree& T = wb.t[i];
+        T.bin = static_cast<const float4*>(split ? bvh->split_nodes : bvh->nodes);
+        T.wide = static_cast<float4*>(nodes[i]);
+        T.tris = static_cast<float4*>(tris[i]);
+        T.queue = ws.queue;
+        T.ctr = ws.ctr;
+        T.status = bvh->status;
+        T.node_cap = leaves - 1;
+        T.tri_cap = leaves * kWideRecordLayers;
+        T.bin_internal = leaves - 1;
+        total_internal += leaves - 1;
+    }
+    for (uint32_t i = 0; i < trees; ++i) {
+        bvhs[i]->wide_nodes = nullptr;
+        bvhs[i]->wide_tris = nullptr;
+        bvhs[i]->wide_capacity = 0;
+    }
+    k_wide_init_batch<<<trees, 32, 0, stream>>>(wb);
+    CPT_LAUNCH_CHECK();
+    static int occ[64] = {0};
+    int dev = 0;
+    CPT_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return CPT_ERR_INVALID_ARGUMENT;
+    if (!occ[dev]) {
+        int o = 0;
+        CPT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_wide_levels_batch, kWideBlock, 0));
+        occ[dev] = std::max(1, o);
+    }
+    const uint64_t widest = std::min<uint64_t>(total_internal, (uint64_t)sm_count() * occ[dev] * kWideBlock);
+    const int blocks = (int)std::max<uint64_t>(1, (widest + kWideBlock - 1) / kWideBlock);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(kWideBlock);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CPT_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_wide_levels_batch, wb));
+    note_launch();
+    k_wide_check_batch<<<1, kWideBatchMax, 0, stream>>>(wb);
+    CPT_LAUNCH_CHECK();
+    for (uint32_t i = 0; i < trees; ++i) {
+        cpt_bvh* bvh = bvhs[i];
+        bvh->wide_nodes = nodes[i];
+        bvh->wide_tris = tris[i];
+        bvh->wide_capacity = bvh->split_nodes ? bvh->split_capacity : bvh->n;
+    }
     return CPT_OK;
 }

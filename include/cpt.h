@@ -327,6 +327,19 @@ size_t cpt_lbvh_wide_bytes(uint32_t leaves, uint32_t flags, size_t* node_bytes,
                            size_t* tri_bytes); /* returns scratch bytes */
 int cpt_lbvh_wide(cpt_bvh* bvh, uint32_t flags, void* nodes, size_t node_bytes, void* tris, size_t tri_bytes,
                   void* scratch, size_t scratch_bytes, cudaStream_t stream);
+/* The wide trees of `trees` (1..CPT_MAX_BATCH_SCENES) built binary trees in one fixed
+ * launch sequence — one cooperative launch walks the levels of all of them — instead of
+ * `trees` cpt_lbvh_wide calls (the largest-child collapse, flags 0): for many small
+ * scenes rebuilt every frame. Host arrays of `trees` entries: bvhs, and each tree's node
+ * and record buffers with their sizes (as cpt_lbvh_wide_bytes gives for that tree);
+ * leaves[i] for the scratch size as for cpt_lbvh_wide. The kernels receive the tree
+ * table by value, so a call can be captured in a CUDA graph. Each tree's wide tree is the
+ * one cpt_lbvh_wide builds from it (node and record counts in its status[2] / status[3];
+ * only where nodes are placed in its arrays may differ). */
+size_t cpt_lbvh_wide_batch_scratch_bytes(const uint32_t* leaves, uint32_t trees);
+int cpt_lbvh_wide_batch(cpt_bvh* const* bvhs, uint32_t trees, void* const* nodes, const size_t* node_bytes,
+                        void* const* tris, const size_t* tri_bytes, void* scratch, size_t scratch_bytes,
+                        cudaStream_t stream);
 
 /* ---- next-event estimation (an extension; no reference counterpart) ----
  * The reference gathers emitted light only where a bounce ray happens to hit an

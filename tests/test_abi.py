@@ -153,6 +153,7 @@ def test_every_entry_point_refuses_null_arguments():
         "cpt_bvh_bind": lambda: L.cpt_bvh_bind(None, 0, 10, 30, None),
         "cpt_status_check": lambda: L.cpt_status_check(None, None),
         "cpt_lbvh_wide": lambda: L.cpt_lbvh_wide(None, 0, None, 0, None, 0, None, 0, None),
+        "cpt_lbvh_wide_batch": lambda: L.cpt_lbvh_wide_batch(None, 1, None, None, None, None, None, 0, None),
         "cpt_emitters_build": lambda: L.cpt_emitters_build(None, None, 4, None, 0, None, None),
         "cpt_render": lambda: L.cpt_render(None, None, None, None, None, None, 0, None, None, None),
         "cpt_render_views": lambda: L.cpt_render_views(None, 0, None, None, 0, None, None, None),

@@ -296,3 +296,49 @@ def test_wide_build_rejects_bad_arguments(cuda):
     torch.cuda.synchronize()
     lb.status()
     assert lb.bvh.wide_nodes == nodes.data_ptr() and lb.bvh.wide_capacity == lb.n
+
+
+def test_wide_batch_matches_single_builds(cuda):
+    """cpt_lbvh_wide_batch over trees of different kinds and sizes (an LBVH at 30 bits,
+    split trees at 63 bits, a five-triangle LBVH): each tree's wide tree has the node and
+    record counts of its cpt_lbvh_wide build and gives the binary tree's hits; a second
+    batch call after a rebuild gives them again."""
+    from cpt.device import WideBatch
+
+    scenes = [(cpt.scene_random(3000, seed=2)[0], 30, 0.0), (hairball(n_hair=20_000)[0], 63, 1.25),
+              (cpt.scene_random(20_000, seed=6)[0], 63, 1.25), (cpt.scene_random(5, seed=1)[0], 30, 0.0)]
+    lbs, singles = [], []
+    for tris, bits, split in scenes:
+        lb = DeviceLbvh(len(tris), bits)
+        lb.build(to_device(tris), check_root=True)
+        if split:
+            lb.split(split)
+        lb.wide()
+        torch.cuda.synchronize()
+        singles.append(lb.status_words()[2:4].copy())
+        lbs.append(lb)
+    for lb in lbs:
+        lb.unwide()
+    wb = WideBatch(lbs)
+    for _ in range(2):
+        wb.build()
+        torch.cuda.synchronize()
+        for (tris, bits, split), lb, counts in zip(scenes, lbs, singles):
+            lb.status()
+            assert np.array_equal(lb.status_words()[2:4], counts)
+            assert lb.bvh.wide_nodes and lb.bvh.wide_capacity == (lb.bvh.split_capacity if split else lb.n)
+            rays = random_rays(4000, 3, inside=True)
+            d_rays = torch.from_numpy(rays).cuda()
+            hw, _, aw = trace_pair(lb, d_rays)
+            wide_nodes, wide_tris = lb.bvh.wide_nodes, lb.bvh.wide_tris
+            lb.unwide()
+            hb, _, ab = trace_pair(lb, d_rays)
+            ok, _ = tie_or_equal(hw, hb)
+            assert ok.all()
+            assert np.array_equal(aw[:, 0] < 3e38, ab[:, 0] < 3e38)
+            lb.bvh.wide_nodes, lb.bvh.wide_tris = wide_nodes, wide_tris
+            lb.bvh.wide_capacity = lb.bvh.split_capacity if split else lb.n
+        for (tris, bits, split), lb in zip(scenes, lbs):  # rebuilt trees drop their wide trees
+            lb.build(to_device(tris))
+            if split:
+                lb.split(split)
