@@ -555,11 +555,27 @@ def run_batch(args, w, world, rank, local):
     wbatch = WideBatch([v[0] for v in views], dev) if args.wide else None  # and every wide tree
     batch.build(keep, boxes, check_root=True)
 
+    # the split trees of different scenes are independent: built on a few side streams
+    # forked from the frame's stream (and joined before the wide trees), so that the
+    # small scenes' kernels run side by side
+    split_streams = [torch.cuda.Stream(dev) for _ in range(max(1, args.split_streams))]
+
+    def split_all():
+        cur = torch.cuda.current_stream()
+        for st in split_streams:
+            st.wait_stream(cur)
+        j = 0
+        for (lb, _, _, _, _), h in zip(views, hair):
+            if h:
+                lb.split(split, keep_scratch=True, flags=split_flags(args),
+                         stream=split_streams[j % len(split_streams)].cuda_stream)
+                j += 1
+        for st in split_streams:
+            cur.wait_stream(st)
+
     def rebuild_all():
         batch.build(keep, boxes)
-        for (lb, _, _, _, _), d, h in zip(views, keep, hair):
-            if h:
-                lb.split(split, keep_scratch=True, flags=split_flags(args))
+        split_all()
         if wbatch is not None:
             wbatch.build()
 
@@ -593,7 +609,8 @@ def run_batch(args, w, world, rank, local):
     rays2 = sum_over_ranks(float(c2n[0] + c2n[1] + c2n[2]), world)
     built_and_rendered = {"mrays_s": round(rays2 / (ms2 / 1e3) / 1e6, 3), "ms_per_step": round(ms2 / args.steps, 3),
                           "note": "one CUDA graph replay per frame: every scene's LBVH (one batched build, "
-                                  "cpt_lbvh_build_batch), the split trees of the hairball scenes, every wide tree "
+                                  "cpt_lbvh_build_batch), the split trees of the hairball scenes (on "
+                                  f"{len(split_streams)} forked streams), every wide tree "
                                   "(one batched build, cpt_lbvh_wide_batch, largest-child collapse), then the render "
                                   "of all scenes"}
     del graph2, br2
@@ -615,8 +632,7 @@ def run_batch(args, w, world, rank, local):
     per_scene_ms = max_over_ranks(time_builds(lambda: [v[0].build(d) for v, d in zip(views, keep)]), world)
     # the frame's rebuild part by part (outside the graph): the batched LBVH build, the
     # split trees of the hairball scenes, the wide trees
-    split_ms = max_over_ranks(time_builds(lambda: [v[0].split(split, keep_scratch=True, flags=split_flags(args))
-                                                   for v, h in zip(views, hair) if h]), world)
+    split_ms = max_over_ranks(time_builds(split_all), world)
     wide_ms = max_over_ranks(time_builds(lambda: wbatch.build()), world) if args.wide else 0.0
     wide_single_ms = max_over_ranks(time_builds(lambda: [v[0].wide(keep_scratch=True) for v in views]), world) \
         if args.wide else 0.0
@@ -1380,6 +1396,8 @@ def main():
                     help="1: the surface-area collapse (CPT_WIDE_SAH) for trees built once before the timed frames; "
                          "trees rebuilt inside a timed step always use the faster largest-child collapse "
                          "(default per workload)")
+    ap.add_argument("--split-streams", type=int, default=8,
+                    help="c3: side streams for the split trees of the frame's rebuild (1: one after another)")
     ap.add_argument("--rc-per-sample", action="store_true",
                     help="c4: 2^16 training suffixes per image sample instead of per render call (frame)")
     ap.add_argument("--rc-interval", type=int, default=12,
