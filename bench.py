@@ -1400,7 +1400,7 @@ def main():
                     help="c3: side streams for the split trees of the frame's rebuild (1: one after another)")
     ap.add_argument("--rc-per-sample", action="store_true",
                     help="c4: 2^16 training suffixes per image sample instead of per render call (frame)")
-    ap.add_argument("--rc-interval", type=int, default=12,
+    ap.add_argument("--rc-interval", type=int, default=16,
                     help="radiance cache: train on every n-th frame's own paths (the others only read the cache)")
     ap.add_argument("--rc-warm", type=int, default=None,
                     help="radiance cache: training-only updates before the first cached frame (default per workload)")
