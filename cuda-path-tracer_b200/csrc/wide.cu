@@ -69,11 +69,11 @@ constexpr int kCtrWords = 4 + kWideLevels + 2;  // alloc nodes, alloc tris, done
 #endif
 constexpr float kSahNode = 1.0f, kSahPrim = CPT_WIDE_SAH_PRIM;
 // choice word of a binary internal node: bit 0 one leaf slot; bit j - 1 (j = 2..8): C(n, j)
-// = C(n, j - 1); bits 8 + 3 (j - 2): the k of D(n, j); bits 29-30: P(n), at most 3
+// = C(n, j - 1); bits 8 + 3 (j - 2): the k of D(n, j); bits 29-31: P(n), 7 meaning 7 or more
 __device__ __forceinline__ bool sah_leaf(uint32_t c) { return c & 1u; }
 __device__ __forceinline__ bool sah_reduce(uint32_t c, int j) { return (c >> (j - 1)) & 1u; }
 __device__ __forceinline__ int sah_split(uint32_t c, int j) { return (int)((c >> (8 + 3 * (j - 2))) & 7u); }
-__device__ __forceinline__ uint32_t sah_leaves(uint32_t c) { return (c >> 29) & 3u; }
+__device__ __forceinline__ uint32_t sah_leaves(uint32_t c) { return c >> 29; }
 
 struct WideScratch {
     float4* queue;  // per wide node: (box lo, binary node) (box hi, 0)
@@ -305,7 +305,7 @@ __device__ void sah_node(const float4* __restrict__ bin, uint32_t bin_internal, 
         ch |= (uint32_t)bk << (8 + 3 * (j - 2));
     }
     const float area = box_area(nb);
-    const uint32_t leaves = min(3u, pc[0] + pc[1]);
+    const uint32_t leaves = min(7u, pc[0] + pc[1]);
     const float c_node = area * kSahNode + d[8];
     const float c_leaf = leaves <= kWideRecordLayers ? area * kSahPrim * (float)leaves : FLT_MAX;
     ch |= leaves << 29;
