@@ -759,6 +759,38 @@ def run_ours(args, w, world, rank, local):
             lb.wide(keep_scratch=True)
     rend = DeviceRenderer(params, dev)
     stream = torch.cuda.current_stream()
+    # Pipelined rebuild (the deforming workload, LBVH trees): two trees and two triangle
+    # buffers; frame f renders tree f % 2 while a side stream deforms and builds frame
+    # f + 1's into the other (after the render that last read it). The renderers read
+    # the tree through one view struct that takes the current tree's fields at each frame.
+    pipelined = deforming and args.c5_pipeline and split <= 0 and not args.wide
+    view = lb
+    if pipelined:
+        import ctypes as _ct
+
+        class _ViewTree:
+            bvh = cpt.Bvh()
+
+        view = _ViewTree()
+        _ct.memmove(_ct.addressof(view.bvh), _ct.addressof(lb.bvh), _ct.sizeof(cpt.Bvh))
+        trees = [lb, DeviceLbvh(n, w["bits"], dev)]
+        tri_bufs = [d_tris, torch.empty_like(d_tris)]
+        bstream = torch.cuda.Stream(dev)
+        ev_built = [torch.cuda.Event(), torch.cuda.Event()]
+        ev_read = [torch.cuda.Event(), torch.cuda.Event()]
+        for e in ev_read:
+            e.record(stream)
+
+        def build_tree(frame_index, slot, st):
+            cpt.check(cpt.lib.cpt_scene_deform(d_rest.data_ptr(), tri_bufs[slot].data_ptr(), n, w["amp"], w["omega"],
+                                               0.1 * frame_index, st.cuda_stream), "cpt_scene_deform")
+            trees[slot].build(tri_bufs[slot], stream=st.cuda_stream)
+            ev_built[slot].record(st)
+
+        def use_tree(slot):
+            stream.wait_event(ev_built[slot])
+            _ct.memmove(_ct.addressof(view.bvh), _ct.addressof(trees[slot].bvh), _ct.sizeof(cpt.Bvh))
+
     cached = None
     if w.get("cache"):
         # every camera is a view of the same BVH; the cache trains on all of them
@@ -767,7 +799,7 @@ def run_ours(args, w, world, rank, local):
         rcache = RadianceCache()
         cparams = make_params(W_, H_, spp, 0, w["bounces"], 3.0, True, w["seed"], cpt.ACCUM_KAHAN,
                               wave_paths=args.wave_paths)
-        cached = CachedRenderer(rcache, [(lb, scene, c_, W_, H_) for c_ in cams], cparams, dev)
+        cached = CachedRenderer(rcache, [(view, scene, c_, W_, H_) for c_ in cams], cparams, dev)
 
     # --- one instrumented frame: node fetches and triangle tests per closest-hit ray
     rend.reset()
@@ -790,12 +822,27 @@ def run_ours(args, w, world, rank, local):
         if cached is not None:
             cached.render(frame0=f0)
         else:
-            rend.render(lb, scene, cam, frame0=f0)
+            rend.render(view, scene, cam, frame0=f0)
 
+    def pipelined_step(frame_index, f0):
+        # render frame_index with its tree; build frame_index + 1's beside it
+        cur = frame_index % 2
+        use_tree(cur)
+        frame_step(f0)
+        ev_read[cur].record(stream)
+        nxt = 1 - cur
+        bstream.wait_event(ev_read[nxt])  # the render of frame_index - 1 read that tree
+        build_tree(frame_index + 1, nxt, bstream)
+
+    if pipelined:
+        build_tree(0, 0, stream)
     for i in range(args.warmup):
-        if deforming:
-            deform_and_rebuild(i)
-        frame_step(rank_frame0(frame, rank))
+        if pipelined:
+            pipelined_step(i, rank_frame0(frame, rank))
+        else:
+            if deforming:
+                deform_and_rebuild(i)
+            frame_step(rank_frame0(frame, rank))
         frame += spp
     torch.cuda.synchronize()
     rend.counts.zero_()
@@ -817,13 +864,18 @@ def run_ours(args, w, world, rank, local):
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for k in range(args.steps):
-        if deforming:
-            deform_and_rebuild(args.warmup + k)
-        frame_step(rank_frame0(frame, rank))
+        if pipelined:
+            pipelined_step(args.warmup + k, rank_frame0(frame, rank))
+        else:
+            if deforming:
+                deform_and_rebuild(args.warmup + k)
+            frame_step(rank_frame0(frame, rank))
         frame += spp
         if world > 1:  # the one exchange of the path: framebuffer reduce to rank 0 every frame
             for acc, disp in zip(my_accums, display):
                 reduce_accumulator(acc, disp, dst=0, mode=cpt.ACCUM_KAHAN)
+    if pipelined:
+        stream.wait_stream(bstream)  # the build of the next frame, started in the last step
     ev1.record(stream)
     torch.cuda.synchronize()
     prof = cpt.profile_end()
@@ -936,6 +988,13 @@ def run_ours(args, w, world, rank, local):
             "roofline": {"bound": "hbm", "achieved": round(b_ach, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(b_ach / peak, 4), "bytes_per_triangle": bpt},
             "kernel_ms_per_build": {k: round(v[0] / nb, 4) for k, v in sorted(bprof.items())}}
+    if args.dump_accum and rank == 0:  # the first view's Kahan accumulator after the timed frames (checks)
+        torch.cuda.synchronize()
+        np.save(args.dump_accum, my_accums[0].cpu().numpy())
+    if deforming and pipelined:
+        lbvh["note"] = ("every frame's rebuild (deform + cpt_lbvh_build) runs on a side stream beside the previous "
+                        "frame's render (two trees): these kernel times include that contention; the uncontended "
+                        "build of this mesh is the C2 line's builds_c5_c3.c5_rebuild")
 
     # --- end to end through the tracer object (host buffers, pinned)
     e2e = None
@@ -1396,6 +1455,11 @@ def main():
                     help="1: the surface-area collapse (CPT_WIDE_SAH) for trees built once before the timed frames; "
                          "trees rebuilt inside a timed step always use the faster largest-child collapse "
                          "(default per workload)")
+    ap.add_argument("--dump-accum", default=None, help="save the first view's accumulator after the timed frames "
+                                                        "(a .npy path; for checks)")
+    ap.add_argument("--c5-pipeline", type=int, default=1,
+                    help="c5: build frame f+1's tree on a side stream while frame f renders (two trees); 0: rebuild "
+                         "then render, one after the other")
     ap.add_argument("--split-streams", type=int, default=8,
                     help="c3: side streams for the split trees of the frame's rebuild (1: one after another)")
     ap.add_argument("--rc-per-sample", action="store_true",

@@ -342,3 +342,21 @@ def test_wide_batch_matches_single_builds(cuda):
             lb.build(to_device(tris))
             if split:
                 lb.split(split)
+
+
+def test_wide_sah_collapse_does_not_cost_node_fetches(cuda):
+    """The surface-area collapse fetches no more wide nodes per ray than the largest-child
+    collapse, within a tenth, on a split hairball (a guard against a cost model that
+    lets subtrees too large for one leaf slot compete as leaf slots)."""
+    tris, _ = hairball(n_hair=30_000)
+    lb = DeviceLbvh(len(tris), 63)
+    lb.build(to_device(tris), check_root=True)
+    lb.split(1.25)
+    d_rays = torch.from_numpy(random_rays(20_000, 5, inside=True)).cuda()
+    lb.wide()
+    hg, sg, _ = trace_pair(lb, d_rays)
+    lb.wide(sah=True)
+    hs, ss, _ = trace_pair(lb, d_rays)
+    ok, _ = tie_or_equal(hs, hg)
+    assert ok.all()
+    assert ss[:, 0].mean() <= 1.1 * sg[:, 0].mean(), (ss[:, 0].mean(), sg[:, 0].mean())
