@@ -39,7 +39,7 @@ WORKLOADS = {
                # every e2e step rebuilds the trees inside its timed region: there the cheaper build wins
                e2e_split=4.0, e2e_treelet=0),
     "c1": dict(kind="random", n=65536, bits=30, width=512, height=512, spp=1, bounces=3, eye=(0.5, 0.5, -1.2),
-               target=(0.5, 0.5, 0.0), seed=0),
+               target=(0.5, 0.5, 0.0), seed=0, wide=1, wide_sah=1),
     # 64 scenes, 10k-2M triangles (log-uniform, alternating generators), 256^2-1024^2, one graph launch per frame
     "c3": dict(kind="batch", scenes=64, tri_min=10_000, tri_max=2_000_000, res_min=256, res_max=1024, spp=4,
                bounces=5, bits=63, seed=0, width=0, height=0, split=1.25, wide=1, wide_sah=1),
