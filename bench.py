@@ -763,7 +763,7 @@ def run_ours(args, w, world, rank, local):
     # buffers; frame f renders tree f % 2 while a side stream deforms and builds frame
     # f + 1's into the other (after the render that last read it). The renderers read
     # the tree through one view struct that takes the current tree's fields at each frame.
-    pipelined = deforming and args.c5_pipeline and split <= 0 and not args.wide
+    pipelined = deforming and args.c5_pipeline and split <= 0
     view = lb
     if pipelined:
         import ctypes as _ct
@@ -785,6 +785,8 @@ def run_ours(args, w, world, rank, local):
             cpt.check(cpt.lib.cpt_scene_deform(d_rest.data_ptr(), tri_bufs[slot].data_ptr(), n, w["amp"], w["omega"],
                                                0.1 * frame_index, st.cuda_stream), "cpt_scene_deform")
             trees[slot].build(tri_bufs[slot], stream=st.cuda_stream)
+            if args.wide:
+                trees[slot].wide(stream=st.cuda_stream, keep_scratch=True)
             ev_built[slot].record(st)
 
         def use_tree(slot):
