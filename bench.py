@@ -46,7 +46,7 @@ WORKLOADS = {
     # radiance cache on the C2 scene: 1 spp frames through the cache vs plain 16 spp, RMSE vs an FP64 image
     "c4": dict(kind="sphere_hairball", nu=2048, nv=1024, n_hair=1 << 20, bits=63, width=1920, height=1080, spp=1,
                bounces=7, eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, plain_spp=64, ref_spp=4096,
-               ref_div=4, warm_updates=2, max_spp=256, split=8.0, wide=1, treelet=1, wide_sah=1),
+               ref_div=4, warm_updates=1, max_spp=256, split=8.0, wide=1, treelet=1, wide_sah=1),
     # deforming 16.8 M-triangle displaced sphere, full rebuild every frame, 8 cameras
     "c5": dict(kind="deform", nu=4096, nv=2048, n_hair=0, bits=63, width=1280, height=720, spp=1, bounces=7,
                eye=(0.0, 0.35, -3.6), target=(0.0, 0.0, 0.0), seed=0, cameras=8, amp=0.01, omega=40.0, cache=True),
