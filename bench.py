@@ -768,8 +768,9 @@ def run_ours(args, w, world, rank, local):
     if pipelined:
         import ctypes as _ct
 
-        class _ViewTree:
-            bvh = cpt.Bvh()
+        class _ViewTree:  # what the renderers read as "the LBVH": a bvh struct
+            def __init__(self):
+                self.bvh = cpt.Bvh()
 
         view = _ViewTree()
         _ct.memmove(_ct.addressof(view.bvh), _ct.addressof(lb.bvh), _ct.sizeof(cpt.Bvh))
