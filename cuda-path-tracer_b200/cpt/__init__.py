@@ -448,9 +448,10 @@ class Tracer:
     def set_split(self, extra_ratio: float, flags: int = 0) -> None:
         check(lib.cpt_tracer_set_split(self._h, float(extra_ratio), int(flags)), "cpt_tracer_set_split")
 
-    def set_wide(self, on: bool) -> None:
-        """Every later upload also builds the compressed wide tree and renders through it."""
-        check(lib.cpt_tracer_set_wide(self._h, int(bool(on))), "cpt_tracer_set_wide")
+    def set_wide(self, on) -> None:
+        """Every later upload also builds the compressed wide tree and renders through it
+        (True / 1; 2: with the surface-area collapse, for a scene uploaded once)."""
+        check(lib.cpt_tracer_set_wide(self._h, int(on)), "cpt_tracer_set_wide")
 
     def set_nee(self, on: bool) -> None:
         """Next-event estimation on / off (restarts the accumulation when it changes)."""

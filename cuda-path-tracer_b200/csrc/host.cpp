@@ -508,7 +508,7 @@ struct cpt_tracer {
     int rendered = -1;  // the scene of the last frame (its status word is the frame's)
     float split_ratio = 0.f;  // 0: traverse the LBVH itself
     uint32_t split_flags = 0;
-    bool wide = false;
+    uint32_t wide = 0;  // 0 off, 1 the largest-child collapse, 2 the surface-area collapse
     bool nee = false;
     void* d_textures = nullptr;  // cudaTextureObject_t handles (the caller owns the textures)
     size_t textures_cap = 0;
@@ -642,12 +642,13 @@ extern "C" int cpt_tracer_upload(cpt_tracer* t, const cpt_triangle* tris, uint32
     if (t->wide) {
         const uint32_t leaves = S.bvh.split_nodes ? S.bvh.split_capacity : n;
         size_t nb = 0, tb = 0;
-        const size_t sb = cpt_lbvh_wide_bytes(leaves, 0, &nb, &tb);
+        const uint32_t wflags = t->wide == 2 ? CPT_WIDE_SAH : 0u;
+        const size_t sb = cpt_lbvh_wide_bytes(leaves, wflags, &nb, &tb);
         if (!sb) return CPT_ERR_INVALID_ARGUMENT;
         if ((rc = ensure(&S.d_wide_nodes, &S.wide_nodes_cap, nb))) return rc;
         if ((rc = ensure(&S.d_wide_tris, &S.wide_tris_cap, tb))) return rc;
         if ((rc = ensure(&S.d_wide_scratch, &S.wide_scratch_cap, sb))) return rc;
-        rc = cpt_lbvh_wide(&S.bvh, 0, S.d_wide_nodes, S.wide_nodes_cap, S.d_wide_tris, S.wide_tris_cap,
+        rc = cpt_lbvh_wide(&S.bvh, wflags, S.d_wide_nodes, S.wide_nodes_cap, S.d_wide_tris, S.wide_tris_cap,
                            S.d_wide_scratch, S.wide_scratch_cap, t->build_stream);
         if (rc) return rc;
     }
@@ -674,8 +675,8 @@ extern "C" int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio, uint32_t f
 
 extern "C" int cpt_tracer_set_wide(cpt_tracer* t, uint32_t on)
 {
-    if (!t || on > 1) return CPT_ERR_INVALID_ARGUMENT;
-    t->wide = on != 0;
+    if (!t || on > 2) return CPT_ERR_INVALID_ARGUMENT;
+    t->wide = on;
     return CPT_OK;
 }
 

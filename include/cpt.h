@@ -412,7 +412,9 @@ int cpt_tracer_upload_textures(cpt_tracer* t, const cudaTextureObject_t* texture
  * (cpt_lbvh_split with `flags`) and renders through it; 0 (default) renders over the LBVH. */
 int cpt_tracer_set_split(cpt_tracer* t, float extra_ratio, uint32_t flags);
 /* on = 1: every later upload also builds the compressed wide tree (cpt_lbvh_wide) of
- * the traversal tree (after the split tree, when one is set) and renders through it. */
+ * the traversal tree (after the split tree, when one is set) and renders through it;
+ * on = 2: the same with the surface-area collapse (CPT_WIDE_SAH: a longer build, a
+ * faster render; for scenes uploaded once and rendered many times). 0: off. */
 int cpt_tracer_set_wide(cpt_tracer* t, uint32_t on);
 /* on = 1: render with next-event estimation (cpt_render_params.nee); the tracer
  * builds the uploaded scene's emitter table on the next raytrace. Switching

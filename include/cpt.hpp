@@ -297,7 +297,11 @@ public:
     {
         check(cpt_tracer_set_split(m_t, extraRatio, flags), "CUDAPathTracer::setSplit");
     }
-    void setWide(bool on) { check(cpt_tracer_set_wide(m_t, on ? 1u : 0u), "CUDAPathTracer::setWide"); }
+    // sah: the surface-area collapse (a longer build, a faster render; a scene uploaded once)
+    void setWide(bool on, bool sah = false)
+    {
+        check(cpt_tracer_set_wide(m_t, on ? (sah ? 2u : 1u) : 0u), "CUDAPathTracer::setWide");
+    }
     // the accumulated image, width x height RGBA32F (replaces the GL surface)
     std::vector<float> readImage(int screenWidth, int screenHeight)
     {

@@ -113,11 +113,12 @@ def test_wide_render_matches_binary(cuda, nee, sah):
 
 def test_tracer_object_with_wide_tree(cuda):
     """cpt_tracer_set_wide: the tracer builds the wide tree on upload (after the split
-    tree) and its image equals the binary tree's up to exact ties."""
+    tree; 2: with the surface-area collapse) and its image equals the binary tree's up
+    to exact ties."""
     tris, infos = hairball(n_hair=10_000)
     cam = cpt.camera_look_at((0.0, 0.35, -3.6), (0.0, 0.0, 0.0), aspect=64 / 48)
     imgs = []
-    for wide in (False, True):
+    for wide in (0, 1, 2):
         t = cpt.Tracer(63)
         t.set_split(2.0)
         t.set_wide(wide)
@@ -129,8 +130,9 @@ def test_tracer_object_with_wide_tree(cuda):
         b = t.bvh()
         assert b.wide_capacity == (b.split_capacity if wide else 0)
         t.close()
-    differ = (imgs[0].view(np.uint32) != imgs[1].view(np.uint32)).any(-1)
-    assert differ.mean() < 0.002
+    for img in imgs[1:]:
+        differ = (imgs[0].view(np.uint32) != img.view(np.uint32)).any(-1)
+        assert differ.mean() < 0.002
 
 
 def _closest_brute(tris, rays):
