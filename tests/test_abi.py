@@ -130,6 +130,30 @@ def test_split_sizes_and_flags(bits):
         assert sizes(n, ratio, 0)[0] == 0, ratio
 
 
+def test_wide_sizes_and_flags():
+    # wide tree sizing (host-only): nodes for the binary tree's internal nodes, two record
+    # positions per leaf, more scratch with the surface-area collapse's cost tables,
+    # unknown flags refused; the batched build's scratch is the trees' own plus bounds
+    def sizes(leaves, flags):
+        nb, tb = ctypes.c_size_t(), ctypes.c_size_t()
+        sb = cpt.lib.cpt_lbvh_wide_bytes(leaves, flags, ctypes.byref(nb), ctypes.byref(tb))
+        return int(sb), nb.value, tb.value
+
+    leaves = 100_000
+    s0, nb, tb = sizes(leaves, 0)
+    s1, nb1, tb1 = sizes(leaves, cpt.WIDE_SAH)
+    assert s0 > 0 and nb == nb1 >= (leaves - 1) * 80 and tb == tb1 >= 2 * leaves * 48
+    assert s1 - s0 >= 44 * (leaves - 1)  # parent, arrivals, choice word and 8 costs per node
+    assert sizes(leaves, 2)[0] == 0 and sizes(1, 0)[0] == 0
+    arr = (ctypes.c_uint32 * 3)(1000, leaves, 5)
+    b3 = int(cpt.lib.cpt_lbvh_wide_batch_scratch_bytes(arr, 3))
+    assert b3 >= sum(sizes(x, 0)[0] for x in (1000, leaves, 5))
+    assert cpt.lib.cpt_lbvh_wide_batch_scratch_bytes(arr, 0) == 0
+    assert cpt.lib.cpt_lbvh_wide_batch_scratch_bytes(None, 3) == 0
+    assert cpt.lib.cpt_lbvh_wide_batch_scratch_bytes((ctypes.c_uint32 * 65)(*([100] * 65)), 65) == 0
+    assert cpt.lib.cpt_lbvh_wide_batch_scratch_bytes((ctypes.c_uint32 * 2)(100, 1), 2) == 0
+
+
 def test_render_sizes_and_rejections():
     from cpt import RenderParams
     p = RenderParams(64, 48, 4, 0, 3, 3.0, 1, 0, 0, cpt.ACCUM_KAHAN, 0, 0)
